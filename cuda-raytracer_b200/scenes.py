@@ -1,0 +1,445 @@
+"""Seeded synthetic scenes in the reference's JSON scene schema.
+
+Every scene is written as a reference-schema JSON document
+(``{"scene": {"camera", "assets", "shaders"}, "tracer": [...]}``, the schema read
+by src/core/renderer/renderer.hpp:17-23 and src/core/meta/scene.cu:18-219 of
+xlnx/cuda-raytracer) plus one mesh file named by an ``["import", {"path"}]``
+asset.  Meshes are split per material, one group per material name, the way the
+reference's importer splits an imported scene into one Mesh per material
+(src/core/primitive/mesh.cu:332-402).
+
+Mesh file format ``CRM1`` (little-endian)::
+
+    char[4] "CRM1"; u32 n_groups
+    per group: u32 name_len; char name[name_len]; u32 nv; u32 nt;
+               f32 v[nv*3]; f32 n[nv*3]; u32 idx[nt*3]
+
+Geometry conventions shared by all scenes:
+  * z is up; the Cornell-style box is 5.55 units wide (x) and tall (z).
+  * the whole scene is rotated 30 degrees about z so that no flat face has a
+    normal parallel to +-y: the reference builds its shading frame from
+    cross(n, (0,1,0)) (src/core/meta/scene.hpp:48-50), which is NaN for such
+    faces and silently drops their samples.
+  * lights are quads of two equal-area triangles.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import struct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+S = 5.55          # box width/height
+FRONT = -2.6      # y of the wall behind the camera (the box is closed)
+ROT_DEG = 30.0    # rotation about z around the box centre
+
+
+@dataclass
+class Group:
+    name: str
+    v: np.ndarray          # (nv, 3) float32
+    n: np.ndarray          # (nv, 3) float32
+    f: np.ndarray          # (nt, 3) uint32
+
+
+@dataclass
+class SceneDesc:
+    groups: list = field(default_factory=list)
+    spheres: list = field(default_factory=list)     # dicts {o, r, shader}
+    shaders: dict = field(default_factory=dict)     # name -> [Type, props]
+    camera: dict = field(default_factory=dict)
+    width: int = 256
+    height: int = 256
+    spp: int = 64
+    max_bounce: int = 7
+    name: str = "scene"
+
+    @property
+    def n_triangles(self) -> int:
+        return int(sum(len(g.f) for g in self.groups))
+
+
+# ----------------------------------------------------------------------------
+# small geometry helpers
+
+def _rot_matrix(deg: float) -> np.ndarray:
+    a = math.radians(deg)
+    c, s = math.cos(a), math.sin(a)
+    return np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+
+
+_PIVOT = np.array([S / 2, S / 2, 0.0])
+
+
+def _rot_points(p, deg=ROT_DEG):
+    p = np.asarray(p, dtype=np.float64)
+    return (p - _PIVOT) @ _rot_matrix(deg).T + _PIVOT
+
+
+def _rot_dirs(d, deg=ROT_DEG):
+    return np.asarray(d, dtype=np.float64) @ _rot_matrix(deg).T
+
+
+def quad(p0, p1, p2, p3, normal):
+    """Two triangles (p0,p1,p2), (p0,p2,p3) with separate vertices and a flat normal."""
+    v = np.array([p0, p1, p2, p3], dtype=np.float64)
+    n = np.tile(np.asarray(normal, dtype=np.float64), (4, 1))
+    f = np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32)
+    return v, n, f
+
+
+def _merge(parts):
+    vs, ns, fs, off = [], [], [], 0
+    for v, n, f in parts:
+        vs.append(v)
+        ns.append(n)
+        fs.append(f + off)
+        off += len(v)
+    return np.concatenate(vs), np.concatenate(ns), np.concatenate(fs).astype(np.uint32)
+
+
+def _finish(name, v, n, f, rotate=True):
+    if rotate:
+        v = _rot_points(v)
+        n = _rot_dirs(n)
+    n = n / np.linalg.norm(n, axis=1, keepdims=True)
+    return Group(name, v.astype(np.float32), n.astype(np.float32), np.ascontiguousarray(f, dtype=np.uint32))
+
+
+def box_groups(light_x=(2.125, 3.425), light_y=(1.9, 2.95), light_z=S - 0.25, with_light=True,
+               light_name="light"):
+    """Closed box of 10 quads (floor, ceiling, back and front walls split in two;
+    left and right walls whole) plus a light panel hanging 0.25 below the
+    ceiling.  Normals face inward.  The panel hangs clear of the ceiling because
+    the reference's 1024-point light tables include points outside the light's
+    faces (src/core/primitive/mesh.hpp:71-73); a panel flush with the ceiling
+    would put such points a hair away from lit ceiling points and make the
+    reference's estimator heavy-tailed."""
+    lx0, lx1 = light_x
+    ly0, ly1 = light_y
+    y0, y1, zc, ym, xm = FRONT, S, S, 1.5, S / 2
+    white = [
+        quad((0, y0, 0), (S, y0, 0), (S, ym, 0), (0, ym, 0), (0, 0, 1)),            # floor front
+        quad((0, ym, 0), (S, ym, 0), (S, y1, 0), (0, y1, 0), (0, 0, 1)),            # floor back
+        quad((0, y0, zc), (0, ym, zc), (S, ym, zc), (S, y0, zc), (0, 0, -1)),       # ceiling front
+        quad((0, ym, zc), (0, y1, zc), (S, y1, zc), (S, ym, zc), (0, 0, -1)),       # ceiling back
+        quad((0, y1, 0), (xm, y1, 0), (xm, y1, zc), (0, y1, zc), (0, -1, 0)),       # back wall left
+        quad((xm, y1, 0), (S, y1, 0), (S, y1, zc), (xm, y1, zc), (0, -1, 0)),       # back wall right
+        quad((0, y0, 0), (0, y0, zc), (xm, y0, zc), (xm, y0, 0), (0, 1, 0)),        # front wall left
+        quad((xm, y0, 0), (xm, y0, zc), (S, y0, zc), (S, y0, 0), (0, 1, 0)),        # front wall right
+    ]
+    red = [quad((0, y0, 0), (0, y1, 0), (0, y1, zc), (0, y0, zc), (1, 0, 0))]
+    green = [quad((S, y0, 0), (S, y0, zc), (S, y1, zc), (S, y1, 0), (-1, 0, 0))]
+    groups = [
+        _finish("white", *_merge(white)),
+        _finish("red", *_merge(red)),
+        _finish("green", *_merge(green)),
+    ]
+    if with_light:
+        lq = quad((lx0, ly0, light_z), (lx0, ly1, light_z), (lx1, ly1, light_z), (lx1, ly0, light_z), (0, 0, -1))
+        groups.append(_finish(light_name, *lq))
+    return groups
+
+
+def box_shaders(strength=50.0):
+    return {
+        "white": ["Lambert", {"R": [0.73, 0.73, 0.73], "color": [1, 1, 1]}],
+        "red": ["Lambert", {"R": [0.65, 0.05, 0.05], "color": [1, 1, 1]}],
+        "green": ["Lambert", {"R": [0.12, 0.45, 0.15], "color": [1, 1, 1]}],
+        "light": ["Emission", {"color": [1, 1, 1], "strength": float(strength)}],
+    }
+
+
+def box_camera(fovx=40.0):
+    pos = _rot_points([S / 2, FRONT + 0.1, S / 2])
+    tgt = _rot_dirs([0.0, 1.0, 0.0])
+    return {"lens": "pinhole", "fovx": float(fovx), "position": [float(x) for x in pos],
+            "target": [float(x) for x in tgt], "upaxis": [0.0, 0.0, 1.0]}
+
+
+# ----------------------------------------------------------------------------
+# icosphere + value noise
+
+def icosphere(level: int):
+    """Unit icosphere; the 4 children of face f after one split are 4f..4f+3,
+    so face f at level L belongs to base face f // 4**L."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                  [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]],
+                 dtype=np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9],
+                  [5, 11, 4], [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2],
+                  [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+                  [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    for _ in range(level):
+        a, b, c = f[:, 0], f[:, 1], f[:, 2]
+        e = np.stack([np.stack([a, b], 1), np.stack([b, c], 1), np.stack([c, a], 1)], 1).reshape(-1, 2)
+        e.sort(axis=1)
+        key = e[:, 0] * (len(v) + 1) + e[:, 1]
+        uk, inv = np.unique(key, return_inverse=True)
+        ua, ub = uk // (len(v) + 1), uk % (len(v) + 1)
+        mid = v[ua] + v[ub]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        mid_idx = (len(v) + np.arange(len(uk)))[inv].reshape(-1, 3)
+        v = np.concatenate([v, mid])
+        ab, bc, ca = mid_idx[:, 0], mid_idx[:, 1], mid_idx[:, 2]
+        f = np.stack([np.stack([a, ab, ca], 1), np.stack([ab, b, bc], 1),
+                      np.stack([ca, bc, c], 1), np.stack([ab, bc, ca], 1)], 1).reshape(-1, 3)
+    return v, f
+
+
+def value_noise(p: np.ndarray, seed: int, octaves: int = 4, freq: float = 2.0) -> np.ndarray:
+    """Fractal lattice value noise in [-1, 1] (smoothstep-interpolated)."""
+    rng = np.random.default_rng(seed)
+    table = rng.uniform(-1.0, 1.0, 4096)
+    perm = rng.permutation(4096)
+    out = np.zeros(len(p))
+    amp, norm, f = 1.0, 0.0, freq
+    for o in range(octaves):
+        q = p * f + 17.31 * o
+        i0 = np.floor(q).astype(np.int64)
+        w = q - i0
+        w = w * w * (3 - 2 * w)
+        acc = np.zeros(len(p))
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    ix, iy, iz = i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz
+                    h = perm[(ix * 73856093 ^ iy * 19349663 ^ iz * 83492791) & 4095]
+                    wt = (w[:, 0] if dx else 1 - w[:, 0]) * (w[:, 1] if dy else 1 - w[:, 1]) * \
+                         (w[:, 2] if dz else 1 - w[:, 2])
+                    acc += wt * table[h]
+        out += amp * acc
+        norm += amp
+        amp *= 0.5
+        f *= 2.0
+    return out / norm
+
+
+def smooth_normals(v, f):
+    fn = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    n = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(n, f[:, k], fn)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    return n
+
+
+def displaced_icosphere(level, seed, center, radius, amp=0.15):
+    v, f = icosphere(level)
+    d = value_noise(v, seed)
+    v = v * (radius * (1.0 + amp * d))[:, None] + np.asarray(center)[None, :]
+    n = smooth_normals(v, f)
+    return v, n, f
+
+
+def split_groups(v, n, f, face_group, names, rotate=True):
+    """One Group per material id, each with its own compacted vertex set."""
+    out = []
+    for gi, name in enumerate(names):
+        sel = np.nonzero(face_group == gi)[0]
+        if len(sel) == 0:
+            continue
+        ff = f[sel]
+        used, inv = np.unique(ff.reshape(-1), return_inverse=True)
+        out.append(_finish(name, v[used], n[used], inv.reshape(-1, 3), rotate=rotate))
+    return out
+
+
+def _random_material(rng, name_prefix, i, alpha_range=(0.05, 0.8)):
+    if rng.uniform() < 0.5:
+        alb = rng.uniform(0.2, 0.9, 3)
+        return f"{name_prefix}{i:02d}", ["Lambert", {"R": [float(x) for x in alb], "color": [1, 1, 1]}]
+    a = rng.uniform(*alpha_range)
+    col = rng.uniform(0.4, 0.9, 3)
+    return f"{name_prefix}{i:02d}", ["GlossyBSDF", {"distribution": ["Beckmann", {"roughness": float(a)}],
+                                                    "color": [float(x) for x in col]}]
+
+
+# ----------------------------------------------------------------------------
+# the configurations
+
+def config0(width=256, height=256, spp=64) -> SceneDesc:
+    """Box + ceiling light + Beckmann sphere + Lambert sphere (the small case that
+    the reference's CPU tracer renders in seconds)."""
+    sh = box_shaders(50.0)
+    sh["glossy"] = ["GlossyBSDF", {"distribution": ["Beckmann", {"roughness": 0.3}],
+                                   "color": [0.545, 0.463, 0.427]}]
+    sh["ball"] = ["Lambert", {"R": [0.73, 0.73, 0.73], "color": [1, 1, 1]}]
+    spheres = [
+        {"o": [float(x) for x in _rot_points([1.85, 1.7, 1.0])], "r": 1.0, "shader": "glossy"},
+        {"o": [float(x) for x in _rot_points([3.7, 3.5, 1.0])], "r": 1.0, "shader": "ball"},
+    ]
+    return SceneDesc(groups=box_groups(), spheres=spheres, shaders=sh, camera=box_camera(),
+                     width=width, height=height, spp=spp, max_bounce=7, name="config0")
+
+
+def config1(level=8, seed=1, width=1024, height=768, spp=256) -> SceneDesc:
+    """Displaced icosphere (20*4**level triangles) inside the box.  Materials are
+    drawn per icosahedron patch (20 patches), 50 % Lambert albedo U[0.2,0.9]^3 and
+    50 % Beckmann roughness U[0.05,0.8], so that every material group is a
+    spatially compact mesh for the reference's per-mesh BVH."""
+    rng = np.random.default_rng(seed)
+    sh = box_shaders(50.0)
+    names = []
+    for i in range(20):
+        nm, cfg = _random_material(rng, "m", i)
+        names.append(nm)
+        sh[nm] = cfg
+    v, n, f = displaced_icosphere(level, seed, center=(S / 2, 1.7, 1.75), radius=1.45)
+    patch = np.arange(len(f)) // (4 ** level)
+    groups = box_groups() + split_groups(v, n, f, patch, names)
+    return SceneDesc(groups=groups, shaders=sh, camera=box_camera(), width=width, height=height,
+                     spp=spp, max_bounce=7, name=f"config1_l{level}")
+
+
+def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
+    """Occluded light: the box is split by a wall at y=2.6 with a 0.4x0.4 aperture;
+    a single 0.3x0.3 light of strength 400 hangs on the far side; a displaced
+    icosphere (20*4**level triangles, ~330k at level 7) with Beckmann roughness
+    U[0.05,0.5] is the receiver on the camera side."""
+    rng = np.random.default_rng(seed)
+    sh = box_shaders(400.0)
+    names = []
+    for i in range(20):
+        nm, cfg = _random_material(rng, "g", i, alpha_range=(0.05, 0.5))
+        if cfg[0] == "Lambert":
+            a = rng.uniform(0.05, 0.5)
+            cfg = ["GlossyBSDF", {"distribution": ["Beckmann", {"roughness": float(a)}],
+                                  "color": [0.8, 0.8, 0.8]}]
+        names.append(nm)
+        sh[nm] = cfg
+    wall_y = 2.6
+    ax0, ax1, az0, az1 = S / 2 - 0.2, S / 2 + 0.2, 2.6, 3.0
+    groups = box_groups(with_light=False)
+    parts = []
+    for side, nrm in ((wall_y - 1e-3, (0, -1, 0)), (wall_y + 1e-3, (0, 1, 0))):
+        y = side
+        rects = [(0, ax0, 0, S), (ax1, S, 0, S), (ax0, ax1, 0, az0), (ax0, ax1, az1, S)]
+        for x0, x1, z0, z1 in rects:
+            if nrm[1] < 0:
+                parts.append(quad((x0, y, z0), (x0, y, z1), (x1, y, z1), (x1, y, z0), nrm))
+            else:
+                parts.append(quad((x0, y, z0), (x1, y, z0), (x1, y, z1), (x0, y, z1), nrm))
+    groups.append(_finish("divider", *_merge(parts)))
+    sh["divider"] = ["Lambert", {"R": [0.73, 0.73, 0.73], "color": [1, 1, 1]}]
+    lx, ly, lz = S / 2, 4.6, S - 0.25
+    lq = quad((lx - .15, ly - .15, lz), (lx - .15, ly + .15, lz), (lx + .15, ly + .15, lz),
+              (lx + .15, ly - .15, lz), (0, 0, -1))
+    groups.append(_finish("light", *lq))
+    v, n, f = displaced_icosphere(level, seed, center=(S / 2, 0.4, 1.3), radius=1.2)
+    patch = np.arange(len(f)) // (4 ** level)
+    groups += split_groups(v, n, f, patch, names)
+    return SceneDesc(groups=groups, shaders=sh, camera=box_camera(), width=width, height=height,
+                     spp=spp, max_bounce=7, name=f"config3_l{level}")
+
+
+# ----------------------------------------------------------------------------
+# I/O
+
+def write_crm(path, groups):
+    with open(path, "wb") as fh:
+        fh.write(b"CRM1")
+        fh.write(struct.pack("<I", len(groups)))
+        for g in groups:
+            nb = g.name.encode()
+            fh.write(struct.pack("<I", len(nb)))
+            fh.write(nb)
+            fh.write(struct.pack("<II", len(g.v), len(g.f)))
+            fh.write(np.ascontiguousarray(g.v, dtype="<f4").tobytes())
+            fh.write(np.ascontiguousarray(g.n, dtype="<f4").tobytes())
+            fh.write(np.ascontiguousarray(g.f, dtype="<u4").tobytes())
+
+
+def read_crm(path):
+    groups = []
+    with open(path, "rb") as fh:
+        data = fh.read()
+    assert data[:4] == b"CRM1"
+    (ng,), off = struct.unpack_from("<I", data, 4), 8
+    for _ in range(ng):
+        (ln,) = struct.unpack_from("<I", data, off)
+        off += 4
+        name = data[off:off + ln].decode()
+        off += ln
+        nv, nt = struct.unpack_from("<II", data, off)
+        off += 8
+        v = np.frombuffer(data, "<f4", nv * 3, off).reshape(nv, 3)
+        off += nv * 12
+        n = np.frombuffer(data, "<f4", nv * 3, off).reshape(nv, 3)
+        off += nv * 12
+        f = np.frombuffer(data, "<u4", nt * 3, off).reshape(nt, 3)
+        off += nt * 12
+        groups.append(Group(name, v, n, f))
+    return groups
+
+
+def write_obj(path, groups):
+    """Wavefront OBJ with one `usemtl` block per group (for importer tests)."""
+    with open(path, "w") as fh:
+        base = 1
+        for g in groups:
+            fh.write(f"o {g.name}\nusemtl {g.name}\n")
+            for p in g.v:
+                fh.write(f"v {p[0]:.9g} {p[1]:.9g} {p[2]:.9g}\n")
+            for q in g.n:
+                fh.write(f"vn {q[0]:.9g} {q[1]:.9g} {q[2]:.9g}\n")
+            for t in g.f:
+                a, b, c = (int(x) + base for x in t)
+                fh.write(f"f {a}//{a} {b}//{b} {c}//{c}\n")
+            base += len(g.v)
+
+
+def scene_json(desc: SceneDesc, mesh_path: str, tracer="CudaWavefront", estimator=None):
+    kern = {"maxBounce": int(desc.max_bounce)}
+    if estimator:
+        kern["estimator"] = estimator
+    assets = []
+    if desc.groups:
+        assets.append(["import", {"path": mesh_path}])
+    for s in desc.spheres:
+        assets.append(["sphere", {"o": s["o"], "r": s["r"], "shader": s["shader"]}])
+    return {
+        "scene": {"camera": [desc.camera], "assets": assets, "shaders": desc.shaders},
+        "tracer": [tracer, {"kernel": ["Radiance", kern]}],
+    }
+
+
+def write_scene(desc: SceneDesc, out_dir: str, fmt="crm", **kw) -> str:
+    os.makedirs(out_dir, exist_ok=True)
+    mesh_name = f"{desc.name}.{fmt}"
+    if desc.groups:
+        (write_crm if fmt == "crm" else write_obj)(os.path.join(out_dir, mesh_name), desc.groups)
+    path = os.path.join(out_dir, f"{desc.name}.json")
+    with open(path, "w") as fh:
+        json.dump(scene_json(desc, mesh_name, **kw), fh, indent=1)
+    return path
+
+
+# ----------------------------------------------------------------------------
+# camera rays, restating PinholeLens::sample (src/core/misc/lens.hpp:15-27,62-66)
+
+def pinhole_rays(camera, w, h, spp, pixels, ks):
+    """float32 primary rays (o, d) for pixel indices (x, y) and sample indices k."""
+    f32 = np.float32
+    fov = f32(camera.get("fovx", 90.0))
+    tgt = np.asarray(camera.get("target", [-1, 0, 0]), f32)
+    up = np.asarray(camera.get("upaxis", [0, 0, 1]), f32)
+    pos = np.asarray(camera.get("position", [1, 0, 0]), f32)
+    pw = int(math.ceil(math.sqrt(spp)))
+    nrm = lambda a: (a / np.sqrt(np.sum(a * a, axis=-1, keepdims=True))).astype(f32)
+    n = (nrm(tgt) * f32(w) / f32(2 * math.tan(math.radians(float(fov) * 0.5)))).astype(f32)
+    u = nrm(np.cross(n, up))
+    v = nrm(np.cross(n, u))
+    du, dv = (u / f32(pw)).astype(f32), (v / f32(pw)).astype(f32)
+    x = pixels[:, 0].astype(f32)[:, None]
+    y = pixels[:, 1].astype(f32)[:, None]
+    k = np.asarray(ks)
+    t = n[None] + u[None] * (x - f32(w * 0.5)) + v[None] * (y - f32(h * 0.5))
+    d = nrm(t + du[None] * (k % pw).astype(f32)[:, None] + dv[None] * (k // pw).astype(f32)[:, None])
+    o = np.broadcast_to(pos, d.shape).astype(f32)
+    return o, d

@@ -1,0 +1,1131 @@
+// FP64 CPU oracle for the Radiance path of xlnx/cuda-raytracer.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle.h): the checker the CUDA path is
+// compared with.  Every function cites the reference file:line it restates;
+// ORC_MIS functions restate the corrected estimator documented in oracle.h.
+#include "oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace
+{
+constexpr double PI = 3.14159265358979323846;
+constexpr double INF = std::numeric_limits<double>::infinity();
+
+struct V3
+{
+	double x = 0, y = 0, z = 0;
+	V3() = default;
+	V3( double a, double b, double c ) : x( a ), y( b ), z( c ) {}
+	double operator[]( int i ) const { return i == 0 ? x : i == 1 ? y : z; }
+	double &operator[]( int i ) { return i == 0 ? x : i == 1 ? y : z; }
+};
+inline V3 operator+( V3 a, V3 b ) { return { a.x + b.x, a.y + b.y, a.z + b.z }; }
+inline V3 operator-( V3 a, V3 b ) { return { a.x - b.x, a.y - b.y, a.z - b.z }; }
+inline V3 operator-( V3 a ) { return { -a.x, -a.y, -a.z }; }
+inline V3 operator*( V3 a, V3 b ) { return { a.x * b.x, a.y * b.y, a.z * b.z }; }
+inline V3 operator*( V3 a, double s ) { return { a.x * s, a.y * s, a.z * s }; }
+inline V3 operator*( double s, V3 a ) { return a * s; }
+inline V3 operator/( V3 a, double s ) { return { a.x / s, a.y / s, a.z / s }; }
+inline double dot( V3 a, V3 b ) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross( V3 a, V3 b ) { return { a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y }; }
+inline double length( V3 a ) { return std::sqrt( dot( a, a ) ); }
+inline V3 normalize( V3 a ) { return a * ( 1.0 / std::sqrt( dot( a, a ) ) ); }
+inline V3 vmin( V3 a, V3 b ) { return { std::min( a.x, b.x ), std::min( a.y, b.y ), std::min( a.z, b.z ) }; }
+inline V3 vmax( V3 a, V3 b ) { return { std::max( a.x, b.x ), std::max( a.y, b.y ), std::max( a.z, b.z ) }; }
+inline double maxc( V3 a ) { return std::max( a.x, std::max( a.y, a.z ) ); }
+inline bool finite3( V3 a ) { return std::isfinite( a.x ) && std::isfinite( a.y ) && std::isfinite( a.z ); }
+
+// float3 helpers used where the reference computes a stored table in float.
+struct F3
+{
+	float x, y, z;
+};
+inline F3 fadd( F3 a, F3 b ) { return { a.x + b.x, a.y + b.y, a.z + b.z }; }
+inline F3 fsub( F3 a, F3 b ) { return { a.x - b.x, a.y - b.y, a.z - b.z }; }
+inline F3 fmul( F3 a, float s ) { return { a.x * s, a.y * s, a.z * s }; }
+inline F3 fcross( F3 a, F3 b ) { return { a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y }; }
+inline F3 fnormalize( F3 a )
+{
+	float r = 1.0f / std::sqrt( a.x * a.x + a.y * a.y + a.z * a.z );
+	return fmul( a, r );
+}
+
+struct Shader
+{
+	int type;
+	V3 R{ 1, 1, 1 }, color{ 1, 1, 1 };
+	double alpha = 0.5;  // Beckmann roughness (alpha2 = roughness^2, beckmann.hpp:11-17)
+	V3 emission;         // color * strength (emission.hpp:12-20)
+};
+
+struct Tri
+{
+	V3 v0, v1, v2, n0, n1, n2;
+	F3 fv0, fv1, fv2, fn0, fn1, fn2;
+	int prim, index;
+};
+
+struct Prim
+{
+	int kind;  // 0 mesh, 1 sphere
+	int shader;
+	int first_tri = 0, n_tri = 0;
+	V3 c;
+	double r = 0;
+	float fc[ 3 ] = { 0, 0, 0 }, fr = 0;
+	int light = -1;
+};
+
+struct Light
+{
+	int prim;
+	int kind;
+	// ORC_KOISHI mesh table (mesh.hpp:61-84)
+	std::vector<F3> tp, tn;
+	float kpdf = 0;
+	// ORC_MIS area sampling
+	std::vector<double> cdf;
+	double area = 0;
+};
+
+struct Node
+{
+	V3 lo, hi;
+	int left = -1, right = -1, first = 0, count = 0;
+};
+
+struct Camera
+{
+	V3 pos{ 1, 0, 0 }, target{ -1, 0, 0 }, up{ 0, 0, 1 };
+	float fpos[ 3 ] = { 1, 0, 0 }, ftarget[ 3 ] = { -1, 0, 0 }, fup[ 3 ] = { 0, 0, 1 };
+	double fovx = 90;
+};
+
+struct Hit
+{
+	double t = INF, u = 0, v = 0;
+	int tri = -1;   // global triangle (tris[]) or -1
+	int prim = -1;  // prim index
+	V3 sphere_n;
+};
+
+// Splitmix64-based per-sample stream (oracle-only randomness).
+struct Rng
+{
+	uint64_t s;
+	static uint64_t mix( uint64_t z )
+	{
+		z += 0x9E3779B97F4A7C15ull;
+		z = ( z ^ ( z >> 30 ) ) * 0xBF58476D1CE4E5B9ull;
+		z = ( z ^ ( z >> 27 ) ) * 0x94D049BB133111EBull;
+		return z ^ ( z >> 31 );
+	}
+	Rng( uint64_t seed, uint64_t a, uint64_t b ) : s( mix( seed ^ mix( a * 0x100000001B3ull + b ) ) ) {}
+	double next()
+	{
+		s = mix( s );
+		return double( s >> 11 ) * ( 1.0 / 9007199254740992.0 );
+	}
+};
+
+}  // namespace
+
+struct orc_scene
+{
+	std::vector<Shader> shaders;
+	std::vector<Prim> prims;
+	std::vector<Tri> tris;
+	std::vector<int> bvh_tris;
+	std::vector<Node> nodes;
+	std::vector<Light> lights;
+	Camera cam;
+	double scale = 1;
+};
+
+namespace
+{
+// ---------------------------------------------------------------- BVH (speed only)
+void build_bvh( orc_scene *s )
+{
+	s->bvh_tris.resize( s->tris.size() );
+	for ( size_t i = 0; i < s->tris.size(); ++i ) s->bvh_tris[ i ] = int( i );
+	s->nodes.clear();
+	if ( s->tris.empty() ) return;
+	std::vector<V3> cen( s->tris.size() );
+	for ( size_t i = 0; i < s->tris.size(); ++i )
+		cen[ i ] = ( s->tris[ i ].v0 + s->tris[ i ].v1 + s->tris[ i ].v2 ) / 3.0;
+	struct Task
+	{
+		int node, first, count;
+	};
+	std::vector<Task> stack;
+	s->nodes.push_back( Node() );
+	stack.push_back( { 0, 0, int( s->tris.size() ) } );
+	while ( !stack.empty() )
+	{
+		Task t = stack.back();
+		stack.pop_back();
+		V3 lo( INF, INF, INF ), hi( -INF, -INF, -INF ), clo = lo, chi = hi;
+		for ( int i = t.first; i < t.first + t.count; ++i )
+		{
+			const Tri &tr = s->tris[ s->bvh_tris[ i ] ];
+			lo = vmin( lo, vmin( tr.v0, vmin( tr.v1, tr.v2 ) ) );
+			hi = vmax( hi, vmax( tr.v0, vmax( tr.v1, tr.v2 ) ) );
+			clo = vmin( clo, cen[ s->bvh_tris[ i ] ] );
+			chi = vmax( chi, cen[ s->bvh_tris[ i ] ] );
+		}
+		s->nodes[ t.node ].lo = lo;
+		s->nodes[ t.node ].hi = hi;
+		V3 e = chi - clo;
+		int axis = e.x >= e.y && e.x >= e.z ? 0 : e.y >= e.z ? 1 : 2;
+		if ( t.count <= 4 || e[ axis ] <= 0 )
+		{
+			s->nodes[ t.node ].first = t.first;
+			s->nodes[ t.node ].count = t.count;
+			continue;
+		}
+		int mid = t.first + t.count / 2;
+		std::nth_element( s->bvh_tris.begin() + t.first, s->bvh_tris.begin() + mid,
+						  s->bvh_tris.begin() + t.first + t.count,
+						  [&]( int a, int b ) { return cen[ a ][ axis ] < cen[ b ][ axis ]; } );
+		int l = int( s->nodes.size() );
+		s->nodes.push_back( Node() );
+		s->nodes.push_back( Node() );
+		s->nodes[ t.node ].left = l;
+		s->nodes[ t.node ].right = l + 1;
+		stack.push_back( { l, t.first, mid - t.first } );
+		stack.push_back( { l + 1, mid, t.first + t.count - mid } );
+	}
+}
+
+inline bool box_hit( const Node &n, V3 o, V3 inv, double tmax )
+{
+	double t0 = 0, t1 = tmax;
+	for ( int a = 0; a < 3; ++a )
+	{
+		double ta = ( n.lo[ a ] - o[ a ] ) * inv[ a ], tb = ( n.hi[ a ] - o[ a ] ) * inv[ a ];
+		if ( ta > tb ) std::swap( ta, tb );
+		if ( std::isnan( ta ) || std::isnan( tb ) ) continue;
+		t0 = std::max( t0, ta );
+		t1 = std::min( t1, tb );
+	}
+	return t0 <= t1 * ( 1 + 1e-9 ) + 1e-12;
+}
+
+// Moller-Trumbore as in Ray::intersect_triangle (src/core/basic/ray.hpp:37-52):
+// t > 0, u >= 0, v >= 0, u + v <= 1, no epsilon.
+inline bool mt( V3 o, V3 d, V3 v0, V3 e1, V3 e2, double &t, double &u, double &v )
+{
+	V3 T = o - v0, P = cross( d, e2 ), Q = cross( T, e1 );
+	double det = dot( e1, P );
+	double inv = 1.0 / det;
+	u = dot( T, P ) * inv;
+	v = dot( d, Q ) * inv;
+	t = dot( e2, Q ) * inv;
+	return t > 0. && u >= 0. && v >= 0. && u + v <= 1.;
+}
+
+// Sphere::intersect (src/core/primitive/sphere.hpp:31-54): near root, else far
+// root, accepted when t >= 0.
+inline bool sphere_hit( V3 c, double r, V3 o, V3 d, double &t )
+{
+	V3 oc = c - o;
+	double poc = dot( d, oc );
+	double d2 = dot( oc, oc ) - poc * poc;
+	double det = r * r - d2;
+	if ( det < 0 ) return false;
+	det = std::sqrt( det );
+	t = poc - det;
+	if ( t < 0 ) t = poc + det;
+	return t >= 0;
+}
+
+// Closest hit over all primitives (src/core/meta/scene.hpp:35-55), FP64.
+bool intersect( const orc_scene *s, V3 o, V3 d, double tmax, Hit &h )
+{
+	h = Hit();
+	h.t = tmax;
+	bool any = false;
+	if ( !s->nodes.empty() )
+	{
+		V3 inv( 1.0 / d.x, 1.0 / d.y, 1.0 / d.z );
+		int stack[ 128 ];
+		int sp = 0;
+		stack[ sp++ ] = 0;
+		while ( sp )
+		{
+			const Node &n = s->nodes[ stack[ --sp ] ];
+			if ( !box_hit( n, o, inv, h.t ) ) continue;
+			if ( n.left < 0 )
+			{
+				for ( int i = n.first; i < n.first + n.count; ++i )
+				{
+					const Tri &tr = s->tris[ s->bvh_tris[ i ] ];
+					double t, u, v;
+					if ( mt( o, d, tr.v0, tr.v1 - tr.v0, tr.v2 - tr.v0, t, u, v ) && t < h.t )
+					{
+						h.t = t, h.u = u, h.v = v, h.tri = s->bvh_tris[ i ], h.prim = tr.prim;
+						any = true;
+					}
+				}
+			}
+			else
+			{
+				stack[ sp++ ] = n.left;
+				stack[ sp++ ] = n.right;
+			}
+		}
+	}
+	for ( size_t p = 0; p < s->prims.size(); ++p )
+	{
+		const Prim &pr = s->prims[ p ];
+		if ( pr.kind != 1 ) continue;
+		double t;
+		if ( sphere_hit( pr.c, pr.r, o, d, t ) && t < h.t )
+		{
+			h.t = t, h.tri = -1, h.prim = int( p );
+			h.sphere_n = normalize( o + d * t - pr.c );
+			any = true;
+		}
+	}
+	return any;
+}
+
+// Any hit on (tmin, tmax) used by ORC_MIS shadow rays.
+bool occluded_ray( const orc_scene *s, V3 o, V3 d, double tmin, double tmax )
+{
+	if ( !s->nodes.empty() )
+	{
+		V3 inv( 1.0 / d.x, 1.0 / d.y, 1.0 / d.z );
+		int stack[ 128 ];
+		int sp = 0;
+		stack[ sp++ ] = 0;
+		while ( sp )
+		{
+			const Node &n = s->nodes[ stack[ --sp ] ];
+			if ( !box_hit( n, o, inv, tmax ) ) continue;
+			if ( n.left < 0 )
+			{
+				for ( int i = n.first; i < n.first + n.count; ++i )
+				{
+					const Tri &tr = s->tris[ s->bvh_tris[ i ] ];
+					double t, u, v;
+					if ( mt( o, d, tr.v0, tr.v1 - tr.v0, tr.v2 - tr.v0, t, u, v ) && t > tmin && t < tmax )
+						return true;
+				}
+			}
+			else
+			{
+				stack[ sp++ ] = n.left;
+				stack[ sp++ ] = n.right;
+			}
+		}
+	}
+	for ( auto &pr : s->prims )
+	{
+		if ( pr.kind != 1 ) continue;
+		V3 oc = pr.c - o;
+		double poc = dot( d, oc ), det = pr.r * pr.r - ( dot( oc, oc ) - poc * poc );
+		if ( det < 0 ) continue;
+		det = std::sqrt( det );
+		double t0 = poc - det, t1 = poc + det;
+		if ( ( t0 > tmin && t0 < tmax ) || ( t1 > tmin && t1 < tmax ) ) return true;
+	}
+	return false;
+}
+
+// Scene::intersect(Seg) (src/core/meta/scene.hpp:57-67): meshes use
+// Seg::intersect_triangle (src/core/basic/ray.hpp:81-90), a plane-side
+// rejection followed by the ray test; spheres use Primitive::intersect(Seg)
+// (src/core/primitive/primitive.hpp:15-20): ray hit with t <= seg.t.
+bool occluded_seg( const orc_scene *s, V3 o, V3 d, double len )
+{
+	V3 e = o + d * len;
+	if ( !s->nodes.empty() )
+	{
+		V3 lo = vmin( o, e ), hi = vmax( o, e );
+		int stack[ 128 ];
+		int sp = 0;
+		stack[ sp++ ] = 0;
+		while ( sp )
+		{
+			const Node &n = s->nodes[ stack[ --sp ] ];
+			if ( n.hi.x < lo.x || n.hi.y < lo.y || n.hi.z < lo.z || n.lo.x > hi.x || n.lo.y > hi.y ||
+				 n.lo.z > hi.z )
+				continue;
+			if ( n.left < 0 )
+			{
+				for ( int i = n.first; i < n.first + n.count; ++i )
+				{
+					const Tri &tr = s->tris[ s->bvh_tris[ i ] ];
+					V3 d1 = tr.v1 - tr.v0, d2 = tr.v2 - tr.v0;
+					V3 nn = cross( d1, d2 );
+					if ( dot( o - tr.v0, nn ) * dot( e - tr.v0, nn ) > 0 ) continue;
+					double t, u, v;
+					if ( mt( o, d, tr.v0, d1, d2, t, u, v ) ) return true;
+				}
+			}
+			else
+			{
+				stack[ sp++ ] = n.left;
+				stack[ sp++ ] = n.right;
+			}
+		}
+	}
+	for ( auto &pr : s->prims )
+	{
+		if ( pr.kind != 1 ) continue;
+		double t;
+		if ( sphere_hit( pr.c, pr.r, o, d, t ) && t <= len ) return true;
+	}
+	return false;
+}
+
+// ---------------------------------------------------------------- camera
+// PinholeLens::sample (src/core/misc/lens.hpp:15-27,62-66) in FP64.
+struct Lens
+{
+	V3 o, n, u, v, du, dv;
+	double w, h;
+	uint32_t pw;
+	Lens( const Camera &c, uint32_t W, uint32_t H, uint32_t spp )
+	{
+		w = W, h = H;
+		pw = uint32_t( std::ceil( std::sqrt( double( spp ) ) ) );
+		o = c.pos;
+		n = normalize( c.target ) * ( double( W ) / ( 2 * std::tan( c.fovx * PI / 180.0 * 0.5 ) ) );
+		u = normalize( cross( n, c.up ) );
+		v = normalize( cross( n, u ) );
+		du = u / double( pw );
+		dv = v / double( pw );
+	}
+	V3 dir( uint32_t x, uint32_t y, uint32_t k ) const
+	{
+		V3 t = n + u * ( double( x ) - w * .5 ) + v * ( double( y ) - h * .5 );
+		return normalize( t + du * double( k % pw ) + dv * double( k / pw ) );
+	}
+};
+
+// ---------------------------------------------------------------- BSDFs
+// H::sampleCos (src/util/hemisphere.hpp:76-95): concentric disk to cosine lobe.
+V3 sample_cos( double r1, double r2 )
+{
+	double ux = 2. * r1 - 1, uy = 2. * r2 - 1;
+	if ( ux == 0 && uy == 0 ) return { 0, 0, 1 };
+	double r, phi;
+	if ( ux * ux > uy * uy )
+		r = ux, phi = ( PI / 4 ) * ( uy / ux );
+	else
+		r = uy, phi = ( PI / 2 ) - ( ( PI / 4 ) * ( ux / uy ) );
+	return { r * std::cos( phi ), r * std::sin( phi ), std::sqrt( std::max( 0., 1. - r * r ) ) };
+}
+
+// BeckmannDistribution::f (src/ext/distribution/beckmann.hpp:19-24): D(h)|cos th|.
+double beckmann_f( double alpha2, V3 w )
+{
+	double c2 = w.z * w.z;
+	double s2 = std::max( 0., 1 - c2 );
+	double tg2 = s2 / c2;
+	return std::exp( -tg2 / alpha2 ) / ( PI * alpha2 * c2 * c2 ) * std::fabs( w.z );
+}
+
+// BeckmannDistribution::sample (src/ext/distribution/beckmann.hpp:26-38).
+V3 beckmann_sample( double alpha2, double u1, double u2 )
+{
+	double tg2 = -alpha2 * std::log( u1 );
+	double phi = u2 * 2 * PI;
+	double costh = 1. / std::sqrt( 1 + tg2 );
+	double sinth = std::sqrt( std::max( 0., 1. - costh * costh ) );
+	return { sinth * std::sin( phi ), sinth * std::cos( phi ), costh };
+}
+
+inline V3 reflect( V3 I, V3 N ) { return N * ( dot( N, I ) * 2. ) - I; }  // vmath.hpp:470-489
+
+// ORC_KOISHI compute_f_by_wi_wo: Lambert (lambert.hpp:31-33), Glossy
+// (glossy.hpp:27-29), Emission as white Lambert (emission.hpp:22-27).
+V3 k_eval( const Shader &sh, V3 wo, V3 wi )
+{
+	if ( sh.type == ORC_GLOSSY ) return sh.color * beckmann_f( sh.alpha * sh.alpha, normalize( wo + wi ) );
+	V3 c = sh.type == ORC_LAMBERT ? sh.color * sh.R : V3( 1, 1, 1 );
+	return wi.z >= 0 ? c * ( 1.0 / PI ) : V3();
+}
+
+// ORC_KOISHI sample_wi_f_by_wo: Lambert (lambert.hpp:26-30, cosine.hpp:16-25:
+// pdf reported as 1/pi so f = color*R), Glossy (glossy.hpp:22-26).
+void k_sample( const Shader &sh, V3 wo, double u1, double u2, V3 &wi, V3 &f )
+{
+	if ( sh.type == ORC_GLOSSY )
+	{
+		V3 h = beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
+		wi = reflect( wo, h );
+		f = wo.z * wi.z > 0. ? sh.color : V3();
+		return;
+	}
+	wi = sample_cos( u1, u2 );
+	V3 c = sh.type == ORC_LAMBERT ? sh.color * sh.R : V3( 1, 1, 1 );
+	f = wi.z >= 0 ? c : V3();
+}
+
+// ORC_MIS BSDFs: Lambert color*R/pi with cosine pdf; Beckmann microfacet
+// reflection color*D*G/(4 cos_o cos_i) with Walter et al.'s Smith G1 and the
+// half-vector pdf D cos_h / (4 |wo.h|); Emission reflects as white Lambert.
+double smith_g1( double alpha, V3 w )
+{
+	double c = w.z;
+	if ( c <= 0 ) return 0;
+	double s = std::sqrt( std::max( 0., 1 - c * c ) );
+	if ( s == 0 ) return 1;
+	double a = c / ( alpha * s );
+	if ( a >= 1.6 ) return 1;
+	return ( 3.535 * a + 2.181 * a * a ) / ( 1 + 2.276 * a + 2.577 * a * a );
+}
+
+void m_eval( const Shader &sh, V3 wo, V3 wi, V3 &f, double &pdf )
+{
+	f = V3(), pdf = 0;
+	if ( wo.z <= 0 || wi.z <= 0 ) return;
+	if ( sh.type == ORC_GLOSSY )
+	{
+		V3 h = normalize( wo + wi );
+		double a2 = sh.alpha * sh.alpha;
+		double dh = beckmann_f( a2, h ) / std::fabs( h.z );
+		double G = smith_g1( sh.alpha, wo ) * smith_g1( sh.alpha, wi );
+		f = sh.color * ( dh * G / ( 4 * wo.z * wi.z ) );
+		pdf = dh * h.z / ( 4 * std::fabs( dot( wo, h ) ) );
+		return;
+	}
+	V3 c = sh.type == ORC_LAMBERT ? sh.color * sh.R : V3( 1, 1, 1 );
+	f = c * ( 1.0 / PI );
+	pdf = wi.z / PI;
+}
+
+void m_sample( const Shader &sh, V3 wo, double u1, double u2, V3 &wi, V3 &weight, double &pdf )
+{
+	weight = V3(), pdf = 0;
+	if ( sh.type == ORC_GLOSSY )
+	{
+		V3 h = beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
+		wi = reflect( wo, h );
+	}
+	else
+		wi = sample_cos( u1, u2 );
+	if ( wo.z <= 0 || wi.z <= 0 ) return;
+	V3 f;
+	m_eval( sh, wo, wi, f, pdf );
+	if ( pdf > 0 ) weight = f * ( wi.z / pdf );
+}
+
+// Building an orthonormal basis, revisited (Duff et al., JCGT 2017).
+void onb( V3 n, V3 &b1, V3 &b2 )
+{
+	double sign = std::copysign( 1.0, n.z );
+	double a = -1.0 / ( sign + n.z );
+	double b = n.x * n.y * a;
+	b1 = V3( 1.0 + sign * n.x * n.x * a, sign * b, -sign * n.x );
+	b2 = V3( b, sign + n.y * n.y * a, -n.y );
+}
+
+// ---------------------------------------------------------------- integrators
+struct Frame
+{
+	V3 u, v, n;
+	V3 local( V3 w ) const { return normalize( V3( dot( w, u ), dot( w, v ), dot( w, n ) ) ); }
+	V3 global( V3 w ) const { return normalize( u * w.x + v * w.y + n * w.z ); }
+};
+
+// RadianceKernel::execute (src/core/kernel/radiance.cu:14-81), reference semantics.
+V3 radiance_koishi( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
+{
+	V3 L, beta( 1, 1, 1 );
+	const double eps = 4e-3;  // varyings.hpp:19-37
+	size_t nl = s->lights.size();
+	for ( uint32_t bounce = 0;; ++bounce )
+	{
+		Hit h;
+		if ( !intersect( s, o, d, INF, h ) ) break;
+		if ( bounce > max_bounce ) break;
+		const Prim &pr = s->prims[ h.prim ];
+		const Shader &sh = s->shaders[ pr.shader ];
+		V3 n;
+		if ( h.tri >= 0 )
+		{
+			const Tri &t = s->tris[ h.tri ];
+			n = normalize( t.n0 * ( 1 - h.u - h.v ) + t.n1 * h.u + t.n2 * h.v );  // mesh.hpp:85-91
+		}
+		else
+			n = h.sphere_n;
+		Frame fr;  // scene.hpp:48-53
+		fr.n = n;
+		fr.u = normalize( cross( n, V3( 0, 1, 0 ) ) );
+		fr.v = normalize( cross( n, fr.u ) );
+		V3 p = o + d * h.t;
+		V3 wo = fr.local( -d );
+		V3 emission;
+		if ( nl )
+		{
+			// radiance.cu:29-38, AreaLight::sample (areaLight.hpp:19-31),
+			// Primitive::sample(p,u,pdf) (primitive.hpp:25-33)
+			size_t idx = std::min( size_t( std::floor( rng.next() * double( nl ) ) ), nl - 1 );
+			double lpdf = 1.0 / double( nl );
+			double ux = rng.next(), uy = rng.next();
+			const Light &lt = s->lights[ idx ];
+			const Prim &lp = s->prims[ lt.prim ];
+			V3 lpos, lnrm;
+			double pdf;
+			if ( lt.kind == 0 )
+			{
+				size_t k = std::min( size_t( std::floor( ux * 1024 ) ), size_t( 1023 ) );  // mesh.hpp:92-98
+				lpos = V3( lt.tp[ k ].x, lt.tp[ k ].y, lt.tp[ k ].z );
+				lnrm = V3( lt.tn[ k ].x, lt.tn[ k ].y, lt.tn[ k ].z );
+				pdf = lt.kpdf;
+			}
+			else
+			{
+				// Sphere::sample (sphere.hpp:22-30): theta uniform in [0, pi].
+				double th = ux * PI, ph = uy * PI * 2;
+				V3 w( std::sin( th ) * std::sin( ph ), std::sin( th ) * std::cos( ph ), std::cos( th ) );
+				lpos = lp.c + w * lp.r;
+				lnrm = w;
+				pdf = 1. / ( 4 * PI * lp.r * lp.r );
+			}
+			V3 wiw = p - lpos;
+			pdf *= dot( wiw, wiw ) / std::fabs( dot( lnrm, normalize( wiw ) ) );
+			V3 dd = lpos - p;  // LocalVaryings::emitSeg (varyings.hpp:27-37)
+			V3 sd = normalize( dd );
+			V3 diff = normalize( sd ) * eps;
+			V3 so = p + diff;
+			double st = length( dd - 2.0 * diff );
+			V3 li = occluded_seg( s, so, sd, st ) ? V3() : s->shaders[ lp.shader ].emission / pdf;
+			V3 wi = fr.local( normalize( lpos - p ) );
+			V3 f = k_eval( sh, wo, wi );
+			L = L + beta * f * li * ( std::fabs( wi.z ) / lpdf );
+			if ( sh.type == ORC_EMISSION ) emission = sh.emission;
+		}
+		L = L + beta * emission;  // radiance.cu:39
+		// radiance.cu:55-60
+		double u1 = rng.next(), u2 = rng.next();
+		V3 wi, f;
+		k_sample( sh, wo, u1, u2, wi, f );
+		beta = beta * f * std::fabs( wi.z );
+		d = fr.global( wi );
+		o = p + d * eps;
+		// radiance.cu:62-68
+		double rr = maxc( beta );
+		if ( rr < 1. && bounce > 3 )
+		{
+			double q = std::max( .05, 1 - rr );
+			if ( rng.next() < q ) break;
+			beta = beta / ( 1 - q );
+		}
+		if ( beta.x == 0 && beta.y == 0 && beta.z == 0 ) break;
+	}
+	return L;
+}
+
+// Light sampling for ORC_MIS: uniform light choice, area-proportional
+// triangle choice, uniform point on the triangle / sphere.
+void mis_light_sample( const orc_scene *s, const Light &lt, double u0, double u1, double u2, V3 &lp,
+					   V3 &ln, double &pdfA )
+{
+	const Prim &pr = s->prims[ lt.prim ];
+	if ( lt.kind == 1 )
+	{
+		double z = 1 - 2 * u1, r = std::sqrt( std::max( 0., 1 - z * z ) ), ph = 2 * PI * u2;
+		V3 w( r * std::cos( ph ), r * std::sin( ph ), z );
+		lp = pr.c + w * pr.r;
+		ln = w;
+		pdfA = 1.0 / ( 4 * PI * pr.r * pr.r );
+		return;
+	}
+	size_t k = std::upper_bound( lt.cdf.begin(), lt.cdf.end(), u0 * lt.cdf.back() ) - lt.cdf.begin();
+	k = std::min( k, lt.cdf.size() - 1 );
+	const Tri &t = s->tris[ pr.first_tri + k ];
+	double su = std::sqrt( u1 ), b0 = 1 - su, b1 = u2 * su;
+	lp = t.v0 * b0 + t.v1 * b1 + t.v2 * ( 1 - b0 - b1 );
+	ln = normalize( cross( t.v1 - t.v0, t.v2 - t.v0 ) );
+	pdfA = 1.0 / lt.area;
+}
+
+V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
+{
+	V3 L, beta( 1, 1, 1 );
+	size_t nl = s->lights.size();
+	double prev_pdf = 0;
+	for ( uint32_t bounce = 0;; ++bounce )
+	{
+		Hit h;
+		if ( !intersect( s, o, d, INF, h ) ) break;
+		if ( bounce > max_bounce ) break;
+		const Prim &pr = s->prims[ h.prim ];
+		const Shader &sh = s->shaders[ pr.shader ];
+		V3 ns, ng;
+		if ( h.tri >= 0 )
+		{
+			const Tri &t = s->tris[ h.tri ];
+			ns = normalize( t.n0 * ( 1 - h.u - h.v ) + t.n1 * h.u + t.n2 * h.v );
+			ng = normalize( cross( t.v1 - t.v0, t.v2 - t.v0 ) );
+		}
+		else
+			ns = ng = h.sphere_n;
+		V3 p = o + d * h.t;
+		if ( sh.type == ORC_EMISSION )
+		{
+			double w = 1;
+			if ( bounce > 0 )
+			{
+				const Light &lt = s->lights[ pr.light ];
+				double cosl = std::fabs( dot( ng, d ) );
+				double pl = cosl > 0 ? ( h.t * h.t / cosl ) / ( lt.kind == 1 ? 4 * PI * pr.r * pr.r : lt.area ) /
+										 double( nl )
+									 : INF;
+				w = prev_pdf * prev_pdf / ( prev_pdf * prev_pdf + pl * pl );
+			}
+			L = L + beta * sh.emission * w;
+		}
+		if ( dot( ng, d ) > 0 ) ng = -ng, ns = -ns;
+		Frame fr;
+		fr.n = ns;
+		onb( ns, fr.u, fr.v );
+		V3 wo = fr.local( -d );
+		if ( nl )
+		{
+			double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+			size_t idx = std::min( size_t( std::floor( u0 * double( nl ) ) ), nl - 1 );
+			double ur = u0 * double( nl ) - double( idx );
+			const Light &lt = s->lights[ idx ];
+			V3 lp, ln;
+			double pdfA;
+			mis_light_sample( s, lt, ur, u1, u2, lp, ln, pdfA );
+			V3 dw = lp - p;
+			double dist2 = dot( dw, dw ), dist = std::sqrt( dist2 );
+			V3 wiw = dw / dist;
+			double cosl = std::fabs( dot( ln, wiw ) );
+			if ( cosl > 0 && dist > 0 )
+			{
+				double pl = pdfA * dist2 / cosl / double( nl );
+				V3 wi = fr.local( wiw );
+				V3 f;
+				double pb;
+				m_eval( sh, wo, wi, f, pb );
+				if ( ( f.x > 0 || f.y > 0 || f.z > 0 ) && dot( wiw, ng ) > 0 &&
+					 !occluded_ray( s, p, wiw, 1e-7 * s->scale, dist * ( 1 - 1e-4 ) ) )
+				{
+					double w = pl * pl / ( pl * pl + pb * pb );
+					L = L + beta * f * s->shaders[ s->prims[ lt.prim ].shader ].emission * ( wi.z * w / pl );
+				}
+			}
+		}
+		double u1 = rng.next(), u2 = rng.next();
+		V3 wi, wt;
+		double pdf;
+		m_sample( sh, wo, u1, u2, wi, wt, pdf );
+		beta = beta * wt;
+		if ( beta.x == 0 && beta.y == 0 && beta.z == 0 ) break;
+		prev_pdf = pdf;
+		d = fr.global( wi );
+		if ( dot( d, ng ) <= 0 ) break;
+		o = p + ng * ( 1e-7 * s->scale );
+		double rr = maxc( beta );
+		if ( rr < 1. && bounce > 3 )
+		{
+			double q = std::max( .05, 1 - rr );
+			if ( rng.next() < q ) break;
+			beta = beta / ( 1 - q );
+		}
+	}
+	return L;
+}
+
+// ---------------------------------------------------------------- koishi light tables
+// Face order of a mesh as the reference stores it: the triangle list padded to
+// a multiple of 4 with copies of its last triangle (createBVH, mesh.cu:135-143)
+// then permuted by the recursive build (doCreateBVH, mesh.cu:35-111).
+struct TInfo
+{
+	uint32_t idx;
+	F3 vmax, vmin;
+};
+
+static float vol( F3 lo, F3 hi ) { return ( hi.x - lo.x ) * ( hi.y - lo.y ) * ( hi.z - lo.z ); }
+
+void koishi_order( std::vector<TInfo> &info, size_t b, size_t e )
+{
+	F3 lo = info[ b ].vmin, hi = info[ b ].vmax;
+	for ( size_t i = b; i < e; ++i )
+	{
+		lo = { std::min( lo.x, info[ i ].vmin.x ), std::min( lo.y, info[ i ].vmin.y ), std::min( lo.z, info[ i ].vmin.z ) };
+		hi = { std::max( hi.x, info[ i ].vmax.x ), std::max( hi.y, info[ i ].vmax.y ), std::max( hi.z, info[ i ].vmax.z ) };
+	}
+	size_t len = e - b;
+	if ( len <= 16 ) return;
+	F3 w = fsub( hi, lo );
+	auto first = info.begin() + b, last = info.begin() + e;
+	if ( w.x >= w.y && w.x >= w.z )
+		std::sort( first, last, []( const TInfo &a, const TInfo &c ) { return a.vmin.x < c.vmin.x; } );
+	else if ( w.y >= w.x && w.y >= w.z )
+		std::sort( first, last, []( const TInfo &a, const TInfo &c ) { return a.vmin.y < c.vmin.y; } );
+	else
+		std::sort( first, last, []( const TInfo &a, const TInfo &c ) { return a.vmin.z < c.vmin.z; } );
+	std::vector<float> low( len ), high( len );
+	const float inf = std::numeric_limits<float>::infinity();
+	F3 a{ inf, inf, inf }, c{ -inf, -inf, -inf };
+	for ( size_t i = 0; i < len; ++i )
+	{
+		auto &t = info[ b + i ];
+		a = { std::min( t.vmin.x, a.x ), std::min( t.vmin.y, a.y ), std::min( t.vmin.z, a.z ) };
+		c = { std::max( t.vmax.x, c.x ), std::max( t.vmax.y, c.y ), std::max( t.vmax.z, c.z ) };
+		low[ i ] = vol( a, c );
+	}
+	a = { inf, inf, inf }, c = { -inf, -inf, -inf };
+	for ( size_t i = len; i-- > 0; )
+	{
+		auto &t = info[ b + i ];
+		a = { std::min( t.vmin.x, a.x ), std::min( t.vmin.y, a.y ), std::min( t.vmin.z, a.z ) };
+		c = { std::max( t.vmax.x, c.x ), std::max( t.vmax.y, c.y ), std::max( t.vmax.z, c.z ) };
+		high[ i ] = vol( a, c );
+	}
+	for ( size_t i = 4; i < len; i += 4 )
+		if ( low[ i - 1 ] - high[ i ] >= 0.f )
+		{
+			koishi_order( info, b, b + i );
+			koishi_order( info, b + i, e );
+			return;
+		}
+	koishi_order( info, b, b + len / 2 );
+	koishi_order( info, b + len / 2, e );
+}
+
+// Mesh::generateSamples (src/core/primitive/mesh.hpp:61-84), drawing from the
+// reference's 48-bit generator (src/core/misc/sampler.hpp:22-36).
+struct Drand48
+{
+	uint64_t x;
+	float next()
+	{
+		x = ( 0x5DEECE66Dull * x + 0xB16ull ) & 0xFFFFFFFFFFFFull;
+		return float( uint32_t( x >> 16 ) ) / float( 0x100000000LL );
+	}
+};
+
+void koishi_table( const orc_scene *s, Light &lt, Drand48 &rng )
+{
+	const Prim &pr = s->prims[ lt.prim ];
+	std::vector<TInfo> info;
+	for ( int i = 0; i < pr.n_tri; ++i )
+	{
+		const Tri &t = s->tris[ pr.first_tri + i ];
+		TInfo ti;
+		ti.idx = uint32_t( i );
+		ti.vmax = { std::max( t.fv0.x, std::max( t.fv1.x, t.fv2.x ) ), std::max( t.fv0.y, std::max( t.fv1.y, t.fv2.y ) ),
+					std::max( t.fv0.z, std::max( t.fv1.z, t.fv2.z ) ) };
+		ti.vmin = { std::min( t.fv0.x, std::min( t.fv1.x, t.fv2.x ) ), std::min( t.fv0.y, std::min( t.fv1.y, t.fv2.y ) ),
+					std::min( t.fv0.z, std::min( t.fv1.z, t.fv2.z ) ) };
+		info.push_back( ti );
+	}
+	TInfo lastInfo = info.back();
+	while ( info.size() % 4 ) info.push_back( lastInfo );
+	koishi_order( info, 0, info.size() );
+	size_t nf = info.size();
+	lt.tp.resize( 1024 );
+	lt.tn.resize( 1024 );
+	for ( int i = 0; i < 1024; ++i )
+	{
+		float r = rng.next();
+		uint32_t idx = std::min( uint32_t( std::floor( r * float( nf ) ) ), uint32_t( nf - 1 ) );
+		float a = rng.next(), b = rng.next();
+		float uu = std::min( a, b ), vv = std::max( a, b );
+		const Tri &t = s->tris[ pr.first_tri + info[ idx ].idx ];
+		F3 d1 = fsub( t.fv1, t.fv0 ), d2 = fsub( t.fv2, t.fv0 );
+		lt.tp[ i ] = fadd( fadd( t.fv0, fmul( d1, uu ) ), fmul( d2, vv ) );
+		float w0 = 1 - uu - vv;
+		lt.tn[ i ] = fnormalize( fadd( fadd( fmul( t.fn0, w0 ), fmul( t.fn1, uu ) ), fmul( t.fn2, vv ) ) );
+	}
+	float area = 0;
+	for ( auto &ti : info )
+	{
+		const Tri &t = s->tris[ pr.first_tri + ti.idx ];
+		F3 c = fcross( fsub( t.fv1, t.fv0 ), fsub( t.fv2, t.fv0 ) );
+		float len = std::sqrt( c.x * c.x + c.y * c.y + c.z * c.z );
+		area = float( double( area ) + double( len ) * .5 );
+	}
+	lt.kpdf = 1.f / area;
+}
+
+V3 fv( const float *p ) { return V3( p[ 0 ], p[ 1 ], p[ 2 ] ); }
+F3 ff( const float *p ) { return F3{ p[ 0 ], p[ 1 ], p[ 2 ] }; }
+
+}  // namespace
+
+extern "C" {
+
+orc_scene *orc_scene_new( void ) { return new orc_scene(); }
+void orc_scene_free( orc_scene *s ) { delete s; }
+
+int orc_add_shader( orc_scene *s, int type, const double *p )
+{
+	Shader sh;
+	sh.type = type;
+	if ( type == ORC_LAMBERT )
+		sh.R = V3( p[ 0 ], p[ 1 ], p[ 2 ] ), sh.color = V3( p[ 3 ], p[ 4 ], p[ 5 ] );
+	else if ( type == ORC_GLOSSY )
+		sh.color = V3( p[ 0 ], p[ 1 ], p[ 2 ] ), sh.alpha = p[ 3 ];
+	else
+	{
+		// Emission stores color * strength computed in float (emission.hpp:12-20).
+		float c[ 3 ] = { float( p[ 0 ] ), float( p[ 1 ] ), float( p[ 2 ] ) }, st = float( p[ 3 ] );
+		sh.emission = V3( c[ 0 ] * st, c[ 1 ] * st, c[ 2 ] * st );
+	}
+	s->shaders.push_back( sh );
+	return int( s->shaders.size() - 1 );
+}
+
+int orc_add_mesh( orc_scene *s, const float *v, uint32_t nv, const float *n, const uint32_t *idx, uint32_t nt,
+				  int shader )
+{
+	Prim pr;
+	pr.kind = 0;
+	pr.shader = shader;
+	pr.first_tri = int( s->tris.size() );
+	pr.n_tri = int( nt );
+	int pid = int( s->prims.size() );
+	for ( uint32_t t = 0; t < nt; ++t )
+	{
+		uint32_t a = idx[ 3 * t ], b = idx[ 3 * t + 1 ], c = idx[ 3 * t + 2 ];
+		if ( a >= nv || b >= nv || c >= nv ) return -1;
+		Tri tr;
+		tr.fv0 = ff( v + 3 * a ), tr.fv1 = ff( v + 3 * b ), tr.fv2 = ff( v + 3 * c );
+		tr.fn0 = ff( n + 3 * a ), tr.fn1 = ff( n + 3 * b ), tr.fn2 = ff( n + 3 * c );
+		tr.v0 = fv( v + 3 * a ), tr.v1 = fv( v + 3 * b ), tr.v2 = fv( v + 3 * c );
+		tr.n0 = fv( n + 3 * a ), tr.n1 = fv( n + 3 * b ), tr.n2 = fv( n + 3 * c );
+		tr.prim = pid;
+		tr.index = int( t );
+		s->tris.push_back( tr );
+	}
+	s->prims.push_back( pr );
+	return pid;
+}
+
+int orc_add_sphere( orc_scene *s, const float *c, float r, int shader )
+{
+	Prim pr;
+	pr.kind = 1;
+	pr.shader = shader;
+	pr.c = fv( c );
+	// The reference keeps r^2 in float and recovers r with sqrt (sphere.hpp:11-16,26).
+	float r2 = r * r;
+	pr.r = std::sqrt( double( r2 ) );
+	pr.fr = r;
+	std::memcpy( pr.fc, c, sizeof pr.fc );
+	s->prims.push_back( pr );
+	return int( s->prims.size() - 1 );
+}
+
+void orc_set_camera( orc_scene *s, const float *pos, const float *target, const float *up, float fovx )
+{
+	s->cam.pos = fv( pos ), s->cam.target = fv( target ), s->cam.up = fv( up );
+	s->cam.fovx = fovx;
+}
+
+int orc_finalize( orc_scene *s, uint64_t light_seed )
+{
+	build_bvh( s );
+	V3 lo( INF, INF, INF ), hi( -INF, -INF, -INF );
+	for ( auto &t : s->tris ) lo = vmin( lo, vmin( t.v0, vmin( t.v1, t.v2 ) ) ), hi = vmax( hi, vmax( t.v0, vmax( t.v1, t.v2 ) ) );
+	for ( auto &p : s->prims )
+		if ( p.kind == 1 ) lo = vmin( lo, p.c - V3( p.r, p.r, p.r ) ), hi = vmax( hi, p.c + V3( p.r, p.r, p.r ) );
+	s->scale = std::isfinite( lo.x ) ? std::max( 1.0, maxc( vmax( vmax( -lo, hi ), V3() ) ) ) : 1.0;
+	s->lights.clear();
+	Drand48 rng{ light_seed & 0xFFFFFFFFFFFFull };
+	for ( size_t p = 0; p < s->prims.size(); ++p )
+	{
+		Prim &pr = s->prims[ p ];
+		if ( s->shaders[ pr.shader ].type != ORC_EMISSION ) continue;
+		if ( pr.kind == 0 && pr.n_tri == 0 ) continue;
+		Light lt;
+		lt.prim = int( p );
+		lt.kind = pr.kind;
+		if ( pr.kind == 0 )
+		{
+			koishi_table( s, lt, rng );
+			double acc = 0;
+			for ( int i = 0; i < pr.n_tri; ++i )
+			{
+				const Tri &t = s->tris[ pr.first_tri + i ];
+				acc += 0.5 * length( cross( t.v1 - t.v0, t.v2 - t.v0 ) );
+				lt.cdf.push_back( acc );
+			}
+			lt.area = acc;
+		}
+		else
+			lt.area = 4 * PI * pr.r * pr.r;
+		pr.light = int( s->lights.size() );
+		s->lights.push_back( std::move( lt ) );
+	}
+	return 0;
+}
+
+int orc_num_lights( const orc_scene *s ) { return int( s->lights.size() ); }
+
+double orc_light_table( const orc_scene *s, int l, float *pts )
+{
+	const Light &lt = s->lights[ l ];
+	if ( lt.kind != 0 ) return -1;
+	for ( int i = 0; i < 1024; ++i )
+	{
+		pts[ 6 * i + 0 ] = lt.tp[ i ].x, pts[ 6 * i + 1 ] = lt.tp[ i ].y, pts[ 6 * i + 2 ] = lt.tp[ i ].z;
+		pts[ 6 * i + 3 ] = lt.tn[ i ].x, pts[ 6 * i + 4 ] = lt.tn[ i ].y, pts[ 6 * i + 5 ] = lt.tn[ i ].z;
+	}
+	return lt.kpdf;
+}
+
+void orc_trace( const orc_scene *s, const float *rays, uint64_t n, int32_t *prim, int32_t *tri, double *t,
+				double *u, double *v )
+{
+	for ( uint64_t i = 0; i < n; ++i )
+	{
+		const float *r = rays + 7 * i;
+		Hit h;
+		double tmax = std::isfinite( r[ 6 ] ) && r[ 6 ] > 0 ? double( r[ 6 ] ) : INF;
+		bool hit = intersect( s, fv( r ), fv( r + 3 ), tmax, h );
+		prim[ i ] = hit ? h.prim : -1;
+		tri[ i ] = hit && h.tri >= 0 ? s->tris[ h.tri ].index : -1;
+		t[ i ] = hit ? h.t : INF;
+		u[ i ] = h.u, v[ i ] = h.v;
+	}
+}
+
+void orc_ray_triangle( const orc_scene *s, const float *ray, int prim, int tri, double *t, double *u, double *v )
+{
+	const Tri &tr = s->tris[ s->prims[ prim ].first_tri + tri ];
+	mt( fv( ray ), fv( ray + 3 ), tr.v0, tr.v1 - tr.v0, tr.v2 - tr.v0, *t, *u, *v );
+}
+
+void orc_occluded( const orc_scene *s, const float *segs, uint64_t n, uint8_t *out )
+{
+	for ( uint64_t i = 0; i < n; ++i )
+	{
+		const float *r = segs + 7 * i;
+		out[ i ] = occluded_seg( s, fv( r ), fv( r + 3 ), r[ 6 ] ) ? 1 : 0;
+	}
+}
+
+int orc_render( const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32_t max_bounce, int estimator,
+				uint64_t seed, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, double *sum,
+				double *sumsq, uint32_t *count )
+{
+	if ( x1 > W || y1 > H || x0 >= x1 || y0 >= y1 || spp == 0 ) return -1;
+	Lens lens( s->cam, W, H, spp );
+	uint32_t ww = x1 - x0;
+	std::atomic<uint32_t> next{ y0 };
+	auto work = [&]() {
+		for ( ;; )
+		{
+			uint32_t y = next.fetch_add( 1 );
+			if ( y >= y1 ) break;
+			for ( uint32_t x = x0; x < x1; ++x )
+			{
+				double a[ 3 ] = { 0, 0, 0 }, q[ 3 ] = { 0, 0, 0 };
+				uint32_t c = 0;
+				for ( uint32_t k = 0; k < spp; ++k )
+				{
+					Rng rng( seed, uint64_t( y ) * W + x, k );
+					V3 d = lens.dir( x, y, k );
+					V3 L = estimator == ORC_MIS ? radiance_mis( s, s->cam.pos, d, max_bounce, rng )
+												: radiance_koishi( s, s->cam.pos, d, max_bounce, rng );
+					if ( !finite3( L ) ) continue;  // cpuMulticore.cu:58-64
+					++c;
+					for ( int ch = 0; ch < 3; ++ch ) a[ ch ] += L[ ch ], q[ ch ] += L[ ch ] * L[ ch ];
+				}
+				size_t px = size_t( y - y0 ) * ww + ( x - x0 );
+				for ( int ch = 0; ch < 3; ++ch ) sum[ 3 * px + ch ] = a[ ch ], sumsq[ 3 * px + ch ] = q[ ch ];
+				count[ px ] = c;
+			}
+		}
+	};
+	if ( threads == 0 ) threads = std::max( 1u, std::thread::hardware_concurrency() );
+	std::vector<std::thread> ts;
+	for ( uint32_t i = 0; i < threads; ++i ) ts.emplace_back( work );
+	for ( auto &t : ts ) t.join();
+	return 0;
+}
+
+static Shader make_shader( int type, const double *p )
+{
+	orc_scene tmp;
+	orc_add_shader( &tmp, type, p );
+	return tmp.shaders[ 0 ];
+}
+
+void orc_bsdf_eval( int estimator, int type, const double *params, const double *wo, const double *wi, double *f,
+					double *pdf )
+{
+	Shader sh = make_shader( type, params );
+	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i( wi[ 0 ], wi[ 1 ], wi[ 2 ] ), ff3;
+	double pp = 0;
+	if ( estimator == ORC_MIS )
+		m_eval( sh, o, i, ff3, pp );
+	else
+		ff3 = k_eval( sh, o, i );
+	f[ 0 ] = ff3.x, f[ 1 ] = ff3.y, f[ 2 ] = ff3.z;
+	*pdf = pp;
+}
+
+void orc_bsdf_sample( int estimator, int type, const double *params, const double *wo, const double *u, double *wi,
+					  double *weight, double *pdf )
+{
+	Shader sh = make_shader( type, params );
+	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i, w;
+	double pp = 0;
+	if ( estimator == ORC_MIS )
+		m_sample( sh, o, u[ 0 ], u[ 1 ], i, w, pp );
+	else
+	{
+		V3 f;
+		k_sample( sh, o, u[ 0 ], u[ 1 ], i, f );
+		w = f * std::fabs( i.z );
+	}
+	wi[ 0 ] = i.x, wi[ 1 ] = i.y, wi[ 2 ] = i.z;
+	weight[ 0 ] = w.x, weight[ 1 ] = w.y, weight[ 2 ] = w.z;
+	*pdf = pp;
+}
+
+// Seg::intersect_bbox (src/core/basic/ray.hpp:59-79): separating-axis test of a
+// segment against a box, restated in float as the reference evaluates it.
+int orc_seg_box( const float *seg, const float *bmin, const float *bmax )
+{
+	float o[ 3 ] = { seg[ 0 ], seg[ 1 ], seg[ 2 ] }, d[ 3 ] = { seg[ 3 ], seg[ 4 ], seg[ 5 ] }, t = seg[ 6 ];
+	float c[ 3 ], l[ 3 ], p0[ 3 ], p1[ 3 ], m[ 3 ], w[ 3 ], W[ 3 ];
+	for ( int a = 0; a < 3; ++a )
+	{
+		c[ a ] = ( bmin[ a ] + bmax[ a ] ) * .5f;
+		l[ a ] = bmax[ a ] - c[ a ];
+		p0[ a ] = o[ a ] - c[ a ];
+		p1[ a ] = p0[ a ] + d[ a ] * t;
+		m[ a ] = ( p0[ a ] + p1[ a ] ) * .5f;
+		w[ a ] = m[ a ] - p0[ a ];
+		W[ a ] = std::fabs( w[ a ] );
+		if ( std::fabs( m[ a ] ) - W[ a ] - l[ a ] > 0 ) return 0;
+	}
+	if ( std::fabs( -w[ 2 ] * m[ 1 ] + w[ 1 ] * m[ 2 ] ) > l[ 1 ] * W[ 2 ] + l[ 2 ] * W[ 1 ] ||
+		 std::fabs( -w[ 2 ] * m[ 0 ] + w[ 0 ] * m[ 2 ] ) > l[ 0 ] * W[ 2 ] + l[ 2 ] * W[ 0 ] ||
+		 std::fabs( -w[ 1 ] * m[ 0 ] + w[ 0 ] * m[ 1 ] ) > l[ 0 ] * W[ 1 ] + l[ 1 ] * W[ 0 ] )
+		return 0;
+	return 1;
+}
+
+int orc_sphere_hit( const float *c, float r, const float *ray, double *t )
+{
+	double tt = INF;
+	bool h = sphere_hit( fv( c ), std::sqrt( double( r * r ) ), fv( ray ), fv( ray + 3 ), tt );
+	*t = tt;
+	return h ? 1 : 0;
+}
+
+}  // extern "C"

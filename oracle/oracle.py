@@ -1,0 +1,234 @@
+"""Python access to the checkers under oracle/ (TEST INFRASTRUCTURE ONLY).
+
+* :class:`OracleScene` wraps build/liboracle.so, the FP64 restatement of the
+  reference's Radiance path (oracle.h documents both estimator modes).
+* :func:`ref_run` runs _ref/cr_ref, the reference's own CPU code compiled from
+  its sources with the harness in ref_harness/ (oracle/Makefile).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module.  The product path never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "cr_ref")
+
+KOISHI, MIS = 0, 1
+LAMBERT, GLOSSY, EMISSION = 0, 1, 2
+LIGHT_SEED = 0x330E
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run make -C oracle oracle)")
+        L = C.CDLL(LIB_PATH)
+        P, U32, U64, I, D, F = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_double, C.c_float
+        sig = {
+            "orc_scene_new": (P, []), "orc_scene_free": (None, [P]),
+            "orc_add_shader": (I, [P, I, P]),
+            "orc_add_mesh": (I, [P, P, U32, P, P, U32, I]),
+            "orc_add_sphere": (I, [P, P, F, I]),
+            "orc_set_camera": (None, [P, P, P, P, F]),
+            "orc_finalize": (I, [P, U64]), "orc_num_lights": (I, [P]),
+            "orc_light_table": (D, [P, I, P]),
+            "orc_trace": (None, [P, P, U64, P, P, P, P, P]),
+            "orc_ray_triangle": (None, [P, P, I, I, P, P, P]),
+            "orc_occluded": (None, [P, P, U64, P]),
+            "orc_render": (I, [P, U32, U32, U32, U32, I, U64, U32, U32, U32, U32, U32, P, P, P]),
+            "orc_bsdf_eval": (None, [I, I, P, P, P, P, P]),
+            "orc_bsdf_sample": (None, [I, I, P, P, P, P, P, P]),
+            "orc_seg_box": (I, [P, P, P]), "orc_sphere_hit": (I, [P, F, P, P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def shader_params(cfg):
+    """(type, params) for a reference-schema shader config [Type, props]
+    (Lambert: lambert.hpp:12-19; GlossyBSDF: glossy.hpp:11-17 with
+    beckmann.hpp:11-17; Emission: emission.hpp:12-20)."""
+    kind, props = cfg[0], (cfg[1] if len(cfg) > 1 else {})
+    if kind == "Lambert":
+        return LAMBERT, list(props.get("R", [1, 1, 1])) + list(props.get("color", [1, 1, 1]))
+    if kind == "GlossyBSDF":
+        dist = props.get("distribution", ["Beckmann", {}])
+        rough = dist[1].get("roughness", 0.5) if len(dist) > 1 else 0.5
+        return GLOSSY, list(props.get("color", [1, 1, 1])) + [rough]
+    if kind == "Emission":
+        return EMISSION, list(props.get("color", [1, 1, 1])) + [props.get("strength", 2.0)]
+    raise ValueError(f"unsupported shader {kind}")
+
+
+class OracleScene:
+    """FP64 oracle scene built from a scenes.SceneDesc (meshes first in group
+    order, then spheres: the reference's primitive order for an import asset
+    listed before the spheres)."""
+
+    def __init__(self, desc, light_seed=LIGHT_SEED):
+        L = lib()
+        self.h = L.orc_scene_new()
+        self.desc = desc
+        ids = {}
+
+        def sid(name):
+            if name not in ids:
+                t, p = shader_params(desc.shaders[name])
+                ids[name] = L.orc_add_shader(self.h, t, _p(np.asarray(p, np.float64)))
+            return ids[name]
+
+        self.prim_kind = []
+        for g in desc.groups:
+            v = np.ascontiguousarray(g.v, np.float32)
+            n = np.ascontiguousarray(g.n, np.float32)
+            f = np.ascontiguousarray(g.f, np.uint32)
+            r = L.orc_add_mesh(self.h, _p(v), len(v), _p(n), _p(f), len(f), sid(g.name))
+            assert r >= 0
+            self.prim_kind.append(0)
+        for s in desc.spheres:
+            L.orc_add_sphere(self.h, _p(np.asarray(s["o"], np.float32)), float(s["r"]), sid(s["shader"]))
+            self.prim_kind.append(1)
+        cam = desc.camera
+        L.orc_set_camera(self.h, _p(np.asarray(cam["position"], np.float32)),
+                         _p(np.asarray(cam["target"], np.float32)),
+                         _p(np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)), float(cam.get("fovx", 90)))
+        L.orc_finalize(self.h, light_seed)
+
+    def __del__(self):
+        try:
+            lib().orc_scene_free(self.h)
+        except Exception:
+            pass
+
+    @property
+    def n_lights(self):
+        return lib().orc_num_lights(self.h)
+
+    def light_table(self, l):
+        pts = np.zeros((1024, 6), np.float32)
+        pdf = lib().orc_light_table(self.h, l, _p(pts))
+        return pts, pdf
+
+    def trace(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        prim = np.zeros(n, np.int32)
+        tri = np.zeros(n, np.int32)
+        t, u, v = (np.zeros(n) for _ in range(3))
+        lib().orc_trace(self.h, _p(rays), n, _p(prim), _p(tri), _p(t), _p(u), _p(v))
+        return prim, tri, t, u, v
+
+    def ray_triangle(self, ray, prim, tri):
+        ray = np.ascontiguousarray(ray, np.float32)
+        t, u, v = (np.zeros(1) for _ in range(3))
+        lib().orc_ray_triangle(self.h, _p(ray), int(prim), int(tri), _p(t), _p(u), _p(v))
+        return float(t[0]), float(u[0]), float(v[0])
+
+    def occluded(self, segs):
+        segs = np.ascontiguousarray(segs, np.float32)
+        out = np.zeros(len(segs), np.uint8)
+        lib().orc_occluded(self.h, _p(segs), len(segs), _p(out))
+        return out
+
+    def render(self, W, H, spp, max_bounce, estimator=KOISHI, seed=1, threads=0, window=None):
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        n = (x1 - x0) * (y1 - y0)
+        s = np.zeros((n, 3))
+        q = np.zeros((n, 3))
+        c = np.zeros(n, np.uint32)
+        r = lib().orc_render(self.h, W, H, spp, max_bounce, estimator, seed, threads, x0, y0, x1, y1,
+                             _p(s), _p(q), _p(c))
+        assert r == 0
+        shp = (y1 - y0, x1 - x0)
+        return Film(s.reshape(*shp, 3), q.reshape(*shp, 3), c.reshape(shp))
+
+
+def bsdf_eval(estimator, cfg, wo, wi):
+    t, p = shader_params(cfg)
+    f = np.zeros(3)
+    pdf = np.zeros(1)
+    lib().orc_bsdf_eval(estimator, t, _p(np.asarray(p, np.float64)), _p(np.asarray(wo, np.float64)),
+                        _p(np.asarray(wi, np.float64)), _p(f), _p(pdf))
+    return f, float(pdf[0])
+
+
+def bsdf_sample(estimator, cfg, wo, u):
+    t, p = shader_params(cfg)
+    wi, w, pdf = np.zeros(3), np.zeros(3), np.zeros(1)
+    lib().orc_bsdf_sample(estimator, t, _p(np.asarray(p, np.float64)), _p(np.asarray(wo, np.float64)),
+                          _p(np.asarray(u, np.float64)), _p(wi), _p(w), _p(pdf))
+    return wi, w, float(pdf[0])
+
+
+def seg_box(seg7, bmin, bmax):
+    return bool(lib().orc_seg_box(_p(np.asarray(seg7, np.float32)), _p(np.asarray(bmin, np.float32)),
+                                  _p(np.asarray(bmax, np.float32))))
+
+
+def sphere_hit(center, r, ray6):
+    t = np.zeros(1)
+    h = lib().orc_sphere_hit(_p(np.asarray(center, np.float32)), float(r), _p(np.asarray(ray6, np.float32)), _p(t))
+    return bool(h), float(t[0])
+
+
+class Film:
+    """Per-pixel sums over finite samples, as CPUMulticoreTracer::execute
+    averages them (src/core/tracer/cpuMulticore.cu:53-64)."""
+
+    def __init__(self, s, q, c):
+        self.sum, self.sumsq, self.count = s, q, c
+
+    @property
+    def mean(self):
+        return self.sum / np.maximum(self.count, 1)[..., None]
+
+    @property
+    def var_of_mean(self):
+        c = np.maximum(self.count, 1)[..., None].astype(np.float64)
+        m = self.sum / c
+        var = np.maximum(self.sumsq / c - m * m, 0.0) * c / np.maximum(c - 1, 1)
+        return var / c
+
+
+def read_crf(path):
+    with open(path, "rb") as fh:
+        d = fh.read()
+    assert d[:4] == b"CRF1"
+    W, H, spp = struct.unpack_from("<III", d, 4)
+    off = 16
+    s = np.frombuffer(d, "<f8", W * H * 3, off).reshape(H, W, 3)
+    off += W * H * 24
+    q = np.frombuffer(d, "<f8", W * H * 3, off).reshape(H, W, 3)
+    off += W * H * 24
+    c = np.frombuffer(d, "<u4", W * H, off).reshape(H, W)
+    return Film(s.copy(), q.copy(), c.copy())
+
+
+def ref_available():
+    return os.path.exists(REF_BIN)
+
+
+def ref_run(*args, cwd=None, timeout=600):
+    """Run the compiled reference harness; returns its CompletedProcess."""
+    if not ref_available():
+        raise RuntimeError(f"reference harness missing: {REF_BIN} (run make -C oracle ref)")
+    return subprocess.run([REF_BIN, *map(str, args)], cwd=cwd, capture_output=True, text=True,
+                          timeout=timeout, check=True)
