@@ -1,0 +1,355 @@
+"""Throughput benchmark of the Radiance path (one JSON line on stdout).
+
+Workload: the 1024x768, 256 spp render of a 1.31M-triangle displaced
+icosphere (subdivision 8, 4-octave value-noise displacement of amplitude 0.15)
+inside the Cornell-style box, 20 patch materials (50 % Lambert albedo
+U[0.2,0.9]^3, 50 % Beckmann roughness U[0.05,0.8]), one ceiling light,
+max depth 8 (maxBounce 7), seeded synthetic data.  One step = one full
+render of that image = 201,326,592 camera paths.  The estimator is the
+reference's (the same arithmetic the reference arm times).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value      Msamples/s of the whole job, device-timed with CUDA events on the
+           render stream, max over ranks; inputs resident in HBM.
+e2e        Msamples/s through the public C ABI from host arrays: scene upload,
+           GPU BVH build, render and the film's device-to-host copy each step.
+roofline   the closest-hit traversal kernel (k_extend): algorithmic bytes per
+           launch (nodes x 80 B + triangles x 48 B + rays x 48 B, counted by
+           the counting build on the same workload) / its mean launch time.
+cpu_baseline / --impl reference
+           the reference's own CPUMulticoreTracer::execute compiled from its
+           sources (oracle/_ref/cr_ref), on this host's cores, on a bounded
+           sample of the same workload (full resolution, fewer spp).
+Multi-GPU: one process per GPU; each rank renders the workload with its own
+seed (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))  # the CPU-baseline leg only
+
+WIDTH, HEIGHT, SPP, LEVEL, MAX_BOUNCE = 1024, 768, 256, 8, 7
+METRIC = "Msamples/s (camera paths per second), plain wavefront, 1024x768x256spp, 1.31M-tri displaced icosphere"
+NODE_BYTES, TRI_BYTES, RAY_BYTES = 80, 48, 32 + 16
+
+
+def load_pkg():
+    """The package directory `cuda-raytracer_b200`, imported as cuda_raytracer_b200."""
+    import importlib.util
+    if "cuda_raytracer_b200" in sys.modules:
+        return sys.modules["cuda_raytracer_b200"]
+    pkg = os.path.join(ROOT, "cuda-raytracer_b200")
+    spec = importlib.util.spec_from_file_location("cuda_raytracer_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["cuda_raytracer_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per k_extend launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "k_extend_traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return None
+
+
+def make_workload(tmpdir):
+    load_pkg()
+    from cuda_raytracer_b200 import scenes
+    desc = scenes.config1(level=LEVEL, width=WIDTH, height=HEIGHT, spp=SPP)
+    path = scenes.write_scene(desc, tmpdir)
+    return desc, path
+
+
+# ---------------------------------------------------------------------------- reference arm
+def reference_rate(scene_json, steps, warmup, spp):
+    """Reference CPU Radiance path (oracle/_ref/cr_ref bench) on all host threads."""
+    import oracle
+    threads = os.cpu_count() or 1
+    r = subprocess.run([oracle.REF_BIN, "bench", os.path.basename(scene_json), str(WIDTH), str(HEIGHT), str(spp),
+                        str(threads), str(MAX_BOUNCE), str(steps + warmup)], cwd=os.path.dirname(scene_json),
+                       capture_output=True, text=True, timeout=3600, check=True)
+    runs = [json.loads(l) for l in r.stderr.splitlines() if l.startswith("{")]
+    timed = runs[warmup:]
+    secs = sum(x["seconds"] for x in timed)
+    samples = sum(x["samples"] for x in timed)
+    # CPUMulticoreTracer runs min(hardware_concurrency()-1, maxThreads) tracer
+    # threads; the last core spins its progress bar (cpuMulticore.cu:19-21,76-114).
+    used = max(1, min(threads, (os.cpu_count() or 1) - 1))
+    return samples / secs / 1e6, secs / max(len(timed), 1), used, samples // max(len(timed), 1)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cr_ref was not built (make -C oracle ref)"}))
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        _, path = make_workload(tmp)
+        rate, sec, cores, samples = reference_rate(path, args.steps, args.warmup, args.ref_spp)
+    sample = f"{WIDTH}x{HEIGHT} at {args.ref_spp} spp per step ({samples} paths), same scene and depth"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(rate, 4), "unit": "Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": "config1: 1024x768x256spp, 1.31M-tri displaced icosphere in the box, depth 8",
+                   "sample_per_step": sample},
+        "cpu_baseline": {"value": round(rate, 4), "unit": "Msamples/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(rate, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    cr = load_pkg()
+    tmp = tempfile.mkdtemp()
+    desc, path = make_workload(tmp)
+    scene = cr.Scene.from_desc(desc)
+    info = scene.info()
+    spp = args.spp or SPP
+    npx = WIDTH * HEIGHT
+    s = torch.zeros(npx * 3, dtype=torch.float64, device=dev)
+    q = torch.zeros(npx * 3, dtype=torch.float64, device=dev)
+    c = torch.zeros(npx, dtype=torch.int32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def step(seed, stats=True):
+        d = cr.render_desc(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=seed,
+                           wave_paths=args.wave_paths)
+        return scene.render_device(d, s.data_ptr(), q.data_ptr(), c.data_ptr(), stream=stream.cuda_stream,
+                                   stats=stats)
+
+    # warm-up
+    for w in range(args.warmup):
+        step(1000 + w)
+    torch.cuda.synchronize(dev)
+
+    # work counts for the roofline (untimed counting pass on one seed)
+    dcount = cr.render_desc(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=4242,
+                            wave_paths=args.wave_paths, count_work=True)
+    cst = scene.render_device(dcount, s.data_ptr(), q.data_ptr(), c.data_ptr(), stream=stream.cuda_stream)
+
+    # timed region
+    clocks = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    totals = {"extend": 0.0, "shadow": 0.0, "shade": 0.0, "other": 0.0, "launches": 0, "ext_launches": 0,
+              "rays_extend": 0, "rays_shadow": 0, "samples": 0}
+    for k in range(args.steps):
+        flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
+        ev[k][0].record(stream)
+        st = step(7 + 1000 * rank + k)
+        ev[k][1].record(stream)
+        totals["extend"] += st.ms_extend
+        totals["shadow"] += st.ms_shadow
+        totals["shade"] += st.ms_shade
+        totals["other"] += st.ms_other
+        totals["launches"] += st.launches
+        totals["ext_launches"] += st.extend_launches
+        totals["rays_extend"] += st.rays_extend
+        totals["rays_shadow"] += st.rays_shadow
+        totals["samples"] += st.samples
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    samples_all = totals["samples"] * world
+    value = samples_all / (ms_max / 1e3) / 1e6
+
+    # roofline of the closest-hit kernel
+    ext_bytes = cst.nodes * NODE_BYTES + cst.tris * TRI_BYTES + cst.rays_extend * RAY_BYTES
+    ext_launch_bytes = ext_bytes / max(cst.extend_launches, 1)
+    ext_launch_ms = totals["extend"] / max(totals["ext_launches"], 1)
+    achieved = ext_launch_bytes / (ext_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic()
+
+    # end to end through the public API from host arrays
+    e2e = None
+    if rank == 0 and args.e2e_steps > 0:
+        import numpy as np
+        h2d = sum(g.v.nbytes + g.n.nbytes + g.f.nbytes for g in desc.groups)
+        d2h = npx * 3 * 8 + npx * 4
+        times = []
+        for k in range(args.e2e_steps):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            sc2 = cr.Scene.from_desc(desc)
+            film, _ = sc2.render(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k,
+                                 wave_paths=args.wave_paths)
+            sc2.close()
+            times.append(time.perf_counter() - t0)
+            assert np.isfinite(film).all()
+        e2e = {"value": round(npx * spp / statistics.mean(times) / 1e6, 4), "unit": "Msamples/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": round(statistics.mean(times) * 1e3, 3),
+               "includes": "scene upload, GPU BVH build, render, film copy to host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            rate, sec, cores, samples = reference_rate(path, 1, 0, args.ref_spp)
+            cpu = {"value": round(rate, 4), "unit": "Msamples/s", "cores": cores, "kind": "reference",
+                   "sample": f"{WIDTH}x{HEIGHT} at {args.ref_spp} spp ({samples} paths) of the same scene, "
+                             f"{sec:.1f} s of CPU time"}
+        else:
+            cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
+                   "sample": "oracle/_ref/cr_ref not built"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene, no dataset)",
+            "config": {"workload": "config1: 1024x768x256spp, 1.31M-tri displaced icosphere in the box, depth 8",
+                       "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"], "spp": spp,
+                       "estimator": "reference (koishi)", "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"replica-per-gpu x{world}"},
+            "mrays_per_s": round((totals["rays_extend"] + totals["rays_shadow"]) * world / (ms_max / 1e3) / 1e6, 2),
+            "stage_ms_per_step": {k: round(totals[k] / args.steps, 3) for k in ("extend", "shadow", "shade", "other")},
+            "roofline": {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                         "algorithmic_bytes_per_launch": round(ext_launch_bytes),
+                         "launch_ms": round(ext_launch_ms, 4),
+                         "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
+                         "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3)},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": totals["launches"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--spp", type=int, default=0, help="override spp per step (default: the workload's 256)")
+    ap.add_argument("--wave-paths", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-spp", type=int, default=4, help="spp of the reference's bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

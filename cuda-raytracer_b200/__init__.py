@@ -1,1 +1,252 @@
-"""B200-native Radiance path tracer (drop-in for xlnx/cuda-raytracer's Radiance path)."""
+"""B200-native Radiance path tracer: drop-in for the Radiance path of
+xlnx/cuda-raytracer ("Koishi").
+
+This module is the Python face of ``include/cr.h`` (ctypes over
+``lib/libcr_b200.so``).  It mirrors the reference's plugin surface for the
+path: the kernel registry (``Factory<Kernel>``, src/core/kernel/kernel.impl.cu:10-15)
+holds ``"Radiance"``, the tracer registry (``Factory<Tracer>``,
+src/core/tracer/tracer.impl.cu:8-11) holds ``"CudaWavefront"`` and accepts the
+reference's ``"CPUMulticore"`` name for scene files written for it.  Every
+query runs on the GPU; there is no CPU fallback, and importing this module
+on a machine where the library is missing raises immediately on first use.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcr_b200.so")
+CLI_PATH = os.path.join(HERE, "lib", "cr")
+
+CR_OK = 0
+KOISHI, MIS = 0, 1
+KERNELS = ("Radiance",)
+TRACERS = ("CudaWavefront", "CPUMulticore")
+DEFAULT_LIGHT_SEED = 0x330E
+U32_MAX = 0xFFFFFFFF
+
+
+class CrError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cr error {code}: {msg}")
+        self.code = code
+
+
+class Hit(C.Structure):
+    _fields_ = [("prim", C.c_int32), ("tri", C.c_int32), ("t", C.c_float), ("u", C.c_float), ("v", C.c_float)]
+
+
+HIT_DTYPE = np.dtype([("prim", "<i4"), ("tri", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+
+
+class RenderDesc(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_bounce", C.c_uint32),
+                ("estimator", C.c_int32), ("x0", C.c_uint32), ("y0", C.c_uint32), ("x1", C.c_uint32),
+                ("y1", C.c_uint32), ("seed", C.c_uint64), ("wave_paths", C.c_uint32), ("guiding", C.c_int32),
+                ("count_work", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_extend", C.c_double), ("ms_shadow", C.c_double),
+                ("ms_shade", C.c_double), ("ms_other", C.c_double), ("samples", C.c_uint64),
+                ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64), ("nodes", C.c_uint64),
+                ("tris", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_tris", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32),
+                ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """The loaded C library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libcr_b200.so not built at {LIB_PATH}; run `make -C cuda-raytracer_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        P, I, U32, U64, F = C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_float
+        sigs = {
+            "cr_last_error": (C.c_char_p, []), "cr_version": (C.c_char_p, []),
+            "cr_scene_create": (I, [C.c_char_p, C.c_char_p, P]),
+            "cr_scene_create_empty": (I, [P]),
+            "cr_scene_add_shader": (I, [P, C.c_char_p, C.c_char_p]),
+            "cr_scene_add_mesh": (I, [P, P, U32, P, P, U32, C.c_char_p]),
+            "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
+            "cr_scene_set_camera": (I, [P, P, P, P, F]),
+            "cr_scene_commit": (I, [P, U64, P]),
+            "cr_scene_info": (I, [P, P, P, P, P]),
+            "cr_scene_destroy": (None, [P]),
+            "cr_light_table": (I, [P, U32, P, P]),
+            "cr_trace_rays": (I, [P, P, U64, P, I]),
+            "cr_trace_rays_device": (I, [P, P, U64, P, I, P]),
+            "cr_render": (I, [P, P, P, P]),
+            "cr_render_device": (I, [P, P, P, P, P, P, P]),
+            "cr_render_file": (I, [C.c_char_p, C.c_char_p, C.c_char_p, U32, U32, U32, C.c_char_p, C.c_char_p]),
+            "cr_write_png": (I, [C.c_char_p, U32, U32, P]),
+            "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
+            "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc < 0:
+        raise CrError(rc, lib().cr_last_error().decode(errors="replace"))
+    return rc
+
+
+def _p(a):
+    # data_as keeps a reference to the array inside the pointer object
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, window=None, wave_paths=0,
+                guiding=False, count_work=False):
+    d = RenderDesc()
+    d.width, d.height, d.spp = width, height, spp
+    d.max_bounce = U32_MAX if max_bounce is None else max_bounce
+    d.estimator = -1 if estimator is None else estimator
+    if window:
+        d.x0, d.y0, d.x1, d.y1 = window
+    d.seed = seed
+    d.wave_paths = wave_paths
+    d.guiding = int(bool(guiding))
+    d.count_work = int(bool(count_work))
+    return d
+
+
+class Scene:
+    """A committed scene on the GPU (Scene, src/core/meta/scene.hpp:15-71)."""
+
+    def __init__(self, handle):
+        self.h = C.c_void_p(handle)
+
+    # -- construction ---------------------------------------------------------
+    @classmethod
+    def from_json(cls, text, base_dir="."):
+        """Scene::Scene from the reference's JSON schema (import/sphere assets)."""
+        out = C.c_void_p()
+        _check(lib().cr_scene_create(text.encode(), base_dir.encode(), C.byref(out)))
+        return cls(out.value)
+
+    @classmethod
+    def from_file(cls, path):
+        with open(path) as fh:
+            return cls.from_json(fh.read(), os.path.dirname(os.path.abspath(path)))
+
+    @classmethod
+    def from_desc(cls, desc, light_seed=DEFAULT_LIGHT_SEED):
+        """Build from a scenes.SceneDesc through the add_* calls: meshes in
+        group order, then spheres (the order the reference's scene loader
+        gives an import asset listed before sphere assets)."""
+        out = C.c_void_p()
+        _check(lib().cr_scene_create_empty(C.byref(out)))
+        s = cls(out.value)
+        for name, cfg in desc.shaders.items():
+            _check(lib().cr_scene_add_shader(s.h, name.encode(), json.dumps(cfg).encode()))
+        for g in desc.groups:
+            v = np.ascontiguousarray(g.v, np.float32)
+            n = np.ascontiguousarray(g.n, np.float32)
+            f = np.ascontiguousarray(g.f, np.uint32)
+            _check(lib().cr_scene_add_mesh(s.h, _p(v), len(v), _p(n), _p(f), len(f), g.name.encode()))
+        for sp in desc.spheres:
+            c = np.asarray(sp["o"], np.float32)
+            _check(lib().cr_scene_add_sphere(s.h, _p(c), float(sp["r"]), sp["shader"].encode()))
+        cam = desc.camera
+        # keep the arrays bound to names: ctypes only holds their addresses
+        pos = np.asarray(cam["position"], np.float32)
+        tgt = np.asarray(cam["target"], np.float32)
+        up = np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)
+        _check(lib().cr_scene_set_camera(s.h, _p(pos), _p(tgt), _p(up), float(cam.get("fovx", 90.0))))
+        _check(lib().cr_scene_commit(s.h, light_seed, None))
+        return s
+
+    def close(self):
+        if self.h and self.h.value:
+            lib().cr_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- queries ----------------------------------------------------------------
+    def info(self):
+        nt, np_, nl, nn = C.c_uint64(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(lib().cr_scene_info(self.h, C.byref(nt), C.byref(np_), C.byref(nl), C.byref(nn)))
+        return {"triangles": nt.value, "primitives": np_.value, "lights": nl.value, "bvh_nodes": nn.value}
+
+    def light_table(self, light):
+        out = np.zeros((1024, 6), np.float32)
+        pdf = C.c_float()
+        _check(lib().cr_light_table(self.h, light, _p(out), C.byref(pdf)))
+        return out, pdf.value
+
+    def trace(self, rays, any_hit=False):
+        """rays: (n, 7) float32 {o, d, tmax}.  Returns a structured array of hits."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros(len(rays), HIT_DTYPE)
+        _check(lib().cr_trace_rays(self.h, _p(rays), len(rays), _p(hits), int(bool(any_hit))))
+        return hits
+
+    def trace_device(self, rays_ptr, n, hits_ptr, any_hit=False, stream=0):
+        _check(lib().cr_trace_rays_device(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr),
+                                          int(bool(any_hit)), C.c_void_p(stream)))
+
+    def render(self, width, height, spp, **kw):
+        """Mean radiance per pixel (window-sized H x W x 3 float64) and stats."""
+        d = render_desc(width, height, spp, **kw)
+        x0, y0, x1, y1 = kw.get("window") or (0, 0, width, height)
+        film = np.zeros((y1 - y0, x1 - x0, 3))
+        st = Stats()
+        _check(lib().cr_render(self.h, C.byref(d), _p(film), C.byref(st)))
+        return film, st
+
+    def render_device(self, desc, sum_ptr, sumsq_ptr, count_ptr, stream=0, stats=True):
+        st = Stats() if stats else None
+        _check(lib().cr_render_device(self.h, C.byref(desc), C.c_void_p(sum_ptr), C.c_void_p(sumsq_ptr),
+                                      C.c_void_p(count_ptr), C.c_void_p(stream),
+                                      C.byref(st) if st is not None else None))
+        return st
+
+
+def render_file(json_path, png_path, spp=1, width=1024, height=768, kernel="Radiance", tracer="CudaWavefront",
+                pfm_path=None):
+    """Renderer::render (src/core/renderer/renderer.cu:13-52)."""
+    _check(lib().cr_render_file(json_path.encode(), png_path.encode(), pfm_path.encode() if pfm_path else None,
+                                spp, width, height, kernel.encode(), tracer.encode()))
+
+
+def bsdf_eval(estimator, shader_cfg, wo, wi):
+    wo = np.ascontiguousarray(wo, np.float32)
+    wi = np.ascontiguousarray(wi, np.float32)
+    n = len(wo)
+    f = np.zeros((n, 3), np.float32)
+    pdf = np.zeros(n, np.float32)
+    _check(lib().cr_bsdf_eval(estimator, json.dumps(shader_cfg).encode(), _p(wo), _p(wi), n, _p(f), _p(pdf)))
+    return f, pdf
+
+
+def bsdf_sample(estimator, shader_cfg, wo, u):
+    wo = np.ascontiguousarray(wo, np.float32)
+    u = np.ascontiguousarray(u, np.float32)
+    n = len(wo)
+    wi = np.zeros((n, 3), np.float32)
+    w = np.zeros((n, 3), np.float32)
+    pdf = np.zeros(n, np.float32)
+    _check(lib().cr_bsdf_sample(estimator, json.dumps(shader_cfg).encode(), _p(wo), _p(u), n, _p(wi), _p(w),
+                                _p(pdf)))
+    return wi, w, pdf

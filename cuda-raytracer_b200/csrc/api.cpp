@@ -1,0 +1,1325 @@
+// Host runtime behind include/cr.h: scene model, reference JSON schema,
+// mesh importers, reference-compatible light tables, device upload, render
+// driver, PNG/PFM output.  No CPU fallback exists: every ray query and every
+// radiance sample is computed by the CUDA kernels in render.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/cr.h"
+#include "bvh_build.h"
+#include "json.h"
+#include "render.h"
+
+using namespace cr;
+
+namespace
+{
+thread_local std::string g_last_error;
+
+struct CrError : std::runtime_error
+{
+	int code;
+	CrError( int c, const std::string &m ) : std::runtime_error( m ), code( c ) {}
+};
+
+[[noreturn]] void fail( int code, const std::string &msg ) { throw CrError( code, msg ); }
+
+void cuda_check( cudaError_t e, const char *what )
+{
+	if ( e != cudaSuccess ) fail( CR_ERR_CUDA, std::string( what ) + ": " + cudaGetErrorString( e ) );
+}
+
+template <typename F>
+int guarded( F &&f )
+{
+	try
+	{
+		f();
+		return CR_OK;
+	}
+	catch ( const CrError &e )
+	{
+		g_last_error = e.what();
+		return e.code;
+	}
+	catch ( const std::exception &e )
+	{
+		g_last_error = e.what();
+		std::string m = e.what();
+		if ( m.find( "json" ) != std::string::npos ) return CR_ERR_PARSE;
+		return CR_ERR_CUDA;
+	}
+	catch ( ... )
+	{
+		g_last_error = "unknown error";
+		return CR_ERR_INVALID;
+	}
+}
+
+// ------------------------------------------------------------------ host scene model
+struct HostMesh
+{
+	std::vector<float> v, n;
+	std::vector<uint32_t> idx;
+	int shader = -1;
+};
+
+struct HostSphere
+{
+	float c[ 3 ];
+	float r;
+	int shader = -1;
+};
+
+struct HostPrim
+{
+	int kind;   // 0 mesh, 1 sphere
+	int index;  // into meshes / spheres
+};
+
+struct HostCamera
+{
+	float pos[ 3 ] = { 1, 0, 0 }, target[ 3 ] = { -1, 0, 0 }, up[ 3 ] = { 0, 0, 1 };
+	float fovx = 90;
+	int lens = 0;  // 0 pinhole, 1 orthographic
+};
+
+template <typename T>
+struct DevBuf
+{
+	T *p = nullptr;
+	size_t n = 0;
+	void upload( const std::vector<T> &h )
+	{
+		release();
+		n = h.size();
+		if ( !n ) return;
+		cuda_check( cudaMalloc( (void **)&p, sizeof( T ) * n ), "cudaMalloc" );
+		cuda_check( cudaMemcpy( p, h.data(), sizeof( T ) * n, cudaMemcpyHostToDevice ), "upload" );
+	}
+	void release()
+	{
+		if ( p ) cudaFree( p );
+		p = nullptr;
+		n = 0;
+	}
+};
+
+}  // namespace
+
+struct cr_scene
+{
+	std::vector<std::pair<std::string, DevShader>> shaders;
+	std::map<std::string, int> shader_ids;
+	Json shader_cfg;  // the scene's "shaders" object, instantiated on first use
+	std::vector<HostMesh> meshes;
+	std::vector<HostSphere> spheres;
+	std::vector<HostPrim> prims;
+	HostCamera cam;
+	bool has_camera = false;
+	uint32_t max_bounce = 16;  // RadianceKernel::Configuration (radiance.hpp:12-15)
+	int estimator = EST_KOISHI;
+	std::string kernel = "Radiance", tracer = "CPUMulticore";
+
+	// committed state
+	bool committed = false;
+	cudaStream_t stream = nullptr;
+	WideBvh bvh;
+	DevBuf<float4> attrs, light_tables, light_tris;
+	DevBuf<float> light_cdf;
+	DevBuf<DevSphere> dspheres;
+	DevBuf<DevShader> dshaders;
+	DevBuf<DevLight> dlights;
+	DevBuf<uint32_t> prim_first;
+	DevBuf<uint32_t> err;
+	std::vector<DevLight> lights;
+	std::vector<float4> tables_host;
+	uint64_t n_tris = 0;
+	float scale = 1;
+	WaveBuffers wave;
+	uint32_t wave_bounces = 0;
+
+	~cr_scene() { release(); }
+	void release_device()
+	{
+		if ( wave.capacity ) free_wave( wave, stream );
+		if ( bvh.nodes ) cudaFreeAsync( bvh.nodes, stream );
+		if ( bvh.tris ) cudaFreeAsync( bvh.tris, stream );
+		bvh = WideBvh();
+		attrs.release(), light_tables.release(), light_tris.release(), light_cdf.release();
+		dspheres.release(), dshaders.release(), dlights.release(), prim_first.release(), err.release();
+		if ( stream ) cudaStreamSynchronize( stream );
+		committed = false;
+	}
+	void release()
+	{
+		release_device();
+		if ( stream ) cudaStreamDestroy( stream );
+		stream = nullptr;
+	}
+};
+
+namespace
+{
+// ------------------------------------------------------------------ shaders
+// Factory<Shader>::create over the shader registry (src/ext/shader/shader.impl.cu:15-24).
+DevShader make_shader( const Json &cfg )
+{
+	if ( !cfg.is_array() || cfg.size() < 1 || !cfg.at( 0 ).is_string() )
+		fail( CR_ERR_PARSE, "shader config must be [Type, {props}]" );
+	const std::string &type = cfg.at( 0 ).str;
+	static const Json empty = [] {
+		Json j;
+		j.type = Json::Object;
+		return j;
+	}();
+	const Json &p = cfg.size() > 1 ? cfg.at( 1 ) : empty;
+	DevShader s;
+	std::memset( &s, 0, sizeof s );
+	float one[ 3 ] = { 1, 1, 1 };
+	if ( type == "Lambert" )  // lambert.hpp:12-19
+	{
+		float R[ 3 ] = { 1, 1, 1 }, c[ 3 ] = { 1, 1, 1 };
+		p.vec3( "R", R ), p.vec3( "color", c );
+		s.type = SH_LAMBERT;
+		for ( int i = 0; i < 3; ++i ) s.albedo[ i ] = c[ i ] * R[ i ], s.color[ i ] = c[ i ];
+	}
+	else if ( type == "GlossyBSDF" )  // glossy.hpp:11-17, beckmann.hpp:11-17
+	{
+		float c[ 3 ] = { 1, 1, 1 };
+		p.vec3( "color", c );
+		const Json *d = p.find( "distribution" );
+		if ( !d ) fail( CR_ERR_PARSE, "GlossyBSDF needs a distribution" );
+		if ( !d->is_array() || d->size() < 1 || !d->at( 0 ).is_string() )
+			fail( CR_ERR_PARSE, "distribution must be [Type, {props}]" );
+		if ( d->at( 0 ).str != "Beckmann" )
+			fail( CR_ERR_UNSUPPORTED, "GlossyBSDF distribution '" + d->at( 0 ).str + "' is not supported (Beckmann only)" );
+		float rough = d->size() > 1 ? float( d->at( 1 ).number_or( "roughness", 0.5 ) ) : 0.5f;
+		s.type = SH_GLOSSY;
+		for ( int i = 0; i < 3; ++i ) s.color[ i ] = c[ i ], s.albedo[ i ] = c[ i ];
+		s.alpha = rough;
+		s.alpha2 = rough * rough;
+	}
+	else if ( type == "Emission" )  // emission.hpp:12-20
+	{
+		float c[ 3 ] = { 1, 1, 1 };
+		p.vec3( "color", c );
+		float strength = float( p.number_or( "strength", 2.0 ) );
+		s.type = SH_EMISSION;
+		for ( int i = 0; i < 3; ++i ) s.emission[ i ] = c[ i ] * strength, s.albedo[ i ] = one[ i ], s.color[ i ] = one[ i ];
+	}
+	else if ( type == "Blackhole" || type == "RefractionBSDF" || type == "Mixed" || type == "Transparent" ||
+			  type == "GlassBSDF" )
+		fail( CR_ERR_UNSUPPORTED, "shader type '" + type + "' is outside the Radiance path implemented here" );
+	else
+		fail( CR_ERR_PARSE, "no such type: " + type );
+	return s;
+}
+
+int shader_id( cr_scene *s, const std::string &name )
+{
+	auto it = s->shader_ids.find( name );
+	if ( it != s->shader_ids.end() ) return it->second;
+	const Json *cfg = s->shader_cfg.find( name );
+	if ( !cfg ) fail( CR_ERR_INVALID, "Configuration for shader {" + name + "} not found." );
+	DevShader sh = make_shader( *cfg );
+	s->shaders.emplace_back( name, sh );
+	int id = int( s->shaders.size() - 1 );
+	s->shader_ids[ name ] = id;
+	return id;
+}
+
+// ------------------------------------------------------------------ meshes
+void smooth_normals( const std::vector<float> &v, const std::vector<uint32_t> &idx, std::vector<float> &n )
+{
+	n.assign( v.size(), 0.f );
+	for ( size_t t = 0; t + 2 < idx.size(); t += 3 )
+	{
+		const float *a = &v[ 3 * idx[ t ] ], *b = &v[ 3 * idx[ t + 1 ] ], *c = &v[ 3 * idx[ t + 2 ] ];
+		float e1[ 3 ] = { b[ 0 ] - a[ 0 ], b[ 1 ] - a[ 1 ], b[ 2 ] - a[ 2 ] };
+		float e2[ 3 ] = { c[ 0 ] - a[ 0 ], c[ 1 ] - a[ 1 ], c[ 2 ] - a[ 2 ] };
+		float fn[ 3 ] = { e1[ 1 ] * e2[ 2 ] - e1[ 2 ] * e2[ 1 ], e1[ 2 ] * e2[ 0 ] - e1[ 0 ] * e2[ 2 ],
+						  e1[ 0 ] * e2[ 1 ] - e1[ 1 ] * e2[ 0 ] };
+		for ( int k = 0; k < 3; ++k )
+			for ( int c3 = 0; c3 < 3; ++c3 ) n[ 3 * idx[ t + k ] + c3 ] += fn[ c3 ];
+	}
+	for ( size_t i = 0; i + 2 < n.size(); i += 3 )
+	{
+		float l = std::sqrt( n[ i ] * n[ i ] + n[ i + 1 ] * n[ i + 1 ] + n[ i + 2 ] * n[ i + 2 ] );
+		if ( l > 0 )
+			n[ i ] /= l, n[ i + 1 ] /= l, n[ i + 2 ] /= l;
+		else
+			n[ i ] = 0, n[ i + 1 ] = 0, n[ i + 2 ] = 1;
+	}
+}
+
+int add_mesh( cr_scene *s, const float *v, uint32_t nv, const float *n, const uint32_t *idx, uint32_t nt, int shader )
+{
+	if ( s->committed ) fail( CR_ERR_STATE, "scene already committed" );
+	if ( ( nv && !v ) || ( nt && !idx ) ) fail( CR_ERR_INVALID, "null mesh array" );
+	HostMesh m;
+	m.v.assign( v, v + size_t( nv ) * 3 );
+	m.idx.assign( idx, idx + size_t( nt ) * 3 );
+	for ( float x : m.v )
+		if ( !std::isfinite( x ) ) fail( CR_ERR_INVALID, "non-finite vertex coordinate" );
+	for ( uint32_t i : m.idx )
+		if ( i >= nv ) fail( CR_ERR_INVALID, "triangle index out of range" );
+	if ( n )
+		m.n.assign( n, n + size_t( nv ) * 3 );
+	else
+		smooth_normals( m.v, m.idx, m.n );
+	m.shader = shader;
+	s->meshes.push_back( std::move( m ) );
+	s->prims.push_back( HostPrim{ 0, int( s->meshes.size() - 1 ) } );
+	return int( s->prims.size() - 1 );
+}
+
+struct Group
+{
+	std::string name;
+	std::vector<float> v, n;
+	std::vector<uint32_t> idx;
+};
+
+std::string read_file( const std::string &path )
+{
+	std::ifstream f( path, std::ios::binary );
+	if ( !f ) fail( CR_ERR_PARSE, "cannot open " + path );
+	std::stringstream ss;
+	ss << f.rdbuf();
+	return ss.str();
+}
+
+// CRM1 binary mesh groups (written by the package's scene generator).
+std::vector<Group> load_crm( const std::string &path )
+{
+	std::string d = read_file( path );
+	size_t off = 0;
+	auto take = [&]( void *dst, size_t n ) {
+		if ( off + n > d.size() ) fail( CR_ERR_PARSE, "truncated mesh file " + path );
+		std::memcpy( dst, d.data() + off, n );
+		off += n;
+	};
+	char magic[ 4 ];
+	take( magic, 4 );
+	if ( std::memcmp( magic, "CRM1", 4 ) ) fail( CR_ERR_PARSE, "not a CRM1 mesh file: " + path );
+	uint32_t ng;
+	take( &ng, 4 );
+	std::vector<Group> out( ng );
+	for ( auto &g : out )
+	{
+		uint32_t len, nv, nt;
+		take( &len, 4 );
+		g.name.resize( len );
+		if ( len ) take( &g.name[ 0 ], len );
+		take( &nv, 4 );
+		take( &nt, 4 );
+		g.v.resize( size_t( nv ) * 3 );
+		g.n.resize( size_t( nv ) * 3 );
+		g.idx.resize( size_t( nt ) * 3 );
+		take( g.v.data(), g.v.size() * 4 );
+		take( g.n.data(), g.n.size() * 4 );
+		take( g.idx.data(), g.idx.size() * 4 );
+	}
+	return out;
+}
+
+// Wavefront OBJ: v / vn / f (polygons fanned into triangles, negative indices
+// allowed), split into one group per `usemtl` material as the reference's
+// importer splits an imported scene per material (mesh.cu:332-402).  Groups
+// without vertex normals get area-weighted smooth normals, as assimp's
+// aiProcess_GenSmoothNormals does for the reference (scene.cu:40-44).
+std::vector<Group> load_obj( const std::string &path )
+{
+	std::istringstream in( read_file( path ) );
+	std::vector<float> P, N;
+	struct Corner
+	{
+		long v, n;
+	};
+	std::vector<std::string> order;
+	std::map<std::string, std::vector<std::array<Corner, 3>>> faces;
+	std::string mat = "default";
+	std::string line;
+	size_t lineno = 0;
+	auto fix = []( long i, size_t count ) -> long { return i < 0 ? long( count ) + i : i - 1; };
+	while ( std::getline( in, line ) )
+	{
+		++lineno;
+		std::istringstream ls( line );
+		std::string tag;
+		if ( !( ls >> tag ) || tag[ 0 ] == '#' ) continue;
+		if ( tag == "v" || tag == "vn" )
+		{
+			float a, b, c;
+			if ( !( ls >> a >> b >> c ) ) fail( CR_ERR_PARSE, path + ":" + std::to_string( lineno ) + ": bad vector" );
+			auto &dst = tag == "v" ? P : N;
+			dst.push_back( a ), dst.push_back( b ), dst.push_back( c );
+		}
+		else if ( tag == "usemtl" )
+			ls >> mat;
+		else if ( tag == "f" )
+		{
+			std::vector<Corner> poly;
+			std::string tok;
+			while ( ls >> tok )
+			{
+				Corner c{ 0, -1 };
+				size_t s1 = tok.find( '/' );
+				c.v = std::stol( tok.substr( 0, s1 ) );
+				c.v = fix( c.v, P.size() / 3 );
+				if ( s1 != std::string::npos )
+				{
+					size_t s2 = tok.find( '/', s1 + 1 );
+					if ( s2 != std::string::npos && s2 + 1 < tok.size() ) c.n = fix( std::stol( tok.substr( s2 + 1 ) ), N.size() / 3 );
+				}
+				if ( c.v < 0 || size_t( c.v ) >= P.size() / 3 || ( c.n >= 0 && size_t( c.n ) >= N.size() / 3 ) )
+					fail( CR_ERR_PARSE, path + ":" + std::to_string( lineno ) + ": index out of range" );
+				poly.push_back( c );
+			}
+			if ( poly.size() < 3 ) continue;
+			if ( !faces.count( mat ) ) order.push_back( mat );
+			for ( size_t k = 1; k + 1 < poly.size(); ++k ) faces[ mat ].push_back( { poly[ 0 ], poly[ k ], poly[ k + 1 ] } );
+		}
+	}
+	std::vector<Group> out;
+	for ( auto &name : order )
+	{
+		Group g;
+		g.name = name;
+		std::map<std::pair<long, long>, uint32_t> remap;
+		bool all_n = true;
+		for ( auto &f : faces[ name ] )
+			for ( auto &c : f )
+			{
+				auto key = std::make_pair( c.v, c.n );
+				auto it = remap.find( key );
+				uint32_t id;
+				if ( it == remap.end() )
+				{
+					id = uint32_t( g.v.size() / 3 );
+					remap[ key ] = id;
+					g.v.insert( g.v.end(), &P[ 3 * c.v ], &P[ 3 * c.v ] + 3 );
+					if ( c.n >= 0 )
+						g.n.insert( g.n.end(), &N[ 3 * c.n ], &N[ 3 * c.n ] + 3 );
+					else
+						all_n = false, g.n.insert( g.n.end(), { 0.f, 0.f, 0.f } );
+				}
+				else
+					id = it->second;
+				g.idx.push_back( id );
+			}
+		if ( !all_n ) smooth_normals( g.v, g.idx, g.n );
+		out.push_back( std::move( g ) );
+	}
+	return out;
+}
+
+std::string join_path( const std::string &base, const std::string &p )
+{
+	if ( p.empty() || p[ 0 ] == '/' || base.empty() ) return p;
+	return base + "/" + p;
+}
+
+bool ends_with( const std::string &s, const std::string &e )
+{
+	return s.size() >= e.size() && std::equal( e.rbegin(), e.rend(), s.rbegin(), []( char a, char b ) {
+			   return std::tolower( (unsigned char)a ) == std::tolower( (unsigned char)b );
+		   } );
+}
+
+// Kernel configuration from the "tracer" entry (tracer.hpp:14-17, radiance.hpp:12-15).
+void read_tracer( cr_scene *s, const Json &doc )
+{
+	const Json *tr = doc.find( "tracer" );
+	if ( !tr ) return;
+	if ( !tr->is_array() || tr->size() < 1 || !tr->at( 0 ).is_string() ) fail( CR_ERR_PARSE, "tracer must be [Name, {props}]" );
+	s->tracer = tr->at( 0 ).str;
+	if ( tr->size() < 2 ) return;
+	const Json *k = tr->at( 1 ).find( "kernel" );
+	if ( !k ) return;
+	if ( !k->is_array() || k->size() < 1 || !k->at( 0 ).is_string() ) fail( CR_ERR_PARSE, "kernel must be [Name, {props}]" );
+	s->kernel = k->at( 0 ).str;
+	if ( k->size() > 1 )
+	{
+		double mb = k->at( 1 ).number_or( "maxBounce", 16 );
+		if ( mb < 0 || mb > 1024 ) fail( CR_ERR_INVALID, "maxBounce out of range" );
+		s->max_bounce = uint32_t( mb );
+		std::string est = k->at( 1 ).string_or( "estimator", "koishi" );
+		if ( est == "koishi" )
+			s->estimator = EST_KOISHI;
+		else if ( est == "mis" )
+			s->estimator = EST_MIS;
+		else
+			fail( CR_ERR_INVALID, "unknown estimator '" + est + "' (koishi or mis)" );
+	}
+}
+
+// Scene::Scene (src/core/meta/scene.cu:18-219).
+void load_scene( cr_scene *s, const std::string &text, const std::string &base )
+{
+	Json doc = parse_json( text );
+	const Json *sc = doc.find( "scene" );
+	if ( !sc || !sc->is_object() ) fail( CR_ERR_PARSE, "missing \"scene\" object" );
+	read_tracer( s, doc );
+	if ( const Json *sh = sc->find( "shaders" ) )
+	{
+		if ( !sh->is_object() ) fail( CR_ERR_PARSE, "\"shaders\" must be an object" );
+		s->shader_cfg = *sh;
+	}
+	else
+		s->shader_cfg.type = Json::Object;
+	if ( const Json *cams = sc->find( "camera" ) )
+	{
+		if ( !cams->is_array() ) fail( CR_ERR_PARSE, "\"camera\" must be an array" );
+		if ( cams->size() )
+		{
+			const Json &c = cams->at( 0 );  // Renderer uses scene.camera[0] (renderer.cu:21-25)
+			HostCamera hc;
+			std::string lens = c.string_or( "lens", "pinhole" );
+			if ( lens == "orthographic" )
+				hc.lens = 1;
+			else if ( lens != "pinhole" )
+				fail( CR_ERR_PARSE, "unknown lens type: " + lens );
+			hc.fovx = float( c.number_or( "fovx", 90 ) );
+			c.vec3( "position", hc.pos ), c.vec3( "target", hc.target ), c.vec3( "upaxis", hc.up );
+			s->cam = hc;
+			s->has_camera = true;
+		}
+	}
+	bool imported = false;
+	if ( const Json *assets = sc->find( "assets" ) )
+	{
+		if ( !assets->is_array() ) fail( CR_ERR_PARSE, "\"assets\" must be an array" );
+		for ( auto &a : assets->arr )
+		{
+			if ( !a.is_array() || a.size() < 1 || !a.at( 0 ).is_string() ) fail( CR_ERR_PARSE, "asset must be [name, {props}]" );
+			const std::string &name = a.at( 0 ).str;
+			Json none;
+			none.type = Json::Object;
+			const Json &p = a.size() > 1 ? a.at( 1 ) : none;
+			if ( name == "import" )
+			{
+				if ( imported ) fail( CR_ERR_INVALID, "importing multiple scenes is not allowed" );
+				imported = true;
+				std::string path = join_path( base, p.string_or( "path", "" ) );
+				std::vector<Group> groups = ends_with( path, ".crm" ) ? load_crm( path ) : load_obj( path );
+				for ( auto &g : groups )
+				{
+					if ( g.idx.empty() ) continue;
+					int sid = shader_id( s, g.name );
+					add_mesh( s, g.v.data(), uint32_t( g.v.size() / 3 ), g.n.data(), g.idx.data(),
+							  uint32_t( g.idx.size() / 3 ), sid );
+				}
+			}
+			else if ( name == "sphere" )
+			{
+				HostSphere hs;
+				if ( !p.vec3( "o", hs.c ) ) fail( CR_ERR_PARSE, "sphere needs \"o\"" );
+				hs.r = float( p.number_or( "r", 1.0 ) );
+				hs.shader = shader_id( s, p.string_or( "shader", "" ) );
+				s->spheres.push_back( hs );
+				s->prims.push_back( HostPrim{ 1, int( s->spheres.size() - 1 ) } );
+			}
+			else if ( name.find( "light" ) != std::string::npos || name.find( "Light" ) != std::string::npos )
+			{
+				if ( name == "pointLight" )
+					fail( CR_ERR_UNSUPPORTED, "pointLight is outside the area-light Radiance path implemented here" );
+				fail( CR_ERR_PARSE, "unknown light type: " + name );
+			}
+			else
+				fail( CR_ERR_PARSE, "unknown asset type: " + name );
+		}
+	}
+}
+
+// ------------------------------------------------------------------ light tables
+// Face order of a mesh as the reference stores it: the list padded to a
+// multiple of 4 with copies of its last triangle (createBVH, mesh.cu:135-143),
+// then permuted by the reference's recursive builder (doCreateBVH, mesh.cu:35-111),
+// whose comparator sorts are reproduced with the same std::sort.
+struct TriBox
+{
+	uint32_t idx;
+	float vmax[ 3 ], vmin[ 3 ];
+};
+
+float box_volume( const float lo[ 3 ], const float hi[ 3 ] )
+{
+	return ( hi[ 0 ] - lo[ 0 ] ) * ( hi[ 1 ] - lo[ 1 ] ) * ( hi[ 2 ] - lo[ 2 ] );
+}
+
+void reference_face_order( std::vector<TriBox> &t, size_t b, size_t e )
+{
+	size_t len = e - b;
+	if ( len <= 16 ) return;
+	float lo[ 3 ], hi[ 3 ];
+	for ( int a = 0; a < 3; ++a ) lo[ a ] = t[ b ].vmin[ a ], hi[ a ] = t[ b ].vmax[ a ];
+	for ( size_t i = b; i < e; ++i )
+		for ( int a = 0; a < 3; ++a ) lo[ a ] = std::min( lo[ a ], t[ i ].vmin[ a ] ), hi[ a ] = std::max( hi[ a ], t[ i ].vmax[ a ] );
+	float w[ 3 ] = { hi[ 0 ] - lo[ 0 ], hi[ 1 ] - lo[ 1 ], hi[ 2 ] - lo[ 2 ] };
+	int ax = ( w[ 0 ] >= w[ 1 ] && w[ 0 ] >= w[ 2 ] ) ? 0 : ( w[ 1 ] >= w[ 0 ] && w[ 1 ] >= w[ 2 ] ) ? 1 : 2;
+	std::sort( t.begin() + b, t.begin() + e, [ax]( const TriBox &x, const TriBox &y ) { return x.vmin[ ax ] < y.vmin[ ax ]; } );
+	const float inf = std::numeric_limits<float>::infinity();
+	std::vector<float> low( len ), high( len );
+	float a0[ 3 ] = { inf, inf, inf }, a1[ 3 ] = { -inf, -inf, -inf };
+	for ( size_t i = 0; i < len; ++i )
+	{
+		for ( int a = 0; a < 3; ++a ) a0[ a ] = std::min( t[ b + i ].vmin[ a ], a0[ a ] ), a1[ a ] = std::max( t[ b + i ].vmax[ a ], a1[ a ] );
+		low[ i ] = box_volume( a0, a1 );
+	}
+	for ( int a = 0; a < 3; ++a ) a0[ a ] = inf, a1[ a ] = -inf;
+	for ( size_t i = len; i-- > 0; )
+	{
+		for ( int a = 0; a < 3; ++a ) a0[ a ] = std::min( t[ b + i ].vmin[ a ], a0[ a ] ), a1[ a ] = std::max( t[ b + i ].vmax[ a ], a1[ a ] );
+		high[ i ] = box_volume( a0, a1 );
+	}
+	for ( size_t i = 4; i < len; i += 4 )
+		if ( low[ i - 1 ] - high[ i ] >= 0.f )
+		{
+			reference_face_order( t, b, b + i );
+			reference_face_order( t, b + i, e );
+			return;
+		}
+	reference_face_order( t, b, b + len / 2 );
+	reference_face_order( t, b + len / 2, e );
+}
+
+// The reference's 48-bit generator (src/core/misc/sampler.hpp:22-36).
+struct Lcg48
+{
+	uint64_t x;
+	float next()
+	{
+		x = ( 0x5DEECE66Dull * x + 0xB16ull ) & 0xFFFFFFFFFFFFull;
+		return float( uint32_t( x >> 16 ) ) / float( 0x100000000LL );
+	}
+};
+
+// Mesh::generateSamples (src/core/primitive/mesh.hpp:61-84): 1024 points,
+// face picked uniformly by index, barycentrics (min, max) of two uniforms;
+// pdf = 1 / total area over the padded face list.
+float reference_light_table( const HostMesh &m, Lcg48 &rng, float4 *out )
+{
+	size_t nt = m.idx.size() / 3;
+	std::vector<TriBox> t( nt );
+	for ( size_t i = 0; i < nt; ++i )
+	{
+		t[ i ].idx = uint32_t( i );
+		for ( int a = 0; a < 3; ++a )
+		{
+			float x0 = m.v[ 3 * m.idx[ 3 * i ] + a ], x1 = m.v[ 3 * m.idx[ 3 * i + 1 ] + a ], x2 = m.v[ 3 * m.idx[ 3 * i + 2 ] + a ];
+			t[ i ].vmax[ a ] = std::max( x0, std::max( x1, x2 ) );
+			t[ i ].vmin[ a ] = std::min( x0, std::min( x1, x2 ) );
+		}
+	}
+	TriBox last = t.back();
+	while ( t.size() % 4 ) t.push_back( last );
+	reference_face_order( t, 0, t.size() );
+	size_t nf = t.size();
+	auto vert = [&]( uint32_t tri, int k, int a ) { return m.v[ 3 * m.idx[ 3 * tri + k ] + a ]; };
+	auto nrm = [&]( uint32_t tri, int k, int a ) { return m.n[ 3 * m.idx[ 3 * tri + k ] + a ]; };
+	for ( int i = 0; i < 1024; ++i )
+	{
+		float r = rng.next();
+		uint32_t f = std::min( uint32_t( std::floor( r * float( nf ) ) ), uint32_t( nf - 1 ) );
+		float a = rng.next(), b = rng.next();
+		float u = std::min( a, b ), v = std::max( a, b );
+		uint32_t tri = t[ f ].idx;
+		float p[ 3 ], n[ 3 ];
+		float w0 = 1 - u - v;
+		for ( int c = 0; c < 3; ++c )
+		{
+			float o = vert( tri, 0, c ), d1 = vert( tri, 1, c ) - o, d2 = vert( tri, 2, c ) - o;
+			p[ c ] = o + d1 * u + d2 * v;
+			n[ c ] = nrm( tri, 0, c ) * w0 + nrm( tri, 1, c ) * u + nrm( tri, 2, c ) * v;
+		}
+		float inv = 1.0f / std::sqrt( n[ 0 ] * n[ 0 ] + n[ 1 ] * n[ 1 ] + n[ 2 ] * n[ 2 ] );
+		out[ 2 * i ] = make_float4( p[ 0 ], p[ 1 ], p[ 2 ], 0.f );
+		out[ 2 * i + 1 ] = make_float4( n[ 0 ] * inv, n[ 1 ] * inv, n[ 2 ] * inv, 0.f );
+	}
+	float area = 0;
+	for ( auto &tb : t )
+	{
+		float d1[ 3 ], d2[ 3 ];
+		for ( int c = 0; c < 3; ++c ) d1[ c ] = vert( tb.idx, 1, c ) - vert( tb.idx, 0, c ), d2[ c ] = vert( tb.idx, 2, c ) - vert( tb.idx, 0, c );
+		float cx = d1[ 1 ] * d2[ 2 ] - d2[ 1 ] * d1[ 2 ], cy = d1[ 2 ] * d2[ 0 ] - d2[ 2 ] * d1[ 0 ], cz = d1[ 0 ] * d2[ 1 ] - d2[ 0 ] * d1[ 1 ];
+		area = float( double( area ) + double( std::sqrt( cx * cx + cy * cy + cz * cz ) ) * .5 );
+	}
+	return 1.f / area;
+}
+
+// ------------------------------------------------------------------ commit
+void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
+{
+	if ( s->committed ) return;
+	if ( !s->stream ) cuda_check( cudaStreamCreateWithFlags( &s->stream, cudaStreamNonBlocking ), "stream" );
+	cudaStream_t st = user_stream ? user_stream : s->stream;
+	uint64_t nt = 0;
+	for ( auto &m : s->meshes ) nt += m.idx.size() / 3;
+	if ( nt >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many triangles" );
+	s->n_tris = nt;
+	std::vector<float4> src( 3 * nt ), attrs( 3 * nt );
+	std::vector<uint32_t> prim_first( s->prims.size(), 0 );
+	std::vector<int> prim_light( s->prims.size(), -1 );
+	// Lights: every Emission-shaded primitive (scene.cu:200-216), in primitive order.
+	std::vector<DevLight> lights;
+	std::vector<float4> tables, ltris;
+	std::vector<float> cdf;
+	Lcg48 rng{ light_seed & 0xFFFFFFFFFFFFull };
+	for ( size_t p = 0; p < s->prims.size(); ++p )
+	{
+		const HostPrim &hp = s->prims[ p ];
+		int shader = hp.kind == 0 ? s->meshes[ hp.index ].shader : s->spheres[ hp.index ].shader;
+		const DevShader &sh = s->shaders[ shader ].second;
+		if ( sh.type != SH_EMISSION ) continue;
+		DevLight L;
+		std::memset( &L, 0, sizeof L );
+		for ( int c = 0; c < 3; ++c ) L.emission[ c ] = sh.emission[ c ];
+		if ( hp.kind == 1 )
+		{
+			const HostSphere &hs = s->spheres[ hp.index ];
+			L.kind = LIGHT_SPHERE;
+			L.index = hp.index;
+			float r2 = hs.r * hs.r;
+			L.area = float( 4.0 * M_PI * double( r2 ) );
+			L.koishi_pdf = 1.f / ( 4.f * float( M_PI ) * r2 );
+		}
+		else
+		{
+			const HostMesh &m = s->meshes[ hp.index ];
+			if ( m.idx.empty() ) continue;
+			L.kind = LIGHT_MESH;
+			L.index = int( ltris.size() / 3 );
+			L.n_tris = int( m.idx.size() / 3 );
+			L.table = int( tables.size() / 2 );
+			tables.resize( tables.size() + 2048 );
+			L.koishi_pdf = reference_light_table( m, rng, &tables[ tables.size() - 2048 ] );
+			L.cdf = int( cdf.size() );
+			double acc = 0;
+			for ( int t = 0; t < L.n_tris; ++t )
+			{
+				const float *a = &m.v[ 3 * m.idx[ 3 * t ] ], *b = &m.v[ 3 * m.idx[ 3 * t + 1 ] ], *c = &m.v[ 3 * m.idx[ 3 * t + 2 ] ];
+				double e1[ 3 ] = { double( b[ 0 ] ) - a[ 0 ], double( b[ 1 ] ) - a[ 1 ], double( b[ 2 ] ) - a[ 2 ] };
+				double e2[ 3 ] = { double( c[ 0 ] ) - a[ 0 ], double( c[ 1 ] ) - a[ 1 ], double( c[ 2 ] ) - a[ 2 ] };
+				double cx = e1[ 1 ] * e2[ 2 ] - e1[ 2 ] * e2[ 1 ], cy = e1[ 2 ] * e2[ 0 ] - e1[ 0 ] * e2[ 2 ], cz = e1[ 0 ] * e2[ 1 ] - e1[ 1 ] * e2[ 0 ];
+				acc += 0.5 * std::sqrt( cx * cx + cy * cy + cz * cz );  // FP64 prefix sum
+				cdf.push_back( float( acc ) );
+				ltris.push_back( make_float4( a[ 0 ], a[ 1 ], a[ 2 ], 0 ) );
+				ltris.push_back( make_float4( b[ 0 ], b[ 1 ], b[ 2 ], 0 ) );
+				ltris.push_back( make_float4( c[ 0 ], c[ 1 ], c[ 2 ], 0 ) );
+			}
+			L.area = float( acc );
+			if ( !( acc > 0 ) ) continue;  // a degenerate emitter contributes nothing
+		}
+		prim_light[ p ] = int( lights.size() );
+		lights.push_back( L );
+	}
+	// Flatten triangles in primitive order.
+	uint64_t g = 0;
+	float lo[ 3 ] = { INFINITY, INFINITY, INFINITY }, hi[ 3 ] = { -INFINITY, -INFINITY, -INFINITY };
+	for ( size_t p = 0; p < s->prims.size(); ++p )
+	{
+		const HostPrim &hp = s->prims[ p ];
+		prim_first[ p ] = uint32_t( g );
+		if ( hp.kind != 0 ) continue;
+		const HostMesh &m = s->meshes[ hp.index ];
+		for ( size_t t = 0; t < m.idx.size() / 3; ++t, ++g )
+		{
+			for ( int k = 0; k < 3; ++k )
+			{
+				const float *v = &m.v[ 3 * m.idx[ 3 * t + k ] ], *n = &m.n[ 3 * m.idx[ 3 * t + k ] ];
+				src[ 3 * g + k ] = make_float4( v[ 0 ], v[ 1 ], v[ 2 ], 0.f );
+				for ( int a = 0; a < 3; ++a ) lo[ a ] = std::min( lo[ a ], v[ a ] ), hi[ a ] = std::max( hi[ a ], v[ a ] );
+				int w = k == 0 ? m.shader : k == 1 ? int( p ) : prim_light[ p ];
+				float wf;
+				std::memcpy( &wf, &w, 4 );
+				attrs[ 3 * g + k ] = make_float4( n[ 0 ], n[ 1 ], n[ 2 ], wf );
+			}
+		}
+	}
+	std::vector<DevSphere> ds;
+	for ( size_t p = 0; p < s->prims.size(); ++p )
+	{
+		const HostPrim &hp = s->prims[ p ];
+		if ( hp.kind != 1 ) continue;
+		const HostSphere &hs = s->spheres[ hp.index ];
+		DevSphere d;
+		for ( int a = 0; a < 3; ++a )
+			d.c[ a ] = hs.c[ a ], lo[ a ] = std::min( lo[ a ], hs.c[ a ] - hs.r ), hi[ a ] = std::max( hi[ a ], hs.c[ a ] + hs.r );
+		d.r2 = hs.r * hs.r;  // the reference keeps r^2 (sphere.hpp:11-16)
+		d.r = std::sqrt( d.r2 );
+		d.shader = hs.shader;
+		d.prim = int( p );
+		d.light = prim_light[ p ];
+		ds.push_back( d );
+	}
+	float sc = 1;
+	for ( int a = 0; a < 3; ++a )
+		if ( std::isfinite( lo[ a ] ) ) sc = std::max( sc, std::max( std::fabs( lo[ a ] ), std::fabs( hi[ a ] ) ) );
+	s->scale = sc;
+	std::vector<DevShader> dsh;
+	for ( auto &x : s->shaders ) dsh.push_back( x.second );
+
+	s->attrs.upload( attrs );
+	s->dspheres.upload( ds );
+	s->dshaders.upload( dsh );
+	s->dlights.upload( lights );
+	s->light_tables.upload( tables );
+	s->light_tris.upload( ltris );
+	s->light_cdf.upload( cdf );
+	s->prim_first.upload( prim_first );
+	s->err.upload( std::vector<uint32_t>( 1, 0 ) );
+	s->lights = lights;
+	s->tables_host = tables;
+	if ( nt )
+	{
+		float4 *d_src = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&d_src, sizeof( float4 ) * src.size(), st ), "cudaMalloc" );
+		cuda_check( cudaMemcpyAsync( d_src, src.data(), sizeof( float4 ) * src.size(), cudaMemcpyHostToDevice, st ), "upload" );
+		try
+		{
+			build_wide_bvh( d_src, uint32_t( nt ), s->bvh, st );
+		}
+		catch ( const std::exception &e )
+		{
+			cudaFreeAsync( d_src, st );
+			fail( CR_ERR_CUDA, e.what() );
+		}
+		cudaFreeAsync( d_src, st );
+		if ( s->bvh.depth > uint32_t( TRAVERSAL_STACK ) )
+			fail( CR_ERR_INVALID, "BVH depth " + std::to_string( s->bvh.depth ) + " exceeds the traversal stack" );
+	}
+	cuda_check( cudaStreamSynchronize( st ), "commit" );
+	s->committed = true;
+}
+
+DevScene dev_scene( const cr_scene *s )
+{
+	DevScene d;
+	std::memset( &d, 0, sizeof d );
+	d.nodes = s->bvh.nodes;
+	d.tris = s->bvh.tris;
+	d.attrs = s->attrs.p;
+	d.spheres = s->dspheres.p;
+	d.shaders = s->dshaders.p;
+	d.lights = s->dlights.p;
+	d.light_tables = s->light_tables.p;
+	d.light_tris = s->light_tris.p;
+	d.light_cdf = s->light_cdf.p;
+	d.prim_first = s->prim_first.p;
+	d.n_nodes = s->bvh.n_nodes;
+	d.n_tris = uint32_t( s->n_tris );
+	d.n_spheres = uint32_t( s->dspheres.n );
+	d.n_lights = uint32_t( s->dlights.n );
+	d.n_shaders = uint32_t( s->dshaders.n );
+	d.scene_scale = s->scale;
+	return d;
+}
+
+// PinholeLens (src/core/misc/lens.hpp:15-27) for a W x H image at spp.
+DevCamera make_camera( const HostCamera &c, uint32_t w, uint32_t h, uint32_t spp )
+{
+	auto norm = []( const float a[ 3 ], float o[ 3 ] ) {
+		float r = 1.0f / std::sqrt( a[ 0 ] * a[ 0 ] + a[ 1 ] * a[ 1 ] + a[ 2 ] * a[ 2 ] );
+		for ( int i = 0; i < 3; ++i ) o[ i ] = a[ i ] * r;
+	};
+	auto crs = []( const float a[ 3 ], const float b[ 3 ], float o[ 3 ] ) {
+		o[ 0 ] = a[ 1 ] * b[ 2 ] - b[ 1 ] * a[ 2 ];
+		o[ 1 ] = a[ 2 ] * b[ 0 ] - b[ 2 ] * a[ 0 ];
+		o[ 2 ] = a[ 0 ] * b[ 1 ] - b[ 0 ] * a[ 1 ];
+	};
+	DevCamera d;
+	d.width = w, d.height = h;
+	d.pw = uint32_t( std::ceil( std::sqrt( double( spp ) ) ) );
+	float t[ 3 ], tmp[ 3 ];
+	norm( c.target, t );
+	float scale = float( double( w ) / ( 2 * std::tan( double( c.fovx ) * .5 * M_PI / 180.0 ) ) );
+	for ( int i = 0; i < 3; ++i ) d.n[ i ] = t[ i ] * scale, d.o[ i ] = c.pos[ i ];
+	crs( d.n, c.up, tmp );
+	norm( tmp, d.u );
+	crs( d.n, d.u, tmp );
+	norm( tmp, d.v );
+	for ( int i = 0; i < 3; ++i ) d.du[ i ] = d.u[ i ] / float( d.pw ), d.dv[ i ] = d.v[ i ] / float( d.pw );
+	return d;
+}
+
+struct Resolved
+{
+	RenderConfig cfg;
+	DevScene sc;
+	uint64_t samples;
+};
+
+Resolved resolve( cr_scene *s, const cr_render_desc *desc )
+{
+	if ( !s || !desc ) fail( CR_ERR_INVALID, "null argument" );
+	if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+	if ( !desc->width || !desc->height || !desc->spp ) fail( CR_ERR_INVALID, "width, height and spp must be positive" );
+	if ( !s->has_camera ) fail( CR_ERR_INVALID, "no camera in the scene" );
+	if ( s->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, "orthographic lens is outside the Radiance path implemented here" );
+	if ( s->kernel != "Radiance" ) fail( CR_ERR_UNSUPPORTED, "kernel '" + s->kernel + "' is not implemented (Radiance only)" );
+	if ( desc->guiding ) fail( CR_ERR_UNSUPPORTED, "learned path guiding is not available in this build" );
+	Resolved r;
+	RenderConfig &c = r.cfg;
+	uint32_t x0 = desc->x0, y0 = desc->y0, x1 = desc->x1, y1 = desc->y1;
+	if ( !x0 && !y0 && !x1 && !y1 ) x1 = desc->width, y1 = desc->height;
+	if ( x1 > desc->width || y1 > desc->height || x0 >= x1 || y0 >= y1 ) fail( CR_ERR_INVALID, "bad pixel window" );
+	c.spp = desc->spp;
+	c.max_bounce = desc->max_bounce == UINT32_MAX ? s->max_bounce : desc->max_bounce;
+	if ( c.max_bounce > 1024 ) fail( CR_ERR_INVALID, "max_bounce out of range" );
+	c.estimator = desc->estimator < 0 ? s->estimator : desc->estimator;
+	if ( c.estimator != EST_KOISHI && c.estimator != EST_MIS ) fail( CR_ERR_INVALID, "unknown estimator" );
+	c.x0 = x0, c.y0 = y0, c.ww = x1 - x0, c.wh = y1 - y0;
+	c.seed = desc->seed;
+	r.samples = uint64_t( c.ww ) * c.wh * c.spp;
+	uint64_t cap = desc->wave_paths ? desc->wave_paths : ( 1u << 22 );
+	cap = std::min<uint64_t>( cap, r.samples );
+	cap = std::min<uint64_t>( cap, 1ull << 30 );
+	c.wave_paths = uint32_t( cap );
+	c.count_work = desc->count_work != 0;
+	r.sc = dev_scene( s );
+	r.sc.cam = make_camera( s->cam, desc->width, desc->height, desc->spp );
+	return r;
+}
+
+void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t st )
+{
+	if ( s->wave.capacity >= cap && s->wave_bounces >= max_bounce ) return;
+	if ( s->wave.capacity ) free_wave( s->wave, st );
+	alloc_wave( s->wave, cap, max_bounce, st );
+	s->wave_bounces = max_bounce;
+}
+
+void check_device_error( cr_scene *s, cudaStream_t st )
+{
+	uint32_t e = 0;
+	cuda_check( cudaMemcpyAsync( &e, s->wave.capacity ? s->wave.err : s->err.p, 4, cudaMemcpyDeviceToHost, st ), "error word" );
+	cuda_check( cudaStreamSynchronize( st ), "error word" );
+	if ( e ) fail( CR_ERR_DEVICE, "a traversal kernel reported error flags " + std::to_string( e ) +
+								  " (1: stack overflow, 2: node index or budget, 4: triangle index)" );
+}
+
+void fill_stats( cr_stats *out, const StageTimes &t, uint64_t samples )
+{
+	if ( !out ) return;
+	std::memset( out, 0, sizeof *out );
+	out->ms_total = t.total, out->ms_extend = t.extend, out->ms_shadow = t.shadow, out->ms_shade = t.shade;
+	out->ms_other = t.other;
+	out->samples = samples;
+	out->rays_extend = t.rays_extend, out->rays_shadow = t.rays_shadow;
+	out->nodes = t.nodes, out->tris = t.tris, out->shadow_nodes = t.shadow_nodes, out->shadow_tris = t.shadow_tris;
+	out->launches = t.launches, out->waves = t.waves;
+	out->extend_launches = t.extend_launches, out->shadow_launches = t.shadow_launches;
+}
+
+void render_device( cr_scene *s, const cr_render_desc *desc, double *sum, double *sq, uint32_t *cnt, cudaStream_t st,
+					cr_stats *stats )
+{
+	Resolved r = resolve( s, desc );
+	ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st );
+	StageTimes t;
+	render_waves( r.sc, r.cfg, s->wave, sum, sq, cnt, st, stats ? &t : nullptr );
+	if ( stats )
+	{
+		fill_stats( stats, t, r.samples );
+		check_device_error( s, st );
+	}
+}
+
+// ------------------------------------------------------------------ PNG
+uint32_t crc32( const unsigned char *p, size_t n, uint32_t c = 0xFFFFFFFFu )
+{
+	static uint32_t table[ 256 ];
+	static bool init = false;
+	if ( !init )
+	{
+		for ( uint32_t i = 0; i < 256; ++i )
+		{
+			uint32_t x = i;
+			for ( int k = 0; k < 8; ++k ) x = ( x & 1 ) ? 0xEDB88320u ^ ( x >> 1 ) : x >> 1;
+			table[ i ] = x;
+		}
+		init = true;
+	}
+	for ( size_t i = 0; i < n; ++i ) c = table[ ( c ^ p[ i ] ) & 0xFF ] ^ ( c >> 8 );
+	return c;
+}
+
+void put_be32( std::string &s, uint32_t v )
+{
+	s += char( v >> 24 ), s += char( v >> 16 ), s += char( v >> 8 ), s += char( v );
+}
+
+void png_chunk( std::string &out, const char *type, const std::string &data )
+{
+	put_be32( out, uint32_t( data.size() ) );
+	std::string td = std::string( type, 4 ) + data;
+	out += td;
+	put_be32( out, crc32( (const unsigned char *)td.data(), td.size() ) ^ 0xFFFFFFFFu );
+}
+
+// 8-bit RGB PNG with stored (uncompressed) deflate blocks.
+void write_png( const std::string &path, uint32_t w, uint32_t h, const double *rgb )
+{
+	std::string raw;
+	raw.reserve( size_t( h ) * ( 1 + 3 * size_t( w ) ) );
+	for ( uint32_t y = 0; y < h; ++y )
+	{
+		raw += char( 0 );
+		for ( uint32_t x = 0; x < 3 * w; ++x )
+		{
+			double c = rgb[ size_t( y ) * 3 * w + x ];
+			c = std::min( std::max( c, 0.0 ), 1.0 );  // util::Image<3> Component (image.hpp:29-40)
+			raw += char( (unsigned char)( float( c ) * 255 ) );
+		}
+	}
+	std::string z;
+	z += char( 0x78 ), z += char( 0x01 );
+	size_t off = 0;
+	do
+	{
+		size_t n = std::min<size_t>( 65535, raw.size() - off );
+		bool last = off + n == raw.size();
+		z += char( last ? 1 : 0 );
+		z += char( n & 0xFF ), z += char( n >> 8 ), z += char( ~n & 0xFF ), z += char( ( ~n >> 8 ) & 0xFF );
+		z.append( raw, off, n );
+		off += n;
+	} while ( off < raw.size() );
+	uint32_t a = 1, b = 0;
+	for ( unsigned char c : raw ) a = ( a + c ) % 65521, b = ( b + a ) % 65521;
+	put_be32( z, ( b << 16 ) | a );
+	std::string out = "\x89PNG\r\n\x1a\n";
+	std::string ihdr;
+	put_be32( ihdr, w ), put_be32( ihdr, h );
+	ihdr += char( 8 ), ihdr += char( 2 ), ihdr += char( 0 ), ihdr += char( 0 ), ihdr += char( 0 );
+	png_chunk( out, "IHDR", ihdr );
+	png_chunk( out, "IDAT", z );
+	png_chunk( out, "IEND", "" );
+	std::ofstream f( path, std::ios::binary );
+	if ( !f ) fail( CR_ERR_INVALID, "cannot write " + path );
+	f.write( out.data(), std::streamsize( out.size() ) );
+}
+
+void write_pfm( const std::string &path, uint32_t w, uint32_t h, const double *rgb )
+{
+	std::ofstream f( path, std::ios::binary );
+	if ( !f ) fail( CR_ERR_INVALID, "cannot write " + path );
+	f << "PF\n" << w << " " << h << "\n-1.0\n";
+	std::vector<float> row( 3 * size_t( w ) );
+	for ( uint32_t y = h; y-- > 0; )  // PFM rows run bottom to top
+	{
+		for ( size_t x = 0; x < 3 * size_t( w ); ++x ) row[ x ] = float( rgb[ size_t( y ) * 3 * w + x ] );
+		f.write( (const char *)row.data(), std::streamsize( row.size() * 4 ) );
+	}
+}
+
+std::string dir_of( const std::string &p )
+{
+	size_t k = p.find_last_of( '/' );
+	return k == std::string::npos ? std::string( "." ) : p.substr( 0, k );
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char *cr_last_error( void ) { return g_last_error.c_str(); }
+const char *cr_version( void ) { return "cr_b200 1.0 (sm_100a)"; }
+
+int cr_scene_create_empty( cr_scene **out )
+{
+	return guarded( [&] {
+		if ( !out ) fail( CR_ERR_INVALID, "null output" );
+		auto *s = new cr_scene();
+		s->shader_cfg.type = Json::Object;
+		*out = s;
+	} );
+}
+
+int cr_scene_create( const char *json_text, const char *base_dir, cr_scene **out )
+{
+	return guarded( [&] {
+		if ( !json_text || !out ) fail( CR_ERR_INVALID, "null argument" );
+		*out = nullptr;
+		std::unique_ptr<cr_scene> s( new cr_scene() );
+		load_scene( s.get(), json_text, base_dir ? base_dir : "" );
+		commit( s.get(), 0x330E, nullptr );
+		*out = s.release();
+	} );
+}
+
+int cr_scene_add_shader( cr_scene *s, const char *name, const char *config_json )
+{
+	int id = -1;
+	int rc = guarded( [&] {
+		if ( !s || !name || !config_json ) fail( CR_ERR_INVALID, "null argument" );
+		if ( s->committed ) fail( CR_ERR_STATE, "scene already committed" );
+		Json cfg = parse_json( config_json );
+		DevShader sh = make_shader( cfg );
+		auto it = s->shader_ids.find( name );
+		if ( it != s->shader_ids.end() )
+			s->shaders[ it->second ].second = sh, id = it->second;
+		else
+		{
+			s->shaders.emplace_back( name, sh );
+			id = int( s->shaders.size() - 1 );
+			s->shader_ids[ name ] = id;
+		}
+	} );
+	return rc == CR_OK ? id : rc;
+}
+
+int cr_scene_add_mesh( cr_scene *s, const float *v, uint32_t nv, const float *n, const uint32_t *idx, uint32_t nt,
+					   const char *shader )
+{
+	int id = -1;
+	int rc = guarded( [&] {
+		if ( !s || !shader ) fail( CR_ERR_INVALID, "null argument" );
+		id = add_mesh( s, v, nv, n, idx, nt, shader_id( s, shader ) );
+	} );
+	return rc == CR_OK ? id : rc;
+}
+
+int cr_scene_add_sphere( cr_scene *s, const float *c, float r, const char *shader )
+{
+	int id = -1;
+	int rc = guarded( [&] {
+		if ( !s || !c || !shader ) fail( CR_ERR_INVALID, "null argument" );
+		if ( s->committed ) fail( CR_ERR_STATE, "scene already committed" );
+		if ( !( r > 0 ) || !std::isfinite( r ) ) fail( CR_ERR_INVALID, "sphere radius must be positive" );
+		HostSphere hs;
+		std::memcpy( hs.c, c, sizeof hs.c );
+		hs.r = r;
+		hs.shader = shader_id( s, shader );
+		s->spheres.push_back( hs );
+		s->prims.push_back( HostPrim{ 1, int( s->spheres.size() - 1 ) } );
+		id = int( s->prims.size() - 1 );
+	} );
+	return rc == CR_OK ? id : rc;
+}
+
+int cr_scene_set_camera( cr_scene *s, const float *pos, const float *target, const float *up, float fovx )
+{
+	return guarded( [&] {
+		if ( !s || !pos || !target || !up ) fail( CR_ERR_INVALID, "null argument" );
+		std::memcpy( s->cam.pos, pos, 12 );
+		std::memcpy( s->cam.target, target, 12 );
+		std::memcpy( s->cam.up, up, 12 );
+		s->cam.fovx = fovx;
+		s->cam.lens = 0;
+		s->has_camera = true;
+	} );
+}
+
+int cr_scene_commit( cr_scene *s, uint64_t light_seed, void *stream )
+{
+	return guarded( [&] {
+		if ( !s ) fail( CR_ERR_INVALID, "null scene" );
+		commit( s, light_seed, (cudaStream_t)stream );
+	} );
+}
+
+int cr_scene_info( const cr_scene *s, uint64_t *nt, uint32_t *np, uint32_t *nl, uint32_t *nn )
+{
+	return guarded( [&] {
+		if ( !s ) fail( CR_ERR_INVALID, "null scene" );
+		if ( nt ) *nt = s->n_tris;
+		if ( np ) *np = uint32_t( s->prims.size() );
+		if ( nl ) *nl = uint32_t( s->lights.size() );
+		if ( nn ) *nn = s->bvh.n_nodes;
+	} );
+}
+
+void cr_scene_destroy( cr_scene *s ) { delete s; }
+
+int cr_light_table( const cr_scene *s, uint32_t light, float *out, float *pdf )
+{
+	return guarded( [&] {
+		if ( !s || !out ) fail( CR_ERR_INVALID, "null argument" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		if ( light >= s->lights.size() ) fail( CR_ERR_INVALID, "no such light" );
+		const DevLight &L = s->lights[ light ];
+		if ( L.kind != LIGHT_MESH ) fail( CR_ERR_INVALID, "light is not a mesh light" );
+		for ( int i = 0; i < 1024; ++i )
+		{
+			const float4 &p = s->tables_host[ 2 * ( L.table + i ) ], &n = s->tables_host[ 2 * ( L.table + i ) + 1 ];
+			float v[ 6 ] = { p.x, p.y, p.z, n.x, n.y, n.z };
+			std::memcpy( out + 6 * i, v, sizeof v );
+		}
+		if ( pdf ) *pdf = L.koishi_pdf;
+	} );
+}
+
+int cr_trace_rays_device( cr_scene *s, const float *d_rays, uint64_t n, cr_hit *d_hits, int any_hit, void *stream )
+{
+	return guarded( [&] {
+		if ( !s || ( n && ( !d_rays || !d_hits ) ) ) fail( CR_ERR_INVALID, "null argument" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		launch_trace( dev_scene( s ), d_rays, n, any_hit, d_hits, s->err.p, (cudaStream_t)stream );
+	} );
+}
+
+int cr_trace_rays( cr_scene *s, const float *rays, uint64_t n, cr_hit *hits, int any_hit )
+{
+	return guarded( [&] {
+		if ( !s || ( n && ( !rays || !hits ) ) ) fail( CR_ERR_INVALID, "null argument" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		if ( !n ) return;
+		cudaStream_t st = s->stream;
+		float *dr = nullptr;
+		cr_hit *dh = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&dr, sizeof( float ) * 7 * n, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dh, sizeof( cr_hit ) * n, st ), "cudaMalloc" );
+		cuda_check( cudaMemcpyAsync( dr, rays, sizeof( float ) * 7 * n, cudaMemcpyHostToDevice, st ), "upload" );
+		launch_trace( dev_scene( s ), dr, n, any_hit, dh, s->err.p, st );
+		cuda_check( cudaMemcpyAsync( hits, dh, sizeof( cr_hit ) * n, cudaMemcpyDeviceToHost, st ), "download" );
+		cudaFreeAsync( dr, st );
+		cudaFreeAsync( dh, st );
+		cuda_check( cudaStreamSynchronize( st ), "trace" );
+		uint32_t e = 0;
+		cuda_check( cudaMemcpy( &e, s->err.p, 4, cudaMemcpyDeviceToHost ), "error word" );
+		if ( e ) fail( CR_ERR_DEVICE, "a traversal kernel reported error flags " + std::to_string( e ) );
+	} );
+}
+
+int cr_render_device( cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sq, uint32_t *d_cnt,
+					  void *stream, cr_stats *stats )
+{
+	return guarded( [&] {
+		if ( !d_sum || !d_sq || !d_cnt ) fail( CR_ERR_INVALID, "null film" );
+		render_device( s, desc, d_sum, d_sq, d_cnt, (cudaStream_t)stream, stats );
+	} );
+}
+
+int cr_render( cr_scene *s, const cr_render_desc *desc, double *film, cr_stats *stats )
+{
+	return guarded( [&] {
+		if ( !film ) fail( CR_ERR_INVALID, "null film" );
+		Resolved r = resolve( s, desc );
+		cudaStream_t st = s->stream;
+		size_t npx = size_t( r.cfg.ww ) * r.cfg.wh;
+		double *sum, *sq;
+		uint32_t *cnt;
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+		cuda_check( cudaMemsetAsync( sum, 0, npx * 24, st ), "memset" );
+		cuda_check( cudaMemsetAsync( sq, 0, npx * 24, st ), "memset" );
+		cuda_check( cudaMemsetAsync( cnt, 0, npx * 4, st ), "memset" );
+		std::vector<uint32_t> hc( npx );
+		try
+		{
+			render_device( s, desc, sum, sq, cnt, st, stats );
+			cuda_check( cudaMemcpyAsync( film, sum, npx * 24, cudaMemcpyDeviceToHost, st ), "download" );
+			cuda_check( cudaMemcpyAsync( hc.data(), cnt, npx * 4, cudaMemcpyDeviceToHost, st ), "download" );
+			cuda_check( cudaStreamSynchronize( st ), "render" );
+		}
+		catch ( ... )
+		{
+			cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
+			throw;
+		}
+		cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
+		check_device_error( s, st );
+		for ( size_t p = 0; p < npx; ++p )
+			for ( int c = 0; c < 3; ++c ) film[ 3 * p + c ] = hc[ p ] ? film[ 3 * p + c ] / hc[ p ] : 0.0;
+	} );
+}
+
+int cr_write_png( const char *path, uint32_t w, uint32_t h, const double *rgb )
+{
+	return guarded( [&] {
+		if ( !path || !rgb ) fail( CR_ERR_INVALID, "null argument" );
+		write_png( path, w, h, rgb );
+	} );
+}
+
+int cr_render_file( const char *json_path, const char *png_path, const char *pfm_path, uint32_t spp, uint32_t w,
+					uint32_t h, const char *kernel, const char *tracer )
+{
+	return guarded( [&] {
+		if ( !json_path || !png_path ) fail( CR_ERR_INVALID, "null argument" );
+		std::string text = read_file( json_path );
+		std::unique_ptr<cr_scene> s( new cr_scene() );
+		load_scene( s.get(), text, dir_of( json_path ) );
+		if ( kernel && *kernel ) s->kernel = kernel;
+		if ( tracer && *tracer ) s->tracer = tracer;
+		static const char *tracers[] = { "CudaWavefront", "CPUMulticore", "CPUMultiCoreTracer", "CudaSingleGPU" };
+		if ( std::find_if( std::begin( tracers ), std::end( tracers ), [&]( const char *t ) { return s->tracer == t; } ) ==
+			 std::end( tracers ) )
+			fail( CR_ERR_UNSUPPORTED, "no such tracer: " + s->tracer );
+		commit( s.get(), 0x330E, nullptr );
+		cr_render_desc d;
+		std::memset( &d, 0, sizeof d );
+		d.width = w, d.height = h, d.spp = spp, d.max_bounce = UINT32_MAX, d.estimator = -1, d.seed = 1;
+		std::vector<double> film( size_t( w ) * h * 3 );
+		int rc = cr_render( s.get(), &d, film.data(), nullptr );
+		if ( rc != CR_OK ) fail( rc, g_last_error );
+		write_png( png_path, w, h, film.data() );
+		if ( pfm_path && *pfm_path ) write_pfm( pfm_path, w, h, film.data() );
+	} );
+}
+
+static DevShader shader_from_json( const char *js )
+{
+	if ( !js ) fail( CR_ERR_INVALID, "null shader" );
+	return make_shader( parse_json( js ) );
+}
+
+int cr_bsdf_eval( int est, const char *shader_json, const float *wo, const float *wi, uint64_t n, float *f, float *pdf )
+{
+	return guarded( [&] {
+		DevShader sh = shader_from_json( shader_json );
+		if ( !n ) return;
+		if ( !wo || !wi || !f || !pdf ) fail( CR_ERR_INVALID, "null argument" );
+		float *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * 10 * n ), "cudaMalloc" );
+		float *dwo = d, *dwi = d + 3 * n, *df = d + 6 * n, *dp = d + 9 * n;
+		cudaMemcpy( dwo, wo, 12 * n, cudaMemcpyHostToDevice );
+		cudaMemcpy( dwi, wi, 12 * n, cudaMemcpyHostToDevice );
+		launch_bsdf_eval( est, sh, dwo, dwi, n, df, dp, nullptr );
+		cudaMemcpy( f, df, 12 * n, cudaMemcpyDeviceToHost );
+		cudaError_t e = cudaMemcpy( pdf, dp, 4 * n, cudaMemcpyDeviceToHost );
+		cudaFree( d );
+		cuda_check( e, "bsdf eval" );
+	} );
+}
+
+int cr_bsdf_sample( int est, const char *shader_json, const float *wo, const float *u, uint64_t n, float *wi,
+					float *weight, float *pdf )
+{
+	return guarded( [&] {
+		DevShader sh = shader_from_json( shader_json );
+		if ( !n ) return;
+		if ( !wo || !u || !wi || !weight || !pdf ) fail( CR_ERR_INVALID, "null argument" );
+		float *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * 12 * n ), "cudaMalloc" );
+		float *dwo = d, *du = d + 3 * n, *dwi = d + 5 * n, *dw = d + 8 * n, *dp = d + 11 * n;
+		cudaMemcpy( dwo, wo, 12 * n, cudaMemcpyHostToDevice );
+		cudaMemcpy( du, u, 8 * n, cudaMemcpyHostToDevice );
+		launch_bsdf_sample( est, sh, dwo, du, n, dwi, dw, dp, nullptr );
+		cudaMemcpy( wi, dwi, 12 * n, cudaMemcpyDeviceToHost );
+		cudaMemcpy( weight, dw, 12 * n, cudaMemcpyDeviceToHost );
+		cudaError_t e = cudaMemcpy( pdf, dp, 4 * n, cudaMemcpyDeviceToHost );
+		cudaFree( d );
+		cuda_check( e, "bsdf sample" );
+	} );
+}
+
+}  // extern "C"

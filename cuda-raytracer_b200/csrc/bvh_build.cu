@@ -1,0 +1,453 @@
+// GPU BVH builder: replaces the reference's recursive host builder
+// (createBVH / doCreateBVH / plainlizeBVH, src/core/primitive/mesh.cu:35-143).
+//
+//  1. per-triangle boxes, centroid bounds            k_tri_boxes
+//  2. 63-bit Morton codes of the centroids           k_morton
+//  3. radix sort (CUB) of (code, triangle)
+//  4. binary radix tree (Karras, HPG 2012)           k_karras
+//  5. bottom-up boxes and SAH leaf/split costs       k_bottom_up
+//     (leaves of up to 3 triangles where the SAH says a leaf is cheaper)
+//  6. top-down collapse into quantised 8-wide nodes  k_collapse (one level
+//     per launch): each wide node opens its binary subtree greedily by the
+//     largest child surface area until 8 children, assigns children to slots
+//     in ray-octant order, quantises child boxes to 8 bits per plane and
+//     writes its leaf triangles contiguously in traversal order.
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "cr_device.cuh"
+
+namespace cr
+{
+namespace
+{
+constexpr int MAX_LEAF = 3;
+constexpr float COST_NODE = 1.2f;
+constexpr float COST_TRI = 1.0f;
+
+struct BNode
+{
+	float4 lo, hi;       // lo.w = SAH cost, hi.w unused
+	int left, right;     // unified ids: internal i -> i, leaf k -> n_int + k
+	int parent;
+	int first, count;    // sorted primitive range
+	int leaf;            // 1 if this node becomes a wide-BVH leaf
+};
+
+__device__ __forceinline__ void atomic_min_f( float *a, float v )
+{
+	if ( v >= 0.f )
+		atomicMin( reinterpret_cast<int *>( a ), __float_as_int( v ) );
+	else
+		atomicMax( reinterpret_cast<unsigned *>( a ), __float_as_uint( v ) );
+}
+__device__ __forceinline__ void atomic_max_f( float *a, float v )
+{
+	if ( v >= 0.f )
+		atomicMax( reinterpret_cast<int *>( a ), __float_as_int( v ) );
+	else
+		atomicMin( reinterpret_cast<unsigned *>( a ), __float_as_uint( v ) );
+}
+
+__device__ __forceinline__ float area( float3 lo, float3 hi )
+{
+	float3 e = f3( fmaxf( hi.x - lo.x, 0.f ), fmaxf( hi.y - lo.y, 0.f ), fmaxf( hi.z - lo.z, 0.f ) );
+	return 2.f * ( e.x * e.y + e.y * e.z + e.z * e.x );
+}
+
+// src: 3 float4 per triangle (v0, v1, v2) in global order.
+__global__ void k_tri_boxes( const float4 *src, uint32_t n, float4 *blo, float4 *bhi, float *cbounds )
+{
+	float3 lo = f3( INFINITY, INFINITY, INFINITY ), hi = f3( -INFINITY, -INFINITY, -INFINITY );
+	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
+	{
+		float3 a = f3( src[ 3 * i ] ), b = f3( src[ 3 * i + 1 ] ), c = f3( src[ 3 * i + 2 ] );
+		float3 l = f3( fminf( a.x, fminf( b.x, c.x ) ), fminf( a.y, fminf( b.y, c.y ) ), fminf( a.z, fminf( b.z, c.z ) ) );
+		float3 h = f3( fmaxf( a.x, fmaxf( b.x, c.x ) ), fmaxf( a.y, fmaxf( b.y, c.y ) ), fmaxf( a.z, fmaxf( b.z, c.z ) ) );
+		blo[ i ] = make_float4( l.x, l.y, l.z, 0.f );
+		bhi[ i ] = make_float4( h.x, h.y, h.z, 0.f );
+		float3 c3 = ( l + h ) * 0.5f;
+		lo = f3( fminf( lo.x, c3.x ), fminf( lo.y, c3.y ), fminf( lo.z, c3.z ) );
+		hi = f3( fmaxf( hi.x, c3.x ), fmaxf( hi.y, c3.y ), fmaxf( hi.z, c3.z ) );
+	}
+	for ( int o = 16; o; o >>= 1 )
+	{
+		lo.x = fminf( lo.x, __shfl_xor_sync( ~0u, lo.x, o ) );
+		lo.y = fminf( lo.y, __shfl_xor_sync( ~0u, lo.y, o ) );
+		lo.z = fminf( lo.z, __shfl_xor_sync( ~0u, lo.z, o ) );
+		hi.x = fmaxf( hi.x, __shfl_xor_sync( ~0u, hi.x, o ) );
+		hi.y = fmaxf( hi.y, __shfl_xor_sync( ~0u, hi.y, o ) );
+		hi.z = fmaxf( hi.z, __shfl_xor_sync( ~0u, hi.z, o ) );
+	}
+	if ( ( threadIdx.x & 31 ) == 0 )
+	{
+		atomic_min_f( cbounds + 0, lo.x ), atomic_min_f( cbounds + 1, lo.y ), atomic_min_f( cbounds + 2, lo.z );
+		atomic_max_f( cbounds + 3, hi.x ), atomic_max_f( cbounds + 4, hi.y ), atomic_max_f( cbounds + 5, hi.z );
+	}
+}
+
+__device__ __forceinline__ uint64_t spread21( uint64_t x )
+{
+	x &= 0x1FFFFFull;
+	x = ( x | x << 32 ) & 0x1F00000000FFFFull;
+	x = ( x | x << 16 ) & 0x1F0000FF0000FFull;
+	x = ( x | x << 8 ) & 0x100F00F00F00F00Full;
+	x = ( x | x << 4 ) & 0x10C30C30C30C30C3ull;
+	x = ( x | x << 2 ) & 0x1249249249249249ull;
+	return x;
+}
+
+__global__ void k_morton( const float4 *blo, const float4 *bhi, uint32_t n, const float *cb, uint64_t *keys,
+						  uint32_t *vals )
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( i >= n ) return;
+	float3 lo = f3( cb[ 0 ], cb[ 1 ], cb[ 2 ] ), hi = f3( cb[ 3 ], cb[ 4 ], cb[ 5 ] );
+	float3 c = ( f3( blo[ i ] ) + f3( bhi[ i ] ) ) * 0.5f;
+	const float S = 2097151.f;
+	float ex = hi.x - lo.x, ey = hi.y - lo.y, ez = hi.z - lo.z;
+	uint64_t x = uint64_t( ex > 0 ? fminf( fmaxf( ( c.x - lo.x ) / ex, 0.f ), 1.f ) * S : 0.f );
+	uint64_t y = uint64_t( ey > 0 ? fminf( fmaxf( ( c.y - lo.y ) / ey, 0.f ), 1.f ) * S : 0.f );
+	uint64_t z = uint64_t( ez > 0 ? fminf( fmaxf( ( c.z - lo.z ) / ez, 0.f ), 1.f ) * S : 0.f );
+	keys[ i ] = ( spread21( x ) << 2 ) | ( spread21( y ) << 1 ) | spread21( z );
+	vals[ i ] = i;
+}
+
+// Common prefix length of keys i and j (ties broken by index), -1 outside.
+__device__ __forceinline__ int delta( const uint64_t *k, int n, int i, int j )
+{
+	if ( j < 0 || j >= n ) return -1;
+	uint64_t a = k[ i ], b = k[ j ];
+	if ( a == b ) return 64 + __clz( uint32_t( i ^ j ) );
+	return __clzll( a ^ b );
+}
+
+__global__ void k_karras( const uint64_t *k, int n, BNode *nodes )
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	int n_int = n - 1;
+	if ( i >= n_int ) return;
+	int d = ( delta( k, n, i, i + 1 ) - delta( k, n, i, i - 1 ) ) >= 0 ? 1 : -1;
+	int dmin = delta( k, n, i, i - d );
+	int lmax = 2;
+	while ( delta( k, n, i, i + lmax * d ) > dmin ) lmax <<= 1;
+	int l = 0;
+	for ( int t = lmax >> 1; t >= 1; t >>= 1 )
+		if ( delta( k, n, i, i + ( l + t ) * d ) > dmin ) l += t;
+	int j = i + l * d;
+	int dnode = delta( k, n, i, j );
+	int s = 0;
+	int t = l;
+	do
+	{
+		t = ( t + 1 ) >> 1;
+		if ( delta( k, n, i, i + ( s + t ) * d ) > dnode ) s += t;
+	} while ( t > 1 );
+	int g = i + s * d + min( d, 0 );
+	int lo = min( i, j ), hi = max( i, j );
+	int left = ( lo == g ) ? n_int + g : g;
+	int right = ( hi == g + 1 ) ? n_int + g + 1 : g + 1;
+	nodes[ i ].left = left;
+	nodes[ i ].right = right;
+	nodes[ i ].first = lo;
+	nodes[ i ].count = hi - lo + 1;
+	nodes[ left ].parent = i;
+	nodes[ right ].parent = i;
+}
+
+__global__ void k_bottom_up( int n, const uint32_t *order, const float4 *blo, const float4 *bhi, BNode *nodes,
+							 int *flags )
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( k >= n ) return;
+	int n_int = n - 1;
+	int id = n_int + k;
+	uint32_t prim = order[ k ];
+	float4 lo = blo[ prim ], hi = bhi[ prim ];
+	float a = area( f3( lo ), f3( hi ) );
+	lo.w = COST_TRI * a;
+	nodes[ id ].lo = lo;
+	nodes[ id ].hi = hi;
+	nodes[ id ].first = k;
+	nodes[ id ].count = 1;
+	nodes[ id ].leaf = 1;
+	nodes[ id ].left = nodes[ id ].right = -1;
+	if ( n == 1 ) return;
+	int p = nodes[ id ].parent;
+	while ( p >= 0 )
+	{
+		__threadfence();
+		if ( atomicAdd( flags + p, 1 ) == 0 ) return;  // the sibling finishes this node
+		__threadfence();
+		BNode &nd = nodes[ p ];
+		const BNode &L = nodes[ nd.left ];
+		const BNode &R = nodes[ nd.right ];
+		float4 l0 = __ldcg( &L.lo ), l1 = __ldcg( &L.hi );
+		float4 r0 = __ldcg( &R.lo ), r1 = __ldcg( &R.hi );
+		float3 mlo = f3( fminf( l0.x, r0.x ), fminf( l0.y, r0.y ), fminf( l0.z, r0.z ) );
+		float3 mhi = f3( fmaxf( l1.x, r1.x ), fmaxf( l1.y, r1.y ), fmaxf( l1.z, r1.z ) );
+		float A = area( mlo, mhi );
+		float split = COST_NODE * A + l0.w + r0.w;
+		float leafc = COST_TRI * A * float( nd.count );
+		bool as_leaf = nd.count <= MAX_LEAF && leafc <= split;
+		nd.lo = make_float4( mlo.x, mlo.y, mlo.z, as_leaf ? leafc : split );
+		nd.hi = make_float4( mhi.x, mhi.y, mhi.z, 0.f );
+		nd.leaf = as_leaf ? 1 : 0;
+		p = nd.parent;
+	}
+}
+
+struct WorkItem
+{
+	int bnode;
+	uint32_t wnode;
+};
+
+__device__ __forceinline__ uint8_t quant_lo( float c, float p, float s, float inv )
+{
+	float q = floorf( ( c - p ) * inv );
+	q = fminf( fmaxf( q, 0.f ), 255.f );
+	while ( q > 0.f && p + q * s > c ) q -= 1.f;
+	return uint8_t( q );
+}
+__device__ __forceinline__ uint8_t quant_hi( float c, float p, float s, float inv )
+{
+	float q = ceilf( ( c - p ) * inv );
+	q = fminf( fmaxf( q, 0.f ), 255.f );
+	while ( q < 255.f && p + q * s < c ) q += 1.f;
+	return uint8_t( q );
+}
+
+// Smallest biased exponent e with 2^(e-127) * 255 >= extent.
+__device__ __forceinline__ uint32_t quant_exp( float extent )
+{
+	if ( !( extent > 0.f ) ) return 1u;
+	int e = int( ceilf( log2f( extent / 255.f ) ) );
+	e = max( e, -126 );
+	while ( ldexpf( 255.f, e ) < extent ) ++e;
+	return uint32_t( e + 127 );
+}
+
+__global__ void k_collapse( const WorkItem *work, const uint32_t *n_work, WorkItem *next, uint32_t *n_next,
+							const BNode *bn, int n_int, const uint32_t *order, const float4 *src, WNode *wn,
+							float4 *tris, uint32_t *counters /* [0] nodes, [1] tris, [2] max depth */,
+							uint32_t depth )
+{
+	uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( w >= *n_work ) return;
+	WorkItem it = work[ w ];
+	int ch[ 8 ];
+	int nc = 0;
+	const BNode &root = bn[ it.bnode ];
+	if ( root.leaf )
+		ch[ nc++ ] = it.bnode;
+	else
+	{
+		ch[ nc++ ] = root.left;
+		ch[ nc++ ] = root.right;
+		while ( nc < 8 )
+		{
+			int best = -1;
+			float ba = -1.f;
+			for ( int c = 0; c < nc; ++c )
+			{
+				const BNode &b = bn[ ch[ c ] ];
+				if ( b.leaf ) continue;
+				float a = area( f3( b.lo ), f3( b.hi ) );
+				if ( a > ba ) ba = a, best = c;
+			}
+			if ( best < 0 ) break;
+			int id = ch[ best ];
+			ch[ best ] = bn[ id ].left;
+			ch[ nc++ ] = bn[ id ].right;
+		}
+	}
+	// Octant slot assignment: slot s receives the child nearest along
+	// direction signs s (bit0: -x, bit1: -y, bit2: -z), greedily.
+	float3 plo = f3( root.lo ), phi = f3( root.hi );
+	float3 pc = ( plo + phi ) * 0.5f;
+	int child_in[ 8 ];
+	for ( int s = 0; s < 8; ++s ) child_in[ s ] = -1;
+	uint32_t used_c = 0, used_s = 0;
+	for ( int round = 0; round < nc; ++round )
+	{
+		float best = INFINITY;
+		int bc = 0, bs = 0;
+		for ( int c = 0; c < nc; ++c )
+		{
+			if ( used_c >> c & 1u ) continue;
+			const BNode &b = bn[ ch[ c ] ];
+			float3 cc = ( f3( b.lo ) + f3( b.hi ) ) * 0.5f - pc;
+			for ( int s = 0; s < 8; ++s )
+			{
+				if ( used_s >> s & 1u ) continue;
+				float3 dir = f3( ( s & 1 ) ? -1.f : 1.f, ( s & 2 ) ? -1.f : 1.f, ( s & 4 ) ? -1.f : 1.f );
+				float cost = dot( cc, dir );
+				if ( cost < best ) best = cost, bc = c, bs = s;
+			}
+		}
+		used_c |= 1u << bc;
+		used_s |= 1u << bs;
+		child_in[ bs ] = bc;
+	}
+	// Allocate children and triangles.
+	uint32_t n_internal = 0, n_tri = 0;
+	for ( int c = 0; c < nc; ++c )
+	{
+		const BNode &b = bn[ ch[ c ] ];
+		if ( b.leaf )
+			n_tri += b.count;
+		else
+			++n_internal;
+	}
+	uint32_t child_base = n_internal ? atomicAdd( counters + 0, n_internal ) : 0;
+	uint32_t tri_base = atomicAdd( counters + 1, n_tri );
+	WNode nd;
+	float3 ext = phi - plo;
+	uint32_t ex = quant_exp( ext.x ), ey = quant_exp( ext.y ), ez = quant_exp( ext.z );
+	float sx = __uint_as_float( ex << 23 ), sy = __uint_as_float( ey << 23 ), sz = __uint_as_float( ez << 23 );
+	float ix = 1.f / sx, iy = 1.f / sy, iz = 1.f / sz;
+	nd.px = plo.x, nd.py = plo.y, nd.pz = plo.z;
+	nd.ex = uint8_t( ex ), nd.ey = uint8_t( ey ), nd.ez = uint8_t( ez );
+	nd.imask = 0;
+	nd.child_base = child_base;
+	nd.tri_base = tri_base;
+	uint32_t rank = 0, toff = 0;
+	for ( int s = 0; s < 8; ++s )
+	{
+		int c = child_in[ s ];
+		if ( c < 0 )
+		{
+			nd.meta[ s ] = 0;
+			nd.qlo_x[ s ] = nd.qlo_y[ s ] = nd.qlo_z[ s ] = 255;
+			nd.qhi_x[ s ] = nd.qhi_y[ s ] = nd.qhi_z[ s ] = 0;
+			continue;
+		}
+		const BNode &b = bn[ ch[ c ] ];
+		nd.qlo_x[ s ] = quant_lo( b.lo.x, plo.x, sx, ix );
+		nd.qlo_y[ s ] = quant_lo( b.lo.y, plo.y, sy, iy );
+		nd.qlo_z[ s ] = quant_lo( b.lo.z, plo.z, sz, iz );
+		nd.qhi_x[ s ] = quant_hi( b.hi.x, plo.x, sx, ix );
+		nd.qhi_y[ s ] = quant_hi( b.hi.y, plo.y, sy, iy );
+		nd.qhi_z[ s ] = quant_hi( b.hi.z, plo.z, sz, iz );
+		if ( b.leaf )
+		{
+			nd.meta[ s ] = uint8_t( ( b.count << 5 ) | toff );
+			for ( int k = 0; k < b.count; ++k )
+			{
+				uint32_t prim = order[ b.first + k ];
+				float4 *dst = tris + 3 * size_t( tri_base + toff + k );
+				float4 a = src[ 3 * size_t( prim ) ], bb = src[ 3 * size_t( prim ) + 1 ], cc = src[ 3 * size_t( prim ) + 2 ];
+				dst[ 0 ] = make_float4( a.x, a.y, a.z, __uint_as_float( prim ) );
+				dst[ 1 ] = make_float4( bb.x, bb.y, bb.z, 0.f );
+				dst[ 2 ] = make_float4( cc.x, cc.y, cc.z, 0.f );
+			}
+			toff += b.count;
+		}
+		else
+		{
+			nd.meta[ s ] = 0;
+			nd.imask |= uint8_t( 1u << s );
+			uint32_t q = atomicAdd( n_next, 1u );
+			next[ q ] = WorkItem{ ch[ c ], child_base + rank };
+			++rank;
+		}
+	}
+	wn[ it.wnode ] = nd;
+	atomicMax( counters + 2, depth );
+}
+
+void check( cudaError_t e, const char *what )
+{
+	if ( e != cudaSuccess ) throw std::runtime_error( std::string( what ) + ": " + cudaGetErrorString( e ) );
+}
+
+}  // namespace
+
+void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st )
+{
+	out.n_nodes = 0;
+	out.n_tris = n;
+	out.depth = 0;
+	if ( n == 0 ) return;
+	float4 *blo, *bhi;
+	float *cb;
+	uint64_t *keys, *keys2;
+	uint32_t *vals, *vals2;
+	BNode *bn;
+	int *flags;
+	WorkItem *wa, *wb;
+	uint32_t *cnt;  // [0] nodes [1] tris [2] depth [3] n_work a [4] n_work b
+	size_t n_b = 2 * size_t( n ) - 1;
+	check( cudaMallocAsync( &blo, sizeof( float4 ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &bhi, sizeof( float4 ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &cb, sizeof( float ) * 6, st ), "bvh alloc" );
+	check( cudaMallocAsync( &keys, sizeof( uint64_t ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &keys2, sizeof( uint64_t ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &vals, sizeof( uint32_t ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &vals2, sizeof( uint32_t ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &bn, sizeof( BNode ) * n_b, st ), "bvh alloc" );
+	check( cudaMallocAsync( &flags, sizeof( int ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &wa, sizeof( WorkItem ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &wb, sizeof( WorkItem ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &cnt, sizeof( uint32_t ) * 8, st ), "bvh alloc" );
+	check( cudaMallocAsync( &out.nodes, sizeof( WNode ) * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &out.tris, sizeof( float4 ) * 3 * n, st ), "bvh alloc" );
+
+	float init[ 6 ] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
+	check( cudaMemcpyAsync( cb, init, sizeof init, cudaMemcpyHostToDevice, st ), "bvh init" );
+	check( cudaMemsetAsync( flags, 0, sizeof( int ) * n, st ), "bvh init" );
+	check( cudaMemsetAsync( bn, 0xFF, sizeof( BNode ) * n_b, st ), "bvh init" );
+	int tb = 256;
+	int gb = int( std::min<uint32_t>( ( n + tb - 1 ) / tb, 148u * 8u ) );
+	k_tri_boxes<<<gb, tb, 0, st>>>( d_src, n, blo, bhi, cb );
+	k_morton<<<( n + tb - 1 ) / tb, tb, 0, st>>>( blo, bhi, n, cb, keys, vals );
+	size_t temp = 0;
+	check( cub::DeviceRadixSort::SortPairs( nullptr, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
+	void *dtemp;
+	check( cudaMallocAsync( &dtemp, temp, st ), "bvh alloc" );
+	check( cub::DeviceRadixSort::SortPairs( dtemp, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
+	if ( n > 1 ) k_karras<<<( n - 1 + tb - 1 ) / tb, tb, 0, st>>>( keys2, int( n ), bn );
+	k_bottom_up<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, flags );
+	check( cudaGetLastError(), "bvh kernels" );
+
+	// Root work item: binary root (internal 0, or the single leaf) -> wide node 0.
+	WorkItem root{ 0, 0 };
+	uint32_t c0[ 5 ] = { 1, 0, 0, 1, 0 };
+	check( cudaMemcpyAsync( wa, &root, sizeof root, cudaMemcpyHostToDevice, st ), "bvh root" );
+	check( cudaMemcpyAsync( cnt, c0, sizeof c0, cudaMemcpyHostToDevice, st ), "bvh root" );
+	uint32_t n_work = 1, depth = 0;
+	WorkItem *cur = wa, *nxt = wb;
+	uint32_t *ncur = cnt + 3, *nnext = cnt + 4;
+	while ( n_work )
+	{
+		check( cudaMemsetAsync( nnext, 0, sizeof( uint32_t ), st ), "bvh level" );
+		k_collapse<<<( n_work + 127 ) / 128, 128, 0, st>>>( cur, ncur, nxt, nnext, bn, int( n ) - 1, vals2, d_src,
+															out.nodes, out.tris, cnt, depth + 1 );
+		check( cudaGetLastError(), "bvh collapse" );
+		check( cudaMemcpyAsync( &n_work, nnext, sizeof( uint32_t ), cudaMemcpyDeviceToHost, st ), "bvh level" );
+		check( cudaStreamSynchronize( st ), "bvh level" );
+		std::swap( cur, nxt );
+		std::swap( ncur, nnext );
+		++depth;
+		if ( depth > 4096 ) throw std::runtime_error( "bvh: collapse did not terminate" );
+	}
+	uint32_t res[ 3 ];
+	check( cudaMemcpyAsync( res, cnt, sizeof res, cudaMemcpyDeviceToHost, st ), "bvh result" );
+	check( cudaStreamSynchronize( st ), "bvh result" );
+	out.n_nodes = res[ 0 ];
+	out.depth = res[ 2 ];
+	if ( res[ 1 ] != n ) throw std::runtime_error( "bvh: triangle count mismatch after collapse" );
+	for ( void *p : { (void *)blo, (void *)bhi, (void *)cb, (void *)keys, (void *)keys2, (void *)vals, (void *)vals2,
+					  (void *)bn, (void *)flags, (void *)wa, (void *)wb, (void *)cnt, dtemp } )
+		cudaFreeAsync( p, st );
+}
+
+}  // namespace cr

@@ -1,0 +1,21 @@
+// GPU builder of the quantised 8-wide BVH (see bvh_build.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "cr_common.h"
+
+namespace cr
+{
+struct WideBvh
+{
+	WNode *nodes = nullptr;   // device, n_nodes entries (allocation holds n_tris)
+	float4 *tris = nullptr;   // device, 3 float4 per triangle in leaf order
+	uint32_t n_nodes = 0, n_tris = 0, depth = 0;
+};
+
+// d_src: 3 float4 (v0, v1, v2) per triangle in global order, on the device.
+// Allocates out.nodes / out.tris with cudaMallocAsync on `st`; throws
+// std::runtime_error on failure.  Synchronises `st` once per tree level.
+void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st );
+}  // namespace cr

@@ -1,0 +1,467 @@
+// Device code shared by the traversal, shading and parity kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "cr_common.h"
+
+namespace cr
+{
+// ------------------------------------------------------------------ float3 math
+__device__ __forceinline__ float3 f3( float x, float y, float z ) { return make_float3( x, y, z ); }
+__device__ __forceinline__ float3 f3( const float *p ) { return make_float3( p[ 0 ], p[ 1 ], p[ 2 ] ); }
+__device__ __forceinline__ float3 f3( float4 a ) { return make_float3( a.x, a.y, a.z ); }
+__device__ __forceinline__ float3 operator+( float3 a, float3 b ) { return f3( a.x + b.x, a.y + b.y, a.z + b.z ); }
+__device__ __forceinline__ float3 operator-( float3 a, float3 b ) { return f3( a.x - b.x, a.y - b.y, a.z - b.z ); }
+__device__ __forceinline__ float3 operator-( float3 a ) { return f3( -a.x, -a.y, -a.z ); }
+__device__ __forceinline__ float3 operator*( float3 a, float3 b ) { return f3( a.x * b.x, a.y * b.y, a.z * b.z ); }
+__device__ __forceinline__ float3 operator*( float3 a, float s ) { return f3( a.x * s, a.y * s, a.z * s ); }
+__device__ __forceinline__ float3 operator*( float s, float3 a ) { return f3( a.x * s, a.y * s, a.z * s ); }
+__device__ __forceinline__ float3 operator/( float3 a, float s ) { return f3( a.x / s, a.y / s, a.z / s ); }
+__device__ __forceinline__ float dot( float3 a, float3 b ) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross( float3 a, float3 b )
+{
+	return f3( a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y );
+}
+__device__ __forceinline__ float length( float3 a ) { return sqrtf( dot( a, a ) ); }
+__device__ __forceinline__ float3 normalize( float3 a ) { return a * ( 1.0f / sqrtf( dot( a, a ) ) ); }
+__device__ __forceinline__ float maxc( float3 a ) { return fmaxf( a.x, fmaxf( a.y, a.z ) ); }
+__device__ __forceinline__ bool finite3( float3 a ) { return isfinite( a.x ) && isfinite( a.y ) && isfinite( a.z ); }
+__device__ __forceinline__ bool is_zero( float3 a ) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
+__device__ __forceinline__ float comp( float3 a, int k ) { return k == 0 ? a.x : ( k == 1 ? a.y : a.z ); }
+
+constexpr float PI_F = 3.14159265358979323846f;
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Counter-based generator of Salmon, Moraes, Dror and Shaw, "Parallel random
+// numbers: as easy as 1, 2, 3" (SC'11): 10 rounds of two 32x32->64 multiplies
+// with the published round multipliers and Weyl key increments.
+__device__ __forceinline__ uint4 philox4x32_10( uint4 c, uint2 k )
+{
+	const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+	for ( int r = 0; r < 10; ++r )
+	{
+		uint32_t hi0 = __umulhi( M0, c.x ), lo0 = M0 * c.x;
+		uint32_t hi1 = __umulhi( M1, c.z ), lo1 = M1 * c.z;
+		c = make_uint4( hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0 );
+		k.x += W0;
+		k.y += W1;
+	}
+	return c;
+}
+
+// Uniform in (0, 1): 24 random bits, centred in their interval so that 0 and 1
+// never occur (the Beckmann sampler takes log(u)).
+__device__ __forceinline__ float u01( uint32_t x ) { return ( float( x >> 8 ) + 0.5f ) * ( 1.0f / 16777216.0f ); }
+
+// Four uniforms for (sample id, bounce, stream) under the render's key.
+__device__ __forceinline__ float4 rand4( uint2 key, uint64_t sample, uint32_t bounce, uint32_t stream )
+{
+	uint4 r = philox4x32_10( make_uint4( uint32_t( sample ), uint32_t( sample >> 32 ), bounce, stream ), key );
+	return make_float4( u01( r.x ), u01( r.y ), u01( r.z ), u01( r.w ) );
+}
+
+// ------------------------------------------------------------------ traversal
+struct RayPre
+{
+	float3 o, d, invd;
+	uint32_t oct;
+	int kx, ky, kz;
+	float sx, sy, sz;
+};
+
+__device__ __forceinline__ RayPre make_ray( float3 o, float3 d )
+{
+	RayPre r;
+	r.o = o;
+	r.d = d;
+	const float tiny = 1e-30f;
+	float dx = fabsf( d.x ) < tiny ? copysignf( tiny, d.x ) : d.x;
+	float dy = fabsf( d.y ) < tiny ? copysignf( tiny, d.y ) : d.y;
+	float dz = fabsf( d.z ) < tiny ? copysignf( tiny, d.z ) : d.z;
+	r.invd = f3( 1.0f / dx, 1.0f / dy, 1.0f / dz );
+	r.oct = ( d.x < 0.f ? 1u : 0u ) | ( d.y < 0.f ? 2u : 0u ) | ( d.z < 0.f ? 4u : 0u );
+	// Watertight ray/triangle set-up (Woop, Benthin and Wald, JCGT 2013):
+	// kz = dominant axis, winding preserved by swapping kx/ky when d[kz] < 0.
+	float ax = fabsf( d.x ), ay = fabsf( d.y ), az = fabsf( d.z );
+	int kz = ( ax >= ay && ax >= az ) ? 0 : ( ay >= az ? 1 : 2 );
+	int kx = kz == 2 ? 0 : kz + 1;
+	int ky = kx == 2 ? 0 : kx + 1;
+	if ( comp( d, kz ) < 0.f )
+	{
+		int t = kx;
+		kx = ky;
+		ky = t;
+	}
+	r.kx = kx, r.ky = ky, r.kz = kz;
+	float dkz = comp( d, kz );
+	r.sx = comp( d, kx ) / dkz;
+	r.sy = comp( d, ky ) / dkz;
+	r.sz = 1.0f / dkz;
+	return r;
+}
+
+// Watertight ray/triangle test; accepts tmin < t < tmax, edges inclusive,
+// no back-face culling.  Returns u, v = weights of v1 and v2.
+__device__ __forceinline__ bool tri_test( const RayPre &r, float3 v0, float3 v1, float3 v2, float tmin, float tmax,
+										  float &t, float &u, float &v )
+{
+	float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+	float Akz = comp( A, r.kz ), Bkz = comp( B, r.kz ), Ckz = comp( C, r.kz );
+	float Ax = fmaf( -r.sx, Akz, comp( A, r.kx ) ), Ay = fmaf( -r.sy, Akz, comp( A, r.ky ) );
+	float Bx = fmaf( -r.sx, Bkz, comp( B, r.kx ) ), By = fmaf( -r.sy, Bkz, comp( B, r.ky ) );
+	float Cx = fmaf( -r.sx, Ckz, comp( C, r.kx ) ), Cy = fmaf( -r.sy, Ckz, comp( C, r.ky ) );
+	float U = Cx * By - Cy * Bx;
+	float V = Ax * Cy - Ay * Cx;
+	float W = Bx * Ay - By * Ax;
+	if ( U == 0.f || V == 0.f || W == 0.f )
+	{
+		// Exact fallback on an edge, as the watertight method prescribes.
+		U = float( double( Cx ) * double( By ) - double( Cy ) * double( Bx ) );
+		V = float( double( Ax ) * double( Cy ) - double( Ay ) * double( Cx ) );
+		W = float( double( Bx ) * double( Ay ) - double( By ) * double( Ax ) );
+	}
+	if ( ( U < 0.f || V < 0.f || W < 0.f ) && ( U > 0.f || V > 0.f || W > 0.f ) ) return false;
+	float det = U + V + W;
+	if ( det == 0.f ) return false;
+	float T = U * ( r.sz * Akz ) + V * ( r.sz * Bkz ) + W * ( r.sz * Ckz );
+	float sdet = fabsf( det );
+	float sT = det < 0.f ? -T : T;
+	if ( !( sT > tmin * sdet ) || !( sT < tmax * sdet ) ) return false;
+	float rcp = 1.0f / det;
+	t = T * rcp;
+	u = V * rcp;
+	v = W * rcp;
+	return true;
+}
+
+// Sphere::intersect (reference src/core/primitive/sphere.hpp:31-54): near
+// root, else far root, accepted when t >= 0 and within (tmin, tmax).
+// The roots are formed without the reference's cancellation-prone
+// |oc|^2 - (d.oc)^2: the squared distance of the centre from the ray line is
+// taken from the perpendicular vector itself, and the smaller-magnitude root
+// comes from the product of the roots (c / q), as in Haines et al.,
+// "Precision Improvements for Ray/Sphere Intersection" (Ray Tracing Gems, 2019).
+__device__ __forceinline__ bool sphere_test( const DevSphere &s, float3 o, float3 d, float tmin, float tmax, float &t )
+{
+	float3 oc = f3( s.c ) - o;
+	float poc = dot( d, oc );
+	float3 perp = oc - d * poc;
+	float det = s.r2 - dot( perp, perp );
+	if ( det < 0.f ) return false;
+	float q = poc + copysignf( sqrtf( det ), poc );  // root of larger magnitude
+	float c = dot( oc, oc ) - s.r2;
+	float r0 = q != 0.f ? c / q : 0.f, r1 = q;
+	float t_near = fminf( r0, r1 ), t_far = fmaxf( r0, r1 );
+	t = t_near < 0.f ? t_far : t_near;
+	return t >= 0.f && t > tmin && t < tmax;
+}
+
+__device__ __forceinline__ float q8( uint32_t w, int sh ) { return float( ( w >> sh ) & 0xFFu ); }
+
+struct WorkCount
+{
+	uint32_t nodes, tris;
+};
+
+// Quantised 8-wide BVH traversal with a short stack of (base, hit-mask) node
+// groups.  ANY = shadow query (first hit ends it).  Returns true on a hit;
+// the closest-hit result is written to `hit` (t, BVH-order triangle slot or
+// HIT_SPHERE | sphere, u, v).  *err is set when the stack would overflow.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ bool traverse( const DevScene &sc, float3 o, float3 d, float tmin, float tmax,
+										  HitRec &hit, WorkCount &wc, uint32_t *err )
+{
+	hit.t = tmax;
+	hit.id = HIT_MISS;
+	hit.u = hit.v = 0.f;
+	bool found = false;
+	for ( uint32_t s = 0; s < sc.n_spheres; ++s )
+	{
+		float t;
+		if ( sphere_test( sc.spheres[ s ], o, d, tmin, hit.t, t ) )
+		{
+			hit.t = t;
+			hit.id = HIT_SPHERE | s;
+			found = true;
+			if ( ANY ) return true;
+		}
+	}
+	// A NaN ray would pass every slab test (fminf/fmaxf drop NaN operands)
+	// and walk the whole tree; it hits nothing.
+	if ( sc.n_nodes == 0 || !finite3( o ) || !finite3( d ) ) return found;
+	RayPre r = make_ray( o, d );
+	// Node boxes are tested against a slightly widened interval so that float
+	// rounding in the slab test never culls a triangle the exact test accepts.
+	const float grow = 1.0f + 4.0f * 5.96e-8f;
+	uint2 stack[ TRAVERSAL_STACK ];
+	int sp = 0;
+	// Start with the root as the only child of a virtual group: slot 0, internal.
+	uint2 ng = make_uint2( 0u, ( 1u << ( 24 + r.oct ) ) | 1u );
+	const uint4 *base = reinterpret_cast<const uint4 *>( sc.nodes );
+	// A tree visits each node at most once per ray; the cap and the index
+	// checks turn a malformed tree into an error flag instead of a hang or
+	// an out-of-bounds read.
+	uint32_t budget = sc.n_nodes;
+	for ( ;; )
+	{
+		// Next child node of the current node group, nearest octant slot first.
+		uint32_t b = __ffs( ng.y >> 24 ) - 1;
+		ng.y &= ~( 1u << ( 24 + b ) );
+		uint32_t slot = b ^ r.oct;
+		uint32_t node = ng.x + __popc( ng.y & 0xFFu & ( ( 1u << slot ) - 1u ) );
+		if ( node >= sc.n_nodes || budget-- == 0 )
+		{
+			atomicOr( err, 2u );
+			break;
+		}
+		if ( ng.y > 0x00FFFFFFu )
+		{
+			if ( sp < TRAVERSAL_STACK )
+				stack[ sp++ ] = ng;
+			else
+				atomicOr( err, 1u );
+		}
+		const uint4 *np = base + 5 * size_t( node );
+		uint4 n0 = __ldg( np ), n1 = __ldg( np + 1 ), n2 = __ldg( np + 2 ), n3 = __ldg( np + 3 ), n4 = __ldg( np + 4 );
+		if ( COUNT ) ++wc.nodes;
+		float3 p = f3( __uint_as_float( n0.x ), __uint_as_float( n0.y ), __uint_as_float( n0.z ) );
+		uint32_t ex = n0.w & 0xFFu, ey = ( n0.w >> 8 ) & 0xFFu, ez = ( n0.w >> 16 ) & 0xFFu, imask = n0.w >> 24;
+		float3 adj_s = f3( __uint_as_float( ex << 23 ) * r.invd.x, __uint_as_float( ey << 23 ) * r.invd.y,
+						   __uint_as_float( ez << 23 ) * r.invd.z );
+		float3 adj_o = ( p - o ) * r.invd;
+		// Near/far quantised planes per axis, by ray direction sign.
+		uint32_t nx0 = n2.x, nx1 = n2.y, fx0 = n3.z, fx1 = n3.w;
+		uint32_t ny0 = n2.z, ny1 = n2.w, fy0 = n4.x, fy1 = n4.y;
+		uint32_t nz0 = n3.x, nz1 = n3.y, fz0 = n4.z, fz1 = n4.w;
+		if ( r.oct & 1u ) { uint32_t t0 = nx0, t1 = nx1; nx0 = fx0, nx1 = fx1, fx0 = t0, fx1 = t1; }
+		if ( r.oct & 2u ) { uint32_t t0 = ny0, t1 = ny1; ny0 = fy0, ny1 = fy1, fy0 = t0, fy1 = t1; }
+		if ( r.oct & 4u ) { uint32_t t0 = nz0, t1 = nz1; nz0 = fz0, nz1 = fz1, fz0 = t0, fz1 = t1; }
+		const float tlim = hit.t * grow;
+		uint32_t node_hits = 0, tri_hits = 0;
+#pragma unroll
+		for ( int i = 0; i < 8; ++i )
+		{
+			const int sh = 8 * ( i & 3 );
+			uint32_t wnx = i < 4 ? nx0 : nx1, wny = i < 4 ? ny0 : ny1, wnz = i < 4 ? nz0 : nz1;
+			uint32_t wfx = i < 4 ? fx0 : fx1, wfy = i < 4 ? fy0 : fy1, wfz = i < 4 ? fz0 : fz1;
+			float tnx = fmaf( q8( wnx, sh ), adj_s.x, adj_o.x ), tfx = fmaf( q8( wfx, sh ), adj_s.x, adj_o.x );
+			float tny = fmaf( q8( wny, sh ), adj_s.y, adj_o.y ), tfy = fmaf( q8( wfy, sh ), adj_s.y, adj_o.y );
+			float tnz = fmaf( q8( wnz, sh ), adj_s.z, adj_o.z ), tfz = fmaf( q8( wfz, sh ), adj_s.z, adj_o.z );
+			float tn = fmaxf( fmaxf( tnx, tny ), fmaxf( tnz, tmin ) );
+			float tf = fminf( fminf( tfx, tfy ), fminf( tfz, tlim ) );
+			uint32_t meta = ( ( i < 4 ? n1.z : n1.w ) >> sh ) & 0xFFu;
+			bool internal = ( imask >> i ) & 1u;
+			if ( tn <= tf )
+			{
+				if ( internal )
+					node_hits |= 1u << ( i ^ r.oct );
+				else if ( meta )
+					tri_hits |= ( ( 1u << ( meta >> 5 ) ) - 1u ) << ( meta & 31u );
+			}
+		}
+		ng = node_hits ? make_uint2( n1.x, ( node_hits << 24 ) | imask ) : make_uint2( 0u, 0u );
+		// Leaf triangles of this node.
+		while ( tri_hits )
+		{
+			uint32_t k = __ffs( tri_hits ) - 1;
+			tri_hits &= tri_hits - 1;
+			uint32_t ti = n1.y + k;
+			if ( ti >= sc.n_tris )
+			{
+				atomicOr( err, 4u );
+				break;
+			}
+			const float4 *tp = sc.tris + 3 * size_t( ti );
+			float4 a = __ldg( tp ), bq = __ldg( tp + 1 ), c = __ldg( tp + 2 );
+			if ( COUNT ) ++wc.tris;
+			float t, u, v;
+			if ( tri_test( r, f3( a ), f3( bq ), f3( c ), tmin, hit.t, t, u, v ) )
+			{
+				hit.t = t;
+				hit.id = ti;
+				hit.u = u;
+				hit.v = v;
+				found = true;
+				if ( ANY ) return true;
+			}
+		}
+		if ( ng.y <= 0x00FFFFFFu )
+		{
+			if ( sp == 0 ) break;
+			ng = stack[ --sp ];
+		}
+	}
+	return found;
+}
+
+// ------------------------------------------------------------------ shading helpers
+// Reference frame (src/core/meta/scene.hpp:48-53): u = n x (0,1,0), v = n x u,
+// both normalised (NaN when n is parallel to +-y, as in the reference).
+struct Frame
+{
+	float3 u, v, n;
+	__device__ float3 local( float3 w ) const { return normalize( f3( dot( w, u ), dot( w, v ), dot( w, n ) ) ); }
+	__device__ float3 global( float3 w ) const { return normalize( u * w.x + v * w.y + n * w.z ); }
+};
+
+__device__ __forceinline__ Frame koishi_frame( float3 n )
+{
+	Frame f;
+	f.n = n;
+	f.u = normalize( f3( -n.z, 0.f, n.x ) );
+	f.v = normalize( cross( n, f.u ) );
+	return f;
+}
+
+// Orthonormal basis of Duff et al., "Building an Orthonormal Basis, Revisited"
+// (JCGT 2017).
+__device__ __forceinline__ Frame onb_frame( float3 n )
+{
+	Frame f;
+	f.n = n;
+	float sign = copysignf( 1.0f, n.z );
+	float a = -1.0f / ( sign + n.z );
+	float b = n.x * n.y * a;
+	f.u = f3( 1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x );
+	f.v = f3( b, sign + n.y * n.y * a, -n.y );
+	return f;
+}
+
+// H::sampleCos (src/util/hemisphere.hpp:76-95): concentric disk mapping.
+__device__ __forceinline__ float3 sample_cos( float r1, float r2 )
+{
+	float ux = 2.f * r1 - 1.f, uy = 2.f * r2 - 1.f;
+	if ( ux == 0.f && uy == 0.f ) return f3( 0.f, 0.f, 1.f );
+	float r, phi;
+	if ( ux * ux > uy * uy )
+		r = ux, phi = ( PI_F / 4.f ) * ( uy / ux );
+	else
+		r = uy, phi = ( PI_F / 2.f ) - ( PI_F / 4.f ) * ( ux / uy );
+	float s, c;
+	sincosf( phi, &s, &c );
+	return f3( r * c, r * s, sqrtf( fmaxf( 0.f, 1.f - r * r ) ) );
+}
+
+// BeckmannDistribution::f (src/ext/distribution/beckmann.hpp:19-24): D(h)|cos|.
+__device__ __forceinline__ float beckmann_f( float alpha2, float3 w )
+{
+	float c2 = w.z * w.z;
+	float s2 = fmaxf( 0.f, 1.f - c2 );
+	float tg2 = s2 / c2;
+	return expf( -tg2 / alpha2 ) / ( PI_F * alpha2 * c2 * c2 ) * fabsf( w.z );
+}
+
+// BeckmannDistribution::sample (src/ext/distribution/beckmann.hpp:26-38).
+__device__ __forceinline__ float3 beckmann_sample( float alpha2, float u1, float u2 )
+{
+	float tg2 = -alpha2 * logf( u1 );
+	float phi = u2 * 2.f * PI_F;
+	float costh = 1.f / sqrtf( 1.f + tg2 );
+	float sinth = sqrtf( fmaxf( 0.f, 1.f - costh * costh ) );
+	float s, c;
+	sincosf( phi, &s, &c );
+	return f3( sinth * s, sinth * c, costh );
+}
+
+__device__ __forceinline__ float3 reflect( float3 I, float3 N ) { return N * ( dot( N, I ) * 2.f ) - I; }
+
+// Koishi estimator, compute_f_by_wi_wo: Lambert (lambert.hpp:31-33),
+// GlossyBSDF (glossy.hpp:27-29), Emission = white Lambert (emission.hpp:22-27).
+__device__ __forceinline__ float3 koishi_eval( const DevShader &sh, float3 wo, float3 wi )
+{
+	if ( sh.type == SH_GLOSSY ) return f3( sh.color ) * beckmann_f( sh.alpha2, normalize( wo + wi ) );
+	return wi.z >= 0.f ? f3( sh.albedo ) * ( 1.0f / PI_F ) : f3( 0.f, 0.f, 0.f );
+}
+
+// Koishi estimator, sample_wi_f_by_wo (lambert.hpp:26-30 with cosine.hpp:16-25,
+// glossy.hpp:22-26).  Returns f; the caller multiplies by |cos|.
+__device__ __forceinline__ float3 koishi_sample( const DevShader &sh, float3 wo, float u1, float u2, float3 &wi )
+{
+	if ( sh.type == SH_GLOSSY )
+	{
+		float3 h = beckmann_sample( sh.alpha2, u1, u2 );
+		wi = reflect( wo, h );
+		return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
+	}
+	wi = sample_cos( u1, u2 );
+	return wi.z >= 0.f ? f3( sh.albedo ) : f3( 0.f, 0.f, 0.f );
+}
+
+// MIS estimator BSDFs: Lambert albedo/pi with cosine pdf; Beckmann microfacet
+// reflection color*D*G/(4 cos_o cos_i) with the Smith G1 rational fit of
+// Walter et al. (EGSR 2007) and pdf D cos_h / (4 |wo.h|).
+__device__ __forceinline__ float smith_g1( float alpha, float3 w )
+{
+	float c = w.z;
+	if ( c <= 0.f ) return 0.f;
+	float s = sqrtf( fmaxf( 0.f, 1.f - c * c ) );
+	if ( s == 0.f ) return 1.f;
+	float a = c / ( alpha * s );
+	if ( a >= 1.6f ) return 1.f;
+	return ( 3.535f * a + 2.181f * a * a ) / ( 1.f + 2.276f * a + 2.577f * a * a );
+}
+
+// Beckmann D(h) with tan^2 from the tangential components, which keeps FP32
+// accuracy for half-vectors near the normal (1 - cos^2 cancels there).
+__device__ __forceinline__ float beckmann_d( float alpha2, float3 h )
+{
+	float c2 = h.z * h.z;
+	float tg2 = ( h.x * h.x + h.y * h.y ) / c2;
+	return expf( -tg2 / alpha2 ) / ( PI_F * alpha2 * c2 * c2 );
+}
+
+__device__ __forceinline__ float3 mis_eval( const DevShader &sh, float3 wo, float3 wi, float &pdf )
+{
+	pdf = 0.f;
+	if ( wo.z <= 0.f || wi.z <= 0.f ) return f3( 0.f, 0.f, 0.f );
+	if ( sh.type == SH_GLOSSY )
+	{
+		float3 h = normalize( wo + wi );
+		float dh = beckmann_d( sh.alpha2, h );
+		float G = smith_g1( sh.alpha, wo ) * smith_g1( sh.alpha, wi );
+		pdf = dh * h.z / ( 4.f * fabsf( dot( wo, h ) ) );
+		return f3( sh.color ) * ( dh * G / ( 4.f * wo.z * wi.z ) );
+	}
+	pdf = wi.z * ( 1.0f / PI_F );
+	return f3( sh.albedo ) * ( 1.0f / PI_F );
+}
+
+// Returns the sample weight f*cos/pdf (zero when the sample is rejected).
+// For the Beckmann lobe D cancels: weight = color * G * |wo.h| / (cos_o cos_h).
+__device__ __forceinline__ float3 mis_sample( const DevShader &sh, float3 wo, float u1, float u2, float3 &wi, float &pdf )
+{
+	pdf = 0.f;
+	if ( sh.type == SH_GLOSSY )
+	{
+		float3 h = beckmann_sample( sh.alpha2, u1, u2 );
+		wi = reflect( wo, h );
+		float woh = dot( wo, h );
+		if ( wo.z <= 0.f || wi.z <= 0.f || woh <= 0.f ) return f3( 0.f, 0.f, 0.f );
+		float G = smith_g1( sh.alpha, wo ) * smith_g1( sh.alpha, wi );
+		pdf = beckmann_d( sh.alpha2, h ) * h.z / ( 4.f * woh );
+		return f3( sh.color ) * ( G * woh / ( wo.z * h.z ) );
+	}
+	wi = sample_cos( u1, u2 );
+	if ( wo.z <= 0.f || wi.z <= 0.f ) return f3( 0.f, 0.f, 0.f );
+	pdf = wi.z * ( 1.0f / PI_F );
+	return f3( sh.albedo );
+}
+
+// Spawn point offset off a surface along its geometric normal by an amount
+// that scales with the point's magnitude (Waechter and Binder, "A Fast and
+// Robust Method for Avoiding Self-Intersection", Ray Tracing Gems 2019).
+__device__ __forceinline__ float3 offset_ray( float3 p, float3 n )
+{
+	const float origin = 1.0f / 32.0f, float_scale = 1.0f / 65536.0f, int_scale = 256.0f;
+	int3 of_i = make_int3( int( int_scale * n.x ), int( int_scale * n.y ), int( int_scale * n.z ) );
+	float3 p_i = f3( __int_as_float( __float_as_int( p.x ) + ( p.x < 0 ? -of_i.x : of_i.x ) ),
+					 __int_as_float( __float_as_int( p.y ) + ( p.y < 0 ? -of_i.y : of_i.y ) ),
+					 __int_as_float( __float_as_int( p.z ) + ( p.z < 0 ? -of_i.z : of_i.z ) ) );
+	return f3( fabsf( p.x ) < origin ? p.x + float_scale * n.x : p_i.x,
+			   fabsf( p.y ) < origin ? p.y + float_scale * n.y : p_i.y,
+			   fabsf( p.z ) < origin ? p.z + float_scale * n.z : p_i.z );
+}
+
+}  // namespace cr

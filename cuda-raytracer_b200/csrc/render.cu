@@ -1,0 +1,757 @@
+// Wavefront Radiance integrator and batched ray queries.
+//
+// The reference runs one RadianceKernel::execute per (pixel, sample) on a CPU
+// thread (src/core/kernel/radiance.cu:14-81, src/core/tracer/cpuMulticore.cu:53-64).
+// Here a wave of paths advances one bounce at a time through separate
+// kernels so every stage runs with coherent control flow:
+//
+//   k_generate   camera rays (PinholeLens::sample, src/core/misc/lens.hpp:62-66)
+//   per bounce:
+//     k_extend   closest hit for the live queue            (Scene::intersect(Ray))
+//     k_shade    emission, NEE set-up, BSDF continuation, Russian roulette;
+//                appends to the shadow queue and the next live queue with one
+//                warp ballot + one atomic per warp
+//     k_shadow   any hit for the shadow queue; unoccluded contributions added
+//   k_accumulate per-pixel FP64 sums of the finite samples (cpuMulticore.cu:58-64)
+//
+// Queue lengths live in device memory, so a wave needs no host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cr.h"
+#include "cr_device.cuh"
+#include "render.h"
+
+namespace cr
+{
+namespace
+{
+constexpr float KOISHI_EPS = 4e-3f;  // LocalVaryings::emitRay/emitSeg offset (varyings.hpp:19-37)
+
+struct WaveArgs
+{
+	uint64_t first;  // first global sample of the wave
+	uint32_t n;      // samples in the wave
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated append: every lane of the warp calls this with its flag.
+__device__ __forceinline__ uint32_t warp_append( bool want, uint32_t *counter )
+{
+	uint32_t mask = __ballot_sync( ~0u, want );
+	if ( !mask ) return 0;
+	uint32_t leader = __ffs( mask ) - 1;
+	uint32_t base = 0;
+	if ( lane_id() == leader ) base = atomicAdd( counter, __popc( mask ) );
+	base = __shfl_sync( ~0u, base, leader );
+	return base + __popc( mask & ( ( 1u << lane_id() ) - 1u ) );
+}
+
+__global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa )
+{
+	if ( blockIdx.x == 0 && threadIdx.x == 0 ) wb.counters[ 0 ] = wa.n;
+	for ( uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < wa.n; s += gridDim.x * blockDim.x )
+	{
+		uint64_t g = wa.first + s;
+		uint32_t pix = uint32_t( g / cfg.spp ), k = uint32_t( g % cfg.spp );
+		uint32_t x = cfg.x0 + pix % cfg.ww, y = cfg.y0 + pix / cfg.ww;
+		const DevCamera &c = sc.cam;
+		float fx = float( x ) - float( c.width ) * 0.5f, fy = float( y ) - float( c.height ) * 0.5f;
+		float3 t = f3( c.n ) + f3( c.u ) * fx + f3( c.v ) * fy;
+		float3 d = normalize( t + f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
+		wb.ray_o[ s ] = make_float4( c.o[ 0 ], c.o[ 1 ], c.o[ 2 ], 0.f );
+		wb.ray_d[ s ] = make_float4( d.x, d.y, d.z, INFINITY );
+		wb.beta[ s ] = make_float4( 1.f, 1.f, 1.f, 0.f );
+		wb.L[ s ] = make_float4( 0.f, 0.f, 0.f, 0.f );
+		wb.queue[ 0 ][ s ] = s;
+	}
+}
+
+template <bool COUNT>
+__device__ __forceinline__ void flush_work( WorkCount &wc, unsigned long long *work )
+{
+	if ( !COUNT ) return;
+	uint32_t n = wc.nodes, t = wc.tris;
+	for ( int o = 16; o; o >>= 1 )
+	{
+		n += __shfl_xor_sync( ~0u, n, o );
+		t += __shfl_xor_sync( ~0u, t, o );
+	}
+	if ( lane_id() == 0 )
+	{
+		atomicAdd( work, (unsigned long long)n );
+		atomicAdd( work + 1, (unsigned long long)t );
+	}
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__( 128 ) k_extend( DevScene sc, WaveBuffers wb, uint32_t bounce )
+{
+	const uint32_t n = wb.counters[ 2 * bounce ];
+	const uint32_t *q = wb.queue[ bounce & 1 ];
+	WorkCount wc{ 0, 0 };
+	const uint32_t stride = gridDim.x * blockDim.x;
+	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
+	{
+		uint32_t i = base + lane_id();
+		if ( i < n )
+		{
+			uint32_t path = q[ i ];
+			float4 o = wb.ray_o[ path ], d = wb.ray_d[ path ];
+			HitRec h;
+			traverse<false, COUNT>( sc, f3( o ), f3( d ), o.w, d.w, h, wc, wb.err );
+			wb.hit[ path ] = h;
+		}
+	}
+	flush_work<COUNT>( wc, wb.work );
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__( 128 ) k_shadow( DevScene sc, WaveBuffers wb, uint32_t bounce )
+{
+	const uint32_t n = wb.counters[ 2 * bounce + 1 ];
+	WorkCount wc{ 0, 0 };
+	const uint32_t stride = gridDim.x * blockDim.x;
+	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
+	{
+		uint32_t i = base + lane_id();
+		if ( i < n )
+		{
+			uint32_t path = wb.shadow_queue[ i ];
+			float4 o = wb.sh_o[ path ], d = wb.sh_d[ path ];
+			HitRec h;
+			if ( !traverse<true, COUNT>( sc, f3( o ), f3( d ), o.w, d.w, h, wc, wb.err ) )
+			{
+				float4 c = wb.sh_c[ path ], l = wb.L[ path ];
+				wb.L[ path ] = make_float4( l.x + c.x, l.y + c.y, l.z + c.z, l.w );
+			}
+		}
+	}
+	flush_work<COUNT>( wc, wb.work + 2 );
+}
+
+struct Surface
+{
+	float3 p, ns, ng;
+	int32_t shader, light;
+};
+
+__device__ __forceinline__ Surface surface_at( const DevScene &sc, float3 o, float3 d, const HitRec &h, bool need_ng )
+{
+	Surface s;
+	s.p = o + d * h.t;
+	if ( h.id & HIT_SPHERE )
+	{
+		const DevSphere &sp = sc.spheres[ h.id & ~HIT_SPHERE ];
+		s.ns = normalize( s.p - f3( sp.c ) );  // Sphere::normal (sphere.hpp:18-21, 52)
+		s.ng = s.ns;
+		s.shader = sp.shader;
+		s.light = sp.light;
+		return s;
+	}
+	const float4 *tp = sc.tris + 3 * size_t( h.id );
+	float4 a = __ldg( tp );
+	uint32_t gid = __float_as_uint( a.w );
+	const float4 *ap = sc.attrs + 3 * size_t( gid );
+	float4 n0 = __ldg( ap ), n1 = __ldg( ap + 1 ), n2 = __ldg( ap + 2 );
+	// Mesh::normal (mesh.hpp:85-91) with interplot (ray.hpp:93-98).
+	s.ns = normalize( f3( n0 ) * ( 1.f - h.u - h.v ) + f3( n1 ) * h.u + f3( n2 ) * h.v );
+	s.shader = __float_as_int( n0.w );
+	s.light = __float_as_int( n2.w );
+	if ( need_ng )
+	{
+		float4 b = __ldg( tp + 1 ), c = __ldg( tp + 2 );
+		s.ng = normalize( cross( f3( b ) - f3( a ), f3( c ) - f3( a ) ) );
+	}
+	else
+		s.ng = s.ns;
+	return s;
+}
+
+// Light point for the reference estimator: AreaLight::sample via
+// Mesh::sample (mesh.hpp:92-98, 1024-point table) or Sphere::sample
+// (sphere.hpp:22-30, theta uniform in [0, pi]); area pdf.
+__device__ __forceinline__ void koishi_light_point( const DevScene &sc, const DevLight &lt, float ux, float uy,
+													float3 &lp, float3 &ln, float &pdf )
+{
+	if ( lt.kind == LIGHT_MESH )
+	{
+		uint32_t k = min( uint32_t( floorf( ux * 1024.f ) ), 1023u );
+		lp = f3( sc.light_tables[ 2 * ( lt.table + k ) ] );
+		ln = f3( sc.light_tables[ 2 * ( lt.table + k ) + 1 ] );
+		pdf = lt.koishi_pdf;
+		return;
+	}
+	const DevSphere &sp = sc.spheres[ lt.index ];
+	float th = ux * PI_F, ph = uy * PI_F * 2.f;
+	float st, ct, sph, cph;
+	sincosf( th, &st, &ct );
+	sincosf( ph, &sph, &cph );
+	float3 w = f3( st * sph, st * cph, ct );
+	lp = f3( sp.c ) + w * sp.r;
+	ln = w;
+	pdf = 1.f / ( 4.f * PI_F * sp.r2 );
+}
+
+// Light point for the MIS estimator: area-proportional triangle, uniform point.
+__device__ __forceinline__ void mis_light_point( const DevScene &sc, const DevLight &lt, float u0, float u1, float u2,
+												 float3 &lp, float3 &ln, float &pdfA )
+{
+	if ( lt.kind == LIGHT_SPHERE )
+	{
+		const DevSphere &sp = sc.spheres[ lt.index ];
+		float z = 1.f - 2.f * u1, r = sqrtf( fmaxf( 0.f, 1.f - z * z ) ), s, c;
+		sincosf( 2.f * PI_F * u2, &s, &c );
+		float3 w = f3( r * c, r * s, z );
+		lp = f3( sp.c ) + w * sp.r;
+		ln = w;
+		pdfA = 1.f / lt.area;
+		return;
+	}
+	const float *cdf = sc.light_cdf + lt.cdf;
+	float target = u0 * cdf[ lt.n_tris - 1 ];
+	int lo = 0, hi = lt.n_tris - 1;
+	while ( lo < hi )
+	{
+		int mid = ( lo + hi ) >> 1;
+		if ( cdf[ mid ] > target )
+			hi = mid;
+		else
+			lo = mid + 1;
+	}
+	const float4 *tv = sc.light_tris + 3 * size_t( lt.index + lo );
+	float3 v0 = f3( tv[ 0 ] ), v1 = f3( tv[ 1 ] ), v2 = f3( tv[ 2 ] );
+	float su = sqrtf( u1 ), b0 = 1.f - su, b1 = u2 * su;
+	lp = v0 * b0 + v1 * b1 + v2 * ( 1.f - b0 - b1 );
+	ln = normalize( cross( v1 - v0, v2 - v0 ) );
+	pdfA = 1.f / lt.area;
+}
+
+struct PathOut
+{
+	bool alive = false, shadow = false;
+	float4 ro, rd, so, sd, sc;
+};
+
+// One vertex of RadianceKernel::execute (radiance.cu:22-71), reference semantics.
+__device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
+											  uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
+											  float4 &L4, PathOut &out )
+{
+	float3 o = f3( ro ), d = f3( rd );
+	Surface s = surface_at( sc, o, d, h, false );
+	const DevShader sh = sc.shaders[ s.shader ];
+	Frame fr = koishi_frame( s.ns );
+	float3 wo = fr.local( -d );
+	float3 beta = f3( beta4 ), L = f3( L4 );
+	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
+	if ( sc.n_lights )
+	{
+		uint32_t nl = sc.n_lights;
+		uint32_t idx = min( uint32_t( floorf( r0.x * float( nl ) ) ), nl - 1 );
+		float lpdf = 1.f / float( nl );
+		const DevLight lt = sc.lights[ idx ];
+		float3 lp, ln;
+		float pdf;
+		koishi_light_point( sc, lt, r0.y, r0.z, lp, ln, pdf );
+		float3 wiw = s.p - lp;  // Primitive::sample(p,u,pdf) (primitive.hpp:25-33)
+		pdf *= dot( wiw, wiw ) / fabsf( dot( ln, normalize( wiw ) ) );
+		float3 dd = lp - s.p;   // LocalVaryings::emitSeg (varyings.hpp:27-37)
+		float3 sd = normalize( dd );
+		float3 diff = normalize( sd ) * KOISHI_EPS;
+		float3 so = s.p + diff;
+		float st = length( dd - 2.f * diff );
+		float3 wi = fr.local( normalize( lp - s.p ) );
+		float3 f = koishi_eval( sh, wo, wi );
+		float3 li = f3( lt.emission ) / pdf;
+		float3 c = beta * f * li * ( fabsf( wi.z ) / lpdf );
+		if ( !finite3( c ) )
+			L = f3( NAN, NAN, NAN );
+		else if ( !is_zero( c ) )
+		{
+			out.shadow = true;
+			out.so = make_float4( so.x, so.y, so.z, 0.f );
+			out.sd = make_float4( sd.x, sd.y, sd.z, st );
+			out.sc = make_float4( c.x, c.y, c.z, 0.f );
+		}
+		if ( sh.type == SH_EMISSION ) L = L + beta * f3( sh.emission );  // radiance.cu:39
+	}
+	float3 wi;
+	float3 f = koishi_sample( sh, wo, r1.x, r1.y, wi );  // radiance.cu:55-60
+	beta = beta * f * fabsf( wi.z );
+	float3 nd = fr.global( wi );
+	float3 no = s.p + nd * KOISHI_EPS;
+	bool alive = true;
+	float rr = maxc( beta );  // radiance.cu:62-68
+	if ( rr < 1.f && bounce > 3 )
+	{
+		float q = fmaxf( .05f, 1.f - rr );
+		if ( r0.w < q )
+			alive = false;
+		else
+			beta = beta / ( 1.f - q );
+	}
+	if ( bounce + 1 > cfg.max_bounce || is_zero( beta ) || !finite3( L ) || !finite3( beta ) ) alive = false;
+	if ( !finite3( L ) ) out.shadow = false;
+	beta4 = make_float4( beta.x, beta.y, beta.z, 0.f );
+	L4 = make_float4( L.x, L.y, L.z, 0.f );
+	out.alive = alive;
+	out.ro = make_float4( no.x, no.y, no.z, 0.f );
+	out.rd = make_float4( nd.x, nd.y, nd.z, INFINITY );
+}
+
+// One vertex of the MIS estimator (power heuristic over BSDF sampling and
+// area-light NEE; see cr_device.cuh for the BSDFs).
+__device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
+										   uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
+										   float4 &L4, PathOut &out )
+{
+	float3 o = f3( ro ), d = f3( rd );
+	Surface s = surface_at( sc, o, d, h, true );
+	const DevShader sh = sc.shaders[ s.shader ];
+	float3 beta = f3( beta4 ), L = f3( L4 );
+	float nl = float( sc.n_lights );
+	if ( sh.type == SH_EMISSION )
+	{
+		float w = 1.f;
+		if ( bounce > 0 && s.light >= 0 )
+		{
+			float cosl = fabsf( dot( s.ng, d ) );
+			float pb = beta4.w;
+			float pl = cosl > 0.f ? h.t * h.t / cosl / sc.lights[ s.light ].area / nl : INFINITY;
+			w = pb * pb / ( pb * pb + pl * pl );
+		}
+		L = L + beta * f3( sh.emission ) * w;
+	}
+	// Two-sided shading: the geometric normal faces the incoming ray and the
+	// shading normal is put on the same side.
+	if ( dot( s.ng, d ) > 0.f ) s.ng = -s.ng;
+	if ( dot( s.ns, s.ng ) < 0.f ) s.ns = -s.ns;
+	Frame fr = onb_frame( s.ns );
+	float3 wo = fr.local( -d );
+	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
+	if ( sc.n_lights )
+	{
+		uint32_t nli = sc.n_lights;
+		uint32_t idx = min( uint32_t( floorf( r0.x * nl ) ), nli - 1 );
+		float ur = r0.x * nl - float( idx );
+		const DevLight lt = sc.lights[ idx ];
+		float3 lp, ln;
+		float pdfA;
+		mis_light_point( sc, lt, ur, r0.y, r0.z, lp, ln, pdfA );
+		float3 dw = lp - s.p;
+		float dist2 = dot( dw, dw ), dist = sqrtf( dist2 );
+		float3 wiw = dw / dist;
+		float cosl = fabsf( dot( ln, wiw ) );
+		if ( cosl > 0.f && dist > 0.f && dot( wiw, s.ng ) > 0.f )
+		{
+			float pl = pdfA * dist2 / cosl / nl;
+			float3 wi = fr.local( wiw );
+			float pb;
+			float3 f = mis_eval( sh, wo, wi, pb );
+			if ( !is_zero( f ) )
+			{
+				float w = pl * pl / ( pl * pl + pb * pb );
+				float3 c = beta * f * f3( lt.emission ) * ( wi.z * w / pl );
+				if ( finite3( c ) && !is_zero( c ) )
+				{
+					// Both ends leave their surfaces: the shading point along its
+					// geometric normal, the light point along the light's normal
+					// towards the shading point; the ray runs between the two.
+					float3 so = offset_ray( s.p, s.ng );
+					float3 to = offset_ray( lp, dot( ln, wiw ) < 0.f ? ln : -ln );
+					float3 sd = to - so;
+					float len = length( sd );
+					sd = sd / len;
+					out.shadow = true;
+					out.so = make_float4( so.x, so.y, so.z, 0.f );
+					out.sd = make_float4( sd.x, sd.y, sd.z, len );
+					out.sc = make_float4( c.x, c.y, c.z, 0.f );
+				}
+			}
+		}
+	}
+	float3 wi;
+	float pdf;
+	float3 wt = mis_sample( sh, wo, r1.x, r1.y, wi, pdf );
+	beta = beta * wt;
+	float3 nd = fr.global( wi );
+	bool alive = !is_zero( beta ) && dot( nd, s.ng ) > 0.f;
+	float rr = maxc( beta );
+	if ( alive && rr < 1.f && bounce > 3 )
+	{
+		float q = fmaxf( .05f, 1.f - rr );
+		if ( r0.w < q )
+			alive = false;
+		else
+			beta = beta / ( 1.f - q );
+	}
+	if ( bounce + 1 > cfg.max_bounce || !finite3( beta ) ) alive = false;
+	float3 no = offset_ray( s.p, s.ng );
+	beta4 = make_float4( beta.x, beta.y, beta.z, pdf );
+	L4 = make_float4( L.x, L.y, L.z, 0.f );
+	out.alive = alive;
+	out.ro = make_float4( no.x, no.y, no.z, 0.f );
+	out.rd = make_float4( nd.x, nd.y, nd.z, INFINITY );
+}
+
+__global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
+												  uint32_t bounce, uint2 key )
+{
+	const uint32_t n = wb.counters[ 2 * bounce ];
+	const uint32_t *q = wb.queue[ bounce & 1 ];
+	uint32_t *nq = wb.queue[ ( bounce + 1 ) & 1 ];
+	uint32_t *next_count = wb.counters + 2 * ( bounce + 1 );
+	uint32_t *shadow_count = wb.counters + 2 * bounce + 1;
+	const uint32_t stride = gridDim.x * blockDim.x;
+	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
+	{
+		uint32_t i = base + lane_id();
+		PathOut out;
+		uint32_t path = 0;
+		if ( i < n )
+		{
+			path = q[ i ];
+			HitRec h = wb.hit[ path ];
+			if ( h.id != HIT_MISS )
+			{
+				float4 beta = wb.beta[ path ], L = wb.L[ path ];
+				float4 ro = wb.ray_o[ path ], rd = wb.ray_d[ path ];
+				// Random streams are keyed by the absolute (pixel, sample), so a
+				// film does not depend on the window or the wave size.
+				uint64_t gw = wa.first + path;
+				uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
+				uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
+				if ( cfg.estimator == EST_MIS )
+					shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
+				else
+					shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
+				wb.beta[ path ] = beta;
+				wb.L[ path ] = L;
+				if ( out.alive )
+				{
+					wb.ray_o[ path ] = out.ro;
+					wb.ray_d[ path ] = out.rd;
+				}
+				if ( out.shadow )
+				{
+					wb.sh_o[ path ] = out.so;
+					wb.sh_d[ path ] = out.sd;
+					wb.sh_c[ path ] = out.sc;
+				}
+			}
+		}
+		uint32_t si = warp_append( out.shadow, shadow_count );
+		if ( out.shadow ) wb.shadow_queue[ si ] = path;
+		uint32_t ni = warp_append( out.alive, next_count );
+		if ( out.alive ) nq[ ni ] = path;
+	}
+}
+
+__global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, double *sum, double *sumsq,
+							  uint32_t *count )
+{
+	uint64_t p0 = wa.first / cfg.spp, p1 = ( wa.first + wa.n - 1 ) / cfg.spp;
+	for ( uint64_t p = p0 + blockIdx.x * blockDim.x + threadIdx.x; p <= p1; p += gridDim.x * blockDim.x )
+	{
+		uint64_t s0 = max( p * cfg.spp, wa.first ), s1 = min( ( p + 1 ) * cfg.spp, wa.first + wa.n );
+		double a0 = 0, a1 = 0, a2 = 0, q0 = 0, q1 = 0, q2 = 0;
+		uint32_t c = 0;
+		for ( uint64_t s = s0; s < s1; ++s )
+		{
+			float4 l = wb.L[ s - wa.first ];
+			if ( !isfinite( l.x ) || !isfinite( l.y ) || !isfinite( l.z ) ) continue;  // cpuMulticore.cu:58-64
+			++c;
+			a0 += l.x, a1 += l.y, a2 += l.z;
+			q0 += double( l.x ) * l.x, q1 += double( l.y ) * l.y, q2 += double( l.z ) * l.z;
+		}
+		sum[ 3 * p ] += a0, sum[ 3 * p + 1 ] += a1, sum[ 3 * p + 2 ] += a2;
+		sumsq[ 3 * p ] += q0, sumsq[ 3 * p + 1 ] += q1, sumsq[ 3 * p + 2 ] += q2;
+		count[ p ] += c;
+	}
+}
+
+__global__ void k_trace( DevScene sc, const float *rays, uint64_t n, int any, cr_hit *out, uint32_t *err )
+{
+	WorkCount wc{ 0, 0 };
+	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
+	{
+		const float *r = rays + 7 * i;
+		float3 o = f3( r[ 0 ], r[ 1 ], r[ 2 ] ), d = f3( r[ 3 ], r[ 4 ], r[ 5 ] );
+		float tmax = r[ 6 ] > 0.f ? r[ 6 ] : INFINITY;
+		HitRec h;
+		bool hit = any ? traverse<true, false>( sc, o, d, 0.f, tmax, h, wc, err )
+					   : traverse<false, false>( sc, o, d, 0.f, tmax, h, wc, err );
+		cr_hit res;
+		res.prim = -1, res.tri = -1, res.t = INFINITY, res.u = res.v = 0.f;
+		if ( hit )
+		{
+			res.t = h.t, res.u = h.u, res.v = h.v;
+			if ( h.id & HIT_SPHERE )
+				res.prim = sc.spheres[ h.id & ~HIT_SPHERE ].prim;
+			else
+			{
+				uint32_t gid = __float_as_uint( sc.tris[ 3 * size_t( h.id ) ].w );
+				int prim = __float_as_int( sc.attrs[ 3 * size_t( gid ) + 1 ].w );
+				res.prim = prim;
+				res.tri = int( gid - sc.prim_first[ prim ] );
+			}
+		}
+		out[ i ] = res;
+	}
+}
+
+__global__ void k_bsdf_eval( int est, DevShader sh, const float *wo, const float *wi, uint64_t n, float *f, float *pdf )
+{
+	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
+	{
+		float3 o = f3( wo + 3 * i ), w = f3( wi + 3 * i ), r;
+		float p = 0.f;
+		if ( est == EST_MIS )
+			r = mis_eval( sh, o, w, p );
+		else
+			r = koishi_eval( sh, o, w );
+		f[ 3 * i ] = r.x, f[ 3 * i + 1 ] = r.y, f[ 3 * i + 2 ] = r.z;
+		pdf[ i ] = p;
+	}
+}
+
+__global__ void k_bsdf_sample( int est, DevShader sh, const float *wo, const float *u, uint64_t n, float *wi, float *wt,
+							   float *pdf )
+{
+	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
+	{
+		float3 o = f3( wo + 3 * i ), w, r;
+		float p = 0.f;
+		if ( est == EST_MIS )
+			r = mis_sample( sh, o, u[ 2 * i ], u[ 2 * i + 1 ], w, p );
+		else
+		{
+			r = koishi_sample( sh, o, u[ 2 * i ], u[ 2 * i + 1 ], w );
+			r = r * fabsf( w.z );
+		}
+		wi[ 3 * i ] = w.x, wi[ 3 * i + 1 ] = w.y, wi[ 3 * i + 2 ] = w.z;
+		wt[ 3 * i ] = r.x, wt[ 3 * i + 1 ] = r.y, wt[ 3 * i + 2 ] = r.z;
+		pdf[ i ] = p;
+	}
+}
+
+void check( cudaError_t e, const char *what )
+{
+	if ( e != cudaSuccess ) throw std::runtime_error( std::string( what ) + ": " + cudaGetErrorString( e ) );
+}
+
+template <typename T>
+void alloc( T *&p, size_t n, cudaStream_t st )
+{
+	check( cudaMallocAsync( (void **)&p, sizeof( T ) * std::max<size_t>( n, 1 ), st ), "wave alloc" );
+}
+
+struct EventPool
+{
+	std::vector<cudaEvent_t> ev;
+	size_t used = 0;
+	cudaEvent_t get()
+	{
+		if ( used == ev.size() )
+		{
+			cudaEvent_t e;
+			check( cudaEventCreate( &e ), "event" );
+			ev.push_back( e );
+		}
+		return ev[ used++ ];
+	}
+	~EventPool()
+	{
+		for ( auto e : ev ) cudaEventDestroy( e );
+	}
+};
+
+}  // namespace
+
+int sm_count()
+{
+	static int n = 0;
+	if ( !n )
+	{
+		int dev = 0;
+		cudaGetDevice( &dev );
+		cudaDeviceGetAttribute( &n, cudaDevAttrMultiProcessorCount, dev );
+		if ( n <= 0 ) n = 148;
+	}
+	return n;
+}
+
+void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaStream_t st )
+{
+	wb.capacity = capacity;
+	alloc( wb.ray_o, capacity, st );
+	alloc( wb.ray_d, capacity, st );
+	alloc( wb.hit, capacity, st );
+	alloc( wb.beta, capacity, st );
+	alloc( wb.L, capacity, st );
+	alloc( wb.queue[ 0 ], capacity, st );
+	alloc( wb.queue[ 1 ], capacity, st );
+	alloc( wb.shadow_queue, capacity, st );
+	alloc( wb.sh_o, capacity, st );
+	alloc( wb.sh_d, capacity, st );
+	alloc( wb.sh_c, capacity, st );
+	wb.n_counters = 2 * ( max_bounce + 3 );
+	alloc( wb.counters, wb.n_counters, st );
+	alloc( wb.err, 1, st );
+	alloc( wb.work, 4, st );
+	check( cudaMemsetAsync( wb.err, 0, sizeof( uint32_t ), st ), "wave init" );
+}
+
+void free_wave( WaveBuffers &wb, cudaStream_t st )
+{
+	void *ps[] = { wb.ray_o, wb.ray_d, wb.hit, wb.beta, wb.L, wb.queue[ 0 ], wb.queue[ 1 ], wb.shadow_queue,
+				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work };
+	for ( void *p : ps )
+		if ( p ) cudaFreeAsync( p, st );
+	wb = WaveBuffers();
+}
+
+void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb, double *film_sum, double *film_sumsq,
+				   uint32_t *film_count, cudaStream_t st, StageTimes *times )
+{
+	const uint64_t total = uint64_t( cfg.ww ) * cfg.wh * cfg.spp;
+	const uint32_t P = wb.capacity;
+	const int sms = sm_count();
+	const int g_ext = cfg.grid_extend > 0 ? cfg.grid_extend : sms * 8;
+	const int g_shade = cfg.grid_shade > 0 ? cfg.grid_shade : sms * 8;
+	const uint2 key = make_uint2( uint32_t( cfg.seed ), uint32_t( cfg.seed >> 32 ) ^ 0x5EED5EEDu );
+	EventPool pool;
+	struct Mark
+	{
+		cudaEvent_t a, b;
+		int kind;  // 0 extend 1 shadow 2 shade 3 other
+	};
+	std::vector<Mark> marks;
+	cudaEvent_t t0 = nullptr, t1 = nullptr;
+	if ( times )
+	{
+		t0 = pool.get();
+		t1 = pool.get();
+		check( cudaEventRecord( t0, st ), "event" );
+		if ( cfg.count_work ) check( cudaMemsetAsync( wb.work, 0, 4 * sizeof( unsigned long long ), st ), "memset" );
+	}
+	auto timed = [&]( int kind, auto &&launch ) {
+		if ( !times )
+		{
+			launch();
+			return;
+		}
+		Mark m{ pool.get(), pool.get(), kind };
+		check( cudaEventRecord( m.a, st ), "event" );
+		launch();
+		check( cudaEventRecord( m.b, st ), "event" );
+		marks.push_back( m );
+		times->launches++;
+		if ( kind == 0 ) times->extend_launches++;
+		if ( kind == 1 ) times->shadow_launches++;
+	};
+	std::vector<uint32_t> host_counts;
+	for ( uint64_t first = 0; first < total; first += P )
+	{
+		WaveArgs wa{ first, uint32_t( std::min<uint64_t>( P, total - first ) ) };
+		check( cudaMemsetAsync( wb.counters, 0, sizeof( uint32_t ) * wb.n_counters, st ), "memset" );
+		timed( 3, [&] {
+			int gg = int( std::min<uint64_t>( ( wa.n + 255 ) / 256, uint64_t( sms ) * 16 ) );
+			k_generate<<<gg, 256, 0, st>>>( sc, cfg, wb, wa );
+		} );
+		for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
+		{
+			timed( 0, [&] {
+				if ( cfg.count_work )
+					k_extend<true><<<g_ext, 128, 0, st>>>( sc, wb, b );
+				else
+					k_extend<false><<<g_ext, 128, 0, st>>>( sc, wb, b );
+			} );
+			timed( 2, [&] { k_shade<<<g_shade, 128, 0, st>>>( sc, cfg, wb, wa, b, key ); } );
+			if ( sc.n_lights )
+				timed( 1, [&] {
+					if ( cfg.count_work )
+						k_shadow<true><<<g_ext, 128, 0, st>>>( sc, wb, b );
+					else
+						k_shadow<false><<<g_ext, 128, 0, st>>>( sc, wb, b );
+				} );
+		}
+		timed( 3, [&] {
+			uint64_t npx = ( first + wa.n - 1 ) / cfg.spp - first / cfg.spp + 1;
+			int gg = int( std::min<uint64_t>( ( npx + 255 ) / 256, uint64_t( sms ) * 16 ) );
+			k_accumulate<<<gg, 256, 0, st>>>( cfg, wb, wa, film_sum, film_sumsq, film_count );
+		} );
+		check( cudaGetLastError(), "render launch" );
+		if ( times )
+		{
+			times->waves++;
+			host_counts.resize( wb.n_counters );
+			check( cudaMemcpyAsync( host_counts.data(), wb.counters, sizeof( uint32_t ) * wb.n_counters,
+									cudaMemcpyDeviceToHost, st ),
+				   "counts" );
+			check( cudaStreamSynchronize( st ), "counts" );
+			for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
+			{
+				times->rays_extend += host_counts[ 2 * b ];
+				times->rays_shadow += host_counts[ 2 * b + 1 ];
+			}
+		}
+	}
+	if ( times )
+	{
+		check( cudaEventRecord( t1, st ), "event" );
+		check( cudaEventSynchronize( t1 ), "event" );
+		float ms;
+		check( cudaEventElapsedTime( &ms, t0, t1 ), "event" );
+		times->total += ms;
+		for ( auto &m : marks )
+		{
+			check( cudaEventElapsedTime( &ms, m.a, m.b ), "event" );
+			( m.kind == 0 ? times->extend : m.kind == 1 ? times->shadow : m.kind == 2 ? times->shade : times->other ) += ms;
+		}
+		if ( cfg.count_work )
+		{
+			unsigned long long w[ 4 ];
+			check( cudaMemcpy( w, wb.work, sizeof w, cudaMemcpyDeviceToHost ), "work" );
+			times->nodes += w[ 0 ];
+			times->tris += w[ 1 ];
+			times->shadow_nodes += w[ 2 ];
+			times->shadow_tris += w[ 3 ];
+		}
+	}
+}
+
+void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit, cr_hit *out, uint32_t *err,
+				   cudaStream_t st )
+{
+	if ( !n ) return;
+	int g = int( std::min<uint64_t>( ( n + 127 ) / 128, uint64_t( sm_count() ) * 8 ) );
+	k_trace<<<g, 128, 0, st>>>( sc, rays, n, any_hit, out, err );
+	check( cudaGetLastError(), "trace launch" );
+}
+
+void launch_bsdf_eval( int est, const DevShader &sh, const float *wo, const float *wi, uint64_t n, float *f, float *pdf,
+					   cudaStream_t st )
+{
+	if ( !n ) return;
+	int g = int( std::min<uint64_t>( ( n + 255 ) / 256, 4096 ) );
+	k_bsdf_eval<<<g, 256, 0, st>>>( est, sh, wo, wi, n, f, pdf );
+	check( cudaGetLastError(), "bsdf launch" );
+}
+
+void launch_bsdf_sample( int est, const DevShader &sh, const float *wo, const float *u, uint64_t n, float *wi,
+						 float *wt, float *pdf, cudaStream_t st )
+{
+	if ( !n ) return;
+	int g = int( std::min<uint64_t>( ( n + 255 ) / 256, 4096 ) );
+	k_bsdf_sample<<<g, 256, 0, st>>>( est, sh, wo, u, n, wi, wt, pdf );
+	check( cudaGetLastError(), "bsdf launch" );
+}
+
+}  // namespace cr

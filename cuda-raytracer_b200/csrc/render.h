@@ -1,0 +1,66 @@
+// Host-side launch interface of the CUDA kernels (render.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "cr_common.h"
+
+struct cr_hit;
+
+namespace cr
+{
+// Per-path SoA state of one wave, sized for `capacity` paths.
+struct WaveBuffers
+{
+	uint32_t capacity = 0;
+	float4 *ray_o = nullptr, *ray_d = nullptr;  // (o, tmin), (d, tmax)
+	HitRec *hit = nullptr;
+	float4 *beta = nullptr;                     // (throughput, previous BSDF pdf)
+	float4 *L = nullptr;                        // (radiance, -)
+	uint32_t *queue[ 2 ] = { nullptr, nullptr };
+	uint32_t *shadow_queue = nullptr;
+	float4 *sh_o = nullptr, *sh_d = nullptr, *sh_c = nullptr;
+	uint32_t *counters = nullptr;               // [2b] extension queue, [2b+1] shadow queue of bounce b
+	uint32_t n_counters = 0;
+	uint32_t *err = nullptr;                    // device error word
+	unsigned long long *work = nullptr;         // extension [0] nodes [1] triangles, shadow [2] [3]
+};
+
+struct RenderConfig
+{
+	uint32_t spp, max_bounce;
+	int32_t estimator;
+	uint32_t x0, y0, ww, wh;  // window origin and size
+	uint64_t seed;
+	uint32_t wave_paths;
+	bool count_work;
+	int block_extend = 128, block_shade = 128;
+	int grid_extend = 0, grid_shade = 0;      // 0: device-derived default
+};
+
+struct StageTimes
+{
+	double extend = 0, shadow = 0, shade = 0, other = 0, total = 0;
+	uint32_t launches = 0, waves = 0, extend_launches = 0, shadow_launches = 0;
+	uint64_t rays_extend = 0, rays_shadow = 0, nodes = 0, tris = 0, shadow_nodes = 0, shadow_tris = 0;
+};
+
+void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaStream_t st );
+void free_wave( WaveBuffers &wb, cudaStream_t st );
+
+// Render the window into the film (device buffers, accumulated).  When
+// `times` is not null, stage times are measured with CUDA events and the
+// call synchronises `st` at the end.
+void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb, double *film_sum,
+				   double *film_sumsq, uint32_t *film_count, cudaStream_t st, StageTimes *times );
+
+void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit,
+				   cr_hit *out, uint32_t *err, cudaStream_t st );
+
+void launch_bsdf_eval( int estimator, const DevShader &sh, const float *wo, const float *wi, uint64_t n, float *f,
+					   float *pdf, cudaStream_t st );
+void launch_bsdf_sample( int estimator, const DevShader &sh, const float *wo, const float *u, uint64_t n, float *wi,
+						 float *weight, float *pdf, cudaStream_t st );
+
+int sm_count();
+}  // namespace cr

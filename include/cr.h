@@ -1,0 +1,189 @@
+/*
+ * cr.h: C ABI of the B200-native Radiance path tracer (libcr_b200.so).
+ *
+ * Drop-in replacement for the Radiance path of xlnx/cuda-raytracer
+ * ("Koishi").  Each entry point names the reference interface it replaces
+ * (paths are inside that project).  Plain C types only: pointers, sizes and
+ * opaque handles; no exceptions cross this boundary.  Every call returns
+ * CR_OK (0) or a negative CR_ERR_* code, with a message in cr_last_error().
+ *
+ * Ownership: the library owns every device buffer it allocates; caller host
+ * arrays are copied during the call.  A cr_scene is not thread-safe for
+ * mutation; renders of distinct scenes may run concurrently on distinct
+ * streams.  `stream` arguments are cudaStream_t values passed as void*
+ * (NULL = the legacy default stream).
+ */
+#ifndef CR_H
+#define CR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CR_OK 0
+#define CR_ERR_INVALID -1     /* bad argument or malformed input            */
+#define CR_ERR_PARSE -2       /* JSON / mesh file could not be read          */
+#define CR_ERR_CUDA -3        /* a CUDA call failed                          */
+#define CR_ERR_STATE -4       /* call not valid in the scene's current state */
+#define CR_ERR_UNSUPPORTED -5 /* feature named in input is not implemented   */
+#define CR_ERR_DEVICE -6      /* a kernel reported an internal error flag    */
+
+/* Estimators of the Radiance kernel. */
+#define CR_ESTIMATOR_KOISHI 0 /* reference semantics (radiance.cu:14-81)     */
+#define CR_ESTIMATOR_MIS 1    /* power-heuristic MIS of BSDF and area NEE    */
+
+typedef struct cr_scene cr_scene;
+
+/* One ray query result.  prim is the primitive index in scene order (meshes
+ * of an import asset in file order, spheres in asset order), tri the
+ * triangle index within that mesh (-1 for spheres), prim = -1 on a miss. */
+typedef struct cr_hit {
+    int32_t prim;
+    int32_t tri;
+    float t;
+    float u; /* barycentric weight of the triangle's second vertex */
+    float v; /* barycentric weight of the triangle's third vertex  */
+} cr_hit;
+
+typedef struct cr_render_desc {
+    uint32_t width, height, spp;
+    uint32_t max_bounce;     /* UINT32_MAX: the scene's kernel "maxBounce" (default 16) */
+    int32_t estimator;       /* CR_ESTIMATOR_*, or -1: the scene's kernel "estimator"   */
+    uint32_t x0, y0, x1, y1; /* pixel window [x0,x1)x[y0,y1); all zero = whole image    */
+    uint64_t seed;           /* Philox key for this render                             */
+    uint32_t wave_paths;     /* paths in flight per wave; 0 = autotuned default        */
+    int32_t guiding;         /* 1: learned path guiding (estimator MIS only)           */
+    int32_t count_work;      /* 1: also count BVH nodes / triangles visited            */
+} cr_render_desc;
+
+typedef struct cr_stats {
+    double ms_total;       /* device time of the whole render (CUDA events)  */
+    double ms_extend;      /* closest-hit traversal kernels                   */
+    double ms_shadow;      /* any-hit (shadow) traversal kernels              */
+    double ms_shade;       /* shading / NEE / queue compaction kernels        */
+    double ms_other;       /* generation, film accumulation, guiding          */
+    uint64_t samples;      /* camera paths traced                             */
+    uint64_t rays_extend;  /* closest-hit queries                             */
+    uint64_t rays_shadow;  /* any-hit queries                                 */
+    uint64_t nodes;        /* closest-hit: wide-BVH nodes fetched (count_work = 1) */
+    uint64_t tris;         /* closest-hit: triangles tested (count_work = 1)       */
+    uint64_t shadow_nodes; /* any-hit: wide-BVH nodes fetched (count_work = 1)     */
+    uint64_t shadow_tris;  /* any-hit: triangles tested (count_work = 1)           */
+    uint32_t launches;     /* kernels launched by the call                    */
+    uint32_t waves;        /* waves of paths                                  */
+    uint32_t extend_launches;
+    uint32_t shadow_launches;
+} cr_stats;
+
+/* ------------------------------------------------------------------ errors */
+/* Message for the last failing call on this thread.                        */
+const char *cr_last_error(void);
+/* Library version string. */
+const char *cr_version(void);
+
+/* ------------------------------------------------------------------ scenes */
+/* Scene::Scene(const Properties&) (src/core/meta/scene.cu:18-219) together
+ * with the Renderer's configuration read (src/core/renderer/renderer.cu:13-24,
+ * renderer.hpp:17-23): parses the reference JSON schema, loads the
+ * ["import", {"path"}] mesh file (OBJ, or the CRM binary mesh format,
+ * resolved against base_dir), spheres, shaders and cameras, and makes every
+ * Emission-shaded primitive an area light.  The scene is committed
+ * (uploaded, BVH built) before return. */
+int cr_scene_create(const char *json_text, const char *base_dir, cr_scene **out);
+
+/* An empty scene to be filled by the cr_scene_add_* calls below, then
+ * cr_scene_commit. */
+int cr_scene_create_empty(cr_scene **out);
+
+/* Factory<Shader>::create (src/core/basic/factory.hpp:15-23) over the shader
+ * registry of src/ext/shader/shader.impl.cu:15-24 (Lambert, GlossyBSDF with
+ * a Beckmann distribution, Emission).  config_json is the reference's
+ * [Type, {props}] array.  Returns the shader id (>= 0) or an error code. */
+int cr_scene_add_shader(cr_scene *s, const char *name, const char *config_json);
+
+/* PolyMesh(vertices, normals, indices) (src/core/primitive/mesh.cu:404-433):
+ * one triangle mesh with per-vertex normals, shaded by the named shader.
+ * Returns the primitive id (>= 0) or an error code. */
+int cr_scene_add_mesh(cr_scene *s, const float *vertices, uint32_t n_vertices, const float *normals,
+                      const uint32_t *indices, uint32_t n_triangles, const char *shader);
+
+/* The "sphere" asset (src/core/meta/scene.cu:136-156, sphere.hpp:9-16). */
+int cr_scene_add_sphere(cr_scene *s, const float *center, float radius, const char *shader);
+
+/* CameraConfig (src/util/config.hpp:12-35), pinhole lens; `target` is a
+ * direction, fovx the horizontal field of view in degrees. */
+int cr_scene_set_camera(cr_scene *s, const float *position, const float *target, const float *upaxis,
+                        float fovx);
+
+/* Upload and build the quantised 8-wide BVH on the GPU; replaces the host
+ * builder createBVH / doCreateBVH (src/core/primitive/mesh.cu:35-143).
+ * light_seed seeds the reference-compatible light-point tables
+ * (src/core/primitive/mesh.hpp:61-84). */
+int cr_scene_commit(cr_scene *s, uint64_t light_seed, void *stream);
+
+/* Counts after commit. */
+int cr_scene_info(const cr_scene *s, uint64_t *n_triangles, uint32_t *n_primitives, uint32_t *n_lights,
+                  uint32_t *n_bvh_nodes);
+
+void cr_scene_destroy(cr_scene *s);
+
+/* The 1024-point table of light `light` (mesh lights only; Mesh::samples,
+ * src/core/primitive/mesh.hpp:58-84): out = 1024 x {p.xyz, n.xyz}; *pdf the
+ * table's area pdf. */
+int cr_light_table(const cr_scene *s, uint32_t light, float *out, float *pdf);
+
+/* ------------------------------------------------------------- ray queries */
+/* Scene::intersect(Ray, ...) (src/core/meta/scene.hpp:35-55) when any_hit = 0,
+ * Scene::intersect(Seg, ...) (scene.hpp:57-67) when any_hit = 1, batched.
+ * rays: n x {o.x,o.y,o.z, d.x,d.y,d.z, tmax} floats (tmax <= 0 or inf: none).
+ * Host buffers; copies are part of the call. */
+int cr_trace_rays(cr_scene *s, const float *rays, uint64_t n, cr_hit *hits, int any_hit);
+
+/* Same on device buffers, asynchronous on `stream`. */
+int cr_trace_rays_device(cr_scene *s, const float *d_rays, uint64_t n, cr_hit *d_hits, int any_hit,
+                         void *stream);
+
+/* --------------------------------------------------------------- rendering */
+/* Tracer::execute (src/core/tracer/tracer.hpp:20-21) with the Radiance
+ * kernel (RadianceKernel::execute, src/core/kernel/radiance.cu:14-81) for
+ * every pixel and sample, as CPUMulticoreTracer::execute
+ * (src/core/tracer/cpuMulticore.cu:14-122) does on the CPU: per pixel the
+ * mean of its finite samples.  film_rgb: host, window-sized W x H x 3
+ * doubles (row-major, y down).  Blocks until the film is on the host. */
+int cr_render(cr_scene *s, const cr_render_desc *desc, double *film_rgb, cr_stats *stats);
+
+/* Device variant: accumulates into caller device buffers sized for the
+ * window (sum and sum of squares W x H x 3 doubles, count W x H uint32),
+ * asynchronous on `stream`; the library allocates its wave buffers. */
+int cr_render_device(cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sumsq,
+                     uint32_t *d_count, void *stream, cr_stats *stats);
+
+/* Renderer::render (src/core/renderer/renderer.cu:13-52): load a scene file,
+ * render it with the configured kernel and tracer, write the reference's
+ * clamped 8-bit PNG (src/util/image.cu:15-18) and, when pfm_path is not
+ * NULL, a linear float PFM. */
+int cr_render_file(const char *json_path, const char *png_path, const char *pfm_path, uint32_t spp,
+                   uint32_t width, uint32_t height, const char *kernel, const char *tracer);
+
+/* 8-bit PNG of linear radiance clamped to [0,1] as util::Image<3> stores it
+ * (src/util/image.hpp:16-49). */
+int cr_write_png(const char *path, uint32_t width, uint32_t height, const double *rgb);
+
+/* ----------------------------------------------------- BSDF parity helpers */
+/* Shader::execute(compute_f_by_wi_wo) (src/core/nodes/shader.hpp:17-23) for n
+ * local-frame direction pairs, evaluated by the CUDA path's device code.
+ * f: n x 3, pdf: n (0 for CR_ESTIMATOR_KOISHI, which has no pdf). */
+int cr_bsdf_eval(int estimator, const char *shader_json, const float *wo, const float *wi, uint64_t n,
+                 float *f, float *pdf);
+/* Shader::execute(sample_wi_f_by_wo) for n outgoing directions and uniforms
+ * u (n x 2): wi (n x 3), weight = f*|cos|/pdf (n x 3), pdf (n). */
+int cr_bsdf_sample(int estimator, const char *shader_json, const float *wo, const float *u, uint64_t n,
+                   float *wi, float *weight, float *pdf);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CR_H */

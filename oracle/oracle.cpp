@@ -513,6 +513,7 @@ void m_sample( const Shader &sh, V3 wo, double u1, double u2, V3 &wi, V3 &weight
 	{
 		V3 h = beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
 		wi = reflect( wo, h );
+		if ( wo.z <= 0 || wi.z <= 0 || dot( wo, h ) <= 0 ) return;
 	}
 	else
 		wi = sample_cos( u1, u2 );
@@ -653,7 +654,7 @@ void mis_light_sample( const orc_scene *s, const Light &lt, double u0, double u1
 	pdfA = 1.0 / lt.area;
 }
 
-V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
+V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng, int variant = 0 )
 {
 	V3 L, beta( 1, 1, 1 );
 	size_t nl = s->lights.size();
@@ -678,7 +679,8 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
 		if ( sh.type == ORC_EMISSION )
 		{
 			double w = 1;
-			if ( bounce > 0 )
+			if ( bounce > 0 && variant == 3 ) w = 0;
+			if ( bounce > 0 && variant == 0 )
 			{
 				const Light &lt = s->lights[ pr.light ];
 				double cosl = std::fabs( dot( ng, d ) );
@@ -689,12 +691,13 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
 			}
 			L = L + beta * sh.emission * w;
 		}
-		if ( dot( ng, d ) > 0 ) ng = -ng, ns = -ns;
+		if ( dot( ng, d ) > 0 ) ng = -ng;
+		if ( dot( ns, ng ) < 0 ) ns = -ns;
 		Frame fr;
 		fr.n = ns;
 		onb( ns, fr.u, fr.v );
 		V3 wo = fr.local( -d );
-		if ( nl )
+		if ( nl && variant != 2 )
 		{
 			double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
 			size_t idx = std::min( size_t( std::floor( u0 * double( nl ) ) ), nl - 1 );
@@ -717,7 +720,7 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
 				if ( ( f.x > 0 || f.y > 0 || f.z > 0 ) && dot( wiw, ng ) > 0 &&
 					 !occluded_ray( s, p, wiw, 1e-7 * s->scale, dist * ( 1 - 1e-4 ) ) )
 				{
-					double w = pl * pl / ( pl * pl + pb * pb );
+					double w = variant == 3 ? 1.0 : pl * pl / ( pl * pl + pb * pb );
 					L = L + beta * f * s->shaders[ s->prims[ lt.prim ].shader ].emission * ( wi.z * w / pl );
 				}
 			}
@@ -1037,8 +1040,8 @@ int orc_render( const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32
 				{
 					Rng rng( seed, uint64_t( y ) * W + x, k );
 					V3 d = lens.dir( x, y, k );
-					V3 L = estimator == ORC_MIS ? radiance_mis( s, s->cam.pos, d, max_bounce, rng )
-												: radiance_koishi( s, s->cam.pos, d, max_bounce, rng );
+					V3 L = estimator == ORC_KOISHI ? radiance_koishi( s, s->cam.pos, d, max_bounce, rng )
+												   : radiance_mis( s, s->cam.pos, d, max_bounce, rng, estimator == ORC_MIS ? 0 : estimator );
 					if ( !finite3( L ) ) continue;  // cpuMulticore.cu:58-64
 					++c;
 					for ( int ch = 0; ch < 3; ++ch ) a[ ch ] += L[ ch ], q[ ch ] += L[ ch ] * L[ ch ];

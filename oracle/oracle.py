@@ -92,7 +92,8 @@ class OracleScene:
         def sid(name):
             if name not in ids:
                 t, p = shader_params(desc.shaders[name])
-                ids[name] = L.orc_add_shader(self.h, t, _p(np.asarray(p, np.float64)))
+                params = np.asarray(p, np.float64)  # bound: ctypes keeps only the address
+                ids[name] = L.orc_add_shader(self.h, t, _p(params))
             return ids[name]
 
         self.prim_kind = []
@@ -104,12 +105,14 @@ class OracleScene:
             assert r >= 0
             self.prim_kind.append(0)
         for s in desc.spheres:
-            L.orc_add_sphere(self.h, _p(np.asarray(s["o"], np.float32)), float(s["r"]), sid(s["shader"]))
+            c = np.asarray(s["o"], np.float32)
+            L.orc_add_sphere(self.h, _p(c), float(s["r"]), sid(s["shader"]))
             self.prim_kind.append(1)
         cam = desc.camera
-        L.orc_set_camera(self.h, _p(np.asarray(cam["position"], np.float32)),
-                         _p(np.asarray(cam["target"], np.float32)),
-                         _p(np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)), float(cam.get("fovx", 90)))
+        pos = np.asarray(cam["position"], np.float32)
+        tgt = np.asarray(cam["target"], np.float32)
+        up = np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)
+        L.orc_set_camera(self.h, _p(pos), _p(tgt), _p(up), float(cam.get("fovx", 90)))
         L.orc_finalize(self.h, light_seed)
 
     def __del__(self):
@@ -165,27 +168,28 @@ def bsdf_eval(estimator, cfg, wo, wi):
     t, p = shader_params(cfg)
     f = np.zeros(3)
     pdf = np.zeros(1)
-    lib().orc_bsdf_eval(estimator, t, _p(np.asarray(p, np.float64)), _p(np.asarray(wo, np.float64)),
-                        _p(np.asarray(wi, np.float64)), _p(f), _p(pdf))
+    params, a, b = (np.asarray(x, np.float64) for x in (p, wo, wi))
+    lib().orc_bsdf_eval(estimator, t, _p(params), _p(a), _p(b), _p(f), _p(pdf))
     return f, float(pdf[0])
 
 
 def bsdf_sample(estimator, cfg, wo, u):
     t, p = shader_params(cfg)
     wi, w, pdf = np.zeros(3), np.zeros(3), np.zeros(1)
-    lib().orc_bsdf_sample(estimator, t, _p(np.asarray(p, np.float64)), _p(np.asarray(wo, np.float64)),
-                          _p(np.asarray(u, np.float64)), _p(wi), _p(w), _p(pdf))
+    params, a, b = (np.asarray(x, np.float64) for x in (p, wo, u))
+    lib().orc_bsdf_sample(estimator, t, _p(params), _p(a), _p(b), _p(wi), _p(w), _p(pdf))
     return wi, w, float(pdf[0])
 
 
 def seg_box(seg7, bmin, bmax):
-    return bool(lib().orc_seg_box(_p(np.asarray(seg7, np.float32)), _p(np.asarray(bmin, np.float32)),
-                                  _p(np.asarray(bmax, np.float32))))
+    a, b, c = (np.asarray(x, np.float32) for x in (seg7, bmin, bmax))
+    return bool(lib().orc_seg_box(_p(a), _p(b), _p(c)))
 
 
 def sphere_hit(center, r, ray6):
     t = np.zeros(1)
-    h = lib().orc_sphere_hit(_p(np.asarray(center, np.float32)), float(r), _p(np.asarray(ray6, np.float32)), _p(t))
+    c, ray = np.asarray(center, np.float32), np.asarray(ray6, np.float32)
+    h = lib().orc_sphere_hit(_p(c), float(r), _p(ray), _p(t))
     return bool(h), float(t[0])
 
 

@@ -22,8 +22,8 @@
 //       Scene::intersect(Seg) (src/core/meta/scene.hpp:57-67) per segment.
 //   lights <scene.json> <out.lights>
 //       the 1024-point tables of every emissive mesh (src/core/primitive/mesh.hpp:61-84).
-//   bench  <scene.json> <W> <H> <spp> <threads> [maxBounce]
-//       wall time of the reference's own CPUMulticoreTracer::execute.
+//   bench  <scene.json> <W> <H> <spp> <threads> [maxBounce] [repeats]
+//       wall time of the reference's own CPUMulticoreTracer::execute, once per repeat.
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -453,11 +453,15 @@ int cmd_bench( int argc, char **argv )
 	Properties pp;
 	pp[ "enable" ] = false;
 	Profiler profiler( pp, tracer->getKernel(), W, H, spp );
-	auto t0 = std::chrono::steady_clock::now();
-	tracer->execute( image, lens, gen, *L.scene, spp, profiler );
-	double sec = std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count();
-	std::fprintf( stderr, "{\"seconds\": %.6f, \"samples\": %llu, \"threads\": %u}\n", sec,
-				  (unsigned long long)W * H * spp, nth );
+	int repeats = argc > 8 ? std::stoi( argv[ 8 ] ) : 1;
+	for ( int r = 0; r < repeats; ++r )
+	{
+		auto t0 = std::chrono::steady_clock::now();
+		tracer->execute( image, lens, gen, *L.scene, spp, profiler );
+		double sec = std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count();
+		std::fprintf( stderr, "{\"seconds\": %.6f, \"samples\": %llu, \"threads\": %u}\n", sec,
+					  (unsigned long long)W * H * spp, nth );
+	}
 	return 0;
 }
 

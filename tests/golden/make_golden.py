@@ -1,0 +1,141 @@
+"""Regenerates the golden fixtures in this folder from the reference itself.
+
+Runs oracle/_ref/cr_ref (the reference's own CPU Radiance path compiled from
+its sources by `make -C oracle ref`, with the harness in
+oracle/ref_harness/) on seeded scenes from the package's scene generator, and
+stores its answers:
+
+  c0_lights.npz    the 1024-point light table and pdf of config 0's light
+                   (Mesh::generateSamples, src/core/primitive/mesh.hpp:61-84)
+  c0_trace.npz     closest hits of primary + random rays (Scene::intersect)
+  ico_trace.npz    same on a displaced level-4 icosphere in the box
+  c0_occlude.npz   segment occlusion (Scene::intersect(Seg))
+  c0_film.npz      per-pixel sums / sums of squares / counts of a Radiance
+                   render (RadianceKernel::execute through the harness)
+
+Usage:  python tests/golden/make_golden.py
+"""
+import hashlib
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from conftest import load_package  # noqa: E402
+
+load_package()
+from cuda_raytracer_b200 import scenes  # noqa: E402
+import oracle  # noqa: E402
+
+FILM_W, FILM_H, FILM_SPP = 48, 48, 1024
+
+
+def scene_hash(desc):
+    h = hashlib.sha256()
+    for g in desc.groups:
+        h.update(g.name.encode())
+        h.update(np.ascontiguousarray(g.v).tobytes())
+        h.update(np.ascontiguousarray(g.n).tobytes())
+        h.update(np.ascontiguousarray(g.f).tobytes())
+    for s in desc.spheres:
+        h.update(repr(s).encode())
+    return h.hexdigest()
+
+
+def ico_scene():
+    """Box + light + displaced level-4 icosphere (5120 triangles, 20 patch materials)."""
+    return scenes.config1(level=4, seed=11, width=64, height=48, spp=4)
+
+
+def make_rays(desc, n_random, seed):
+    """Primary rays (PinholeLens::sample) plus rays from random interior points."""
+    rng = np.random.default_rng(seed)
+    w, h, spp = 32, 24, 4
+    px = np.stack(np.meshgrid(np.arange(w), np.arange(h)), -1).reshape(-1, 2)
+    px = np.repeat(px, 2, axis=0)
+    ks = np.tile([0, 3], len(px) // 2)
+    o, d = scenes.pinhole_rays(desc.camera, w, h, spp, px, ks)
+    lo = np.array([0.2, scenes.FRONT + 0.2, 0.2])
+    hi = np.array([scenes.S - 0.2, scenes.S - 0.2, scenes.S - 0.2])
+    ro = scenes._rot_points(lo + (hi - lo) * rng.random((n_random, 3))).astype(np.float32)
+    rd = rng.normal(size=(n_random, 3))
+    rd = (rd / np.linalg.norm(rd, axis=1, keepdims=True)).astype(np.float32)
+    rays = np.zeros((len(o) + n_random, 7), np.float32)
+    rays[:len(o), :3], rays[:len(o), 3:6] = o, d
+    rays[len(o):, :3], rays[len(o):, 3:6] = ro, rd
+    rays[:, 6] = np.inf
+    return rays
+
+
+def make_segments(desc, n, seed):
+    rng = np.random.default_rng(seed)
+    lo = np.array([0.2, scenes.FRONT + 0.2, 0.2])
+    hi = np.array([scenes.S - 0.2, scenes.S - 0.2, scenes.S - 0.2])
+    a = scenes._rot_points(lo + (hi - lo) * rng.random((n, 3)))
+    b = scenes._rot_points(lo + (hi - lo) * rng.random((n, 3)))
+    d = b - a
+    ln = np.linalg.norm(d, axis=1)
+    segs = np.zeros((n, 7), np.float32)
+    segs[:, :3] = a
+    segs[:, 3:6] = d / ln[:, None]
+    segs[:, 6] = ln
+    return segs
+
+
+def run(*args, cwd):
+    return subprocess.run([oracle.REF_BIN, *map(str, args)], cwd=cwd, check=True, capture_output=True, text=True)
+
+
+def main():
+    if not oracle.ref_available():
+        sys.exit("build the reference harness first: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        c0 = scenes.config0()
+        scenes.write_scene(c0, tmp)
+        js = f"{c0.name}.json"
+
+        run("lights", js, "lights.bin", oracle.LIGHT_SEED, cwd=tmp)
+        raw = open(os.path.join(tmp, "lights.bin"), "rb").read()
+        n = np.frombuffer(raw, "<u4", 1, 0)[0]
+        assert n == 1
+        group, = np.frombuffer(raw, "<i4", 1, 4)
+        pdf, = np.frombuffer(raw, "<f4", 1, 8)
+        nf, = np.frombuffer(raw, "<u4", 1, 12)
+        table = np.frombuffer(raw, "<f4", 1024 * 6, 16).reshape(1024, 6)
+        np.savez_compressed(os.path.join(HERE, "c0_lights.npz"), table=table, pdf=pdf, group=group, n_faces=nf,
+                            seed=oracle.LIGHT_SEED, scene_hash=scene_hash(c0))
+
+        for name, desc, nrand, seed in (("c0_trace.npz", c0, 2048, 5), ("ico_trace.npz", ico_scene(), 4096, 6)):
+            scenes.write_scene(desc, tmp)
+            rays = make_rays(desc, nrand, seed)
+            rays.tofile(os.path.join(tmp, "rays.f32"))
+            run("trace", f"{desc.name}.json", "rays.f32", "hits.bin", cwd=tmp)
+            hits = np.fromfile(os.path.join(tmp, "hits.bin"), "<i4").reshape(-1, 4)
+            np.savez_compressed(os.path.join(HERE, name), rays=rays, kind=hits[:, 0], index=hits[:, 1],
+                                tri=hits[:, 2], t=hits[:, 3].view(np.float32), scene_hash=scene_hash(desc))
+
+        segs = make_segments(c0, 4096, 7)
+        segs.tofile(os.path.join(tmp, "segs.f32"))
+        run("occlude", js, "segs.f32", "occ.bin", cwd=tmp)
+        occ = np.fromfile(os.path.join(tmp, "occ.bin"), np.uint8)
+        np.savez_compressed(os.path.join(HERE, "c0_occlude.npz"), segs=segs, occluded=occ,
+                            scene_hash=scene_hash(c0))
+
+        run("render", js, FILM_W, FILM_H, FILM_SPP, os.cpu_count(), "film.crf", c0.max_bounce, 17, cwd=tmp)
+        film = oracle.read_crf(os.path.join(tmp, "film.crf"))
+        np.savez_compressed(os.path.join(HERE, "c0_film.npz"), sum=film.sum, sumsq=film.sumsq, count=film.count,
+                            width=FILM_W, height=FILM_H, spp=FILM_SPP, max_bounce=c0.max_bounce,
+                            scene_hash=scene_hash(c0))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

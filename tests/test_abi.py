@@ -1,0 +1,116 @@
+"""The C-ABI library: it loads, exports every entry point include/cr.h
+declares, and rejects bad input on the host without touching a GPU."""
+import ctypes as C
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "cr.h")).read()
+    return sorted(set(re.findall(r"\b(cr_[a-z_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_symbols()
+    for must in ("cr_scene_create", "cr_trace_rays", "cr_render", "cr_render_device", "cr_last_error",
+                 "cr_scene_destroy", "cr_render_file", "cr_bsdf_eval", "cr_bsdf_sample", "cr_light_table"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(cr):
+    lib = cr.lib()
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_error_strings(cr):
+    assert b"sm_100a" in cr.lib().cr_version()
+    assert isinstance(cr.lib().cr_last_error(), bytes)
+
+
+def _empty(cr):
+    h = C.c_void_p()
+    assert cr.lib().cr_scene_create_empty(C.byref(h)) == cr.CR_OK
+    return h
+
+
+def test_shader_registry_and_errors(cr):
+    lib = cr.lib()
+    h = _empty(cr)
+    try:
+        ok = lib.cr_scene_add_shader(h, b"w", json.dumps(["Lambert", {"R": [0.5, 0.5, 0.5]}]).encode())
+        assert ok == 0
+        ok = lib.cr_scene_add_shader(h, b"g", json.dumps(
+            ["GlossyBSDF", {"distribution": ["Beckmann", {"roughness": 0.3}], "color": [1, 1, 1]}]).encode())
+        assert ok == 1
+        assert lib.cr_scene_add_shader(h, b"e", b'["Emission", {"strength": 5}]') == 2
+        # malformed JSON, unknown type, out-of-scope type
+        assert lib.cr_scene_add_shader(h, b"x", b'["Lambert", {') == -2
+        assert b"json" in lib.cr_last_error()
+        assert lib.cr_scene_add_shader(h, b"x", b'["NoSuchShader", {}]') == -2
+        assert b"no such type" in lib.cr_last_error()
+        assert lib.cr_scene_add_shader(h, b"x", b'["GlassBSDF", {}]') == -5
+        assert lib.cr_scene_add_shader(h, b"x", b'["GlossyBSDF", {"distribution": ["Cosine", {}]}]') == -5
+    finally:
+        lib.cr_scene_destroy(h)
+
+
+def test_mesh_validation(cr):
+    lib = cr.lib()
+    h = _empty(cr)
+    try:
+        lib.cr_scene_add_shader(h, b"w", b'["Lambert", {}]')
+        v = np.zeros((3, 3), np.float32)
+        v[1, 0] = v[2, 1] = 1
+        good = np.array([[0, 1, 2]], np.uint32)
+        bad = np.array([[0, 1, 3]], np.uint32)
+        p = lambda a: C.c_void_p(a.ctypes.data)
+        assert lib.cr_scene_add_mesh(h, p(v), 3, None, p(bad), 1, b"w") == -1
+        assert b"out of range" in lib.cr_last_error()
+        assert lib.cr_scene_add_mesh(h, p(v), 3, None, p(good), 1, b"missing") == -1
+        assert b"not found" in lib.cr_last_error()
+        nanv = v.copy()
+        nanv[0, 0] = np.nan
+        assert lib.cr_scene_add_mesh(h, p(nanv), 3, None, p(good), 1, b"w") == -1
+        assert lib.cr_scene_add_mesh(h, p(v), 3, None, p(good), 1, b"w") == 0
+        c = np.zeros(3, np.float32)
+        assert lib.cr_scene_add_sphere(h, p(c), -1.0, b"w") == -1
+        assert lib.cr_scene_add_sphere(h, p(c), 1.0, b"w") == 1
+        # not committed yet: queries are refused with a state error
+        hits = np.zeros(1, cr.HIT_DTYPE)
+        rays = np.zeros((1, 7), np.float32)
+        assert lib.cr_trace_rays(h, p(rays), 1, p(hits), 0) == -4
+        desc = cr.render_desc(8, 8, 1)
+        film = np.zeros((8, 8, 3))
+        assert lib.cr_render(h, C.byref(desc), p(film), None) == -4
+    finally:
+        lib.cr_scene_destroy(h)
+
+
+def test_null_arguments(cr):
+    lib = cr.lib()
+    assert lib.cr_scene_create(None, None, None) == -1
+    assert lib.cr_scene_create_empty(None) == -1
+    assert lib.cr_write_png(None, 1, 1, None) == -1
+
+
+def test_png_writer(cr, tmp_path):
+    rgb = np.zeros((4, 5, 3))
+    rgb[..., 0] = np.linspace(-1, 2, 5)[None, :]
+    path = str(tmp_path / "x.png")
+    assert cr.lib().cr_write_png(path.encode(), 5, 4, C.c_void_p(rgb.ctypes.data)) == 0
+    data = open(path, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    import zlib
+    # IHDR then IDAT: decode the stored deflate stream and check clamping (image.hpp:29-40)
+    i = data.index(b"IDAT")
+    n = int.from_bytes(data[i - 4:i], "big")
+    raw = zlib.decompress(data[i + 4:i + 4 + n])
+    row = np.frombuffer(raw[1:16], np.uint8).reshape(5, 3)
+    assert list(row[:, 0]) == [0, 0, 127, 255, 255]

@@ -1,0 +1,115 @@
+"""CUDA Radiance renders against the reference's own render (reference
+estimator) and against the FP64 oracle (MIS estimator): per pixel within 3
+sigma of the combined Monte Carlo standard error."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden, require_gpu
+from gpu_util import render_film, zscores
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    require_gpu()
+
+
+@pytest.fixture(scope="module")
+def c0_scene(cr, scenes):
+    return cr.Scene.from_desc(scenes.config0())
+
+
+def test_light_table_matches_reference(c0_scene):
+    g = golden("c0_lights.npz")
+    table, pdf = c0_scene.light_table(0)
+    np.testing.assert_allclose(table, g["table"], rtol=0, atol=2e-6)
+    assert abs(pdf - float(g["pdf"])) <= 1e-7 * pdf
+
+
+def _blocks(film, k=4):
+    """k x k pixel blocks: block means and their standard errors."""
+    H, W = film.count.shape
+    sh = (H // k, k, W // k, k, 3)
+    m = film.mean[:H // k * k, :W // k * k].reshape(sh).mean(axis=(1, 3))
+    v = film.var_of_mean[:H // k * k, :W // k * k].reshape(sh).sum(axis=(1, 3)) / k ** 4
+    return m, v
+
+
+def test_koishi_render_matches_reference(cr, c0_scene):
+    """Per pixel, at the reference's own sample count (1024 per pixel on the
+    same stratified camera rays), within 3 sigma of the combined standard
+    error; then 4x the samples against the reference in 4x4-pixel blocks."""
+    g = golden("c0_film.npz")
+    W, H, spp, mb = int(g["width"]), int(g["height"]), int(g["spp"]), int(g["max_bounce"])
+    ref = O.Film(g["sum"], g["sumsq"], g["count"])
+    f1 = render_film(cr, c0_scene, W, H, spp, seeds=[1], estimator=cr.KOISHI, max_bounce=mb)
+    assert np.all(f1.count == spp)
+    z = zscores(f1, ref)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert z.max() < 5.5
+    f4 = render_film(cr, c0_scene, W, H, spp, seeds=[1, 2, 3, 4], estimator=cr.KOISHI, max_bounce=mb)
+    (ma, va), (mb_, vb) = _blocks(f4), _blocks(ref)
+    zb = np.abs(ma - mb_) / np.sqrt(va + vb)
+    assert (zb > 3).mean() < 0.02 and zb.max() < 5.5, ((zb > 3).mean(), zb.max())
+    assert abs(f4.mean.mean() / ref.mean.mean() - 1) < 0.01
+
+
+def test_mis_render_matches_oracle(cr, scenes, c0_scene):
+    d = scenes.config0()
+    W, H, spp = 32, 32, 256
+    o = O.OracleScene(d).render(W, H, spp, 7, O.MIS, seed=5)
+    f = render_film(cr, c0_scene, W, H, spp, seeds=[11, 12], estimator=cr.MIS)
+    z = zscores(f, o)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert z.max() < 5.5
+    assert abs(f.mean.mean() / o.mean.mean() - 1) < 0.01
+
+
+def test_koishi_mesh_scene_matches_oracle(cr, scenes):
+    d = scenes.config1(level=5)
+    W, H, spp = 32, 24, 256
+    o = O.OracleScene(d).render(W, H, spp, 7, O.KOISHI, seed=5)
+    f = render_film(cr, cr.Scene.from_desc(d), W, H, spp, seeds=[3], estimator=cr.KOISHI)
+    z = zscores(f, o)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert z.max() < 5.5
+
+
+def test_deterministic_and_wave_invariant(cr, c0_scene):
+    a = render_film(cr, c0_scene, 24, 24, 16, seeds=[9])
+    b = render_film(cr, c0_scene, 24, 24, 16, seeds=[9])
+    c = render_film(cr, c0_scene, 24, 24, 16, seeds=[9], wave_paths=1000)
+    assert np.array_equal(a.sum, b.sum) and np.array_equal(a.sum, c.sum)
+    assert np.array_equal(a.count, c.count)
+
+
+def test_window_equals_crop(cr, c0_scene):
+    full = render_film(cr, c0_scene, 24, 24, 16, seeds=[4])
+    win = render_film(cr, c0_scene, 24, 24, 16, seeds=[4], window=(5, 7, 19, 20))
+    assert np.array_equal(win.sum, full.sum[7:20, 5:19])
+
+
+def test_host_render_mean(cr, c0_scene):
+    film, st = c0_scene.render(24, 24, 16, seed=9, max_bounce=7, estimator=cr.KOISHI)
+    ref = render_film(cr, c0_scene, 24, 24, 16, seeds=[9])
+    np.testing.assert_allclose(film, ref.mean, rtol=1e-12)
+    assert st.samples == 24 * 24 * 16 and st.rays_extend > st.samples
+
+
+def test_nan_frame_samples_dropped_like_reference(cr, scenes):
+    """A flat face whose normal is exactly +y makes the reference's frame NaN
+    (scene.hpp:48-50); those samples are dropped (cpuMulticore.cu:58-64) in
+    the reference estimator and kept in the MIS estimator."""
+    d = scenes.config0()
+    g = scenes.Group("floorY", np.array([[0, 3, -5], [10, 3, -5], [10, 3, 10], [0, 3, 10]], np.float32),
+                     np.tile(np.array([[0, 1, 0]], np.float32), (4, 1)), np.array([[0, 1, 2], [0, 2, 3]], np.uint32))
+    d.groups = [g] + d.groups
+    d.shaders["floorY"] = ["Lambert", {"R": [0.5, 0.5, 0.5]}]
+    d.camera = {"lens": "pinhole", "fovx": 60.0, "position": [2.0, 0.0, 2.0], "target": [0.0, 1.0, 0.0],
+                "upaxis": [0.0, 0.0, 1.0]}
+    s = cr.Scene.from_desc(d)
+    k = render_film(cr, s, 16, 16, 4, seeds=[1], estimator=cr.KOISHI)
+    m = render_film(cr, s, 16, 16, 4, seeds=[1], estimator=cr.MIS)
+    assert k.count.min() == 0 and m.count.min() == 4
