@@ -316,7 +316,10 @@ def run_ours(args):
             "stage_ms_per_step": {k: round(totals[k] / args.steps, 3) for k in ("extend", "shadow", "shade", "other")},
             "roofline": {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                         "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                         "traffic": (round(traffic["dram_bytes_per_ray"] * cst.rays_extend / max(cst.extend_launches, 1))
+                                     if traffic else None),
+                         "traffic_note": ("ncu DRAM bytes per ray of a captured launch (profiles/k_extend_traffic.json) "
+                                          "scaled to this run's rays per launch") if traffic else None,
                          "algorithmic_bytes_per_launch": round(ext_launch_bytes),
                          "launch_ms": round(ext_launch_ms, 4),
                          "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
