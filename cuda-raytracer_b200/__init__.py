@@ -88,6 +88,7 @@ def lib():
             "cr_trace_rays_device": (I, [P, P, U64, P, I, P]),
             "cr_render": (I, [P, P, P, P]),
             "cr_render_device": (I, [P, P, P, P, P, P, P]),
+            "cr_render_device_noalloc": (I, [P, P, P, P, P, P]),
             "cr_render_file": (I, [C.c_char_p, C.c_char_p, C.c_char_p, U32, U32, U32, C.c_char_p, C.c_char_p]),
             "cr_write_png": (I, [C.c_char_p, U32, U32, P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),

@@ -21,6 +21,7 @@
 
 #include "../../include/cr.h"
 #include "bvh_build.h"
+#include "internal.h"
 #include "json.h"
 #include "render.h"
 
@@ -1035,6 +1036,20 @@ std::string dir_of( const std::string &p )
 }
 
 }  // namespace
+
+// ====================================================================== internal helpers
+int cr::prepare_render( cr_scene *s, const cr_render_desc *desc, DevScene &sc, RenderConfig &cfg, std::string &err )
+{
+	int rc = guarded( [&] {
+		Resolved r = resolve( s, desc );
+		sc = r.sc;
+		cfg = r.cfg;
+	} );
+	if ( rc != CR_OK ) err = g_last_error;
+	return rc;
+}
+
+void cr::set_last_error( const std::string &msg ) { g_last_error = msg; }
 
 // ====================================================================== C ABI
 extern "C" {

@@ -161,6 +161,28 @@ int cr_render(cr_scene *s, const cr_render_desc *desc, double *film_rgb, cr_stat
 int cr_render_device(cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sumsq,
                      uint32_t *d_count, void *stream, cr_stats *stats);
 
+/* No counterpart in the reference.  Same render as cr_render_device, for
+ * callers that cannot allocate device memory while they render (a frame
+ * callback or real-time loop where cudaMalloc/cudaFree would synchronise the
+ * device, or an application that budgets all device memory at start-up).
+ * The call allocates nothing: the per-path wave state lives in one fixed
+ * device array inside the library, held by every GPU that loads it until the
+ * process exits (CR_NOALLOC_MAX_WAVE_PATHS paths, about 37 MB).  The scene
+ * must already be committed; the caller passes the film buffers as for
+ * cr_render_device.  desc->wave_paths above CR_NOALLOC_MAX_WAVE_PATHS, or a
+ * max_bounce above CR_NOALLOC_MAX_BOUNCE, is rejected with CR_ERR_INVALID
+ * (wave_paths 0 means the maximum).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  Every call on a device
+ * shares the one array, so calls whose work overlaps on the GPU (concurrent
+ * streams, or host threads sharing a device) race and corrupt each other's
+ * films; serialise them.  The call is asynchronous on `stream` and does not
+ * read back the kernels' error word; stats are not collected. */
+#define CR_NOALLOC_MAX_WAVE_PATHS 262144u
+#define CR_NOALLOC_MAX_BOUNCE 64u
+int cr_render_device_noalloc(cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sumsq,
+                             uint32_t *d_count, void *stream);
+
 /* Renderer::render (src/core/renderer/renderer.cu:13-52): load a scene file,
  * render it with the configured kernel and tracer, write the reference's
  * clamped 8-bit PNG (src/util/image.cu:15-18) and, when pfm_path is not

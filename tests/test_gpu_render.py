@@ -81,7 +81,9 @@ def test_deterministic_and_wave_invariant(cr, c0_scene):
     a = render_film(cr, c0_scene, 24, 24, 16, seeds=[9])
     b = render_film(cr, c0_scene, 24, 24, 16, seeds=[9])
     c = render_film(cr, c0_scene, 24, 24, 16, seeds=[9], wave_paths=1000)
-    assert np.array_equal(a.sum, b.sum) and np.array_equal(a.sum, c.sum)
+    assert np.array_equal(a.sum, b.sum)
+    # Waves that split a pixel add its samples in two FP64 partial sums.
+    np.testing.assert_allclose(c.sum, a.sum, rtol=1e-12, atol=0)
     assert np.array_equal(a.count, c.count)
 
 
