@@ -216,6 +216,13 @@ def run_ours(args):
         return scene.render_device(d, s.data_ptr(), q.data_ptr(), c.data_ptr(), stream=stream.cuda_stream,
                                    stats=stats)
 
+    # launch configuration: autotuned on a sample band of the image (untimed)
+    tuning = None
+    if not args.no_autotune:
+        td = cr.render_desc(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=99)
+        tuning = scene.autotune(td, stream=stream.cuda_stream).as_dict()
+        torch.cuda.synchronize(dev)
+
     # warm-up
     for w in range(args.warmup):
         step(1000 + w)
@@ -280,8 +287,8 @@ def run_ours(args):
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
             sc2 = cr.Scene.from_desc(desc)
-            film, _ = sc2.render(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k,
-                                 wave_paths=args.wave_paths)
+            tk = {k2: tuning[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm")} if tuning else {}
+            film, _ = sc2.render(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k, **tk)
             sc2.close()
             times.append(time.perf_counter() - t0)
             assert np.isfinite(film).all()
@@ -311,7 +318,7 @@ def run_ours(args):
             "config": {"workload": "config1: 1024x768x256spp, 1.31M-tri displaced icosphere in the box, depth 8",
                        "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"], "spp": spp,
                        "estimator": "reference (koishi)", "l2": "flushed between timed steps (256 MB write)",
-                       "parallelism": f"replica-per-gpu x{world}"},
+                       "parallelism": f"replica-per-gpu x{world}", "autotuned": tuning},
             "mrays_per_s": round((totals["rays_extend"] + totals["rays_shadow"]) * world / (ms_max / 1e3) / 1e6, 2),
             "stage_ms_per_step": {k: round(totals[k] / args.steps, 3) for k in ("extend", "shadow", "shade", "other")},
             "roofline": {"bound": "hbm", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": peak,
@@ -345,6 +352,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-spp", type=int, default=4, help="spp of the reference's bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

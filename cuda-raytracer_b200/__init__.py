@@ -47,7 +47,16 @@ class RenderDesc(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_bounce", C.c_uint32),
                 ("estimator", C.c_int32), ("x0", C.c_uint32), ("y0", C.c_uint32), ("x1", C.c_uint32),
                 ("y1", C.c_uint32), ("seed", C.c_uint64), ("wave_paths", C.c_uint32), ("guiding", C.c_int32),
-                ("count_work", C.c_int32)]
+                ("count_work", C.c_int32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("wave_paths", C.c_uint32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32),
+                ("candidates_tried", C.c_uint32), ("msamples_per_s", C.c_double),
+                ("default_msamples_per_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Stats(C.Structure):
@@ -91,6 +100,7 @@ def lib():
             "cr_render_device_noalloc": (I, [P, P, P, P, P, P]),
             "cr_render_file": (I, [C.c_char_p, C.c_char_p, C.c_char_p, U32, U32, U32, C.c_char_p, C.c_char_p]),
             "cr_write_png": (I, [C.c_char_p, U32, U32, P]),
+            "cr_autotune": (I, [P, P, P, P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
         }
@@ -113,7 +123,7 @@ def _p(a):
 
 
 def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, window=None, wave_paths=0,
-                guiding=False, count_work=False):
+                guiding=False, count_work=False, refill_min=0, traverse_blocks_per_sm=0):
     d = RenderDesc()
     d.width, d.height, d.spp = width, height, spp
     d.max_bounce = U32_MAX if max_bounce is None else max_bounce
@@ -124,6 +134,8 @@ def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, win
     d.wave_paths = wave_paths
     d.guiding = int(bool(guiding))
     d.count_work = int(bool(count_work))
+    d.refill_min = refill_min
+    d.traverse_blocks_per_sm = traverse_blocks_per_sm
     return d
 
 
@@ -215,6 +227,12 @@ class Scene:
         st = Stats()
         _check(lib().cr_render(self.h, C.byref(d), _p(film), C.byref(st)))
         return film, st
+
+    def autotune(self, desc, stream=0):
+        """cr_autotune: pick and keep the launch configuration for this scene."""
+        t = Tuning()
+        _check(lib().cr_autotune(self.h, C.byref(desc), C.c_void_p(stream), C.byref(t)))
+        return t
 
     def render_device(self, desc, sum_ptr, sumsq_ptr, count_ptr, stream=0, stats=True):
         st = Stats() if stats else None

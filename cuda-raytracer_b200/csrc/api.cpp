@@ -153,6 +153,9 @@ struct cr_scene
 	float scale = 1;
 	WaveBuffers wave;
 	uint32_t wave_bounces = 0;
+	// launch configuration (defaults, or the choice of cr_autotune)
+	uint32_t tune_wave = 1u << 22, tune_refill = 16;
+	int tune_blocks = 8;
 
 	~cr_scene() { release(); }
 	void release_device()
@@ -784,7 +787,7 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	s->light_tris.upload( ltris );
 	s->light_cdf.upload( cdf );
 	s->prim_first.upload( prim_first );
-	s->err.upload( std::vector<uint32_t>( 1, 0 ) );
+	s->err.upload( std::vector<uint32_t>( 2, 0 ) );  // [0] error word, [1] query work cursor
 	s->lights = lights;
 	s->tables_host = tables;
 	if ( nt )
@@ -888,11 +891,14 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	c.x0 = x0, c.y0 = y0, c.ww = x1 - x0, c.wh = y1 - y0;
 	c.seed = desc->seed;
 	r.samples = uint64_t( c.ww ) * c.wh * c.spp;
-	uint64_t cap = desc->wave_paths ? desc->wave_paths : ( 1u << 22 );
+	uint64_t cap = desc->wave_paths ? desc->wave_paths : s->tune_wave;
 	cap = std::min<uint64_t>( cap, r.samples );
 	cap = std::min<uint64_t>( cap, 1ull << 30 );
 	c.wave_paths = uint32_t( cap );
 	c.count_work = desc->count_work != 0;
+	c.refill_min = desc->refill_min ? std::min<uint32_t>( desc->refill_min, 32 ) : s->tune_refill;
+	c.traverse_blocks_per_sm =
+		desc->traverse_blocks_per_sm ? int( std::min<uint32_t>( desc->traverse_blocks_per_sm, 8 ) ) : s->tune_blocks;
 	r.sc = dev_scene( s );
 	r.sc.cam = make_camera( s->cam, desc->width, desc->height, desc->spp );
 	return r;
@@ -1254,6 +1260,73 @@ int cr_render( cr_scene *s, const cr_render_desc *desc, double *film, cr_stats *
 		check_device_error( s, st );
 		for ( size_t p = 0; p < npx; ++p )
 			for ( int c = 0; c < 3; ++c ) film[ 3 * p + c ] = hc[ p ] ? film[ 3 * p + c ] / hc[ p ] : 0.0;
+	} );
+}
+
+int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tuning *out )
+{
+	return guarded( [&] {
+		if ( !out ) fail( CR_ERR_INVALID, "null output" );
+		Resolved base = resolve( s, desc );
+		cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+		// Sample render: a band of 1/8 of the window's rows around its middle,
+		// at the request's spp capped at 64.
+		RenderConfig cfg = base.cfg;
+		uint32_t band = std::max<uint32_t>( 1, cfg.wh / 8 );
+		cfg.y0 = cfg.y0 + ( cfg.wh - band ) / 2;
+		cfg.wh = band;
+		uint32_t spp = std::min<uint32_t>( cfg.spp, 64 );
+		DevScene sc = base.sc;
+		if ( spp != cfg.spp ) sc.cam = make_camera( s->cam, sc.cam.width, sc.cam.height, spp );
+		cfg.spp = spp;
+		cfg.count_work = false;
+		uint64_t samples = uint64_t( cfg.ww ) * cfg.wh * cfg.spp;
+		size_t npx = size_t( cfg.ww ) * cfg.wh;
+		double *sum, *sq;
+		uint32_t *cnt;
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+		uint32_t tried = 0;
+		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
+			RenderConfig c = cfg;
+			c.wave_paths = uint32_t( std::min<uint64_t>( wave, samples ) );
+			c.refill_min = refill;
+			c.traverse_blocks_per_sm = blocks;
+			ensure_wave( s, c.wave_paths, c.max_bounce, st );
+			StageTimes warm, t;
+			render_waves( sc, c, s->wave, sum, sq, cnt, st, &warm );
+			render_waves( sc, c, s->wave, sum, sq, cnt, st, &t );
+			++tried;
+			return double( samples ) / ( t.total * 1e3 );
+		};
+		uint32_t wave = 1u << 22, refill = 16;
+		int blocks = 8;
+		double best = rate( wave, refill, blocks );
+		double dflt = best;
+		for ( uint32_t r : { 4u, 8u, 12u, 24u, 32u } )
+		{
+			double v = rate( wave, r, blocks );
+			if ( v > best ) best = v, refill = r;
+		}
+		for ( int b : { 4, 6 } )
+		{
+			double v = rate( wave, refill, b );
+			if ( v > best ) best = v, blocks = b;
+		}
+		for ( uint32_t w : { 1u << 20, 1u << 21, 1u << 23 } )
+		{
+			if ( w > samples && wave >= samples ) continue;
+			double v = rate( w, refill, blocks );
+			if ( v > best ) best = v, wave = w;
+		}
+		cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
+		cuda_check( cudaStreamSynchronize( st ), "autotune" );
+		s->tune_wave = wave, s->tune_refill = refill, s->tune_blocks = blocks;
+		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
+		out->candidates_tried = tried;
+		out->msamples_per_s = best;
+		out->default_msamples_per_s = dflt;
 	} );
 }
 

@@ -160,142 +160,6 @@ __device__ __forceinline__ bool sphere_test( const DevSphere &s, float3 o, float
 
 __device__ __forceinline__ float q8( uint32_t w, int sh ) { return float( ( w >> sh ) & 0xFFu ); }
 
-struct WorkCount
-{
-	uint32_t nodes, tris;
-};
-
-// Quantised 8-wide BVH traversal with a short stack of (base, hit-mask) node
-// groups.  ANY = shadow query (first hit ends it).  Returns true on a hit;
-// the closest-hit result is written to `hit` (t, BVH-order triangle slot or
-// HIT_SPHERE | sphere, u, v).  *err is set when the stack would overflow.
-template <bool ANY, bool COUNT>
-__device__ __forceinline__ bool traverse( const DevScene &sc, float3 o, float3 d, float tmin, float tmax,
-										  HitRec &hit, WorkCount &wc, uint32_t *err )
-{
-	hit.t = tmax;
-	hit.id = HIT_MISS;
-	hit.u = hit.v = 0.f;
-	bool found = false;
-	for ( uint32_t s = 0; s < sc.n_spheres; ++s )
-	{
-		float t;
-		if ( sphere_test( sc.spheres[ s ], o, d, tmin, hit.t, t ) )
-		{
-			hit.t = t;
-			hit.id = HIT_SPHERE | s;
-			found = true;
-			if ( ANY ) return true;
-		}
-	}
-	// A NaN ray would pass every slab test (fminf/fmaxf drop NaN operands)
-	// and walk the whole tree; it hits nothing.
-	if ( sc.n_nodes == 0 || !finite3( o ) || !finite3( d ) ) return found;
-	RayPre r = make_ray( o, d );
-	// Node boxes are tested against a slightly widened interval so that float
-	// rounding in the slab test never culls a triangle the exact test accepts.
-	const float grow = 1.0f + 4.0f * 5.96e-8f;
-	uint2 stack[ TRAVERSAL_STACK ];
-	int sp = 0;
-	// Start with the root as the only child of a virtual group: slot 0, internal.
-	uint2 ng = make_uint2( 0u, ( 1u << ( 24 + r.oct ) ) | 1u );
-	const uint4 *base = reinterpret_cast<const uint4 *>( sc.nodes );
-	// A tree visits each node at most once per ray; the cap and the index
-	// checks turn a malformed tree into an error flag instead of a hang or
-	// an out-of-bounds read.
-	uint32_t budget = sc.n_nodes;
-	for ( ;; )
-	{
-		// Next child node of the current node group, nearest octant slot first.
-		uint32_t b = __ffs( ng.y >> 24 ) - 1;
-		ng.y &= ~( 1u << ( 24 + b ) );
-		uint32_t slot = b ^ r.oct;
-		uint32_t node = ng.x + __popc( ng.y & 0xFFu & ( ( 1u << slot ) - 1u ) );
-		if ( node >= sc.n_nodes || budget-- == 0 )
-		{
-			atomicOr( err, 2u );
-			break;
-		}
-		if ( ng.y > 0x00FFFFFFu )
-		{
-			if ( sp < TRAVERSAL_STACK )
-				stack[ sp++ ] = ng;
-			else
-				atomicOr( err, 1u );
-		}
-		const uint4 *np = base + 5 * size_t( node );
-		uint4 n0 = __ldg( np ), n1 = __ldg( np + 1 ), n2 = __ldg( np + 2 ), n3 = __ldg( np + 3 ), n4 = __ldg( np + 4 );
-		if ( COUNT ) ++wc.nodes;
-		float3 p = f3( __uint_as_float( n0.x ), __uint_as_float( n0.y ), __uint_as_float( n0.z ) );
-		uint32_t ex = n0.w & 0xFFu, ey = ( n0.w >> 8 ) & 0xFFu, ez = ( n0.w >> 16 ) & 0xFFu, imask = n0.w >> 24;
-		float3 adj_s = f3( __uint_as_float( ex << 23 ) * r.invd.x, __uint_as_float( ey << 23 ) * r.invd.y,
-						   __uint_as_float( ez << 23 ) * r.invd.z );
-		float3 adj_o = ( p - o ) * r.invd;
-		// Near/far quantised planes per axis, by ray direction sign.
-		uint32_t nx0 = n2.x, nx1 = n2.y, fx0 = n3.z, fx1 = n3.w;
-		uint32_t ny0 = n2.z, ny1 = n2.w, fy0 = n4.x, fy1 = n4.y;
-		uint32_t nz0 = n3.x, nz1 = n3.y, fz0 = n4.z, fz1 = n4.w;
-		if ( r.oct & 1u ) { uint32_t t0 = nx0, t1 = nx1; nx0 = fx0, nx1 = fx1, fx0 = t0, fx1 = t1; }
-		if ( r.oct & 2u ) { uint32_t t0 = ny0, t1 = ny1; ny0 = fy0, ny1 = fy1, fy0 = t0, fy1 = t1; }
-		if ( r.oct & 4u ) { uint32_t t0 = nz0, t1 = nz1; nz0 = fz0, nz1 = fz1, fz0 = t0, fz1 = t1; }
-		const float tlim = hit.t * grow;
-		uint32_t node_hits = 0, tri_hits = 0;
-#pragma unroll
-		for ( int i = 0; i < 8; ++i )
-		{
-			const int sh = 8 * ( i & 3 );
-			uint32_t wnx = i < 4 ? nx0 : nx1, wny = i < 4 ? ny0 : ny1, wnz = i < 4 ? nz0 : nz1;
-			uint32_t wfx = i < 4 ? fx0 : fx1, wfy = i < 4 ? fy0 : fy1, wfz = i < 4 ? fz0 : fz1;
-			float tnx = fmaf( q8( wnx, sh ), adj_s.x, adj_o.x ), tfx = fmaf( q8( wfx, sh ), adj_s.x, adj_o.x );
-			float tny = fmaf( q8( wny, sh ), adj_s.y, adj_o.y ), tfy = fmaf( q8( wfy, sh ), adj_s.y, adj_o.y );
-			float tnz = fmaf( q8( wnz, sh ), adj_s.z, adj_o.z ), tfz = fmaf( q8( wfz, sh ), adj_s.z, adj_o.z );
-			float tn = fmaxf( fmaxf( tnx, tny ), fmaxf( tnz, tmin ) );
-			float tf = fminf( fminf( tfx, tfy ), fminf( tfz, tlim ) );
-			uint32_t meta = ( ( i < 4 ? n1.z : n1.w ) >> sh ) & 0xFFu;
-			bool internal = ( imask >> i ) & 1u;
-			if ( tn <= tf )
-			{
-				if ( internal )
-					node_hits |= 1u << ( i ^ r.oct );
-				else if ( meta )
-					tri_hits |= ( ( 1u << ( meta >> 5 ) ) - 1u ) << ( meta & 31u );
-			}
-		}
-		ng = node_hits ? make_uint2( n1.x, ( node_hits << 24 ) | imask ) : make_uint2( 0u, 0u );
-		// Leaf triangles of this node.
-		while ( tri_hits )
-		{
-			uint32_t k = __ffs( tri_hits ) - 1;
-			tri_hits &= tri_hits - 1;
-			uint32_t ti = n1.y + k;
-			if ( ti >= sc.n_tris )
-			{
-				atomicOr( err, 4u );
-				break;
-			}
-			const float4 *tp = sc.tris + 3 * size_t( ti );
-			float4 a = __ldg( tp ), bq = __ldg( tp + 1 ), c = __ldg( tp + 2 );
-			if ( COUNT ) ++wc.tris;
-			float t, u, v;
-			if ( tri_test( r, f3( a ), f3( bq ), f3( c ), tmin, hit.t, t, u, v ) )
-			{
-				hit.t = t;
-				hit.id = ti;
-				hit.u = u;
-				hit.v = v;
-				found = true;
-				if ( ANY ) return true;
-			}
-		}
-		if ( ng.y <= 0x00FFFFFFu )
-		{
-			if ( sp == 0 ) break;
-			ng = stack[ --sp ];
-		}
-	}
-	return found;
-}
-
 // ------------------------------------------------------------------ shading helpers
 // Reference frame (src/core/meta/scene.hpp:48-53): u = n x (0,1,0), v = n x u,
 // both normalised (NaN when n is parallel to +-y, as in the reference).

@@ -30,7 +30,7 @@ namespace
 constexpr size_t align256( size_t x ) { return ( x + 255 ) & ~size_t( 255 ); }
 
 constexpr size_t NA_PATHS = CR_NOALLOC_MAX_WAVE_PATHS;
-constexpr size_t NA_COUNTERS = 2 * ( CR_NOALLOC_MAX_BOUNCE + 3 );
+constexpr size_t NA_COUNTERS = n_counters_for( CR_NOALLOC_MAX_BOUNCE );
 // Byte offsets of the wave arrays inside the scratch array.
 constexpr size_t OFF_RAY_O = 0;
 constexpr size_t OFF_RAY_D = OFF_RAY_O + align256( NA_PATHS * sizeof( float4 ) );
@@ -146,7 +146,7 @@ extern "C" int cr_render_device_noalloc( cr_scene *s, const cr_render_desc *desc
 	wb.sh_d = reinterpret_cast<float4 *>( base + OFF_SH_D );
 	wb.sh_c = reinterpret_cast<float4 *>( base + OFF_SH_C );
 	wb.counters = reinterpret_cast<uint32_t *>( base + OFF_COUNTERS );
-	wb.n_counters = 2 * ( cfg.max_bounce + 3 );
+	wb.n_counters = n_counters_for( cfg.max_bounce );
 	wb.err = reinterpret_cast<uint32_t *>( base + OFF_ERR );
 	wb.work = reinterpret_cast<unsigned long long *>( base + OFF_WORK );
 	cudaStream_t st = static_cast<cudaStream_t>( stream );

@@ -25,6 +25,7 @@
 #include "../../include/cr.h"
 #include "cr_device.cuh"
 #include "render.h"
+#include "traverse.cuh"
 
 namespace cr
 {
@@ -54,7 +55,7 @@ __device__ __forceinline__ uint32_t warp_append( bool want, uint32_t *counter )
 
 __global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa )
 {
-	if ( blockIdx.x == 0 && threadIdx.x == 0 ) wb.counters[ 0 ] = wa.n;
+	if ( blockIdx.x == 0 && threadIdx.x == 0 ) wb.counters[ CNT_EXT ] = wa.n;
 	for ( uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < wa.n; s += gridDim.x * blockDim.x )
 	{
 		uint64_t g = wa.first + s;
@@ -72,68 +73,80 @@ __global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveA
 	}
 }
 
-template <bool COUNT>
-__device__ __forceinline__ void flush_work( WorkCount &wc, unsigned long long *work )
+// Closest-hit queue of one bounce: rays from the path state, hit records out.
+struct ExtendIO
 {
-	if ( !COUNT ) return;
-	uint32_t n = wc.nodes, t = wc.tris;
-	for ( int o = 16; o; o >>= 1 )
+	const uint32_t *queue;
+	const float4 *ray_o, *ray_d;
+	HitRec *hit;
+	__device__ void load( uint32_t i, uint32_t &item, float3 &o, float3 &d, float &tmin, float &tmax ) const
 	{
-		n += __shfl_xor_sync( ~0u, n, o );
-		t += __shfl_xor_sync( ~0u, t, o );
+		item = queue[ i ];
+		float4 a = ray_o[ item ], b = ray_d[ item ];
+		o = f3( a ), d = f3( b ), tmin = a.w, tmax = b.w;
 	}
-	if ( lane_id() == 0 )
-	{
-		atomicAdd( work, (unsigned long long)n );
-		atomicAdd( work + 1, (unsigned long long)t );
-	}
-}
+	__device__ void finish( uint32_t item, const HitRec &h, bool ) const { hit[ item ] = h; }
+};
 
-template <bool COUNT>
-__global__ void __launch_bounds__( 128 ) k_extend( DevScene sc, WaveBuffers wb, uint32_t bounce )
+// Shadow queue of one bounce: an unoccluded ray adds its contribution.
+struct ShadowIO
 {
-	const uint32_t n = wb.counters[ 2 * bounce ];
-	const uint32_t *q = wb.queue[ bounce & 1 ];
-	WorkCount wc{ 0, 0 };
-	const uint32_t stride = gridDim.x * blockDim.x;
-	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
+	const uint32_t *queue;
+	const float4 *ray_o, *ray_d, *contrib;
+	float4 *L;
+	__device__ void load( uint32_t i, uint32_t &item, float3 &o, float3 &d, float &tmin, float &tmax ) const
 	{
-		uint32_t i = base + lane_id();
-		if ( i < n )
-		{
-			uint32_t path = q[ i ];
-			float4 o = wb.ray_o[ path ], d = wb.ray_d[ path ];
-			HitRec h;
-			traverse<false, COUNT>( sc, f3( o ), f3( d ), o.w, d.w, h, wc, wb.err );
-			wb.hit[ path ] = h;
-		}
+		item = queue[ i ];
+		float4 a = ray_o[ item ], b = ray_d[ item ];
+		o = f3( a ), d = f3( b ), tmin = a.w, tmax = b.w;
 	}
-	flush_work<COUNT>( wc, wb.work );
-}
-
-template <bool COUNT>
-__global__ void __launch_bounds__( 128 ) k_shadow( DevScene sc, WaveBuffers wb, uint32_t bounce )
-{
-	const uint32_t n = wb.counters[ 2 * bounce + 1 ];
-	WorkCount wc{ 0, 0 };
-	const uint32_t stride = gridDim.x * blockDim.x;
-	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
+	__device__ void finish( uint32_t item, const HitRec &, bool occluded ) const
 	{
-		uint32_t i = base + lane_id();
-		if ( i < n )
+		if ( occluded ) return;
+		float4 c = contrib[ item ], l = L[ item ];
+		L[ item ] = make_float4( l.x + c.x, l.y + c.y, l.z + c.z, l.w );
+	}
+};
+
+// Batched ray queries of the C ABI: n x {o, d, tmax} in, cr_hit out.
+struct QueryIO
+{
+	const float *rays;
+	cr_hit *out;
+	const float4 *tris, *attrs;
+	const DevSphere *spheres;
+	const uint32_t *prim_first;
+	__device__ void load( uint32_t i, uint32_t &item, float3 &o, float3 &d, float &tmin, float &tmax ) const
+	{
+		item = i;
+		const float *r = rays + 7 * size_t( i );
+		o = f3( r[ 0 ], r[ 1 ], r[ 2 ] ), d = f3( r[ 3 ], r[ 4 ], r[ 5 ] );
+		tmin = 0.f;
+		tmax = r[ 6 ] > 0.f ? r[ 6 ] : INFINITY;
+	}
+	__device__ void finish( uint32_t item, const HitRec &h, bool found ) const
+	{
+		cr_hit res;
+		res.prim = -1, res.tri = -1, res.t = INFINITY, res.u = res.v = 0.f;
+		if ( found )
 		{
-			uint32_t path = wb.shadow_queue[ i ];
-			float4 o = wb.sh_o[ path ], d = wb.sh_d[ path ];
-			HitRec h;
-			if ( !traverse<true, COUNT>( sc, f3( o ), f3( d ), o.w, d.w, h, wc, wb.err ) )
+			res.t = h.t, res.u = h.u, res.v = h.v;
+			if ( h.id & HIT_SPHERE )
+				res.prim = spheres[ h.id & ~HIT_SPHERE ].prim;
+			else
 			{
-				float4 c = wb.sh_c[ path ], l = wb.L[ path ];
-				wb.L[ path ] = make_float4( l.x + c.x, l.y + c.y, l.z + c.z, l.w );
+				uint32_t gid = __float_as_uint( tris[ 3 * size_t( h.id ) ].w );
+				int prim = __float_as_int( attrs[ 3 * size_t( gid ) + 1 ].w );
+				res.prim = prim;
+				res.tri = int( gid - prim_first[ prim ] );
 			}
 		}
+		out[ item ] = res;
 	}
-	flush_work<COUNT>( wc, wb.work + 2 );
-}
+};
+
+// Idle lanes per warp that trigger a refill in batched ray queries.
+constexpr uint32_t QUERY_REFILL_MIN = 16;
 
 struct Surface
 {
@@ -403,11 +416,11 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
 												  uint32_t bounce, uint2 key )
 {
-	const uint32_t n = wb.counters[ 2 * bounce ];
+	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
 	const uint32_t *q = wb.queue[ bounce & 1 ];
 	uint32_t *nq = wb.queue[ ( bounce + 1 ) & 1 ];
-	uint32_t *next_count = wb.counters + 2 * ( bounce + 1 );
-	uint32_t *shadow_count = wb.counters + 2 * bounce + 1;
+	uint32_t *next_count = wb.counters + CPB * ( bounce + 1 ) + CNT_EXT;
+	uint32_t *shadow_count = wb.counters + CPB * bounce + CNT_SHADOW;
 	const uint32_t stride = gridDim.x * blockDim.x;
 	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
 	{
@@ -473,36 +486,6 @@ __global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, dou
 		sum[ 3 * p ] += a0, sum[ 3 * p + 1 ] += a1, sum[ 3 * p + 2 ] += a2;
 		sumsq[ 3 * p ] += q0, sumsq[ 3 * p + 1 ] += q1, sumsq[ 3 * p + 2 ] += q2;
 		count[ p ] += c;
-	}
-}
-
-__global__ void k_trace( DevScene sc, const float *rays, uint64_t n, int any, cr_hit *out, uint32_t *err )
-{
-	WorkCount wc{ 0, 0 };
-	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
-	{
-		const float *r = rays + 7 * i;
-		float3 o = f3( r[ 0 ], r[ 1 ], r[ 2 ] ), d = f3( r[ 3 ], r[ 4 ], r[ 5 ] );
-		float tmax = r[ 6 ] > 0.f ? r[ 6 ] : INFINITY;
-		HitRec h;
-		bool hit = any ? traverse<true, false>( sc, o, d, 0.f, tmax, h, wc, err )
-					   : traverse<false, false>( sc, o, d, 0.f, tmax, h, wc, err );
-		cr_hit res;
-		res.prim = -1, res.tri = -1, res.t = INFINITY, res.u = res.v = 0.f;
-		if ( hit )
-		{
-			res.t = h.t, res.u = h.u, res.v = h.v;
-			if ( h.id & HIT_SPHERE )
-				res.prim = sc.spheres[ h.id & ~HIT_SPHERE ].prim;
-			else
-			{
-				uint32_t gid = __float_as_uint( sc.tris[ 3 * size_t( h.id ) ].w );
-				int prim = __float_as_int( sc.attrs[ 3 * size_t( gid ) + 1 ].w );
-				res.prim = prim;
-				res.tri = int( gid - sc.prim_first[ prim ] );
-			}
-		}
-		out[ i ] = res;
 	}
 }
 
@@ -601,7 +584,7 @@ void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaSt
 	alloc( wb.sh_o, capacity, st );
 	alloc( wb.sh_d, capacity, st );
 	alloc( wb.sh_c, capacity, st );
-	wb.n_counters = 2 * ( max_bounce + 3 );
+	wb.n_counters = n_counters_for( max_bounce );
 	alloc( wb.counters, wb.n_counters, st );
 	alloc( wb.err, 1, st );
 	alloc( wb.work, 4, st );
@@ -623,8 +606,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	const uint64_t total = uint64_t( cfg.ww ) * cfg.wh * cfg.spp;
 	const uint32_t P = wb.capacity;
 	const int sms = sm_count();
-	const int g_ext = cfg.grid_extend > 0 ? cfg.grid_extend : sms * 8;
-	const int g_shade = cfg.grid_shade > 0 ? cfg.grid_shade : sms * 8;
+	const int g_ext = sms * std::max( 1, std::min( 8, cfg.traverse_blocks_per_sm ) );
+	const int g_shade = sms * 8;
 	const uint2 key = make_uint2( uint32_t( cfg.seed ), uint32_t( cfg.seed >> 32 ) ^ 0x5EED5EEDu );
 	EventPool pool;
 	struct Mark
@@ -668,18 +651,24 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
 		{
 			timed( 0, [&] {
+				ExtendIO io{ wb.queue[ b & 1 ], wb.ray_o, wb.ray_d, wb.hit };
+				const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
+				uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
 				if ( cfg.count_work )
-					k_extend<true><<<g_ext, 128, 0, st>>>( sc, wb, b );
+					k_traverse<ExtendIO, false, true><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 				else
-					k_extend<false><<<g_ext, 128, 0, st>>>( sc, wb, b );
+					k_traverse<ExtendIO, false, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 			} );
 			timed( 2, [&] { k_shade<<<g_shade, 128, 0, st>>>( sc, cfg, wb, wa, b, key ); } );
 			if ( sc.n_lights )
 				timed( 1, [&] {
+					ShadowIO io{ wb.shadow_queue, wb.sh_o, wb.sh_d, wb.sh_c, wb.L };
+					const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
+					uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
 					if ( cfg.count_work )
-						k_shadow<true><<<g_ext, 128, 0, st>>>( sc, wb, b );
+						k_traverse<ShadowIO, true, true><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 					else
-						k_shadow<false><<<g_ext, 128, 0, st>>>( sc, wb, b );
+						k_traverse<ShadowIO, true, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 				} );
 		}
 		timed( 3, [&] {
@@ -698,8 +687,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 			check( cudaStreamSynchronize( st ), "counts" );
 			for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
 			{
-				times->rays_extend += host_counts[ 2 * b ];
-				times->rays_shadow += host_counts[ 2 * b + 1 ];
+				times->rays_extend += host_counts[ CPB * b + CNT_EXT ];
+				times->rays_shadow += host_counts[ CPB * b + CNT_SHADOW ];
 			}
 		}
 	}
@@ -731,8 +720,17 @@ void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hi
 				   cudaStream_t st )
 {
 	if ( !n ) return;
+	if ( n >= ( 1ull << 32 ) - 64 ) throw std::runtime_error( "too many rays in one query" );
+	// err[0] is the error word, err[1] the work cursor of this query.
+	check( cudaMemsetAsync( err + 1, 0, sizeof( uint32_t ), st ), "trace cursor" );
 	int g = int( std::min<uint64_t>( ( n + 127 ) / 128, uint64_t( sm_count() ) * 8 ) );
-	k_trace<<<g, 128, 0, st>>>( sc, rays, n, any_hit, out, err );
+	QueryIO io{ rays, out, sc.tris, sc.attrs, sc.spheres, sc.prim_first };
+	if ( any_hit )
+		k_traverse<QueryIO, true, false><<<g, 128, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
+																 QUERY_REFILL_MIN );
+	else
+		k_traverse<QueryIO, false, false><<<g, 128, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
+																  QUERY_REFILL_MIN );
 	check( cudaGetLastError(), "trace launch" );
 }
 

@@ -20,11 +20,16 @@ struct WaveBuffers
 	uint32_t *queue[ 2 ] = { nullptr, nullptr };
 	uint32_t *shadow_queue = nullptr;
 	float4 *sh_o = nullptr, *sh_d = nullptr, *sh_c = nullptr;
-	uint32_t *counters = nullptr;               // [2b] extension queue, [2b+1] shadow queue of bounce b
+	uint32_t *counters = nullptr;               // per bounce b, CPB entries: see CNT_* below
 	uint32_t n_counters = 0;
 	uint32_t *err = nullptr;                    // device error word
 	unsigned long long *work = nullptr;         // extension [0] nodes [1] triangles, shadow [2] [3]
 };
+
+// Device counters per bounce: queue lengths and the traversal kernels' work cursors.
+constexpr uint32_t CPB = 4;
+constexpr uint32_t CNT_EXT = 0, CNT_SHADOW = 1, CNT_EXT_CURSOR = 2, CNT_SHADOW_CURSOR = 3;
+inline constexpr uint32_t n_counters_for( uint32_t max_bounce ) { return CPB * ( max_bounce + 3 ); }
 
 struct RenderConfig
 {
@@ -34,8 +39,8 @@ struct RenderConfig
 	uint64_t seed;
 	uint32_t wave_paths;
 	bool count_work;
-	int block_extend = 128, block_shade = 128;
-	int grid_extend = 0, grid_shade = 0;      // 0: device-derived default
+	uint32_t refill_min = 16;        // traversal: idle lanes per warp that trigger a refill (1..32)
+	int traverse_blocks_per_sm = 8;  // traversal grid = SMs x this (1..8; 128-thread blocks)
 };
 
 struct StageTimes

@@ -1,0 +1,222 @@
+// Persistent wide-BVH traversal kernel shared by the closest-hit queue
+// (k_extend), the shadow queue (k_shadow) and the batched ray queries of the
+// C ABI.
+//
+// Each warp owns 32 traversal states.  A lane that finishes its ray is refilled
+// from the queue (one atomic per warp) once enough lanes are idle, so a warp no
+// longer waits for its slowest ray.  Every iteration the warp votes between a
+// node step (each lane with no pending triangles visits one wide node, pops, or
+// finishes) and a triangle step (each lane with pending triangles tests one).
+// The minority waits, so lanes in one iteration run the same code.
+#pragma once
+#include "cr_device.cuh"
+
+namespace cr
+{
+constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
+
+// Intersects the ray with the 8 children of `node`; returns the node-group
+// hits (bits at slot ^ octant) and the triangle-group hits (24-bit mask).
+__device__ __forceinline__ void visit_node( const DevScene &sc, const RayPre &r, uint32_t node, float tmin,
+											float tlim, uint2 &ng, uint2 &tg )
+{
+	const uint4 *np = reinterpret_cast<const uint4 *>( sc.nodes ) + 5 * size_t( node );
+	uint4 n0 = __ldg( np ), n1 = __ldg( np + 1 ), n2 = __ldg( np + 2 ), n3 = __ldg( np + 3 ), n4 = __ldg( np + 4 );
+	float3 p = f3( __uint_as_float( n0.x ), __uint_as_float( n0.y ), __uint_as_float( n0.z ) );
+	uint32_t ex = n0.w & 0xFFu, ey = ( n0.w >> 8 ) & 0xFFu, ez = ( n0.w >> 16 ) & 0xFFu, imask = n0.w >> 24;
+	float3 adj_s = f3( __uint_as_float( ex << 23 ) * r.invd.x, __uint_as_float( ey << 23 ) * r.invd.y,
+					   __uint_as_float( ez << 23 ) * r.invd.z );
+	float3 adj_o = ( p - r.o ) * r.invd;
+	uint32_t nx0 = n2.x, nx1 = n2.y, fx0 = n3.z, fx1 = n3.w;
+	uint32_t ny0 = n2.z, ny1 = n2.w, fy0 = n4.x, fy1 = n4.y;
+	uint32_t nz0 = n3.x, nz1 = n3.y, fz0 = n4.z, fz1 = n4.w;
+	if ( r.oct & 1u ) { uint32_t t0 = nx0, t1 = nx1; nx0 = fx0, nx1 = fx1, fx0 = t0, fx1 = t1; }
+	if ( r.oct & 2u ) { uint32_t t0 = ny0, t1 = ny1; ny0 = fy0, ny1 = fy1, fy0 = t0, fy1 = t1; }
+	if ( r.oct & 4u ) { uint32_t t0 = nz0, t1 = nz1; nz0 = fz0, nz1 = fz1, fz0 = t0, fz1 = t1; }
+	uint32_t node_hits = 0, tri_hits = 0;
+#pragma unroll
+	for ( int i = 0; i < 8; ++i )
+	{
+		const int sh = 8 * ( i & 3 );
+		uint32_t wnx = i < 4 ? nx0 : nx1, wny = i < 4 ? ny0 : ny1, wnz = i < 4 ? nz0 : nz1;
+		uint32_t wfx = i < 4 ? fx0 : fx1, wfy = i < 4 ? fy0 : fy1, wfz = i < 4 ? fz0 : fz1;
+		float tnx = fmaf( q8( wnx, sh ), adj_s.x, adj_o.x ), tfx = fmaf( q8( wfx, sh ), adj_s.x, adj_o.x );
+		float tny = fmaf( q8( wny, sh ), adj_s.y, adj_o.y ), tfy = fmaf( q8( wfy, sh ), adj_s.y, adj_o.y );
+		float tnz = fmaf( q8( wnz, sh ), adj_s.z, adj_o.z ), tfz = fmaf( q8( wfz, sh ), adj_s.z, adj_o.z );
+		float tn = fmaxf( fmaxf( tnx, tny ), fmaxf( tnz, tmin ) );
+		float tf = fminf( fminf( tfx, tfy ), fminf( tfz, tlim ) );
+		uint32_t meta = ( ( i < 4 ? n1.z : n1.w ) >> sh ) & 0xFFu;
+		bool internal = ( imask >> i ) & 1u;
+		if ( tn <= tf )
+		{
+			if ( internal )
+				node_hits |= 1u << ( i ^ r.oct );
+			else if ( meta )
+				tri_hits |= ( ( 1u << ( meta >> 5 ) ) - 1u ) << ( meta & 31u );
+		}
+	}
+	ng = node_hits ? make_uint2( n1.x, ( node_hits << 24 ) | imask ) : make_uint2( 0u, 0u );
+	tg = make_uint2( n1.y, tri_hits );
+}
+
+// Ray source and result sink of the persistent kernel.  refill_min: idle lanes
+// (1..32) that trigger a refill from the queue.
+//   load(i, item, o, d, tmin, tmax): the i-th queued ray
+//   finish(item, hit, found): store the result
+template <class IO, bool ANY, bool COUNT>
+__global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, const uint32_t *n_ptr, uint32_t n_host,
+														uint32_t *cursor, uint32_t *err, unsigned long long *work,
+														uint32_t refill_min )
+{
+	const uint32_t n = n_ptr ? *n_ptr : n_host;
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t lt_mask = ( 1u << lane ) - 1u;
+	const float grow = 1.0f + 4.0f * 5.96e-8f;
+	uint32_t wnodes = 0, wtris = 0;
+	bool active = false, exhausted = false;
+	uint32_t item = 0, budget = 0;
+	RayPre r;
+	float tmin = 0.f;
+	HitRec hit;
+	bool found = false;
+	uint2 ng = make_uint2( 0u, 0u ), tg = make_uint2( 0u, 0u );
+	int sp = 0;
+	uint2 stack[ TRAVERSAL_STACK ];
+	for ( ;; )
+	{
+		if ( !exhausted )
+		{
+			uint32_t idle = __ballot_sync( FULL_MASK, !active );
+			if ( uint32_t( __popc( idle ) ) >= refill_min )
+			{
+				uint32_t leader = __ffs( idle ) - 1, base = 0;
+				if ( lane == leader ) base = atomicAdd( cursor, uint32_t( __popc( idle ) ) );
+				base = __shfl_sync( FULL_MASK, base, leader );
+				if ( base + __popc( idle ) >= n ) exhausted = true;
+				if ( !active )
+				{
+					uint32_t i = base + __popc( idle & lt_mask );
+					if ( i < n )
+					{
+						float3 o, d;
+						float tmax;
+						io.load( i, item, o, d, tmin, tmax );
+						hit.t = tmax;
+						hit.id = HIT_MISS;
+						hit.u = hit.v = 0.f;
+						found = false;
+						bool done = false;
+						for ( uint32_t s = 0; s < sc.n_spheres && !done; ++s )
+						{
+							float t;
+							if ( sphere_test( sc.spheres[ s ], o, d, tmin, hit.t, t ) )
+							{
+								hit.t = t, hit.id = HIT_SPHERE | s, found = true;
+								if ( ANY ) done = true;
+							}
+						}
+						// A NaN ray would pass every slab test; it hits nothing.
+						if ( done || sc.n_nodes == 0 || !finite3( o ) || !finite3( d ) )
+							io.finish( item, hit, found );
+						else
+						{
+							r = make_ray( o, d );
+							ng = make_uint2( 0u, ( 1u << ( 24 + r.oct ) ) | 1u );
+							tg = make_uint2( 0u, 0u );
+							sp = 0;
+							budget = sc.n_nodes;
+							active = true;
+						}
+					}
+				}
+			}
+		}
+		const uint32_t act = __ballot_sync( FULL_MASK, active );
+		if ( !act )
+		{
+			if ( exhausted ) break;
+			continue;
+		}
+		const uint32_t want_tri = __ballot_sync( FULL_MASK, active && tg.y != 0u );
+		const bool tri_step = 2 * __popc( want_tri ) >= __popc( act );
+		if ( !active ) continue;
+		bool done = false;
+		if ( tri_step )
+		{
+			if ( tg.y )
+			{
+				uint32_t k = __ffs( tg.y ) - 1;
+				tg.y &= tg.y - 1u;
+				uint32_t ti = tg.x + k;
+				if ( ti >= sc.n_tris )
+				{
+					atomicOr( err, 4u );
+					tg.y = 0u;
+				}
+				else
+				{
+					const float4 *tp = sc.tris + 3 * size_t( ti );
+					float4 a = __ldg( tp ), b = __ldg( tp + 1 ), c = __ldg( tp + 2 );
+					if ( COUNT ) ++wtris;
+					float t, u, v;
+					if ( tri_test( r, f3( a ), f3( b ), f3( c ), tmin, hit.t, t, u, v ) )
+					{
+						hit.t = t, hit.id = ti, hit.u = u, hit.v = v, found = true;
+						if ( ANY ) done = true;
+					}
+				}
+			}
+		}
+		else if ( !tg.y )
+		{
+			if ( ng.y > 0x00FFFFFFu )
+			{
+				uint32_t b = __ffs( ng.y >> 24 ) - 1;
+				ng.y &= ~( 1u << ( 24 + b ) );
+				uint32_t slot = b ^ r.oct;
+				uint32_t node = ng.x + __popc( ng.y & 0xFFu & ( ( 1u << slot ) - 1u ) );
+				if ( node >= sc.n_nodes || budget-- == 0 )
+				{
+					atomicOr( err, 2u );
+					done = true;
+				}
+				else
+				{
+					if ( ng.y > 0x00FFFFFFu )
+					{
+						if ( sp < TRAVERSAL_STACK )
+							stack[ sp++ ] = ng;
+						else
+							atomicOr( err, 1u );
+					}
+					if ( COUNT ) ++wnodes;
+					visit_node( sc, r, node, tmin, hit.t * grow, ng, tg );
+				}
+			}
+			else if ( sp > 0 )
+				ng = stack[ --sp ];
+			else
+				done = true;
+		}
+		if ( done )
+		{
+			io.finish( item, hit, found );
+			active = false;
+		}
+	}
+	if ( COUNT )
+	{
+		for ( int o = 16; o; o >>= 1 )
+		{
+			wnodes += __shfl_xor_sync( FULL_MASK, wnodes, o );
+			wtris += __shfl_xor_sync( FULL_MASK, wtris, o );
+		}
+		if ( lane == 0 )
+		{
+			atomicAdd( work, (unsigned long long)wnodes );
+			atomicAdd( work + 1, (unsigned long long)wtris );
+		}
+	}
+}
+
+}  // namespace cr

@@ -57,7 +57,20 @@ typedef struct cr_render_desc {
     uint32_t wave_paths;     /* paths in flight per wave; 0 = autotuned default        */
     int32_t guiding;         /* 1: learned path guiding (estimator MIS only)           */
     int32_t count_work;      /* 1: also count BVH nodes / triangles visited            */
+    uint32_t refill_min;     /* traversal: idle lanes of 32 that trigger a refill; 0 = tuned */
+    uint32_t traverse_blocks_per_sm; /* traversal grid, 1..8 blocks per SM; 0 = tuned    */
 } cr_render_desc;
+
+/* Launch configuration chosen by cr_autotune (also used by later renders of
+ * the scene whose desc fields are 0). */
+typedef struct cr_tuning {
+    uint32_t wave_paths;
+    uint32_t refill_min;
+    uint32_t traverse_blocks_per_sm;
+    uint32_t candidates_tried;
+    double msamples_per_s;   /* rate of the chosen configuration on the sample render */
+    double default_msamples_per_s; /* rate of the built-in defaults on the same sample */
+} cr_tuning;
 
 typedef struct cr_stats {
     double ms_total;       /* device time of the whole render (CUDA events)  */
@@ -182,6 +195,14 @@ int cr_render_device(cr_scene *s, const cr_render_desc *desc, double *d_sum, dou
 #define CR_NOALLOC_MAX_BOUNCE 64u
 int cr_render_device_noalloc(cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sumsq,
                              uint32_t *d_count, void *stream);
+
+/* No counterpart in the reference (its tracer has no launch parameters).
+ * Picks the wave size, the traversal refill threshold and the traversal grid
+ * for this scene by timing a sample render (a band of the requested image,
+ * at most 64 spp) under each candidate, coordinate by coordinate, with CUDA
+ * events.  The choice is stored in the scene and returned in *out.
+ * Synchronises `stream`; allocates temporary device buffers. */
+int cr_autotune(cr_scene *s, const cr_render_desc *desc, void *stream, cr_tuning *out);
 
 /* Renderer::render (src/core/renderer/renderer.cu:13-52): load a scene file,
  * render it with the configured kernel and tracer, write the reference's

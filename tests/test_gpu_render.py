@@ -115,3 +115,16 @@ def test_nan_frame_samples_dropped_like_reference(cr, scenes):
     k = render_film(cr, s, 16, 16, 4, seeds=[1], estimator=cr.KOISHI)
     m = render_film(cr, s, 16, 16, 4, seeds=[1], estimator=cr.MIS)
     assert k.count.min() == 0 and m.count.min() == 4
+
+
+def test_autotune_keeps_results(cr, scenes):
+    """The tuner only changes launch parameters: the film is the same (to FP64
+    summation order) before and after tuning, and the choice is in range."""
+    s = cr.Scene.from_desc(scenes.config1(level=5))
+    before = render_film(cr, s, 64, 48, 16, seeds=[2], estimator=cr.KOISHI)
+    t = s.autotune(cr.render_desc(64, 48, 16, max_bounce=7, estimator=cr.KOISHI))
+    assert 1 <= t.refill_min <= 32 and 1 <= t.traverse_blocks_per_sm <= 8 and t.wave_paths >= 1 << 20
+    assert t.candidates_tried >= 8 and t.msamples_per_s >= t.default_msamples_per_s > 0
+    after = render_film(cr, s, 64, 48, 16, seeds=[2], estimator=cr.KOISHI)
+    np.testing.assert_allclose(after.sum, before.sum, rtol=1e-12, atol=0)
+    assert np.array_equal(after.count, before.count)
