@@ -61,7 +61,7 @@ class Tuning(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_extend", C.c_double), ("ms_shadow", C.c_double),
-                ("ms_shade", C.c_double), ("ms_other", C.c_double), ("samples", C.c_uint64),
+                ("ms_shade", C.c_double), ("ms_other", C.c_double), ("ms_guide", C.c_double), ("samples", C.c_uint64),
                 ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64), ("nodes", C.c_uint64),
                 ("tris", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_tris", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32),
                 ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32)]
@@ -101,6 +101,9 @@ def lib():
             "cr_render_file": (I, [C.c_char_p, C.c_char_p, C.c_char_p, U32, U32, U32, C.c_char_p, C.c_char_p]),
             "cr_write_png": (I, [C.c_char_p, U32, U32, P]),
             "cr_autotune": (I, [P, P, P, P]),
+            "cr_guide_reset": (I, [P, U64]), "cr_guide_info": (I, [P, P, P, P, P]),
+            "cr_guide_params": (I, [P, P, P, P, I]), "cr_guide_forward": (I, [P, P, U64, P]),
+            "cr_guide_gradients": (I, [P, P, U64, P, P, P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
         }
@@ -240,6 +243,47 @@ class Scene:
                                       C.c_void_p(count_ptr), C.c_void_p(stream),
                                       C.byref(st) if st is not None else None))
         return st
+
+
+class Guide:
+    """The scene's learned path guide (cr_guide_*)."""
+
+    def __init__(self, scene):
+        self.scene = scene
+
+    def reset(self, seed=1):
+        _check(lib().cr_guide_reset(self.scene.h, seed))
+        return self
+
+    def info(self):
+        bmin, binv, sizes = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(3, np.uint32)
+        step = C.c_uint32()
+        _check(lib().cr_guide_info(self.scene.h, _p(bmin), _p(binv), C.byref(step), _p(sizes)))
+        return {"bmin": bmin, "binv": binv, "step": step.value, "sizes": sizes}
+
+    def params(self):
+        s = self.info()["sizes"]
+        grid, W, b = (np.zeros(int(n), np.float32) for n in s)
+        _check(lib().cr_guide_params(self.scene.h, _p(grid), _p(W), _p(b), 0))
+        return grid, W, b
+
+    def set_params(self, grid=None, W=None, b=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (grid, W, b)]
+        ptrs = [None if a is None else _p(a) for a in arrs]
+        _check(lib().cr_guide_params(self.scene.h, *ptrs, 1))
+
+    def forward(self, inputs):
+        inputs = np.ascontiguousarray(inputs, np.float32)
+        out = np.zeros((len(inputs), 64), np.float32)
+        _check(lib().cr_guide_forward(self.scene.h, _p(inputs), len(inputs), _p(out)))
+        return out
+
+    def gradients(self, records):
+        records = np.ascontiguousarray(records, np.float32)
+        s = self.info()["sizes"]
+        ggrid, gW, gb = (np.zeros(int(n), np.float32) for n in s)
+        _check(lib().cr_guide_gradients(self.scene.h, _p(records), len(records), _p(gW), _p(gb), _p(ggrid)))
+        return ggrid, gW, gb
 
 
 def render_file(json_path, png_path, spp=1, width=1024, height=768, kernel="Radiance", tracer="CudaWavefront",

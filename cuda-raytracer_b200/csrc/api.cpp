@@ -21,6 +21,7 @@
 
 #include "../../include/cr.h"
 #include "bvh_build.h"
+#include "guide.h"
 #include "internal.h"
 #include "json.h"
 #include "render.h"
@@ -153,6 +154,8 @@ struct cr_scene
 	float scale = 1;
 	WaveBuffers wave;
 	uint32_t wave_bounces = 0;
+	GuideState guide;
+	float3 box_lo{ 0, 0, 0 }, box_hi{ 1, 1, 1 };
 	// launch configuration (defaults, or the choice of cr_autotune)
 	uint32_t tune_wave = 1u << 22, tune_refill = 16;
 	int tune_blocks = 8;
@@ -776,6 +779,8 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	for ( int a = 0; a < 3; ++a )
 		if ( std::isfinite( lo[ a ] ) ) sc = std::max( sc, std::max( std::fabs( lo[ a ] ), std::fabs( hi[ a ] ) ) );
 	s->scale = sc;
+	if ( std::isfinite( lo[ 0 ] ) )
+		s->box_lo = make_float3( lo[ 0 ], lo[ 1 ], lo[ 2 ] ), s->box_hi = make_float3( hi[ 0 ], hi[ 1 ], hi[ 2 ] );
 	std::vector<DevShader> dsh;
 	for ( auto &x : s->shaders ) dsh.push_back( x.second );
 
@@ -877,7 +882,7 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	if ( !s->has_camera ) fail( CR_ERR_INVALID, "no camera in the scene" );
 	if ( s->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, "orthographic lens is outside the Radiance path implemented here" );
 	if ( s->kernel != "Radiance" ) fail( CR_ERR_UNSUPPORTED, "kernel '" + s->kernel + "' is not implemented (Radiance only)" );
-	if ( desc->guiding ) fail( CR_ERR_UNSUPPORTED, "learned path guiding is not available in this build" );
+
 	Resolved r;
 	RenderConfig &c = r.cfg;
 	uint32_t x0 = desc->x0, y0 = desc->y0, x1 = desc->x1, y1 = desc->y1;
@@ -901,15 +906,28 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 		desc->traverse_blocks_per_sm ? int( std::min<uint32_t>( desc->traverse_blocks_per_sm, 8 ) ) : s->tune_blocks;
 	r.sc = dev_scene( s );
 	r.sc.cam = make_camera( s->cam, desc->width, desc->height, desc->spp );
+	if ( desc->guiding )
+	{
+		if ( c.estimator != EST_MIS ) fail( CR_ERR_INVALID, "learned path guiding needs the MIS estimator" );
+		if ( !s->guide.ready ) s->guide.init( s->box_lo, s->box_hi, 0x9E3779B9ull );
+		c.guiding = true;
+		c.guide = s->guide.dev();
+		c.train_paths = std::min( s->guide.train_paths, c.wave_paths );
+		s->guide.ensure_records( c.train_paths * ( c.max_bounce + 1 ) );
+		c.rec = s->guide.rec;
+	}
 	return r;
 }
 
-void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t st )
+void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t st, bool lobes = false )
 {
-	if ( s->wave.capacity >= cap && s->wave_bounces >= max_bounce ) return;
-	if ( s->wave.capacity ) free_wave( s->wave, st );
-	alloc_wave( s->wave, cap, max_bounce, st );
-	s->wave_bounces = max_bounce;
+	if ( !( s->wave.capacity >= cap && s->wave_bounces >= max_bounce ) )
+	{
+		if ( s->wave.capacity ) free_wave( s->wave, st );
+		alloc_wave( s->wave, cap, max_bounce, st );
+		s->wave_bounces = max_bounce;
+	}
+	if ( lobes ) alloc_lobes( s->wave, st );
 }
 
 void check_device_error( cr_scene *s, cudaStream_t st )
@@ -926,7 +944,8 @@ void fill_stats( cr_stats *out, const StageTimes &t, uint64_t samples )
 	if ( !out ) return;
 	std::memset( out, 0, sizeof *out );
 	out->ms_total = t.total, out->ms_extend = t.extend, out->ms_shadow = t.shadow, out->ms_shade = t.shade;
-	out->ms_other = t.other;
+	out->ms_other = t.other + t.guide;
+	out->ms_guide = t.guide;
 	out->samples = samples;
 	out->rays_extend = t.rays_extend, out->rays_shadow = t.rays_shadow;
 	out->nodes = t.nodes, out->tris = t.tris, out->shadow_nodes = t.shadow_nodes, out->shadow_tris = t.shadow_tris;
@@ -938,9 +957,9 @@ void render_device( cr_scene *s, const cr_render_desc *desc, double *sum, double
 					cr_stats *stats )
 {
 	Resolved r = resolve( s, desc );
-	ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st );
+	ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st, r.cfg.guiding );
 	StageTimes t;
-	render_waves( r.sc, r.cfg, s->wave, sum, sq, cnt, st, stats ? &t : nullptr );
+	render_waves( r.sc, r.cfg, s->wave, sum, sq, cnt, st, stats ? &t : nullptr, &s->guide );
 	if ( stats )
 	{
 		fill_stats( stats, t, r.samples );
@@ -1280,6 +1299,7 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		if ( spp != cfg.spp ) sc.cam = make_camera( s->cam, sc.cam.width, sc.cam.height, spp );
 		cfg.spp = spp;
 		cfg.count_work = false;
+		cfg.guiding = false;
 		uint64_t samples = uint64_t( cfg.ww ) * cfg.wh * cfg.spp;
 		size_t npx = size_t( cfg.ww ) * cfg.wh;
 		double *sum, *sq;
@@ -1327,6 +1347,83 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		out->candidates_tried = tried;
 		out->msamples_per_s = best;
 		out->default_msamples_per_s = dflt;
+	} );
+}
+
+int cr_guide_reset( cr_scene *s, uint64_t seed )
+{
+	return guarded( [&] {
+		if ( !s ) fail( CR_ERR_INVALID, "null scene" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		s->guide.init( s->box_lo, s->box_hi, seed );
+	} );
+}
+
+int cr_guide_info( const cr_scene *s, float *bmin, float *binv, uint32_t *step, uint32_t *sizes )
+{
+	return guarded( [&] {
+		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
+		if ( bmin ) bmin[ 0 ] = s->guide.bmin.x, bmin[ 1 ] = s->guide.bmin.y, bmin[ 2 ] = s->guide.bmin.z;
+		if ( binv ) binv[ 0 ] = s->guide.binv.x, binv[ 1 ] = s->guide.binv.y, binv[ 2 ] = s->guide.binv.z;
+		if ( step ) *step = s->guide.step;
+		if ( sizes )
+			sizes[ 0 ] = uint32_t( GuideState::grid_size() ), sizes[ 1 ] = uint32_t( GuideState::w_size() ),
+			sizes[ 2 ] = uint32_t( GuideState::b_size() );
+	} );
+}
+
+int cr_guide_params( cr_scene *s, float *grid, float *W, float *b, int set )
+{
+	return guarded( [&] {
+		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
+		auto io = [&]( float *host, float *dev, size_t n ) {
+			if ( !host ) return;
+			cuda_check( set ? cudaMemcpy( dev, host, n * 4, cudaMemcpyHostToDevice )
+							: cudaMemcpy( host, dev, n * 4, cudaMemcpyDeviceToHost ),
+						"guide params" );
+		};
+		io( grid, s->guide.grid, GuideState::grid_size() );
+		io( W, s->guide.W, GuideState::w_size() );
+		io( b, s->guide.b, GuideState::b_size() );
+	} );
+}
+
+int cr_guide_forward( cr_scene *s, const float *inputs, uint64_t n, float *out )
+{
+	return guarded( [&] {
+		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
+		if ( !n ) return;
+		if ( !inputs || !out ) fail( CR_ERR_INVALID, "null argument" );
+		float *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * ( 9 + G_OUT ) * n ), "cudaMalloc" );
+		cudaMemcpy( d, inputs, sizeof( float ) * 9 * n, cudaMemcpyHostToDevice );
+		s->guide.forward_batch( d, uint32_t( n ), d + 9 * n, nullptr );
+		cudaError_t e = cudaMemcpy( out, d + 9 * n, sizeof( float ) * G_OUT * n, cudaMemcpyDeviceToHost );
+		cudaFree( d );
+		cuda_check( e, "guide forward" );
+	} );
+}
+
+int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid )
+{
+	return guarded( [&] {
+		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
+		if ( !n || !records ) fail( CR_ERR_INVALID, "no records" );
+		float *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * 13 * n ), "cudaMalloc" );
+		cudaMemcpy( d, records, sizeof( float ) * 13 * n, cudaMemcpyHostToDevice );
+		GuideState &g = s->guide;
+		g.load_records( d, uint32_t( n ), nullptr );
+		g.gradients( uint32_t( n ), nullptr );
+		cuda_check( cudaDeviceSynchronize(), "guide gradients" );
+		if ( gW ) cudaMemcpy( gW, g.gW, GuideState::w_size() * 4, cudaMemcpyDeviceToHost );
+		if ( gb ) cudaMemcpy( gb, g.gb, GuideState::b_size() * 4, cudaMemcpyDeviceToHost );
+		if ( ggrid ) cudaMemcpy( ggrid, g.ggrid, GuideState::grid_size() * 4, cudaMemcpyDeviceToHost );
+		cudaMemset( g.gW, 0, GuideState::w_size() * 4 );
+		cudaMemset( g.gb, 0, GuideState::b_size() * 4 );
+		cudaError_t e = cudaMemset( g.ggrid, 0, GuideState::grid_size() * 4 );
+		cudaFree( d );
+		cuda_check( e, "guide gradients" );
 	} );
 }
 

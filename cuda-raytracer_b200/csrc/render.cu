@@ -26,6 +26,7 @@
 #include "cr_device.cuh"
 #include "render.h"
 #include "traverse.cuh"
+#include "guide.cuh"
 
 namespace cr
 {
@@ -320,9 +321,25 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 
 // One vertex of the MIS estimator (power heuristic over BSDF sampling and
 // area-light NEE; see cr_device.cuh for the BSDFs).
+__device__ __forceinline__ void load_lobes( const float *src, Lobe *lb )
+{
+	const float4 *p = reinterpret_cast<const float4 *>( src );
+	float v[ 5 * G_LOBES ];
+#pragma unroll
+	for ( int i = 0; i < 5 * G_LOBES / 4; ++i )
+	{
+		float4 q = p[ i ];
+		v[ 4 * i ] = q.x, v[ 4 * i + 1 ] = q.y, v[ 4 * i + 2 ] = q.z, v[ 4 * i + 3 ] = q.w;
+	}
+#pragma unroll
+	for ( int k = 0; k < G_LOBES; ++k )
+		lb[ k ].mu = f3( v[ 5 * k ], v[ 5 * k + 1 ], v[ 5 * k + 2 ] ), lb[ k ].kappa = v[ 5 * k + 3 ],
+		lb[ k ].weight = v[ 5 * k + 4 ];
+}
+
 __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
 										   uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
-										   float4 &L4, PathOut &out )
+										   float4 &L4, PathOut &out, const float *lobes, uint32_t rec_i )
 {
 	float3 o = f3( ro ), d = f3( rd );
 	Surface s = surface_at( sc, o, d, h, true );
@@ -348,6 +365,9 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	Frame fr = onb_frame( s.ns );
 	float3 wo = fr.local( -d );
 	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
+	Lobe lb[ G_LOBES ];
+	const float sel = cfg.guiding ? cfg.guide.select_prob : 0.f;
+	if ( cfg.guiding ) load_lobes( lobes, lb );
 	if ( sc.n_lights )
 	{
 		uint32_t nli = sc.n_lights;
@@ -367,6 +387,8 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 			float3 wi = fr.local( wiw );
 			float pb;
 			float3 f = mis_eval( sh, wo, wi, pb );
+			// one-sample MIS of guide and BSDF: the continuation density
+			if ( cfg.guiding ) pb = sel * mixture_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
 			if ( !is_zero( f ) )
 			{
 				float w = pl * pl / ( pl * pl + pb * pb );
@@ -391,9 +413,32 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	}
 	float3 wi;
 	float pdf;
-	float3 wt = mis_sample( sh, wo, r1.x, r1.y, wi, pdf );
+	float3 wt, nd;
+	if ( cfg.guiding )
+	{
+		// one-sample MIS: the guide with probability sel, else the BSDF; the
+		// weight uses the combined density of both strategies
+		if ( r1.z < sel )
+		{
+			nd = mixture_sample( lb, r1.w, r1.x, r1.y );
+			wi = fr.local( nd );
+		}
+		else
+		{
+			mis_sample( sh, wo, r1.x, r1.y, wi, pdf );
+			nd = fr.global( wi );
+		}
+		float pb;
+		float3 f = mis_eval( sh, wo, wi, pb );
+		pdf = sel * mixture_pdf( lb, nd ) + ( 1.f - sel ) * pb;
+		wt = pdf > 0.f ? f * ( wi.z / pdf ) : f3( 0.f, 0.f, 0.f );
+	}
+	else
+	{
+		wt = mis_sample( sh, wo, r1.x, r1.y, wi, pdf );
+		nd = fr.global( wi );
+	}
 	beta = beta * wt;
-	float3 nd = fr.global( wi );
 	bool alive = !is_zero( beta ) && dot( nd, s.ng ) > 0.f;
 	float rr = maxc( beta );
 	if ( alive && rr < 1.f && bounce > 3 )
@@ -406,6 +451,16 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	}
 	if ( bounce + 1 > cfg.max_bounce || !finite3( beta ) ) alive = false;
 	float3 no = offset_ray( s.p, s.ng );
+	if ( rec_i != 0xFFFFFFFFu )
+	{
+		// training record of this vertex (its radiance target follows once the
+		// rest of the path is known)
+		cfg.rec.x[ rec_i ] = make_float4( s.p.x, s.p.y, s.p.z, alive ? 1.f : 0.f );
+		cfg.rec.wo[ rec_i ] = make_float4( -d.x, -d.y, -d.z, 0.f );
+		cfg.rec.n[ rec_i ] = make_float4( s.ns.x, s.ns.y, s.ns.z, 0.f );
+		cfg.rec.om[ rec_i ] = make_float4( nd.x, nd.y, nd.z, pdf );
+		cfg.rec.T[ rec_i ] = make_float4( beta.x, beta.y, beta.z, 0.f );
+	}
 	beta4 = make_float4( beta.x, beta.y, beta.z, pdf );
 	L4 = make_float4( L.x, L.y, L.z, 0.f );
 	out.alive = alive;
@@ -431,6 +486,14 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 		{
 			path = q[ i ];
 			HitRec h = wb.hit[ path ];
+			const uint32_t stride = cfg.max_bounce + 1;
+			const bool recorded = cfg.guiding && path < cfg.train_paths;
+			if ( recorded && bounce > 0 )
+			{
+				// radiance gathered through the previous vertex (its shadow ray has run)
+				float4 Lp = wb.L[ path ];
+				cfg.rec.L[ path * stride + bounce - 1 ] = make_float4( Lp.x, Lp.y, Lp.z, 0.f );
+			}
 			if ( h.id != HIT_MISS )
 			{
 				float4 beta = wb.beta[ path ], L = wb.L[ path ];
@@ -441,7 +504,9 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 				uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
 				uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
 				if ( cfg.estimator == EST_MIS )
-					shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
+					shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
+							   cfg.guiding ? wb.lobes + size_t( path ) * 5 * G_LOBES : nullptr,
+							   recorded ? path * stride + bounce : 0xFFFFFFFFu );
 				else
 					shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
 				wb.beta[ path ] = beta;
@@ -463,6 +528,37 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 		if ( out.shadow ) wb.shadow_queue[ si ] = path;
 		uint32_t ni = warp_append( out.alive, next_count );
 		if ( out.alive ) nq[ ni ] = path;
+	}
+}
+
+// Guide inference for the paths of one bounce that hit a surface: inputs as
+// the MIS shading sees them (position, outgoing direction, two-sided shading
+// normal), FP32 forward pass, mixture parameters per path.
+__global__ void k_guide_infer( DevScene sc, RenderConfig cfg, WaveBuffers wb, uint32_t bounce )
+{
+	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
+	const uint32_t *q = wb.queue[ bounce & 1 ];
+	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
+	{
+		uint32_t path = q[ i ];
+		HitRec h = wb.hit[ path ];
+		if ( h.id == HIT_MISS ) continue;
+		float3 o = f3( wb.ray_o[ path ] ), d = f3( wb.ray_d[ path ] );
+		Surface s = surface_at( sc, o, d, h, true );
+		if ( dot( s.ng, d ) > 0.f ) s.ng = -s.ng;
+		if ( dot( s.ns, s.ng ) < 0.f ) s.ns = -s.ns;
+		float in[ G_IN ], outv[ G_OUT ];
+		guide_encode( cfg.guide, s.p, -d, s.ns, in );
+		guide_forward_fp32( cfg.guide.W, cfg.guide.b, in, outv, nullptr );
+		Lobe lb[ G_LOBES ];
+		lobes_from_output( outv, lb );
+		float4 *dst = reinterpret_cast<float4 *>( wb.lobes + size_t( path ) * 5 * G_LOBES );
+		float v[ 5 * G_LOBES ];
+		for ( int k = 0; k < G_LOBES; ++k )
+			v[ 5 * k ] = lb[ k ].mu.x, v[ 5 * k + 1 ] = lb[ k ].mu.y, v[ 5 * k + 2 ] = lb[ k ].mu.z,
+					v[ 5 * k + 3 ] = lb[ k ].kappa, v[ 5 * k + 4 ] = lb[ k ].weight;
+		for ( int j = 0; j < 5 * G_LOBES / 4; ++j )
+			dst[ j ] = make_float4( v[ 4 * j ], v[ 4 * j + 1 ], v[ 4 * j + 2 ], v[ 4 * j + 3 ] );
 	}
 }
 
@@ -594,17 +690,27 @@ void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaSt
 void free_wave( WaveBuffers &wb, cudaStream_t st )
 {
 	void *ps[] = { wb.ray_o, wb.ray_d, wb.hit, wb.beta, wb.L, wb.queue[ 0 ], wb.queue[ 1 ], wb.shadow_queue,
-				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work };
+				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work, wb.lobes };
 	for ( void *p : ps )
 		if ( p ) cudaFreeAsync( p, st );
 	wb = WaveBuffers();
 }
 
-void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb, double *film_sum, double *film_sumsq,
-				   uint32_t *film_count, cudaStream_t st, StageTimes *times )
+void alloc_lobes( WaveBuffers &wb, cudaStream_t st )
 {
+	if ( wb.lobes ) return;
+	alloc( wb.lobes, size_t( wb.capacity ) * 5 * G_LOBES, st );
+}
+
+void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb, double *film_sum, double *film_sumsq,
+				   uint32_t *film_count, cudaStream_t st, StageTimes *times, GuideState *guide )
+{
+	if ( cfg.guiding && ( !guide || !wb.lobes || cfg.estimator != EST_MIS ) )
+		throw std::runtime_error( "guided render without a guide, lobe buffer or MIS estimator" );
 	const uint64_t total = uint64_t( cfg.ww ) * cfg.wh * cfg.spp;
-	const uint32_t P = wb.capacity;
+	if ( cfg.wave_paths == 0 || cfg.wave_paths > wb.capacity )
+		throw std::runtime_error( "wave size exceeds the allocated wave buffers" );
+	const uint32_t P = cfg.wave_paths;
 	const int sms = sm_count();
 	const int g_ext = sms * std::max( 1, std::min( 8, cfg.traverse_blocks_per_sm ) );
 	const int g_shade = sms * 8;
@@ -613,7 +719,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	struct Mark
 	{
 		cudaEvent_t a, b;
-		int kind;  // 0 extend 1 shadow 2 shade 3 other
+		int kind;  // 0 extend 1 shadow 2 shade 3 other 4 guide
 	};
 	std::vector<Mark> marks;
 	cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -644,6 +750,10 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	{
 		WaveArgs wa{ first, uint32_t( std::min<uint64_t>( P, total - first ) ) };
 		check( cudaMemsetAsync( wb.counters, 0, sizeof( uint32_t ) * wb.n_counters, st ), "memset" );
+		const uint32_t train_n = cfg.guiding ? std::min( cfg.train_paths, wa.n ) : 0;
+		if ( train_n )
+			check( cudaMemsetAsync( cfg.rec.x, 0, sizeof( float4 ) * size_t( train_n ) * ( cfg.max_bounce + 1 ), st ),
+				   "memset" );
 		timed( 3, [&] {
 			int gg = int( std::min<uint64_t>( ( wa.n + 255 ) / 256, uint64_t( sms ) * 16 ) );
 			k_generate<<<gg, 256, 0, st>>>( sc, cfg, wb, wa );
@@ -659,6 +769,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				else
 					k_traverse<ExtendIO, false, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 			} );
+			if ( cfg.guiding )
+				timed( 4, [&] { k_guide_infer<<<g_shade, 128, 0, st>>>( sc, cfg, wb, b ); } );
 			timed( 2, [&] { k_shade<<<g_shade, 128, 0, st>>>( sc, cfg, wb, wa, b, key ); } );
 			if ( sc.n_lights )
 				timed( 1, [&] {
@@ -671,6 +783,12 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 						k_traverse<ShadowIO, true, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 				} );
 		}
+		if ( train_n )
+			timed( 4, [&] {
+				// online training on this wave's recorded vertices
+				guide->compute_targets( wb.L, train_n, cfg.max_bounce + 1, st );
+				guide->train_from_records( train_n * ( cfg.max_bounce + 1 ), st );
+			} );
 		timed( 3, [&] {
 			uint64_t npx = ( first + wa.n - 1 ) / cfg.spp - first / cfg.spp + 1;
 			int gg = int( std::min<uint64_t>( ( npx + 255 ) / 256, uint64_t( sms ) * 16 ) );
@@ -702,7 +820,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		for ( auto &m : marks )
 		{
 			check( cudaEventElapsedTime( &ms, m.a, m.b ), "event" );
-			( m.kind == 0 ? times->extend : m.kind == 1 ? times->shadow : m.kind == 2 ? times->shade : times->other ) += ms;
+			( m.kind == 0 ? times->extend : m.kind == 1 ? times->shadow : m.kind == 2 ? times->shade
+																  : m.kind == 4 ? times->guide : times->other ) += ms;
 		}
 		if ( cfg.count_work )
 		{

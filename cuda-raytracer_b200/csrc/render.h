@@ -4,6 +4,7 @@
 #include <cstdint>
 
 #include "cr_common.h"
+#include "guide.h"
 
 struct cr_hit;
 
@@ -24,6 +25,7 @@ struct WaveBuffers
 	uint32_t n_counters = 0;
 	uint32_t *err = nullptr;                    // device error word
 	unsigned long long *work = nullptr;         // extension [0] nodes [1] triangles, shadow [2] [3]
+	float *lobes = nullptr;                     // guided renders: 8 lobes x (mean, kappa, weight) per path
 };
 
 // Device counters per bounce: queue lengths and the traversal kernels' work cursors.
@@ -39,13 +41,17 @@ struct RenderConfig
 	uint64_t seed;
 	uint32_t wave_paths;
 	bool count_work;
+	bool guiding = false;            // learned guide mixed with BSDF sampling (MIS estimator)
+	GuideDev guide{};
+	GuideRecords rec{};              // training records of the first train_paths paths of a wave
+	uint32_t train_paths = 0;
 	uint32_t refill_min = 16;        // traversal: idle lanes per warp that trigger a refill (1..32)
 	int traverse_blocks_per_sm = 8;  // traversal grid = SMs x this (1..8; 128-thread blocks)
 };
 
 struct StageTimes
 {
-	double extend = 0, shadow = 0, shade = 0, other = 0, total = 0;
+	double extend = 0, shadow = 0, shade = 0, other = 0, total = 0, guide = 0;
 	uint32_t launches = 0, waves = 0, extend_launches = 0, shadow_launches = 0;
 	uint64_t rays_extend = 0, rays_shadow = 0, nodes = 0, tris = 0, shadow_nodes = 0, shadow_tris = 0;
 };
@@ -57,7 +63,9 @@ void free_wave( WaveBuffers &wb, cudaStream_t st );
 // `times` is not null, stage times are measured with CUDA events and the
 // call synchronises `st` at the end.
 void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb, double *film_sum,
-				   double *film_sumsq, uint32_t *film_count, cudaStream_t st, StageTimes *times );
+				   double *film_sumsq, uint32_t *film_count, cudaStream_t st, StageTimes *times,
+				   GuideState *guide = nullptr );
+void alloc_lobes( WaveBuffers &wb, cudaStream_t st );
 
 void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit,
 				   cr_hit *out, uint32_t *err, cudaStream_t st );

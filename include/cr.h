@@ -78,6 +78,7 @@ typedef struct cr_stats {
     double ms_shadow;      /* any-hit (shadow) traversal kernels              */
     double ms_shade;       /* shading / NEE / queue compaction kernels        */
     double ms_other;       /* generation, film accumulation, guiding          */
+    double ms_guide;       /* guide inference and training (part of ms_other) */
     uint64_t samples;      /* camera paths traced                             */
     uint64_t rays_extend;  /* closest-hit queries                             */
     uint64_t rays_shadow;  /* any-hit queries                                 */
@@ -203,6 +204,26 @@ int cr_render_device_noalloc(cr_scene *s, const cr_render_desc *desc, double *d_
  * events.  The choice is stored in the scene and returned in *out.
  * Synchronises `stream`; allocates temporary device buffers. */
 int cr_autotune(cr_scene *s, const cr_render_desc *desc, void *stream, cr_tuning *out);
+
+/* ------------------------------------------------------ learned guiding */
+/* No counterpart in the reference.  A committed scene owns one path guide:
+ * a 12-level hash-grid + SH encoding feeding a 4 x 64 MLP whose output is a
+ * mixture of 8 von Mises-Fisher lobes over incident directions.  Renders with
+ * desc->guiding = 1 (MIS estimator) sample it by one-sample MIS with the BSDF
+ * and train it online (Adam) on their own path vertices; it persists across
+ * renders of the scene.  cr_guide_reset (re)initialises it from `seed`. */
+int cr_guide_reset(cr_scene *s, uint64_t seed);
+/* Normalisation box (x -> (x - bmin) * binv), training steps taken, and the
+ * sizes (in floats) of the grid, weight and bias arrays. */
+int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, uint32_t *sizes);
+/* Copy the parameters out (set = 0) or in (set = 1); NULL arrays are skipped.
+ * grid: [12][65536][2], W: [5][64 out][64 in], b: [5][64]. */
+int cr_guide_params(cr_scene *s, float *grid, float *W, float *b, int set);
+/* Network outputs (n x 64, FP32 path) for inputs n x {x, wo, n} (9 floats). */
+int cr_guide_forward(cr_scene *s, const float *inputs, uint64_t n, float *out);
+/* Gradients of the weighted mixture NLL over records n x {x, wo, n, w, weight}
+ * (13 floats), normalised by the total weight; parameters are not updated. */
+int cr_guide_gradients(cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid);
 
 /* Renderer::render (src/core/renderer/renderer.cu:13-52): load a scene file,
  * render it with the configured kernel and tracer, write the reference's

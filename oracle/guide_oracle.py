@@ -1,0 +1,178 @@
+"""FP64 restatement of the learned path guide (TEST INFRASTRUCTURE ONLY).
+
+Restates, in double precision with numpy, what the CUDA guide computes
+(cuda-raytracer_b200/csrc/guide.cuh, guide.cu), so that its forward outputs
+and its gradients can be checked:
+
+* encoding: 12-level hash grid (resolution floor(4 * 1.5**l), direct indexing
+  where the lattice fits 2**16 entries, else the xor-of-primes spatial hash),
+  2 features per level, trilinear; 16 real SH terms of wo; the normal; zeros
+  up to 64 inputs;
+* MLP: 5 linear layers 64 -> 64, ReLU after the first four;
+* output: 8 vMF lobes (normalised mean, softplus concentration clamped to
+  [0.05, 5000], softmax weights);
+* loss: sum_r w_r * -log q(w_r) / sum_r w_r, and its exact gradients.
+
+The reference has no learned component; this module is checked against
+finite differences of its own loss (tests/test_oracle_guide.py).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+LEVELS, FEAT, LOG2T = 12, 2, 16
+T = 1 << LOG2T
+IN = HID = OUT = 64
+LAYERS, LOBES = 5, 8
+ENC, SH = LEVELS * FEAT, 16
+KMIN, KMAX = 0.05, 5000.0
+
+
+def grid_res(l):
+    r = np.float32(4.0)
+    for _ in range(l):
+        r = np.float32(r * np.float32(1.5))
+    return float(np.floor(r))
+
+
+def grid_index(l, ix, iy, iz):
+    res = int(grid_res(l)) + 1
+    if res ** 3 <= T:
+        return (ix + res * (iy + res * iz)) & 0xFFFFFFFF
+    h = (ix * 1) ^ ((iy * 2654435761) & 0xFFFFFFFF) ^ ((iz * 805459861) & 0xFFFFFFFF)
+    return h & (T - 1)
+
+
+def sh16(x, y, z):
+    c0, c1 = 0.28209479177387814, 0.4886025119029199
+    c2a, c2b, c2c = 1.0925484305920792, 0.31539156525252005, 0.5462742152960396
+    c3a, c3b, c3c, c3d, c3e = 0.5900435899266435, 2.890611442640554, 0.4570457994644658, 0.3731763325901154, 1.445305721320277
+    xx, yy, zz = x * x, y * y, z * z
+    return np.array([c0, -c1 * y, c1 * z, -c1 * x,
+                     c2a * x * y, -c2a * y * z, c2b * (3 * zz - 1), -c2a * x * z, c2c * (xx - yy),
+                     -c3a * y * (3 * xx - yy), c3b * x * y * z, -c3c * y * (5 * zz - 1), c3d * z * (5 * zz - 3),
+                     -c3c * x * (5 * zz - 1), c3e * z * (xx - yy), -c3a * x * (xx - 3 * yy)])
+
+
+def corners(l, u):
+    res = grid_res(l)
+    p = np.clip(u, 0.0, 1.0) * res
+    f = np.floor(p)
+    i = f.astype(np.int64)
+    t = p - f
+    idx, w = [], []
+    for k in range(8):
+        d = ((k & 1), (k >> 1) & 1, (k >> 2) & 1)
+        idx.append(grid_index(l, int(i[0] + d[0]), int(i[1] + d[1]), int(i[2] + d[2])))
+        w.append((t[0] if d[0] else 1 - t[0]) * (t[1] if d[1] else 1 - t[1]) * (t[2] if d[2] else 1 - t[2]))
+    return idx, w
+
+
+def encode(grid, bmin, binv, x, wo, n):
+    """grid: (LEVELS, T, FEAT) float64."""
+    u = (np.asarray(x, np.float64) - bmin) * binv
+    v = np.zeros(IN)
+    cs = []
+    for l in range(LEVELS):
+        idx, w = corners(l, u)
+        cs.append((idx, w))
+        for k in range(8):
+            v[2 * l:2 * l + 2] += w[k] * grid[l, idx[k]]
+    v[ENC:ENC + SH] = sh16(*np.asarray(wo, np.float64))
+    v[ENC + SH:ENC + SH + 3] = n
+    return v, cs
+
+
+def forward(W, b, h0):
+    """W: (LAYERS, 64, 64), b: (LAYERS, 64). Returns output and pre-activations z_1..z_4."""
+    zs, h = [], h0
+    for l in range(LAYERS):
+        z = W[l] @ h + b[l]
+        if l == LAYERS - 1:
+            return z, zs
+        zs.append(z)
+        h = np.maximum(z, 0.0)
+
+
+def softplus(x):
+    return x if x > 20 else np.log1p(np.exp(x))
+
+
+def lobes(o):
+    mus, kaps, logits = [], [], []
+    for k in range(LOBES):
+        m = o[5 * k:5 * k + 3]
+        mus.append(m / np.linalg.norm(m))
+        kaps.append(min(max(softplus(o[5 * k + 3]), KMIN), KMAX))
+        logits.append(o[5 * k + 4])
+    logits = np.array(logits)
+    w = np.exp(logits - logits.max())
+    return np.array(mus), np.array(kaps), w / w.sum()
+
+
+def vmf(mu, kap, w):
+    return kap / (2 * np.pi * (-np.expm1(-2 * kap))) * np.exp(kap * (mu @ w - 1))
+
+
+def mixture_pdf(o, w):
+    mus, kaps, pis = lobes(o)
+    return sum(pis[k] * vmf(mus[k], kaps[k], w) for k in range(LOBES))
+
+
+def nll_grad(o, w, scale):
+    """d(-scale * log q(w)) / d o  (first 40 outputs; the rest are zero)."""
+    mus, kaps, pis = lobes(o)
+    v = np.array([vmf(mus[k], kaps[k], w) for k in range(LOBES)])
+    q = max((pis * v).sum(), 1e-300)
+    g = np.zeros(OUT)
+    for k in range(LOBES):
+        gam = pis[k] * v[k] / q
+        g[5 * k + 4] = scale * (pis[k] - gam)
+        raw = o[5 * k + 3]
+        sp = softplus(raw)
+        clamped = sp < KMIN or sp > KMAX
+        kap = kaps[k]
+        dlogv = 1 / kap - 2 / np.expm1(2 * kap) + mus[k] @ w - 1
+        sig = 1 / (1 + np.exp(-raw))
+        g[5 * k + 3] = 0.0 if clamped else -scale * gam * dlogv * sig
+        m = o[5 * k:5 * k + 3]
+        ln = np.linalg.norm(m)
+        g[5 * k:5 * k + 3] = -scale * gam * kap * (w - mus[k] * (mus[k] @ w)) / ln
+    return g
+
+
+def loss(grid, W, b, bmin, binv, records):
+    """Weighted NLL of records (n x 13: x, wo, n, w, weight), normalised."""
+    tot = sum(r[12] for r in records if r[12] > 0)
+    s = 0.0
+    for r in records:
+        if r[12] <= 0:
+            continue
+        h0, _ = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
+        o, _ = forward(W, b, h0)
+        s += r[12] * -np.log(mixture_pdf(o, r[9:12]))
+    return s / tot
+
+
+def gradients(grid, W, b, bmin, binv, records):
+    """Exact gradients of `loss` with respect to W, b and the grid."""
+    gW, gb, ggrid = np.zeros_like(W), np.zeros_like(b), np.zeros_like(grid)
+    tot = sum(r[12] for r in records if r[12] > 0)
+    for r in records:
+        if r[12] <= 0:
+            continue
+        h0, cs = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
+        o, zs = forward(W, b, h0)
+        dz = nll_grad(o, np.asarray(r[9:12], np.float64), r[12] / tot)
+        for l in range(LAYERS - 1, -1, -1):
+            h = h0 if l == 0 else np.maximum(zs[l - 1], 0.0)
+            gW[l] += np.outer(dz, h)
+            gb[l] += dz
+            dh = W[l].T @ dz
+            if l > 0:
+                dz = dh * (zs[l - 1] > 0)
+            else:
+                for lv, (idx, w) in enumerate(cs):
+                    for k in range(8):
+                        ggrid[lv, idx[k]] += w[k] * dh[2 * lv:2 * lv + 2]
+    return gW, gb, ggrid

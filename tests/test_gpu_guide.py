@@ -1,0 +1,91 @@
+"""The CUDA path guide against the FP64 guide oracle (forward outputs and
+training gradients), and guided rendering against plain MIS rendering (the
+guide changes the variance, never the expectation)."""
+import numpy as np
+import pytest
+
+import guide_oracle as G
+import oracle as O
+from conftest import require_gpu
+from gpu_util import render_film, zscores
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def guided(cr, scenes):
+    require_gpu()
+    s = cr.Scene.from_desc(scenes.config0())
+    g = cr.Guide(s).reset(seed=5)
+    rng = np.random.default_rng(7)
+    grid = rng.uniform(-0.5, 0.5, (G.LEVELS, G.T, G.FEAT)).astype(np.float32)
+    W = rng.uniform(-0.3, 0.3, (G.LAYERS, 64, 64)).astype(np.float32)
+    W[0][:, 43:] = 0
+    b = rng.uniform(-0.1, 0.1, (G.LAYERS, 64)).astype(np.float32)
+    g.set_params(grid, W, b)
+    info = g.info()
+    return s, g, grid.astype(np.float64), W.astype(np.float64), b.astype(np.float64), info
+
+
+def _inputs(rng, n):
+    x = rng.uniform(0.5, 5.0, (n, 3))
+    wo = rng.normal(size=(n, 3)); wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    nn = rng.normal(size=(n, 3)); nn /= np.linalg.norm(nn, axis=1, keepdims=True)
+    return np.concatenate([x, wo, nn], 1).astype(np.float32)
+
+
+def test_forward_matches_fp64(guided):
+    s, g, grid, W, b, info = guided
+    rng = np.random.default_rng(1)
+    inp = _inputs(rng, 200)
+    out = g.forward(inp)
+    for i in range(0, 200, 5):
+        h0, _ = G.encode(grid, info["bmin"].astype(np.float64), info["binv"].astype(np.float64),
+                         inp[i, :3].astype(np.float64), inp[i, 3:6].astype(np.float64), inp[i, 6:9].astype(np.float64))
+        ref, _ = G.forward(W, b, h0)
+        np.testing.assert_allclose(out[i], ref, rtol=2e-4, atol=2e-4 * np.abs(ref).max())
+
+
+def test_gradients_match_fp64(guided):
+    s, g, grid, W, b, info = guided
+    rng = np.random.default_rng(2)
+    n = 64
+    inp = _inputs(rng, n)
+    om = rng.normal(size=(n, 3)); om /= np.linalg.norm(om, axis=1, keepdims=True)
+    wts = rng.uniform(0.05, 3.0, n)
+    wts[::9] = 0.0  # some records carry no weight
+    recs = np.concatenate([inp, om, wts[:, None]], 1).astype(np.float32)
+    ggrid, gW, gb = g.gradients(recs)
+    rW, rb, rgrid = G.gradients(grid, W, b, info["bmin"].astype(np.float64), info["binv"].astype(np.float64),
+                                recs.astype(np.float64))
+    for got, ref in ((gW, rW), (gb, rb), (ggrid, rgrid)):
+        got = got.reshape(ref.shape)
+        rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert rel < 2e-3, rel
+
+
+def test_guided_render_is_unbiased(cr, scenes):
+    """Guided MIS and plain MIS films agree within 3 sigma: one-sample MIS of
+    the learned mixture with the BSDF keeps the estimator unbiased while the
+    guide trains online during the render."""
+    require_gpu()
+    d = scenes.config0()
+    s = cr.Scene.from_desc(d)
+    cr.Guide(s).reset(seed=3)
+    W, H, spp = 32, 32, 256
+    plain = render_film(cr, s, W, H, spp, seeds=[21, 22], estimator=cr.MIS)
+    import torch
+    n = W * H
+    acc = [torch.zeros(n * 3, dtype=torch.float64, device="cuda"), torch.zeros(n * 3, dtype=torch.float64, device="cuda"),
+           torch.zeros(n, dtype=torch.int32, device="cuda")]
+    for seed in (31, 32):
+        desc = cr.render_desc(W, H, spp, max_bounce=7, estimator=cr.MIS, seed=seed, guiding=True, wave_paths=65536)
+        s.render_device(desc, acc[0].data_ptr(), acc[1].data_ptr(), acc[2].data_ptr(),
+                        stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    guided = O.Film(acc[0].cpu().numpy().reshape(H, W, 3), acc[1].cpu().numpy().reshape(H, W, 3),
+                    acc[2].cpu().numpy().astype(np.uint32).reshape(H, W))
+    assert cr.Guide(s).info()["step"] >= 8  # trained once per wave
+    z = zscores(guided, plain)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert abs(guided.mean.mean() / plain.mean.mean() - 1) < 0.01
