@@ -64,7 +64,16 @@ class Stats(C.Structure):
                 ("ms_shade", C.c_double), ("ms_other", C.c_double), ("ms_guide", C.c_double), ("samples", C.c_uint64),
                 ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64), ("nodes", C.c_uint64),
                 ("tris", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_tris", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32),
-                ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32)]
+                ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32), ("ms_guide_train", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GuideConfig(C.Structure):
+    """cr_guide_config: the guide's training schedule."""
+    _fields_ = [("lr", C.c_float), ("select_prob", C.c_float), ("train_paths", C.c_uint32),
+                ("steps_per_wave", C.c_uint32), ("warmup_steps", C.c_uint32), ("product_target", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -104,6 +113,8 @@ def lib():
             "cr_guide_reset": (I, [P, U64]), "cr_guide_info": (I, [P, P, P, P, P]),
             "cr_guide_params": (I, [P, P, P, P, I]), "cr_guide_forward": (I, [P, P, U64, P]),
             "cr_guide_gradients": (I, [P, P, U64, P, P, P]),
+            "cr_guide_configure": (I, [P, P, P]), "cr_guide_loss": (I, [P, P]),
+            "cr_guide_forward_tc": (I, [P, P, U64, P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
         }
@@ -272,11 +283,32 @@ class Guide:
         ptrs = [None if a is None else _p(a) for a in arrs]
         _check(lib().cr_guide_params(self.scene.h, *ptrs, 1))
 
-    def forward(self, inputs):
+    def forward(self, inputs, tensor_cores=False):
+        """Network outputs (n x 64) for n x {x, wo, n}: FP32 CUDA-core path, or
+        the BF16 tensor-core path the renderer samples with."""
         inputs = np.ascontiguousarray(inputs, np.float32)
         out = np.zeros((len(inputs), 64), np.float32)
-        _check(lib().cr_guide_forward(self.scene.h, _p(inputs), len(inputs), _p(out)))
+        fn = lib().cr_guide_forward_tc if tensor_cores else lib().cr_guide_forward
+        _check(fn(self.scene.h, _p(inputs), len(inputs), _p(out)))
         return out
+
+    def configure(self, **kw):
+        """cr_guide_configure: set the given schedule fields, return the schedule."""
+        cur = GuideConfig()
+        _check(lib().cr_guide_configure(self.scene.h, None, C.byref(cur)))
+        if kw:
+            for k, v in kw.items():
+                if k not in dict(GuideConfig._fields_):
+                    raise KeyError(k)
+                setattr(cur, k, v)
+            _check(lib().cr_guide_configure(self.scene.h, C.byref(cur), C.byref(cur)))
+        return cur.as_dict()
+
+    def loss(self):
+        """Weighted NLL of the last training batch."""
+        v = C.c_float()
+        _check(lib().cr_guide_loss(self.scene.h, C.byref(v)))
+        return v.value
 
     def gradients(self, records):
         records = np.ascontiguousarray(records, np.float32)

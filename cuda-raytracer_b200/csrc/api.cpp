@@ -912,8 +912,11 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 		if ( !s->guide.ready ) s->guide.init( s->box_lo, s->box_hi, 0x9E3779B9ull );
 		c.guiding = true;
 		c.guide = s->guide.dev();
-		c.train_paths = std::min( s->guide.train_paths, c.wave_paths );
-		s->guide.ensure_records( c.train_paths * ( c.max_bounce + 1 ) );
+		const uint64_t rec_paths =
+			std::min<uint64_t>( uint64_t( s->guide.train_paths ) * s->guide.steps_per_wave, c.wave_paths );
+		const uint64_t slots = rec_paths * ( uint64_t( c.max_bounce ) + 1 );
+		if ( slots > ( 1ull << 28 ) ) fail( CR_ERR_INVALID, "guide training records exceed 2^28 vertices per wave" );
+		s->guide.ensure_records( uint32_t( slots ) );
 		c.rec = s->guide.rec;
 	}
 	return r;
@@ -936,7 +939,7 @@ void check_device_error( cr_scene *s, cudaStream_t st )
 	cuda_check( cudaMemcpyAsync( &e, s->wave.capacity ? s->wave.err : s->err.p, 4, cudaMemcpyDeviceToHost, st ), "error word" );
 	cuda_check( cudaStreamSynchronize( st ), "error word" );
 	if ( e ) fail( CR_ERR_DEVICE, "a traversal kernel reported error flags " + std::to_string( e ) +
-								  " (1: stack overflow, 2: node index or budget, 4: triangle index)" );
+								  " (1: stack overflow, 2: node index or budget, 4: triangle index, 8: guide MMA wait timed out)" );
 }
 
 void fill_stats( cr_stats *out, const StageTimes &t, uint64_t samples )
@@ -946,6 +949,7 @@ void fill_stats( cr_stats *out, const StageTimes &t, uint64_t samples )
 	out->ms_total = t.total, out->ms_extend = t.extend, out->ms_shadow = t.shadow, out->ms_shade = t.shade;
 	out->ms_other = t.other + t.guide;
 	out->ms_guide = t.guide;
+	out->ms_guide_train = t.guide_train;
 	out->samples = samples;
 	out->rays_extend = t.rays_extend, out->rays_shadow = t.rays_shadow;
 	out->nodes = t.nodes, out->tris = t.tris, out->shadow_nodes = t.shadow_nodes, out->shadow_tris = t.shadow_tris;
@@ -1372,6 +1376,42 @@ int cr_guide_info( const cr_scene *s, float *bmin, float *binv, uint32_t *step, 
 	} );
 }
 
+int cr_guide_configure( cr_scene *s, const cr_guide_config *in, cr_guide_config *out )
+{
+	return guarded( [&] {
+		if ( !s ) fail( CR_ERR_INVALID, "null scene" );
+		GuideState &g = s->guide;
+		if ( in )
+		{
+			if ( !( in->lr > 0.f && in->lr < 1.f ) ) fail( CR_ERR_INVALID, "guide lr must be in (0, 1)" );
+			if ( !( in->select_prob >= 0.f && in->select_prob < 1.f ) )
+				fail( CR_ERR_INVALID, "guide select_prob must be in [0, 1)" );
+			if ( in->train_paths < 1 || in->train_paths > ( 1u << 20 ) )
+				fail( CR_ERR_INVALID, "guide train_paths must be in [1, 2^20]" );
+			if ( in->steps_per_wave < 1 || in->steps_per_wave > 64 )
+				fail( CR_ERR_INVALID, "guide steps_per_wave must be in [1, 64]" );
+			g.lr = in->lr, g.select_prob = in->select_prob, g.train_paths = in->train_paths;
+			g.steps_per_wave = in->steps_per_wave, g.warmup_steps = in->warmup_steps;
+			g.product_target = in->product_target != 0;
+		}
+		if ( out )
+		{
+			out->lr = g.lr, out->select_prob = g.select_prob, out->train_paths = g.train_paths;
+			out->steps_per_wave = g.steps_per_wave, out->warmup_steps = g.warmup_steps;
+			out->product_target = g.product_target ? 1u : 0u;
+		}
+	} );
+}
+
+int cr_guide_loss( const cr_scene *s, float *loss )
+{
+	return guarded( [&] {
+		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
+		if ( !loss ) fail( CR_ERR_INVALID, "null argument" );
+		cuda_check( cudaMemcpy( loss, s->guide.loss, 4, cudaMemcpyDeviceToHost ), "guide loss" );
+	} );
+}
+
 int cr_guide_params( cr_scene *s, float *grid, float *W, float *b, int set )
 {
 	return guarded( [&] {
@@ -1404,6 +1444,34 @@ int cr_guide_forward( cr_scene *s, const float *inputs, uint64_t n, float *out )
 	} );
 }
 
+int cr_guide_forward_tc( cr_scene *s, const float *inputs, uint64_t n, float *out )
+{
+	return guarded( [&] {
+		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
+		if ( !n ) return;
+		if ( !inputs || !out ) fail( CR_ERR_INVALID, "null argument" );
+		if ( n > ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many inputs" );
+		// outputs after the inputs, at a 256-byte boundary: the kernel stores them as float4
+		const size_t out_off = ( 9 * n + 63 ) / 64 * 64;
+		float *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * ( out_off + G_OUT * n ) ), "cudaMalloc" );
+		uint32_t e = 0;
+		try
+		{
+			cuda_check( cudaMemcpy( d, inputs, sizeof( float ) * 9 * n, cudaMemcpyHostToDevice ), "guide forward" );
+			e = s->guide.forward_batch_tc( d, uint32_t( n ), d + out_off, nullptr );
+			cuda_check( cudaMemcpy( out, d + out_off, sizeof( float ) * G_OUT * n, cudaMemcpyDeviceToHost ), "guide forward" );
+		}
+		catch ( ... )
+		{
+			cudaFree( d );
+			throw;
+		}
+		cudaFree( d );
+		if ( e ) fail( CR_ERR_DEVICE, "guide tensor-core forward: an MMA wait timed out (error word " + std::to_string( e ) + ")" );
+	} );
+}
+
 int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid )
 {
 	return guarded( [&] {
@@ -1414,7 +1482,7 @@ int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW
 		cudaMemcpy( d, records, sizeof( float ) * 13 * n, cudaMemcpyHostToDevice );
 		GuideState &g = s->guide;
 		g.load_records( d, uint32_t( n ), nullptr );
-		g.gradients( uint32_t( n ), nullptr );
+		g.gradients( g.rec, uint32_t( n ), nullptr );
 		cuda_check( cudaDeviceSynchronize(), "guide gradients" );
 		if ( gW ) cudaMemcpy( gW, g.gW, GuideState::w_size() * 4, cudaMemcpyDeviceToHost );
 		if ( gb ) cudaMemcpy( gb, g.gb, GuideState::b_size() * 4, cudaMemcpyDeviceToHost );

@@ -2,9 +2,12 @@
 //
 // Training data are the tracer's own path vertices.  For a vertex with inputs
 // (x, wo, n) that continued along direction w sampled with density p, the
-// incident radiance estimate is Li = (L_path - L_after_vertex) / T, where T is
-// the path throughput after the vertex and L_after_vertex the radiance the
-// path had gathered up to and including that vertex.  The network is fitted by
+// incident radiance estimate is Li = (L_path - L_next) / T, where T is the
+// path throughput after the vertex and L_next the radiance the path had
+// gathered once it reached the next vertex, that vertex's emission included.
+// Li is thus the light arriving through other surfaces (indirect light); the
+// lights themselves are left to next-event estimation, so the guide does not
+// take their share away from it.  The network is fitted by
 // minimising the weighted negative log-likelihood
 //     sum_r w_r * -log q(w_r | x_r, wo_r, n_r) / sum_r w_r,   w_r = lum(Li_r) / p_r,
 // a Monte Carlo estimate of the KL divergence from the normalised incident
@@ -20,6 +23,7 @@
 
 #include "guide.cuh"
 #include "guide.h"
+#include "guide_tc.cuh"
 
 namespace cr
 {
@@ -33,10 +37,10 @@ void check( cudaError_t e, const char *what )
 constexpr int ROW = G_HID + 1;  // padded shared-memory row (floats): conflict-free row access
 constexpr int TRAIN_ROWS = 128;
 
-__device__ __forceinline__ float lum( float3 c ) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
 // Radiance targets of the recorded vertices and the total weight.
-__global__ void k_guide_targets( GuideRecords rec, const float4 *L, uint32_t n_paths, uint32_t stride, float *wsum )
+__global__ void k_guide_targets( GuideRecords rec, const float4 *L, uint32_t n_paths, uint32_t stride, uint32_t j0,
+								 uint32_t rec_offset, uint32_t rec_stride, bool product, float *wsum )
 {
 	float local = 0.f;
 	uint32_t n = n_paths * stride;
@@ -44,9 +48,11 @@ __global__ void k_guide_targets( GuideRecords rec, const float4 *L, uint32_t n_p
 	{
 		float4 x = rec.x[ r ];
 		if ( x.w <= 0.f ) continue;  // not a valid record
-		float4 Lf = L[ r / stride ], La = rec.L[ r ], T = rec.T[ r ], om = rec.om[ r ];
+		const uint32_t path = rec_offset + ( j0 + r / stride ) * rec_stride;
+		float4 Lf = L[ path ], La = rec.L[ r ], T = rec.T[ r ], om = rec.om[ r ];
 		float3 li = f3( ( Lf.x - La.x ) / T.x, ( Lf.y - La.y ) / T.y, ( Lf.z - La.z ) / T.z );
-		float w = fmaxf( lum( li ), 0.f ) / om.w;
+		// incident radiance Li, or the product Li f cos (the integrand), per unit density
+		float w = fmaxf( lum( li ), 0.f ) / om.w * ( product ? rec.wo[ r ].w : 1.f );
 		if ( !isfinite( w ) || !finite3( f3( Lf ) ) ) w = 0.f;
 		rec.x[ r ].w = w > 0.f ? 1.f : 0.f;
 		rec.T[ r ].w = w;
@@ -61,7 +67,7 @@ __global__ void k_guide_targets( GuideRecords rec, const float4 *L, uint32_t n_p
 // block; activations live in shared memory (rows padded to 65 floats).
 __global__ void __launch_bounds__( TRAIN_ROWS ) k_guide_train_fp32( GuideRecords rec, uint32_t n, GuideDev g,
 																	const float *wsum, float *gW, float *gb,
-																	float *ggrid )
+																	float *ggrid, float *loss )
 {
 	extern __shared__ float sm[];
 	float *H0 = sm;                               // inputs          [128][65]
@@ -86,10 +92,13 @@ __global__ void __launch_bounds__( TRAIN_ROWS ) k_guide_train_fp32( GuideRecords
 		for ( int l = 0; l < 4; ++l )
 			for ( int i = 0; i < G_HID; ++i ) Z[ ( l * TRAIN_ROWS + m ) * ROW + i ] = acts[ l * G_HID + i ];
 		float g_out[ G_OUT ];
+		float nll = 0.f;
 		if ( w > 0.f )
-			mixture_nll_grad( out, om, w, g_out );
+			nll = -w * logf( mixture_nll_grad( out, om, w, g_out ) );
 		else
 			for ( int i = 0; i < G_OUT; ++i ) g_out[ i ] = 0.f;
+		for ( int o = 16; o; o >>= 1 ) nll += __shfl_xor_sync( 0xFFFFFFFFu, nll, o );
+		if ( ( m & 31 ) == 0 && nll != 0.f ) atomicAdd( loss, nll );
 		for ( int i = 0; i < G_OUT; ++i ) DZ[ m * ROW + i ] = g_out[ i ];
 		__syncthreads();
 		for ( int l = G_LAYERS - 1; l >= 0; --l )
@@ -185,6 +194,35 @@ __global__ void k_guide_forward_batch( GuideDev g, const float *inp, uint32_t n,
 	}
 }
 
+// FP32 master weights [G_LAYERS][64 out][64 in] -> the BF16 shared-memory image
+// of the tensor-core forward (layer l at l * W_BYTES, element (out, in) at
+// canon(out, in)).
+__global__ void k_pack_weights_bf16( const float *__restrict__ W, uint8_t *__restrict__ Wp )
+{
+	for ( uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < uint32_t( G_LAYERS * G_W ); e += gridDim.x * blockDim.x )
+	{
+		uint32_t l = e / G_W, o = ( e % G_W ) / G_IN, in = e % G_IN;
+		*reinterpret_cast<__nv_bfloat16 *>( Wp + l * tc::W_BYTES + tc::canon( o, in ) ) = __float2bfloat16_rn( W[ e ] );
+	}
+}
+
+__global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_forward_batch_tc( GuideDev g, const uint8_t *Wp,
+																			   const float *inp, uint32_t n,
+																			   float *out, uint32_t *err )
+{
+	auto src = [&]( uint32_t i, float3 &x, float3 &wo, float3 &nrm ) -> bool {
+		const float *q = inp + 9 * size_t( i );
+		x = f3( q[ 0 ], q[ 1 ], q[ 2 ] ), wo = f3( q[ 3 ], q[ 4 ], q[ 5 ] ), nrm = f3( q[ 6 ], q[ 7 ], q[ 8 ] );
+		return true;
+	};
+	auto sink = [&]( uint32_t i, const float *o ) {
+		// out is 16-byte aligned (checked by the host) and rows are 256 bytes
+		float4 *dst = reinterpret_cast<float4 *>( out + G_OUT * size_t( i ) );
+		for ( int j = 0; j < G_OUT / 4; ++j ) dst[ j ] = make_float4( o[ 4 * j ], o[ 4 * j + 1 ], o[ 4 * j + 2 ], o[ 4 * j + 3 ] );
+	};
+	tc::mlp_forward_tc( g, Wp, n, src, sink, err );
+}
+
 __global__ void k_records_from_host( GuideRecords rec, const float *src, uint32_t n )
 {
 	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
@@ -233,7 +271,8 @@ void GuideState::init( float3 lo, float3 hi, uint64_t seed )
 	dalloc( grid, grid_size() ), dalloc( grid_m, grid_size() ), dalloc( grid_v, grid_size() ), dalloc( ggrid, grid_size() );
 	dalloc( W, w_size() ), dalloc( W_m, w_size() ), dalloc( W_v, w_size() ), dalloc( gW, w_size() );
 	dalloc( b, b_size() ), dalloc( b_m, b_size() ), dalloc( b_v, b_size() ), dalloc( gb, b_size() );
-	dalloc( wsum, 1 );
+	dalloc( wsum, 1 ), dalloc( loss, 1 ), dalloc( err, 1 ), dalloc( Wp, size_t( tc::W_BYTES ) * G_LAYERS );
+	check( cudaMemset( loss, 0, 4 ), "guide init" );
 	std::mt19937_64 rng( seed );
 	std::uniform_real_distribution<float> ug( -1e-4f, 1e-4f );
 	std::vector<float> h( grid_size() );
@@ -254,14 +293,18 @@ void GuideState::init( float3 lo, float3 hi, uint64_t seed )
 	for ( float *p : { W_m, W_v, gW } ) check( cudaMemset( p, 0, w_size() * 4 ), "guide init" );
 	for ( float *p : { b, b_m, b_v, gb } ) check( cudaMemset( p, 0, b_size() * 4 ), "guide init" );
 	step = 0;
+	waves = 0;
 	ready = true;
 }
 
 void GuideState::release()
 {
-	for ( float *p : { grid, grid_m, grid_v, ggrid, W, W_m, W_v, gW, b, b_m, b_v, gb, wsum } )
+	for ( float *p : { grid, grid_m, grid_v, ggrid, W, W_m, W_v, gW, b, b_m, b_v, gb, wsum, loss } )
 		if ( p ) cudaFree( p );
-	grid = grid_m = grid_v = ggrid = W = W_m = W_v = gW = b = b_m = b_v = gb = wsum = nullptr;
+	grid = grid_m = grid_v = ggrid = W = W_m = W_v = gW = b = b_m = b_v = gb = wsum = loss = nullptr;
+	if ( Wp ) cudaFree( Wp );
+	if ( err ) cudaFree( err );
+	Wp = nullptr, err = nullptr;
 	if ( rec.x ) free_records();
 	ready = false;
 }
@@ -289,15 +332,22 @@ void GuideState::free_records()
 	rec_capacity = 0;
 }
 
-void GuideState::compute_targets( const float4 *L, uint32_t n_paths, uint32_t stride, cudaStream_t st )
+void GuideState::train_step( const float4 *L, uint32_t j0, uint32_t n_paths, uint32_t stride, uint32_t rec_offset,
+							 uint32_t rec_stride, cudaStream_t st )
 {
+	GuideRecords r = rec;
+	const size_t first = size_t( j0 ) * stride;
+	for ( float4 **p : { &r.x, &r.wo, &r.n, &r.om, &r.T, &r.L } ) *p += first;
 	check( cudaMemsetAsync( wsum, 0, 4, st ), "guide targets" );
 	uint32_t n = n_paths * stride;
-	k_guide_targets<<<std::min<uint32_t>( ( n + 255 ) / 256, 2048 ), 256, 0, st>>>( rec, L, n_paths, stride, wsum );
+	k_guide_targets<<<std::min<uint32_t>( ( n + 255 ) / 256, 2048 ), 256, 0, st>>>( r, L, n_paths, stride, j0, rec_offset,
+																				 rec_stride, product_target, wsum );
 	check( cudaGetLastError(), "guide targets" );
+	gradients( r, n, st );
+	adam( st );
 }
 
-void GuideState::gradients( uint32_t n, cudaStream_t st )
+void GuideState::gradients( const GuideRecords &r, uint32_t n, cudaStream_t st )
 {
 	static bool attr = false;
 	if ( !attr )
@@ -308,7 +358,8 @@ void GuideState::gradients( uint32_t n, cudaStream_t st )
 	}
 	uint32_t blocks = std::min<uint32_t>( ( n + TRAIN_ROWS - 1 ) / TRAIN_ROWS, 148 * 2 );
 	if ( blocks == 0 ) return;
-	k_guide_train_fp32<<<blocks, TRAIN_ROWS, TRAIN_SMEM, st>>>( rec, n, dev(), wsum, gW, gb, ggrid );
+	check( cudaMemsetAsync( loss, 0, 4, st ), "guide train" );
+	k_guide_train_fp32<<<blocks, TRAIN_ROWS, TRAIN_SMEM, st>>>( r, n, dev(), wsum, gW, gb, ggrid, loss );
 	check( cudaGetLastError(), "guide train" );
 }
 
@@ -326,16 +377,42 @@ void GuideState::adam( cudaStream_t st )
 	check( cudaGetLastError(), "guide adam" );
 }
 
-void GuideState::train_from_records( uint32_t n, cudaStream_t st )
-{
-	gradients( n, st );
-	adam( st );
-}
-
 void GuideState::forward_batch( const float *d_in, uint32_t n, float *d_out, cudaStream_t st )
 {
 	k_guide_forward_batch<<<std::min<uint32_t>( ( n + 127 ) / 128, 4096 ), 128, 0, st>>>( dev(), d_in, n, d_out );
 	check( cudaGetLastError(), "guide forward" );
+}
+
+void GuideState::pack_weights( cudaStream_t st )
+{
+	k_pack_weights_bf16<<<( G_LAYERS * G_W + 255 ) / 256, 256, 0, st>>>( W, Wp );
+	check( cudaGetLastError(), "guide weight packing" );
+}
+
+uint32_t GuideState::forward_batch_tc( const float *d_in, uint32_t n, float *d_out, cudaStream_t st )
+{
+	if ( reinterpret_cast<uintptr_t>( d_out ) % 16 ) throw std::runtime_error( "guide forward: output not 16-byte aligned" );
+	static bool attr = false;
+	if ( !attr )
+	{
+		check( cudaFuncSetAttribute( k_guide_forward_batch_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+									 int( tc::SMEM_BYTES ) ),
+			   "guide tc smem" );
+		attr = true;
+	}
+	check( cudaMemsetAsync( err, 0, 4, st ), "guide forward" );
+	pack_weights( st );
+	int device = 0, sms = 0;
+	check( cudaGetDevice( &device ), "device" );
+	check( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, device ), "device" );
+	uint32_t blocks = std::min<uint32_t>( ( n + tc::THREADS - 1 ) / tc::THREADS, uint32_t( sms ) * 2 );
+	if ( blocks )
+		k_guide_forward_batch_tc<<<blocks, tc::THREADS, tc::SMEM_BYTES, st>>>( dev(), Wp, d_in, n, d_out, err );
+	check( cudaGetLastError(), "guide forward" );
+	uint32_t e = 0;
+	check( cudaMemcpyAsync( &e, err, 4, cudaMemcpyDeviceToHost, st ), "guide forward" );
+	check( cudaStreamSynchronize( st ), "guide forward" );
+	return e;
 }
 
 void GuideState::load_records( const float *d_src, uint32_t n, cudaStream_t st )

@@ -29,6 +29,9 @@ struct GuideDev
 	float select_prob;   // probability of sampling the guide at a vertex
 };
 
+// Luminance (Rec. 709 weights): the scalar the guide's training weights use.
+__host__ __device__ __forceinline__ float lum( float3 c ) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
 // Resolution of level l: 4 * 1.5^l cells per axis (4 .. 346).
 __host__ __device__ __forceinline__ float grid_res( int l )
 {
@@ -94,6 +97,7 @@ __device__ __forceinline__ void grid_corners( int l, float3 u, GridCorners &c )
 __device__ __forceinline__ void guide_encode( const GuideDev &g, float3 x, float3 wo, float3 n, float *in )
 {
 	float3 u = ( x - g.bmin ) * g.binv;
+#pragma unroll
 	for ( int l = 0; l < G_LEVELS; ++l )
 	{
 		GridCorners c;
@@ -209,8 +213,9 @@ __device__ __forceinline__ void guide_forward_fp32( const float *__restrict__ W,
 	}
 }
 
-// Gradient of -log q(w) with respect to the 40 used outputs, times `scale`.
-__device__ __forceinline__ void mixture_nll_grad( const float *o, float3 w, float scale, float *g )
+// Gradient of -log q(w) with respect to the 40 used outputs, times `scale`;
+// returns q(w) (floored at 1e-30).
+__device__ __forceinline__ float mixture_nll_grad( const float *o, float3 w, float scale, float *g )
 {
 	Lobe lb[ G_LOBES ];
 	lobes_from_output( o, lb );
@@ -236,5 +241,6 @@ __device__ __forceinline__ void mixture_nll_grad( const float *o, float3 w, floa
 		float3 dm = ( w - lb[ k ].mu * dot( lb[ k ].mu, w ) ) * ( -scale * gam * kap / len );
 		g[ 5 * k ] = dm.x, g[ 5 * k + 1 ] = dm.y, g[ 5 * k + 2 ] = dm.z;
 	}
+	return q;
 }
 }  // namespace cr

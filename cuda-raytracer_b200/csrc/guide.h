@@ -10,8 +10,10 @@ namespace cr
 // Training records, SoA (one entry per recorded path vertex):
 //   x  = (position, valid)       wo = (outgoing direction, -)
 //   n  = (shading normal, -)     om = (sampled direction, sampling pdf)
+//   wo.w = luminance of f * cos for the sampled direction
 //   T  = (throughput after the vertex, training weight)
-//   L  = (radiance gathered up to and including the vertex, -)
+//   L  = (radiance the path had gathered once it reached the next vertex,
+//         that vertex's emission included, -)
 struct GuideRecords
 {
 	float4 *x = nullptr, *wo = nullptr, *n = nullptr, *om = nullptr, *T = nullptr, *L = nullptr;
@@ -23,12 +25,19 @@ struct GuideState
 	float *grid = nullptr, *grid_m = nullptr, *grid_v = nullptr, *ggrid = nullptr;
 	float *W = nullptr, *W_m = nullptr, *W_v = nullptr, *gW = nullptr;
 	float *b = nullptr, *b_m = nullptr, *b_v = nullptr, *gb = nullptr;
-	float *wsum = nullptr;
+	uint8_t *Wp = nullptr;    // device: BF16 weights in the tensor-core operand layout (guide_tc.cuh)
+	uint32_t *err = nullptr;  // device: error word of the batch forward calls
+	float *wsum = nullptr;    // device: total weight of the current batch
+	float *loss = nullptr;    // device: weighted NLL of the last batch trained on
 	float3 bmin{ 0, 0, 0 }, binv{ 1, 1, 1 };
 	float lr = 1e-2f;
 	float select_prob = 0.5f;
-	uint32_t step = 0;
-	uint32_t train_paths = 32768;  // paths per wave whose vertices are recorded
+	uint32_t step = 0;              // Adam steps taken
+	uint64_t waves = 0;             // waves trained on (moves the record offset)
+	uint32_t train_paths = 32768;   // paths per batch: up to 32768 x 8 = 2^18 vertices at max_bounce 7
+	uint32_t steps_per_wave = 4;    // batches (Adam steps) recorded and trained per wave
+	uint32_t warmup_steps = 16;     // steps before the guide is first sampled
+	bool product_target = true;     // fit Li * f * cos (the integrand) instead of Li
 	GuideRecords rec;
 	uint32_t rec_capacity = 0;
 
@@ -42,12 +51,21 @@ struct GuideState
 	GuideDev dev() const;
 	void ensure_records( uint32_t n );
 	void free_records();
-	// radiance targets of the recorded vertices of one wave (paths 0..n_paths-1)
-	void compute_targets( const float4 *L, uint32_t n_paths, uint32_t stride, cudaStream_t st );
-	void gradients( uint32_t n, cudaStream_t st );  // accumulate into gW, gb, ggrid
-	void adam( cudaStream_t st );                   // update and clear the gradients
-	void train_from_records( uint32_t n, cudaStream_t st );
+	// One training step on recorded paths j0 .. j0+n_paths-1 of a wave (slots
+	// j * stride + bounce; path j of the record is wave path rec_offset + j *
+	// rec_stride, whose final radiance is L[path]): radiance targets, gradients
+	// of the weighted NLL, Adam.
+	void train_step( const float4 *L, uint32_t j0, uint32_t n_paths, uint32_t stride, uint32_t rec_offset,
+					 uint32_t rec_stride, cudaStream_t st );
+	// accumulate into gW, gb, ggrid over n record slots of r (weights in T.w, total in wsum)
+	void gradients( const GuideRecords &r, uint32_t n, cudaStream_t st );
+	void adam( cudaStream_t st );  // update and clear the gradients
 	void forward_batch( const float *d_in, uint32_t n, float *d_out, cudaStream_t st );
+	void pack_weights( cudaStream_t st );  // W -> Wp
+	// BF16 tensor-core forward of n inputs {x, wo, n} (9 floats) to 64 outputs
+	// each (d_out 16-byte aligned: stored as float4); returns the device error
+	// word (0: no MMA timed out)
+	uint32_t forward_batch_tc( const float *d_in, uint32_t n, float *d_out, cudaStream_t st );
 	// records from n x 13 floats {x, wo, n, w, weight} (device), for tests
 	void load_records( const float *d_src, uint32_t n, cudaStream_t st );
 };

@@ -1,0 +1,267 @@
+// Tensor-core forward pass of the guide MLP on sm_100a (tcgen05 + TMEM).
+//
+// One CTA of 256 threads takes two tiles of 128 rows (queries) at a time.
+// Every thread owns one row: it gathers the row's encoding (hash grid, SH,
+// normal) in FP32, rounds it to BF16 and stores it into the tile's shared
+// memory operand.  For each of the 5 layers one thread issues tcgen05.mma
+// (kind::f16, BF16 x BF16 -> FP32, M = 128, N = 64, K = 16; four K steps per
+// layer and tile) with the activations as A and the layer's BF16 weights as
+// B, both in shared memory; the accumulators live in tensor memory (64
+// columns per tile).  tcgen05.commit signals an mbarrier; the threads then
+// read their row back with tcgen05.ld, add the bias, apply the ReLU, round to
+// BF16 and overwrite their A row for the next layer.  The last layer's row is
+// handed to the caller's sink in FP32.
+//
+// Shared-memory operands use the canonical K-major layout without swizzle:
+// 8 x 16-byte core matrices, element (r, k) at
+//     (r / 8) * SBO + (k / 8) * LBO + (r % 8) * 16 + (k % 8) * 2
+// with LBO = 128 bytes (next 8 columns of K) and SBO = 1024 bytes (next 8
+// rows), so one 64-wide block of 8 rows is 1 KB and a K step of 16 advances
+// the descriptor start by 256 bytes.
+//
+// Every wait on the mbarrier is bounded; on a timeout the kernel records
+// error bit 8 in the device error word, waits (bounded) for the MMAs it has
+// in flight, frees its tensor memory and returns.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "guide.cuh"
+
+namespace cr
+{
+namespace tc
+{
+constexpr uint32_t ROWS = 128;                      // MMA tile rows (M)
+constexpr uint32_t TILES = 2;                       // tiles per CTA iteration
+constexpr uint32_t THREADS = ROWS * TILES;          // one thread per row
+constexpr uint32_t LBO = 128, SBO = 1024;           // canonical K-major strides (bytes)
+constexpr uint32_t TILE_BYTES = ROWS * G_IN * 2;    // 16 KB of BF16 activations
+constexpr uint32_t W_BYTES = G_HID * G_IN * 2;      // 8 KB of BF16 weights per layer
+constexpr uint32_t TMEM_COLS = 64 * TILES;          // FP32 accumulators: 64 columns per tile
+
+// Shared-memory map, from a 128-byte aligned base.
+constexpr uint32_t OFF_W = 0;
+constexpr uint32_t OFF_A = OFF_W + G_LAYERS * W_BYTES;          // 40960
+constexpr uint32_t OFF_BIAS = OFF_A + TILES * TILE_BYTES;       // 73728
+constexpr uint32_t OFF_BAR = OFF_BIAS + G_LAYERS * G_HID * 4;   // 75008
+constexpr uint32_t OFF_TMEM = OFF_BAR + 8;                      // 75016
+constexpr uint32_t SMEM_USED = OFF_TMEM + 8;                    // 75024
+constexpr uint32_t SMEM_BYTES = SMEM_USED + 128;                // slack for the alignment
+
+constexpr uint32_t WAIT_LIMIT = 1u << 22;  // try_wait rounds before an MMA wait gives up
+constexpr uint32_t ERR_MMA_TIMEOUT = 8u;   // device error word bit
+
+// Instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t IDESC = ( 1u << 4 ) | ( 1u << 7 ) | ( 1u << 10 ) | ( ( 64u >> 3 ) << 17 ) | ( ( ROWS >> 4 ) << 24 );
+
+__host__ __device__ constexpr uint32_t canon( uint32_t r, uint32_t k )
+{
+	return ( r >> 3 ) * SBO + ( k >> 3 ) * LBO + ( r & 7u ) * 16u + ( k & 7u ) * 2u;
+}
+
+// Shared-memory matrix descriptor (sm_100 format): start address >> 4 at bits
+// 0-13, LBO >> 4 at 16-29, SBO >> 4 at 32-45, version 1 at 46-47, base offset
+// 0, layout type 0 (no swizzle) at 61-63.
+__device__ __forceinline__ uint64_t sdesc( uint32_t saddr )
+{
+	return uint64_t( ( saddr >> 4 ) & 0x3FFFu ) | ( uint64_t( LBO >> 4 ) << 16 ) | ( uint64_t( SBO >> 4 ) << 32 ) |
+		   ( 1ull << 46 );
+}
+
+__device__ __forceinline__ uint32_t smem_u32( const void *p ) { return uint32_t( __cvta_generic_to_shared( p ) ); }
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" ); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile( "tcgen05.fence::before_thread_sync;" ::: "memory" ); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile( "tcgen05.fence::after_thread_sync;" ::: "memory" ); }
+
+__device__ __forceinline__ void mma_bf16( uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate )
+{
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+		:
+		: "r"( d_tmem ), "l"( a ), "l"( b ), "r"( IDESC ), "r"( accumulate )
+		: "memory" );
+}
+
+__device__ __forceinline__ void mma_commit( uint32_t bar )
+{
+	asm volatile( "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"( bar ) : "memory" );
+}
+
+__device__ __forceinline__ bool mbar_wait( uint32_t bar, uint32_t parity )
+{
+	for ( uint32_t i = 0; i < WAIT_LIMIT; ++i )
+	{
+		uint32_t done;
+		asm volatile(
+			"{\n\t.reg .pred p;\n\t"
+			"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+			"selp.u32 %0, 1, 0, p;\n\t}"
+			: "=r"( done )
+			: "r"( bar ), "r"( parity )
+			: "memory" );
+		if ( done ) return true;
+	}
+	return false;
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16( uint32_t taddr, float *v )
+{
+	uint32_t r[ 16 ];
+	asm volatile(
+		"tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+		"{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+		: "=r"( r[ 0 ] ), "=r"( r[ 1 ] ), "=r"( r[ 2 ] ), "=r"( r[ 3 ] ), "=r"( r[ 4 ] ), "=r"( r[ 5 ] ), "=r"( r[ 6 ] ),
+		  "=r"( r[ 7 ] ), "=r"( r[ 8 ] ), "=r"( r[ 9 ] ), "=r"( r[ 10 ] ), "=r"( r[ 11 ] ), "=r"( r[ 12 ] ),
+		  "=r"( r[ 13 ] ), "=r"( r[ 14 ] ), "=r"( r[ 15 ] )
+		: "r"( taddr ) );
+#pragma unroll
+	for ( int i = 0; i < 16; ++i ) v[ i ] = __uint_as_float( r[ i ] );
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile( "tcgen05.wait::ld.sync.aligned;" ::: "memory" ); }
+
+__device__ __forceinline__ uint32_t pack_bf16x2( float a, float b )
+{
+	__nv_bfloat162 h = __floats2bfloat162_rn( a, b );
+	return *reinterpret_cast<uint32_t *>( &h );
+}
+
+// Stores 64 values of row r as BF16 into a canonical K-major tile.
+__device__ __forceinline__ void store_row( uint8_t *tile, uint32_t r, const float *v )
+{
+#pragma unroll
+	for ( int j = 0; j < 8; ++j )
+	{
+		uint4 q = make_uint4( pack_bf16x2( v[ 8 * j ], v[ 8 * j + 1 ] ), pack_bf16x2( v[ 8 * j + 2 ], v[ 8 * j + 3 ] ),
+							  pack_bf16x2( v[ 8 * j + 4 ], v[ 8 * j + 5 ] ), pack_bf16x2( v[ 8 * j + 6 ], v[ 8 * j + 7 ] ) );
+		*reinterpret_cast<uint4 *>( tile + canon( r, 8 * j ) ) = q;
+	}
+}
+
+// Runs the network over rows 0..n-1.  src(i, x, wo, nrm) -> bool fetches row
+// i's inputs (false: the row is skipped); sink(i, out) receives the 64 FP32
+// outputs of a fetched row.  Wp: the BF16 weights in the shared-memory image
+// (G_LAYERS x W_BYTES, canonical layout, 16-byte aligned).  Called by every
+// thread of a THREADS-wide CTA with SMEM_BYTES of dynamic shared memory.
+template <class Src, class Sink>
+__device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t *__restrict__ Wp, uint32_t n,
+												Src &&src, Sink &&sink, uint32_t *err )
+{
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t *sm = reinterpret_cast<uint8_t *>( ( reinterpret_cast<uintptr_t>( smem_raw ) + 127 ) & ~uintptr_t( 127 ) );
+	const uint32_t tid = threadIdx.x, warp = tid >> 5;
+	const uint32_t tile = tid / ROWS, row = tid % ROWS;
+	const uint32_t bar = smem_u32( sm + OFF_BAR );
+	uint32_t *tmem_slot = reinterpret_cast<uint32_t *>( sm + OFF_TMEM );
+	float *bias = reinterpret_cast<float *>( sm + OFF_BIAS );
+
+	// weights and biases into shared memory (16-byte copies)
+	{
+		const uint4 *src4 = reinterpret_cast<const uint4 *>( Wp );
+		uint4 *dst4 = reinterpret_cast<uint4 *>( sm + OFF_W );
+		for ( uint32_t i = tid; i < G_LAYERS * W_BYTES / 16; i += THREADS ) dst4[ i ] = __ldg( src4 + i );
+		for ( uint32_t i = tid; i < G_LAYERS * G_HID; i += THREADS ) bias[ i ] = g.b[ i ];
+	}
+	if ( tid == 0 )
+	{
+		asm volatile( "mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"( bar ) : "memory" );
+		asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+	}
+	if ( warp == 0 )
+	{
+		asm volatile( "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"( smem_u32( tmem_slot ) ),
+					  "r"( TMEM_COLS )
+					  : "memory" );
+		asm volatile( "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory" );
+	}
+	fence_async_smem();
+	tc_before_sync();
+	__syncthreads();
+	tc_after_sync();
+	const uint32_t tmem = *tmem_slot;
+	// this thread's TMEM lane (row) and its tile's 64 accumulator columns
+	const uint32_t my_tmem = tmem + ( ( ( warp & 3u ) * 32u ) << 16 ) + tile * 64u;
+	uint8_t *my_tile = sm + OFF_A + tile * TILE_BYTES;
+	uint32_t phase = 0;
+	bool failed = false;
+
+	for ( uint32_t base = blockIdx.x * THREADS; base < n; base += gridDim.x * THREADS )
+	{
+		const uint32_t i = base + tid;
+		float3 x = f3( 0.f, 0.f, 0.f ), wo = f3( 0.f, 0.f, 1.f ), nrm = f3( 0.f, 0.f, 1.f );
+		const bool valid = i < n && src( i, x, wo, nrm );
+		float v[ G_IN ];
+		if ( valid )
+			guide_encode( g, x, wo, nrm, v );
+		else
+			for ( int k = 0; k < G_IN; ++k ) v[ k ] = 0.f;
+		store_row( my_tile, row, v );
+		for ( int l = 0; l < G_LAYERS; ++l )
+		{
+			// make this thread's A row visible to the tensor core, then one
+			// thread issues the layer for both tiles
+			fence_async_smem();
+			tc_before_sync();
+			__syncthreads();
+			if ( tid == 0 )
+			{
+				tc_after_sync();
+				for ( uint32_t t = 0; t < TILES; ++t )
+					for ( uint32_t k = 0; k < G_IN / 16; ++k )
+						mma_bf16( tmem + t * 64u, sdesc( smem_u32( sm + OFF_A + t * TILE_BYTES ) + k * 2u * LBO ),
+								  sdesc( smem_u32( sm + OFF_W + l * W_BYTES ) + k * 2u * LBO ), k > 0 );
+				mma_commit( bar );
+			}
+			const bool ok = mbar_wait( bar, phase );
+			phase ^= 1u;
+			if ( __syncthreads_or( !ok ) )
+			{
+				failed = true;
+				break;
+			}
+			tc_after_sync();
+			float acc[ 64 ];
+#pragma unroll
+			for ( int c = 0; c < 4; ++c ) tmem_ld16( my_tmem + 16u * c, acc + 16 * c );
+			tmem_wait_ld();
+			const float *bl = bias + l * G_HID;
+			if ( l < G_LAYERS - 1 )
+			{
+#pragma unroll
+				for ( int k = 0; k < G_HID; ++k ) acc[ k ] = fmaxf( acc[ k ] + bl[ k ], 0.f );
+				store_row( my_tile, row, acc );
+			}
+			else
+			{
+#pragma unroll
+				for ( int k = 0; k < G_OUT; ++k ) acc[ k ] += bl[ k ];
+				if ( valid ) sink( i, acc );
+			}
+			// the next MMA overwrites the accumulators: finish this thread's reads first
+			tc_before_sync();
+		}
+		if ( failed ) break;
+	}
+	if ( failed )
+	{
+		if ( tid == 0 ) atomicOr( err, ERR_MMA_TIMEOUT );
+		// the timed-out phase once more (bounded): no MMA may still write TMEM below
+		mbar_wait( bar, phase ^ 1u );
+	}
+	tc_before_sync();
+	__syncthreads();
+	if ( warp == 0 )
+	{
+		tc_after_sync();
+		asm volatile( "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"( tmem ), "r"( TMEM_COLS ) : "memory" );
+	}
+}
+
+}  // namespace tc
+}  // namespace cr

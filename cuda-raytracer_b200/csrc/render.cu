@@ -27,6 +27,7 @@
 #include "render.h"
 #include "traverse.cuh"
 #include "guide.cuh"
+#include "guide_tc.cuh"
 
 namespace cr
 {
@@ -358,6 +359,11 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		}
 		L = L + beta * f3( sh.emission ) * w;
 	}
+	// Training target of the previous vertex: the radiance gathered so far,
+	// taken after this vertex's emission, so the target holds the light that
+	// reached the previous vertex through this surface (indirect light) and
+	// leaves the lights themselves to next-event estimation.
+	if ( rec_i != 0xFFFFFFFFu && bounce > 0 ) cfg.rec.L[ rec_i - 1 ] = make_float4( L.x, L.y, L.z, 0.f );
 	// Two-sided shading: the geometric normal faces the incoming ray and the
 	// shading normal is put on the same side.
 	if ( dot( s.ng, d ) > 0.f ) s.ng = -s.ng;
@@ -366,8 +372,8 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	float3 wo = fr.local( -d );
 	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
 	Lobe lb[ G_LOBES ];
-	const float sel = cfg.guiding ? cfg.guide.select_prob : 0.f;
-	if ( cfg.guiding ) load_lobes( lobes, lb );
+	const float sel = cfg.guide_sample ? cfg.guide.select_prob : 0.f;
+	if ( cfg.guide_sample ) load_lobes( lobes, lb );
 	if ( sc.n_lights )
 	{
 		uint32_t nli = sc.n_lights;
@@ -388,7 +394,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 			float pb;
 			float3 f = mis_eval( sh, wo, wi, pb );
 			// one-sample MIS of guide and BSDF: the continuation density
-			if ( cfg.guiding ) pb = sel * mixture_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
+			if ( cfg.guide_sample ) pb = sel * mixture_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
 			if ( !is_zero( f ) )
 			{
 				float w = pl * pl / ( pl * pl + pb * pb );
@@ -414,7 +420,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	float3 wi;
 	float pdf;
 	float3 wt, nd;
-	if ( cfg.guiding )
+	if ( cfg.guide_sample )
 	{
 		// one-sample MIS: the guide with probability sel, else the BSDF; the
 		// weight uses the combined density of both strategies
@@ -456,7 +462,8 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		// training record of this vertex (its radiance target follows once the
 		// rest of the path is known)
 		cfg.rec.x[ rec_i ] = make_float4( s.p.x, s.p.y, s.p.z, alive ? 1.f : 0.f );
-		cfg.rec.wo[ rec_i ] = make_float4( -d.x, -d.y, -d.z, 0.f );
+		// w: luminance of f * cos for the sampled direction (wt = f cos / pdf)
+		cfg.rec.wo[ rec_i ] = make_float4( -d.x, -d.y, -d.z, lum( wt ) * pdf );
 		cfg.rec.n[ rec_i ] = make_float4( s.ns.x, s.ns.y, s.ns.z, 0.f );
 		cfg.rec.om[ rec_i ] = make_float4( nd.x, nd.y, nd.z, pdf );
 		cfg.rec.T[ rec_i ] = make_float4( beta.x, beta.y, beta.z, 0.f );
@@ -487,12 +494,18 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 			path = q[ i ];
 			HitRec h = wb.hit[ path ];
 			const uint32_t stride = cfg.max_bounce + 1;
-			const bool recorded = cfg.guiding && path < cfg.train_paths;
-			if ( recorded && bounce > 0 )
+			uint32_t rec_j = 0xFFFFFFFFu;
+			if ( cfg.guiding && path >= cfg.rec_offset )
 			{
-				// radiance gathered through the previous vertex (its shadow ray has run)
+				uint32_t off = path - cfg.rec_offset, j = off / cfg.rec_stride;
+				if ( j * cfg.rec_stride == off && j < cfg.rec_paths ) rec_j = j;
+			}
+			const bool recorded = rec_j != 0xFFFFFFFFu;
+			if ( recorded && bounce > 0 && h.id == HIT_MISS )
+			{
+				// the previous vertex's continuation left the scene: no indirect light
 				float4 Lp = wb.L[ path ];
-				cfg.rec.L[ path * stride + bounce - 1 ] = make_float4( Lp.x, Lp.y, Lp.z, 0.f );
+				cfg.rec.L[ rec_j * stride + bounce - 1 ] = make_float4( Lp.x, Lp.y, Lp.z, 0.f );
 			}
 			if ( h.id != HIT_MISS )
 			{
@@ -505,8 +518,8 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 				uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
 				if ( cfg.estimator == EST_MIS )
 					shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
-							   cfg.guiding ? wb.lobes + size_t( path ) * 5 * G_LOBES : nullptr,
-							   recorded ? path * stride + bounce : 0xFFFFFFFFu );
+							   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 * G_LOBES : nullptr,
+							   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
 				else
 					shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
 				wb.beta[ path ] = beta;
@@ -533,33 +546,37 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 
 // Guide inference for the paths of one bounce that hit a surface: inputs as
 // the MIS shading sees them (position, outgoing direction, two-sided shading
-// normal), FP32 forward pass, mixture parameters per path.
-__global__ void k_guide_infer( DevScene sc, RenderConfig cfg, WaveBuffers wb, uint32_t bounce )
+// normal), BF16 tensor-core forward pass (guide_tc.cuh), mixture parameters
+// per path.
+__global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_infer( DevScene sc, RenderConfig cfg, WaveBuffers wb,
+																	uint32_t bounce, const uint8_t *Wp )
 {
 	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
 	const uint32_t *q = wb.queue[ bounce & 1 ];
-	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
-	{
-		uint32_t path = q[ i ];
-		HitRec h = wb.hit[ path ];
-		if ( h.id == HIT_MISS ) continue;
-		float3 o = f3( wb.ray_o[ path ] ), d = f3( wb.ray_d[ path ] );
+	auto src = [&]( uint32_t i, float3 &x, float3 &wo, float3 &nrm ) -> bool {
+		const uint32_t path = q[ i ];
+		const HitRec h = wb.hit[ path ];
+		if ( h.id == HIT_MISS ) return false;
+		const float3 o = f3( wb.ray_o[ path ] ), d = f3( wb.ray_d[ path ] );
 		Surface s = surface_at( sc, o, d, h, true );
 		if ( dot( s.ng, d ) > 0.f ) s.ng = -s.ng;
 		if ( dot( s.ns, s.ng ) < 0.f ) s.ns = -s.ns;
-		float in[ G_IN ], outv[ G_OUT ];
-		guide_encode( cfg.guide, s.p, -d, s.ns, in );
-		guide_forward_fp32( cfg.guide.W, cfg.guide.b, in, outv, nullptr );
+		x = s.p, wo = -d, nrm = s.ns;
+		return true;
+	};
+	auto sink = [&]( uint32_t i, const float *out ) {
 		Lobe lb[ G_LOBES ];
-		lobes_from_output( outv, lb );
-		float4 *dst = reinterpret_cast<float4 *>( wb.lobes + size_t( path ) * 5 * G_LOBES );
+		lobes_from_output( out, lb );
+		// 40 floats per path: 16-byte aligned for every path (160-byte stride)
+		float4 *dst = reinterpret_cast<float4 *>( wb.lobes + size_t( q[ i ] ) * 5 * G_LOBES );
 		float v[ 5 * G_LOBES ];
 		for ( int k = 0; k < G_LOBES; ++k )
 			v[ 5 * k ] = lb[ k ].mu.x, v[ 5 * k + 1 ] = lb[ k ].mu.y, v[ 5 * k + 2 ] = lb[ k ].mu.z,
 					v[ 5 * k + 3 ] = lb[ k ].kappa, v[ 5 * k + 4 ] = lb[ k ].weight;
 		for ( int j = 0; j < 5 * G_LOBES / 4; ++j )
 			dst[ j ] = make_float4( v[ 4 * j ], v[ 4 * j + 1 ], v[ 4 * j + 2 ], v[ 4 * j + 3 ] );
-	}
+	};
+	tc::mlp_forward_tc( cfg.guide, Wp, n, src, sink, wb.err );
 }
 
 __global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, double *sum, double *sumsq,
@@ -719,7 +736,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	struct Mark
 	{
 		cudaEvent_t a, b;
-		int kind;  // 0 extend 1 shadow 2 shade 3 other 4 guide
+		int kind;  // 0 extend 1 shadow 2 shade 3 other 4 guide inference 5 guide training
 	};
 	std::vector<Mark> marks;
 	cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -750,13 +767,35 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	{
 		WaveArgs wa{ first, uint32_t( std::min<uint64_t>( P, total - first ) ) };
 		check( cudaMemsetAsync( wb.counters, 0, sizeof( uint32_t ) * wb.n_counters, st ), "memset" );
-		const uint32_t train_n = cfg.guiding ? std::min( cfg.train_paths, wa.n ) : 0;
-		if ( train_n )
-			check( cudaMemsetAsync( cfg.rec.x, 0, sizeof( float4 ) * size_t( train_n ) * ( cfg.max_bounce + 1 ), st ),
+		// per-wave copy: which paths are recorded, and whether the guide is sampled
+		RenderConfig wc = cfg;
+		uint32_t steps = 0, batch = 0;
+		if ( cfg.guiding )
+		{
+			batch = std::min( guide->train_paths, wa.n );
+			wc.rec_paths = uint32_t( std::min<uint64_t>( uint64_t( batch ) * guide->steps_per_wave, wa.n ) );
+			steps = ( wc.rec_paths + batch - 1 ) / batch;
+			wc.rec_stride = wa.n / wc.rec_paths;
+			wc.rec_offset = uint32_t( ( guide->waves++ * 2654435761ull ) % wc.rec_stride );
+			wc.guide_sample = guide->step >= guide->warmup_steps;
+			if ( wc.guide_sample )
+			{
+				static bool smem_attr = false;
+				if ( !smem_attr )
+				{
+					check( cudaFuncSetAttribute( k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+												 int( tc::SMEM_BYTES ) ),
+						   "guide inference smem" );
+					smem_attr = true;
+				}
+				guide->pack_weights( st );  // BF16 copy of the weights this wave samples with
+			}
+			check( cudaMemsetAsync( cfg.rec.x, 0, sizeof( float4 ) * size_t( wc.rec_paths ) * ( cfg.max_bounce + 1 ), st ),
 				   "memset" );
+		}
 		timed( 3, [&] {
 			int gg = int( std::min<uint64_t>( ( wa.n + 255 ) / 256, uint64_t( sms ) * 16 ) );
-			k_generate<<<gg, 256, 0, st>>>( sc, cfg, wb, wa );
+			k_generate<<<gg, 256, 0, st>>>( sc, wc, wb, wa );
 		} );
 		for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
 		{
@@ -769,9 +808,11 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				else
 					k_traverse<ExtendIO, false, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 			} );
-			if ( cfg.guiding )
-				timed( 4, [&] { k_guide_infer<<<g_shade, 128, 0, st>>>( sc, cfg, wb, b ); } );
-			timed( 2, [&] { k_shade<<<g_shade, 128, 0, st>>>( sc, cfg, wb, wa, b, key ); } );
+			if ( wc.guide_sample )
+				timed( 4, [&] {
+					k_guide_infer<<<sms * 2, tc::THREADS, tc::SMEM_BYTES, st>>>( sc, wc, wb, b, guide->Wp );
+				} );
+			timed( 2, [&] { k_shade<<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key ); } );
 			if ( sc.n_lights )
 				timed( 1, [&] {
 					ShadowIO io{ wb.shadow_queue, wb.sh_o, wb.sh_d, wb.sh_c, wb.L };
@@ -783,16 +824,20 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 						k_traverse<ShadowIO, true, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 				} );
 		}
-		if ( train_n )
-			timed( 4, [&] {
-				// online training on this wave's recorded vertices
-				guide->compute_targets( wb.L, train_n, cfg.max_bounce + 1, st );
-				guide->train_from_records( train_n * ( cfg.max_bounce + 1 ), st );
+		if ( steps )
+			timed( 5, [&] {
+				// online training on this wave's recorded vertices, one Adam step per batch
+				for ( uint32_t k = 0; k < steps; ++k )
+				{
+					uint32_t j0 = k * batch;
+					guide->train_step( wb.L, j0, std::min( batch, wc.rec_paths - j0 ), cfg.max_bounce + 1, wc.rec_offset,
+									   wc.rec_stride, st );
+				}
 			} );
 		timed( 3, [&] {
 			uint64_t npx = ( first + wa.n - 1 ) / cfg.spp - first / cfg.spp + 1;
 			int gg = int( std::min<uint64_t>( ( npx + 255 ) / 256, uint64_t( sms ) * 16 ) );
-			k_accumulate<<<gg, 256, 0, st>>>( cfg, wb, wa, film_sum, film_sumsq, film_count );
+			k_accumulate<<<gg, 256, 0, st>>>( wc, wb, wa, film_sum, film_sumsq, film_count );
 		} );
 		check( cudaGetLastError(), "render launch" );
 		if ( times )
@@ -821,7 +866,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		{
 			check( cudaEventElapsedTime( &ms, m.a, m.b ), "event" );
 			( m.kind == 0 ? times->extend : m.kind == 1 ? times->shadow : m.kind == 2 ? times->shade
-																  : m.kind == 4 ? times->guide : times->other ) += ms;
+																  : m.kind >= 4 ? times->guide : times->other ) += ms;
+			if ( m.kind == 5 ) times->guide_train += ms;
 		}
 		if ( cfg.count_work )
 		{

@@ -41,17 +41,21 @@ struct RenderConfig
 	uint64_t seed;
 	uint32_t wave_paths;
 	bool count_work;
-	bool guiding = false;            // learned guide mixed with BSDF sampling (MIS estimator)
+	bool guiding = false;            // learned guide: records and training (MIS estimator)
+	bool guide_sample = false;       // guided renders: sample the guide (off while it warms up)
 	GuideDev guide{};
-	GuideRecords rec{};              // training records of the first train_paths paths of a wave
-	uint32_t train_paths = 0;
+	// Training records of one wave: the vertices of paths rec_offset + j * rec_stride,
+	// j < rec_paths, at slots j * (max_bounce + 1) + bounce.  The paths are spread over
+	// the whole wave (a wave is pixel-major) and the offset moves from wave to wave.
+	GuideRecords rec{};
+	uint32_t rec_paths = 0, rec_stride = 1, rec_offset = 0;
 	uint32_t refill_min = 16;        // traversal: idle lanes per warp that trigger a refill (1..32)
 	int traverse_blocks_per_sm = 8;  // traversal grid = SMs x this (1..8; 128-thread blocks)
 };
 
 struct StageTimes
 {
-	double extend = 0, shadow = 0, shade = 0, other = 0, total = 0, guide = 0;
+	double extend = 0, shadow = 0, shade = 0, other = 0, total = 0, guide = 0, guide_train = 0;
 	uint32_t launches = 0, waves = 0, extend_launches = 0, shadow_launches = 0;
 	uint64_t rays_extend = 0, rays_shadow = 0, nodes = 0, tris = 0, shadow_nodes = 0, shadow_tris = 0;
 };

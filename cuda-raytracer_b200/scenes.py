@@ -299,9 +299,9 @@ def config1(level=8, seed=1, width=1024, height=768, spp=256) -> SceneDesc:
 
 def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
     """Occluded light: the box is split by a wall at y=2.6 with a 0.4x0.4 aperture;
-    a single 0.3x0.3 light of strength 400 hangs on the far side; a displaced
-    icosphere (20*4**level triangles, ~330k at level 7) with Beckmann roughness
-    U[0.05,0.5] is the receiver on the camera side."""
+    a single 0.3x0.3 light of strength 400 hangs on the far side; three displaced
+    icospheres (one at `level`, two at `level - 1`: ~492k triangles at level 7)
+    with Beckmann roughness U[0.05,0.5] are the receivers on the camera side."""
     rng = np.random.default_rng(seed)
     sh = box_shaders(400.0)
     names = []
@@ -331,9 +331,22 @@ def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
     lq = quad((lx - .15, ly - .15, lz), (lx - .15, ly + .15, lz), (lx + .15, ly + .15, lz),
               (lx + .15, ly - .15, lz), (0, 0, -1))
     groups.append(_finish("light", *lq))
-    v, n, f = displaced_icosphere(level, seed, center=(S / 2, 0.4, 1.3), radius=1.2)
-    patch = np.arange(len(f)) // (4 ** level)
-    groups += split_groups(v, n, f, patch, names)
+    # receivers: one displaced icosphere at `level` and two at `level - 1`
+    for ci, (cen, rad, lv) in enumerate((((S / 2, 0.4, 1.3), 1.2, level), ((1.0, -1.3, 0.8), 0.7, level - 1),
+                                         ((4.5, -1.0, 0.9), 0.8, level - 1))):
+        v, n, f = displaced_icosphere(lv, seed + ci, center=cen, radius=rad)
+        patch = np.arange(len(f)) // (4 ** lv)
+        groups += split_groups(v, n, f, patch, names)
+    # the receivers share one material palette: one group per material
+    merged = {}
+    for g in groups:
+        if g.name in merged:
+            a = merged[g.name]
+            merged[g.name] = Group(g.name, np.concatenate([a.v, g.v]), np.concatenate([a.n, g.n]),
+                                   np.concatenate([a.f, g.f + len(a.v)]).astype(np.uint32))
+        else:
+            merged[g.name] = g
+    groups = list(merged.values())
     return SceneDesc(groups=groups, shaders=sh, camera=box_camera(), width=width, height=height,
                      spp=spp, max_bounce=7, name=f"config3_l{level}")
 

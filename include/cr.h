@@ -90,6 +90,7 @@ typedef struct cr_stats {
     uint32_t waves;        /* waves of paths                                  */
     uint32_t extend_launches;
     uint32_t shadow_launches;
+    double ms_guide_train; /* guide training steps (part of ms_guide)         */
 } cr_stats;
 
 /* ------------------------------------------------------------------ errors */
@@ -216,11 +217,38 @@ int cr_guide_reset(cr_scene *s, uint64_t seed);
 /* Normalisation box (x -> (x - bmin) * binv), training steps taken, and the
  * sizes (in floats) of the grid, weight and bias arrays. */
 int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, uint32_t *sizes);
+/* Training schedule of the scene's guide, defaults in brackets.  Each wave of
+ * a guided render records the vertices of steps_per_wave x train_paths paths
+ * spread over the wave and takes one Adam step per train_paths of them.
+ *   lr              Adam step size [1e-2]
+ *   select_prob     probability of sampling the guide at a vertex [0.5]
+ *   train_paths     paths per training batch [32768: up to 2^18 vertices at
+ *                   max_bounce 7]
+ *   steps_per_wave  batches (Adam steps) per wave [4]
+ *   warmup_steps    steps taken before the guide is first sampled [16]; until
+ *                   then a guided render samples the BSDF only and trains
+ *   product_target  1: fit the integrand Li f cos at each vertex; 0: fit the
+ *                   incident (indirect) radiance Li alone [1] */
+typedef struct cr_guide_config {
+    float lr;
+    float select_prob;
+    uint32_t train_paths;
+    uint32_t steps_per_wave;
+    uint32_t warmup_steps;
+    uint32_t product_target;
+} cr_guide_config;
+/* Apply `in` (when not NULL) and report the schedule in `out` (when not NULL). */
+int cr_guide_configure(cr_scene *s, const cr_guide_config *in, cr_guide_config *out);
+/* Weighted NLL (normalised by the batch weight) of the last training batch. */
+int cr_guide_loss(const cr_scene *s, float *loss);
 /* Copy the parameters out (set = 0) or in (set = 1); NULL arrays are skipped.
  * grid: [12][65536][2], W: [5][64 out][64 in], b: [5][64]. */
 int cr_guide_params(cr_scene *s, float *grid, float *W, float *b, int set);
 /* Network outputs (n x 64, FP32 path) for inputs n x {x, wo, n} (9 floats). */
 int cr_guide_forward(cr_scene *s, const float *inputs, uint64_t n, float *out);
+/* The same through the path the renderer samples with: BF16 weights and
+ * activations on the tensor cores (tcgen05), FP32 accumulation. */
+int cr_guide_forward_tc(cr_scene *s, const float *inputs, uint64_t n, float *out);
 /* Gradients of the weighted mixture NLL over records n x {x, wo, n, w, weight}
  * (13 floats), normalised by the total weight; parameters are not updated. */
 int cr_guide_gradients(cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid);
