@@ -114,7 +114,7 @@ def lib():
             "cr_guide_params": (I, [P, P, P, P, I]), "cr_guide_forward": (I, [P, P, U64, P]),
             "cr_guide_gradients": (I, [P, P, U64, P, P, P]),
             "cr_guide_configure": (I, [P, P, P]), "cr_guide_loss": (I, [P, P]),
-            "cr_guide_forward_tc": (I, [P, P, U64, P]),
+            "cr_guide_forward_tc": (I, [P, P, U64, P]), "cr_guide_gradients_tc": (I, [P, P, U64, P, P, P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
         }
@@ -310,11 +310,15 @@ class Guide:
         _check(lib().cr_guide_loss(self.scene.h, C.byref(v)))
         return v.value
 
-    def gradients(self, records):
+    def gradients(self, records, tensor_cores=False):
+        """Gradients (grid, W, b) of the weighted mixture NLL over records
+        n x {x, wo, n, w, weight}: FP32 pass, or the BF16 tensor-core pass the
+        renderer trains with."""
         records = np.ascontiguousarray(records, np.float32)
         s = self.info()["sizes"]
         ggrid, gW, gb = (np.zeros(int(n), np.float32) for n in s)
-        _check(lib().cr_guide_gradients(self.scene.h, _p(records), len(records), _p(gW), _p(gb), _p(ggrid)))
+        fn = lib().cr_guide_gradients_tc if tensor_cores else lib().cr_guide_gradients
+        _check(fn(self.scene.h, _p(records), len(records), _p(gW), _p(gb), _p(ggrid)))
         return ggrid, gW, gb
 
 

@@ -1472,7 +1472,9 @@ int cr_guide_forward_tc( cr_scene *s, const float *inputs, uint64_t n, float *ou
 	} );
 }
 
-int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid )
+namespace
+{
+int guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid, bool tc )
 {
 	return guarded( [&] {
 		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
@@ -1482,8 +1484,16 @@ int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW
 		cudaMemcpy( d, records, sizeof( float ) * 13 * n, cudaMemcpyHostToDevice );
 		GuideState &g = s->guide;
 		g.load_records( d, uint32_t( n ), nullptr );
-		g.gradients( g.rec, uint32_t( n ), nullptr );
+		cuda_check( cudaMemset( g.err_train, 0, 4 ), "guide gradients" );
+		g.gradients( g.rec, uint32_t( n ), nullptr, tc );
 		cuda_check( cudaDeviceSynchronize(), "guide gradients" );
+		uint32_t ew = 0;
+		cudaMemcpy( &ew, g.err_train, 4, cudaMemcpyDeviceToHost );
+		if ( ew )
+		{
+			cudaFree( d );
+			fail( CR_ERR_DEVICE, "guide tensor-core training pass: an MMA wait timed out" );
+		}
 		if ( gW ) cudaMemcpy( gW, g.gW, GuideState::w_size() * 4, cudaMemcpyDeviceToHost );
 		if ( gb ) cudaMemcpy( gb, g.gb, GuideState::b_size() * 4, cudaMemcpyDeviceToHost );
 		if ( ggrid ) cudaMemcpy( ggrid, g.ggrid, GuideState::grid_size() * 4, cudaMemcpyDeviceToHost );
@@ -1493,6 +1503,17 @@ int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW
 		cudaFree( d );
 		cuda_check( e, "guide gradients" );
 	} );
+}
+}  // namespace
+
+int cr_guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid )
+{
+	return guide_gradients( s, records, n, gW, gb, ggrid, false );
+}
+
+int cr_guide_gradients_tc( cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid )
+{
+	return guide_gradients( s, records, n, gW, gb, ggrid, true );
 }
 
 int cr_write_png( const char *path, uint32_t w, uint32_t h, const double *rgb )

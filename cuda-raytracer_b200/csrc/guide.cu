@@ -167,6 +167,284 @@ __global__ void __launch_bounds__( TRAIN_ROWS ) k_guide_train_fp32( GuideRecords
 	}
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core training pass (tcgen05): the same gradients as k_guide_train_fp32
+// with BF16 operands and FP32 accumulation.  One CTA of 128 threads takes a
+// tile of 128 records at a time, one record per thread.
+//   forward   z_l = W_l h_l + b_l:      A = h_l (rows x in), B = W_l (out x in)
+//   backward  dh_l = W_l^T delta_l:     A = delta_l (rows x out), B = W_l^T (in x out)
+//             gW_l += delta_l^T h_l:    A = delta_l^T (out x rows, padded to 128
+//                                       rows of zeros), B = h_l^T (in x rows)
+// gW accumulates in tensor memory over all tiles of the CTA and is added to
+// global memory once at the end; bias gradients are reduced across each warp
+// (lane L ends with columns 2L and 2L+1) and hash-grid gradients are scattered
+// with FP32 atomics, as in the FP32 pass.
+namespace tt
+{
+constexpr uint32_t THREADS = 128;
+constexpr uint32_t H_BYTES = tc::TILE_BYTES;                // one 128 x 64 BF16 tile
+constexpr uint32_t SBO128 = 16 * tc::LBO;                   // row-group stride of K = 128 tiles
+constexpr uint32_t OFF_W = 0;                               // forward weight image
+constexpr uint32_t OFF_WT = OFF_W + tc::WIMG_BYTES;         // transposed weight image
+constexpr uint32_t OFF_H = OFF_WT + tc::WIMG_BYTES;         // h_0 .. h_4
+constexpr uint32_t OFF_DZ = OFF_H + G_LAYERS * H_BYTES;     // delta (rows x out)
+constexpr uint32_t OFF_DZT = OFF_DZ + H_BYTES;              // delta^T (128 x 128, rows 64.. zero)
+constexpr uint32_t OFF_HT = OFF_DZT + 2 * H_BYTES;          // h^T (64 x 128)
+constexpr uint32_t OFF_BIAS = OFF_HT + H_BYTES;             // 5 x 64 floats
+constexpr uint32_t OFF_BAR = OFF_BIAS + G_LAYERS * G_HID * 4;
+constexpr uint32_t OFF_TMEM = OFF_BAR + 8;
+constexpr uint32_t SMEM_BYTES = OFF_TMEM + 8 + 128;
+constexpr uint32_t TMEM_COLS = 512;                         // D (64) + gW of 5 layers (5 x 64)
+constexpr uint32_t COL_DW = 64;
+static_assert( SMEM_BYTES <= 232448, "training tile exceeds the shared memory of one CTA" );
+static_assert( OFF_WT == OFF_W + tc::WIMG_BYTES, "weight images must be contiguous" );
+}  // namespace tt
+
+// One layer's MMAs for the whole tile, issued by thread 0 and committed to
+// `bar`; every thread then waits (bounded) for the commit.  Returns false on a
+// timeout (the same on every thread).
+template <class Issue>
+__device__ __forceinline__ bool tc_step( uint32_t tid, uint32_t bar, uint32_t &phase, Issue &&issue )
+{
+	tc::fence_async_smem();
+	tc::tc_before_sync();
+	__syncthreads();
+	if ( tid == 0 )
+	{
+		tc::tc_after_sync();
+		issue();
+		tc::mma_commit( bar );
+	}
+	const bool ok = tc::mbar_wait( bar, phase );
+	phase ^= 1u;
+	if ( __syncthreads_or( !ok ) ) return false;
+	tc::tc_after_sync();
+	return true;
+}
+
+__device__ __forceinline__ void tmem_ld64( uint32_t taddr, float *v )
+{
+#pragma unroll
+	for ( int c = 0; c < 4; ++c ) tc::tmem_ld16( taddr + 16u * c, v + 16 * c );
+	tc::tmem_wait_ld();
+}
+
+__device__ __forceinline__ void st_bf16( uint8_t *p, float v )
+{
+	*reinterpret_cast<__nv_bfloat16 *>( p ) = __float2bfloat16_rn( v );
+}
+
+__global__ void __launch_bounds__( tt::THREADS, 1 ) k_guide_train_tc( GuideRecords rec, uint32_t n, GuideDev g,
+																	   const uint8_t *Wp, const float *wsum, float *gW,
+																	   float *gb, float *ggrid, float *loss,
+																	   uint32_t *err )
+{
+	using namespace tt;
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t *sm = reinterpret_cast<uint8_t *>( ( reinterpret_cast<uintptr_t>( smem_raw ) + 127 ) & ~uintptr_t( 127 ) );
+	const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+	const uint32_t bar = tc::smem_u32( sm + OFF_BAR );
+	uint32_t *tmem_slot = reinterpret_cast<uint32_t *>( sm + OFF_TMEM );
+	float *bias = reinterpret_cast<float *>( sm + OFF_BIAS );
+	{
+		const uint4 *s4 = reinterpret_cast<const uint4 *>( Wp );
+		uint4 *d4 = reinterpret_cast<uint4 *>( sm + OFF_W );
+		for ( uint32_t i = tid; i < tc::WP_BYTES / 16; i += THREADS ) d4[ i ] = __ldg( s4 + i );
+		for ( uint32_t i = tid; i < G_LAYERS * G_HID; i += THREADS ) bias[ i ] = g.b[ i ];
+		// rows 64..127 of delta^T stay zero: the gW product is padded to M = 128
+		uint4 *z = reinterpret_cast<uint4 *>( sm + OFF_DZT + 8 * SBO128 );
+		for ( uint32_t i = tid; i < 8 * SBO128 / 16; i += THREADS ) z[ i ] = make_uint4( 0u, 0u, 0u, 0u );
+	}
+	if ( tid == 0 )
+	{
+		asm volatile( "mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"( bar ) : "memory" );
+		asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+	}
+	if ( warp == 0 )
+	{
+		asm volatile( "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"( tc::smem_u32( tmem_slot ) ),
+					  "r"( TMEM_COLS )
+					  : "memory" );
+		asm volatile( "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory" );
+	}
+	tc::fence_async_smem();
+	tc::tc_before_sync();
+	__syncthreads();
+	tc::tc_after_sync();
+	const uint32_t tmem = *tmem_slot;
+	const uint32_t my_lane = tmem + ( ( warp * 32u ) << 16 );  // this thread's TMEM lane (row), column 0
+	const float norm = *wsum > 0.f ? 1.f / *wsum : 0.f;
+	const uint32_t a_dz = tc::smem_u32( sm + OFF_DZ ), a_dzt = tc::smem_u32( sm + OFF_DZT ), a_ht = tc::smem_u32( sm + OFF_HT );
+	uint32_t phase = 0;
+	bool failed = false, any = false;
+	float gbacc[ G_LAYERS ][ 2 ];
+#pragma unroll
+	for ( int l = 0; l < G_LAYERS; ++l ) gbacc[ l ][ 0 ] = gbacc[ l ][ 1 ] = 0.f;
+
+	for ( uint32_t base = blockIdx.x * THREADS; base < n; base += gridDim.x * THREADS )
+	{
+		const uint32_t r = base + tid;
+		float w = 0.f;
+		float3 x = f3( 0.f, 0.f, 0.f ), wo = f3( 0.f, 0.f, 1.f ), nn = f3( 0.f, 0.f, 1.f ), om = f3( 0.f, 0.f, 1.f );
+		if ( r < n && rec.x[ r ].w > 0.f )
+		{
+			x = f3( rec.x[ r ] ), wo = f3( rec.wo[ r ] ), nn = f3( rec.n[ r ] ), om = f3( rec.om[ r ] );
+			w = rec.T[ r ].w * norm;
+		}
+		float v[ G_IN ];
+		if ( w > 0.f )
+			guide_encode( g, x, wo, nn, v );
+		else
+#pragma unroll
+			for ( int k = 0; k < G_IN; ++k ) v[ k ] = 0.f;
+		tc::store_row( sm + OFF_H, tid, v );
+		// ---- forward
+		for ( int l = 0; l < G_LAYERS && !failed; ++l )
+		{
+			const uint32_t a_h = tc::smem_u32( sm + OFF_H + l * H_BYTES ), a_w = tc::smem_u32( sm + OFF_W + l * tc::W_BYTES );
+			if ( !tc_step( tid, bar, phase, [&] {
+					 for ( uint32_t k = 0; k < 4; ++k )
+						 tc::mma_bf16( tmem, tc::sdesc( a_h + 256u * k ), tc::sdesc( a_w + 256u * k ), k > 0 );
+				 } ) )
+			{
+				failed = true;
+				break;
+			}
+			tmem_ld64( my_lane, v );
+			const float *bl = bias + l * G_HID;
+			if ( l < G_LAYERS - 1 )
+			{
+#pragma unroll
+				for ( int k = 0; k < G_HID; ++k ) v[ k ] = fmaxf( v[ k ] + bl[ k ], 0.f );
+				tc::store_row( sm + OFF_H + ( l + 1 ) * H_BYTES, tid, v );
+			}
+			else
+#pragma unroll
+				for ( int k = 0; k < G_OUT; ++k ) v[ k ] += bl[ k ];
+			tc::tc_before_sync();
+		}
+		if ( failed ) break;
+		// ---- loss gradient at the output
+		float dz[ G_OUT ];
+		float nll = 0.f;
+		if ( w > 0.f )
+			nll = -w * logf( mixture_nll_grad( v, om, w, dz ) );
+		else
+#pragma unroll
+			for ( int k = 0; k < G_OUT; ++k ) dz[ k ] = 0.f;
+		for ( int o = 16; o; o >>= 1 ) nll += __shfl_xor_sync( 0xFFFFFFFFu, nll, o );
+		if ( lane == 0 && nll != 0.f ) atomicAdd( loss, nll );
+		// ---- backward
+		for ( int l = G_LAYERS - 1; l >= 0; --l )
+		{
+			uint8_t *hl = sm + OFF_H + l * H_BYTES;
+			// this row of h_l (BF16) for h_l^T and the ReLU mask
+			uint4 hrow[ 8 ];
+#pragma unroll
+			for ( int j = 0; j < 8; ++j ) hrow[ j ] = *reinterpret_cast<const uint4 *>( hl + tc::canon( tid, 8 * j ) );
+			const __nv_bfloat16 *hb = reinterpret_cast<const __nv_bfloat16 *>( hrow );
+			tc::store_row( sm + OFF_DZ, tid, dz );
+#pragma unroll
+			for ( int k = 0; k < 64; ++k )
+			{
+				st_bf16( sm + OFF_DZT + tc::canon128( k, tid ), dz[ k ] );
+				*reinterpret_cast<__nv_bfloat16 *>( sm + OFF_HT + tc::canon128( k, tid ) ) = hb[ k ];
+			}
+			// bias gradient: reduce-scatter of dz over the warp's 32 rows
+			{
+				float t[ 64 ];
+#pragma unroll
+				for ( int k = 0; k < 64; ++k ) t[ k ] = dz[ k ];
+#pragma unroll
+				for ( int h = 32, o = 16; o; h >>= 1, o >>= 1 )
+				{
+					const bool hi = lane & uint32_t( o );
+#pragma unroll
+					for ( int j = 0; j < h; ++j )
+					{
+						float send = hi ? t[ j ] : t[ j + h ];
+						float keep = hi ? t[ j + h ] : t[ j ];
+						t[ j ] = keep + __shfl_xor_sync( 0xFFFFFFFFu, send, o );
+					}
+				}
+				gbacc[ l ][ 0 ] += t[ 0 ], gbacc[ l ][ 1 ] += t[ 1 ];
+			}
+			const uint32_t a_wt = tc::smem_u32( sm + OFF_WT + l * tc::W_BYTES );
+			const uint32_t first = any ? 1u : 0u;
+			if ( !tc_step( tid, bar, phase, [&] {
+					 for ( uint32_t k = 0; k < 8; ++k )
+						 tc::mma_bf16( tmem + COL_DW + 64u * l, tc::sdesc( a_dzt + 256u * k, SBO128 ),
+									   tc::sdesc( a_ht + 256u * k, SBO128 ), ( k > 0 ) | first );
+					 for ( uint32_t k = 0; k < 4; ++k )
+						 tc::mma_bf16( tmem, tc::sdesc( a_dz + 256u * k ), tc::sdesc( a_wt + 256u * k ), k > 0 );
+				 } ) )
+			{
+				failed = true;
+				break;
+			}
+			float dh[ G_IN ];
+			tmem_ld64( my_lane, dh );
+			tc::tc_before_sync();
+			if ( l > 0 )
+			{
+#pragma unroll
+				for ( int k = 0; k < G_HID; ++k ) dz[ k ] = __bfloat162float( hb[ k ] ) > 0.f ? dh[ k ] : 0.f;
+			}
+			else if ( w > 0.f )
+			{
+				// hash-grid features: scatter the gradient to the 8 corners per level
+				float3 u = ( x - g.bmin ) * g.binv;
+				for ( int lv = 0; lv < G_LEVELS; ++lv )
+				{
+					float d0 = dh[ 2 * lv ], d1 = dh[ 2 * lv + 1 ];
+					if ( d0 == 0.f && d1 == 0.f ) continue;
+					GridCorners c;
+					grid_corners( lv, u, c );
+					float *tab = ggrid + size_t( lv ) * G_T * G_FEAT;
+					for ( int k = 0; k < 8; ++k )
+					{
+						atomicAdd( tab + 2 * c.idx[ k ], c.w[ k ] * d0 );
+						atomicAdd( tab + 2 * c.idx[ k ] + 1, c.w[ k ] * d1 );
+					}
+				}
+			}
+		}
+		if ( failed ) break;
+		any = true;
+	}
+	if ( failed )
+	{
+		if ( tid == 0 ) atomicOr( err, tc::ERR_MMA_TIMEOUT );
+		tc::mbar_wait( bar, phase ^ 1u );  // the timed-out commit, once more (bounded)
+	}
+	else if ( any )
+	{
+		// gW rows (output units) live in TMEM lanes 0..63: warps 0 and 1
+		if ( warp < 2 )
+			for ( int l = 0; l < G_LAYERS; ++l )
+			{
+				float dw[ G_IN ];
+				tmem_ld64( my_lane + COL_DW + 64u * l, dw );
+				float *dst = gW + size_t( l ) * G_W + size_t( tid ) * G_IN;
+				for ( int k = 0; k < G_IN; ++k )
+					if ( dw[ k ] != 0.f ) atomicAdd( dst + k, dw[ k ] );
+			}
+#pragma unroll
+		for ( int l = 0; l < G_LAYERS; ++l )
+		{
+			if ( gbacc[ l ][ 0 ] != 0.f ) atomicAdd( gb + l * G_HID + 2 * lane, gbacc[ l ][ 0 ] );
+			if ( gbacc[ l ][ 1 ] != 0.f ) atomicAdd( gb + l * G_HID + 2 * lane + 1, gbacc[ l ][ 1 ] );
+		}
+	}
+	tc::tc_before_sync();
+	__syncthreads();
+	if ( warp == 0 )
+	{
+		tc::tc_after_sync();
+		asm volatile( "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"( tmem ), "r"( TMEM_COLS ) : "memory" );
+	}
+}
+
 // Adam (Kingma and Ba 2015) on a flat parameter array; clears the gradient.
 __global__ void k_adam( float *p, float *grad, float *m, float *v, uint32_t n, float lr, float b1, float b2, float eps,
 						float c1, float c2 )
@@ -194,15 +472,18 @@ __global__ void k_guide_forward_batch( GuideDev g, const float *inp, uint32_t n,
 	}
 }
 
-// FP32 master weights [G_LAYERS][64 out][64 in] -> the BF16 shared-memory image
-// of the tensor-core forward (layer l at l * W_BYTES, element (out, in) at
-// canon(out, in)).
+// FP32 master weights [G_LAYERS][64 out][64 in] -> the BF16 shared-memory
+// images of the tensor-core passes: forward (layer l at l * W_BYTES, element
+// (out, in) at canon(out, in)) and, after it, transposed (element (out, in) at
+// canon(in, out)).
 __global__ void k_pack_weights_bf16( const float *__restrict__ W, uint8_t *__restrict__ Wp )
 {
 	for ( uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < uint32_t( G_LAYERS * G_W ); e += gridDim.x * blockDim.x )
 	{
 		uint32_t l = e / G_W, o = ( e % G_W ) / G_IN, in = e % G_IN;
-		*reinterpret_cast<__nv_bfloat16 *>( Wp + l * tc::W_BYTES + tc::canon( o, in ) ) = __float2bfloat16_rn( W[ e ] );
+		const __nv_bfloat16 v = __float2bfloat16_rn( W[ e ] );
+		*reinterpret_cast<__nv_bfloat16 *>( Wp + l * tc::W_BYTES + tc::canon( o, in ) ) = v;
+		*reinterpret_cast<__nv_bfloat16 *>( Wp + tc::WIMG_BYTES + l * tc::W_BYTES + tc::canon( in, o ) ) = v;
 	}
 }
 
@@ -271,8 +552,9 @@ void GuideState::init( float3 lo, float3 hi, uint64_t seed )
 	dalloc( grid, grid_size() ), dalloc( grid_m, grid_size() ), dalloc( grid_v, grid_size() ), dalloc( ggrid, grid_size() );
 	dalloc( W, w_size() ), dalloc( W_m, w_size() ), dalloc( W_v, w_size() ), dalloc( gW, w_size() );
 	dalloc( b, b_size() ), dalloc( b_m, b_size() ), dalloc( b_v, b_size() ), dalloc( gb, b_size() );
-	dalloc( wsum, 1 ), dalloc( loss, 1 ), dalloc( err, 1 ), dalloc( Wp, size_t( tc::W_BYTES ) * G_LAYERS );
+	dalloc( wsum, 1 ), dalloc( loss, 1 ), dalloc( err, 1 ), dalloc( err_train, 1 ), dalloc( Wp, size_t( tc::WP_BYTES ) );
 	check( cudaMemset( loss, 0, 4 ), "guide init" );
+	check( cudaMemset( err_train, 0, 4 ), "guide init" );
 	std::mt19937_64 rng( seed );
 	std::uniform_real_distribution<float> ug( -1e-4f, 1e-4f );
 	std::vector<float> h( grid_size() );
@@ -304,7 +586,8 @@ void GuideState::release()
 	grid = grid_m = grid_v = ggrid = W = W_m = W_v = gW = b = b_m = b_v = gb = wsum = loss = nullptr;
 	if ( Wp ) cudaFree( Wp );
 	if ( err ) cudaFree( err );
-	Wp = nullptr, err = nullptr;
+	if ( err_train ) cudaFree( err_train );
+	Wp = nullptr, err = nullptr, err_train = nullptr;
 	if ( rec.x ) free_records();
 	ready = false;
 }
@@ -343,12 +626,33 @@ void GuideState::train_step( const float4 *L, uint32_t j0, uint32_t n_paths, uin
 	k_guide_targets<<<std::min<uint32_t>( ( n + 255 ) / 256, 2048 ), 256, 0, st>>>( r, L, n_paths, stride, j0, rec_offset,
 																				 rec_stride, product_target, wsum );
 	check( cudaGetLastError(), "guide targets" );
-	gradients( r, n, st );
+	gradients( r, n, st, tc_train );
 	adam( st );
 }
 
-void GuideState::gradients( const GuideRecords &r, uint32_t n, cudaStream_t st )
+void GuideState::gradients( const GuideRecords &r, uint32_t n, cudaStream_t st, bool tensor_cores )
 {
+	if ( tensor_cores )
+	{
+		static bool tattr = false;
+		if ( !tattr )
+		{
+			check( cudaFuncSetAttribute( k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+										 int( tt::SMEM_BYTES ) ),
+				   "guide tc train smem" );
+			tattr = true;
+		}
+		int device = 0, sms = 0;
+		check( cudaGetDevice( &device ), "device" );
+		check( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, device ), "device" );
+		uint32_t blocks = std::min<uint32_t>( ( n + tt::THREADS - 1 ) / tt::THREADS, uint32_t( sms ) );
+		if ( blocks == 0 ) return;
+		pack_weights( st );
+		check( cudaMemsetAsync( loss, 0, 4, st ), "guide train" );
+		k_guide_train_tc<<<blocks, tt::THREADS, tt::SMEM_BYTES, st>>>( r, n, dev(), Wp, wsum, gW, gb, ggrid, loss, err_train );
+		check( cudaGetLastError(), "guide train" );
+		return;
+	}
 	static bool attr = false;
 	if ( !attr )
 	{

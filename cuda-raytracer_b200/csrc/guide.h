@@ -27,6 +27,8 @@ struct GuideState
 	float *b = nullptr, *b_m = nullptr, *b_v = nullptr, *gb = nullptr;
 	uint8_t *Wp = nullptr;    // device: BF16 weights in the tensor-core operand layout (guide_tc.cuh)
 	uint32_t *err = nullptr;  // device: error word of the batch forward calls
+	uint32_t *err_train = nullptr;  // device: error word of the tensor-core training pass
+	bool tc_train = true;     // train with the tensor-core pass (false: the FP32 pass)
 	float *wsum = nullptr;    // device: total weight of the current batch
 	float *loss = nullptr;    // device: weighted NLL of the last batch trained on
 	float3 bmin{ 0, 0, 0 }, binv{ 1, 1, 1 };
@@ -35,8 +37,8 @@ struct GuideState
 	uint32_t step = 0;              // Adam steps taken
 	uint64_t waves = 0;             // waves trained on (moves the record offset)
 	uint32_t train_paths = 32768;   // paths per batch: up to 32768 x 8 = 2^18 vertices at max_bounce 7
-	uint32_t steps_per_wave = 4;    // batches (Adam steps) recorded and trained per wave
-	uint32_t warmup_steps = 16;     // steps before the guide is first sampled
+	uint32_t steps_per_wave = 2;    // batches (Adam steps) recorded and trained per wave
+	uint32_t warmup_steps = 8;      // steps before the guide is first sampled
 	bool product_target = true;     // fit Li * f * cos (the integrand) instead of Li
 	GuideRecords rec;
 	uint32_t rec_capacity = 0;
@@ -57,8 +59,9 @@ struct GuideState
 	// of the weighted NLL, Adam.
 	void train_step( const float4 *L, uint32_t j0, uint32_t n_paths, uint32_t stride, uint32_t rec_offset,
 					 uint32_t rec_stride, cudaStream_t st );
-	// accumulate into gW, gb, ggrid over n record slots of r (weights in T.w, total in wsum)
-	void gradients( const GuideRecords &r, uint32_t n, cudaStream_t st );
+	// accumulate into gW, gb, ggrid over n record slots of r (weights in T.w, total
+	// in wsum), with the tensor-core pass or the FP32 pass
+	void gradients( const GuideRecords &r, uint32_t n, cudaStream_t st, bool tensor_cores );
 	void adam( cudaStream_t st );  // update and clear the gradients
 	void forward_batch( const float *d_in, uint32_t n, float *d_out, cudaStream_t st );
 	void pack_weights( cudaStream_t st );  // W -> Wp

@@ -48,6 +48,11 @@ constexpr uint32_t OFF_TMEM = OFF_BAR + 8;                      // 75016
 constexpr uint32_t SMEM_USED = OFF_TMEM + 8;                    // 75024
 constexpr uint32_t SMEM_BYTES = SMEM_USED + 128;                // slack for the alignment
 
+// Weight images in device memory: the forward image (layer l: N = out, K = in)
+// followed by the transposed image the backward pass uses (N = in, K = out).
+constexpr uint32_t WIMG_BYTES = G_LAYERS * W_BYTES;   // 40960
+constexpr uint32_t WP_BYTES = 2 * WIMG_BYTES;
+
 constexpr uint32_t WAIT_LIMIT = 1u << 22;  // try_wait rounds before an MMA wait gives up
 constexpr uint32_t ERR_MMA_TIMEOUT = 8u;   // device error word bit
 
@@ -64,10 +69,16 @@ __host__ __device__ constexpr uint32_t canon( uint32_t r, uint32_t k )
 // Shared-memory matrix descriptor (sm_100 format): start address >> 4 at bits
 // 0-13, LBO >> 4 at 16-29, SBO >> 4 at 32-45, version 1 at 46-47, base offset
 // 0, layout type 0 (no swizzle) at 61-63.
-__device__ __forceinline__ uint64_t sdesc( uint32_t saddr )
+__device__ __forceinline__ uint64_t sdesc( uint32_t saddr, uint32_t sbo = SBO )
 {
-	return uint64_t( ( saddr >> 4 ) & 0x3FFFu ) | ( uint64_t( LBO >> 4 ) << 16 ) | ( uint64_t( SBO >> 4 ) << 32 ) |
+	return uint64_t( ( saddr >> 4 ) & 0x3FFFu ) | ( uint64_t( LBO >> 4 ) << 16 ) | ( uint64_t( sbo >> 4 ) << 32 ) |
 		   ( 1ull << 46 );
+}
+
+// Canonical K-major offset for a tile whose K extent is 128 (SBO = 16 * LBO).
+__host__ __device__ constexpr uint32_t canon128( uint32_t r, uint32_t k )
+{
+	return ( r >> 3 ) * ( 16u * LBO ) + ( k >> 3 ) * LBO + ( r & 7u ) * 16u + ( k & 7u ) * 2u;
 }
 
 __device__ __forceinline__ uint32_t smem_u32( const void *p ) { return uint32_t( __cvta_generic_to_shared( p ) ); }

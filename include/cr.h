@@ -224,8 +224,8 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   select_prob     probability of sampling the guide at a vertex [0.5]
  *   train_paths     paths per training batch [32768: up to 2^18 vertices at
  *                   max_bounce 7]
- *   steps_per_wave  batches (Adam steps) per wave [4]
- *   warmup_steps    steps taken before the guide is first sampled [16]; until
+ *   steps_per_wave  batches (Adam steps) per wave [2]
+ *   warmup_steps    steps taken before the guide is first sampled [8]; until
  *                   then a guided render samples the BSDF only and trains
  *   product_target  1: fit the integrand Li f cos at each vertex; 0: fit the
  *                   incident (indirect) radiance Li alone [1] */
@@ -252,6 +252,9 @@ int cr_guide_forward_tc(cr_scene *s, const float *inputs, uint64_t n, float *out
 /* Gradients of the weighted mixture NLL over records n x {x, wo, n, w, weight}
  * (13 floats), normalised by the total weight; parameters are not updated. */
 int cr_guide_gradients(cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid);
+/* The same through the training pass the renderer uses: BF16 operands on the
+ * tensor cores (tcgen05), FP32 accumulation. */
+int cr_guide_gradients_tc(cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid);
 
 /* Renderer::render (src/core/renderer/renderer.cu:13-52): load a scene file,
  * render it with the configured kernel and tracer, write the reference's

@@ -176,3 +176,57 @@ def gradients(grid, W, b, bmin, binv, records):
                     for k in range(8):
                         ggrid[lv, idx[k]] += w[k] * dh[2 * lv:2 * lv + 2]
     return gW, gb, ggrid
+
+
+# ---------------------------------------------------------------------------
+# BF16 emulation of the tensor-core passes (cuda-raytracer_b200/csrc/guide_tc.cuh
+# and k_guide_train_tc): the same arithmetic in FP64 with the operands rounded
+# to BF16 (round to nearest even) where the kernels round them: the encoding and
+# the hidden activations, the weights, and the output gradient of every layer as
+# it enters the two backward products.  Biases, accumulations, bias gradients and
+# the ReLU masks stay unrounded.
+
+def bf16(a):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    f = np.asarray(a, np.float64).astype(np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward_bf16(W, b, h0):
+    """Forward pass as the tensor cores compute it; returns the output and the
+    BF16 layer inputs h_0..h_4."""
+    Wb = bf16(W)
+    hs, h = [], bf16(h0)
+    for l in range(LAYERS):
+        hs.append(h)
+        z = Wb[l] @ h + b[l]
+        if l == LAYERS - 1:
+            return z, hs
+        h = bf16(np.maximum(z, 0.0))
+
+
+def gradients_bf16(grid, W, b, bmin, binv, records):
+    """Gradients of `loss` as the tensor-core training pass forms them."""
+    gW, gb, ggrid = np.zeros_like(W), np.zeros_like(b), np.zeros_like(grid)
+    Wb = bf16(W)
+    tot = sum(r[12] for r in records if r[12] > 0)
+    for r in records:
+        if r[12] <= 0:
+            continue
+        h0, cs = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
+        o, hs = forward_bf16(W, b, h0)
+        dz = nll_grad(o, np.asarray(r[9:12], np.float64), r[12] / tot)
+        for l in range(LAYERS - 1, -1, -1):
+            dzb = bf16(dz)
+            gW[l] += np.outer(dzb, hs[l])
+            gb[l] += dz
+            dh = Wb[l].T @ dzb
+            if l > 0:
+                dz = dh * (hs[l] > 0)
+            else:
+                for lv, (idx, w) in enumerate(cs):
+                    for k in range(8):
+                        ggrid[lv, idx[k]] += w[k] * dh[2 * lv:2 * lv + 2]
+    return gW, gb, ggrid

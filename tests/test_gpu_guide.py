@@ -89,7 +89,8 @@ def test_guide_configure_validates(guided):
     s, g, grid, W, b, info = guided
     import cuda_raytracer_b200 as crm
     cfg = g.configure()
-    assert cfg["train_paths"] == 32768 and cfg["steps_per_wave"] == 4 and cfg["warmup_steps"] == 16
+    assert cfg["train_paths"] == 32768 and cfg["steps_per_wave"] == 2 and cfg["warmup_steps"] == 8
+    assert cfg["product_target"] == 1
     for bad in ({"lr": 0.0}, {"select_prob": 1.0}, {"train_paths": 0}, {"steps_per_wave": 65}):
         with pytest.raises(crm.CrError):
             g.configure(**bad)
@@ -112,6 +113,37 @@ def test_gradients_match_fp64(guided):
         got = got.reshape(ref.shape)
         rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
         assert rel < 2e-3, rel
+
+
+def test_tc_gradients_match_fp64(guided):
+    """The tensor-core training pass (BF16 operands, FP32 accumulation) against
+    the FP64 gradients: BF16 rounding of activations, weights and output
+    gradients leaves a few percent of relative error; 300 records span three
+    128-row tiles with a ragged tail."""
+    s, g, grid, W, b, info = guided
+    rng = np.random.default_rng(3)
+    n = 300
+    inp = _inputs(rng, n)
+    om = rng.normal(size=(n, 3)); om /= np.linalg.norm(om, axis=1, keepdims=True)
+    wts = rng.uniform(0.05, 3.0, n)
+    wts[::7] = 0.0
+    recs = np.concatenate([inp, om, wts[:, None]], 1).astype(np.float32)
+    ggrid, gW, gb = g.gradients(recs, tensor_cores=True)
+    bmin, binv = info["bmin"].astype(np.float64), info["binv"].astype(np.float64)
+    # exact FP64 gradients: BF16 rounding alone separates them
+    rW, rb, rgrid = G.gradients(grid, W, b, bmin, binv, recs.astype(np.float64))
+    # FP64 with the kernel's BF16 roundings: only FP32 accumulation separates them
+    eW, eb, egrid = G.gradients_bf16(grid, W, b, bmin, binv, recs.astype(np.float64))
+    errs = {}
+    for name, got, ref, emu in (("W", gW, rW, eW), ("b", gb, rb, eb), ("grid", ggrid, rgrid, egrid)):
+        got = got.reshape(ref.shape)
+        errs[name] = (np.linalg.norm(got - ref) / np.linalg.norm(ref), np.linalg.norm(got - emu) / np.linalg.norm(emu))
+    for l in range(G.LAYERS):
+        got, emu = gW.reshape(rW.shape)[l], eW[l]
+        errs[f"W{l}"] = (0.0, np.linalg.norm(got - emu) / np.linalg.norm(emu))
+    for name, (exact, emulated) in errs.items():
+        assert emulated < 5e-3, (name, errs)
+        assert exact < 0.15, (name, errs)
 
 
 def test_guided_render_is_unbiased(cr, scenes):
@@ -139,4 +171,7 @@ def test_guided_render_is_unbiased(cr, scenes):
     assert cr.Guide(s).info()["step"] == 16  # 2 renders x 4 waves, two steps each
     z = zscores(guided, plain)
     assert (z > 3).mean() < 0.01, (z > 3).mean()
-    assert abs(guided.mean.mean() / plain.mean.mean() - 1) < 0.01
+    # the image means: their difference against its standard error (all pixels)
+    diff = guided.mean.sum() - plain.mean.sum()
+    se = np.sqrt((guided.var_of_mean + plain.var_of_mean).sum())
+    assert abs(diff) < 4 * se, (diff / se, guided.mean.mean(), plain.mean.mean())

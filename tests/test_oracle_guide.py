@@ -69,3 +69,13 @@ def test_mixture_is_a_density():
     q = sum(pis[k] * kaps[k] / (2 * np.pi * (-np.expm1(-2 * kaps[k]))) * np.exp(kaps[k] * (v @ mus[k] - 1))
             for k in range(G.LOBES))
     assert abs(q.mean() * 4 * np.pi - 1) < 0.02
+
+
+def test_bf16_rounding_is_nearest_even():
+    import guide_oracle as G
+    x = np.array([1.0, 1 + 2 ** -8, 1 + 3 * 2 ** -8, -(1 + 2 ** -7), 3.0e38, 1e-40])
+    got = G.bf16(x)
+    np.testing.assert_array_equal(got[:4], [1.0, 1.0, 1 + 2 ** -6, -(1 + 2 ** -7)])
+    assert np.isfinite(got[4]) and abs(got[4] / 3.0e38 - 1) < 2 ** -8
+    # BF16 keeps FP32's exponent range: tiny values are not flushed
+    assert got[5] > 0
