@@ -21,6 +21,9 @@ cpu_baseline / --impl reference
            the reference's own CPUMulticoreTracer::execute compiled from its
            sources (oracle/_ref/cr_ref), on this host's cores, on a bounded
            sample of the same workload (full resolution, fewer spp).
+guiding    time to relMSE 1e-3, plain MIS vs learned guiding (tensor-core
+           inference and online training included), on the occluded-light
+           scene at 1024x1024 (see guided_vs_plain); rank 0 at N = 1 only.
 Multi-GPU: one process per GPU; each rank renders the workload with its own
 seed (weak scaling, no data-path collective).
 """
@@ -40,7 +43,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))  # the CPU-baseline leg only
 
 WIDTH, HEIGHT, SPP, LEVEL, MAX_BOUNCE = 1024, 768, 256, 8, 7
-METRIC = "Msamples/s (camera paths per second), plain wavefront, 1024x768x256spp, 1.31M-tri displaced icosphere"
+METRIC = ("Msamples/s (camera paths per second), plain wavefront, 1024x768x256spp, 1.31M-tri displaced icosphere; "
+          "time-to-relMSE 1e-3 guided vs plain in 'guiding'")
 NODE_BYTES, TRI_BYTES, RAY_BYTES = 80, 48, 32 + 16
 
 
@@ -188,6 +192,80 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------- our arm
+def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
+    """Time to relMSE <= target, plain MIS vs learned guiding, on the
+    occluded-light scene (1024x1024, ~492k triangles, max depth 8).
+
+    relMSE = mean over pixels and channels of ((I - R)^2 - Var[R]) / (R^2 + 1e-2),
+    R a plain MIS render of ref_spp samples per pixel (Var[R] its per-pixel
+    variance of the mean, removed so that the figure estimates the error
+    against the converged image).  Each run renders 4 spp per call into one
+    film; its clock is the device time of those calls (CUDA events), guided
+    runs including their inference and online training.  A run stops at the
+    target or after tmax_s."""
+    import torch
+    from cuda_raytracer_b200 import scenes
+    res = 1024
+    d = scenes.config3(width=res, height=res)
+    sc = cr.Scene.from_desc(d)
+    n = res * res
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def film():
+        return (torch.zeros(n * 3, dtype=torch.float64, device=dev), torch.zeros(n * 3, dtype=torch.float64, device=dev),
+                torch.zeros(n, dtype=torch.int32, device=dev))
+
+    def render(f, spp, seed, guiding):
+        desc = cr.render_desc(res, res, spp, max_bounce=MAX_BOUNCE, estimator=cr.MIS, seed=seed, guiding=guiding)
+        sc.render_device(desc, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), stream=stream, stats=False)
+
+    R = film()
+    for i in range(ref_spp // 64):
+        render(R, 64, 1_000_000 + i, False)
+    torch.cuda.synchronize(dev)
+    cnt = R[2].double().repeat_interleave(3)
+    Rm = R[0] / cnt
+    Rvar = (R[1] / cnt - Rm * Rm).clamp_min(0) / cnt
+    den = Rm * Rm + 1e-2
+    del R
+
+    def run(guiding):
+        if guiding:
+            cr.Guide(sc).reset(seed=7)
+        F = film()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms, spp, k, hit, err = 0.0, 0, 0, None, None
+        while ms < tmax_s * 1e3:
+            e0.record()
+            render(F, 4, 1 + k, guiding)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms += e0.elapsed_time(e1)
+            spp += 4
+            k += 1
+            c2 = F[2].double().repeat_interleave(3)
+            err = (((F[0] / c2 - Rm) ** 2 - Rvar) / den).mean().item()
+            if err <= target:
+                hit = ms / 1e3
+                break
+        return {"time_to_target_s": None if hit is None else round(hit, 3), "spp": spp,
+                "relmse_at_stop": float(f"{err:.4e}"), "device_s": round(ms / 1e3, 3),
+                "msamples_per_s": round(n * spp / (ms / 1e3) / 1e6, 2)}
+
+    plain = run(False)
+    guided = run(True)
+    g = cr.Guide(sc)
+    out = {"workload": "config3: occluded light (wall with a 0.4x0.4 aperture), 1024x1024, "
+                       f"{sc.info()['triangles']} triangles, max depth 8, MIS estimator",
+           "metric": f"device seconds to relMSE <= {target:g} against a {ref_spp}-spp plain reference",
+           "reference_spp": ref_spp, "max_seconds": tmax_s, "plain": plain, "guided": guided,
+           "guide": {"steps": g.info()["step"], **{k: v for k, v in g.configure().items()}},
+           "speedup": (round(plain["time_to_target_s"] / guided["time_to_target_s"], 3)
+                       if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
+    sc.close()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -309,6 +387,12 @@ def run_ours(args):
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/cr_ref not built"}
 
+    guiding = None
+    if rank == 0 and world == 1 and args.guide_seconds > 0:
+        del s, q, c, flush
+        torch.cuda.empty_cache()
+        guiding = guided_vs_plain(cr, dev, args.guide_seconds, args.guide_ref_spp)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -335,6 +419,7 @@ def run_ours(args):
             "e2e": e2e,
             "clocks": clk,
             "gpu_launches": totals["launches"],
+            "guiding": guiding,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -353,6 +438,9 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=4, help="spp of the reference's bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--guide-seconds", type=float, default=25.0,
+                    help="device-time cap of each guided/plain time-to-relMSE run (0: skip them)")
+    ap.add_argument("--guide-ref-spp", type=int, default=4096)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
