@@ -79,6 +79,12 @@ class GuideConfig(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchJob(C.Structure):
+    """cr_batch_job: one scene's render inside a batch."""
+    _fields_ = [("scene", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("seed", C.c_uint64), ("d_sum", C.c_void_p), ("d_sumsq", C.c_void_p), ("d_count", C.c_void_p)]
+
+
 _lib = None
 
 
@@ -115,6 +121,8 @@ def lib():
             "cr_guide_gradients": (I, [P, P, U64, P, P, P]),
             "cr_guide_configure": (I, [P, P, P]), "cr_guide_loss": (I, [P, P]),
             "cr_guide_forward_tc": (I, [P, P, U64, P]), "cr_guide_gradients_tc": (I, [P, P, U64, P, P, P]),
+            "cr_batch_create": (I, [P, U32, U32, C.c_int32, P, P]), "cr_batch_autotune": (I, [P, P]),
+            "cr_batch_render": (I, [P, U64, P]), "cr_batch_destroy": (None, [P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
         }
@@ -320,6 +328,43 @@ class Guide:
         fn = lib().cr_guide_gradients_tc if tensor_cores else lib().cr_guide_gradients
         _check(fn(self.scene.h, _p(records), len(records), _p(gW), _p(gb), _p(ggrid)))
         return ggrid, gW, gb
+
+
+class Batch:
+    """A batched render of many scenes (cr_batch_*): jobs are (scene, width,
+    height, spp, seed, sum_ptr, sumsq_ptr, count_ptr) with device films; the
+    first render captures a CUDA graph that later renders replay."""
+
+    def __init__(self, jobs, max_bounce=7, estimator=KOISHI, stream=0):
+        self.scenes = [j[0] for j in jobs]  # keep the scenes alive with the batch
+        arr = (BatchJob * len(jobs))()
+        for a, (sc, w, h, spp, seed, ps, pq, pc) in zip(arr, jobs):
+            a.scene, a.width, a.height, a.spp, a.seed = sc.h.value, w, h, spp, seed
+            a.d_sum, a.d_sumsq, a.d_count = ps, pq, pc
+        out = C.c_void_p()
+        _check(lib().cr_batch_create(arr, len(jobs), max_bounce, estimator, C.c_void_p(stream), C.byref(out)))
+        self.h = out
+
+    def autotune(self):
+        t = Tuning()
+        _check(lib().cr_batch_autotune(self.h, C.byref(t)))
+        return t
+
+    def render(self, seed_offset=0, stats=True):
+        st = Stats() if stats else None
+        _check(lib().cr_batch_render(self.h, seed_offset, C.byref(st) if st is not None else None))
+        return st
+
+    def close(self):
+        if self.h and self.h.value:
+            lib().cr_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def render_file(json_path, png_path, spp=1, width=1024, height=768, kernel="Radiance", tracer="CudaWavefront",

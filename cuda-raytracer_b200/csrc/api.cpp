@@ -1354,6 +1354,280 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 	} );
 }
 
+// ------------------------------------------------------------------ batches
+struct cr_batch
+{
+	std::vector<cr_batch_job> req;   // the caller's job table
+	std::vector<BatchJobDev> jobs;   // host copy of the device table
+	DevScene *d_scenes = nullptr;
+	BatchJobDev *d_jobs = nullptr;
+	uint64_t *d_seed = nullptr;
+	uint64_t total = 0;              // samples per render
+	uint32_t max_bounce = 7;
+	int estimator = EST_KOISHI;
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	WaveBuffers wave;
+	uint32_t wave_bounces = 0;
+	uint32_t tune_wave = 1u << 22, tune_refill = 16;
+	int tune_blocks = 8;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	uint32_t launches_per_render = 0;
+
+	void drop_graph()
+	{
+		if ( exec ) cudaGraphExecDestroy( exec );
+		if ( graph ) cudaGraphDestroy( graph );
+		exec = nullptr, graph = nullptr;
+	}
+	~cr_batch()
+	{
+		drop_graph();
+		if ( wave.capacity ) free_wave( wave, stream );
+		if ( stream ) cudaStreamSynchronize( stream );
+		for ( void *p : { (void *)d_scenes, (void *)d_jobs, (void *)d_seed } )
+			if ( p ) cudaFree( p );
+		if ( own_stream && stream ) cudaStreamDestroy( stream );
+	}
+};
+
+namespace
+{
+// Device scene and job tables of a batch, every job at spp / spp_div (>= 1);
+// films: the caller's, or `films` (sum, sumsq, count base pointers laid out job
+// after job) when not null.
+void batch_tables( const cr_batch *b, uint32_t spp_div, double *films_sum, double *films_sq, uint32_t *films_cnt,
+				   std::vector<BatchJobDev> &jobs, std::vector<DevScene> &scenes )
+{
+	jobs.clear(), scenes.clear();
+	uint64_t fs = 0, fp = 0;
+	for ( const cr_batch_job &r : b->req )
+	{
+		BatchJobDev j{};
+		j.width = r.width, j.height = r.height, j.spp = std::max<uint32_t>( 1, r.spp / spp_div );
+		j.first_sample = fs, j.first_pixel = fp, j.seed = r.seed;
+		if ( films_sum )
+			j.sum = films_sum + 3 * fp, j.sumsq = films_sq + 3 * fp, j.count = films_cnt + fp;
+		else
+			j.sum = r.d_sum, j.sumsq = r.d_sumsq, j.count = r.d_count;
+		DevScene sc = dev_scene( r.scene );
+		sc.cam = make_camera( r.scene->cam, r.width, r.height, j.spp );
+		jobs.push_back( j ), scenes.push_back( sc );
+		fs += uint64_t( r.width ) * r.height * j.spp;
+		fp += uint64_t( r.width ) * r.height;
+	}
+}
+
+void upload( void *dst, const void *src, size_t bytes, cudaStream_t st )
+{
+	cuda_check( cudaMemcpyAsync( dst, src, bytes, cudaMemcpyHostToDevice, st ), "batch upload" );
+}
+
+void batch_ensure_wave( cr_batch *b, uint32_t cap )
+{
+	if ( !( b->wave.capacity >= cap && b->wave_bounces >= b->max_bounce ) )
+	{
+		if ( b->wave.capacity ) free_wave( b->wave, b->stream );
+		alloc_wave( b->wave, cap, b->max_bounce, b->stream );
+		b->wave_bounces = b->max_bounce;
+	}
+	alloc_batch_state( b->wave, b->stream );
+}
+
+RenderConfig batch_config( const cr_batch *b, uint32_t wave, uint32_t refill, int blocks, uint64_t total )
+{
+	RenderConfig c{};
+	c.spp = 1, c.max_bounce = b->max_bounce, c.estimator = b->estimator;
+	c.x0 = c.y0 = 0, c.ww = c.wh = 1, c.seed = 0;
+	c.wave_paths = uint32_t( std::min<uint64_t>( wave, total ) );
+	c.count_work = false;
+	c.refill_min = refill, c.traverse_blocks_per_sm = blocks;
+	return c;
+}
+
+void batch_check_error( cr_batch *b )
+{
+	uint32_t e = 0;
+	cuda_check( cudaMemcpyAsync( &e, b->wave.err, 4, cudaMemcpyDeviceToHost, b->stream ), "error word" );
+	cuda_check( cudaStreamSynchronize( b->stream ), "error word" );
+	if ( e ) fail( CR_ERR_DEVICE, "a batched render kernel reported error flags " + std::to_string( e ) );
+}
+}  // namespace
+
+int cr_batch_create( const cr_batch_job *jobs, uint32_t n_jobs, uint32_t max_bounce, int32_t estimator, void *stream,
+					 cr_batch **out )
+{
+	return guarded( [&] {
+		if ( !out ) fail( CR_ERR_INVALID, "null output" );
+		*out = nullptr;
+		if ( !jobs || n_jobs == 0 ) fail( CR_ERR_INVALID, "empty batch" );
+		if ( n_jobs > 65536 ) fail( CR_ERR_INVALID, "more than 65536 jobs in a batch" );
+		if ( max_bounce > 1024 ) fail( CR_ERR_INVALID, "max_bounce out of range" );
+		if ( estimator != EST_KOISHI && estimator != EST_MIS ) fail( CR_ERR_INVALID, "unknown estimator" );
+		for ( uint32_t i = 0; i < n_jobs; ++i )
+		{
+			const cr_batch_job &j = jobs[ i ];
+			const std::string at = "batch job " + std::to_string( i ) + ": ";
+			if ( !j.scene || !j.scene->committed ) fail( CR_ERR_STATE, at + "scene missing or not committed" );
+			if ( !j.scene->has_camera ) fail( CR_ERR_INVALID, at + "no camera in the scene" );
+			if ( j.scene->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, at + "orthographic lens is outside the Radiance path" );
+			if ( !j.width || !j.height || !j.spp ) fail( CR_ERR_INVALID, at + "width, height and spp must be positive" );
+			if ( !j.d_sum || !j.d_sumsq || !j.d_count ) fail( CR_ERR_INVALID, at + "null film" );
+		}
+		std::unique_ptr<cr_batch> b( new cr_batch );
+		b->req.assign( jobs, jobs + n_jobs );
+		b->max_bounce = max_bounce, b->estimator = estimator;
+		if ( stream )
+			b->stream = (cudaStream_t)stream;
+		else
+		{
+			cuda_check( cudaStreamCreateWithFlags( &b->stream, cudaStreamNonBlocking ), "batch stream" );
+			b->own_stream = true;
+		}
+		std::vector<DevScene> scenes;
+		batch_tables( b.get(), 1, nullptr, nullptr, nullptr, b->jobs, scenes );
+		const BatchJobDev &last = b->jobs.back();
+		b->total = last.first_sample + uint64_t( last.width ) * last.height * last.spp;
+		cuda_check( cudaMalloc( (void **)&b->d_scenes, sizeof( DevScene ) * n_jobs ), "cudaMalloc" );
+		cuda_check( cudaMalloc( (void **)&b->d_jobs, sizeof( BatchJobDev ) * n_jobs ), "cudaMalloc" );
+		cuda_check( cudaMalloc( (void **)&b->d_seed, sizeof( uint64_t ) ), "cudaMalloc" );
+		upload( b->d_scenes, scenes.data(), sizeof( DevScene ) * n_jobs, b->stream );
+		upload( b->d_jobs, b->jobs.data(), sizeof( BatchJobDev ) * n_jobs, b->stream );
+		cuda_check( cudaMemsetAsync( b->d_seed, 0, sizeof( uint64_t ), b->stream ), "batch" );
+		cuda_check( cudaStreamSynchronize( b->stream ), "batch" );
+		*out = b.release();
+	} );
+}
+
+int cr_batch_autotune( cr_batch *b, cr_tuning *out )
+{
+	return guarded( [&] {
+		if ( !b || !out ) fail( CR_ERR_INVALID, "null argument" );
+		cudaStream_t st = b->stream;
+		uint64_t npx = b->jobs.back().first_pixel + uint64_t( b->jobs.back().width ) * b->jobs.back().height;
+		double *sum = nullptr, *sq = nullptr;
+		uint32_t *cnt = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+		std::vector<BatchJobDev> jobs;
+		std::vector<DevScene> scenes;
+		batch_tables( b, 16, sum, sq, cnt, jobs, scenes );
+		const uint32_t n = uint32_t( jobs.size() );
+		const uint64_t total = jobs.back().first_sample + uint64_t( jobs.back().width ) * jobs.back().height * jobs.back().spp;
+		DevScene *d_scenes = nullptr;
+		BatchJobDev *d_jobs = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&d_scenes, sizeof( DevScene ) * n, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_jobs, sizeof( BatchJobDev ) * n, st ), "cudaMalloc" );
+		upload( d_scenes, scenes.data(), sizeof( DevScene ) * n, st );
+		upload( d_jobs, jobs.data(), sizeof( BatchJobDev ) * n, st );
+		BatchDev bd{ d_scenes, d_jobs, b->d_seed, n };
+		uint32_t tried = 0;
+		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
+			RenderConfig c = batch_config( b, wave, refill, blocks, total );
+			batch_ensure_wave( b, c.wave_paths );
+			StageTimes warm, t;
+			render_batch_waves( bd, jobs.data(), n, c, b->wave, st, &warm );
+			render_batch_waves( bd, jobs.data(), n, c, b->wave, st, &t );
+			++tried;
+			return double( total ) / ( t.total * 1e3 );
+		};
+		uint32_t wave = 1u << 22, refill = 16;
+		int blocks = 8;
+		double best = rate( wave, refill, blocks ), dflt = best;
+		for ( uint32_t r : { 8u, 12u, 24u } )
+		{
+			double v = rate( wave, r, blocks );
+			if ( v > best ) best = v, refill = r;
+		}
+		for ( int bl : { 4, 6 } )
+		{
+			double v = rate( wave, refill, bl );
+			if ( v > best ) best = v, blocks = bl;
+		}
+		for ( uint32_t w : { 1u << 21, 1u << 23 } )
+		{
+			if ( w > total && wave >= total ) continue;
+			double v = rate( w, refill, blocks );
+			if ( v > best ) best = v, wave = w;
+		}
+		for ( void *p : { (void *)sum, (void *)sq, (void *)cnt, (void *)d_scenes, (void *)d_jobs } ) cudaFreeAsync( p, st );
+		cuda_check( cudaStreamSynchronize( st ), "batch autotune" );
+		batch_check_error( b );
+		b->tune_wave = wave, b->tune_refill = refill, b->tune_blocks = blocks;
+		b->drop_graph();
+		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
+		out->candidates_tried = tried;
+		out->msamples_per_s = best;
+		out->default_msamples_per_s = dflt;
+	} );
+}
+
+int cr_batch_render( cr_batch *b, uint64_t seed_offset, cr_stats *stats )
+{
+	return guarded( [&] {
+		if ( !b ) fail( CR_ERR_INVALID, "null batch" );
+		cudaStream_t st = b->stream;
+		const uint32_t n = uint32_t( b->jobs.size() );
+		RenderConfig c = batch_config( b, b->tune_wave, b->tune_refill, b->tune_blocks, b->total );
+		if ( !b->exec )
+		{
+			// capture the whole batch (every wave, every bounce) once
+			batch_ensure_wave( b, c.wave_paths );
+			cuda_check( cudaStreamSynchronize( st ), "batch" );
+			BatchDev bd{ b->d_scenes, b->d_jobs, b->d_seed, n };
+			cuda_check( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ), "graph capture" );
+			try
+			{
+				render_batch_waves( bd, b->jobs.data(), n, c, b->wave, st, nullptr );
+			}
+			catch ( ... )
+			{
+				cudaGraph_t g = nullptr;
+				cudaStreamEndCapture( st, &g );
+				if ( g ) cudaGraphDestroy( g );
+				throw;
+			}
+			cuda_check( cudaStreamEndCapture( st, &b->graph ), "graph capture" );
+			cuda_check( cudaGraphInstantiate( &b->exec, b->graph, 0 ), "graph instantiate" );
+			size_t nodes = 0;
+			cuda_check( cudaGraphGetNodes( b->graph, nullptr, &nodes ), "graph" );
+			b->launches_per_render = uint32_t( nodes );
+		}
+		upload( b->d_seed, &seed_offset, sizeof( uint64_t ), st );
+		cudaEvent_t e0 = nullptr, e1 = nullptr;
+		if ( stats )
+		{
+			cuda_check( cudaEventCreate( &e0 ), "event" ), cuda_check( cudaEventCreate( &e1 ), "event" );
+			cuda_check( cudaEventRecord( e0, st ), "event" );
+		}
+		cudaError_t le = cudaGraphLaunch( b->exec, st );
+		if ( stats )
+		{
+			cudaEventRecord( e1, st );
+			cudaError_t se = cudaEventSynchronize( e1 );
+			float ms = 0.f;
+			if ( le == cudaSuccess && se == cudaSuccess ) cudaEventElapsedTime( &ms, e0, e1 );
+			cudaEventDestroy( e0 ), cudaEventDestroy( e1 );
+			cuda_check( le, "graph launch" );
+			cuda_check( se, "batched render" );
+			batch_check_error( b );
+			unsigned long long t[ 2 ] = { 0, 0 };
+			cuda_check( cudaMemcpy( t, b->wave.tally, sizeof t, cudaMemcpyDeviceToHost ), "tally" );
+			StageTimes tm;
+			tm.total = ms, tm.rays_extend = t[ 0 ], tm.rays_shadow = t[ 1 ];
+			tm.launches = b->launches_per_render;
+			tm.waves = uint32_t( ( b->total + c.wave_paths - 1 ) / c.wave_paths );
+			fill_stats( stats, tm, b->total );
+		}
+		else
+			cuda_check( le, "graph launch" );
+	} );
+}
+
+void cr_batch_destroy( cr_batch *b ) { delete b; }
+
 int cr_guide_reset( cr_scene *s, uint64_t seed )
 {
 	return guarded( [&] {

@@ -78,6 +78,7 @@ __global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveA
 // Closest-hit queue of one bounce: rays from the path state, hit records out.
 struct ExtendIO
 {
+	static constexpr bool MULTI = false;
 	const uint32_t *queue;
 	const float4 *ray_o, *ray_d;
 	HitRec *hit;
@@ -93,6 +94,7 @@ struct ExtendIO
 // Shadow queue of one bounce: an unoccluded ray adds its contribution.
 struct ShadowIO
 {
+	static constexpr bool MULTI = false;
 	const uint32_t *queue;
 	const float4 *ray_o, *ray_d, *contrib;
 	float4 *L;
@@ -110,9 +112,27 @@ struct ShadowIO
 	}
 };
 
+// The same queues in a batched render: each path's scene is its job's.
+struct BatchExtendIO : ExtendIO
+{
+	static constexpr bool MULTI = true;
+	const DevScene *scenes;
+	const uint32_t *path_job;
+	__device__ const DevScene *scene( uint32_t item ) const { return scenes + path_job[ item ]; }
+};
+
+struct BatchShadowIO : ShadowIO
+{
+	static constexpr bool MULTI = true;
+	const DevScene *scenes;
+	const uint32_t *path_job;
+	__device__ const DevScene *scene( uint32_t item ) const { return scenes + path_job[ item ]; }
+};
+
 // Batched ray queries of the C ABI: n x {o, d, tmax} in, cr_hit out.
 struct QueryIO
 {
+	static constexpr bool MULTI = false;
 	const float *rays;
 	cr_hit *out;
 	const float4 *tris, *attrs;
@@ -475,8 +495,57 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	out.rd = make_float4( nd.x, nd.y, nd.z, INFINITY );
 }
 
+__device__ __forceinline__ uint2 philox_key( uint64_t seed )
+{
+	return make_uint2( uint32_t( seed ), uint32_t( seed >> 32 ) ^ 0x5EED5EEDu );
+}
+
+// Last job whose first global sample (pixel) is <= g: binary search.
+template <bool PIXELS>
+__device__ __forceinline__ uint32_t find_job( const BatchJobDev *jobs, uint32_t n, uint64_t g )
+{
+	uint32_t lo = 0, hi = n;
+	while ( hi - lo > 1 )
+	{
+		uint32_t mid = ( lo + hi ) >> 1;
+		if ( ( PIXELS ? jobs[ mid ].first_pixel : jobs[ mid ].first_sample ) <= g )
+			lo = mid;
+		else
+			hi = mid;
+	}
+	return lo;
+}
+
+// Camera rays of a batched wave: global sample -> job -> pixel and sample index.
+__global__ void k_generate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa )
+{
+	if ( blockIdx.x == 0 && threadIdx.x == 0 ) wb.counters[ CNT_EXT ] = wa.n;
+	for ( uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < wa.n; s += gridDim.x * blockDim.x )
+	{
+		const uint64_t g = wa.first + s;
+		const uint32_t j = find_job<false>( bd.jobs, bd.n_jobs, g );
+		const BatchJobDev &job = bd.jobs[ j ];
+		const uint64_t local = g - job.first_sample;
+		const uint32_t pix = uint32_t( local / job.spp ), k = uint32_t( local % job.spp );
+		const uint32_t x = pix % job.width, y = pix / job.width;
+		const DevCamera &c = bd.scenes[ j ].cam;
+		float fx = float( x ) - float( c.width ) * 0.5f, fy = float( y ) - float( c.height ) * 0.5f;
+		float3 t = f3( c.n ) + f3( c.u ) * fx + f3( c.v ) * fy;
+		float3 d = normalize( t + f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
+		wb.ray_o[ s ] = make_float4( c.o[ 0 ], c.o[ 1 ], c.o[ 2 ], 0.f );
+		wb.ray_d[ s ] = make_float4( d.x, d.y, d.z, INFINITY );
+		wb.beta[ s ] = make_float4( 1.f, 1.f, 1.f, 0.f );
+		wb.L[ s ] = make_float4( 0.f, 0.f, 0.f, 0.f );
+		wb.queue[ 0 ][ s ] = s;
+		wb.path_job[ s ] = j;
+	}
+}
+
+// BATCH: the wave mixes several jobs; each path shades in its job's scene with
+// its job's random key, and `sc` and `key` are unused.
+template <bool BATCH>
 __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
-												  uint32_t bounce, uint2 key )
+												  uint32_t bounce, uint2 key, BatchDev bd )
 {
 	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
 	const uint32_t *q = wb.queue[ bounce & 1 ];
@@ -514,14 +583,29 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 				// Random streams are keyed by the absolute (pixel, sample), so a
 				// film does not depend on the window or the wave size.
 				uint64_t gw = wa.first + path;
-				uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
-				uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
-				if ( cfg.estimator == EST_MIS )
-					shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
-							   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 * G_LOBES : nullptr,
-							   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
+				if constexpr ( BATCH )
+				{
+					// a job renders its whole image: its local sample index is the key
+					const uint32_t j = wb.path_job[ path ];
+					const BatchJobDev &job = bd.jobs[ j ];
+					const uint2 jkey = philox_key( job.seed + *bd.seed_offset );
+					const uint64_t g = gw - job.first_sample;
+					if ( cfg.estimator == EST_MIS )
+						shade_mis( bd.scenes[ j ], cfg, jkey, g, bounce, ro, rd, h, beta, L, out, nullptr, 0xFFFFFFFFu );
+					else
+						shade_koishi( bd.scenes[ j ], cfg, jkey, g, bounce, ro, rd, h, beta, L, out );
+				}
 				else
-					shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
+				{
+					uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
+					uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
+					if ( cfg.estimator == EST_MIS )
+						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
+								   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 * G_LOBES : nullptr,
+								   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
+					else
+						shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
+				}
 				wb.beta[ path ] = beta;
 				wb.L[ path ] = L;
 				if ( out.alive )
@@ -600,6 +684,43 @@ __global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, dou
 		sumsq[ 3 * p ] += q0, sumsq[ 3 * p + 1 ] += q1, sumsq[ 3 * p + 2 ] += q2;
 		count[ p ] += c;
 	}
+}
+
+// Film accumulation of a batched wave: global pixels p0..p1 (those whose
+// samples meet the wave), each into its job's film.
+__global__ void k_accumulate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa, uint64_t p0, uint64_t p1 )
+{
+	for ( uint64_t p = p0 + blockIdx.x * blockDim.x + threadIdx.x; p <= p1; p += gridDim.x * blockDim.x )
+	{
+		const uint32_t j = find_job<true>( bd.jobs, bd.n_jobs, p );
+		const BatchJobDev &job = bd.jobs[ j ];
+		const uint64_t lp = p - job.first_pixel;
+		const uint64_t f0 = job.first_sample + lp * job.spp;
+		uint64_t s0 = max( f0, wa.first ), s1 = min( f0 + job.spp, wa.first + wa.n );
+		double a0 = 0, a1 = 0, a2 = 0, q0 = 0, q1 = 0, q2 = 0;
+		uint32_t c = 0;
+		for ( uint64_t s = s0; s < s1; ++s )
+		{
+			float4 l = wb.L[ s - wa.first ];
+			if ( !isfinite( l.x ) || !isfinite( l.y ) || !isfinite( l.z ) ) continue;  // cpuMulticore.cu:58-64
+			++c;
+			a0 += l.x, a1 += l.y, a2 += l.z;
+			q0 += double( l.x ) * l.x, q1 += double( l.y ) * l.y, q2 += double( l.z ) * l.z;
+		}
+		job.sum[ 3 * lp ] += a0, job.sum[ 3 * lp + 1 ] += a1, job.sum[ 3 * lp + 2 ] += a2;
+		job.sumsq[ 3 * lp ] += q0, job.sumsq[ 3 * lp + 1 ] += q1, job.sumsq[ 3 * lp + 2 ] += q2;
+		job.count[ lp ] += c;
+	}
+}
+
+// Adds one wave's queue lengths to the running ray tally (batched renders,
+// which keep no host round trip per wave).
+__global__ void k_tally( const uint32_t *counters, uint32_t max_bounce, unsigned long long *tally )
+{
+	if ( threadIdx.x != 0 || blockIdx.x != 0 ) return;
+	unsigned long long e = 0, sh = 0;
+	for ( uint32_t b = 0; b <= max_bounce; ++b ) e += counters[ CPB * b + CNT_EXT ], sh += counters[ CPB * b + CNT_SHADOW ];
+	tally[ 0 ] += e, tally[ 1 ] += sh;
 }
 
 __global__ void k_bsdf_eval( int est, DevShader sh, const float *wo, const float *wi, uint64_t n, float *f, float *pdf )
@@ -707,7 +828,7 @@ void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaSt
 void free_wave( WaveBuffers &wb, cudaStream_t st )
 {
 	void *ps[] = { wb.ray_o, wb.ray_d, wb.hit, wb.beta, wb.L, wb.queue[ 0 ], wb.queue[ 1 ], wb.shadow_queue,
-				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work, wb.lobes };
+				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work, wb.lobes, wb.path_job, wb.tally };
 	for ( void *p : ps )
 		if ( p ) cudaFreeAsync( p, st );
 	wb = WaveBuffers();
@@ -717,6 +838,121 @@ void alloc_lobes( WaveBuffers &wb, cudaStream_t st )
 {
 	if ( wb.lobes ) return;
 	alloc( wb.lobes, size_t( wb.capacity ) * 5 * G_LOBES, st );
+}
+
+void alloc_batch_state( WaveBuffers &wb, cudaStream_t st )
+{
+	if ( !wb.path_job ) alloc( wb.path_job, wb.capacity, st );
+	if ( !wb.tally ) alloc( wb.tally, 2, st );
+}
+
+void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
+						 WaveBuffers &wb, cudaStream_t st, StageTimes *times )
+{
+	if ( n_jobs == 0 ) return;
+	if ( !wb.path_job || !wb.tally ) throw std::runtime_error( "batched render without its wave state" );
+	if ( cfg.wave_paths == 0 || cfg.wave_paths > wb.capacity )
+		throw std::runtime_error( "wave size exceeds the allocated wave buffers" );
+	const BatchJobDev &last = jobs[ n_jobs - 1 ];
+	const uint64_t total = last.first_sample + uint64_t( last.width ) * last.height * last.spp;
+	const uint32_t P = cfg.wave_paths;
+	const int sms = sm_count();
+	const int g_ext = sms * std::max( 1, std::min( 8, cfg.traverse_blocks_per_sm ) );
+	const int g_shade = sms * 8;
+	EventPool pool;
+	struct Mark
+	{
+		cudaEvent_t a, b;
+		int kind;
+	};
+	std::vector<Mark> marks;
+	cudaEvent_t t0 = nullptr, t1 = nullptr;
+	if ( times )
+	{
+		t0 = pool.get(), t1 = pool.get();
+		check( cudaEventRecord( t0, st ), "event" );
+	}
+	auto timed = [&]( int kind, auto &&launch ) {
+		if ( !times )
+		{
+			launch();
+			return;
+		}
+		Mark m{ pool.get(), pool.get(), kind };
+		check( cudaEventRecord( m.a, st ), "event" );
+		launch();
+		check( cudaEventRecord( m.b, st ), "event" );
+		marks.push_back( m );
+		times->launches++;
+		if ( kind == 0 ) times->extend_launches++;
+		if ( kind == 1 ) times->shadow_launches++;
+	};
+	// global pixel of a global sample (host copy of the job table)
+	auto pixel_of = [&]( uint64_t g ) {
+		uint32_t lo = 0, hi = n_jobs;
+		while ( hi - lo > 1 )
+		{
+			uint32_t mid = ( lo + hi ) >> 1;
+			( jobs[ mid ].first_sample <= g ? lo : hi ) = mid;
+		}
+		return jobs[ lo ].first_pixel + ( g - jobs[ lo ].first_sample ) / jobs[ lo ].spp;
+	};
+	check( cudaMemsetAsync( wb.tally, 0, 2 * sizeof( unsigned long long ), st ), "memset" );
+	for ( uint64_t first = 0; first < total; first += P )
+	{
+		WaveArgs wa{ first, uint32_t( std::min<uint64_t>( P, total - first ) ) };
+		check( cudaMemsetAsync( wb.counters, 0, sizeof( uint32_t ) * wb.n_counters, st ), "memset" );
+		timed( 3, [&] {
+			int gg = int( std::min<uint64_t>( ( wa.n + 255 ) / 256, uint64_t( sms ) * 16 ) );
+			k_generate_batch<<<gg, 256, 0, st>>>( bd, wb, wa );
+		} );
+		for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
+		{
+			timed( 0, [&] {
+				BatchExtendIO io;
+				io.queue = wb.queue[ b & 1 ], io.ray_o = wb.ray_o, io.ray_d = wb.ray_d, io.hit = wb.hit;
+				io.scenes = bd.scenes, io.path_job = wb.path_job;
+				const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
+				uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
+				k_traverse<BatchExtendIO, false, false><<<g_ext, 128, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err, wb.work,
+																			   cfg.refill_min );
+			} );
+			timed( 2, [&] { k_shade<true><<<g_shade, 128, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd ); } );
+			timed( 1, [&] {
+				BatchShadowIO io;
+				io.queue = wb.shadow_queue, io.ray_o = wb.sh_o, io.ray_d = wb.sh_d, io.contrib = wb.sh_c, io.L = wb.L;
+				io.scenes = bd.scenes, io.path_job = wb.path_job;
+				const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
+				uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
+				k_traverse<BatchShadowIO, true, false><<<g_ext, 128, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
+																			  wb.work + 2, cfg.refill_min );
+			} );
+		}
+		timed( 3, [&] {
+			const uint64_t p0 = pixel_of( first ), p1 = pixel_of( first + wa.n - 1 );
+			int gg = int( std::min<uint64_t>( ( p1 - p0 + 256 ) / 256, uint64_t( sms ) * 16 ) );
+			k_accumulate_batch<<<gg, 256, 0, st>>>( bd, wb, wa, p0, p1 );
+			k_tally<<<1, 32, 0, st>>>( wb.counters, cfg.max_bounce, wb.tally );
+		} );
+		check( cudaGetLastError(), "batched render launch" );
+		if ( times ) times->waves++;
+	}
+	if ( times )
+	{
+		check( cudaEventRecord( t1, st ), "event" );
+		check( cudaEventSynchronize( t1 ), "event" );
+		float ms;
+		check( cudaEventElapsedTime( &ms, t0, t1 ), "event" );
+		times->total += ms;
+		for ( auto &m : marks )
+		{
+			check( cudaEventElapsedTime( &ms, m.a, m.b ), "event" );
+			( m.kind == 0 ? times->extend : m.kind == 1 ? times->shadow : m.kind == 2 ? times->shade : times->other ) += ms;
+		}
+		unsigned long long t[ 2 ];
+		check( cudaMemcpy( t, wb.tally, sizeof t, cudaMemcpyDeviceToHost ), "tally" );
+		times->rays_extend += t[ 0 ], times->rays_shadow += t[ 1 ];
+	}
 }
 
 void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb, double *film_sum, double *film_sumsq,
@@ -812,7 +1048,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				timed( 4, [&] {
 					k_guide_infer<<<sms * 2, tc::THREADS, tc::SMEM_BYTES, st>>>( sc, wc, wb, b, guide->Wp );
 				} );
-			timed( 2, [&] { k_shade<<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key ); } );
+			timed( 2, [&] { k_shade<false><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} ); } );
 			if ( sc.n_lights )
 				timed( 1, [&] {
 					ShadowIO io{ wb.shadow_queue, wb.sh_o, wb.sh_d, wb.sh_c, wb.L };

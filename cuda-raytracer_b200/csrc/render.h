@@ -26,6 +26,28 @@ struct WaveBuffers
 	uint32_t *err = nullptr;                    // device error word
 	unsigned long long *work = nullptr;         // extension [0] nodes [1] triangles, shadow [2] [3]
 	float *lobes = nullptr;                     // guided renders: 8 lobes x (mean, kappa, weight) per path
+	uint32_t *path_job = nullptr;               // batched renders: the job (scene render) of each path
+	unsigned long long *tally = nullptr;        // batched renders: closest-hit and shadow rays traced
+};
+
+// One scene's render inside a batch (device copy).  A job renders its whole
+// image; its samples are global samples first_sample .. + width*height*spp,
+// pixel-major, and its pixels global pixels first_pixel .. + width*height.
+struct BatchJobDev
+{
+	uint64_t first_sample, first_pixel;
+	uint32_t width, height, spp, pad;
+	uint64_t seed;
+	double *sum, *sumsq;
+	uint32_t *count;
+};
+
+struct BatchDev
+{
+	const DevScene *scenes;        // one per job, with the job's camera
+	const BatchJobDev *jobs;
+	const uint64_t *seed_offset;   // added to every job's seed (changes between graph replays)
+	uint32_t n_jobs;
 };
 
 // Device counters per bounce: queue lengths and the traversal kernels' work cursors.
@@ -70,6 +92,16 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				   double *film_sumsq, uint32_t *film_count, cudaStream_t st, StageTimes *times,
 				   GuideState *guide = nullptr );
 void alloc_lobes( WaveBuffers &wb, cudaStream_t st );
+void alloc_batch_state( WaveBuffers &wb, cudaStream_t st );
+
+// Batched render of many scenes: the waves run over the concatenated samples
+// of all jobs, so one launch per stage serves every scene.  `jobs` is the host
+// copy of the device job table.  cfg carries the launch configuration, the
+// estimator and max_bounce (window and spp fields are unused).  With `times`
+// null the call issues kernels and memsets only (no synchronisation), so it
+// can be captured into a CUDA graph.
+void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
+						 WaveBuffers &wb, cudaStream_t st, StageTimes *times );
 
 void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit,
 				   cr_hit *out, uint32_t *err, cudaStream_t st );

@@ -17,10 +17,10 @@ constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
 
 // Intersects the ray with the 8 children of `node`; returns the node-group
 // hits (bits at slot ^ octant) and the triangle-group hits (24-bit mask).
-__device__ __forceinline__ void visit_node( const DevScene &sc, const RayPre &r, uint32_t node, float tmin,
+__device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r, uint32_t node, float tmin,
 											float tlim, uint2 &ng, uint2 &tg )
 {
-	const uint4 *np = reinterpret_cast<const uint4 *>( sc.nodes ) + 5 * size_t( node );
+	const uint4 *np = reinterpret_cast<const uint4 *>( nodes ) + 5 * size_t( node );
 	uint4 n0 = __ldg( np ), n1 = __ldg( np + 1 ), n2 = __ldg( np + 2 ), n3 = __ldg( np + 3 ), n4 = __ldg( np + 4 );
 	float3 p = f3( __uint_as_float( n0.x ), __uint_as_float( n0.y ), __uint_as_float( n0.z ) );
 	uint32_t ex = n0.w & 0xFFu, ey = ( n0.w >> 8 ) & 0xFFu, ez = ( n0.w >> 16 ) & 0xFFu, imask = n0.w >> 24;
@@ -63,6 +63,8 @@ __device__ __forceinline__ void visit_node( const DevScene &sc, const RayPre &r,
 // (1..32) that trigger a refill from the queue.
 //   load(i, item, o, d, tmin, tmax): the i-th queued ray
 //   finish(item, hit, found): store the result
+//   MULTI: the queue mixes the rays of several scenes (a batched render);
+//          scene(item) is the ray's scene, otherwise every ray uses `sc`
 template <class IO, bool ANY, bool COUNT>
 __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, const uint32_t *n_ptr, uint32_t n_host,
 														uint32_t *cursor, uint32_t *err, unsigned long long *work,
@@ -82,6 +84,11 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 	uint2 ng = make_uint2( 0u, 0u ), tg = make_uint2( 0u, 0u );
 	int sp = 0;
 	uint2 stack[ TRAVERSAL_STACK ];
+	// this lane's geometry: the kernel's scene, or the current ray's in a batch
+	const WNode *nodes = sc.nodes;
+	const float4 *tris = sc.tris;
+	const DevSphere *spheres = sc.spheres;
+	uint32_t n_nodes = sc.n_nodes, n_tris = sc.n_tris, n_spheres = sc.n_spheres;
 	for ( ;; )
 	{
 		if ( !exhausted )
@@ -101,22 +108,28 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 						float3 o, d;
 						float tmax;
 						io.load( i, item, o, d, tmin, tmax );
+						if constexpr ( IO::MULTI )
+						{
+							const DevScene *ps = io.scene( item );
+							nodes = ps->nodes, tris = ps->tris, spheres = ps->spheres;
+							n_nodes = ps->n_nodes, n_tris = ps->n_tris, n_spheres = ps->n_spheres;
+						}
 						hit.t = tmax;
 						hit.id = HIT_MISS;
 						hit.u = hit.v = 0.f;
 						found = false;
 						bool done = false;
-						for ( uint32_t s = 0; s < sc.n_spheres && !done; ++s )
+						for ( uint32_t s = 0; s < n_spheres && !done; ++s )
 						{
 							float t;
-							if ( sphere_test( sc.spheres[ s ], o, d, tmin, hit.t, t ) )
+							if ( sphere_test( spheres[ s ], o, d, tmin, hit.t, t ) )
 							{
 								hit.t = t, hit.id = HIT_SPHERE | s, found = true;
 								if ( ANY ) done = true;
 							}
 						}
 						// A NaN ray would pass every slab test; it hits nothing.
-						if ( done || sc.n_nodes == 0 || !finite3( o ) || !finite3( d ) )
+						if ( done || n_nodes == 0 || !finite3( o ) || !finite3( d ) )
 							io.finish( item, hit, found );
 						else
 						{
@@ -124,7 +137,7 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 							ng = make_uint2( 0u, ( 1u << ( 24 + r.oct ) ) | 1u );
 							tg = make_uint2( 0u, 0u );
 							sp = 0;
-							budget = sc.n_nodes;
+							budget = n_nodes;
 							active = true;
 						}
 					}
@@ -148,14 +161,14 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 				uint32_t k = __ffs( tg.y ) - 1;
 				tg.y &= tg.y - 1u;
 				uint32_t ti = tg.x + k;
-				if ( ti >= sc.n_tris )
+				if ( ti >= n_tris )
 				{
 					atomicOr( err, 4u );
 					tg.y = 0u;
 				}
 				else
 				{
-					const float4 *tp = sc.tris + 3 * size_t( ti );
+					const float4 *tp = tris + 3 * size_t( ti );
 					float4 a = __ldg( tp ), b = __ldg( tp + 1 ), c = __ldg( tp + 2 );
 					if ( COUNT ) ++wtris;
 					float t, u, v;
@@ -175,7 +188,7 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 				ng.y &= ~( 1u << ( 24 + b ) );
 				uint32_t slot = b ^ r.oct;
 				uint32_t node = ng.x + __popc( ng.y & 0xFFu & ( ( 1u << slot ) - 1u ) );
-				if ( node >= sc.n_nodes || budget-- == 0 )
+				if ( node >= n_nodes || budget-- == 0 )
 				{
 					atomicOr( err, 2u );
 					done = true;
@@ -190,7 +203,7 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 							atomicOr( err, 1u );
 					}
 					if ( COUNT ) ++wnodes;
-					visit_node( sc, r, node, tmin, hit.t * grow, ng, tg );
+					visit_node( nodes, r, node, tmin, hit.t * grow, ng, tg );
 				}
 			}
 			else if ( sp > 0 )

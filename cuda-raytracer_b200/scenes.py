@@ -297,6 +297,92 @@ def config1(level=8, seed=1, width=1024, height=768, spp=256) -> SceneDesc:
                      spp=spp, max_bounce=7, name=f"config1_l{level}")
 
 
+def _boxes(rng, count, lo, hi):
+    """`count` axis-aligned boxes (12 triangles each, flat outward normals) with
+    random centres in [lo, hi] and edge lengths U[0.05, 0.4]."""
+    if count <= 0:
+        return np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 3), np.uint32)
+    c = rng.uniform(lo, hi, (count, 3))
+    h = rng.uniform(0.025, 0.2, (count, 3))
+    # 6 faces x 4 corners: (axis, sign) faces with corner offsets in the other two axes
+    vs, ns = [], []
+    for axis in range(3):
+        a1, a2 = (axis + 1) % 3, (axis + 2) % 3
+        for sign in (-1.0, 1.0):
+            nrm = np.zeros(3)
+            nrm[axis] = sign
+            for s1, s2 in ((-1, -1), (1, -1), (1, 1), (-1, 1)) if sign > 0 else ((-1, -1), (-1, 1), (1, 1), (1, -1)):
+                off = np.zeros((count, 3))
+                off[:, axis] = sign * h[:, axis]
+                off[:, a1] = s1 * h[:, a1]
+                off[:, a2] = s2 * h[:, a2]
+                vs.append(c + off)
+                ns.append(np.tile(nrm, (count, 1)))
+    v = np.stack(vs, 1).reshape(-1, 3)      # box-major: 24 vertices per box
+    n = np.stack(ns, 1).reshape(-1, 3)
+    quad = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    per_box = np.concatenate([quad + 4 * q for q in range(6)])             # 12 x 3
+    f = (per_box[None, :, :] + 24 * np.arange(count, dtype=np.uint32)[:, None, None]).reshape(-1, 3)
+    return v, n, f.astype(np.uint32)
+
+
+def config2_params(index, seed=2):
+    """Size of scene `index` of the batched workload: triangle count log-uniform in
+    [1e3, 2e6], square resolution log-uniform in 128..1024 (multiple of 16), spp
+    from {16, 32, 64, 128, 256}, 1-4 lights of emission U[10, 80]."""
+    rng = np.random.default_rng(seed * 100003 + index)
+    tris = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e6)))))
+    side = int(round(math.exp(rng.uniform(math.log(128), math.log(1024))) / 16.0)) * 16
+    spp = int(rng.choice([16, 32, 64, 128, 256]))
+    lights = int(rng.integers(1, 5))
+    return {"triangles": tris, "width": side, "height": side, "spp": spp, "lights": lights, "rng": rng}
+
+
+def config2(index, seed=2, max_triangles=None) -> SceneDesc:
+    """Scene `index` of the batched workload: a displaced icosphere of the largest
+    subdivision level below the drawn triangle count, topped up with random
+    boxes, inside the box with 1-4 ceiling lights; 8 materials (50 % Lambert,
+    50 % Beckmann).  `max_triangles` caps the count (small test batches)."""
+    p = config2_params(index, seed)
+    rng = p["rng"]
+    target = p["triangles"] if max_triangles is None else min(p["triangles"], max_triangles)
+    level = max(0, int(math.floor(math.log(max(target, 20) / 20.0, 4))))
+    sh = box_shaders(50.0)
+    del sh["light"]
+    names = []
+    for i in range(8):
+        nm, cfg = _random_material(rng, "b", i)
+        names.append(nm)
+        sh[nm] = cfg
+    v, n, f = displaced_icosphere(level, seed * 1000 + index, center=(S / 2, 1.7, 1.6), radius=1.2)
+    groups = box_groups(with_light=False)
+    patch = (np.arange(len(f)) // (4 ** level)) % len(names)
+    groups += split_groups(v, n, f, patch, names)
+    nbox = max(0, (target - len(f)) // 12)
+    bv, bn, bf = _boxes(rng, nbox, (0.3, -2.2, 0.05), (S - 0.3, S - 0.3, S - 1.0))
+    if nbox:
+        bmat = rng.integers(0, len(names), nbox)
+        fm = np.repeat(bmat, 12)
+        groups += split_groups(bv, bn, bf, fm, names)
+    for li in range(p["lights"]):
+        lx, ly = rng.uniform(0.8, S - 1.6), rng.uniform(-1.5, S - 1.6)
+        wx, wy = rng.uniform(0.4, 1.2), rng.uniform(0.4, 1.2)
+        z = S - 0.25
+        lq = quad((lx, ly, z), (lx, ly + wy, z), (lx + wx, ly + wy, z), (lx + wx, ly, z), (0, 0, -1))
+        groups.append(_finish(f"light{li}", *lq))
+        sh[f"light{li}"] = ["Emission", {"color": [1, 1, 1], "strength": float(rng.uniform(10, 80))}]
+    merged = {}
+    for g in groups:
+        if g.name in merged:
+            a = merged[g.name]
+            merged[g.name] = Group(g.name, np.concatenate([a.v, g.v]), np.concatenate([a.n, g.n]),
+                                   np.concatenate([a.f, g.f + len(a.v)]).astype(np.uint32))
+        else:
+            merged[g.name] = g
+    return SceneDesc(groups=list(merged.values()), shaders=sh, camera=box_camera(), width=p["width"],
+                     height=p["height"], spp=p["spp"], max_bounce=7, name=f"config2_{index}")
+
+
 def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
     """Occluded light: the box is split by a wall at y=2.6 with a 0.4x0.4 aperture;
     a single 0.3x0.3 light of strength 400 hangs on the far side; three displaced

@@ -206,6 +206,42 @@ int cr_render_device_noalloc(cr_scene *s, const cr_render_desc *desc, double *d_
  * Synchronises `stream`; allocates temporary device buffers. */
 int cr_autotune(cr_scene *s, const cr_render_desc *desc, void *stream, cr_tuning *out);
 
+/* ------------------------------------------------------ batched renders */
+/* No counterpart in the reference (its tracer renders one scene per call).
+ * A batch renders many committed scenes, each at its own resolution and spp,
+ * in shared waves: the paths of all jobs are concatenated, so one persistent
+ * traversal launch per bounce serves every scene and small images do not
+ * leave the GPU idle.  The first cr_batch_render captures the batch's whole
+ * kernel sequence into a CUDA graph on the batch's stream; later calls
+ * replay it.  Jobs render their whole image; estimator and max_bounce are
+ * shared; learned guiding is not used in batches. */
+typedef struct cr_batch cr_batch;
+typedef struct cr_batch_job {
+    cr_scene *scene;         /* committed scene (may appear in several jobs) */
+    uint32_t width, height;  /* image size */
+    uint32_t spp;            /* samples per pixel per render call */
+    uint64_t seed;           /* random seed of this job (plus the call's offset) */
+    double *d_sum;           /* device film: width x height x 3 doubles, accumulated */
+    double *d_sumsq;         /* width x height x 3 doubles */
+    uint32_t *d_count;       /* width x height finite-sample counts */
+} cr_batch_job;
+/* stream: the stream the batch captures and replays on; NULL: a stream of
+ * the batch's own.  The job table is copied; the films stay the caller's, and
+ * the scenes must stay alive and unchanged while the batch exists. */
+int cr_batch_create(const cr_batch_job *jobs, uint32_t n_jobs, uint32_t max_bounce, int32_t estimator,
+                    void *stream, cr_batch **out);
+/* Picks wave size, refill threshold and traversal grid for the batch by
+ * timing a reduced batch (every job at spp / 16, at least 1) under each
+ * candidate; the choice is kept (the next render captures a new graph).
+ * Synchronises; allocates temporary films. */
+int cr_batch_autotune(cr_batch *b, cr_tuning *out);
+/* One render of every job into its film, job seeds offset by seed_offset.
+ * With stats NULL the call only enqueues the graph (asynchronous); with
+ * stats it waits, checks the device error word and fills the totals and the
+ * device time of the replay. */
+int cr_batch_render(cr_batch *b, uint64_t seed_offset, cr_stats *stats);
+void cr_batch_destroy(cr_batch *b);
+
 /* ------------------------------------------------------ learned guiding */
 /* No counterpart in the reference.  A committed scene owns one path guide:
  * a 12-level hash-grid + SH encoding feeding a 4 x 64 MLP whose output is a

@@ -114,3 +114,9 @@ def test_png_writer(cr, tmp_path):
     raw = zlib.decompress(data[i + 4:i + 4 + n])
     row = np.frombuffer(raw[1:16], np.uint8).reshape(5, 3)
     assert list(row[:, 0]) == [0, 0, 127, 255, 255]
+
+
+def test_empty_batch_is_rejected(cr):
+    """cr_batch_create refuses an empty job table before touching the GPU."""
+    with pytest.raises(cr.CrError):
+        cr.Batch([])
