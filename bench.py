@@ -21,6 +21,9 @@ cpu_baseline / --impl reference
            the reference's own CPUMulticoreTracer::execute compiled from its
            sources (oracle/_ref/cr_ref), on this host's cores, on a bounded
            sample of the same workload (full resolution, fewer spp).
+batch      the batched workload (64 scenes of uneven size, resolution and spp)
+           as one batch replayed from a CUDA graph, against one call per
+           scene; rank 0 at N = 1 only.
 guiding    time to relMSE 1e-3, plain MIS vs learned guiding (tensor-core
            inference and online training included), on the occluded-light
            scene at 1024x1024 (see guided_vs_plain); rank 0 at N = 1 only.
@@ -266,6 +269,50 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     return out
 
 
+def batched_workload(cr, dev, n_scenes, seed=2):
+    """The batched workload: n_scenes seeded scenes (triangle counts
+    log-uniform in [1e3, 2e6], square images log-uniform 128..1024, spp from
+    {16..256}, 1-4 lights) rendered as one batch replayed from a CUDA graph,
+    against one render call per scene with the same work.  Device time (CUDA
+    events) of one replay, after an autotune and a warm-up replay."""
+    import torch
+    from cuda_raytracer_b200 import scenes
+    t0 = time.perf_counter()
+    descs = [scenes.config2(i, seed) for i in range(n_scenes)]
+    scs = [cr.Scene.from_desc(d) for d in descs]
+    t_build = time.perf_counter() - t0
+    films = []
+    for d in descs:
+        n = d.width * d.height
+        films.append((torch.zeros(n * 3, dtype=torch.float64, device=dev), torch.zeros(n * 3, dtype=torch.float64, device=dev),
+                      torch.zeros(n, dtype=torch.int32, device=dev)))
+    jobs = [(sc, d.width, d.height, d.spp, 1 + i, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr())
+            for i, (sc, d, f) in enumerate(zip(scs, descs, films))]
+    total = sum(d.width * d.height * d.spp for d in descs)
+    b = cr.Batch(jobs, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI)
+    tune = b.autotune().as_dict()
+    b.render(0, stats=True)  # capture + warm-up
+    st = b.render(1, stats=True)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for (sc, w, h, spp, sd, *_), f in zip(jobs, films):
+        dd = cr.render_desc(w, h, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=sd + 2)
+        sc.render_device(dd, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), stream=stream, stats=False)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms_single = e0.elapsed_time(e1)
+    out = {"workload": f"config2: {n_scenes} scenes, {sum(d.n_triangles for d in descs)} triangles, "
+                       f"{total} samples per replay, depth 8, reference estimator",
+           "msamples_per_s": round(total / st.ms_total / 1e3, 2), "ms_per_replay": round(st.ms_total, 2),
+           "per_scene_calls_msamples_per_s": round(total / ms_single / 1e3, 2),
+           "speedup_vs_per_scene_calls": round(ms_single / st.ms_total, 3),
+           "graph_nodes": st.launches, "waves": st.waves, "autotuned": tune,
+           "scene_build_s": round(t_build, 1)}
+    b.close()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -392,6 +439,9 @@ def run_ours(args):
         del s, q, c, flush
         torch.cuda.empty_cache()
         guiding = guided_vs_plain(cr, dev, args.guide_seconds, args.guide_ref_spp)
+    batch = None
+    if rank == 0 and world == 1 and args.batch_scenes > 0:
+        batch = batched_workload(cr, dev, args.batch_scenes)
 
     if rank == 0:
         line = {
@@ -420,6 +470,7 @@ def run_ours(args):
             "clocks": clk,
             "gpu_launches": totals["launches"],
             "guiding": guiding,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -441,6 +492,7 @@ def main():
     ap.add_argument("--guide-seconds", type=float, default=25.0,
                     help="device-time cap of each guided/plain time-to-relMSE run (0: skip them)")
     ap.add_argument("--guide-ref-spp", type=int, default=4096)
+    ap.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (0: skip it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
