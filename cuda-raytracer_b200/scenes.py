@@ -383,6 +383,63 @@ def config2(index, seed=2, max_triangles=None) -> SceneDesc:
                      height=p["height"], spp=p["spp"], max_bounce=7, name=f"config2_{index}")
 
 
+def _rotation(rng):
+    """Uniformly random rotation matrix (QR of a Gaussian matrix, sign-fixed)."""
+    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+    q = q * np.sign(np.diag(r))[None, :]
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    return q
+
+
+def config4(level=8, seed=4, instances=16, bases=4, width=3840, height=2160, spp=1024) -> SceneDesc:
+    """Large combined scene: `instances` copies of `bases` displaced icospheres
+    (20*4**level triangles each, 1.31M at level 8) under random rigid
+    transforms, flattened into one triangle set on a 4 x 4 grid over the box
+    floor; 6 ceiling lights of emission U[10, 80]; 16 materials (50 % Lambert,
+    50 % Beckmann roughness U[0.05, 0.8]); depth 12 (max_bounce 11)."""
+    rng = np.random.default_rng(seed)
+    sh = box_shaders(50.0)
+    del sh["light"]
+    names = []
+    for i in range(16):
+        nm, cfg = _random_material(rng, "c", i)
+        names.append(nm)
+        sh[nm] = cfg
+    base = [displaced_icosphere(level, seed * 100 + b, center=(0.0, 0.0, 0.0), radius=0.55) for b in range(bases)]
+    groups = box_groups(with_light=False)
+    xs = np.linspace(0.75, S - 0.75, 4)
+    ys = np.linspace(-1.6, S - 0.9, 4)
+    for k in range(instances):
+        v, n, f = base[k % bases]
+        R = _rotation(rng)
+        c = np.array([xs[k % 4], ys[(k // 4) % 4], rng.uniform(0.6, 1.6)])
+        vi = v @ R.T + c[None, :]
+        ni = n @ R.T
+        patch = (np.arange(len(f)) // (4 ** level) + k) % len(names)
+        groups += split_groups(vi, ni, f, patch, names)
+    for li in range(6):
+        lx, ly = rng.uniform(0.5, S - 1.5), rng.uniform(-2.0, S - 1.5)
+        wx, wy = rng.uniform(0.4, 1.0), rng.uniform(0.4, 1.0)
+        z = S - 0.25
+        lq = quad((lx, ly, z), (lx, ly + wy, z), (lx + wx, ly + wy, z), (lx + wx, ly, z), (0, 0, -1))
+        groups.append(_finish(f"light{li}", *lq))
+        sh[f"light{li}"] = ["Emission", {"color": [1, 1, 1], "strength": float(rng.uniform(10, 80))}]
+    merged = {}
+    for g in groups:
+        merged.setdefault(g.name, []).append(g)
+    out = []
+    for name, gs in merged.items():
+        if len(gs) == 1:
+            out.append(gs[0])
+            continue
+        offs = np.cumsum([0] + [len(g.v) for g in gs[:-1]])
+        out.append(Group(name, np.concatenate([g.v for g in gs]), np.concatenate([g.n for g in gs]),
+                         np.concatenate([g.f + o for g, o in zip(gs, offs)]).astype(np.uint32)))
+    return SceneDesc(groups=out, shaders=sh, camera=box_camera(), width=width, height=height, spp=spp,
+                     max_bounce=11, name=f"config4_l{level}")
+
+
 def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
     """Occluded light: the box is split by a wall at y=2.6 with a 0.4x0.4 aperture;
     a single 0.3x0.3 light of strength 400 hangs on the far side; three displaced
