@@ -4,15 +4,18 @@
 //  1. per-triangle boxes, centroid bounds            k_tri_boxes
 //  2. 63-bit Morton codes of the centroids           k_morton
 //  3. radix sort (CUB) of (code, triangle)
-//  4. binary radix tree (Karras, HPG 2012)           k_karras
+//  4. binary tree: locally-ordered clustering (PLOC, the default:
+//     k_ploc_*), or the radix tree of Karras (HPG 2012, k_karras) with
 //  5. bottom-up boxes and SAH leaf/split costs       k_bottom_up
-//     (leaves of up to 3 triangles where the SAH says a leaf is cheaper)
+//     (leaves of up to 3 triangles where the SAH says a leaf is cheaper;
+//     PLOC takes the same decision as it merges)
 //  6. top-down collapse into quantised 8-wide nodes  k_collapse (one level
 //     per launch): each wide node opens its binary subtree greedily by the
 //     largest child surface area until 8 children, assigns children to slots
 //     in ray-octant order, quantises child boxes to 8 bits per plane and
 //     writes its leaf triangles contiguously in traversal order.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -204,6 +207,120 @@ __global__ void k_bottom_up( int n, const uint32_t *order, const float4 *blo, co
 	}
 }
 
+// ----------------------------------------------------------------------------
+// Locally-ordered clustering (PLOC; Meister and Bittner, "Parallel Locally-
+// Ordered Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG
+// 2018), in our own code.  The clusters start as the Morton-sorted leaves; each
+// round every cluster finds the cluster within PLOC_R positions whose merged
+// box has the smallest surface area, mutual nearest neighbours merge into a new
+// internal node (kept at the lower position, bottom-up SAH leaf decision as in
+// k_bottom_up), and the survivors are compacted in order.
+constexpr int PLOC_R = 16;
+
+__global__ void k_ploc_leaves( int n, const uint32_t *order, const float4 *blo, const float4 *bhi, BNode *nodes,
+							   int *clusters )
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( k >= n ) return;
+	int id = ( n - 1 ) + k;
+	uint32_t prim = order[ k ];
+	float4 lo = blo[ prim ], hi = bhi[ prim ];
+	lo.w = COST_TRI * area( f3( lo ), f3( hi ) );
+	BNode &b = nodes[ id ];
+	b.lo = lo, b.hi = hi;
+	b.left = b.right = -1, b.parent = -1;
+	b.first = k, b.count = 1, b.leaf = 1;
+	clusters[ k ] = id;
+}
+
+__device__ __forceinline__ float merged_area( const BNode &a, const BNode &b )
+{
+	return area( f3( fminf( a.lo.x, b.lo.x ), fminf( a.lo.y, b.lo.y ), fminf( a.lo.z, b.lo.z ) ),
+				 f3( fmaxf( a.hi.x, b.hi.x ), fmaxf( a.hi.y, b.hi.y ), fmaxf( a.hi.z, b.hi.z ) ) );
+}
+
+// Nearest neighbour of every cluster within PLOC_R positions (ties: lower position).
+__global__ void k_ploc_nn( const int *clusters, int m, const BNode *nodes, int *nn )
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( i >= m ) return;
+	const BNode &a = nodes[ clusters[ i ] ];
+	float best = INFINITY;
+	int bj = -1;
+	int j0 = max( 0, i - PLOC_R ), j1 = min( m - 1, i + PLOC_R );
+	for ( int j = j0; j <= j1; ++j )
+	{
+		if ( j == i ) continue;
+		float d = merged_area( a, nodes[ clusters[ j ] ] );
+		if ( d < best ) best = d, bj = j;
+	}
+	nn[ i ] = bj;
+}
+
+// Mutual nearest neighbours merge; `keep` flags the surviving positions.
+__global__ void k_ploc_merge( int *clusters, const int *nn, int m, BNode *nodes, int *node_counter, int *keep )
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( i >= m ) return;
+	int j = nn[ i ];
+	bool mutual = j >= 0 && nn[ j ] == i;
+	if ( !mutual )
+	{
+		keep[ i ] = 1;
+		return;
+	}
+	if ( i > j )
+	{
+		keep[ i ] = 0;  // merged into position j
+		return;
+	}
+	int l = clusters[ i ], r = clusters[ j ];
+	int id = atomicAdd( node_counter, 1 );
+	const BNode &L = nodes[ l ];
+	const BNode &R = nodes[ r ];
+	float3 mlo = f3( fminf( L.lo.x, R.lo.x ), fminf( L.lo.y, R.lo.y ), fminf( L.lo.z, R.lo.z ) );
+	float3 mhi = f3( fmaxf( L.hi.x, R.hi.x ), fmaxf( L.hi.y, R.hi.y ), fmaxf( L.hi.z, R.hi.z ) );
+	float A = area( mlo, mhi );
+	int count = L.count + R.count;
+	float split = COST_NODE * A + L.lo.w + R.lo.w;
+	float leafc = COST_TRI * A * float( count );
+	bool as_leaf = count <= MAX_LEAF && leafc <= split;
+	BNode &nd = nodes[ id ];
+	nd.lo = make_float4( mlo.x, mlo.y, mlo.z, as_leaf ? leafc : split );
+	nd.hi = make_float4( mhi.x, mhi.y, mhi.z, 0.f );
+	nd.left = l, nd.right = r, nd.parent = -1;
+	nd.first = 0, nd.count = count, nd.leaf = as_leaf ? 1 : 0;
+	nodes[ l ].parent = id, nodes[ r ].parent = id;
+	clusters[ i ] = id;
+	keep[ i ] = 1;
+}
+
+__global__ void k_ploc_compact( const int *clusters, const int *keep, const int *pos, int m, int *out )
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( i < m && keep[ i ] ) out[ pos[ i ] ] = clusters[ i ];
+}
+
+// Depth-first leaf ranges, top-down over the internal nodes created in one
+// merge round (ids id0 .. id1-1; their parents were created later).
+__global__ void k_ploc_ranges( BNode *nodes, int id0, int id1 )
+{
+	int id = id0 + blockIdx.x * blockDim.x + threadIdx.x;
+	if ( id >= id1 ) return;
+	const BNode &nd = nodes[ id ];
+	nodes[ nd.left ].first = nd.first;
+	nodes[ nd.right ].first = nd.first + nodes[ nd.left ].count;
+}
+
+// Leaf k (Morton position) -> its depth-first position: the primitive order
+// the collapse writes triangles in.
+__global__ void k_ploc_order( int n, const BNode *nodes, const uint32_t *sorted, uint32_t *order )
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( k >= n ) return;
+	order[ nodes[ n - 1 + k ].first ] = sorted[ k ];
+}
+
 struct WorkItem
 {
 	int bnode;
@@ -371,7 +488,7 @@ void check( cudaError_t e, const char *what )
 
 }  // namespace
 
-void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st )
+void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st, bool ploc )
 {
 	out.n_nodes = 0;
 	out.n_tris = n;
@@ -414,12 +531,71 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	void *dtemp;
 	check( cudaMallocAsync( &dtemp, temp, st ), "bvh alloc" );
 	check( cub::DeviceRadixSort::SortPairs( dtemp, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
-	if ( n > 1 ) k_karras<<<( n - 1 + tb - 1 ) / tb, tb, 0, st>>>( keys2, int( n ), bn );
-	k_bottom_up<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, flags );
-	check( cudaGetLastError(), "bvh kernels" );
+	int root_id = 0;
+	const uint32_t *order = vals2;
+	if ( !ploc || n < 2 )
+	{
+		if ( n > 1 ) k_karras<<<( n - 1 + tb - 1 ) / tb, tb, 0, st>>>( keys2, int( n ), bn );
+		k_bottom_up<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, flags );
+		check( cudaGetLastError(), "bvh kernels" );
+	}
+	else
+	{
+		// clusters, neighbours, flags, positions and the depth-first order reuse
+		// the Morton buffers: keys (as two int arrays), keys2's second half, vals
+		int *cl = reinterpret_cast<int *>( keys ), *cl2 = cl + n;
+		int *nn = reinterpret_cast<int *>( keys2 ) + n, *keep = flags, *pos = reinterpret_cast<int *>( wa );
+		int *counter = reinterpret_cast<int *>( cnt ) + 6;
+		check( cudaMemsetAsync( counter, 0, sizeof( int ), st ), "bvh init" );
+		k_ploc_leaves<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, cl );
+		size_t scan_temp = 0;
+		check( cub::DeviceScan::ExclusiveSum( nullptr, scan_temp, keep, pos, int( n ), st ), "scan" );
+		void *stemp;
+		check( cudaMallocAsync( &stemp, scan_temp, st ), "bvh alloc" );
+		std::vector<int> round_base;  // first internal id of each merge round
+		int m = int( n ), created = 0;
+		while ( m > 1 )
+		{
+			int gm = ( m + tb - 1 ) / tb;
+			k_ploc_nn<<<gm, tb, 0, st>>>( cl, m, bn, nn );
+			k_ploc_merge<<<gm, tb, 0, st>>>( cl, nn, m, bn, counter, keep );
+			check( cub::DeviceScan::ExclusiveSum( stemp, scan_temp, keep, pos, m, st ), "scan" );
+			k_ploc_compact<<<gm, tb, 0, st>>>( cl, keep, pos, m, cl2 );
+			check( cudaGetLastError(), "bvh ploc" );
+			int last[ 2 ], made = 0;
+			check( cudaMemcpyAsync( last, pos + m - 1, sizeof( int ), cudaMemcpyDeviceToHost, st ), "bvh ploc" );
+			check( cudaMemcpyAsync( last + 1, keep + m - 1, sizeof( int ), cudaMemcpyDeviceToHost, st ), "bvh ploc" );
+			check( cudaMemcpyAsync( &made, counter, sizeof( int ), cudaMemcpyDeviceToHost, st ), "bvh ploc" );
+			check( cudaStreamSynchronize( st ), "bvh ploc" );
+			int m2 = last[ 0 ] + last[ 1 ];
+			if ( m2 >= m || made <= created ) throw std::runtime_error( "bvh: clustering made no progress" );
+			round_base.push_back( created );
+			created = made;
+			std::swap( cl, cl2 );
+			m = m2;
+		}
+		if ( created != int( n ) - 1 ) throw std::runtime_error( "bvh: clustering left unmerged clusters" );
+		check( cudaMemcpyAsync( &root_id, cl, sizeof( int ), cudaMemcpyDeviceToHost, st ), "bvh ploc" );
+		check( cudaStreamSynchronize( st ), "bvh ploc" );
+		// depth-first ranges: the root starts at 0; rounds top-down
+		int zero = 0;
+		check( cudaMemcpyAsync( &bn[ root_id ].first, &zero, sizeof( int ), cudaMemcpyHostToDevice, st ), "bvh ploc" );
+		round_base.push_back( created );
+		for ( int r = int( round_base.size() ) - 2; r >= 0; --r )
+		{
+			int id0 = round_base[ r ], id1 = round_base[ r + 1 ];
+			k_ploc_ranges<<<( id1 - id0 + tb - 1 ) / tb, tb, 0, st>>>( bn, id0, id1 );
+		}
+		// the depth-first primitive order replaces the Morton order (vals)
+		k_ploc_order<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), bn, vals2, vals );
+		check( cudaGetLastError(), "bvh ploc" );
+		check( cudaStreamSynchronize( st ), "bvh ploc" );
+		cudaFreeAsync( stemp, st );
+		order = vals;
+	}
 
-	// Root work item: binary root (internal 0, or the single leaf) -> wide node 0.
-	WorkItem root{ 0, 0 };
+	// Root work item: binary root -> wide node 0.
+	WorkItem root{ root_id, 0 };
 	uint32_t c0[ 5 ] = { 1, 0, 0, 1, 0 };
 	check( cudaMemcpyAsync( wa, &root, sizeof root, cudaMemcpyHostToDevice, st ), "bvh root" );
 	check( cudaMemcpyAsync( cnt, c0, sizeof c0, cudaMemcpyHostToDevice, st ), "bvh root" );
@@ -429,7 +605,7 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	while ( n_work )
 	{
 		check( cudaMemsetAsync( nnext, 0, sizeof( uint32_t ), st ), "bvh level" );
-		k_collapse<<<( n_work + 127 ) / 128, 128, 0, st>>>( cur, ncur, nxt, nnext, bn, int( n ) - 1, vals2, d_src,
+		k_collapse<<<( n_work + 127 ) / 128, 128, 0, st>>>( cur, ncur, nxt, nnext, bn, int( n ) - 1, order, d_src,
 															out.nodes, out.tris, cnt, depth + 1 );
 		check( cudaGetLastError(), "bvh collapse" );
 		check( cudaMemcpyAsync( &n_work, nnext, sizeof( uint32_t ), cudaMemcpyDeviceToHost, st ), "bvh level" );

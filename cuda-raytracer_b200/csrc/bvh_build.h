@@ -17,5 +17,7 @@ struct WideBvh
 // d_src: 3 float4 (v0, v1, v2) per triangle in global order, on the device.
 // Allocates out.nodes / out.tris with cudaMallocAsync on `st`; throws
 // std::runtime_error on failure.  Synchronises `st` once per tree level.
-void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st );
+// ploc: binary tree by locally-ordered clustering (higher quality); false:
+// the Karras radix tree over the Morton order (faster build)
+void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st, bool ploc = true );
 }  // namespace cr
