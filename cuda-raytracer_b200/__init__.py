@@ -79,6 +79,12 @@ class GuideConfig(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BuildConfig(C.Structure):
+    """cr_build_config: BVH build options."""
+    _fields_ = [("builder", C.c_int32), ("ploc_radius", C.c_uint32), ("max_leaf", C.c_uint32),
+                ("cost_node", C.c_float), ("cost_tri", C.c_float)]
+
+
 class BatchJob(C.Structure):
     """cr_batch_job: one scene's render inside a batch."""
     _fields_ = [("scene", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
@@ -104,7 +110,7 @@ def lib():
             "cr_scene_add_mesh": (I, [P, P, U32, P, P, U32, C.c_char_p]),
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
-            "cr_scene_commit": (I, [P, U64, P]),
+            "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
             "cr_scene_info": (I, [P, P, P, P, P]),
             "cr_scene_destroy": (None, [P]),
             "cr_light_table": (I, [P, U32, P, P]),
@@ -181,7 +187,7 @@ class Scene:
             return cls.from_json(fh.read(), os.path.dirname(os.path.abspath(path)))
 
     @classmethod
-    def from_desc(cls, desc, light_seed=DEFAULT_LIGHT_SEED):
+    def from_desc(cls, desc, light_seed=DEFAULT_LIGHT_SEED, build=None):
         """Build from a scenes.SceneDesc through the add_* calls: meshes in
         group order, then spheres (the order the reference's scene loader
         gives an import asset listed before sphere assets)."""
@@ -204,6 +210,11 @@ class Scene:
         tgt = np.asarray(cam["target"], np.float32)
         up = np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)
         _check(lib().cr_scene_set_camera(s.h, _p(pos), _p(tgt), _p(up), float(cam.get("fovx", 90.0))))
+        if build:
+            bc = BuildConfig(builder=build.get("builder", 0), ploc_radius=build.get("ploc_radius", 10),
+                             max_leaf=build.get("max_leaf", 3), cost_node=build.get("cost_node", 1.2),
+                             cost_tri=build.get("cost_tri", 1.0))
+            _check(lib().cr_scene_set_build(s.h, C.byref(bc)))
         _check(lib().cr_scene_commit(s.h, light_seed, None))
         return s
 

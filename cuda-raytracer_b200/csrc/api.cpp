@@ -159,6 +159,7 @@ struct cr_scene
 	// launch configuration (defaults, or the choice of cr_autotune)
 	uint32_t tune_wave = 1u << 22, tune_refill = 16;
 	int tune_blocks = 8;
+	BuildParams build;  // BVH build options (cr_scene_set_build)
 
 	~cr_scene() { release(); }
 	void release_device()
@@ -802,7 +803,7 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 		cuda_check( cudaMemcpyAsync( d_src, src.data(), sizeof( float4 ) * src.size(), cudaMemcpyHostToDevice, st ), "upload" );
 		try
 		{
-			build_wide_bvh( d_src, uint32_t( nt ), s->bvh, st );
+			build_wide_bvh( d_src, uint32_t( nt ), s->bvh, st, s->build );
 		}
 		catch ( const std::exception &e )
 		{
@@ -1454,6 +1455,22 @@ void batch_check_error( cr_batch *b )
 	if ( e ) fail( CR_ERR_DEVICE, "a batched render kernel reported error flags " + std::to_string( e ) );
 }
 }  // namespace
+
+int cr_scene_set_build( cr_scene *s, const cr_build_config *cfg )
+{
+	return guarded( [&] {
+		if ( !s || !cfg ) fail( CR_ERR_INVALID, "null argument" );
+		if ( s->committed ) fail( CR_ERR_STATE, "the BVH options must be set before cr_scene_commit" );
+		if ( cfg->builder != CR_BUILD_PLOC && cfg->builder != CR_BUILD_LBVH ) fail( CR_ERR_INVALID, "unknown builder" );
+		if ( cfg->max_leaf < 1 || cfg->max_leaf > 4 ) fail( CR_ERR_INVALID, "max_leaf must be in [1, 4]" );
+		if ( cfg->ploc_radius < 1 || cfg->ploc_radius > 256 ) fail( CR_ERR_INVALID, "ploc_radius must be in [1, 256]" );
+		if ( !( cfg->cost_node > 0.f ) || !( cfg->cost_tri > 0.f ) ) fail( CR_ERR_INVALID, "SAH costs must be positive" );
+		s->build.ploc = cfg->builder == CR_BUILD_PLOC;
+		s->build.radius = int( cfg->ploc_radius );
+		s->build.max_leaf = int( cfg->max_leaf );
+		s->build.cost_node = cfg->cost_node, s->build.cost_tri = cfg->cost_tri;
+	} );
+}
 
 int cr_batch_create( const cr_batch_job *jobs, uint32_t n_jobs, uint32_t max_bounce, int32_t estimator, void *stream,
 					 cr_batch **out )

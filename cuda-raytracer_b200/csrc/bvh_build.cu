@@ -31,9 +31,6 @@ namespace cr
 {
 namespace
 {
-constexpr int MAX_LEAF = 3;
-constexpr float COST_NODE = 1.2f;
-constexpr float COST_TRI = 1.0f;
 
 struct BNode
 {
@@ -166,7 +163,7 @@ __global__ void k_karras( const uint64_t *k, int n, BNode *nodes )
 }
 
 __global__ void k_bottom_up( int n, const uint32_t *order, const float4 *blo, const float4 *bhi, BNode *nodes,
-							 int *flags )
+							 int *flags, BuildParams bp )
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if ( k >= n ) return;
@@ -175,7 +172,7 @@ __global__ void k_bottom_up( int n, const uint32_t *order, const float4 *blo, co
 	uint32_t prim = order[ k ];
 	float4 lo = blo[ prim ], hi = bhi[ prim ];
 	float a = area( f3( lo ), f3( hi ) );
-	lo.w = COST_TRI * a;
+	lo.w = bp.cost_tri * a;
 	nodes[ id ].lo = lo;
 	nodes[ id ].hi = hi;
 	nodes[ id ].first = k;
@@ -197,9 +194,9 @@ __global__ void k_bottom_up( int n, const uint32_t *order, const float4 *blo, co
 		float3 mlo = f3( fminf( l0.x, r0.x ), fminf( l0.y, r0.y ), fminf( l0.z, r0.z ) );
 		float3 mhi = f3( fmaxf( l1.x, r1.x ), fmaxf( l1.y, r1.y ), fmaxf( l1.z, r1.z ) );
 		float A = area( mlo, mhi );
-		float split = COST_NODE * A + l0.w + r0.w;
-		float leafc = COST_TRI * A * float( nd.count );
-		bool as_leaf = nd.count <= MAX_LEAF && leafc <= split;
+		float split = bp.cost_node * A + l0.w + r0.w;
+		float leafc = bp.cost_tri * A * float( nd.count );
+		bool as_leaf = nd.count <= bp.max_leaf && leafc <= split;
 		nd.lo = make_float4( mlo.x, mlo.y, mlo.z, as_leaf ? leafc : split );
 		nd.hi = make_float4( mhi.x, mhi.y, mhi.z, 0.f );
 		nd.leaf = as_leaf ? 1 : 0;
@@ -211,21 +208,19 @@ __global__ void k_bottom_up( int n, const uint32_t *order, const float4 *blo, co
 // Locally-ordered clustering (PLOC; Meister and Bittner, "Parallel Locally-
 // Ordered Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG
 // 2018), in our own code.  The clusters start as the Morton-sorted leaves; each
-// round every cluster finds the cluster within PLOC_R positions whose merged
+// round every cluster finds the cluster within `radius` positions whose merged
 // box has the smallest surface area, mutual nearest neighbours merge into a new
 // internal node (kept at the lower position, bottom-up SAH leaf decision as in
 // k_bottom_up), and the survivors are compacted in order.
-constexpr int PLOC_R = 16;
-
 __global__ void k_ploc_leaves( int n, const uint32_t *order, const float4 *blo, const float4 *bhi, BNode *nodes,
-							   int *clusters )
+							   int *clusters, BuildParams bp )
 {
 	int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if ( k >= n ) return;
 	int id = ( n - 1 ) + k;
 	uint32_t prim = order[ k ];
 	float4 lo = blo[ prim ], hi = bhi[ prim ];
-	lo.w = COST_TRI * area( f3( lo ), f3( hi ) );
+	lo.w = bp.cost_tri * area( f3( lo ), f3( hi ) );
 	BNode &b = nodes[ id ];
 	b.lo = lo, b.hi = hi;
 	b.left = b.right = -1, b.parent = -1;
@@ -239,15 +234,15 @@ __device__ __forceinline__ float merged_area( const BNode &a, const BNode &b )
 				 f3( fmaxf( a.hi.x, b.hi.x ), fmaxf( a.hi.y, b.hi.y ), fmaxf( a.hi.z, b.hi.z ) ) );
 }
 
-// Nearest neighbour of every cluster within PLOC_R positions (ties: lower position).
-__global__ void k_ploc_nn( const int *clusters, int m, const BNode *nodes, int *nn )
+// Nearest neighbour of every cluster within `radius` positions (ties: lower position).
+__global__ void k_ploc_nn( const int *clusters, int m, const BNode *nodes, int *nn, int radius )
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if ( i >= m ) return;
 	const BNode &a = nodes[ clusters[ i ] ];
 	float best = INFINITY;
 	int bj = -1;
-	int j0 = max( 0, i - PLOC_R ), j1 = min( m - 1, i + PLOC_R );
+	int j0 = max( 0, i - radius ), j1 = min( m - 1, i + radius );
 	for ( int j = j0; j <= j1; ++j )
 	{
 		if ( j == i ) continue;
@@ -258,7 +253,8 @@ __global__ void k_ploc_nn( const int *clusters, int m, const BNode *nodes, int *
 }
 
 // Mutual nearest neighbours merge; `keep` flags the surviving positions.
-__global__ void k_ploc_merge( int *clusters, const int *nn, int m, BNode *nodes, int *node_counter, int *keep )
+__global__ void k_ploc_merge( int *clusters, const int *nn, int m, BNode *nodes, int *node_counter, int *keep,
+							  BuildParams bp )
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if ( i >= m ) return;
@@ -282,9 +278,9 @@ __global__ void k_ploc_merge( int *clusters, const int *nn, int m, BNode *nodes,
 	float3 mhi = f3( fmaxf( L.hi.x, R.hi.x ), fmaxf( L.hi.y, R.hi.y ), fmaxf( L.hi.z, R.hi.z ) );
 	float A = area( mlo, mhi );
 	int count = L.count + R.count;
-	float split = COST_NODE * A + L.lo.w + R.lo.w;
-	float leafc = COST_TRI * A * float( count );
-	bool as_leaf = count <= MAX_LEAF && leafc <= split;
+	float split = bp.cost_node * A + L.lo.w + R.lo.w;
+	float leafc = bp.cost_tri * A * float( count );
+	bool as_leaf = count <= bp.max_leaf && leafc <= split;
 	BNode &nd = nodes[ id ];
 	nd.lo = make_float4( mlo.x, mlo.y, mlo.z, as_leaf ? leafc : split );
 	nd.hi = make_float4( mhi.x, mhi.y, mhi.z, 0.f );
@@ -488,8 +484,11 @@ void check( cudaError_t e, const char *what )
 
 }  // namespace
 
-void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st, bool ploc )
+void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st, const BuildParams &bp )
 {
+	if ( bp.max_leaf < 1 || bp.max_leaf > 4 || bp.radius < 1 || bp.radius > 256 || !( bp.cost_node > 0.f ) ||
+		 !( bp.cost_tri > 0.f ) )
+		throw std::runtime_error( "bvh: build parameters out of range" );
 	out.n_nodes = 0;
 	out.n_tris = n;
 	out.depth = 0;
@@ -533,10 +532,10 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	check( cub::DeviceRadixSort::SortPairs( dtemp, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
 	int root_id = 0;
 	const uint32_t *order = vals2;
-	if ( !ploc || n < 2 )
+	if ( !bp.ploc || n < 2 )
 	{
 		if ( n > 1 ) k_karras<<<( n - 1 + tb - 1 ) / tb, tb, 0, st>>>( keys2, int( n ), bn );
-		k_bottom_up<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, flags );
+		k_bottom_up<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, flags, bp );
 		check( cudaGetLastError(), "bvh kernels" );
 	}
 	else
@@ -547,7 +546,7 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 		int *nn = reinterpret_cast<int *>( keys2 ) + n, *keep = flags, *pos = reinterpret_cast<int *>( wa );
 		int *counter = reinterpret_cast<int *>( cnt ) + 6;
 		check( cudaMemsetAsync( counter, 0, sizeof( int ), st ), "bvh init" );
-		k_ploc_leaves<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, cl );
+		k_ploc_leaves<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), vals2, blo, bhi, bn, cl, bp );
 		size_t scan_temp = 0;
 		check( cub::DeviceScan::ExclusiveSum( nullptr, scan_temp, keep, pos, int( n ), st ), "scan" );
 		void *stemp;
@@ -557,8 +556,8 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 		while ( m > 1 )
 		{
 			int gm = ( m + tb - 1 ) / tb;
-			k_ploc_nn<<<gm, tb, 0, st>>>( cl, m, bn, nn );
-			k_ploc_merge<<<gm, tb, 0, st>>>( cl, nn, m, bn, counter, keep );
+			k_ploc_nn<<<gm, tb, 0, st>>>( cl, m, bn, nn, bp.radius );
+			k_ploc_merge<<<gm, tb, 0, st>>>( cl, nn, m, bn, counter, keep, bp );
 			check( cub::DeviceScan::ExclusiveSum( stemp, scan_temp, keep, pos, m, st ), "scan" );
 			k_ploc_compact<<<gm, tb, 0, st>>>( cl, keep, pos, m, cl2 );
 			check( cudaGetLastError(), "bvh ploc" );

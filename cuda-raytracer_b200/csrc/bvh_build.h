@@ -17,7 +17,17 @@ struct WideBvh
 // d_src: 3 float4 (v0, v1, v2) per triangle in global order, on the device.
 // Allocates out.nodes / out.tris with cudaMallocAsync on `st`; throws
 // std::runtime_error on failure.  Synchronises `st` once per tree level.
-// ploc: binary tree by locally-ordered clustering (higher quality); false:
-// the Karras radix tree over the Morton order (faster build)
-void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st, bool ploc = true );
+// Build options.  ploc: binary tree by locally-ordered clustering (higher
+// quality) within `radius` positions of the Morton order; otherwise the
+// Karras radix tree (faster build).  max_leaf (1..4) triangles per leaf;
+// cost_node / cost_tri: SAH costs of a node visit and a triangle test.
+struct BuildParams
+{
+	bool ploc = true;
+	int radius = 10;
+	int max_leaf = 3;
+	float cost_node = 1.2f, cost_tri = 1.0f;
+};
+void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st,
+					 const BuildParams &bp = BuildParams() );
 }  // namespace cr

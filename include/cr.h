@@ -139,6 +139,25 @@ int cr_scene_set_camera(cr_scene *s, const float *position, const float *target,
  * (src/core/primitive/mesh.hpp:61-84). */
 int cr_scene_commit(cr_scene *s, uint64_t light_seed, void *stream);
 
+/* No counterpart in the reference.  BVH build options, set before
+ * cr_scene_commit (defaults in brackets):
+ *   builder      CR_BUILD_PLOC: locally-ordered clustering [default], or
+ *                CR_BUILD_LBVH: the Morton radix tree (faster build, more
+ *                nodes visited per ray)
+ *   ploc_radius  clustering search radius in Morton positions [10]
+ *   max_leaf     triangles per leaf, 1..4 [3]
+ *   cost_node, cost_tri  SAH costs of a node visit and a triangle test [1.2, 1] */
+#define CR_BUILD_PLOC 0
+#define CR_BUILD_LBVH 1
+typedef struct cr_build_config {
+    int32_t builder;
+    uint32_t ploc_radius;
+    uint32_t max_leaf;
+    float cost_node;
+    float cost_tri;
+} cr_build_config;
+int cr_scene_set_build(cr_scene *s, const cr_build_config *cfg);
+
 /* Counts after commit. */
 int cr_scene_info(const cr_scene *s, uint64_t *n_triangles, uint32_t *n_primitives, uint32_t *n_lights,
                   uint32_t *n_bvh_nodes);
