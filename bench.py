@@ -486,6 +486,10 @@ def run_ours(args):
     achieved = ext_launch_bytes / (ext_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = profiled_traffic()
+    # L2-resident read bandwidth and FP32 FMA rate of this GPU, measured now:
+    # the working set of this workload's traversal fits in L2
+    l2_gbs, fp32_tflops = cr.measure_peaks(stream.cuda_stream)
+    ext_flops = (cst.nodes * 96 + cst.tris * 40) / max(cst.extend_launches, 1)  # 8 slab tests x 12 + 40 per triangle
 
     # end to end through the public API from host arrays
     e2e = None
@@ -550,7 +554,15 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": round(ext_launch_bytes),
                          "launch_ms": round(ext_launch_ms, 4),
                          "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
-                         "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3)},
+                         "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3),
+                         "l2": {"achieved": round(achieved, 1), "peak": round(l2_gbs, 1), "unit": "GB/s",
+                                "frac": round(achieved / l2_gbs, 4),
+                                "peak_source": "measured in this run (cr_measure_peaks: 32 MB L2-resident reads)"},
+                         "fp32": {"achieved": round(ext_flops / (ext_launch_ms / 1e3) / 1e12, 3),
+                                  "peak": round(fp32_tflops, 2), "unit": "TFLOP/s",
+                                  "frac": round(ext_flops / (ext_launch_ms / 1e3) / 1e12 / fp32_tflops, 4),
+                                  "peak_source": "measured in this run (cr_measure_peaks: FMA chains)",
+                                  "flops_per_unit": "96 per wide node (8 slab tests) + 40 per triangle test"}},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,

@@ -111,6 +111,7 @@ def lib():
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
+            "cr_measure_peaks": (I, [P, P, P]),
             "cr_scene_info": (I, [P, P, P, P, P]),
             "cr_scene_destroy": (None, [P]),
             "cr_light_table": (I, [P, U32, P, P]),
@@ -339,6 +340,13 @@ class Guide:
         fn = lib().cr_guide_gradients_tc if tensor_cores else lib().cr_guide_gradients
         _check(fn(self.scene.h, _p(records), len(records), _p(gW), _p(gb), _p(ggrid)))
         return ggrid, gW, gb
+
+
+def measure_peaks(stream=0):
+    """cr_measure_peaks: (L2-resident read GB/s, FP32 FMA TFLOP/s) of this GPU."""
+    l2, fp = C.c_double(), C.c_double()
+    _check(lib().cr_measure_peaks(C.c_void_p(stream), C.byref(l2), C.byref(fp)))
+    return l2.value, fp.value
 
 
 class Batch:

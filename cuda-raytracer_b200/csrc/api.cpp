@@ -1456,6 +1456,17 @@ void batch_check_error( cr_batch *b )
 }
 }  // namespace
 
+extern "C" int cr_measure_peaks_impl( void *stream, double *l2_gbs, double *fp32_tflops, const char **err );
+
+int cr_measure_peaks( void *stream, double *l2_read_gbs, double *fp32_tflops )
+{
+	return guarded( [&] {
+		const char *err = nullptr;
+		if ( cr_measure_peaks_impl( stream, l2_read_gbs, fp32_tflops, &err ) != 0 )
+			fail( CR_ERR_CUDA, err ? err : "peak measurement failed" );
+	} );
+}
+
 int cr_scene_set_build( cr_scene *s, const cr_build_config *cfg )
 {
 	return guarded( [&] {

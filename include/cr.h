@@ -225,6 +225,13 @@ int cr_render_device_noalloc(cr_scene *s, const cr_render_desc *desc, double *d_
  * Synchronises `stream`; allocates temporary device buffers. */
 int cr_autotune(cr_scene *s, const cr_render_desc *desc, void *stream, cr_tuning *out);
 
+/* No counterpart in the reference.  Measures, on the current device, the
+ * L2-resident read bandwidth (a 32 MB buffer read 64 times with 16-byte
+ * loads) and the FP32 FMA throughput (8 independent chains per thread): the
+ * rooflines of traversal when the scene fits in L2 and of its box and
+ * triangle tests.  Synchronises `stream`; allocates 32 MB for the call. */
+int cr_measure_peaks(void *stream, double *l2_read_gbs, double *fp32_tflops);
+
 /* ------------------------------------------------------ batched renders */
 /* No counterpart in the reference (its tracer renders one scene per call).
  * A batch renders many committed scenes, each at its own resolution and spp,
