@@ -440,11 +440,12 @@ def config4(level=8, seed=4, instances=16, bases=4, width=3840, height=2160, spp
                      max_bounce=11, name=f"config4_l{level}")
 
 
-def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
+def config3(level=7, seed=3, width=1024, height=1024, spp=64, diffuse=False) -> SceneDesc:
     """Occluded light: the box is split by a wall at y=2.6 with a 0.4x0.4 aperture;
     a single 0.3x0.3 light of strength 400 hangs on the far side; three displaced
     icospheres (one at `level`, two at `level - 1`: ~492k triangles at level 7)
-    with Beckmann roughness U[0.05,0.5] are the receivers on the camera side."""
+    with Beckmann roughness U[0.05,0.5] are the receivers on the camera side
+    (`diffuse`: Lambert receivers of albedo 0.7 instead)."""
     rng = np.random.default_rng(seed)
     sh = box_shaders(400.0)
     names = []
@@ -454,6 +455,8 @@ def config3(level=7, seed=3, width=1024, height=1024, spp=64) -> SceneDesc:
             a = rng.uniform(0.05, 0.5)
             cfg = ["GlossyBSDF", {"distribution": ["Beckmann", {"roughness": float(a)}],
                                   "color": [0.8, 0.8, 0.8]}]
+        if diffuse:  # the same geometry with Lambert receivers (no glossy caustics)
+            cfg = ["Lambert", {"R": [0.7, 0.7, 0.7], "color": [1, 1, 1]}]
         names.append(nm)
         sh[nm] = cfg
     wall_y = 2.6
