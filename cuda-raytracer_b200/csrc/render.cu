@@ -392,8 +392,10 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	float3 wo = fr.local( -d );
 	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
 	Lobe lb[ G_LOBES ];
-	const float sel = cfg.guide_sample ? cfg.guide.select_prob : 0.f;
-	if ( cfg.guide_sample ) load_lobes( lobes, lb );
+	// the guide shapes continuations only: none follows the last vertex
+	const bool guided = cfg.guide_sample && bounce < cfg.max_bounce;
+	const float sel = guided ? cfg.guide.select_prob : 0.f;
+	if ( guided ) load_lobes( lobes, lb );
 	if ( sc.n_lights )
 	{
 		uint32_t nli = sc.n_lights;
@@ -414,10 +416,12 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 			float pb;
 			float3 f = mis_eval( sh, wo, wi, pb );
 			// one-sample MIS of guide and BSDF: the continuation density
-			if ( cfg.guide_sample ) pb = sel * mixture_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
+			if ( guided ) pb = sel * mixture_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
 			if ( !is_zero( f ) )
 			{
-				float w = pl * pl / ( pl * pl + pb * pb );
+				// the last vertex has no continuation that could reach the light:
+				// its light sample takes the whole weight
+				float w = bounce == cfg.max_bounce ? 1.f : pl * pl / ( pl * pl + pb * pb );
 				float3 c = beta * f * f3( lt.emission ) * ( wi.z * w / pl );
 				if ( finite3( c ) && !is_zero( c ) )
 				{
@@ -440,7 +444,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	float3 wi;
 	float pdf;
 	float3 wt, nd;
-	if ( cfg.guide_sample )
+	if ( guided )
 	{
 		// one-sample MIS: the guide with probability sel, else the BSDF; the
 		// weight uses the combined density of both strategies
@@ -1044,7 +1048,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				else
 					k_traverse<ExtendIO, false, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 			} );
-			if ( wc.guide_sample )
+			if ( wc.guide_sample && b < cfg.max_bounce )
 				timed( 4, [&] {
 					k_guide_infer<<<sms * 2, tc::THREADS, tc::SMEM_BYTES, st>>>( sc, wc, wb, b, guide->Wp );
 				} );

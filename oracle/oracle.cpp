@@ -720,7 +720,11 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng, 
 				if ( ( f.x > 0 || f.y > 0 || f.z > 0 ) && dot( wiw, ng ) > 0 &&
 					 !occluded_ray( s, p, wiw, 1e-7 * s->scale, dist * ( 1 - 1e-4 ) ) )
 				{
-					double w = variant == 3 ? 1.0 : pl * pl / ( pl * pl + pb * pb );
+					// The last vertex has no continuation that could reach the light,
+					// so its light sample takes the whole weight: the estimate is then
+					// the light of all paths of at most max_bounce + 1 segments, for
+					// whatever continuation density the other vertices use.
+					double w = variant == 3 || bounce == max_bounce ? 1.0 : pl * pl / ( pl * pl + pb * pb );
 					L = L + beta * f * s->shaders[ s->prims[ lt.prim ].shader ].emission * ( wi.z * w / pl );
 				}
 			}
