@@ -501,7 +501,7 @@ __global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_forward_batch_tc( Gu
 		float4 *dst = reinterpret_cast<float4 *>( out + G_OUT * size_t( i ) );
 		for ( int j = 0; j < G_OUT / 4; ++j ) dst[ j ] = make_float4( o[ 4 * j ], o[ 4 * j + 1 ], o[ 4 * j + 2 ], o[ 4 * j + 3 ] );
 	};
-	tc::mlp_forward_tc( g, Wp, n, src, sink, err );
+	tc::mlp_forward_tc<G_OUT>( g, Wp, n, src, sink, err );
 }
 
 __global__ void k_records_from_host( GuideRecords rec, const float *src, uint32_t n )

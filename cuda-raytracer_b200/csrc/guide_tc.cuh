@@ -155,12 +155,51 @@ __device__ __forceinline__ void store_row( uint8_t *tile, uint32_t r, const floa
 	}
 }
 
+// Row r's network input for (x, wo, n), as guide_encode lays it out, written
+// straight into a canonical K-major tile as BF16, 8 values at a time.
+__device__ __forceinline__ void encode_store_row( const GuideDev &g, float3 x, float3 wo, float3 n, uint8_t *tile,
+												  uint32_t r )
+{
+	const float3 u = ( x - g.bmin ) * g.binv;
+	uint32_t w[ 4 ];
+#pragma unroll
+	for ( int l = 0; l < G_LEVELS; ++l )
+	{
+		GridCorners c;
+		grid_corners( l, u, c );
+		float f0 = 0.f, f1 = 0.f;
+		const float *tab = g.grid + size_t( l ) * G_T * G_FEAT;
+#pragma unroll
+		for ( int k = 0; k < 8; ++k )
+		{
+			float2 v = *reinterpret_cast<const float2 *>( tab + 2 * c.idx[ k ] );
+			f0 += c.w[ k ] * v.x;
+			f1 += c.w[ k ] * v.y;
+		}
+		w[ l & 3 ] = pack_bf16x2( f0, f1 );
+		if ( ( l & 3 ) == 3 )
+			*reinterpret_cast<uint4 *>( tile + canon( r, 8 * ( l >> 2 ) ) ) = make_uint4( w[ 0 ], w[ 1 ], w[ 2 ], w[ 3 ] );
+	}
+	float sh[ G_SH ];
+	sh16( wo.x, wo.y, wo.z, sh );
+#pragma unroll
+	for ( int j = 0; j < 2; ++j )
+		*reinterpret_cast<uint4 *>( tile + canon( r, G_ENC + 8 * j ) ) =
+			make_uint4( pack_bf16x2( sh[ 8 * j ], sh[ 8 * j + 1 ] ), pack_bf16x2( sh[ 8 * j + 2 ], sh[ 8 * j + 3 ] ),
+						pack_bf16x2( sh[ 8 * j + 4 ], sh[ 8 * j + 5 ] ), pack_bf16x2( sh[ 8 * j + 6 ], sh[ 8 * j + 7 ] ) );
+	*reinterpret_cast<uint4 *>( tile + canon( r, G_ENC + G_SH ) ) =
+		make_uint4( pack_bf16x2( n.x, n.y ), pack_bf16x2( n.z, 0.f ), 0u, 0u );
+	*reinterpret_cast<uint4 *>( tile + canon( r, 48 ) ) = make_uint4( 0u, 0u, 0u, 0u );
+	*reinterpret_cast<uint4 *>( tile + canon( r, 56 ) ) = make_uint4( 0u, 0u, 0u, 0u );
+}
+
 // Runs the network over rows 0..n-1.  src(i, x, wo, nrm) -> bool fetches row
 // i's inputs (false: the row is skipped); sink(i, out) receives the 64 FP32
-// outputs of a fetched row.  Wp: the BF16 weights in the shared-memory image
+// outputs of a fetched row (the first OUT_COLS of them: 48 covers the 40 the
+// lobes use, 64 gives all).  Wp: the BF16 weights in the shared-memory image
 // (G_LAYERS x W_BYTES, canonical layout, 16-byte aligned).  Called by every
 // thread of a THREADS-wide CTA with SMEM_BYTES of dynamic shared memory.
-template <class Src, class Sink>
+template <int OUT_COLS, class Src, class Sink>
 __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t *__restrict__ Wp, uint32_t n,
 												Src &&src, Sink &&sink, uint32_t *err )
 {
@@ -207,12 +246,11 @@ __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t
 		const uint32_t i = base + tid;
 		float3 x = f3( 0.f, 0.f, 0.f ), wo = f3( 0.f, 0.f, 1.f ), nrm = f3( 0.f, 0.f, 1.f );
 		const bool valid = i < n && src( i, x, wo, nrm );
-		float v[ G_IN ];
 		if ( valid )
-			guide_encode( g, x, wo, nrm, v );
+			encode_store_row( g, x, wo, nrm, my_tile, row );
 		else
-			for ( int k = 0; k < G_IN; ++k ) v[ k ] = 0.f;
-		store_row( my_tile, row, v );
+#pragma unroll
+			for ( int j = 0; j < 8; ++j ) *reinterpret_cast<uint4 *>( my_tile + canon( row, 8 * j ) ) = make_uint4( 0u, 0u, 0u, 0u );
 		for ( int l = 0; l < G_LAYERS; ++l )
 		{
 			// make this thread's A row visible to the tensor core, then one
@@ -237,22 +275,34 @@ __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t
 				break;
 			}
 			tc_after_sync();
-			float acc[ 64 ];
-#pragma unroll
-			for ( int c = 0; c < 4; ++c ) tmem_ld16( my_tmem + 16u * c, acc + 16 * c );
-			tmem_wait_ld();
 			const float *bl = bias + l * G_HID;
 			if ( l < G_LAYERS - 1 )
 			{
+				// 16 columns at a time: bias, ReLU, BF16, back into this row
 #pragma unroll
-				for ( int k = 0; k < G_HID; ++k ) acc[ k ] = fmaxf( acc[ k ] + bl[ k ], 0.f );
-				store_row( my_tile, row, acc );
+				for ( int c = 0; c < 4; ++c )
+				{
+					float a[ 16 ];
+					tmem_ld16( my_tmem + 16u * c, a );
+					tmem_wait_ld();
+					uint32_t q[ 8 ];
+#pragma unroll
+					for ( int k = 0; k < 8; ++k )
+						q[ k ] = pack_bf16x2( fmaxf( a[ 2 * k ] + bl[ 16 * c + 2 * k ], 0.f ),
+											  fmaxf( a[ 2 * k + 1 ] + bl[ 16 * c + 2 * k + 1 ], 0.f ) );
+					*reinterpret_cast<uint4 *>( my_tile + canon( row, 16 * c ) ) = make_uint4( q[ 0 ], q[ 1 ], q[ 2 ], q[ 3 ] );
+					*reinterpret_cast<uint4 *>( my_tile + canon( row, 16 * c + 8 ) ) = make_uint4( q[ 4 ], q[ 5 ], q[ 6 ], q[ 7 ] );
+				}
 			}
 			else
 			{
+				float out[ OUT_COLS ];
 #pragma unroll
-				for ( int k = 0; k < G_OUT; ++k ) acc[ k ] += bl[ k ];
-				if ( valid ) sink( i, acc );
+				for ( int c = 0; c < OUT_COLS / 16; ++c ) tmem_ld16( my_tmem + 16u * c, out + 16 * c );
+				tmem_wait_ld();
+#pragma unroll
+				for ( int k = 0; k < OUT_COLS; ++k ) out[ k ] += bl[ k ];
+				if ( valid ) sink( i, out );
 			}
 			// the next MMA overwrites the accumulators: finish this thread's reads first
 			tc_before_sync();

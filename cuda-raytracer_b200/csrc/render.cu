@@ -15,6 +15,7 @@
 //   k_accumulate per-pixel FP64 sums of the finite samples (cpuMulticore.cu:58-64)
 //
 // Queue lengths live in device memory, so a wave needs no host round trip.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -342,25 +343,61 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 
 // One vertex of the MIS estimator (power heuristic over BSDF sampling and
 // area-light NEE; see cr_device.cuh for the BSDFs).
-__device__ __forceinline__ void load_lobes( const float *src, Lobe *lb )
+// Lobes of one path: 40 FP16 values (mean xyz, kappa, weight per lobe) in 5 x 16
+// bytes.  Decoding renormalises the means and the weights, so that sampling
+// and density evaluation see one exactly normalised mixture.
+__device__ __forceinline__ void store_lobes( uint4 *dst, const Lobe *lb )
 {
-	const float4 *p = reinterpret_cast<const float4 *>( src );
 	float v[ 5 * G_LOBES ];
 #pragma unroll
-	for ( int i = 0; i < 5 * G_LOBES / 4; ++i )
+	for ( int k = 0; k < G_LOBES; ++k )
+		v[ 5 * k ] = lb[ k ].mu.x, v[ 5 * k + 1 ] = lb[ k ].mu.y, v[ 5 * k + 2 ] = lb[ k ].mu.z,
+				v[ 5 * k + 3 ] = lb[ k ].kappa, v[ 5 * k + 4 ] = lb[ k ].weight;
+	uint32_t h[ 5 * G_LOBES / 2 ];
+#pragma unroll
+	for ( int i = 0; i < 5 * G_LOBES / 2; ++i )
 	{
-		float4 q = p[ i ];
-		v[ 4 * i ] = q.x, v[ 4 * i + 1 ] = q.y, v[ 4 * i + 2 ] = q.z, v[ 4 * i + 3 ] = q.w;
+		__half2 p = __floats2half2_rn( v[ 2 * i ], v[ 2 * i + 1 ] );
+		h[ i ] = *reinterpret_cast<uint32_t *>( &p );
 	}
 #pragma unroll
+	for ( int j = 0; j < 5; ++j ) dst[ j ] = make_uint4( h[ 4 * j ], h[ 4 * j + 1 ], h[ 4 * j + 2 ], h[ 4 * j + 3 ] );
+}
+
+__device__ __forceinline__ void load_lobes( const uint4 *src, Lobe *lb )
+{
+	float v[ 5 * G_LOBES ];
+#pragma unroll
+	for ( int j = 0; j < 5; ++j )
+	{
+		uint4 q = src[ j ];
+		uint32_t w[ 4 ] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+		for ( int t = 0; t < 4; ++t )
+		{
+			float2 f = __half22float2( *reinterpret_cast<const __half2 *>( &w[ t ] ) );
+			v[ 8 * j + 2 * t ] = f.x, v[ 8 * j + 2 * t + 1 ] = f.y;
+		}
+	}
+	float wsum = 0.f;
+#pragma unroll
 	for ( int k = 0; k < G_LOBES; ++k )
-		lb[ k ].mu = f3( v[ 5 * k ], v[ 5 * k + 1 ], v[ 5 * k + 2 ] ), lb[ k ].kappa = v[ 5 * k + 3 ],
-		lb[ k ].weight = v[ 5 * k + 4 ];
+	{
+		float3 m = f3( v[ 5 * k ], v[ 5 * k + 1 ], v[ 5 * k + 2 ] );
+		float l2 = dot( m, m );
+		lb[ k ].mu = l2 > 1e-20f ? m * rsqrtf( l2 ) : f3( 0.f, 0.f, 1.f );
+		lb[ k ].kappa = fminf( fmaxf( v[ 5 * k + 3 ], G_KAPPA_MIN ), G_KAPPA_MAX );
+		lb[ k ].weight = fmaxf( v[ 5 * k + 4 ], 0.f );
+		wsum += lb[ k ].weight;
+	}
+	const float inv = wsum > 0.f ? 1.f / wsum : 0.f;
+#pragma unroll
+	for ( int k = 0; k < G_LOBES; ++k ) lb[ k ].weight = wsum > 0.f ? lb[ k ].weight * inv : 1.f / G_LOBES;
 }
 
 __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
 										   uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
-										   float4 &L4, PathOut &out, const float *lobes, uint32_t rec_i )
+										   float4 &L4, PathOut &out, const uint4 *lobes, uint32_t rec_i )
 {
 	float3 o = f3( ro ), d = f3( rd );
 	Surface s = surface_at( sc, o, d, h, true );
@@ -605,7 +642,7 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 					uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
 					if ( cfg.estimator == EST_MIS )
 						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
-								   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 * G_LOBES : nullptr,
+								   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 : nullptr,
 								   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
 					else
 						shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
@@ -655,16 +692,9 @@ __global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_infer( DevScene sc, 
 	auto sink = [&]( uint32_t i, const float *out ) {
 		Lobe lb[ G_LOBES ];
 		lobes_from_output( out, lb );
-		// 40 floats per path: 16-byte aligned for every path (160-byte stride)
-		float4 *dst = reinterpret_cast<float4 *>( wb.lobes + size_t( q[ i ] ) * 5 * G_LOBES );
-		float v[ 5 * G_LOBES ];
-		for ( int k = 0; k < G_LOBES; ++k )
-			v[ 5 * k ] = lb[ k ].mu.x, v[ 5 * k + 1 ] = lb[ k ].mu.y, v[ 5 * k + 2 ] = lb[ k ].mu.z,
-					v[ 5 * k + 3 ] = lb[ k ].kappa, v[ 5 * k + 4 ] = lb[ k ].weight;
-		for ( int j = 0; j < 5 * G_LOBES / 4; ++j )
-			dst[ j ] = make_float4( v[ 4 * j ], v[ 4 * j + 1 ], v[ 4 * j + 2 ], v[ 4 * j + 3 ] );
+		store_lobes( wb.lobes + size_t( q[ i ] ) * 5, lb );
 	};
-	tc::mlp_forward_tc( cfg.guide, Wp, n, src, sink, wb.err );
+	tc::mlp_forward_tc<48>( cfg.guide, Wp, n, src, sink, wb.err );
 }
 
 __global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, double *sum, double *sumsq,
@@ -841,7 +871,7 @@ void free_wave( WaveBuffers &wb, cudaStream_t st )
 void alloc_lobes( WaveBuffers &wb, cudaStream_t st )
 {
 	if ( wb.lobes ) return;
-	alloc( wb.lobes, size_t( wb.capacity ) * 5 * G_LOBES, st );
+	alloc( wb.lobes, size_t( wb.capacity ) * 5, st );
 }
 
 void alloc_batch_state( WaveBuffers &wb, cudaStream_t st )
