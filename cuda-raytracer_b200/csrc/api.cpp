@@ -1695,12 +1695,14 @@ int cr_guide_configure( cr_scene *s, const cr_guide_config *in, cr_guide_config 
 			g.lr = in->lr, g.select_prob = in->select_prob, g.train_paths = in->train_paths;
 			g.steps_per_wave = in->steps_per_wave, g.warmup_steps = in->warmup_steps;
 			g.product_target = in->product_target != 0;
+			g.max_steps = in->max_steps;
 		}
 		if ( out )
 		{
 			out->lr = g.lr, out->select_prob = g.select_prob, out->train_paths = g.train_paths;
 			out->steps_per_wave = g.steps_per_wave, out->warmup_steps = g.warmup_steps;
 			out->product_target = g.product_target ? 1u : 0u;
+			out->max_steps = g.max_steps;
 		}
 	} );
 }
@@ -1727,6 +1729,7 @@ int cr_guide_params( cr_scene *s, float *grid, float *W, float *b, int set )
 		io( grid, s->guide.grid, GuideState::grid_size() );
 		io( W, s->guide.W, GuideState::w_size() );
 		io( b, s->guide.b, GuideState::b_size() );
+		if ( set ) s->guide.packed_step = ~0u;  // the tensor-core weight image is stale
 	} );
 }
 

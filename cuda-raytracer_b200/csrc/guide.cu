@@ -576,6 +576,7 @@ void GuideState::init( float3 lo, float3 hi, uint64_t seed )
 	for ( float *p : { b, b_m, b_v, gb } ) check( cudaMemset( p, 0, b_size() * 4 ), "guide init" );
 	step = 0;
 	waves = 0;
+	packed_step = ~0u;
 	ready = true;
 }
 

@@ -1040,26 +1040,32 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		// per-wave copy: which paths are recorded, and whether the guide is sampled
 		RenderConfig wc = cfg;
 		uint32_t steps = 0, batch = 0;
-		if ( cfg.guiding )
+		// record and train only while the training budget lasts; sample the guide after warm-up
+		const bool training = cfg.guiding && ( guide->max_steps == 0 || guide->step < guide->max_steps );
+		if ( cfg.guiding && !training ) wc.guiding = false;
+		if ( cfg.guiding && guide->step >= guide->warmup_steps )
+		{
+			wc.guide_sample = true;
+			static bool smem_attr0 = false;
+			if ( !smem_attr0 )
+			{
+				check( cudaFuncSetAttribute( k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int( tc::SMEM_BYTES ) ),
+					   "guide inference smem" );
+				smem_attr0 = true;
+			}
+			if ( guide->packed_step != guide->step )  // BF16 copy of the weights this wave samples with
+			{
+				guide->pack_weights( st );
+				guide->packed_step = guide->step;
+			}
+		}
+		if ( training )
 		{
 			batch = std::min( guide->train_paths, wa.n );
 			wc.rec_paths = uint32_t( std::min<uint64_t>( uint64_t( batch ) * guide->steps_per_wave, wa.n ) );
 			steps = ( wc.rec_paths + batch - 1 ) / batch;
 			wc.rec_stride = wa.n / wc.rec_paths;
 			wc.rec_offset = uint32_t( ( guide->waves++ * 2654435761ull ) % wc.rec_stride );
-			wc.guide_sample = guide->step >= guide->warmup_steps;
-			if ( wc.guide_sample )
-			{
-				static bool smem_attr = false;
-				if ( !smem_attr )
-				{
-					check( cudaFuncSetAttribute( k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-												 int( tc::SMEM_BYTES ) ),
-						   "guide inference smem" );
-					smem_attr = true;
-				}
-				guide->pack_weights( st );  // BF16 copy of the weights this wave samples with
-			}
 			check( cudaMemsetAsync( cfg.rec.x, 0, sizeof( float4 ) * size_t( wc.rec_paths ) * ( cfg.max_bounce + 1 ), st ),
 				   "memset" );
 		}

@@ -290,7 +290,9 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   warmup_steps    steps taken before the guide is first sampled [8]; until
  *                   then a guided render samples the BSDF only and trains
  *   product_target  1: fit the integrand Li f cos at each vertex; 0: fit the
- *                   incident (indirect) radiance Li alone [1] */
+ *                   incident (indirect) radiance Li alone [1]
+ *   max_steps       training budget: after this many Adam steps renders sample
+ *                   the guide without recording or training (0: no budget) [0] */
 typedef struct cr_guide_config {
     float lr;
     float select_prob;
@@ -298,6 +300,7 @@ typedef struct cr_guide_config {
     uint32_t steps_per_wave;
     uint32_t warmup_steps;
     uint32_t product_target;
+    uint32_t max_steps;
 } cr_guide_config;
 /* Apply `in` (when not NULL) and report the schedule in `out` (when not NULL). */
 int cr_guide_configure(cr_scene *s, const cr_guide_config *in, cr_guide_config *out);
