@@ -65,6 +65,27 @@ def load_pkg():
     return mod
 
 
+def replica_seed(rank, k):
+    """Seed of timed step k on `rank`: every replica renders independent samples."""
+    return 7 + 1000 * rank + k
+
+
+def job_throughput(ms_local, samples_local, device, world):
+    """Whole-job Msamples/s of the replicas: all ranks' samples over the slowest
+    rank's device time (ms); returns (value, ms_max, samples_all)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms_local, float(samples_local)], dtype=torch.float64, device=device)
+    if world > 1:
+        mx = t[:1].clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t[1:].clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        t = torch.cat([mx, sm])
+    ms_max, samples_all = float(t[0].item()), float(t[1].item())
+    return samples_all / (ms_max / 1e3) / 1e6, ms_max, int(samples_all)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -456,7 +477,7 @@ def run_ours(args):
     for k in range(args.steps):
         flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
         ev[k][0].record(stream)
-        st = step(7 + 1000 * rank + k)
+        st = step(replica_seed(rank, k))
         ev[k][1].record(stream)
         totals["extend"] += st.ms_extend
         totals["shadow"] += st.ms_shadow
@@ -472,12 +493,7 @@ def run_ours(args):
         dist.barrier()
     clk = clocks.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    samples_all = totals["samples"] * world
-    value = samples_all / (ms_max / 1e3) / 1e6
+    value, ms_max, samples_all = job_throughput(ms, totals["samples"], dev, world)
 
     # roofline of the closest-hit kernel
     ext_bytes = cst.nodes * NODE_BYTES + cst.tris * TRI_BYTES + cst.rays_extend * RAY_BYTES
