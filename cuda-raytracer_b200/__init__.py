@@ -83,7 +83,8 @@ class GuideConfig(C.Structure):
 class BuildConfig(C.Structure):
     """cr_build_config: BVH build options."""
     _fields_ = [("builder", C.c_int32), ("ploc_radius", C.c_uint32), ("max_leaf", C.c_uint32),
-                ("cost_node", C.c_float), ("cost_tri", C.c_float)]
+                ("cost_node", C.c_float), ("cost_tri", C.c_float), ("collapse", C.c_int32),
+                ("wide_cost_node", C.c_float), ("wide_cost_tri", C.c_float)]
 
 
 class BatchJob(C.Structure):
@@ -215,7 +216,9 @@ class Scene:
         if build:
             bc = BuildConfig(builder=build.get("builder", 0), ploc_radius=build.get("ploc_radius", 10),
                              max_leaf=build.get("max_leaf", 3), cost_node=build.get("cost_node", 1.2),
-                             cost_tri=build.get("cost_tri", 1.0))
+                             cost_tri=build.get("cost_tri", 1.0), collapse=build.get("collapse", 0),
+                             wide_cost_node=build.get("wide_cost_node", 1.0),
+                             wide_cost_tri=build.get("wide_cost_tri", 0.3))
             _check(lib().cr_scene_set_build(s.h, C.byref(bc)))
         _check(lib().cr_scene_commit(s.h, light_seed, None))
         return s

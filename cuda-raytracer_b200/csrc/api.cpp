@@ -1475,11 +1475,16 @@ int cr_scene_set_build( cr_scene *s, const cr_build_config *cfg )
 		if ( cfg->builder != CR_BUILD_PLOC && cfg->builder != CR_BUILD_LBVH ) fail( CR_ERR_INVALID, "unknown builder" );
 		if ( cfg->max_leaf < 1 || cfg->max_leaf > 4 ) fail( CR_ERR_INVALID, "max_leaf must be in [1, 4]" );
 		if ( cfg->ploc_radius < 1 || cfg->ploc_radius > 256 ) fail( CR_ERR_INVALID, "ploc_radius must be in [1, 256]" );
-		if ( !( cfg->cost_node > 0.f ) || !( cfg->cost_tri > 0.f ) ) fail( CR_ERR_INVALID, "SAH costs must be positive" );
+		if ( !( cfg->cost_node > 0.f ) || !( cfg->cost_tri > 0.f ) || !( cfg->wide_cost_node > 0.f ) ||
+			 !( cfg->wide_cost_tri > 0.f ) )
+			fail( CR_ERR_INVALID, "SAH costs must be positive" );
+		if ( cfg->collapse != CR_COLLAPSE_SAH && cfg->collapse != CR_COLLAPSE_GREEDY ) fail( CR_ERR_INVALID, "unknown collapse" );
 		s->build.ploc = cfg->builder == CR_BUILD_PLOC;
 		s->build.radius = int( cfg->ploc_radius );
 		s->build.max_leaf = int( cfg->max_leaf );
 		s->build.cost_node = cfg->cost_node, s->build.cost_tri = cfg->cost_tri;
+		s->build.dp_collapse = cfg->collapse == CR_COLLAPSE_SAH;
+		s->build.dp_cost_node = cfg->wide_cost_node, s->build.dp_cost_tri = cfg->wide_cost_tri;
 	} );
 }
 

@@ -317,6 +317,102 @@ __global__ void k_ploc_order( int n, const BNode *nodes, const uint32_t *sorted,
 	order[ nodes[ n - 1 + k ].first ] = sorted[ k ];
 }
 
+// ----------------------------------------------------------------------------
+// Collapse planning by dynamic programming over the binary tree (after Ylitie,
+// Karras and Laine, "Efficient Incoherent Ray Traversal on GPUs Through
+// Compressed Wide BVHs", HPG 2017, section 4.1), in our own code.  For every
+// binary node m and slot budget i = 1..8, C(m, i) is the least SAH cost of
+// representing m's subtree by at most i wide-node children:
+//   C(m, 1)  = min(leaf: A(m) count c_tri  if count <= max_leaf,
+//                  wide node: A(m) c_node + D(m, 8))
+//   C(m, i)  = min(C(m, i-1), D(m, i))                          (i >= 2)
+//   D(m, i)  = min over k of C(left, k) + C(right, i - k)
+// One decision byte per (m, i): bit 7 = "C(m, i) is C(m, i-1)", low bits = the
+// best k of D(m, i); byte 0 = "m is a leaf" for i = 1.  Byte 0 of a node that
+// becomes a wide node also keeps, in bits 1-3, the best k of D(m, 8) - 1.
+constexpr float DP_INF = 3.0e38f;
+
+__global__ void k_dp_leaves( int n, const BNode *nodes, float *cost, uint8_t *dec, BuildParams bp )
+{
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if ( k >= n ) return;
+	int id = ( n - 1 ) + k;
+	const BNode &b = nodes[ id ];
+	float c = bp.dp_cost_tri * area( f3( b.lo ), f3( b.hi ) );
+	for ( int i = 0; i < 8; ++i ) cost[ 8 * size_t( id ) + i ] = c;
+	dec[ 8 * size_t( id ) ] = 1;
+	for ( int i = 1; i < 8; ++i ) dec[ 8 * size_t( id ) + i ] = 0x80;
+}
+
+// The internal nodes created in one clustering round (their children exist).
+__global__ void k_dp_round( BNode *nodes, int id0, int id1, float *cost, uint8_t *dec, BuildParams bp )
+{
+	int id = id0 + blockIdx.x * blockDim.x + threadIdx.x;
+	if ( id >= id1 ) return;
+	BNode &nd = nodes[ id ];
+	const float *cl = cost + 8 * size_t( nd.left ), *cr = cost + 8 * size_t( nd.right );
+	float A = area( f3( nd.lo ), f3( nd.hi ) );
+	float D[ 9 ];
+	uint8_t K[ 9 ];
+	for ( int i = 2; i <= 8; ++i )
+	{
+		float best = DP_INF;
+		uint8_t bk = 1;
+		for ( int k = 1; k < i; ++k )
+		{
+			float c = cl[ k - 1 ] + cr[ i - k - 1 ];
+			if ( c < best ) best = c, bk = uint8_t( k );
+		}
+		D[ i ] = best, K[ i ] = bk;
+	}
+	float leafc = nd.count <= bp.max_leaf ? bp.dp_cost_tri * A * float( nd.count ) : DP_INF;
+	float internal = bp.dp_cost_node * A + D[ 8 ];
+	bool leaf = leafc <= internal;
+	float C[ 8 ];
+	C[ 0 ] = leaf ? leafc : internal;
+	uint8_t *d = dec + 8 * size_t( id );
+	d[ 0 ] = uint8_t( ( leaf ? 1 : 0 ) | ( ( K[ 8 ] - 1 ) << 1 ) );
+	for ( int i = 2; i <= 8; ++i )
+	{
+		bool prev = C[ i - 2 ] <= D[ i ];
+		C[ i - 1 ] = prev ? C[ i - 2 ] : D[ i ];
+		d[ i - 1 ] = uint8_t( ( prev ? 0x80 : 0 ) | K[ i ] );
+	}
+	for ( int i = 0; i < 8; ++i ) cost[ 8 * size_t( id ) + i ] = C[ i ];
+	nd.leaf = leaf ? 1 : 0;
+}
+
+// The children of a wide node built from binary node m: the roots of the best
+// representation of m's two subtrees with 8 slots.  Returns their count (0 on
+// a stack overflow, which the caller reports).
+__device__ __forceinline__ int dp_children( const BNode *bn, const uint8_t *dec, int m, int *ch )
+{
+	int sn[ 16 ], si[ 16 ], sp = 0, nc = 0;
+	const int k8 = ( ( dec[ 8 * size_t( m ) ] >> 1 ) & 7 ) + 1;
+	sn[ sp ] = bn[ m ].right, si[ sp++ ] = 8 - k8;
+	sn[ sp ] = bn[ m ].left, si[ sp++ ] = k8;
+	while ( sp > 0 )
+	{
+		--sp;
+		int x = sn[ sp ], i = si[ sp ];
+		const uint8_t *d = dec + 8 * size_t( x );
+		while ( i > 1 && ( d[ i - 1 ] & 0x80 ) ) --i;
+		if ( i == 1 )
+		{
+			if ( nc == 8 ) return 0;
+			ch[ nc++ ] = x;
+		}
+		else
+		{
+			if ( sp + 2 > 16 ) return 0;
+			int k = d[ i - 1 ] & 0x7F;
+			sn[ sp ] = bn[ x ].right, si[ sp++ ] = i - k;
+			sn[ sp ] = bn[ x ].left, si[ sp++ ] = k;
+		}
+	}
+	return nc;
+}
+
 struct WorkItem
 {
 	int bnode;
@@ -350,8 +446,8 @@ __device__ __forceinline__ uint32_t quant_exp( float extent )
 
 __global__ void k_collapse( const WorkItem *work, const uint32_t *n_work, WorkItem *next, uint32_t *n_next,
 							const BNode *bn, int n_int, const uint32_t *order, const float4 *src, WNode *wn,
-							float4 *tris, uint32_t *counters /* [0] nodes, [1] tris, [2] max depth */,
-							uint32_t depth )
+							float4 *tris, uint32_t *counters /* [0] nodes, [1] tris, [2] max depth, [7] errors */,
+							uint32_t depth, const uint8_t *dec )
 {
 	uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
 	if ( w >= *n_work ) return;
@@ -361,6 +457,16 @@ __global__ void k_collapse( const WorkItem *work, const uint32_t *n_work, WorkIt
 	const BNode &root = bn[ it.bnode ];
 	if ( root.leaf )
 		ch[ nc++ ] = it.bnode;
+	else if ( dec )
+	{
+		nc = dp_children( bn, dec, it.bnode, ch );
+		if ( nc == 0 )
+		{
+			// cannot happen for a consistent plan; fall back to the two children
+			atomicAdd( counters + 7, 1u );
+			ch[ 0 ] = root.left, ch[ 1 ] = root.right, nc = 2;
+		}
+	}
 	else
 	{
 		ch[ nc++ ] = root.left;
@@ -532,6 +638,8 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	check( cub::DeviceRadixSort::SortPairs( dtemp, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
 	int root_id = 0;
 	const uint32_t *order = vals2;
+	float *dp_cost = nullptr;
+	uint8_t *dp_dec = nullptr;
 	if ( !bp.ploc || n < 2 )
 	{
 		if ( n > 1 ) k_karras<<<( n - 1 + tb - 1 ) / tb, tb, 0, st>>>( keys2, int( n ), bn );
@@ -585,6 +693,19 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 			int id0 = round_base[ r ], id1 = round_base[ r + 1 ];
 			k_ploc_ranges<<<( id1 - id0 + tb - 1 ) / tb, tb, 0, st>>>( bn, id0, id1 );
 		}
+		if ( bp.dp_collapse )
+		{
+			// collapse plan, bottom-up in creation order (children come from earlier rounds)
+			check( cudaMallocAsync( &dp_cost, sizeof( float ) * 8 * n_b, st ), "bvh alloc" );
+			check( cudaMallocAsync( &dp_dec, 8 * n_b, st ), "bvh alloc" );
+			k_dp_leaves<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), bn, dp_cost, dp_dec, bp );
+			for ( size_t r = 0; r + 1 < round_base.size(); ++r )
+			{
+				int id0 = round_base[ r ], id1 = round_base[ r + 1 ];
+				k_dp_round<<<( id1 - id0 + tb - 1 ) / tb, tb, 0, st>>>( bn, id0, id1, dp_cost, dp_dec, bp );
+			}
+			check( cudaGetLastError(), "bvh plan" );
+		}
 		// the depth-first primitive order replaces the Morton order (vals)
 		k_ploc_order<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), bn, vals2, vals );
 		check( cudaGetLastError(), "bvh ploc" );
@@ -595,7 +716,7 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 
 	// Root work item: binary root -> wide node 0.
 	WorkItem root{ root_id, 0 };
-	uint32_t c0[ 5 ] = { 1, 0, 0, 1, 0 };
+	uint32_t c0[ 8 ] = { 1, 0, 0, 1, 0, 0, 0, 0 };
 	check( cudaMemcpyAsync( wa, &root, sizeof root, cudaMemcpyHostToDevice, st ), "bvh root" );
 	check( cudaMemcpyAsync( cnt, c0, sizeof c0, cudaMemcpyHostToDevice, st ), "bvh root" );
 	uint32_t n_work = 1, depth = 0;
@@ -605,7 +726,7 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	{
 		check( cudaMemsetAsync( nnext, 0, sizeof( uint32_t ), st ), "bvh level" );
 		k_collapse<<<( n_work + 127 ) / 128, 128, 0, st>>>( cur, ncur, nxt, nnext, bn, int( n ) - 1, order, d_src,
-															out.nodes, out.tris, cnt, depth + 1 );
+															out.nodes, out.tris, cnt, depth + 1, dp_dec );
 		check( cudaGetLastError(), "bvh collapse" );
 		check( cudaMemcpyAsync( &n_work, nnext, sizeof( uint32_t ), cudaMemcpyDeviceToHost, st ), "bvh level" );
 		check( cudaStreamSynchronize( st ), "bvh level" );
@@ -614,12 +735,15 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 		++depth;
 		if ( depth > 4096 ) throw std::runtime_error( "bvh: collapse did not terminate" );
 	}
-	uint32_t res[ 3 ];
+	uint32_t res[ 8 ];
 	check( cudaMemcpyAsync( res, cnt, sizeof res, cudaMemcpyDeviceToHost, st ), "bvh result" );
 	check( cudaStreamSynchronize( st ), "bvh result" );
 	out.n_nodes = res[ 0 ];
 	out.depth = res[ 2 ];
 	if ( res[ 1 ] != n ) throw std::runtime_error( "bvh: triangle count mismatch after collapse" );
+	if ( res[ 7 ] ) throw std::runtime_error( "bvh: inconsistent collapse plan" );
+	if ( dp_cost ) cudaFreeAsync( dp_cost, st );
+	if ( dp_dec ) cudaFreeAsync( dp_dec, st );
 	for ( void *p : { (void *)blo, (void *)bhi, (void *)cb, (void *)keys, (void *)keys2, (void *)vals, (void *)vals2,
 					  (void *)bn, (void *)flags, (void *)wa, (void *)wb, (void *)cnt, dtemp } )
 		cudaFreeAsync( p, st );

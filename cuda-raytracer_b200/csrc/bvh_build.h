@@ -27,6 +27,11 @@ struct BuildParams
 	int radius = 10;
 	int max_leaf = 3;
 	float cost_node = 1.2f, cost_tri = 1.0f;
+	// 8-wide collapse: plan by dynamic programming over the SAH (PLOC trees),
+	// with the costs of a wide-node visit and a triangle test; false: greedy
+	// (open the largest child first)
+	bool dp_collapse = true;
+	float dp_cost_node = 1.0f, dp_cost_tri = 0.3f;
 };
 void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st,
 					 const BuildParams &bp = BuildParams() );

@@ -146,15 +146,26 @@ int cr_scene_commit(cr_scene *s, uint64_t light_seed, void *stream);
  *                nodes visited per ray)
  *   ploc_radius  clustering search radius in Morton positions [10]
  *   max_leaf     triangles per leaf, 1..4 [3]
- *   cost_node, cost_tri  SAH costs of a node visit and a triangle test [1.2, 1] */
+ *   cost_node, cost_tri  binary-tree SAH costs of a node visit and a triangle
+ *                test [1.2, 1]
+ *   collapse     CR_COLLAPSE_SAH: plan the 8-wide collapse by dynamic
+ *                programming over the SAH (PLOC trees) [default], or
+ *                CR_COLLAPSE_GREEDY: open the largest child first
+ *   wide_cost_node, wide_cost_tri  SAH costs of a wide-node visit and a
+ *                triangle test in that plan [1, 0.3] */
 #define CR_BUILD_PLOC 0
 #define CR_BUILD_LBVH 1
+#define CR_COLLAPSE_SAH 0
+#define CR_COLLAPSE_GREEDY 1
 typedef struct cr_build_config {
     int32_t builder;
     uint32_t ploc_radius;
     uint32_t max_leaf;
     float cost_node;
     float cost_tri;
+    int32_t collapse;
+    float wide_cost_node;
+    float wide_cost_tri;
 } cr_build_config;
 int cr_scene_set_build(cr_scene *s, const cr_build_config *cfg);
 
