@@ -24,7 +24,7 @@ CLI_PATH = os.path.join(HERE, "lib", "cr")
 
 CR_OK = 0
 KOISHI, MIS = 0, 1
-KERNELS = ("Radiance",)
+KERNELS = ("Radiance", "Normal", "Visibility", "HalfVector")
 TRACERS = ("CudaWavefront", "CPUMulticore")
 DEFAULT_LIGHT_SEED = 0x330E
 U32_MAX = 0xFFFFFFFF
@@ -113,6 +113,7 @@ def lib():
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
+            "cr_scene_set_kernel": (I, [P, C.c_char_p]),
             "cr_measure_peaks": (I, [P, P, P]),
             "cr_scene_info": (I, [P, P, P, P, P]),
             "cr_scene_destroy": (None, [P]),
@@ -256,6 +257,11 @@ class Scene:
     def trace_device(self, rays_ptr, n, hits_ptr, any_hit=False, stream=0):
         _check(lib().cr_trace_rays_device(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr),
                                           int(bool(any_hit)), C.c_void_p(stream)))
+
+    def set_kernel(self, name):
+        """cr_scene_set_kernel: Radiance, or the debug kernels Normal, Visibility, HalfVector."""
+        _check(lib().cr_scene_set_kernel(self.h, name.encode()))
+        return self
 
     def render(self, width, height, spp, **kw):
         """Mean radiance per pixel (window-sized H x W x 3 float64) and stats."""

@@ -875,6 +875,16 @@ struct Resolved
 	uint64_t samples;
 };
 
+// Factory<Kernel> names (src/core/kernel/kernel.impl.cu:10-15) -> KERNEL_*; -1 if unknown.
+int kernel_id( const std::string &name )
+{
+	if ( name == "Radiance" ) return KERNEL_RADIANCE;
+	if ( name == "Normal" ) return KERNEL_NORMAL;
+	if ( name == "Visibility" ) return KERNEL_VISIBILITY;
+	if ( name == "HalfVector" ) return KERNEL_HALFVECTOR;
+	return -1;
+}
+
 Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 {
 	if ( !s || !desc ) fail( CR_ERR_INVALID, "null argument" );
@@ -882,7 +892,9 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	if ( !desc->width || !desc->height || !desc->spp ) fail( CR_ERR_INVALID, "width, height and spp must be positive" );
 	if ( !s->has_camera ) fail( CR_ERR_INVALID, "no camera in the scene" );
 	if ( s->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, "orthographic lens is outside the Radiance path implemented here" );
-	if ( s->kernel != "Radiance" ) fail( CR_ERR_UNSUPPORTED, "kernel '" + s->kernel + "' is not implemented (Radiance only)" );
+	const int kernel = kernel_id( s->kernel );
+	if ( kernel < 0 )
+		fail( CR_ERR_UNSUPPORTED, "kernel '" + s->kernel + "' is not registered (Radiance, Normal, Visibility, HalfVector)" );
 
 	Resolved r;
 	RenderConfig &c = r.cfg;
@@ -907,6 +919,11 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 		desc->traverse_blocks_per_sm ? int( std::min<uint32_t>( desc->traverse_blocks_per_sm, 8 ) ) : s->tune_blocks;
 	r.sc = dev_scene( s );
 	r.sc.cam = make_camera( s->cam, desc->width, desc->height, desc->spp );
+	c.kernel = kernel;
+	if ( ( kernel == KERNEL_VISIBILITY || kernel == KERNEL_HALFVECTOR ) && s->lights.empty() )
+		fail( CR_ERR_INVALID, "kernel '" + s->kernel + "' samples light 0, and the scene has no light" );
+	if ( kernel != KERNEL_RADIANCE && desc->guiding )
+		fail( CR_ERR_INVALID, "learned path guiding needs the Radiance kernel" );
 	if ( desc->guiding )
 	{
 		if ( c.estimator != EST_MIS ) fail( CR_ERR_INVALID, "learned path guiding needs the MIS estimator" );
@@ -1464,6 +1481,16 @@ int cr_measure_peaks( void *stream, double *l2_read_gbs, double *fp32_tflops )
 		const char *err = nullptr;
 		if ( cr_measure_peaks_impl( stream, l2_read_gbs, fp32_tflops, &err ) != 0 )
 			fail( CR_ERR_CUDA, err ? err : "peak measurement failed" );
+	} );
+}
+
+int cr_scene_set_kernel( cr_scene *s, const char *name )
+{
+	return guarded( [&] {
+		if ( !s || !name ) fail( CR_ERR_INVALID, "null argument" );
+		if ( kernel_id( name ) < 0 )
+			fail( CR_ERR_UNSUPPORTED, std::string( "kernel '" ) + name + "' is not registered (Radiance, Normal, Visibility, HalfVector)" );
+		s->kernel = name;
 	} );
 }
 

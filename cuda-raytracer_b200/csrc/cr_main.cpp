@@ -19,7 +19,7 @@ static void usage()
 		"  -o <file>            Place the output into <file>. (a.png)\n"
 		"  -s, --sample-per-pixel <n>  Number of sample points per pixel. (1)\n"
 		"  --resolution=<WxH>   Target resolution. (1024x768)\n"
-		"  -k, --kernel <name>  Kernel function. (Radiance)\n"
+		"  -k, --kernel <name>  Kernel function: Radiance, Normal, Visibility, HalfVector. (Radiance)\n"
 		"  -t, --tracer <name>  Tracer. (CudaWavefront)\n"
 		"  -a, --allocator <n>  Accepted for compatibility; device memory is managed internally.\n"
 		"  --pfm <file>         Also write linear radiance as a PFM.\n"
@@ -56,7 +56,7 @@ int main( int argc, char **argv )
 		}
 		else if ( a == "-l" || a == "--list" )
 		{
-			std::printf( "kernels: Radiance\ntracers: CudaWavefront (also accepts CPUMulticore)\n" );
+			std::printf( "kernels: Radiance Normal Visibility HalfVector\ntracers: CudaWavefront (also accepts CPUMulticore)\n" );
 			return 0;
 		}
 		else if ( a == "-v" || a == "--visualize" )

@@ -720,6 +720,80 @@ __global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, dou
 	}
 }
 
+// The reference's debug kernels on the bounce-0 hits (L was zeroed by
+// k_generate): NormalKernel (normal.hpp:17-31) writes n * 0.5 + 0.5;
+// HalfVectorKernel (halfVector.hpp:17-43) the angle between the normal and the
+// half vector of the view direction and a light-0 sample, * 2 / pi;
+// VisibilityKernel (visibility.hpp:17-41) queues the light-0 sample's segment,
+// whose any-hit pass adds (1, 1, 1) when it is unoccluded and its radiance
+// E / pdf is not zero.  Light sampling is AreaLight::sample as in
+// shade_koishi, with the reference's 4e-3 segment offsets.
+__global__ void __launch_bounds__( 128 ) k_aov( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa, uint2 key )
+{
+	const uint32_t n = wb.counters[ CNT_EXT ];
+	const uint32_t *q = wb.queue[ 0 ];
+	uint32_t *shadow_count = wb.counters + CNT_SHADOW;
+	const uint32_t stride = gridDim.x * blockDim.x;
+	for ( uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane_id(); base < n; base += stride )
+	{
+		const uint32_t i = base + lane_id();
+		bool shadow = false;
+		uint32_t path = 0;
+		if ( i < n )
+		{
+			path = q[ i ];
+			const HitRec h = wb.hit[ path ];
+			if ( h.id != HIT_MISS )
+			{
+				const float3 o = f3( wb.ray_o[ path ] ), d = f3( wb.ray_d[ path ] );
+				const Surface s = surface_at( sc, o, d, h, false );
+				float3 L = f3( 0.f, 0.f, 0.f );
+				if ( cfg.kernel == KERNEL_NORMAL )
+					L = s.ns * 0.5f + f3( 0.5f, 0.5f, 0.5f );
+				else
+				{
+					const uint64_t gw = wa.first + path;
+					const uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
+					const uint64_t g =
+						( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
+					const float4 r0 = rand4( key, g, 0, 0 );
+					const DevLight lt = sc.lights[ 0 ];
+					float3 lp, ln;
+					float pdf;
+					koishi_light_point( sc, lt, r0.x, r0.y, lp, ln, pdf );
+					float3 wiw = s.p - lp;
+					pdf *= dot( wiw, wiw ) / fabsf( dot( ln, normalize( wiw ) ) );
+					if ( cfg.kernel == KERNEL_HALFVECTOR )
+					{
+						const Frame fr = koishi_frame( s.ns );
+						const float3 wo = fr.local( -d ), wi = fr.local( normalize( lp - s.p ) );
+						const float a = acosf( normalize( wi + wo ).z ) * ( 2.f / PI_F );
+						L = f3( a, a, a );
+					}
+					else
+					{
+						const float3 li = f3( lt.emission ) / pdf;
+						if ( !( li.x == 0.f && li.y == 0.f && li.z == 0.f ) )
+						{
+							const float3 dd = lp - s.p;
+							const float3 sd = normalize( dd );
+							const float3 diff = sd * KOISHI_EPS;
+							const float3 so = s.p + diff;
+							wb.sh_o[ path ] = make_float4( so.x, so.y, so.z, 0.f );
+							wb.sh_d[ path ] = make_float4( sd.x, sd.y, sd.z, length( dd - 2.f * diff ) );
+							wb.sh_c[ path ] = make_float4( 1.f, 1.f, 1.f, 0.f );
+							shadow = true;
+						}
+					}
+				}
+				wb.L[ path ] = make_float4( L.x, L.y, L.z, 0.f );
+			}
+		}
+		const uint32_t si = warp_append( shadow, shadow_count );
+		if ( shadow ) wb.shadow_queue[ si ] = path;
+	}
+}
+
 // Film accumulation of a batched wave: global pixels p0..p1 (those whose
 // samples meet the wave), each into its job's film.
 __global__ void k_accumulate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa, uint64_t p0, uint64_t p1 )
@@ -1073,7 +1147,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 			int gg = int( std::min<uint64_t>( ( wa.n + 255 ) / 256, uint64_t( sms ) * 16 ) );
 			k_generate<<<gg, 256, 0, st>>>( sc, wc, wb, wa );
 		} );
-		for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
+		for ( uint32_t b = 0; b <= ( cfg.kernel == KERNEL_RADIANCE ? cfg.max_bounce : 0u ); ++b )
 		{
 			timed( 0, [&] {
 				ExtendIO io{ wb.queue[ b & 1 ], wb.ray_o, wb.ray_d, wb.hit };
@@ -1088,8 +1162,11 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				timed( 4, [&] {
 					k_guide_infer<<<sms * 2, tc::THREADS, tc::SMEM_BYTES, st>>>( sc, wc, wb, b, guide->Wp );
 				} );
-			timed( 2, [&] { k_shade<false><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} ); } );
-			if ( sc.n_lights )
+			if ( cfg.kernel != KERNEL_RADIANCE )
+				timed( 2, [&] { k_aov<<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, key ); } );
+			else
+				timed( 2, [&] { k_shade<false><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} ); } );
+			if ( sc.n_lights && cfg.kernel != KERNEL_NORMAL && cfg.kernel != KERNEL_HALFVECTOR )
 				timed( 1, [&] {
 					ShadowIO io{ wb.shadow_queue, wb.sh_o, wb.sh_d, wb.sh_c, wb.L };
 					const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;

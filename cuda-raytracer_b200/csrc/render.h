@@ -56,10 +56,20 @@ constexpr uint32_t CPB = 4;
 constexpr uint32_t CNT_EXT = 0, CNT_SHADOW = 1, CNT_EXT_CURSOR = 2, CNT_SHADOW_CURSOR = 3;
 inline constexpr uint32_t n_counters_for( uint32_t max_bounce ) { return CPB * ( max_bounce + 3 ); }
 
+// The reference's kernel registry (src/core/kernel/kernel.impl.cu:10-15).
+enum : int32_t
+{
+	KERNEL_RADIANCE = 0,
+	KERNEL_NORMAL = 1,      // NormalKernel (normal.hpp:17-31)
+	KERNEL_VISIBILITY = 2,  // VisibilityKernel (visibility.hpp:17-41)
+	KERNEL_HALFVECTOR = 3   // HalfVectorKernel (halfVector.hpp:17-43)
+};
+
 struct RenderConfig
 {
 	uint32_t spp, max_bounce;
 	int32_t estimator;
+	int32_t kernel = KERNEL_RADIANCE;
 	uint32_t x0, y0, ww, wh;  // window origin and size
 	uint64_t seed;
 	uint32_t wave_paths;

@@ -139,6 +139,14 @@ int cr_scene_set_camera(cr_scene *s, const float *position, const float *target,
  * (src/core/primitive/mesh.hpp:61-84). */
 int cr_scene_commit(cr_scene *s, uint64_t light_seed, void *stream);
 
+/* Selects the kernel by its Factory<Kernel> name (kernel.impl.cu:10-15), as
+ * the scene file's ["tracer", {"kernel": [name, ...]}] or `cr -k` does:
+ * "Radiance" (default), or the debug kernels "Normal" (shading normal * 0.5 +
+ * 0.5, normal.hpp:17-31), "Visibility" (1 where a sample of light 0 is
+ * unoccluded, visibility.hpp:17-41) and "HalfVector" (angle of the view/light-0
+ * half vector from the normal, * 2 / pi, halfVector.hpp:17-43). */
+int cr_scene_set_kernel(cr_scene *s, const char *name);
+
 /* No counterpart in the reference.  BVH build options, set before
  * cr_scene_commit (defaults in brackets):
  *   builder      CR_BUILD_PLOC: locally-ordered clustering [default], or

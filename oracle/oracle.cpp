@@ -630,6 +630,73 @@ V3 radiance_koishi( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rn
 	return L;
 }
 
+// The reference's debug kernels: NormalKernel (normal.hpp:17-31),
+// VisibilityKernel (visibility.hpp:17-41) and HalfVectorKernel
+// (halfVector.hpp:17-43).  Visibility and HalfVector draw one sample of light 0
+// through AreaLight::sample (areaLight.hpp:19-31), as the Radiance kernel's
+// light sampling above does for the chosen light.
+V3 aov_koishi( const orc_scene *s, V3 o, V3 d, int kind, Rng &rng )
+{
+	const double eps = 4e-3;  // varyings.hpp:19-37
+	Hit h;
+	if ( !intersect( s, o, d, INF, h ) ) return V3();
+	const Prim &pr = s->prims[ h.prim ];
+	V3 n;
+	if ( h.tri >= 0 )
+	{
+		const Tri &t = s->tris[ h.tri ];
+		n = normalize( t.n0 * ( 1 - h.u - h.v ) + t.n1 * h.u + t.n2 * h.v );
+	}
+	else
+		n = h.sphere_n;
+	(void)pr;
+	if ( kind == ORC_AOV_NORMAL ) return n * 0.5 + V3( 0.5, 0.5, 0.5 );
+	if ( s->lights.empty() ) return V3();
+	Frame fr;
+	fr.n = n;
+	fr.u = normalize( cross( n, V3( 0, 1, 0 ) ) );
+	fr.v = normalize( cross( n, fr.u ) );
+	V3 p = o + d * h.t;
+	V3 wo = fr.local( -d );
+	double ux = rng.next(), uy = rng.next();
+	const Light &lt = s->lights[ 0 ];
+	const Prim &lp = s->prims[ lt.prim ];
+	V3 lpos, lnrm;
+	double pdf;
+	if ( lt.kind == 0 )
+	{
+		size_t k = std::min( size_t( std::floor( ux * 1024 ) ), size_t( 1023 ) );
+		lpos = V3( lt.tp[ k ].x, lt.tp[ k ].y, lt.tp[ k ].z );
+		lnrm = V3( lt.tn[ k ].x, lt.tn[ k ].y, lt.tn[ k ].z );
+		pdf = lt.kpdf;
+	}
+	else
+	{
+		double th = ux * PI, ph = uy * PI * 2;
+		V3 w( std::sin( th ) * std::sin( ph ), std::sin( th ) * std::cos( ph ), std::cos( th ) );
+		lpos = lp.c + w * lp.r;
+		lnrm = w;
+		pdf = 1. / ( 4 * PI * lp.r * lp.r );
+	}
+	V3 wiw = p - lpos;
+	pdf *= dot( wiw, wiw ) / std::fabs( dot( lnrm, normalize( wiw ) ) );
+	if ( kind == ORC_AOV_HALFVECTOR )
+	{
+		V3 wi = fr.local( normalize( lpos - p ) );
+		V3 hv = normalize( wi + wo );
+		double a = std::acos( hv.z ) * 2 / PI;
+		return V3( a, a, a );
+	}
+	V3 dd = lpos - p;
+	V3 sd = normalize( dd );
+	V3 diff = normalize( sd ) * eps;
+	V3 so = p + diff;
+	double st = length( dd - 2.0 * diff );
+	V3 li = occluded_seg( s, so, sd, st ) ? V3() : s->shaders[ lp.shader ].emission / pdf;
+	bool zero = li.x == 0 && li.y == 0 && li.z == 0;
+	return zero ? V3() : V3( 1, 1, 1 );
+}
+
 // Light sampling for ORC_MIS: uniform light choice, area-proportional
 // triangle choice, uniform point on the triangle / sphere.
 void mis_light_sample( const orc_scene *s, const Light &lt, double u0, double u1, double u2, V3 &lp,
@@ -1045,7 +1112,9 @@ int orc_render( const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32
 					Rng rng( seed, uint64_t( y ) * W + x, k );
 					V3 d = lens.dir( x, y, k );
 					V3 L = estimator == ORC_KOISHI ? radiance_koishi( s, s->cam.pos, d, max_bounce, rng )
-												   : radiance_mis( s, s->cam.pos, d, max_bounce, rng, estimator == ORC_MIS ? 0 : estimator );
+						   : estimator >= ORC_AOV_NORMAL
+							   ? aov_koishi( s, s->cam.pos, d, estimator, rng )
+							   : radiance_mis( s, s->cam.pos, d, max_bounce, rng, estimator == ORC_MIS ? 0 : estimator );
 					if ( !finite3( L ) ) continue;  // cpuMulticore.cu:58-64
 					++c;
 					for ( int ch = 0; ch < 3; ++ch ) a[ ch ] += L[ ch ], q[ ch ] += L[ ch ] * L[ ch ];

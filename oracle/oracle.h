@@ -25,6 +25,11 @@ extern "C" {
 #endif
 
 enum { ORC_KOISHI = 0, ORC_MIS = 1 };
+/* The reference's debug kernels (src/core/kernel/{normal,visibility,halfVector}.hpp),
+ * as orc_render estimators: shading normal * 0.5 + 0.5; 1 where the light-0
+ * sample is unoccluded with nonzero radiance; the half-vector angle of the
+ * light-0 sample and the view direction, * 2 / pi. */
+enum { ORC_AOV_NORMAL = 4, ORC_AOV_VISIBILITY = 5, ORC_AOV_HALFVECTOR = 6 };
 enum { ORC_LAMBERT = 0, ORC_GLOSSY = 1, ORC_EMISSION = 2 };
 
 typedef struct orc_scene orc_scene;

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "cr_ref")
 
 KOISHI, MIS = 0, 1
+AOV_NORMAL, AOV_VISIBILITY, AOV_HALFVECTOR = 4, 5, 6  # the reference's debug kernels
 LAMBERT, GLOSSY, EMISSION = 0, 1, 2
 LIGHT_SEED = 0x330E
 

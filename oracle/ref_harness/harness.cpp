@@ -10,7 +10,7 @@
 // as src/core/meta/scene.cu:200-216 does for imported meshes.
 //
 // Sub-commands (all binary files are little-endian):
-//   render <scene.json> <W> <H> <spp> <threads> <out.crf> [maxBounce] [seed]
+//   render <scene.json> <W> <H> <spp> <threads> <out.crf> [maxBounce] [seed] [kernel]
 //       per-pixel float film through RadianceKernel::execute
 //       (src/core/kernel/radiance.cu:14-81), driven pixel by pixel like
 //       CPUMulticoreTracer::execute (src/core/tracer/cpuMulticore.cu:53-64):
@@ -251,11 +251,11 @@ void load( const std::string &path, Loaded &L, uint64_t light_seed )
 	}
 }
 
-Config kernel_config( uint32_t maxBounce )
+Config kernel_config( uint32_t maxBounce, const std::string &name = "Radiance" )
 {
 	Properties kp;
 	kp[ "maxBounce" ] = maxBounce;
-	return Config( "Radiance", kp );
+	return Config( name, kp );
 }
 
 int cmd_render( int argc, char **argv )
@@ -266,11 +266,12 @@ int cmd_render( int argc, char **argv )
 	uint32_t nth = std::stoul( argv[ 6 ] );
 	std::string out = argv[ 7 ];
 	uint64_t seed = argc > 9 ? std::stoull( argv[ 9 ] ) : 7;
+	std::string kname = argc > 10 ? argv[ 10 ] : "Radiance";  // any Factory<Kernel> name
 	Loaded L;
 	load( path, L, 0x330E );
 	uint32_t mb = argc > 8 ? std::stoul( argv[ 8 ] ) : L.max_bounce;
 	harness_rng::base_seed() = seed;
-	auto kern = Factory<Kernel>::create( kernel_config( mb ) );
+	auto kern = Factory<Kernel>::create( kernel_config( mb, kname ) );
 	PinholeLens lens( L.scene->camera[ 0 ], W, H, spp );
 	std::vector<double> sum( size_t( W ) * H * 3 ), sq( size_t( W ) * H * 3 );
 	std::vector<uint32_t> cnt( size_t( W ) * H );

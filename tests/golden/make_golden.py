@@ -12,8 +12,10 @@ stores its answers:
   c0_occlude.npz   segment occlusion (Scene::intersect(Seg))
   c0_film.npz      per-pixel sums / sums of squares / counts of a Radiance
                    render (RadianceKernel::execute through the harness)
+  c0_aov_*.npz     the same for the reference's debug kernels Normal,
+                   Visibility and HalfVector (src/core/kernel/*.hpp)
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [--aov-only]
 """
 import hashlib
 import os
@@ -92,7 +94,11 @@ def run(*args, cwd):
     return subprocess.run([oracle.REF_BIN, *map(str, args)], cwd=cwd, check=True, capture_output=True, text=True)
 
 
-def main():
+AOV_KERNELS = ("Normal", "Visibility", "HalfVector")
+AOV_W, AOV_H, AOV_SPP = 48, 48, 256
+
+
+def main(aov_only=False):
     if not oracle.ref_available():
         sys.exit("build the reference harness first: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
@@ -100,33 +106,43 @@ def main():
         scenes.write_scene(c0, tmp)
         js = f"{c0.name}.json"
 
-        run("lights", js, "lights.bin", oracle.LIGHT_SEED, cwd=tmp)
-        raw = open(os.path.join(tmp, "lights.bin"), "rb").read()
-        n = np.frombuffer(raw, "<u4", 1, 0)[0]
-        assert n == 1
-        group, = np.frombuffer(raw, "<i4", 1, 4)
-        pdf, = np.frombuffer(raw, "<f4", 1, 8)
-        nf, = np.frombuffer(raw, "<u4", 1, 12)
-        table = np.frombuffer(raw, "<f4", 1024 * 6, 16).reshape(1024, 6)
-        np.savez_compressed(os.path.join(HERE, "c0_lights.npz"), table=table, pdf=pdf, group=group, n_faces=nf,
-                            seed=oracle.LIGHT_SEED, scene_hash=scene_hash(c0))
+        if not aov_only:
+            run("lights", js, "lights.bin", oracle.LIGHT_SEED, cwd=tmp)
+            raw = open(os.path.join(tmp, "lights.bin"), "rb").read()
+            n = np.frombuffer(raw, "<u4", 1, 0)[0]
+            assert n == 1
+            group, = np.frombuffer(raw, "<i4", 1, 4)
+            pdf, = np.frombuffer(raw, "<f4", 1, 8)
+            nf, = np.frombuffer(raw, "<u4", 1, 12)
+            table = np.frombuffer(raw, "<f4", 1024 * 6, 16).reshape(1024, 6)
+            np.savez_compressed(os.path.join(HERE, "c0_lights.npz"), table=table, pdf=pdf, group=group, n_faces=nf,
+                                seed=oracle.LIGHT_SEED, scene_hash=scene_hash(c0))
 
-        for name, desc, nrand, seed in (("c0_trace.npz", c0, 2048, 5), ("ico_trace.npz", ico_scene(), 4096, 6)):
-            scenes.write_scene(desc, tmp)
-            rays = make_rays(desc, nrand, seed)
-            rays.tofile(os.path.join(tmp, "rays.f32"))
-            run("trace", f"{desc.name}.json", "rays.f32", "hits.bin", cwd=tmp)
-            hits = np.fromfile(os.path.join(tmp, "hits.bin"), "<i4").reshape(-1, 4)
-            np.savez_compressed(os.path.join(HERE, name), rays=rays, kind=hits[:, 0], index=hits[:, 1],
-                                tri=hits[:, 2], t=hits[:, 3].view(np.float32), scene_hash=scene_hash(desc))
+            for name, desc, nrand, seed in (("c0_trace.npz", c0, 2048, 5), ("ico_trace.npz", ico_scene(), 4096, 6)):
+                scenes.write_scene(desc, tmp)
+                rays = make_rays(desc, nrand, seed)
+                rays.tofile(os.path.join(tmp, "rays.f32"))
+                run("trace", f"{desc.name}.json", "rays.f32", "hits.bin", cwd=tmp)
+                hits = np.fromfile(os.path.join(tmp, "hits.bin"), "<i4").reshape(-1, 4)
+                np.savez_compressed(os.path.join(HERE, name), rays=rays, kind=hits[:, 0], index=hits[:, 1],
+                                    tri=hits[:, 2], t=hits[:, 3].view(np.float32), scene_hash=scene_hash(desc))
 
-        segs = make_segments(c0, 4096, 7)
-        segs.tofile(os.path.join(tmp, "segs.f32"))
-        run("occlude", js, "segs.f32", "occ.bin", cwd=tmp)
-        occ = np.fromfile(os.path.join(tmp, "occ.bin"), np.uint8)
-        np.savez_compressed(os.path.join(HERE, "c0_occlude.npz"), segs=segs, occluded=occ,
-                            scene_hash=scene_hash(c0))
+            segs = make_segments(c0, 4096, 7)
+            segs.tofile(os.path.join(tmp, "segs.f32"))
+            run("occlude", js, "segs.f32", "occ.bin", cwd=tmp)
+            occ = np.fromfile(os.path.join(tmp, "occ.bin"), np.uint8)
+            np.savez_compressed(os.path.join(HERE, "c0_occlude.npz"), segs=segs, occluded=occ,
+                                scene_hash=scene_hash(c0))
 
+        # the reference's debug kernels on the same scene (Normal, Visibility, HalfVector)
+        for kname in AOV_KERNELS:
+            run("render", js, AOV_W, AOV_H, AOV_SPP, os.cpu_count(), "aov.crf", c0.max_bounce, 19, kname, cwd=tmp)
+            film = oracle.read_crf(os.path.join(tmp, "aov.crf"))
+            np.savez_compressed(os.path.join(HERE, f"c0_aov_{kname.lower()}.npz"), sum=film.sum, sumsq=film.sumsq,
+                                count=film.count, width=AOV_W, height=AOV_H, spp=AOV_SPP, kernel=kname,
+                                scene_hash=scene_hash(c0))
+        if aov_only:
+            return
         run("render", js, FILM_W, FILM_H, FILM_SPP, os.cpu_count(), "film.crf", c0.max_bounce, 17, cwd=tmp)
         film = oracle.read_crf(os.path.join(tmp, "film.crf"))
         np.savez_compressed(os.path.join(HERE, "c0_film.npz"), sum=film.sum, sumsq=film.sumsq, count=film.count,
@@ -138,4 +154,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(aov_only="--aov-only" in sys.argv)

@@ -78,3 +78,27 @@ def test_koishi_render_matches_reference(oracle, c0):
     # image-level agreement of the mean
     rel = abs(f.mean.mean() - ref.mean.mean()) / ref.mean.mean()
     assert rel < 0.01
+
+
+@pytest.mark.parametrize("kernel", ["Normal", "Visibility", "HalfVector"])
+def test_debug_kernels_match_reference(oracle, c0, kernel):
+    """The oracle's restatement of the reference's debug kernels against the
+    reference's own renders of them (NormalKernel, VisibilityKernel,
+    HalfVectorKernel through the harness).  Normal is deterministic per
+    sub-pixel sample: pixels agree except where an object edge splits the
+    pixel's samples; the two light-sampling kernels agree within 3 sigma."""
+    g = golden(f"c0_aov_{kernel.lower()}.npz")
+    W, H, spp = int(g["width"]), int(g["height"]), int(g["spp"])
+    est = {"Normal": oracle.AOV_NORMAL, "Visibility": oracle.AOV_VISIBILITY, "HalfVector": oracle.AOV_HALFVECTOR}[kernel]
+    f = oracle.OracleScene(c0).render(W, H, spp, 7, est, seed=29)
+    ref = oracle.Film(g["sum"], g["sumsq"], g["count"])
+    assert np.all(ref.count == spp) and np.all(f.count == spp)
+    if kernel == "Normal":
+        d = np.abs(f.mean - ref.mean)
+        assert (d > 1e-3).mean() < 0.02, (d > 1e-3).mean()
+        assert abs(f.mean.mean() - ref.mean.mean()) < 1e-4
+    else:
+        floor = (1e-6 * np.maximum(np.abs(f.mean), np.abs(ref.mean))) ** 2
+        z = np.abs(f.mean - ref.mean) / np.sqrt(f.var_of_mean + ref.var_of_mean + floor + 1e-30)
+        assert (z > 3).mean() < 0.01, (z > 3).mean()
+        assert abs(f.mean.mean() / ref.mean.mean() - 1) < 0.01
