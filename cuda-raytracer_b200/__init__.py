@@ -4,7 +4,8 @@ xlnx/cuda-raytracer ("Koishi").
 This module is the Python face of ``include/cr.h`` (ctypes over
 ``lib/libcr_b200.so``).  It mirrors the reference's plugin surface for the
 path: the kernel registry (``Factory<Kernel>``, src/core/kernel/kernel.impl.cu:10-15)
-holds ``"Radiance"``, the tracer registry (``Factory<Tracer>``,
+holds ``"Radiance"`` and the reference's debug kernels ``"Normal"``,
+``"Visibility"`` and ``"HalfVector"``, the tracer registry (``Factory<Tracer>``,
 src/core/tracer/tracer.impl.cu:8-11) holds ``"CudaWavefront"`` and accepts the
 reference's ``"CPUMulticore"`` name for scene files written for it.  Every
 query runs on the GPU; there is no CPU fallback, and importing this module
@@ -113,7 +114,7 @@ def lib():
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
-            "cr_scene_set_kernel": (I, [P, C.c_char_p]),
+            "cr_scene_set_kernel": (I, [P, C.c_char_p]), "cr_mesh_file_info": (I, [C.c_char_p, P, P, P, P]),
             "cr_measure_peaks": (I, [P, P, P]),
             "cr_scene_info": (I, [P, P, P, P, P]),
             "cr_scene_destroy": (None, [P]),
@@ -350,6 +351,13 @@ class Guide:
         fn = lib().cr_guide_gradients_tc if tensor_cores else lib().cr_guide_gradients
         _check(fn(self.scene.h, _p(records), len(records), _p(gW), _p(gb), _p(ggrid)))
         return ggrid, gW, gb
+
+
+def mesh_file_info(path):
+    """cr_mesh_file_info: (groups, vertices, triangles, checksum) of an OBJ / PLY / CRM file."""
+    ng, nv, nt, cs = C.c_uint32(), C.c_uint64(), C.c_uint64(), C.c_double()
+    _check(lib().cr_mesh_file_info(path.encode(), C.byref(ng), C.byref(nv), C.byref(nt), C.byref(cs)))
+    return ng.value, nv.value, nt.value, cs.value
 
 
 def measure_peaks(stream=0):

@@ -437,6 +437,211 @@ std::vector<Group> load_obj( const std::string &path )
 	return out;
 }
 
+bool ends_with( const std::string &s, const std::string &e );
+
+// Stanford PLY: ascii, binary_little_endian or binary_big_endian, any
+// elements and properties (scalars and lists of every PLY type).  The vertex
+// element gives x, y, z and, when all three are present, nx, ny, nz; the face
+// element's vertex_indices (or vertex_index) list gives polygons, fanned into
+// triangles.  A PLY file carries no materials, so its mesh is one group named
+// "DefaultMaterial", the name assimp gives an imported mesh without one (the
+// reference binds imported meshes to shaders by material name,
+// scene.cu:180-198).  Missing normals are generated as for OBJ.
+std::vector<Group> load_ply( const std::string &path )
+{
+	const std::string d = read_file( path );
+	size_t pos = 0;
+	auto line = [&]() {
+		size_t e = d.find( '\n', pos );
+		if ( e == std::string::npos ) fail( CR_ERR_PARSE, path + ": truncated PLY header" );
+		std::string l = d.substr( pos, e - pos );
+		pos = e + 1;
+		if ( !l.empty() && l.back() == '\r' ) l.pop_back();
+		return l;
+	};
+	if ( line() != "ply" ) fail( CR_ERR_PARSE, path + ": not a PLY file" );
+	enum Fmt { ASCII, LE, BE } fmt = ASCII;
+	struct Prop
+	{
+		std::string name;
+		int type = 0, count_type = 0;  // bytes of the value / of the list count (0: scalar)
+		bool is_float = false, is_signed = false, list = false;
+		bool count_signed = false;
+	};
+	struct Elem
+	{
+		std::string name;
+		uint64_t count = 0;
+		std::vector<Prop> props;
+	};
+	std::vector<Elem> elems;
+	auto type_of = [&]( const std::string &t, int &bytes, bool &fl, bool &sg ) {
+		static const std::map<std::string, std::array<int, 3>> T = {
+			{ "char", { 1, 0, 1 } },    { "int8", { 1, 0, 1 } },   { "uchar", { 1, 0, 0 } },   { "uint8", { 1, 0, 0 } },
+			{ "short", { 2, 0, 1 } },   { "int16", { 2, 0, 1 } },  { "ushort", { 2, 0, 0 } },  { "uint16", { 2, 0, 0 } },
+			{ "int", { 4, 0, 1 } },     { "int32", { 4, 0, 1 } },  { "uint", { 4, 0, 0 } },    { "uint32", { 4, 0, 0 } },
+			{ "float", { 4, 1, 1 } },   { "float32", { 4, 1, 1 } }, { "double", { 8, 1, 1 } }, { "float64", { 8, 1, 1 } } };
+		auto it = T.find( t );
+		if ( it == T.end() ) fail( CR_ERR_PARSE, path + ": unknown PLY type '" + t + "'" );
+		bytes = it->second[ 0 ], fl = it->second[ 1 ] != 0, sg = it->second[ 2 ] != 0;
+	};
+	for ( ;; )
+	{
+		std::istringstream ls( line() );
+		std::string tag;
+		ls >> tag;
+		if ( tag == "end_header" ) break;
+		if ( tag == "format" )
+		{
+			std::string f;
+			ls >> f;
+			fmt = f == "ascii" ? ASCII : f == "binary_little_endian" ? LE : f == "binary_big_endian" ? BE : ( fail( CR_ERR_PARSE, path + ": unknown PLY format '" + f + "'" ), ASCII );
+		}
+		else if ( tag == "element" )
+		{
+			Elem e;
+			ls >> e.name >> e.count;
+			elems.push_back( e );
+		}
+		else if ( tag == "property" )
+		{
+			if ( elems.empty() ) fail( CR_ERR_PARSE, path + ": PLY property before any element" );
+			Prop p;
+			std::string t;
+			ls >> t;
+			if ( t == "list" )
+			{
+				std::string ct, vt;
+				ls >> ct >> vt >> p.name;
+				bool fl;
+				type_of( ct, p.count_type, fl, p.count_signed );
+				if ( fl ) fail( CR_ERR_PARSE, path + ": PLY list count of a floating type" );
+				type_of( vt, p.type, p.is_float, p.is_signed );
+				p.list = true;
+			}
+			else
+			{
+				ls >> p.name;
+				type_of( t, p.type, p.is_float, p.is_signed );
+			}
+			elems.back().props.push_back( p );
+		}
+		// comment / obj_info lines are skipped
+	}
+	// value readers
+	std::istringstream ascii( fmt == ASCII ? d.substr( pos ) : std::string() );
+	auto read_bin = [&]( int bytes, bool fl, bool sg ) -> double {
+		if ( pos + size_t( bytes ) > d.size() ) fail( CR_ERR_PARSE, path + ": truncated PLY data" );
+		unsigned char b[ 8 ];
+		std::memcpy( b, d.data() + pos, bytes );
+		pos += bytes;
+		if ( fmt == BE ) std::reverse( b, b + bytes );
+		if ( fl )
+		{
+			if ( bytes == 4 )
+			{
+				float f;
+				std::memcpy( &f, b, 4 );
+				return f;
+			}
+			double v;
+			std::memcpy( &v, b, 8 );
+			return v;
+		}
+		uint64_t u = 0;
+		std::memcpy( &u, b, bytes );
+		if ( sg && bytes < 8 && ( u >> ( 8 * bytes - 1 ) ) & 1 ) u |= ~uint64_t( 0 ) << ( 8 * bytes );
+		return sg ? double( int64_t( u ) ) : double( u );
+	};
+	auto read_val = [&]( int bytes, bool fl, bool sg ) -> double {
+		if ( fmt != ASCII ) return read_bin( bytes, fl, sg );
+		double v;
+		if ( !( ascii >> v ) ) fail( CR_ERR_PARSE, path + ": truncated PLY data" );
+		return v;
+	};
+	std::vector<float> P, N;
+	std::vector<uint32_t> F;
+	uint64_t nv = 0;
+	bool has_n = false;
+	for ( const Elem &e : elems )
+	{
+		int ix = -1, iy = -1, iz = -1, inx = -1, iny = -1, inz = -1, iface = -1;
+		for ( size_t k = 0; k < e.props.size(); ++k )
+		{
+			const std::string &n = e.props[ k ].name;
+			if ( e.name == "vertex" )
+			{
+				if ( n == "x" ) ix = int( k );
+				if ( n == "y" ) iy = int( k );
+				if ( n == "z" ) iz = int( k );
+				if ( n == "nx" ) inx = int( k );
+				if ( n == "ny" ) iny = int( k );
+				if ( n == "nz" ) inz = int( k );
+			}
+			if ( e.name == "face" && e.props[ k ].list && ( n == "vertex_indices" || n == "vertex_index" ) ) iface = int( k );
+		}
+		if ( e.name == "vertex" )
+		{
+			if ( ix < 0 || iy < 0 || iz < 0 ) fail( CR_ERR_PARSE, path + ": PLY vertices without x, y, z" );
+			has_n = inx >= 0 && iny >= 0 && inz >= 0;
+			nv = e.count;
+			if ( nv > ( 1ull << 31 ) ) fail( CR_ERR_PARSE, path + ": too many PLY vertices" );
+			P.reserve( 3 * nv ), N.reserve( has_n ? 3 * nv : 0 );
+		}
+		for ( uint64_t i = 0; i < e.count; ++i )
+		{
+			double vals[ 6 ] = { 0, 0, 0, 0, 0, 0 };
+			for ( size_t k = 0; k < e.props.size(); ++k )
+			{
+				const Prop &p = e.props[ k ];
+				if ( !p.list )
+				{
+					double v = read_val( p.type, p.is_float, p.is_signed );
+					int slot = int( k ) == ix ? 0 : int( k ) == iy ? 1 : int( k ) == iz ? 2 : int( k ) == inx ? 3 : int( k ) == iny ? 4 : int( k ) == inz ? 5 : -1;
+					if ( e.name == "vertex" && slot >= 0 ) vals[ slot ] = v;
+					continue;
+				}
+				double cnt = read_val( p.count_type, false, p.count_signed );
+				if ( !( cnt >= 0 && cnt < 1e6 ) ) fail( CR_ERR_PARSE, path + ": bad PLY list length" );
+				std::vector<uint32_t> poly;
+				for ( uint32_t j = 0; j < uint32_t( cnt ); ++j )
+				{
+					double v = read_val( p.type, p.is_float, p.is_signed );
+					if ( int( k ) == iface )
+					{
+						if ( !( v >= 0 && v < double( nv ) ) ) fail( CR_ERR_PARSE, path + ": PLY face index out of range" );
+						poly.push_back( uint32_t( v ) );
+					}
+				}
+				for ( size_t j = 1; j + 1 < poly.size(); ++j ) F.insert( F.end(), { poly[ 0 ], poly[ j ], poly[ j + 1 ] } );
+			}
+			if ( e.name == "vertex" )
+			{
+				P.insert( P.end(), { float( vals[ 0 ] ), float( vals[ 1 ] ), float( vals[ 2 ] ) } );
+				if ( has_n ) N.insert( N.end(), { float( vals[ 3 ] ), float( vals[ 4 ] ), float( vals[ 5 ] ) } );
+			}
+		}
+	}
+	Group g;
+	g.name = "DefaultMaterial";
+	g.v = std::move( P );
+	g.idx = std::move( F );
+	if ( has_n )
+		g.n = std::move( N );
+	else
+		smooth_normals( g.v, g.idx, g.n );
+	std::vector<Group> out;
+	out.push_back( std::move( g ) );
+	return out;
+}
+
+std::vector<Group> load_mesh_file( const std::string &path )
+{
+	if ( ends_with( path, ".crm" ) ) return load_crm( path );
+	if ( ends_with( path, ".ply" ) ) return load_ply( path );
+	return load_obj( path );
+}
+
 std::string join_path( const std::string &base, const std::string &p )
 {
 	if ( p.empty() || p[ 0 ] == '/' || base.empty() ) return p;
@@ -525,7 +730,7 @@ void load_scene( cr_scene *s, const std::string &text, const std::string &base )
 				if ( imported ) fail( CR_ERR_INVALID, "importing multiple scenes is not allowed" );
 				imported = true;
 				std::string path = join_path( base, p.string_or( "path", "" ) );
-				std::vector<Group> groups = ends_with( path, ".crm" ) ? load_crm( path ) : load_obj( path );
+				std::vector<Group> groups = load_mesh_file( path );
 				for ( auto &g : groups )
 				{
 					if ( g.idx.empty() ) continue;
@@ -1481,6 +1686,29 @@ int cr_measure_peaks( void *stream, double *l2_read_gbs, double *fp32_tflops )
 		const char *err = nullptr;
 		if ( cr_measure_peaks_impl( stream, l2_read_gbs, fp32_tflops, &err ) != 0 )
 			fail( CR_ERR_CUDA, err ? err : "peak measurement failed" );
+	} );
+}
+
+int cr_mesh_file_info( const char *path, uint32_t *n_groups, uint64_t *n_vertices, uint64_t *n_triangles,
+					   double *checksum )
+{
+	return guarded( [&] {
+		if ( !path ) fail( CR_ERR_INVALID, "null path" );
+		std::vector<Group> groups = load_mesh_file( path );
+		uint64_t nv = 0, nt = 0, corner = 0;
+		double cs = 0;
+		for ( const Group &g : groups )
+		{
+			nv += g.v.size() / 3, nt += g.idx.size() / 3;
+			// positions of the triangle corners, weighted by the corner's rank in
+			// the whole file: sensitive to order, not to the grouping
+			for ( size_t t = 0; t < g.idx.size(); ++t, ++corner )
+				for ( int c = 0; c < 3; ++c ) cs += double( g.v[ 3 * size_t( g.idx[ t ] ) + c ] ) * double( ( corner % 7 ) + 1 );
+		}
+		if ( n_groups ) *n_groups = uint32_t( groups.size() );
+		if ( n_vertices ) *n_vertices = nv;
+		if ( n_triangles ) *n_triangles = nt;
+		if ( checksum ) *checksum = cs;
 	} );
 }
 

@@ -553,6 +553,69 @@ def write_obj(path, groups):
             base += len(g.v)
 
 
+def write_ply(path, groups, encoding="binary_little_endian", normals=True, quads=False, extras=False):
+    """Stanford PLY of all groups merged into one mesh (PLY carries no
+    materials; an importer names it "DefaultMaterial").  encoding: "ascii",
+    "binary_little_endian" or "binary_big_endian".  quads: a triangle
+    (a, b, c) followed by (a, c, d) is written as the 4-gon (a, b, c, d), which
+    a reader fans back into the same two triangles.  extras: add per-vertex
+    colours and an "edge" element, which a reader must skip."""
+    v = np.concatenate([g.v for g in groups]).astype(np.float32)
+    n = np.concatenate([g.n for g in groups]).astype(np.float32)
+    offs = np.cumsum([0] + [len(g.v) for g in groups[:-1]])
+    f = np.concatenate([g.f.astype(np.int64) + o for g, o in zip(groups, offs)])
+    polys = []
+    i = 0
+    while i < len(f):
+        a, b, c = f[i]
+        if quads and i + 1 < len(f) and f[i + 1][0] == a and f[i + 1][1] == c:
+            polys.append((a, b, c, f[i + 1][2]))
+            i += 2
+        else:
+            polys.append((a, b, c))
+            i += 1
+    hdr = ["ply", f"format {encoding} 1.0", "comment written by the cuda-raytracer_b200 scene generator",
+           f"element vertex {len(v)}", "property float x", "property float y", "property float z"]
+    if normals:
+        hdr += ["property float nx", "property float ny", "property float nz"]
+    if extras:
+        hdr += ["property uchar red", "property uchar green", "property uchar blue"]
+    hdr += [f"element face {len(polys)}", "property list uchar int vertex_indices"]
+    if extras:
+        hdr += ["element edge 1", "property int vertex1", "property int vertex2"]
+    hdr += ["end_header"]
+    with open(path, "wb") as fh:
+        fh.write(("\n".join(hdr) + "\n").encode())
+        if encoding == "ascii":
+            for k in range(len(v)):
+                row = [f"{x:.9g}" for x in v[k]] + ([f"{x:.9g}" for x in n[k]] if normals else [])
+                row += ["200", "100", "50"] if extras else []
+                fh.write((" ".join(row) + "\n").encode())
+            for p in polys:
+                fh.write((f"{len(p)} " + " ".join(str(int(x)) for x in p) + "\n").encode())
+            if extras:
+                fh.write(b"0 1\n")
+            return
+        e = "<" if encoding == "binary_little_endian" else ">"
+        cols = [v] + ([n] if normals else [])
+        vdt = [("x", e + "f4"), ("y", e + "f4"), ("z", e + "f4")]
+        if normals:
+            vdt += [("nx", e + "f4"), ("ny", e + "f4"), ("nz", e + "f4")]
+        if extras:
+            vdt += [("r", "u1"), ("g", "u1"), ("b", "u1")]
+        rec = np.zeros(len(v), dtype=vdt)
+        rec["x"], rec["y"], rec["z"] = v[:, 0], v[:, 1], v[:, 2]
+        if normals:
+            rec["nx"], rec["ny"], rec["nz"] = n[:, 0], n[:, 1], n[:, 2]
+        if extras:
+            rec["r"], rec["g"], rec["b"] = 200, 100, 50
+        fh.write(rec.tobytes())
+        for p in polys:
+            fh.write(np.uint8(len(p)).tobytes() + np.asarray(p, dtype=e + "i4").tobytes())
+        if extras:
+            fh.write(np.asarray([0, 1], dtype=e + "i4").tobytes())
+
+
 def scene_json(desc: SceneDesc, mesh_path: str, tracer="CudaWavefront", estimator=None):
     kern = {"maxBounce": int(desc.max_bounce)}
     if estimator:

@@ -139,6 +139,14 @@ int cr_scene_set_camera(cr_scene *s, const float *position, const float *target,
  * (src/core/primitive/mesh.hpp:61-84). */
 int cr_scene_commit(cr_scene *s, uint64_t light_seed, void *stream);
 
+/* Parses a mesh file the way an ["import", {"path"}] asset does (OBJ with
+ * per-usemtl groups, PLY as one "DefaultMaterial" group, or CRM) without
+ * building a scene: groups, vertices, triangles and a checksum of the
+ * triangle corner positions.  Host only; replaces the Assimp::Importer read
+ * of Scene::Scene (src/core/meta/scene.cu:37-44). */
+int cr_mesh_file_info(const char *path, uint32_t *n_groups, uint64_t *n_vertices, uint64_t *n_triangles,
+                      double *checksum);
+
 /* Selects the kernel by its Factory<Kernel> name (kernel.impl.cu:10-15), as
  * the scene file's ["tracer", {"kernel": [name, ...]}] or `cr -k` does:
  * "Radiance" (default), or the debug kernels "Normal" (shading normal * 0.5 +

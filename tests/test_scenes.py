@@ -3,6 +3,7 @@ import json
 import os
 
 import numpy as np
+import pytest
 
 
 def test_config0_shape(scenes):
@@ -54,3 +55,40 @@ def test_pinhole_rays_match_lens_formula(scenes):
     # the centre pixel's first sub-sample looks along the target direction
     t = np.asarray(d.camera["target"])
     assert np.dot(dirs[0], t / np.linalg.norm(t)) > 0.9999
+
+
+@pytest.mark.parametrize("encoding", ["ascii", "binary_little_endian", "binary_big_endian"])
+@pytest.mark.parametrize("quads,extras", [(False, False), (True, True)])
+def test_ply_import_reads_what_obj_import_reads(cr, scenes, tmp_path, encoding, quads, extras):
+    """The PLY reader (cr_mesh_file_info parses without a GPU) sees the same
+    triangles, in the same order, as the OBJ reader: 4-gons fan back into
+    their two triangles and unknown properties and elements are skipped."""
+    d = scenes.config0()
+    obj, ply = str(tmp_path / "m.obj"), str(tmp_path / "m.ply")
+    scenes.write_obj(obj, d.groups)
+    scenes.write_ply(ply, d.groups, encoding=encoding, quads=quads, extras=extras)
+    go, vo, to, co = cr.mesh_file_info(obj)
+    gp, vp, tp, cp = cr.mesh_file_info(ply)
+    assert go == len(d.groups) and gp == 1          # PLY: one "DefaultMaterial" group
+    assert to == tp == d.n_triangles
+    assert vp == sum(len(g.v) for g in d.groups)
+    assert cp == pytest.approx(co, rel=1e-12)
+
+
+def test_ply_without_normals_and_bad_files(cr, scenes, tmp_path):
+    d = scenes.config1(level=2)
+    ply = str(tmp_path / "n.ply")
+    scenes.write_ply(ply, d.groups, normals=False)
+    assert cr.mesh_file_info(ply)[2] == d.n_triangles
+    bad = tmp_path / "bad.ply"
+    bad.write_bytes(b"ply\nformat ascii 1.0\nelement vertex 3\nproperty float x\nproperty float y\nproperty float z\n"
+                    b"element face 1\nproperty list uchar int vertex_indices\nend_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 7\n")
+    with pytest.raises(cr.CrError, match="out of range"):
+        cr.mesh_file_info(str(bad))
+    trunc = tmp_path / "trunc.ply"
+    trunc.write_bytes(b"ply\nformat binary_little_endian 1.0\nelement vertex 3\nproperty float x\nproperty float y\n"
+                      b"property float z\nend_header\n\x00\x00")
+    with pytest.raises(cr.CrError, match="truncated"):
+        cr.mesh_file_info(str(trunc))
+    with pytest.raises(cr.CrError):
+        cr.mesh_file_info(str(tmp_path / "missing.ply"))
