@@ -112,6 +112,7 @@ def lib():
             "cr_scene_add_shader": (I, [P, C.c_char_p, C.c_char_p]),
             "cr_scene_add_mesh": (I, [P, P, U32, P, P, U32, C.c_char_p]),
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
+            "cr_scene_add_point_light": (I, [P, P, P, F]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
             "cr_scene_set_kernel": (I, [P, C.c_char_p]), "cr_mesh_file_info": (I, [C.c_char_p, P, P, P, P]),
@@ -136,6 +137,7 @@ def lib():
             "cr_batch_render": (I, [P, U64, P]), "cr_batch_destroy": (None, [P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
+            "cr_shader_execute": (I, [C.c_char_p, I, P, P, P, U32, U64, P, P, P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -209,6 +211,10 @@ class Scene:
         for sp in desc.spheres:
             c = np.asarray(sp["o"], np.float32)
             _check(lib().cr_scene_add_sphere(s.h, _p(c), float(sp["r"]), sp["shader"].encode()))
+        for pl in getattr(desc, "point_lights", []):
+            pos = np.asarray(pl["position"], np.float32)
+            col = np.asarray(pl.get("color", [1, 1, 1]), np.float32)
+            _check(lib().cr_scene_add_point_light(s.h, _p(pos), _p(col), float(pl.get("strength", 2.0))))
         cam = desc.camera
         # keep the arrays bound to names: ctypes only holds their addresses
         pos = np.asarray(cam["position"], np.float32)
@@ -419,6 +425,27 @@ def bsdf_eval(estimator, shader_cfg, wo, wi):
     pdf = np.zeros(n, np.float32)
     _check(lib().cr_bsdf_eval(estimator, json.dumps(shader_cfg).encode(), _p(wo), _p(wi), n, _p(f), _p(pdf)))
     return f, pdf
+
+
+SHADE_EVAL, SHADE_SAMPLE = 0, 1
+
+
+def shader_execute(shader_cfg, target, wo, u, wi=None):
+    """Shader::execute of a [Type, {props}] shader config (nested Mixed
+    included) with the reference estimator's semantics, for n local-frame
+    samples: target SHADE_EVAL (compute_f_by_wi_wo, wi given) or SHADE_SAMPLE
+    (sample_wi_f_by_wo).  u is (n, k) uniforms drawn in order.  Returns
+    (f, wi, emission, used)."""
+    wo = np.ascontiguousarray(wo, np.float32)
+    n = len(wo)
+    u = np.ascontiguousarray(np.asarray(u, np.float32).reshape(n, -1))
+    wi = np.zeros((n, 3), np.float32) if wi is None else np.array(wi, np.float32, order="C", copy=True)
+    f = np.zeros((n, 3), np.float32)
+    em = np.zeros((n, 3), np.float32)
+    used = np.zeros(n, np.uint32)
+    _check(lib().cr_shader_execute(json.dumps(shader_cfg).encode(), target, _p(wo), _p(wi), _p(u), u.shape[1], n,
+                                   _p(f), _p(em), _p(used)))
+    return f, wi, em, used
 
 
 def bsdf_sample(estimator, shader_cfg, wo, u):

@@ -131,6 +131,7 @@ struct cr_scene
 	std::vector<HostMesh> meshes;
 	std::vector<HostSphere> spheres;
 	std::vector<HostPrim> prims;
+	std::vector<DevLight> point_lights;  // pointLight assets, in asset order
 	HostCamera cam;
 	bool has_camera = false;
 	uint32_t max_bounce = 16;  // RadianceKernel::Configuration (radiance.hpp:12-15)
@@ -150,6 +151,7 @@ struct cr_scene
 	DevBuf<uint32_t> err;
 	std::vector<DevLight> lights;
 	std::vector<float4> tables_host;
+	std::string mis_blocker;  // why the MIS estimator cannot render this scene (empty: it can)
 	uint64_t n_tris = 0;
 	float scale = 1;
 	WaveBuffers wave;
@@ -185,20 +187,66 @@ namespace
 {
 // ------------------------------------------------------------------ shaders
 // Factory<Shader>::create over the shader registry (src/ext/shader/shader.impl.cu:15-24).
-DevShader make_shader( const Json &cfg )
+using ShaderTable = std::vector<std::pair<std::string, DevShader>>;
+
+// A [Type, {props}] config (util/config.hpp:39-49) or the error the reference
+// would raise for a malformed one.
+const Json &config_props( const Json &cfg, const char *what )
 {
 	if ( !cfg.is_array() || cfg.size() < 1 || !cfg.at( 0 ).is_string() )
-		fail( CR_ERR_PARSE, "shader config must be [Type, {props}]" );
-	const std::string &type = cfg.at( 0 ).str;
+		fail( CR_ERR_PARSE, std::string( what ) + " config must be [Type, {props}]" );
 	static const Json empty = [] {
 		Json j;
 		j.type = Json::Object;
 		return j;
 	}();
-	const Json &p = cfg.size() > 1 ? cfg.at( 1 ) : empty;
+	return cfg.size() > 1 ? cfg.at( 1 ) : empty;
+}
+
+// A required number property (the reference's get<float>( props, key ) throws
+// when it is absent).
+float required_number( const Json &p, const char *key, const std::string &owner )
+{
+	const Json *v = p.find( key );
+	if ( !v || !v->is_number() ) fail( CR_ERR_PARSE, owner + " needs a number \"" + key + "\"" );
+	return float( v->num );
+}
+
+// The SphericalDistribution of a GlossyBSDF, RefractionBSDF or GlassBSDF
+// (distribution.impl.cu: "Cosine", "Beckmann" with roughness, beckmann.hpp:11-17).
+void parse_distribution( const Json &p, const std::string &owner, DevShader &s )
+{
+	const Json *d = p.find( "distribution" );
+	if ( !d ) fail( CR_ERR_PARSE, owner + " needs a distribution" );
+	const Json &dp = config_props( *d, "distribution" );
+	const std::string &kind = d->at( 0 ).str;
+	if ( kind == "Beckmann" )
+	{
+		float rough = float( dp.number_or( "roughness", 0.5 ) );
+		s.dist = DIST_BECKMANN, s.alpha = rough, s.alpha2 = rough * rough;
+	}
+	else if ( kind == "Cosine" )
+		s.dist = DIST_COSINE;
+	else
+		fail( CR_ERR_PARSE, "no such type: " + kind );
+}
+
+// Factory<Shader>::create (shader.impl.cu:16-23) into a flat table: returns
+// the entry for cfg; the shaders a Mixed nests are appended to tab first and
+// referenced by index.
+DevShader make_shader( const Json &cfg, ShaderTable &tab, const std::string &name, int depth = 0 )
+{
+	if ( depth >= MAX_SHADER_DEPTH ) fail( CR_ERR_UNSUPPORTED, "shader " + name + " nests Mixed shaders too deeply" );
+	const Json &p = config_props( cfg, "shader" );
+	const std::string &type = cfg.at( 0 ).str;
 	DevShader s;
 	std::memset( &s, 0, sizeof s );
 	float one[ 3 ] = { 1, 1, 1 };
+	auto tint = [&]( DevShader &x ) {
+		float c[ 3 ] = { 1, 1, 1 };
+		p.vec3( "color", c );
+		for ( int i = 0; i < 3; ++i ) x.color[ i ] = c[ i ], x.albedo[ i ] = c[ i ];
+	};
 	if ( type == "Lambert" )  // lambert.hpp:12-19
 	{
 		float R[ 3 ] = { 1, 1, 1 }, c[ 3 ] = { 1, 1, 1 };
@@ -206,21 +254,11 @@ DevShader make_shader( const Json &cfg )
 		s.type = SH_LAMBERT;
 		for ( int i = 0; i < 3; ++i ) s.albedo[ i ] = c[ i ] * R[ i ], s.color[ i ] = c[ i ];
 	}
-	else if ( type == "GlossyBSDF" )  // glossy.hpp:11-17, beckmann.hpp:11-17
+	else if ( type == "GlossyBSDF" )  // glossy.hpp:11-17
 	{
-		float c[ 3 ] = { 1, 1, 1 };
-		p.vec3( "color", c );
-		const Json *d = p.find( "distribution" );
-		if ( !d ) fail( CR_ERR_PARSE, "GlossyBSDF needs a distribution" );
-		if ( !d->is_array() || d->size() < 1 || !d->at( 0 ).is_string() )
-			fail( CR_ERR_PARSE, "distribution must be [Type, {props}]" );
-		if ( d->at( 0 ).str != "Beckmann" )
-			fail( CR_ERR_UNSUPPORTED, "GlossyBSDF distribution '" + d->at( 0 ).str + "' is not supported (Beckmann only)" );
-		float rough = d->size() > 1 ? float( d->at( 1 ).number_or( "roughness", 0.5 ) ) : 0.5f;
+		tint( s );
+		parse_distribution( p, "GlossyBSDF", s );
 		s.type = SH_GLOSSY;
-		for ( int i = 0; i < 3; ++i ) s.color[ i ] = c[ i ], s.albedo[ i ] = c[ i ];
-		s.alpha = rough;
-		s.alpha2 = rough * rough;
 	}
 	else if ( type == "Emission" )  // emission.hpp:12-20
 	{
@@ -230,12 +268,56 @@ DevShader make_shader( const Json &cfg )
 		s.type = SH_EMISSION;
 		for ( int i = 0; i < 3; ++i ) s.emission[ i ] = c[ i ] * strength, s.albedo[ i ] = one[ i ], s.color[ i ] = one[ i ];
 	}
-	else if ( type == "Blackhole" || type == "RefractionBSDF" || type == "Mixed" || type == "Transparent" ||
-			  type == "GlassBSDF" )
-		fail( CR_ERR_UNSUPPORTED, "shader type '" + type + "' is outside the Radiance path implemented here" );
+	else if ( type == "Transparent" )  // transparent.hpp:11-15
+	{
+		tint( s );
+		s.type = SH_TRANSPARENT;
+	}
+	else if ( type == "Blackhole" )  // blackhole.hpp:11
+		s.type = SH_BLACKHOLE;
+	else if ( type == "RefractionBSDF" || type == "GlassBSDF" )  // refraction.hpp:11-19, glass.hpp:11-21
+	{
+		tint( s );
+		s.ior = required_number( p, "ior", type );
+		parse_distribution( p, type, s );
+		s.type = type == "GlassBSDF" ? SH_GLASS : SH_REFRACTION;
+	}
+	else if ( type == "Mixed" )  // mixed.hpp:11-20
+	{
+		const Json *fac = p.find( "fac" );
+		if ( !fac ) fail( CR_ERR_PARSE, "Mixed needs a fac" );
+		const Json &fp = config_props( *fac, "fac" );
+		const std::string &fk = fac->at( 0 ).str;
+		if ( fk == "Constant" )  // constant.hpp:11-20
+			s.fac_kind = FAC_CONSTANT, s.fac = required_number( fp, "value", "Constant" );
+		else if ( fk == "Fresnel" )  // fresnel.hpp:11-16
+			s.fac_kind = FAC_FRESNEL, s.ior = required_number( fp, "ior", "Fresnel" );
+		else
+			fail( CR_ERR_PARSE, "no such type: " + fk );
+		const Json *shs = p.find( "shaders" );
+		if ( !shs || !shs->is_array() || shs->size() < 2 ) fail( CR_ERR_PARSE, "Mixed needs two \"shaders\"" );
+		for ( int k = 0; k < 2; ++k )
+		{
+			std::string child = name + ".shaders[" + std::to_string( k ) + "]";
+			DevShader c = make_shader( shs->at( k ), tab, child, depth + 1 );
+			tab.emplace_back( child, c );
+			s.child[ k ] = int( tab.size() - 1 );
+		}
+		s.type = SH_MIXED;
+	}
 	else
 		fail( CR_ERR_PARSE, "no such type: " + type );
 	return s;
+}
+
+// Whether a shader is outside the MIS estimator's BSDFs (Lambert, Beckmann
+// GlossyBSDF, Emission); Mixed and the transmissive shaders have reference
+// semantics only.
+bool koishi_only( const DevShader &s )
+{
+	if ( s.type == SH_MIXED ) return true;
+	if ( s.type == SH_GLOSSY ) return s.dist != DIST_BECKMANN;
+	return s.type != SH_LAMBERT && s.type != SH_EMISSION;
 }
 
 int shader_id( cr_scene *s, const std::string &name )
@@ -244,7 +326,7 @@ int shader_id( cr_scene *s, const std::string &name )
 	if ( it != s->shader_ids.end() ) return it->second;
 	const Json *cfg = s->shader_cfg.find( name );
 	if ( !cfg ) fail( CR_ERR_INVALID, "Configuration for shader {" + name + "} not found." );
-	DevShader sh = make_shader( *cfg );
+	DevShader sh = make_shader( *cfg, s->shaders, name );
 	s->shaders.emplace_back( name, sh );
 	int id = int( s->shaders.size() - 1 );
 	s->shader_ids[ name ] = id;
@@ -750,9 +832,17 @@ void load_scene( cr_scene *s, const std::string &text, const std::string &base )
 			}
 			else if ( name.find( "light" ) != std::string::npos || name.find( "Light" ) != std::string::npos )
 			{
-				if ( name == "pointLight" )
-					fail( CR_ERR_UNSUPPORTED, "pointLight is outside the area-light Radiance path implemented here" );
-				fail( CR_ERR_PARSE, "unknown light type: " + name );
+				if ( name != "pointLight" ) fail( CR_ERR_PARSE, "unknown light type: " + name );
+				// PointLight (pointLight.hpp:13-18): position required, color * strength
+				DevLight L;
+				std::memset( &L, 0, sizeof L );
+				L.kind = LIGHT_POINT;
+				if ( !p.vec3( "position", L.pos ) ) fail( CR_ERR_PARSE, "pointLight needs \"position\"" );
+				float c[ 3 ] = { 1, 1, 1 };
+				p.vec3( "color", c );
+				float strength = float( p.number_or( "strength", 2.0 ) );
+				for ( int k = 0; k < 3; ++k ) L.emission[ k ] = c[ k ] * strength;
+				s->point_lights.push_back( L );
 			}
 			else
 				fail( CR_ERR_PARSE, "unknown asset type: " + name );
@@ -889,8 +979,17 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	std::vector<float4> src( 3 * nt ), attrs( 3 * nt );
 	std::vector<uint32_t> prim_first( s->prims.size(), 0 );
 	std::vector<int> prim_light( s->prims.size(), -1 );
-	// Lights: every Emission-shaded primitive (scene.cu:200-216), in primitive order.
-	std::vector<DevLight> lights;
+	// Lights: the pointLight assets in asset order (scene.cu:156-163), then
+	// every Emission-shaded primitive in primitive order (scene.cu:200-216).
+	std::vector<DevLight> lights( s->point_lights );
+	s->mis_blocker.clear();
+	if ( !s->point_lights.empty() ) s->mis_blocker = "pointLight";
+	for ( const HostPrim &hp : s->prims )
+	{
+		int shader = hp.kind == 0 ? s->meshes[ hp.index ].shader : s->spheres[ hp.index ].shader;
+		if ( s->mis_blocker.empty() && koishi_only( s->shaders[ shader ].second ) )
+			s->mis_blocker = "shader " + s->shaders[ shader ].first;
+	}
 	std::vector<float4> tables, ltris;
 	std::vector<float> cdf;
 	Lcg48 rng{ light_seed & 0xFFFFFFFFFFFFull };
@@ -1111,6 +1210,9 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	if ( c.max_bounce > 1024 ) fail( CR_ERR_INVALID, "max_bounce out of range" );
 	c.estimator = desc->estimator < 0 ? s->estimator : desc->estimator;
 	if ( c.estimator != EST_KOISHI && c.estimator != EST_MIS ) fail( CR_ERR_INVALID, "unknown estimator" );
+	if ( c.estimator == EST_MIS && !s->mis_blocker.empty() )
+		fail( CR_ERR_UNSUPPORTED, "the MIS estimator covers Lambert, Beckmann GlossyBSDF and Emission area lights; " +
+									  s->mis_blocker + " has the reference estimator only" );
 	c.x0 = x0, c.y0 = y0, c.ww = x1 - x0, c.wh = y1 - y0;
 	c.seed = desc->seed;
 	r.samples = uint64_t( c.ww ) * c.wh * c.spp;
@@ -1338,7 +1440,7 @@ int cr_scene_add_shader( cr_scene *s, const char *name, const char *config_json 
 		if ( !s || !name || !config_json ) fail( CR_ERR_INVALID, "null argument" );
 		if ( s->committed ) fail( CR_ERR_STATE, "scene already committed" );
 		Json cfg = parse_json( config_json );
-		DevShader sh = make_shader( cfg );
+		DevShader sh = make_shader( cfg, s->shaders, name );
 		auto it = s->shader_ids.find( name );
 		if ( it != s->shader_ids.end() )
 			s->shaders[ it->second ].second = sh, id = it->second;
@@ -1377,6 +1479,23 @@ int cr_scene_add_sphere( cr_scene *s, const float *c, float r, const char *shade
 		s->spheres.push_back( hs );
 		s->prims.push_back( HostPrim{ 1, int( s->spheres.size() - 1 ) } );
 		id = int( s->prims.size() - 1 );
+	} );
+	return rc == CR_OK ? id : rc;
+}
+
+int cr_scene_add_point_light( cr_scene *s, const float *position, const float *color, float strength )
+{
+	int id = -1;
+	int rc = guarded( [&] {
+		if ( !s || !position ) fail( CR_ERR_INVALID, "null argument" );
+		if ( s->committed ) fail( CR_ERR_STATE, "scene already committed" );
+		DevLight L;
+		std::memset( &L, 0, sizeof L );
+		L.kind = LIGHT_POINT;
+		std::memcpy( L.pos, position, sizeof L.pos );
+		for ( int k = 0; k < 3; ++k ) L.emission[ k ] = ( color ? color[ k ] : 1.f ) * strength;
+		s->point_lights.push_back( L );
+		id = int( s->point_lights.size() - 1 );
 	} );
 	return rc == CR_OK ? id : rc;
 }
@@ -1762,6 +1881,8 @@ int cr_batch_create( const cr_batch_job *jobs, uint32_t n_jobs, uint32_t max_bou
 			if ( j.scene->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, at + "orthographic lens is outside the Radiance path" );
 			if ( !j.width || !j.height || !j.spp ) fail( CR_ERR_INVALID, at + "width, height and spp must be positive" );
 			if ( !j.d_sum || !j.d_sumsq || !j.d_count ) fail( CR_ERR_INVALID, at + "null film" );
+			if ( estimator == EST_MIS && !j.scene->mis_blocker.empty() )
+				fail( CR_ERR_UNSUPPORTED, at + "the MIS estimator does not cover " + j.scene->mis_blocker );
 		}
 		std::unique_ptr<cr_batch> b( new cr_batch );
 		b->req.assign( jobs, jobs + n_jobs );
@@ -2115,16 +2236,23 @@ int cr_render_file( const char *json_path, const char *png_path, const char *pfm
 	} );
 }
 
-static DevShader shader_from_json( const char *js )
+// A single-node shader for cr_bsdf_eval / cr_bsdf_sample: those take two
+// uniforms per sample and no selection numbers.
+static DevShader shader_from_json( int est, const char *js )
 {
 	if ( !js ) fail( CR_ERR_INVALID, "null shader" );
-	return make_shader( parse_json( js ) );
+	ShaderTable tab;
+	DevShader sh = make_shader( parse_json( js ), tab, "shader" );
+	if ( sh.type == SH_MIXED || sh.type == SH_GLASS )
+		fail( CR_ERR_INVALID, "Mixed and GlassBSDF draw selection numbers: use cr_shader_execute" );
+	if ( est == EST_MIS && koishi_only( sh ) ) fail( CR_ERR_UNSUPPORTED, "the MIS estimator does not cover this shader" );
+	return sh;
 }
 
 int cr_bsdf_eval( int est, const char *shader_json, const float *wo, const float *wi, uint64_t n, float *f, float *pdf )
 {
 	return guarded( [&] {
-		DevShader sh = shader_from_json( shader_json );
+		DevShader sh = shader_from_json( est, shader_json );
 		if ( !n ) return;
 		if ( !wo || !wi || !f || !pdf ) fail( CR_ERR_INVALID, "null argument" );
 		float *d;
@@ -2144,7 +2272,7 @@ int cr_bsdf_sample( int est, const char *shader_json, const float *wo, const flo
 					float *weight, float *pdf )
 {
 	return guarded( [&] {
-		DevShader sh = shader_from_json( shader_json );
+		DevShader sh = shader_from_json( est, shader_json );
 		if ( !n ) return;
 		if ( !wo || !u || !wi || !weight || !pdf ) fail( CR_ERR_INVALID, "null argument" );
 		float *d;
@@ -2158,6 +2286,43 @@ int cr_bsdf_sample( int est, const char *shader_json, const float *wo, const flo
 		cudaError_t e = cudaMemcpy( pdf, dp, 4 * n, cudaMemcpyDeviceToHost );
 		cudaFree( d );
 		cuda_check( e, "bsdf sample" );
+	} );
+}
+
+int cr_shader_execute( const char *shader_json, int target, const float *wo, float *wi, const float *u, uint32_t k,
+					   uint64_t n, float *f, float *emission, uint32_t *used )
+{
+	return guarded( [&] {
+		if ( !shader_json ) fail( CR_ERR_INVALID, "null shader" );
+		if ( target != CR_SHADE_EVAL && target != CR_SHADE_SAMPLE ) fail( CR_ERR_INVALID, "unknown shader target" );
+		ShaderTable tab;
+		DevShader root = make_shader( parse_json( shader_json ), tab, "shader" );
+		if ( !n ) return;
+		if ( !wo || !wi || !f || !emission || !used || ( k && !u ) ) fail( CR_ERR_INVALID, "null argument" );
+		if ( n > ( 1ull << 28 ) || uint64_t( k ) > 64 ) fail( CR_ERR_INVALID, "at most 2^28 samples of 64 uniforms" );
+		// entry 0 is the root; nested entries keep their order, one slot later
+		std::vector<DevShader> dt( 1, root );
+		for ( auto &x : tab ) dt.push_back( x.second );
+		for ( auto &x : dt )
+			if ( x.type == SH_MIXED ) ++x.child[ 0 ], ++x.child[ 1 ];
+		const size_t tb = ( sizeof( DevShader ) * dt.size() + 255 ) / 256 * 256;
+		const size_t bytes = tb + 4 * ( 12 * n + size_t( k ) * n + n );
+		char *d;
+		cuda_check( cudaMalloc( (void **)&d, bytes ), "cudaMalloc" );
+		DevShader *dtab = (DevShader *)d;
+		float *dwo = (float *)( d + tb ), *dwi = dwo + 3 * n, *df = dwi + 3 * n, *de = df + 3 * n, *du = de + 3 * n;
+		uint32_t *dused = (uint32_t *)( du + size_t( k ) * n );
+		cudaMemcpy( dtab, dt.data(), sizeof( DevShader ) * dt.size(), cudaMemcpyHostToDevice );
+		cudaMemcpy( dwo, wo, 12 * n, cudaMemcpyHostToDevice );
+		cudaMemcpy( dwi, wi, 12 * n, cudaMemcpyHostToDevice );
+		if ( k ) cudaMemcpy( du, u, 4 * size_t( k ) * n, cudaMemcpyHostToDevice );
+		launch_shader_execute( dtab, target == CR_SHADE_EVAL ? 0 : 1, dwo, dwi, du, k, n, df, de, dused, nullptr );
+		cudaMemcpy( wi, dwi, 12 * n, cudaMemcpyDeviceToHost );
+		cudaMemcpy( f, df, 12 * n, cudaMemcpyDeviceToHost );
+		cudaMemcpy( emission, de, 12 * n, cudaMemcpyDeviceToHost );
+		cudaError_t e = cudaMemcpy( used, dused, 4 * n, cudaMemcpyDeviceToHost );
+		cudaFree( d );
+		cuda_check( e, "shader execute" );
 	} );
 }
 

@@ -25,8 +25,32 @@ enum ShaderType : int32_t
 {
 	SH_LAMBERT = 0,
 	SH_GLOSSY = 1,
-	SH_EMISSION = 2
+	SH_EMISSION = 2,
+	SH_TRANSPARENT = 3,  // transparent.hpp
+	SH_BLACKHOLE = 4,    // blackhole.hpp
+	SH_REFRACTION = 5,   // refraction.hpp ("RefractionBSDF")
+	SH_GLASS = 6,        // glass.hpp ("GlassBSDF")
+	SH_MIXED = 7         // mixed.hpp
 };
+
+// SphericalDistribution of a GlossyBSDF, RefractionBSDF or GlassBSDF
+// (src/ext/distribution/distribution.impl.cu).
+enum DistKind : int32_t
+{
+	DIST_BECKMANN = 0,
+	DIST_COSINE = 1
+};
+
+// Scala<float> of a Mixed shader's "fac" (src/ext/scala/scala.impl.cu).
+enum FacKind : int32_t
+{
+	FAC_CONSTANT = 0,
+	FAC_FRESNEL = 1
+};
+
+// Deepest chain of Mixed shaders a shader table may hold (the device walks
+// it with a bounded loop).
+constexpr int MAX_SHADER_DEPTH = 16;
 
 enum Estimator : int32_t
 {
@@ -54,13 +78,20 @@ struct alignas( 16 ) WNode
 };
 static_assert( sizeof( WNode ) == 80, "WNode must be 80 bytes" );
 
+// One node of a scene's shader table.  Named shaders come first (their index
+// is the shader id primitives carry); the shaders nested in a Mixed follow.
 struct DevShader
 {
 	int32_t type;
 	float albedo[ 3 ];    // Lambert: color * R; Emission: 1
-	float color[ 3 ];     // Glossy tint
+	float color[ 3 ];     // Glossy, Transparent, Refraction, Glass tint
 	float alpha, alpha2;  // Beckmann roughness and its square
 	float emission[ 3 ];  // Emission: color * strength
+	float ior;            // Refraction, Glass; Mixed with a Fresnel fac
+	float fac;            // Mixed with a Constant fac: its value
+	int32_t fac_kind;     // Mixed: FacKind
+	int32_t dist;         // Glossy, Refraction, Glass: DistKind
+	int32_t child[ 2 ];   // Mixed: table indices of shaders[0] and shaders[1]
 };
 
 struct DevSphere
@@ -76,7 +107,8 @@ struct DevSphere
 enum LightKind : int32_t
 {
 	LIGHT_MESH = 0,
-	LIGHT_SPHERE = 1
+	LIGHT_SPHERE = 1,
+	LIGHT_POINT = 2  // pointLight asset (src/core/light/pointLight.hpp)
 };
 
 struct DevLight
@@ -89,6 +121,7 @@ struct DevLight
 	float koishi_pdf;     // area pdf of the reference's table (incl. padding copies)
 	float area;           // true area (MIS)
 	int32_t cdf;          // offset of the area CDF in light_cdf
+	float pos[ 3 ];       // point lights: position
 };
 
 struct DevCamera

@@ -231,26 +231,182 @@ __device__ __forceinline__ float3 beckmann_sample( float alpha2, float u1, float
 
 __device__ __forceinline__ float3 reflect( float3 I, float3 N ) { return N * ( dot( N, I ) * 2.f ) - I; }
 
-// Koishi estimator, compute_f_by_wi_wo: Lambert (lambert.hpp:31-33),
-// GlossyBSDF (glossy.hpp:27-29), Emission = white Lambert (emission.hpp:22-27).
-__device__ __forceinline__ float3 koishi_eval( const DevShader &sh, float3 wo, float3 wi )
+// Uniform stream of one path vertex, served in the order the reference's
+// Sampler serves RadianceKernel::execute (radiance.cu:29-68) and the shaders
+// it runs: Philox blocks (sample, bounce, 0), (sample, bounce, 1), ... drawn
+// four at a time as they are consumed.
+struct VertexRng
 {
-	if ( sh.type == SH_GLOSSY ) return f3( sh.color ) * beckmann_f( sh.alpha2, normalize( wo + wi ) );
-	return wi.z >= 0.f ? f3( sh.albedo ) * ( 1.0f / PI_F ) : f3( 0.f, 0.f, 0.f );
+	uint2 key;
+	uint64_t g;
+	uint32_t bounce, blk;
+	float4 b;
+	int i;
+	__device__ __forceinline__ VertexRng( uint2 k, uint64_t s, uint32_t bn ) : key( k ), g( s ), bounce( bn ), blk( 0 ), i( 4 ) {}
+	__device__ __forceinline__ float next()
+	{
+		if ( i == 4 ) b = rand4( key, g, bounce, blk++ ), i = 0;
+		const float v = i == 0 ? b.x : i == 1 ? b.y : i == 2 ? b.z : b.w;
+		++i;
+		return v;
+	}
+};
+
+// Uniforms read from an array (n per sample) in the order they are drawn;
+// draws past the end read 0.5 and are still counted.
+struct ArrayRng
+{
+	const float *u;
+	uint32_t n, used;
+	__device__ __forceinline__ float next()
+	{
+		const float v = used < n ? u[ used ] : 0.5f;
+		++used;
+		return v;
+	}
+};
+
+// SphericalDistribution::f of a shader's distribution: Beckmann D(h)|cos|
+// (beckmann.hpp:19-24) or the cosine lobe (cosine.hpp:14-17).
+__device__ __forceinline__ float dist_f( const DevShader &sh, float3 w )
+{
+	if ( sh.dist == DIST_COSINE ) return w.z >= 0.f ? 1.0f / PI_F : 0.f;
+	return beckmann_f( sh.alpha2, w );
 }
 
-// Koishi estimator, sample_wi_f_by_wo (lambert.hpp:26-30 with cosine.hpp:16-25,
-// glossy.hpp:22-26).  Returns f; the caller multiplies by |cos|.
-__device__ __forceinline__ float3 koishi_sample( const DevShader &sh, float3 wo, float u1, float u2, float3 &wi )
+// distribution->sample( sampler.sample3() ): three draws, the first two used
+// (beckmann.hpp:26-38, cosine.hpp:18-23).
+template <class Rng>
+__device__ __forceinline__ float3 dist_sample( const DevShader &sh, Rng &rng )
 {
-	if ( sh.type == SH_GLOSSY )
+	const float u1 = rng.next(), u2 = rng.next();
+	rng.next();
+	return sh.dist == DIST_COSINE ? sample_cos( u1, u2 ) : beckmann_sample( sh.alpha2, u1, u2 );
+}
+
+// The Fresnel scala (src/ext/scala/fresnel.hpp:17-31): unpolarised dielectric
+// reflectance for the outgoing direction, 1 past the critical angle.
+__device__ __forceinline__ float fresnel_fac( float ior, float3 wo )
+{
+	const float eta = wo.z > 0.f ? 1.f / ior : ior;
+	const float ci = fabsf( wo.z );
+	const float st = eta * sqrtf( fmaxf( 0.f, 1.f - ci * ci ) );
+	if ( st >= 1.f ) return 1.f;
+	const float q = ci / sqrtf( fmaxf( 0.f, 1.f - st * st ) );
+	const float a = ( q - eta ) / ( q + eta ), b = ( eta * q - 1.f ) / ( eta * q + 1.f );
+	return .5f * ( a * a + b * b );
+}
+
+// refract (src/vec/vmath.hpp:517-526): I refracted about N with relative
+// index eta; false (R untouched) past the critical angle.
+__device__ __forceinline__ bool refract_dir( float3 I, float3 N, float eta, float3 &R )
+{
+	const float c = dot( N, I );
+	const float s2 = fmaxf( 0.f, 1.f - c * c ) * eta * eta;
+	if ( s2 >= 1.f ) return false;
+	R = normalize( -I * eta + N * ( eta * c - sqrtf( 1.f - s2 ) ) );
+	return true;
+}
+
+// Walks the Mixed shaders from table entry idx to the leaf that executes:
+// each Mixed draws one number and runs shaders[1] below its fac, else
+// shaders[0] (mixed.hpp:24-29).  The host bounds the depth.
+template <class Rng>
+__device__ __forceinline__ int koishi_leaf( const DevShader *tab, int idx, float3 wo, Rng &rng )
+{
+	for ( int d = 0; d < MAX_SHADER_DEPTH && tab[ idx ].type == SH_MIXED; ++d )
 	{
-		float3 h = beckmann_sample( sh.alpha2, u1, u2 );
-		wi = reflect( wo, h );
-		return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
+		const DevShader &m = tab[ idx ];
+		const float f = m.fac_kind == FAC_FRESNEL ? fresnel_fac( m.ior, wo ) : m.fac;
+		idx = m.child[ rng.next() < f ? 1 : 0 ];
 	}
-	wi = sample_cos( u1, u2 );
-	return wi.z >= 0.f ? f3( sh.albedo ) : f3( 0.f, 0.f, 0.f );
+	return idx;
+}
+
+// Koishi estimator, compute_f_by_wi_wo of table entry idx: Lambert
+// (lambert.hpp:31-33), GlossyBSDF (glossy.hpp:27-29), Emission as white
+// Lambert that also sets the varyings' emission (emission.hpp:22-27),
+// GlassBSDF (glass.hpp:25-53: a Fresnel draw picks the reflection or the
+// transmission half-vector), and zero for Transparent (transparent.hpp:24-26),
+// Blackhole (blackhole.hpp:17-20) and RefractionBSDF (refraction.hpp:35-38).
+template <class Rng>
+__device__ __forceinline__ float3 koishi_eval( const DevShader *tab, int idx, float3 wo, float3 wi, Rng &rng,
+											   float3 &emission )
+{
+	const DevShader &sh = tab[ koishi_leaf( tab, idx, wo, rng ) ];
+	emission = f3( 0.f, 0.f, 0.f );
+	switch ( sh.type )
+	{
+	case SH_EMISSION:
+		emission = f3( sh.emission );
+		// fall through: Emission shades as white Lambert
+	case SH_LAMBERT:
+		return wi.z >= 0.f ? f3( sh.albedo ) * ( 1.0f / PI_F ) : f3( 0.f, 0.f, 0.f );
+	case SH_GLOSSY:
+		return f3( sh.color ) * dist_f( sh, normalize( wo + wi ) );
+	case SH_GLASS:
+		if ( rng.next() < fresnel_fac( sh.ior, wo ) ) return f3( sh.color ) * dist_f( sh, normalize( wo + wi ) );
+		return f3( sh.color ) * dist_f( sh, normalize( wo + wi * sh.ior ) );
+	default:
+		return f3( 0.f, 0.f, 0.f );
+	}
+}
+
+// The transmission half of RefractionBSDF and GlassBSDF (refraction.hpp:24-33,
+// glass.hpp:40-49): a half-vector from the distribution, flipped to wo's side,
+// refracts wo; f = color scaled by 1/eta^2 when entering.  wi is left as it
+// was when the refraction fails (f = 0).
+template <class Rng>
+__device__ __forceinline__ float3 koishi_refract( const DevShader &sh, float3 wo, Rng &rng, float3 &wi )
+{
+	float3 h = dist_sample( sh, rng );
+	const float eta = wo.z > 0.f ? 1.f / sh.ior : sh.ior;
+	if ( wo.z < 0.f ) h = -h;
+	if ( !refract_dir( wo, h, eta, wi ) ) return f3( 0.f, 0.f, 0.f );
+	return f3( sh.color ) / ( eta < 1.f ? eta * eta : 1.f );
+}
+
+// Koishi estimator, sample_wi_f_by_wo of table entry idx: Lambert
+// (lambert.hpp:26-30 with cosine.hpp:18-23: f = color * R), GlossyBSDF
+// (glossy.hpp:22-26), Transparent (wi = -wo, f = color), Blackhole
+// (wi = +z, f = 0), RefractionBSDF and GlassBSDF (glass.hpp:25-49).  Returns
+// f; the caller multiplies by |cos|.  wi is in/out (see koishi_refract);
+// emission is what the leaf writes to the varyings (Emission only).
+template <class Rng>
+__device__ __forceinline__ float3 koishi_sample( const DevShader *tab, int idx, float3 wo, Rng &rng, float3 &wi,
+												 float3 &emission )
+{
+	const DevShader &sh = tab[ koishi_leaf( tab, idx, wo, rng ) ];
+	emission = sh.type == SH_EMISSION ? f3( sh.emission ) : f3( 0.f, 0.f, 0.f );
+	switch ( sh.type )
+	{
+	case SH_LAMBERT:
+	case SH_EMISSION:
+	{
+		const float u1 = rng.next(), u2 = rng.next();
+		rng.next();
+		wi = sample_cos( u1, u2 );
+		return wi.z >= 0.f ? f3( sh.albedo ) : f3( 0.f, 0.f, 0.f );
+	}
+	case SH_GLOSSY:
+		wi = reflect( wo, dist_sample( sh, rng ) );
+		return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
+	case SH_TRANSPARENT:
+		wi = -wo;
+		return f3( sh.color );
+	case SH_REFRACTION:
+		return koishi_refract( sh, wo, rng, wi );
+	case SH_GLASS:
+		if ( rng.next() < fresnel_fac( sh.ior, wo ) )
+		{
+			wi = reflect( wo, dist_sample( sh, rng ) );
+			return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
+		}
+		return koishi_refract( sh, wo, rng, wi );
+	default:  // Blackhole
+		wi = f3( 0.f, 0.f, 1.f );
+		return f3( 0.f, 0.f, 0.f );
+	}
 }
 
 // MIS estimator BSDFs: Lambert albedo/pi with cosine pdf; Beckmann microfacet

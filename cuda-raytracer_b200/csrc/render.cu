@@ -274,37 +274,58 @@ struct PathOut
 	float4 ro, rd, so, sd, sc;
 };
 
-// One vertex of RadianceKernel::execute (radiance.cu:22-71), reference semantics.
+// Light::sample of the reference estimator for a point p: the light point lp
+// and the unoccluded radiance li it delivers.  Area lights
+// (areaLight.hpp:19-31, Primitive::sample primitive.hpp:25-33) divide the
+// emission by the solid-angle pdf; a point light (pointLight.hpp:21-29)
+// delivers its emission as it is.
+__device__ __forceinline__ void koishi_light_sample( const DevScene &sc, const DevLight &lt, float3 p, float ux, float uy,
+													 float3 &lp, float3 &li )
+{
+	if ( lt.kind == LIGHT_POINT )
+	{
+		lp = f3( lt.pos );
+		li = f3( lt.emission );
+		return;
+	}
+	float3 ln;
+	float pdf;
+	koishi_light_point( sc, lt, ux, uy, lp, ln, pdf );
+	const float3 wiw = p - lp;
+	pdf *= dot( wiw, wiw ) / fabsf( dot( ln, normalize( wiw ) ) );
+	li = f3( lt.emission ) / pdf;
+}
+
+// One vertex of RadianceKernel::execute (radiance.cu:22-71), reference
+// semantics, with the vertex's uniforms drawn in the reference's order.
 __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
 											  uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
 											  float4 &L4, PathOut &out )
 {
 	float3 o = f3( ro ), d = f3( rd );
 	Surface s = surface_at( sc, o, d, h, false );
-	const DevShader sh = sc.shaders[ s.shader ];
 	Frame fr = koishi_frame( s.ns );
 	float3 wo = fr.local( -d );
 	float3 beta = f3( beta4 ), L = f3( L4 );
-	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
+	VertexRng rng( key, g, bounce );
+	float3 wi = f3( 0.f, 0.f, 0.f );
 	if ( sc.n_lights )
 	{
 		uint32_t nl = sc.n_lights;
-		uint32_t idx = min( uint32_t( floorf( r0.x * float( nl ) ) ), nl - 1 );
+		uint32_t idx = min( uint32_t( floorf( rng.next() * float( nl ) ) ), nl - 1 );
 		float lpdf = 1.f / float( nl );
 		const DevLight lt = sc.lights[ idx ];
-		float3 lp, ln;
-		float pdf;
-		koishi_light_point( sc, lt, r0.y, r0.z, lp, ln, pdf );
-		float3 wiw = s.p - lp;  // Primitive::sample(p,u,pdf) (primitive.hpp:25-33)
-		pdf *= dot( wiw, wiw ) / fabsf( dot( ln, normalize( wiw ) ) );
+		const float ux = rng.next(), uy = rng.next();
+		float3 lp, li;
+		koishi_light_sample( sc, lt, s.p, ux, uy, lp, li );
 		float3 dd = lp - s.p;   // LocalVaryings::emitSeg (varyings.hpp:27-37)
 		float3 sd = normalize( dd );
 		float3 diff = normalize( sd ) * KOISHI_EPS;
 		float3 so = s.p + diff;
 		float st = length( dd - 2.f * diff );
-		float3 wi = fr.local( normalize( lp - s.p ) );
-		float3 f = koishi_eval( sh, wo, wi );
-		float3 li = f3( lt.emission ) / pdf;
+		wi = fr.local( normalize( lp - s.p ) );
+		float3 emission;
+		float3 f = koishi_eval( sc.shaders, s.shader, wo, wi, rng, emission );
 		float3 c = beta * f * li * ( fabsf( wi.z ) / lpdf );
 		if ( !finite3( c ) )
 			L = f3( NAN, NAN, NAN );
@@ -315,10 +336,10 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 			out.sd = make_float4( sd.x, sd.y, sd.z, st );
 			out.sc = make_float4( c.x, c.y, c.z, 0.f );
 		}
-		if ( sh.type == SH_EMISSION ) L = L + beta * f3( sh.emission );  // radiance.cu:39
+		L = L + beta * emission;  // radiance.cu:39
 	}
-	float3 wi;
-	float3 f = koishi_sample( sh, wo, r1.x, r1.y, wi );  // radiance.cu:55-60
+	float3 emission_s;
+	float3 f = koishi_sample( sc.shaders, s.shader, wo, rng, wi, emission_s );  // radiance.cu:55-60
 	beta = beta * f * fabsf( wi.z );
 	float3 nd = fr.global( wi );
 	float3 no = s.p + nd * KOISHI_EPS;
@@ -327,7 +348,7 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 	if ( rr < 1.f && bounce > 3 )
 	{
 		float q = fmaxf( .05f, 1.f - rr );
-		if ( r0.w < q )
+		if ( rng.next() < q )
 			alive = false;
 		else
 			beta = beta / ( 1.f - q );
@@ -758,11 +779,8 @@ __global__ void __launch_bounds__( 128 ) k_aov( DevScene sc, RenderConfig cfg, W
 						( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
 					const float4 r0 = rand4( key, g, 0, 0 );
 					const DevLight lt = sc.lights[ 0 ];
-					float3 lp, ln;
-					float pdf;
-					koishi_light_point( sc, lt, r0.x, r0.y, lp, ln, pdf );
-					float3 wiw = s.p - lp;
-					pdf *= dot( wiw, wiw ) / fabsf( dot( ln, normalize( wiw ) ) );
+					float3 lp, li;
+					koishi_light_sample( sc, lt, s.p, r0.x, r0.y, lp, li );
 					if ( cfg.kernel == KERNEL_HALFVECTOR )
 					{
 						const Frame fr = koishi_frame( s.ns );
@@ -772,7 +790,6 @@ __global__ void __launch_bounds__( 128 ) k_aov( DevScene sc, RenderConfig cfg, W
 					}
 					else
 					{
-						const float3 li = f3( lt.emission ) / pdf;
 						if ( !( li.x == 0.f && li.y == 0.f && li.z == 0.f ) )
 						{
 							const float3 dd = lp - s.p;
@@ -831,16 +848,22 @@ __global__ void k_tally( const uint32_t *counters, uint32_t max_bounce, unsigned
 	tally[ 0 ] += e, tally[ 1 ] += sh;
 }
 
+// Single-node shader kernels behind cr_bsdf_eval / cr_bsdf_sample (the host
+// refuses shaders that draw selection numbers there).
 __global__ void k_bsdf_eval( int est, DevShader sh, const float *wo, const float *wi, uint64_t n, float *f, float *pdf )
 {
+	const DevShader tab[ 1 ] = { sh };
 	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
 	{
-		float3 o = f3( wo + 3 * i ), w = f3( wi + 3 * i ), r;
+		float3 o = f3( wo + 3 * i ), w = f3( wi + 3 * i ), r, e;
 		float p = 0.f;
 		if ( est == EST_MIS )
 			r = mis_eval( sh, o, w, p );
 		else
-			r = koishi_eval( sh, o, w );
+		{
+			ArrayRng rng{ nullptr, 0, 0 };
+			r = koishi_eval( tab, 0, o, w, rng, e );
+		}
 		f[ 3 * i ] = r.x, f[ 3 * i + 1 ] = r.y, f[ 3 * i + 2 ] = r.z;
 		pdf[ i ] = p;
 	}
@@ -849,20 +872,42 @@ __global__ void k_bsdf_eval( int est, DevShader sh, const float *wo, const float
 __global__ void k_bsdf_sample( int est, DevShader sh, const float *wo, const float *u, uint64_t n, float *wi, float *wt,
 							   float *pdf )
 {
+	const DevShader tab[ 1 ] = { sh };
 	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
 	{
-		float3 o = f3( wo + 3 * i ), w, r;
+		float3 o = f3( wo + 3 * i ), w = f3( 0.f, 0.f, 0.f ), r, e;
 		float p = 0.f;
 		if ( est == EST_MIS )
 			r = mis_sample( sh, o, u[ 2 * i ], u[ 2 * i + 1 ], w, p );
 		else
 		{
-			r = koishi_sample( sh, o, u[ 2 * i ], u[ 2 * i + 1 ], w );
+			ArrayRng rng{ u + 2 * i, 2, 0 };
+			r = koishi_sample( tab, 0, o, rng, w, e );
 			r = r * fabsf( w.z );
 		}
 		wi[ 3 * i ] = w.x, wi[ 3 * i + 1 ] = w.y, wi[ 3 * i + 2 ] = w.z;
 		wt[ 3 * i ] = r.x, wt[ 3 * i + 1 ] = r.y, wt[ 3 * i + 2 ] = r.z;
 		pdf[ i ] = p;
+	}
+}
+
+// Shader::execute of table entry 0 (nested Mixed entries follow it) over n
+// samples with scripted uniforms, k per sample (cr_shader_execute).
+__global__ void k_shader_execute( const DevShader *tab, int target, const float *wo, float *wi, const float *u,
+								  uint32_t k, uint64_t n, float *f, float *em, uint32_t *used )
+{
+	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
+	{
+		float3 o = f3( wo + 3 * i ), w = f3( wi + 3 * i ), r, e;
+		ArrayRng rng{ u + uint64_t( k ) * i, k, 0 };
+		if ( target == 0 )
+			r = koishi_eval( tab, 0, o, w, rng, e );
+		else
+			r = koishi_sample( tab, 0, o, rng, w, e );
+		wi[ 3 * i ] = w.x, wi[ 3 * i + 1 ] = w.y, wi[ 3 * i + 2 ] = w.z;
+		f[ 3 * i ] = r.x, f[ 3 * i + 1 ] = r.y, f[ 3 * i + 2 ] = r.z;
+		em[ 3 * i ] = e.x, em[ 3 * i + 1 ] = e.y, em[ 3 * i + 2 ] = e.z;
+		used[ i ] = rng.used;
 	}
 }
 
@@ -1268,6 +1313,15 @@ void launch_bsdf_sample( int est, const DevShader &sh, const float *wo, const fl
 	int g = int( std::min<uint64_t>( ( n + 255 ) / 256, 4096 ) );
 	k_bsdf_sample<<<g, 256, 0, st>>>( est, sh, wo, u, n, wi, wt, pdf );
 	check( cudaGetLastError(), "bsdf launch" );
+}
+
+void launch_shader_execute( const DevShader *tab, int target, const float *wo, float *wi, const float *u, uint32_t k,
+							uint64_t n, float *f, float *emission, uint32_t *used, cudaStream_t st )
+{
+	if ( !n ) return;
+	int g = int( std::min<uint64_t>( ( n + 255 ) / 256, 4096 ) );
+	k_shader_execute<<<g, 256, 0, st>>>( tab, target, wo, wi, u, k, n, f, emission, used );
+	check( cudaGetLastError(), "shader launch" );
 }
 
 }  // namespace cr

@@ -121,6 +121,10 @@ void launch_bsdf_eval( int estimator, const DevShader &sh, const float *wo, cons
 					   float *pdf, cudaStream_t st );
 void launch_bsdf_sample( int estimator, const DevShader &sh, const float *wo, const float *u, uint64_t n, float *wi,
 						 float *weight, float *pdf, cudaStream_t st );
+// Shader::execute of tab[0] (target 0 compute_f_by_wi_wo, 1 sample_wi_f_by_wo),
+// k scripted uniforms per sample; device arrays.
+void launch_shader_execute( const DevShader *tab, int target, const float *wo, float *wi, const float *u, uint32_t k,
+							uint64_t n, float *f, float *emission, uint32_t *used, cudaStream_t st );
 
 int sm_count();
 }  // namespace cr

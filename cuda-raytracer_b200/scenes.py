@@ -50,6 +50,7 @@ class SceneDesc:
     groups: list = field(default_factory=list)
     spheres: list = field(default_factory=list)     # dicts {o, r, shader}
     shaders: dict = field(default_factory=dict)     # name -> [Type, props]
+    point_lights: list = field(default_factory=list)  # dicts {position, color, strength}
     camera: dict = field(default_factory=dict)
     width: int = 256
     height: int = 256
@@ -276,6 +277,32 @@ def config0(width=256, height=256, spp=64) -> SceneDesc:
     ]
     return SceneDesc(groups=box_groups(), spheres=spheres, shaders=sh, camera=box_camera(),
                      width=width, height=height, spp=spp, max_bounce=7, name="config0")
+
+
+def config_materials(width=256, height=256, spp=64) -> SceneDesc:
+    """The box with the reference's remaining shaders and a point light:
+    GlassBSDF, RefractionBSDF, Transparent, Blackhole, Mixed over a Fresnel
+    and over a Constant fac (one with a Cosine GlossyBSDF), lit by the ceiling
+    panel and by a pointLight (the first light in the list)."""
+    sh = box_shaders(50.0)
+    beck = lambda a: ["Beckmann", {"roughness": a}]
+    sh["glass"] = ["GlassBSDF", {"ior": 1.5, "distribution": beck(0.2), "color": [0.95, 0.97, 1.0]}]
+    sh["coat"] = ["Mixed", {"fac": ["Fresnel", {"ior": 1.5}],
+                            "shaders": [["Lambert", {"R": [0.6, 0.3, 0.2], "color": [1, 1, 1]}],
+                                        ["GlossyBSDF", {"distribution": beck(0.15), "color": [1, 1, 1]}]]}]
+    sh["water"] = ["RefractionBSDF", {"ior": 1.33, "distribution": beck(0.25), "color": [0.9, 0.95, 1.0]}]
+    sh["veil"] = ["Transparent", {"color": [0.85, 0.9, 0.7]}]
+    sh["hole"] = ["Blackhole", {}]
+    sh["blend"] = ["Mixed", {"fac": ["Constant", {"value": 0.35}],
+                             "shaders": [["Lambert", {"R": [0.2, 0.5, 0.7], "color": [1, 1, 1]}],
+                                         ["GlossyBSDF", {"distribution": ["Cosine", {}], "color": [0.8, 0.8, 0.6]}]]}]
+    place = [("glass", [1.6, 1.6, 1.0], 1.0), ("coat", [3.9, 3.6, 1.0], 1.0), ("water", [3.8, 1.0, 0.6], 0.6),
+             ("veil", [1.4, 3.9, 0.8], 0.8), ("hole", [2.8, 4.7, 2.8], 0.4), ("blend", [2.6, 2.6, 0.45], 0.45)]
+    spheres = [{"o": [float(x) for x in _rot_points(c)], "r": r, "shader": n} for n, c, r in place]
+    lights = [{"position": [float(x) for x in _rot_points([2.0, 2.0, 4.2])], "color": [1.0, 0.9, 0.8],
+               "strength": 1.5}]
+    return SceneDesc(groups=box_groups(), spheres=spheres, shaders=sh, camera=box_camera(), point_lights=lights,
+                     width=width, height=height, spp=spp, max_bounce=7, name="materials")
 
 
 def config1(level=8, seed=1, width=1024, height=768, spp=256) -> SceneDesc:
@@ -625,6 +652,8 @@ def scene_json(desc: SceneDesc, mesh_path: str, tracer="CudaWavefront", estimato
         assets.append(["import", {"path": mesh_path}])
     for s in desc.spheres:
         assets.append(["sphere", {"o": s["o"], "r": s["r"], "shader": s["shader"]}])
+    for pl in desc.point_lights:
+        assets.append(["pointLight", dict(pl)])
     return {
         "scene": {"camera": [desc.camera], "assets": assets, "shaders": desc.shaders},
         "tracer": [tracer, {"kernel": ["Radiance", kern]}],

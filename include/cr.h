@@ -104,8 +104,8 @@ const char *cr_version(void);
  * with the Renderer's configuration read (src/core/renderer/renderer.cu:13-24,
  * renderer.hpp:17-23): parses the reference JSON schema, loads the
  * ["import", {"path"}] mesh file (OBJ, or the CRM binary mesh format,
- * resolved against base_dir), spheres, shaders and cameras, and makes every
- * Emission-shaded primitive an area light.  The scene is committed
+ * resolved against base_dir), spheres, pointLight assets, shaders and
+ * cameras, and makes every Emission-shaded primitive an area light.  The scene is committed
  * (uploaded, BVH built) before return. */
 int cr_scene_create(const char *json_text, const char *base_dir, cr_scene **out);
 
@@ -114,9 +114,13 @@ int cr_scene_create(const char *json_text, const char *base_dir, cr_scene **out)
 int cr_scene_create_empty(cr_scene **out);
 
 /* Factory<Shader>::create (src/core/basic/factory.hpp:15-23) over the shader
- * registry of src/ext/shader/shader.impl.cu:15-24 (Lambert, GlossyBSDF with
- * a Beckmann distribution, Emission).  config_json is the reference's
- * [Type, {props}] array.  Returns the shader id (>= 0) or an error code. */
+ * registry of src/ext/shader/shader.impl.cu:15-24: Lambert, GlossyBSDF
+ * (Beckmann or Cosine distribution), Emission, Transparent, Blackhole,
+ * RefractionBSDF, GlassBSDF and Mixed (fac Constant or Fresnel, nested
+ * Mixed up to 16 deep).  config_json is the reference's [Type, {props}]
+ * array.  The MIS estimator renders Lambert, Beckmann GlossyBSDF and
+ * Emission only; the others have reference semantics (CR_ESTIMATOR_KOISHI).
+ * Returns the shader id (>= 0) or an error code. */
 int cr_scene_add_shader(cr_scene *s, const char *name, const char *config_json);
 
 /* PolyMesh(vertices, normals, indices) (src/core/primitive/mesh.cu:404-433):
@@ -127,6 +131,12 @@ int cr_scene_add_mesh(cr_scene *s, const float *vertices, uint32_t n_vertices, c
 
 /* The "sphere" asset (src/core/meta/scene.cu:136-156, sphere.hpp:9-16). */
 int cr_scene_add_sphere(cr_scene *s, const float *center, float radius, const char *shader);
+
+/* The "pointLight" asset (src/core/meta/scene.cu:156-163, pointLight.hpp:13-18):
+ * emission = color (null: white) * strength, delivered to a lit point without
+ * distance falloff.  Point lights precede the area lights in the light list.
+ * Reference estimator only.  Returns the point light's index. */
+int cr_scene_add_point_light(cr_scene *s, const float *position, const float *color, float strength);
 
 /* CameraConfig (src/util/config.hpp:12-35), pinhole lens; `target` is a
  * direction, fovx the horizontal field of view in degrees. */
@@ -369,6 +379,26 @@ int cr_bsdf_eval(int estimator, const char *shader_json, const float *wo, const 
  * u (n x 2): wi (n x 3), weight = f*|cos|/pdf (n x 3), pdf (n). */
 int cr_bsdf_sample(int estimator, const char *shader_json, const float *wo, const float *u, uint64_t n,
                    float *wi, float *weight, float *pdf);
+/* The two helpers above take single-node shaders without selection draws
+ * (not Mixed, not GlassBSDF); cr_shader_execute takes any shader. */
+
+/* Shader::execute(varyings, sampler, pool, target) (src/core/nodes/shader.hpp:17-23)
+ * with the reference estimator's shaders, nested Mixed included, for n
+ * samples in the local shading frame (z = normal), run by the CUDA path's
+ * device code:
+ *   CR_SHADE_EVAL   compute_f_by_wi_wo: f for (wo, wi)
+ *   CR_SHADE_SAMPLE sample_wi_f_by_wo:  wi and f for wo; wi is in/out and
+ *                   keeps its input where the shader leaves it unchanged
+ *                   (a refraction past the critical angle)
+ * u holds k uniforms per sample (k <= 64), handed out in the order the
+ * reference's Sampler would serve them (sample3 draws three); used[i] is how
+ * many sample i drew (draws past k read 0.5).  emission (n x 3) is what the
+ * executed shader writes to varyings.emission (non-zero for Emission only).
+ * Replaces direct calls of the poly::object<Shader> in scene.shaders. */
+#define CR_SHADE_EVAL 0
+#define CR_SHADE_SAMPLE 1
+int cr_shader_execute(const char *shader_json, int target, const float *wo, float *wi, const float *u, uint32_t k,
+                      uint64_t n, float *f, float *emission, uint32_t *used);
 
 #ifdef __cplusplus
 }

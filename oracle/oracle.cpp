@@ -63,6 +63,11 @@ struct Shader
 	V3 R{ 1, 1, 1 }, color{ 1, 1, 1 };
 	double alpha = 0.5;  // Beckmann roughness (alpha2 = roughness^2, beckmann.hpp:11-17)
 	V3 emission;         // color * strength (emission.hpp:12-20)
+	int dist = ORC_DIST_BECKMANN;       // Glossy, Refraction, Glass distribution
+	double ior = 1;                     // Refraction, Glass, Mixed with a Fresnel fac
+	int fac_kind = ORC_FAC_CONSTANT;    // Mixed
+	double fac = 0;                     // Mixed with a Constant fac
+	int child[ 2 ] = { -1, -1 };        // Mixed: shaders[0], shaders[1]
 };
 
 struct Tri
@@ -85,8 +90,9 @@ struct Prim
 
 struct Light
 {
-	int prim;
-	int kind;
+	int prim = -1;
+	int kind;  // 0 mesh, 1 sphere, 2 point (pointLight.hpp)
+	V3 pos, emission;  // point lights
 	// ORC_KOISHI mesh table (mesh.hpp:61-84)
 	std::vector<F3> tp, tn;
 	float kpdf = 0;
@@ -145,6 +151,7 @@ struct orc_scene
 	std::vector<int> bvh_tris;
 	std::vector<Node> nodes;
 	std::vector<Light> lights;
+	std::vector<Light> point_lights;  // pointLight assets, in asset order
 	Camera cam;
 	double scale = 1;
 };
@@ -448,29 +455,155 @@ V3 beckmann_sample( double alpha2, double u1, double u2 )
 
 inline V3 reflect( V3 I, V3 N ) { return N * ( dot( N, I ) * 2. ) - I; }  // vmath.hpp:470-489
 
-// ORC_KOISHI compute_f_by_wi_wo: Lambert (lambert.hpp:31-33), Glossy
-// (glossy.hpp:27-29), Emission as white Lambert (emission.hpp:22-27).
-V3 k_eval( const Shader &sh, V3 wo, V3 wi )
+// A Sampler as a shader sees it: one draw at a time, in order.
+struct Draws
 {
-	if ( sh.type == ORC_GLOSSY ) return sh.color * beckmann_f( sh.alpha * sh.alpha, normalize( wo + wi ) );
-	V3 c = sh.type == ORC_LAMBERT ? sh.color * sh.R : V3( 1, 1, 1 );
-	return wi.z >= 0 ? c * ( 1.0 / PI ) : V3();
+	virtual double next() = 0;
+};
+struct RngDraws : Draws
+{
+	Rng &r;
+	explicit RngDraws( Rng &x ) : r( x ) {}
+	double next() override { return r.next(); }
+};
+// Scripted draws; past the end 0.5, still counted.
+struct ArrayDraws : Draws
+{
+	const double *u;
+	int n, used = 0;
+	ArrayDraws( const double *a, int k ) : u( a ), n( k ) {}
+	double next() override
+	{
+		double v = used < n ? u[ used ] : 0.5;
+		++used;
+		return v;
+	}
+};
+
+// SphericalDistribution::f and ::sample( sampler.sample3() ): Beckmann
+// (beckmann.hpp:19-38) or the cosine lobe (cosine.hpp:14-23); sampling draws
+// three numbers and uses two.
+double dist_f( const Shader &sh, V3 w )
+{
+	if ( sh.dist == ORC_DIST_COSINE ) return w.z >= 0 ? 1.0 / PI : 0.0;
+	return beckmann_f( sh.alpha * sh.alpha, w );
+}
+V3 dist_sample( const Shader &sh, Draws &u )
+{
+	double u1 = u.next(), u2 = u.next();
+	u.next();
+	return sh.dist == ORC_DIST_COSINE ? sample_cos( u1, u2 ) : beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
 }
 
-// ORC_KOISHI sample_wi_f_by_wo: Lambert (lambert.hpp:26-30, cosine.hpp:16-25:
-// pdf reported as 1/pi so f = color*R), Glossy (glossy.hpp:22-26).
-void k_sample( const Shader &sh, V3 wo, double u1, double u2, V3 &wi, V3 &f )
+// Fresnel::compute (src/ext/scala/fresnel.hpp:17-31): dielectric reflectance
+// for wo, 1 past the critical angle.
+double fresnel( double ior, V3 wo )
 {
-	if ( sh.type == ORC_GLOSSY )
+	double e = wo.z > 0 ? 1 / ior : ior;
+	double ci = std::fabs( wo.z );
+	double sr = e * std::sqrt( std::max( 0., 1 - ci * ci ) );
+	if ( sr >= 1 ) return 1;
+	double cr = std::sqrt( std::max( 0., 1 - sr * sr ) );
+	double par = ( ci - e * cr ) / ( ci + e * cr ), perp = ( e * ci - cr ) / ( e * ci + cr );
+	return .5 * ( par * par + perp * perp );
+}
+
+// refract (src/vec/vmath.hpp:517-526).
+bool refract( V3 I, V3 N, double eta, V3 &R )
+{
+	double c = dot( N, I );
+	double s2 = std::max( 0., 1 - c * c ) * eta * eta;
+	if ( s2 >= 1 ) return false;
+	R = normalize( -I * eta + N * ( eta * c - std::sqrt( 1 - s2 ) ) );
+	return true;
+}
+
+// Mixed::execute (mixed.hpp:24-29): one draw per Mixed, shaders[1] below fac.
+int leaf( const std::vector<Shader> &tab, int idx, V3 wo, Draws &u )
+{
+	while ( tab[ idx ].type == ORC_MIXED )
 	{
-		V3 h = beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
-		wi = reflect( wo, h );
-		f = wo.z * wi.z > 0. ? sh.color : V3();
-		return;
+		const Shader &m = tab[ idx ];
+		double f = m.fac_kind == ORC_FAC_FRESNEL ? fresnel( m.ior, wo ) : m.fac;
+		idx = m.child[ u.next() < f ? 1 : 0 ];
 	}
-	wi = sample_cos( u1, u2 );
-	V3 c = sh.type == ORC_LAMBERT ? sh.color * sh.R : V3( 1, 1, 1 );
-	f = wi.z >= 0 ? c : V3();
+	return idx;
+}
+
+// ORC_KOISHI compute_f_by_wi_wo: Lambert (lambert.hpp:31-33), Glossy
+// (glossy.hpp:27-29), Emission as white Lambert that sets the emission
+// (emission.hpp:22-27), Glass (glass.hpp:25-53), zero for Transparent,
+// Blackhole and Refraction (transparent.hpp:24-26, blackhole.hpp:17-20,
+// refraction.hpp:35-38).
+V3 k_eval( const std::vector<Shader> &tab, int idx, V3 wo, V3 wi, Draws &u, V3 &emission )
+{
+	const Shader &sh = tab[ leaf( tab, idx, wo, u ) ];
+	emission = sh.type == ORC_EMISSION ? sh.emission : V3();
+	switch ( sh.type )
+	{
+	case ORC_LAMBERT:
+		return wi.z >= 0 ? sh.color * sh.R * ( 1.0 / PI ) : V3();
+	case ORC_EMISSION:
+		return wi.z >= 0 ? V3( 1, 1, 1 ) * ( 1.0 / PI ) : V3();
+	case ORC_GLOSSY:
+		return sh.color * dist_f( sh, normalize( wo + wi ) );
+	case ORC_GLASS:
+		if ( u.next() < fresnel( sh.ior, wo ) ) return sh.color * dist_f( sh, normalize( wo + wi ) );
+		return sh.color * dist_f( sh, normalize( wo + wi * sh.ior ) );
+	default:
+		return V3();
+	}
+}
+
+// Refraction through a sampled half-vector (refraction.hpp:24-33,
+// glass.hpp:40-49); wi unchanged and f = 0 past the critical angle.
+V3 k_refract( const Shader &sh, V3 wo, Draws &u, V3 &wi )
+{
+	V3 h = dist_sample( sh, u );
+	double e = wo.z > 0 ? 1 / sh.ior : sh.ior;
+	if ( wo.z < 0 ) h = -h;
+	if ( !refract( wo, h, e, wi ) ) return V3();
+	return sh.color / ( e < 1 ? e * e : 1 );
+}
+
+// ORC_KOISHI sample_wi_f_by_wo: Lambert (lambert.hpp:26-30, cosine.hpp:18-23:
+// pdf 1/pi so f = color*R), Glossy (glossy.hpp:22-26), Transparent
+// (transparent.hpp:20-23), Blackhole (blackhole.hpp:14-16), Refraction,
+// Glass (glass.hpp:25-49).  wi is in/out.
+V3 k_sample( const std::vector<Shader> &tab, int idx, V3 wo, Draws &u, V3 &wi, V3 &emission )
+{
+	const Shader &sh = tab[ leaf( tab, idx, wo, u ) ];
+	emission = sh.type == ORC_EMISSION ? sh.emission : V3();
+	switch ( sh.type )
+	{
+	case ORC_LAMBERT:
+	case ORC_EMISSION:
+	{
+		double u1 = u.next(), u2 = u.next();
+		u.next();
+		wi = sample_cos( u1, u2 );
+		V3 c = sh.type == ORC_LAMBERT ? sh.color * sh.R : V3( 1, 1, 1 );
+		return wi.z >= 0 ? c : V3();
+	}
+	case ORC_GLOSSY:
+		wi = reflect( wo, dist_sample( sh, u ) );
+		return wo.z * wi.z > 0. ? sh.color : V3();
+	case ORC_TRANSPARENT:
+		wi = -wo;
+		return sh.color;
+	case ORC_REFRACTION:
+		return k_refract( sh, wo, u, wi );
+	case ORC_GLASS:
+		if ( u.next() < fresnel( sh.ior, wo ) )
+		{
+			wi = reflect( wo, dist_sample( sh, u ) );
+			return wo.z * wi.z > 0. ? sh.color : V3();
+		}
+		return k_refract( sh, wo, u, wi );
+	default:
+		wi = V3( 0, 0, 1 );
+		return V3();
+	}
 }
 
 // ORC_MIS BSDFs: Lambert color*R/pi with cosine pdf; Beckmann microfacet
@@ -541,6 +674,41 @@ struct Frame
 	V3 global( V3 w ) const { return normalize( u * w.x + v * w.y + n * w.z ); }
 };
 
+// Light::sample for a point p of the reference estimator, before the
+// occlusion test: AreaLight::sample (areaLight.hpp:19-31) through the mesh
+// table (mesh.hpp:92-98) or Sphere::sample (sphere.hpp:22-30, theta uniform
+// in [0, pi]) with Primitive::sample's solid-angle pdf (primitive.hpp:25-33);
+// PointLight::sample (pointLight.hpp:21-29) delivers its emission unscaled.
+void koishi_light( const orc_scene *s, const Light &lt, V3 p, double ux, double uy, V3 &lpos, V3 &li )
+{
+	if ( lt.kind == 2 )
+	{
+		lpos = lt.pos, li = lt.emission;
+		return;
+	}
+	const Prim &lp = s->prims[ lt.prim ];
+	V3 lnrm;
+	double pdf;
+	if ( lt.kind == 0 )
+	{
+		size_t k = std::min( size_t( std::floor( ux * 1024 ) ), size_t( 1023 ) );
+		lpos = V3( lt.tp[ k ].x, lt.tp[ k ].y, lt.tp[ k ].z );
+		lnrm = V3( lt.tn[ k ].x, lt.tn[ k ].y, lt.tn[ k ].z );
+		pdf = lt.kpdf;
+	}
+	else
+	{
+		double th = ux * PI, ph = uy * PI * 2;
+		V3 w( std::sin( th ) * std::sin( ph ), std::sin( th ) * std::cos( ph ), std::cos( th ) );
+		lpos = lp.c + w * lp.r;
+		lnrm = w;
+		pdf = 1. / ( 4 * PI * lp.r * lp.r );
+	}
+	V3 wiw = p - lpos;
+	pdf *= dot( wiw, wiw ) / std::fabs( dot( lnrm, normalize( wiw ) ) );
+	li = s->shaders[ lp.shader ].emission / pdf;
+}
+
 // RadianceKernel::execute (src/core/kernel/radiance.cu:14-81), reference semantics.
 V3 radiance_koishi( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng )
 {
@@ -553,7 +721,6 @@ V3 radiance_koishi( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rn
 		if ( !intersect( s, o, d, INF, h ) ) break;
 		if ( bounce > max_bounce ) break;
 		const Prim &pr = s->prims[ h.prim ];
-		const Shader &sh = s->shaders[ pr.shader ];
 		V3 n;
 		if ( h.tri >= 0 )
 		{
@@ -568,52 +735,30 @@ V3 radiance_koishi( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rn
 		fr.v = normalize( cross( n, fr.u ) );
 		V3 p = o + d * h.t;
 		V3 wo = fr.local( -d );
-		V3 emission;
+		RngDraws u( rng );
+		V3 emission, wi;
 		if ( nl )
 		{
-			// radiance.cu:29-38, AreaLight::sample (areaLight.hpp:19-31),
-			// Primitive::sample(p,u,pdf) (primitive.hpp:25-33)
-			size_t idx = std::min( size_t( std::floor( rng.next() * double( nl ) ) ), nl - 1 );
+			// radiance.cu:29-38: light choice, Light::sample with sample2()
+			size_t idx = std::min( size_t( std::floor( u.next() * double( nl ) ) ), nl - 1 );
 			double lpdf = 1.0 / double( nl );
-			double ux = rng.next(), uy = rng.next();
-			const Light &lt = s->lights[ idx ];
-			const Prim &lp = s->prims[ lt.prim ];
-			V3 lpos, lnrm;
-			double pdf;
-			if ( lt.kind == 0 )
-			{
-				size_t k = std::min( size_t( std::floor( ux * 1024 ) ), size_t( 1023 ) );  // mesh.hpp:92-98
-				lpos = V3( lt.tp[ k ].x, lt.tp[ k ].y, lt.tp[ k ].z );
-				lnrm = V3( lt.tn[ k ].x, lt.tn[ k ].y, lt.tn[ k ].z );
-				pdf = lt.kpdf;
-			}
-			else
-			{
-				// Sphere::sample (sphere.hpp:22-30): theta uniform in [0, pi].
-				double th = ux * PI, ph = uy * PI * 2;
-				V3 w( std::sin( th ) * std::sin( ph ), std::sin( th ) * std::cos( ph ), std::cos( th ) );
-				lpos = lp.c + w * lp.r;
-				lnrm = w;
-				pdf = 1. / ( 4 * PI * lp.r * lp.r );
-			}
-			V3 wiw = p - lpos;
-			pdf *= dot( wiw, wiw ) / std::fabs( dot( lnrm, normalize( wiw ) ) );
+			double ux = u.next(), uy = u.next();
+			V3 lpos, li;
+			koishi_light( s, s->lights[ idx ], p, ux, uy, lpos, li );
 			V3 dd = lpos - p;  // LocalVaryings::emitSeg (varyings.hpp:27-37)
 			V3 sd = normalize( dd );
 			V3 diff = normalize( sd ) * eps;
 			V3 so = p + diff;
 			double st = length( dd - 2.0 * diff );
-			V3 li = occluded_seg( s, so, sd, st ) ? V3() : s->shaders[ lp.shader ].emission / pdf;
-			V3 wi = fr.local( normalize( lpos - p ) );
-			V3 f = k_eval( sh, wo, wi );
+			if ( occluded_seg( s, so, sd, st ) ) li = V3();
+			wi = fr.local( normalize( lpos - p ) );
+			V3 f = k_eval( s->shaders, pr.shader, wo, wi, u, emission );
 			L = L + beta * f * li * ( std::fabs( wi.z ) / lpdf );
-			if ( sh.type == ORC_EMISSION ) emission = sh.emission;
 		}
 		L = L + beta * emission;  // radiance.cu:39
 		// radiance.cu:55-60
-		double u1 = rng.next(), u2 = rng.next();
-		V3 wi, f;
-		k_sample( sh, wo, u1, u2, wi, f );
+		V3 es;
+		V3 f = k_sample( s->shaders, pr.shader, wo, u, wi, es );
 		beta = beta * f * std::fabs( wi.z );
 		d = fr.global( wi );
 		o = p + d * eps;
@@ -622,7 +767,7 @@ V3 radiance_koishi( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rn
 		if ( rr < 1. && bounce > 3 )
 		{
 			double q = std::max( .05, 1 - rr );
-			if ( rng.next() < q ) break;
+			if ( u.next() < q ) break;
 			beta = beta / ( 1 - q );
 		}
 		if ( beta.x == 0 && beta.y == 0 && beta.z == 0 ) break;
@@ -659,27 +804,8 @@ V3 aov_koishi( const orc_scene *s, V3 o, V3 d, int kind, Rng &rng )
 	V3 p = o + d * h.t;
 	V3 wo = fr.local( -d );
 	double ux = rng.next(), uy = rng.next();
-	const Light &lt = s->lights[ 0 ];
-	const Prim &lp = s->prims[ lt.prim ];
-	V3 lpos, lnrm;
-	double pdf;
-	if ( lt.kind == 0 )
-	{
-		size_t k = std::min( size_t( std::floor( ux * 1024 ) ), size_t( 1023 ) );
-		lpos = V3( lt.tp[ k ].x, lt.tp[ k ].y, lt.tp[ k ].z );
-		lnrm = V3( lt.tn[ k ].x, lt.tn[ k ].y, lt.tn[ k ].z );
-		pdf = lt.kpdf;
-	}
-	else
-	{
-		double th = ux * PI, ph = uy * PI * 2;
-		V3 w( std::sin( th ) * std::sin( ph ), std::sin( th ) * std::cos( ph ), std::cos( th ) );
-		lpos = lp.c + w * lp.r;
-		lnrm = w;
-		pdf = 1. / ( 4 * PI * lp.r * lp.r );
-	}
-	V3 wiw = p - lpos;
-	pdf *= dot( wiw, wiw ) / std::fabs( dot( lnrm, normalize( wiw ) ) );
+	V3 lpos, li;
+	koishi_light( s, s->lights[ 0 ], p, ux, uy, lpos, li );
 	if ( kind == ORC_AOV_HALFVECTOR )
 	{
 		V3 wi = fr.local( normalize( lpos - p ) );
@@ -692,7 +818,7 @@ V3 aov_koishi( const orc_scene *s, V3 o, V3 d, int kind, Rng &rng )
 	V3 diff = normalize( sd ) * eps;
 	V3 so = p + diff;
 	double st = length( dd - 2.0 * diff );
-	V3 li = occluded_seg( s, so, sd, st ) ? V3() : s->shaders[ lp.shader ].emission / pdf;
+	if ( occluded_seg( s, so, sd, st ) ) li = V3();
 	bool zero = li.x == 0 && li.y == 0 && li.z == 0;
 	return zero ? V3() : V3( 1, 1, 1 );
 }
@@ -946,18 +1072,71 @@ int orc_add_shader( orc_scene *s, int type, const double *p )
 {
 	Shader sh;
 	sh.type = type;
-	if ( type == ORC_LAMBERT )
+	switch ( type )
+	{
+	case ORC_LAMBERT:
 		sh.R = V3( p[ 0 ], p[ 1 ], p[ 2 ] ), sh.color = V3( p[ 3 ], p[ 4 ], p[ 5 ] );
-	else if ( type == ORC_GLOSSY )
-		sh.color = V3( p[ 0 ], p[ 1 ], p[ 2 ] ), sh.alpha = p[ 3 ];
-	else
+		break;
+	case ORC_GLOSSY:
+		sh.color = V3( p[ 0 ], p[ 1 ], p[ 2 ] ), sh.alpha = p[ 3 ], sh.dist = int( p[ 4 ] );
+		break;
+	case ORC_EMISSION:
 	{
 		// Emission stores color * strength computed in float (emission.hpp:12-20).
 		float c[ 3 ] = { float( p[ 0 ] ), float( p[ 1 ] ), float( p[ 2 ] ) }, st = float( p[ 3 ] );
 		sh.emission = V3( c[ 0 ] * st, c[ 1 ] * st, c[ 2 ] * st );
+		break;
+	}
+	case ORC_TRANSPARENT:
+		sh.color = V3( p[ 0 ], p[ 1 ], p[ 2 ] );
+		break;
+	case ORC_BLACKHOLE:
+		break;
+	case ORC_REFRACTION:
+	case ORC_GLASS:
+		sh.color = V3( p[ 0 ], p[ 1 ], p[ 2 ] ), sh.ior = float( p[ 3 ] ), sh.alpha = p[ 4 ], sh.dist = int( p[ 5 ] );
+		break;
+	case ORC_MIXED:
+		sh.fac_kind = int( p[ 0 ] );
+		if ( sh.fac_kind == ORC_FAC_FRESNEL )
+			sh.ior = float( p[ 1 ] );
+		else
+			sh.fac = float( p[ 1 ] );
+		sh.child[ 0 ] = int( p[ 2 ] ), sh.child[ 1 ] = int( p[ 3 ] );
+		for ( int k = 0; k < 2; ++k )  // children first: the table stays acyclic
+			if ( sh.child[ k ] < 0 || sh.child[ k ] >= int( s->shaders.size() ) ) return -1;
+		break;
+	default:
+		return -1;
 	}
 	s->shaders.push_back( sh );
 	return int( s->shaders.size() - 1 );
+}
+
+int orc_add_point_light( orc_scene *s, const float *pos, const double *color, double strength )
+{
+	// PointLight (pointLight.hpp:13-18): emission = color * strength in float
+	Light lt;
+	lt.kind = 2;
+	lt.pos = fv( pos );
+	float st = float( strength );
+	lt.emission = V3( float( color[ 0 ] ) * st, float( color[ 1 ] ) * st, float( color[ 2 ] ) * st );
+	s->point_lights.push_back( lt );
+	return int( s->point_lights.size() - 1 );
+}
+
+int orc_shade( const orc_scene *s, int shader, int target, const double *wo, double *wi, const double *u, int k,
+			   double *f, double *emission )
+{
+	if ( shader < 0 || shader >= int( s->shaders.size() ) ) return -1;
+	ArrayDraws d( u, k );
+	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i( wi[ 0 ], wi[ 1 ], wi[ 2 ] ), e, r;
+	if ( target == 0 )
+		r = k_eval( s->shaders, shader, o, i, d, e );
+	else
+		r = k_sample( s->shaders, shader, o, d, i, e );
+	for ( int c = 0; c < 3; ++c ) f[ c ] = r[ c ], emission[ c ] = e[ c ], wi[ c ] = i[ c ];
+	return d.used;
 }
 
 int orc_add_mesh( orc_scene *s, const float *v, uint32_t nv, const float *n, const uint32_t *idx, uint32_t nt,
@@ -1015,7 +1194,8 @@ int orc_finalize( orc_scene *s, uint64_t light_seed )
 	for ( auto &p : s->prims )
 		if ( p.kind == 1 ) lo = vmin( lo, p.c - V3( p.r, p.r, p.r ) ), hi = vmax( hi, p.c + V3( p.r, p.r, p.r ) );
 	s->scale = std::isfinite( lo.x ) ? std::max( 1.0, maxc( vmax( vmax( -lo, hi ), V3() ) ) ) : 1.0;
-	s->lights.clear();
+	// point lights first, in asset order (scene.cu:156-163), then area lights
+	s->lights = s->point_lights;
 	Drand48 rng{ light_seed & 0xFFFFFFFFFFFFull };
 	for ( size_t p = 0; p < s->prims.size(); ++p )
 	{
@@ -1095,6 +1275,18 @@ int orc_render( const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32
 				double *sumsq, uint32_t *count )
 {
 	if ( x1 > W || y1 > H || x0 >= x1 || y0 >= y1 || spp == 0 ) return -1;
+	if ( estimator != ORC_KOISHI && estimator < ORC_AOV_NORMAL )
+	{
+		// the corrected estimator covers Lambert, Beckmann Glossy and Emission area lights
+		if ( !s->point_lights.empty() ) return -2;
+		for ( const Prim &p : s->prims )
+		{
+			const Shader &sh = s->shaders[ p.shader ];
+			bool ok = sh.type == ORC_LAMBERT || sh.type == ORC_EMISSION ||
+					  ( sh.type == ORC_GLOSSY && sh.dist == ORC_DIST_BECKMANN );
+			if ( !ok ) return -2;
+		}
+	}
 	Lens lens( s->cam, W, H, spp );
 	uint32_t ww = x1 - x0;
 	std::atomic<uint32_t> next{ y0 };
@@ -1143,12 +1335,15 @@ void orc_bsdf_eval( int estimator, int type, const double *params, const double 
 					double *pdf )
 {
 	Shader sh = make_shader( type, params );
-	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i( wi[ 0 ], wi[ 1 ], wi[ 2 ] ), ff3;
+	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i( wi[ 0 ], wi[ 1 ], wi[ 2 ] ), ff3, e;
 	double pp = 0;
 	if ( estimator == ORC_MIS )
 		m_eval( sh, o, i, ff3, pp );
 	else
-		ff3 = k_eval( sh, o, i );
+	{
+		ArrayDraws d( nullptr, 0 );
+		ff3 = k_eval( std::vector<Shader>{ sh }, 0, o, i, d, e );
+	}
 	f[ 0 ] = ff3.x, f[ 1 ] = ff3.y, f[ 2 ] = ff3.z;
 	*pdf = pp;
 }
@@ -1163,8 +1358,8 @@ void orc_bsdf_sample( int estimator, int type, const double *params, const doubl
 		m_sample( sh, o, u[ 0 ], u[ 1 ], i, w, pp );
 	else
 	{
-		V3 f;
-		k_sample( sh, o, u[ 0 ], u[ 1 ], i, f );
+		ArrayDraws d( u, 2 );
+		V3 e, f = k_sample( std::vector<Shader>{ sh }, 0, o, d, i, e );
 		w = f * std::fabs( i.z );
 	}
 	wi[ 0 ] = i.x, wi[ 1 ] = i.y, wi[ 2 ] = i.z;

@@ -30,16 +30,31 @@ enum { ORC_KOISHI = 0, ORC_MIS = 1 };
  * sample is unoccluded with nonzero radiance; the half-vector angle of the
  * light-0 sample and the view direction, * 2 / pi. */
 enum { ORC_AOV_NORMAL = 4, ORC_AOV_VISIBILITY = 5, ORC_AOV_HALFVECTOR = 6 };
-enum { ORC_LAMBERT = 0, ORC_GLOSSY = 1, ORC_EMISSION = 2 };
+enum { ORC_LAMBERT = 0, ORC_GLOSSY = 1, ORC_EMISSION = 2, ORC_TRANSPARENT = 3, ORC_BLACKHOLE = 4,
+       ORC_REFRACTION = 5, ORC_GLASS = 6, ORC_MIXED = 7 };
+enum { ORC_DIST_BECKMANN = 0, ORC_DIST_COSINE = 1 };
+enum { ORC_FAC_CONSTANT = 0, ORC_FAC_FRESNEL = 1 };
 
 typedef struct orc_scene orc_scene;
 
 orc_scene *orc_scene_new(void);
 void orc_scene_free(orc_scene *s);
 
-/* params: LAMBERT {R[3], color[3]}; GLOSSY {color[3], roughness};
- * EMISSION {color[3], strength}.  Returns the shader id. */
+/* params: LAMBERT {R[3], color[3]}; GLOSSY {color[3], roughness, dist};
+ * EMISSION {color[3], strength}; TRANSPARENT {color[3]}; BLACKHOLE {};
+ * REFRACTION and GLASS {color[3], ior, roughness, dist}; MIXED {fac kind,
+ * fac value (Constant) or ior (Fresnel), shader a, shader b} with a and b
+ * ids returned earlier.  Returns the shader id (-1 for a bad type or child). */
 int orc_add_shader(orc_scene *s, int type, const double *params);
+/* A pointLight asset (position, color, strength); point lights precede the
+ * area lights in the light list.  Returns its index among point lights. */
+int orc_add_point_light(orc_scene *s, const float *pos, const double *color, double strength);
+/* Shader::execute of shader id with k scripted draws u (target 0
+ * compute_f_by_wi_wo, 1 sample_wi_f_by_wo; wi is in/out).  Writes f[3] and
+ * the emission the executed shader sets; returns the number of draws made
+ * (draws past k read 0.5). */
+int orc_shade(const orc_scene *s, int shader, int target, const double *wo, double *wi, const double *u, int k,
+              double *f, double *emission);
 /* Primitives are numbered in the order they are added. Returns the prim id. */
 int orc_add_mesh(orc_scene *s, const float *v, uint32_t nv, const float *n, const uint32_t *idx,
                  uint32_t nt, int shader);
@@ -65,7 +80,9 @@ void orc_ray_triangle(const orc_scene *s, const float *ray, int prim, int tri, d
 void orc_occluded(const orc_scene *s, const float *segs, uint64_t n, uint8_t *out);
 
 /* Per-pixel film over the window [x0,x1) x [y0,y1) of a W x H image:
- * sum, sum of squares (3 doubles each) and the number of finite samples. */
+ * sum, sum of squares (3 doubles each) and the number of finite samples.
+ * Returns -1 for a bad window, -2 when ORC_MIS meets a point light or a
+ * shader other than Lambert, Beckmann Glossy and Emission. */
 int orc_render(const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32_t max_bounce,
                int estimator, uint64_t seed, uint32_t threads, uint32_t x0, uint32_t y0,
                uint32_t x1, uint32_t y1, double *sum, double *sumsq, uint32_t *count);

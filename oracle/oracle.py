@@ -23,7 +23,9 @@ REF_BIN = os.path.join(HERE, "_ref", "cr_ref")
 
 KOISHI, MIS = 0, 1
 AOV_NORMAL, AOV_VISIBILITY, AOV_HALFVECTOR = 4, 5, 6  # the reference's debug kernels
-LAMBERT, GLOSSY, EMISSION = 0, 1, 2
+LAMBERT, GLOSSY, EMISSION, TRANSPARENT, BLACKHOLE, REFRACTION, GLASS, MIXED = range(8)
+DIST = {"Beckmann": 0, "Cosine": 1}
+FAC_CONSTANT, FAC_FRESNEL = 0, 1
 LIGHT_SEED = 0x330E
 
 _lib = None
@@ -39,6 +41,8 @@ def lib():
         sig = {
             "orc_scene_new": (P, []), "orc_scene_free": (None, [P]),
             "orc_add_shader": (I, [P, I, P]),
+            "orc_add_point_light": (I, [P, P, P, D]),
+            "orc_shade": (I, [P, I, I, P, P, P, I, P, P]),
             "orc_add_mesh": (I, [P, P, U32, P, P, U32, I]),
             "orc_add_sphere": (I, [P, P, F, I]),
             "orc_set_camera": (None, [P, P, P, P, F]),
@@ -63,20 +67,66 @@ def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def _dist(props, owner):
+    d = props.get("distribution")
+    if d is None:
+        raise ValueError(f"{owner} needs a distribution")
+    kind = d[0]
+    if kind not in DIST:
+        raise ValueError(f"no such type: {kind}")
+    rough = (d[1].get("roughness", 0.5) if len(d) > 1 else 0.5) if kind == "Beckmann" else 0.5
+    return rough, DIST[kind]
+
+
 def shader_params(cfg):
-    """(type, params) for a reference-schema shader config [Type, props]
-    (Lambert: lambert.hpp:12-19; GlossyBSDF: glossy.hpp:11-17 with
-    beckmann.hpp:11-17; Emission: emission.hpp:12-20)."""
+    """(type, params) for a reference-schema single-node shader config
+    [Type, props] (shader.impl.cu:16-23: Lambert lambert.hpp:12-19;
+    GlossyBSDF glossy.hpp:11-17 with beckmann.hpp:11-17 or cosine.hpp;
+    Emission emission.hpp:12-20; Transparent transparent.hpp:11-15;
+    Blackhole; RefractionBSDF refraction.hpp:11-19; GlassBSDF glass.hpp:11-21).
+    Mixed nests shaders: use add_shader."""
     kind, props = cfg[0], (cfg[1] if len(cfg) > 1 else {})
+    color = list(props.get("color", [1, 1, 1]))
     if kind == "Lambert":
-        return LAMBERT, list(props.get("R", [1, 1, 1])) + list(props.get("color", [1, 1, 1]))
+        return LAMBERT, list(props.get("R", [1, 1, 1])) + color
     if kind == "GlossyBSDF":
-        dist = props.get("distribution", ["Beckmann", {}])
-        rough = dist[1].get("roughness", 0.5) if len(dist) > 1 else 0.5
-        return GLOSSY, list(props.get("color", [1, 1, 1])) + [rough]
+        rough, dist = _dist(props, kind)
+        return GLOSSY, color + [rough, dist]
     if kind == "Emission":
-        return EMISSION, list(props.get("color", [1, 1, 1])) + [props.get("strength", 2.0)]
+        return EMISSION, color + [props.get("strength", 2.0)]
+    if kind == "Transparent":
+        return TRANSPARENT, color
+    if kind == "Blackhole":
+        return BLACKHOLE, []
+    if kind in ("RefractionBSDF", "GlassBSDF"):
+        rough, dist = _dist(props, kind)
+        return (GLASS if kind == "GlassBSDF" else REFRACTION), color + [float(props["ior"]), rough, dist]
     raise ValueError(f"unsupported shader {kind}")
+
+
+def add_shader(h, cfg):
+    """Adds cfg to the oracle scene h (nested Mixed children first,
+    mixed.hpp:11-20 with constant.hpp / fresnel.hpp for fac); returns its id."""
+    L = lib()
+    if cfg[0] == "Mixed":
+        props = cfg[1]
+        fac = props["fac"]
+        fk, fp = fac[0], (fac[1] if len(fac) > 1 else {})
+        if fk == "Constant":
+            fv = (FAC_CONSTANT, float(fp["value"]))
+        elif fk == "Fresnel":
+            fv = (FAC_FRESNEL, float(fp["ior"]))
+        else:
+            raise ValueError(f"no such type: {fk}")
+        a, b = (add_shader(h, c) for c in props["shaders"][:2])
+        params = np.asarray([fv[0], fv[1], a, b], np.float64)
+        r = L.orc_add_shader(h, MIXED, _p(params))
+    else:
+        t, p = shader_params(cfg)
+        params = np.asarray(p + [0.0], np.float64)  # bound: ctypes keeps only the address
+        r = L.orc_add_shader(h, t, _p(params))
+    assert r >= 0
+    return r
 
 
 class OracleScene:
@@ -92,9 +142,7 @@ class OracleScene:
 
         def sid(name):
             if name not in ids:
-                t, p = shader_params(desc.shaders[name])
-                params = np.asarray(p, np.float64)  # bound: ctypes keeps only the address
-                ids[name] = L.orc_add_shader(self.h, t, _p(params))
+                ids[name] = add_shader(self.h, desc.shaders[name])
             return ids[name]
 
         self.prim_kind = []
@@ -109,6 +157,10 @@ class OracleScene:
             c = np.asarray(s["o"], np.float32)
             L.orc_add_sphere(self.h, _p(c), float(s["r"]), sid(s["shader"]))
             self.prim_kind.append(1)
+        for pl in getattr(desc, "point_lights", []):
+            p = np.asarray(pl["position"], np.float32)
+            col = np.asarray(pl.get("color", [1, 1, 1]), np.float64)
+            L.orc_add_point_light(self.h, _p(p), _p(col), float(pl.get("strength", 2.0)))
         cam = desc.camera
         pos = np.asarray(cam["position"], np.float32)
         tgt = np.asarray(cam["target"], np.float32)
@@ -160,9 +212,40 @@ class OracleScene:
         c = np.zeros(n, np.uint32)
         r = lib().orc_render(self.h, W, H, spp, max_bounce, estimator, seed, threads, x0, y0, x1, y1,
                              _p(s), _p(q), _p(c))
-        assert r == 0
+        if r != 0:
+            raise RuntimeError(f"orc_render returned {r}")
         shp = (y1 - y0, x1 - x0)
         return Film(s.reshape(*shp, 3), q.reshape(*shp, 3), c.reshape(shp))
+
+
+class OracleShader:
+    """One shader config (nested Mixed included) in an otherwise empty oracle
+    scene, for Shader::execute with scripted draws."""
+
+    def __init__(self, cfg):
+        self.h = lib().orc_scene_new()
+        self.id = add_shader(self.h, cfg)
+
+    def __del__(self):
+        try:
+            lib().orc_scene_free(self.h)
+        except Exception:
+            pass
+
+    def execute(self, target, wo, u, wi=None):
+        """Per sample: f, wi, emission, draws used (target 0 eval, 1 sample)."""
+        wo = np.ascontiguousarray(wo, np.float64)
+        n = len(wo)
+        u = np.ascontiguousarray(np.asarray(u, np.float64).reshape(n, -1))
+        wi = np.zeros((n, 3)) if wi is None else np.array(wi, np.float64, order="C", copy=True)
+        f, em, used = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n, np.int32)
+        L = lib()
+        ff, ee = np.zeros(3), np.zeros(3)
+        for i in range(n):
+            w = np.ascontiguousarray(wi[i])
+            used[i] = L.orc_shade(self.h, self.id, target, _p(wo[i]), _p(w), _p(u[i]), u.shape[1], _p(ff), _p(ee))
+            f[i], em[i], wi[i] = ff, ee, w
+        return f, wi, em, used
 
 
 def bsdf_eval(estimator, cfg, wo, wi):

@@ -10,7 +10,9 @@
 // keeps a single process-wide static state seeded from time() and shared by all
 // tracer threads (a data race, and no two runs alike).  Here each thread owns its
 // state, seeded deterministically from harness_seed() and a per-thread index, so
-// light-point tables and parity runs are reproducible.
+// light-point tables and parity runs are reproducible.  A thread may also
+// script its draws (harness_rng::script()), which the harness's `shade`
+// command uses to run one Shader::execute on known numbers.
 #pragma once
 
 #include <atomic>
@@ -57,6 +59,18 @@ inline State &state()
 	}
 	return st;
 }
+// Scripted draws of the calling thread: while u is set, sample() hands out
+// u[0..n) in order (0.5 past the end) and counts them in used.
+struct Script
+{
+	const float *u = nullptr;
+	uint32_t n = 0, used = 0;
+};
+inline Script &script()
+{
+	thread_local Script sc;
+	return sc;
+}
 // Set the calling thread's 48-bit state exactly (used before the scene is
 // built so that Mesh::generateSamples draws a known sequence).
 inline void seed_this_thread( uint64_t x48 )
@@ -73,6 +87,13 @@ struct Sampler
 
 	float sample()
 	{
+		auto &sc = harness_rng::script();
+		if ( sc.u )
+		{
+			float v = sc.used < sc.n ? sc.u[ sc.used ] : 0.5f;
+			++sc.used;
+			return v;
+		}
 		auto &st = harness_rng::state();
 		st.x = ( 0x5DEECE66Dull * st.x + 0xB16ull ) & 0xFFFFFFFFFFFFull;
 		unsigned int x = unsigned( st.x >> 16 );

@@ -24,6 +24,14 @@
 //       the 1024-point tables of every emissive mesh (src/core/primitive/mesh.hpp:61-84).
 //   bench  <scene.json> <W> <H> <spp> <threads> [maxBounce] [repeats]
 //       wall time of the reference's own CPUMulticoreTracer::execute, once per repeat.
+//   shade  <shader.json> <records.f32> <k> <out.f32>
+//       Shader::execute (src/core/nodes/shader.hpp:17-23) of the [Type, {props}]
+//       shader in shader.json, built by Factory<Shader>::create, for records
+//       {wo.xyz, wi.xyz, u[k]}: once with compute_f_by_wi_wo on (wo, wi) and
+//       once with sample_wi_f_by_wo on wo (wi preset), each with the sampler
+//       scripted to hand out u from its start.  Out per record (float):
+//       eval f.xyz, eval emission.xyz, eval draws, sample wi.xyz, sample f.xyz,
+//       sample emission.xyz, sample draws.
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -468,6 +476,44 @@ int cmd_bench( int argc, char **argv )
 
 }  // namespace
 
+int cmd_shade( int argc, char **argv )
+{
+	if ( argc < 6 ) return 1;
+	std::ifstream jf( argv[ 2 ] );
+	json j;
+	jf >> j;
+	auto shader = Factory<Shader>::create( j.get<Config>() );
+	const uint32_t k = std::stoul( argv[ 4 ] );
+	auto rec = read_f32( argv[ 3 ] );
+	const size_t stride = 6 + k, n = rec.size() / stride;
+	static constexpr uint32_t block_size = 1 << 16;
+	std::vector<char> block( block_size );
+	HybridAllocator pool( block.data(), block_size );
+	Sampler rng;
+	auto &sc = harness_rng::script();
+	std::vector<float> out;
+	out.reserve( n * 17 );
+	for ( size_t i = 0; i < n; ++i )
+	{
+		const float *r = &rec[ i * stride ];
+		for ( int target = 0; target < 2; ++target )
+		{
+			Varyings v;
+			static_cast<float3 &>( v.wo ) = float3{ r[ 0 ], r[ 1 ], r[ 2 ] };
+			static_cast<float3 &>( v.wi ) = float3{ r[ 3 ], r[ 4 ], r[ 5 ] };
+			sc.u = r + 6, sc.n = k, sc.used = 0;
+			shader->execute( v, rng, pool, target == 0 ? compute_f_by_wi_wo : sample_wi_f_by_wo );
+			pool.clear();
+			if ( target == 1 ) out.insert( out.end(), { v.wi.x, v.wi.y, v.wi.z } );
+			out.insert( out.end(), { v.f.x, v.f.y, v.f.z, v.emission.x, v.emission.y, v.emission.z, float( sc.used ) } );
+		}
+	}
+	sc.u = nullptr;
+	std::ofstream f( argv[ 5 ], std::ios::binary );
+	f.write( (const char *)out.data(), out.size() * 4 );
+	return 0;
+}
+
 int main( int argc, char **argv )
 {
 	if ( argc < 2 )
@@ -484,6 +530,7 @@ int main( int argc, char **argv )
 		else if ( cmd == "occlude" ) rc = cmd_occlude( argc, argv );
 		else if ( cmd == "lights" ) rc = cmd_lights( argc, argv );
 		else if ( cmd == "bench" ) rc = cmd_bench( argc, argv );
+		else if ( cmd == "shade" ) rc = cmd_shade( argc, argv );
 	}
 	catch ( const std::exception &e )
 	{

@@ -14,9 +14,21 @@ stores its answers:
                    render (RadianceKernel::execute through the harness)
   c0_aov_*.npz     the same for the reference's debug kernels Normal,
                    Visibility and HalfVector (src/core/kernel/*.hpp)
+  materials_film.npz, materials_aov_*.npz
+                   Radiance, Visibility and HalfVector renders of the box with
+                   GlassBSDF, RefractionBSDF, Transparent, Blackhole, Mixed
+                   (Fresnel and Constant fac) and a pointLight as light 0
+  shaders.npz      Shader::execute of each reference shader (nested Mixed
+                   included) on scripted draws: for shared records
+                   {wo, wi, u[12]} the f, emission and draw count of
+                   compute_f_by_wi_wo and the wi, f, emission and draw count
+                   of sample_wi_f_by_wo (the harness's `shade` command)
 
-Usage:  python tests/golden/make_golden.py [--aov-only]
+Usage:  python tests/golden/make_golden.py [--aov-only | --materials-only]
+(the harness's render threads take rows dynamically, so a film regenerated
+from the same seed is a different Monte Carlo draw of the same image)
 """
+import json
 import hashlib
 import os
 import subprocess
@@ -38,8 +50,11 @@ import oracle  # noqa: E402
 FILM_W, FILM_H, FILM_SPP = 48, 48, 1024
 
 
-def scene_hash(desc):
+def scene_hash(desc, full=False):
+    """Geometry hash; full=True also covers the shaders and the point lights."""
     h = hashlib.sha256()
+    if full:
+        h.update(json.dumps([desc.shaders, desc.point_lights], sort_keys=True).encode())
     for g in desc.groups:
         h.update(g.name.encode())
         h.update(np.ascontiguousarray(g.v).tobytes())
@@ -97,11 +112,87 @@ def run(*args, cwd):
 AOV_KERNELS = ("Normal", "Visibility", "HalfVector")
 AOV_W, AOV_H, AOV_SPP = 48, 48, 256
 
+SHADE_N, SHADE_K = 512, 12
 
-def main(aov_only=False):
+
+def shader_configs():
+    """The reference's shader registry (shader.impl.cu:16-23) with both
+    distributions, both fac scalas and a nested Mixed."""
+    beck = ["Beckmann", {"roughness": 0.3}]
+    return [
+        ["Lambert", {"R": [0.5, 0.6, 0.7], "color": [1, 0.9, 0.8]}],
+        ["GlossyBSDF", {"distribution": beck, "color": [0.9, 0.8, 0.7]}],
+        ["GlossyBSDF", {"distribution": ["Cosine", {}], "color": [0.9, 0.8, 0.7]}],
+        ["Emission", {"color": [1, 0.5, 0.25], "strength": 3}],
+        ["Transparent", {"color": [0.9, 0.9, 0.5]}],
+        ["Blackhole", {}],
+        ["RefractionBSDF", {"ior": 1.5, "distribution": beck, "color": [1, 1, 0.9]}],
+        ["RefractionBSDF", {"ior": 1.33, "distribution": ["Cosine", {}]}],
+        ["GlassBSDF", {"ior": 1.45, "distribution": ["Beckmann", {"roughness": 0.1}], "color": [0.95, 1, 1]}],
+        ["Mixed", {"fac": ["Fresnel", {"ior": 1.5}],
+                   "shaders": [["Lambert", {"R": [0.3, 0.3, 0.3]}], ["GlossyBSDF", {"distribution": beck}]]}],
+        ["Mixed", {"fac": ["Constant", {"value": 0.3}],
+                   "shaders": [["Mixed", {"fac": ["Constant", {"value": 0.6}],
+                                          "shaders": [["Emission", {"strength": 4}],
+                                                      ["GlassBSDF", {"ior": 1.3, "distribution": beck}]]}],
+                               ["Transparent", {}]]}],
+    ]
+
+
+def shade_records(seed=41):
+    """wo, wi uniform on the sphere (both sides of the surface), with grazing
+    and near-normal directions mixed in; u uniform in [0, 1)."""
+    rng = np.random.default_rng(seed)
+
+    def dirs(n):
+        d = rng.normal(size=(n, 3))
+        return d / np.linalg.norm(d, axis=1, keepdims=True)
+    wo, wi = dirs(SHADE_N), dirs(SHADE_N)
+    k = SHADE_N // 8
+    wo[:k, 2] *= 1e-3        # grazing
+    wo[k:2 * k, :2] *= 1e-3  # near the normal (both sides)
+    wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    return wo.astype(np.float32), wi.astype(np.float32), rng.random((SHADE_N, SHADE_K)).astype(np.float32)
+
+
+def make_shaders(tmp):
+    wo, wi, u = shade_records()
+    np.concatenate([wo, wi, u], 1).astype(np.float32).tofile(os.path.join(tmp, "rec.f32"))
+    outs = []
+    for cfg in shader_configs():
+        with open(os.path.join(tmp, "shader.json"), "w") as fh:
+            json.dump(cfg, fh)
+        run("shade", "shader.json", "rec.f32", SHADE_K, "shade.f32", cwd=tmp)
+        outs.append(np.fromfile(os.path.join(tmp, "shade.f32"), np.float32).reshape(SHADE_N, 17))
+    np.savez_compressed(os.path.join(HERE, "shaders.npz"), wo=wo, wi=wi, u=u, out=np.stack(outs),
+                        configs=json.dumps(shader_configs()))
+
+
+def make_materials(tmp):
+    m = scenes.config_materials()
+    scenes.write_scene(m, tmp)
+    js = f"{m.name}.json"
+    for kname in ("Visibility", "HalfVector"):
+        run("render", js, AOV_W, AOV_H, AOV_SPP, os.cpu_count(), "aov.crf", m.max_bounce, 31, kname, cwd=tmp)
+        film = oracle.read_crf(os.path.join(tmp, "aov.crf"))
+        np.savez_compressed(os.path.join(HERE, f"materials_aov_{kname.lower()}.npz"), sum=film.sum, sumsq=film.sumsq,
+                            count=film.count, width=AOV_W, height=AOV_H, spp=AOV_SPP, kernel=kname,
+                            scene_hash=scene_hash(m, full=True))
+    run("render", js, FILM_W, FILM_H, FILM_SPP, os.cpu_count(), "film.crf", m.max_bounce, 37, cwd=tmp)
+    film = oracle.read_crf(os.path.join(tmp, "film.crf"))
+    np.savez_compressed(os.path.join(HERE, "materials_film.npz"), sum=film.sum, sumsq=film.sumsq, count=film.count,
+                        width=FILM_W, height=FILM_H, spp=FILM_SPP, max_bounce=m.max_bounce,
+                        scene_hash=scene_hash(m, full=True))
+
+
+def main(aov_only=False, materials_only=False):
     if not oracle.ref_available():
         sys.exit("build the reference harness first: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
+        if materials_only:
+            make_shaders(tmp)
+            make_materials(tmp)
+            return
         c0 = scenes.config0()
         scenes.write_scene(c0, tmp)
         js = f"{c0.name}.json"
@@ -154,4 +245,4 @@ def main(aov_only=False):
 
 
 if __name__ == "__main__":
-    main(aov_only="--aov-only" in sys.argv)
+    main(aov_only="--aov-only" in sys.argv, materials_only="--materials-only" in sys.argv)

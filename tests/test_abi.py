@@ -55,8 +55,35 @@ def test_shader_registry_and_errors(cr):
         assert b"json" in lib.cr_last_error()
         assert lib.cr_scene_add_shader(h, b"x", b'["NoSuchShader", {}]') == -2
         assert b"no such type" in lib.cr_last_error()
-        assert lib.cr_scene_add_shader(h, b"x", b'["GlassBSDF", {}]') == -5
-        assert lib.cr_scene_add_shader(h, b"x", b'["GlossyBSDF", {"distribution": ["Cosine", {}]}]') == -5
+        # the whole registry (shader.impl.cu:16-23); required properties as
+        # the reference's get<T>( props, key ) demands them
+        assert lib.cr_scene_add_shader(h, b"x", b'["GlassBSDF", {}]') == -2
+        assert b"ior" in lib.cr_last_error()
+        assert lib.cr_scene_add_shader(h, b"x", b'["GlassBSDF", {"ior": 1.5}]') == -2
+        assert b"distribution" in lib.cr_last_error()
+        beck = ["Beckmann", {"roughness": 0.2}]
+        for cfg in (["GlossyBSDF", {"distribution": ["Cosine", {}]}], ["Transparent", {"color": [1, 1, 0]}],
+                    ["Blackhole", {}], ["RefractionBSDF", {"ior": 1.33, "distribution": beck}],
+                    ["GlassBSDF", {"ior": 1.5, "distribution": beck}],
+                    ["Mixed", {"fac": ["Fresnel", {"ior": 1.5}], "shaders": [["Lambert", {}], ["Blackhole", {}]]}]):
+            assert lib.cr_scene_add_shader(h, b"ok", json.dumps(cfg).encode()) >= 0, lib.cr_last_error()
+        assert lib.cr_scene_add_shader(h, b"x", b'["GlossyBSDF", {"distribution": ["GGX", {}]}]') == -2
+        assert lib.cr_scene_add_shader(h, b"x", b'["Mixed", {"shaders": [["Lambert", {}], ["Lambert", {}]]}]') == -2
+        assert b"fac" in lib.cr_last_error()
+        assert lib.cr_scene_add_shader(h, b"x", b'["Mixed", {"fac": ["Constant", {"value": 0.5}], '
+                                                b'"shaders": [["Lambert", {}]]}]') == -2
+        assert lib.cr_scene_add_shader(h, b"x", b'["Mixed", {"fac": ["Noise", {}], '
+                                                b'"shaders": [["Lambert", {}], ["Lambert", {}]]}]') == -2
+        assert lib.cr_scene_add_shader(h, b"x", b'["Mixed", {"fac": ["Constant", {}], '
+                                                b'"shaders": [["Lambert", {}], ["Lambert", {}]]}]') == -2
+        deep = ["Lambert", {}]
+        for _ in range(17):
+            deep = ["Mixed", {"fac": ["Constant", {"value": 0.5}], "shaders": [deep, ["Lambert", {}]]}]
+        assert lib.cr_scene_add_shader(h, b"x", json.dumps(deep).encode()) == -5
+        # the pointLight asset (pointLight.hpp:13-18)
+        pos = np.array([1, 2, 3], np.float32)
+        assert lib.cr_scene_add_point_light(h, C.c_void_p(pos.ctypes.data), None, 2.0) == 0
+        assert lib.cr_scene_add_point_light(h, None, None, 2.0) == -1
     finally:
         lib.cr_scene_destroy(h)
 

@@ -1,0 +1,113 @@
+"""The reference's remaining shaders and the pointLight on the GPU: the device
+Shader::execute against the reference's own outputs on scripted draws
+(tests/golden/shaders.npz), and renders of the materials scene against the
+reference's films (materials_*.npz) and the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden, require_gpu
+from golden.make_golden import shader_configs
+from gpu_util import render_film, zscores
+
+pytestmark = pytest.mark.gpu
+
+# float against float with different operation order: the same tolerances as
+# the oracle's, and at most a few records whose selection draw sits within
+# rounding of its threshold
+F_RTOL, F_ATOL, WI_ATOL = 2e-4, 1e-6, 1e-3
+
+
+@pytest.fixture(scope="module")
+def mats(scenes):
+    return scenes.config_materials()
+
+
+@pytest.fixture(scope="module")
+def mats_scene(cr, mats):
+    require_gpu()
+    return cr.Scene.from_desc(mats)
+
+
+@pytest.mark.parametrize("index", range(len(shader_configs())))
+def test_device_shader_execute_matches_reference(cr, index):
+    require_gpu()
+    g = golden("shaders.npz")
+    cfg = shader_configs()[index]
+    out = g["out"][index]
+    fe, _, ee, ue = cr.shader_execute(cfg, cr.SHADE_EVAL, g["wo"], g["u"], g["wi"])
+    fs, ws, es, us = cr.shader_execute(cfg, cr.SHADE_SAMPLE, g["wo"], g["u"], g["wi"])
+    same = (ue == out[:, 6]) & (us == out[:, 16])
+    assert same.sum() >= len(same) - 2, (cfg, np.nonzero(~same))
+    for a, b, tol in ((fe, out[:, 0:3], None), (ee, out[:, 3:6], None), (ws, out[:, 7:10], WI_ATOL),
+                      (fs, out[:, 10:13], None), (es, out[:, 13:16], None)):
+        if tol is None:
+            np.testing.assert_allclose(a[same], b[same], rtol=F_RTOL, atol=F_ATOL)
+        else:
+            np.testing.assert_allclose(a[same], b[same], rtol=0, atol=tol)
+
+
+# Caustics through the glass spheres (a Lambert floor vertex, two refractions
+# with the reference's 1/eta^2 gain, then the emitter) make the image mean
+# heavy-tailed: across oracle seeds at 512 spp it spreads by +-0.7%, about
+# twice its sample standard error.  The image-level check allows 2%.
+IMAGE_RTOL = 0.02
+
+
+def test_materials_render_matches_reference(cr, mats_scene):
+    """Per pixel at the reference's sample count within 3 sigma of the
+    combined standard error, and the image mean within IMAGE_RTOL."""
+    g = golden("materials_film.npz")
+    W, H, spp, mb = int(g["width"]), int(g["height"]), int(g["spp"]), int(g["max_bounce"])
+    ref = O.Film(g["sum"], g["sumsq"], g["count"])
+    f = render_film(cr, mats_scene, W, H, spp, seeds=[3], estimator=cr.KOISHI, max_bounce=mb)
+    assert f.count.sum() >= 0.999 * W * H * spp
+    z = zscores(f, ref)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert z.max() < 5.5
+    assert abs(f.mean.mean() / ref.mean.mean() - 1) < IMAGE_RTOL
+
+
+def test_materials_render_matches_oracle(cr, mats, mats_scene):
+    W, H, spp = 32, 32, 1024
+    o = O.OracleScene(mats).render(W, H, spp, 7, O.KOISHI, seed=53)
+    f = render_film(cr, mats_scene, W, H, spp, seeds=[7, 8], estimator=cr.KOISHI)
+    z = zscores(f, o)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert z.max() < 5.5
+    assert abs(f.mean.mean() / o.mean.mean() - 1) < IMAGE_RTOL
+
+
+@pytest.mark.parametrize("kernel", ["Visibility", "HalfVector"])
+def test_point_light_debug_kernels_match_reference(cr, mats, kernel):
+    require_gpu()
+    g = golden(f"materials_aov_{kernel.lower()}.npz")
+    W, H, spp = int(g["width"]), int(g["height"]), int(g["spp"])
+    ref = O.Film(g["sum"], g["sumsq"], g["count"])
+    f = render_film(cr, cr.Scene.from_desc(mats).set_kernel(kernel), W, H, spp, seeds=[9], estimator=cr.KOISHI)
+    d = np.abs(f.mean - ref.mean)
+    assert (d > 1e-3).mean() < 0.02, (d > 1e-3).mean()  # per-sample deterministic: edges only
+    assert abs(f.mean.mean() / ref.mean.mean() - 1) < 0.01
+
+
+def test_json_scene_with_point_light(cr, scenes, mats, mats_scene, tmp_path):
+    """The reference's JSON schema path: a pointLight asset and the shader
+    registry through cr_scene_create, rendering what the add_* path renders."""
+    path = scenes.write_scene(mats, str(tmp_path))
+    s = cr.Scene.from_file(path)
+    assert s.info()["lights"] == 2 == mats_scene.info()["lights"]  # the point light, then the panel
+    a = render_film(cr, s, 24, 24, 64, seeds=[5], estimator=cr.KOISHI)
+    b = render_film(cr, mats_scene, 24, 24, 64, seeds=[5], estimator=cr.KOISHI)
+    np.testing.assert_allclose(a.sum, b.sum, rtol=1e-12, atol=0)
+
+
+def test_mis_and_guiding_refuse_reference_only_shaders(cr, mats_scene):
+    require_gpu()
+    with pytest.raises(cr.CrError, match="reference estimator only"):
+        mats_scene.render(8, 8, 1, estimator=cr.MIS)
+    with pytest.raises(cr.CrError):
+        mats_scene.render(8, 8, 1, estimator=cr.MIS, guiding=True)
+    with pytest.raises(cr.CrError, match="selection numbers"):
+        cr.bsdf_eval(cr.KOISHI, shader_configs()[-1], np.zeros((1, 3)) + [0, 0, 1], np.zeros((1, 3)) + [0, 0, 1])
+    film, _ = mats_scene.render(8, 8, 4, estimator=cr.KOISHI)
+    assert np.isfinite(film).all()
