@@ -113,6 +113,7 @@ def lib():
             "cr_scene_add_mesh": (I, [P, P, U32, P, P, U32, C.c_char_p]),
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
             "cr_scene_add_point_light": (I, [P, P, P, F]),
+            "cr_scene_set_lens": (I, [P, I]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
             "cr_scene_set_kernel": (I, [P, C.c_char_p]), "cr_mesh_file_info": (I, [C.c_char_p, P, P, P, P]),
@@ -221,6 +222,10 @@ class Scene:
         tgt = np.asarray(cam["target"], np.float32)
         up = np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)
         _check(lib().cr_scene_set_camera(s.h, _p(pos), _p(tgt), _p(up), float(cam.get("fovx", 90.0))))
+        lens = cam.get("lens", "pinhole")
+        if lens not in ("pinhole", "orthographic"):
+            raise CrError(-2, f"unknown lens type: {lens}")
+        _check(lib().cr_scene_set_lens(s.h, 1 if lens == "orthographic" else 0))
         if build:
             bc = BuildConfig(builder=build.get("builder", 0), ploc_radius=build.get("ploc_radius", 10),
                              max_leaf=build.get("max_leaf", 3), cost_node=build.get("cost_node", 1.2),

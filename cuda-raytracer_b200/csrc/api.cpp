@@ -1145,7 +1145,8 @@ DevScene dev_scene( const cr_scene *s )
 	return d;
 }
 
-// PinholeLens (src/core/misc/lens.hpp:15-27) for a W x H image at spp.
+// The Lens base (src/core/misc/lens.hpp:15-27) for a W x H image at spp; the
+// lens kind selects PinholeLens or OrthographicLens (renderer.cu:30-38).
 DevCamera make_camera( const HostCamera &c, uint32_t w, uint32_t h, uint32_t spp )
 {
 	auto norm = []( const float a[ 3 ], float o[ 3 ] ) {
@@ -1159,6 +1160,7 @@ DevCamera make_camera( const HostCamera &c, uint32_t w, uint32_t h, uint32_t spp
 	};
 	DevCamera d;
 	d.width = w, d.height = h;
+	d.lens = uint32_t( c.lens );
 	d.pw = uint32_t( std::ceil( std::sqrt( double( spp ) ) ) );
 	float t[ 3 ], tmp[ 3 ];
 	norm( c.target, t );
@@ -1195,7 +1197,6 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
 	if ( !desc->width || !desc->height || !desc->spp ) fail( CR_ERR_INVALID, "width, height and spp must be positive" );
 	if ( !s->has_camera ) fail( CR_ERR_INVALID, "no camera in the scene" );
-	if ( s->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, "orthographic lens is outside the Radiance path implemented here" );
 	const int kernel = kernel_id( s->kernel );
 	if ( kernel < 0 )
 		fail( CR_ERR_UNSUPPORTED, "kernel '" + s->kernel + "' is not registered (Radiance, Normal, Visibility, HalfVector)" );
@@ -1510,6 +1511,15 @@ int cr_scene_set_camera( cr_scene *s, const float *pos, const float *target, con
 		s->cam.fovx = fovx;
 		s->cam.lens = 0;
 		s->has_camera = true;
+	} );
+}
+
+int cr_scene_set_lens( cr_scene *s, int lens )
+{
+	return guarded( [&] {
+		if ( !s ) fail( CR_ERR_INVALID, "null scene" );
+		if ( lens != CR_LENS_PINHOLE && lens != CR_LENS_ORTHOGRAPHIC ) fail( CR_ERR_INVALID, "unknown lens type" );
+		s->cam.lens = lens;
 	} );
 }
 
@@ -1878,7 +1888,6 @@ int cr_batch_create( const cr_batch_job *jobs, uint32_t n_jobs, uint32_t max_bou
 			const std::string at = "batch job " + std::to_string( i ) + ": ";
 			if ( !j.scene || !j.scene->committed ) fail( CR_ERR_STATE, at + "scene missing or not committed" );
 			if ( !j.scene->has_camera ) fail( CR_ERR_INVALID, at + "no camera in the scene" );
-			if ( j.scene->cam.lens != 0 ) fail( CR_ERR_UNSUPPORTED, at + "orthographic lens is outside the Radiance path" );
 			if ( !j.width || !j.height || !j.spp ) fail( CR_ERR_INVALID, at + "width, height and spp must be positive" );
 			if ( !j.d_sum || !j.d_sumsq || !j.d_count ) fail( CR_ERR_INVALID, at + "null film" );
 			if ( estimator == EST_MIS && !j.scene->mis_blocker.empty() )

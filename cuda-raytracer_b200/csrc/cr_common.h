@@ -128,6 +128,7 @@ struct DevCamera
 {
 	float o[ 3 ], n[ 3 ], u[ 3 ], v[ 3 ], du[ 3 ], dv[ 3 ];
 	uint32_t width, height, pw;
+	uint32_t lens;  // CameraConfig::lens: 0 pinhole, 1 orthographic
 };
 
 // Everything a kernel needs to know about one committed scene.

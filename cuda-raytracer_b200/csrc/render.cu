@@ -56,6 +56,25 @@ __device__ __forceinline__ uint32_t warp_append( bool want, uint32_t *counter )
 	return base + __popc( mask & ( ( 1u << lane_id() ) - 1u ) );
 }
 
+// Lens::sample of sub-pixel sample k of pixel (x, y) (src/core/misc/lens.hpp):
+// PinholeLens (:56-66) shoots from the camera through the stratified point on
+// the image plane; OrthographicLens (:40-53) moves the origin by that plane
+// offset times 4 / width and shoots along the view direction.
+__device__ __forceinline__ void camera_ray( const DevCamera &c, uint32_t x, uint32_t y, uint32_t k, float3 &o, float3 &d )
+{
+	const float fx = float( x ) - float( c.width ) * 0.5f, fy = float( y ) - float( c.height ) * 0.5f;
+	if ( c.lens == 1 )
+	{
+		const float3 p = f3( c.u ) * fx + f3( c.v ) * fy + ( f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
+		o = f3( c.o ) + p * 4.f / float( c.width );
+		d = normalize( f3( c.n ) );
+		return;
+	}
+	const float3 t = f3( c.n ) + f3( c.u ) * fx + f3( c.v ) * fy;
+	o = f3( c.o );
+	d = normalize( t + f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
+}
+
 __global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa )
 {
 	if ( blockIdx.x == 0 && threadIdx.x == 0 ) wb.counters[ CNT_EXT ] = wa.n;
@@ -64,11 +83,9 @@ __global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveA
 		uint64_t g = wa.first + s;
 		uint32_t pix = uint32_t( g / cfg.spp ), k = uint32_t( g % cfg.spp );
 		uint32_t x = cfg.x0 + pix % cfg.ww, y = cfg.y0 + pix / cfg.ww;
-		const DevCamera &c = sc.cam;
-		float fx = float( x ) - float( c.width ) * 0.5f, fy = float( y ) - float( c.height ) * 0.5f;
-		float3 t = f3( c.n ) + f3( c.u ) * fx + f3( c.v ) * fy;
-		float3 d = normalize( t + f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
-		wb.ray_o[ s ] = make_float4( c.o[ 0 ], c.o[ 1 ], c.o[ 2 ], 0.f );
+		float3 o, d;
+		camera_ray( sc.cam, x, y, k, o, d );
+		wb.ray_o[ s ] = make_float4( o.x, o.y, o.z, 0.f );
 		wb.ray_d[ s ] = make_float4( d.x, d.y, d.z, INFINITY );
 		wb.beta[ s ] = make_float4( 1.f, 1.f, 1.f, 0.f );
 		wb.L[ s ] = make_float4( 0.f, 0.f, 0.f, 0.f );
@@ -590,11 +607,9 @@ __global__ void k_generate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa )
 		const uint64_t local = g - job.first_sample;
 		const uint32_t pix = uint32_t( local / job.spp ), k = uint32_t( local % job.spp );
 		const uint32_t x = pix % job.width, y = pix / job.width;
-		const DevCamera &c = bd.scenes[ j ].cam;
-		float fx = float( x ) - float( c.width ) * 0.5f, fy = float( y ) - float( c.height ) * 0.5f;
-		float3 t = f3( c.n ) + f3( c.u ) * fx + f3( c.v ) * fy;
-		float3 d = normalize( t + f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
-		wb.ray_o[ s ] = make_float4( c.o[ 0 ], c.o[ 1 ], c.o[ 2 ], 0.f );
+		float3 o, d;
+		camera_ray( bd.scenes[ j ].cam, x, y, k, o, d );
+		wb.ray_o[ s ] = make_float4( o.x, o.y, o.z, 0.f );
 		wb.ray_d[ s ] = make_float4( d.x, d.y, d.z, INFINITY );
 		wb.beta[ s ] = make_float4( 1.f, 1.f, 1.f, 0.f );
 		wb.L[ s ] = make_float4( 0.f, 0.f, 0.f, 0.f );

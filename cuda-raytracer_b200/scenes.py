@@ -279,6 +279,15 @@ def config0(width=256, height=256, spp=64) -> SceneDesc:
                      width=width, height=height, spp=spp, max_bounce=7, name="config0")
 
 
+def config0_ortho(width=256, height=256, spp=64) -> SceneDesc:
+    """Config 0 seen through the reference's OrthographicLens (lens.hpp:40-53):
+    parallel rays from a 4-unit-wide plane at the camera position."""
+    d = config0(width, height, spp)
+    d.camera = dict(d.camera, lens="orthographic")
+    d.name = "config0_ortho"
+    return d
+
+
 def config_materials(width=256, height=256, spp=64) -> SceneDesc:
     """The box with the reference's remaining shaders and a point light:
     GlassBSDF, RefractionBSDF, Transparent, Blackhole, Mixed over a Fresnel
@@ -672,7 +681,8 @@ def write_scene(desc: SceneDesc, out_dir: str, fmt="crm", **kw) -> str:
 
 
 # ----------------------------------------------------------------------------
-# camera rays, restating PinholeLens::sample (src/core/misc/lens.hpp:15-27,62-66)
+# camera rays, restating PinholeLens::sample and OrthographicLens::sample
+# (src/core/misc/lens.hpp:15-27, 40-66)
 
 def pinhole_rays(camera, w, h, spp, pixels, ks):
     """float32 primary rays (o, d) for pixel indices (x, y) and sample indices k."""
@@ -690,7 +700,14 @@ def pinhole_rays(camera, w, h, spp, pixels, ks):
     x = pixels[:, 0].astype(f32)[:, None]
     y = pixels[:, 1].astype(f32)[:, None]
     k = np.asarray(ks)
+    ju, jv = (k % pw).astype(f32)[:, None], (k // pw).astype(f32)[:, None]
+    if camera.get("lens", "pinhole") == "orthographic":
+        # OrthographicLens::sample (lens.hpp:40-53)
+        p = u[None] * (x - f32(w * 0.5)) + v[None] * (y - f32(h * 0.5)) + (du[None] * ju + dv[None] * jv)
+        o = (pos[None] + p * f32(4.0) / f32(w)).astype(f32)
+        d = np.broadcast_to(nrm(n), o.shape).astype(f32)
+        return o, d
     t = n[None] + u[None] * (x - f32(w * 0.5)) + v[None] * (y - f32(h * 0.5))
-    d = nrm(t + du[None] * (k % pw).astype(f32)[:, None] + dv[None] * (k // pw).astype(f32)[:, None])
+    d = nrm(t + du[None] * ju + dv[None] * jv)
     o = np.broadcast_to(pos, d.shape).astype(f32)
     return o, d

@@ -143,6 +143,15 @@ int cr_scene_add_point_light(cr_scene *s, const float *position, const float *co
 int cr_scene_set_camera(cr_scene *s, const float *position, const float *target, const float *upaxis,
                         float fovx);
 
+/* CameraConfig::lens ("pinhole" / "orthographic", config.hpp:14-27), which
+ * the Renderer turns into a PinholeLens or an OrthographicLens
+ * (src/core/renderer/renderer.cu:30-38, lens.hpp:40-66).  The orthographic
+ * lens shoots along the view direction from the camera position moved by
+ * the image-plane offset times 4 / width.  Call after cr_scene_set_camera. */
+#define CR_LENS_PINHOLE 0
+#define CR_LENS_ORTHOGRAPHIC 1
+int cr_scene_set_lens(cr_scene *s, int lens);
+
 /* Upload and build the quantised 8-wide BVH on the GPU; replaces the host
  * builder createBVH / doCreateBVH (src/core/primitive/mesh.cu:35-143).
  * light_seed seeds the reference-compatible light-point tables

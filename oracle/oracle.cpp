@@ -112,6 +112,7 @@ struct Camera
 	V3 pos{ 1, 0, 0 }, target{ -1, 0, 0 }, up{ 0, 0, 1 };
 	float fpos[ 3 ] = { 1, 0, 0 }, ftarget[ 3 ] = { -1, 0, 0 }, fup[ 3 ] = { 0, 0, 1 };
 	double fovx = 90;
+	int lens = 0;  // CameraConfig::lens: 0 pinhole, 1 orthographic
 };
 
 struct Hit
@@ -396,15 +397,17 @@ bool occluded_seg( const orc_scene *s, V3 o, V3 d, double len )
 }
 
 // ---------------------------------------------------------------- camera
-// PinholeLens::sample (src/core/misc/lens.hpp:15-27,62-66) in FP64.
+// PinholeLens::sample and OrthographicLens::sample (src/core/misc/lens.hpp:15-66)
+// in FP64.
 struct Lens
 {
 	V3 o, n, u, v, du, dv;
 	double w, h;
 	uint32_t pw;
+	int kind;
 	Lens( const Camera &c, uint32_t W, uint32_t H, uint32_t spp )
 	{
-		w = W, h = H;
+		w = W, h = H, kind = c.lens;
 		pw = uint32_t( std::ceil( std::sqrt( double( spp ) ) ) );
 		o = c.pos;
 		n = normalize( c.target ) * ( double( W ) / ( 2 * std::tan( c.fovx * PI / 180.0 * 0.5 ) ) );
@@ -413,10 +416,13 @@ struct Lens
 		du = u / double( pw );
 		dv = v / double( pw );
 	}
-	V3 dir( uint32_t x, uint32_t y, uint32_t k ) const
+	void ray( uint32_t x, uint32_t y, uint32_t k, V3 &ro, V3 &rd ) const
 	{
-		V3 t = n + u * ( double( x ) - w * .5 ) + v * ( double( y ) - h * .5 );
-		return normalize( t + du * double( k % pw ) + dv * double( k / pw ) );
+		V3 p = u * ( double( x ) - w * .5 ) + v * ( double( y ) - h * .5 ) + du * double( k % pw ) + dv * double( k / pw );
+		if ( kind == 1 )  // lens.hpp:47-52: origin moved by the plane offset * 4 / w
+			ro = o + p * ( 4.0 / w ), rd = normalize( n );
+		else
+			ro = o, rd = normalize( n + p );
 	}
 };
 
@@ -1186,6 +1192,8 @@ void orc_set_camera( orc_scene *s, const float *pos, const float *target, const 
 	s->cam.fovx = fovx;
 }
 
+void orc_set_lens( orc_scene *s, int lens ) { s->cam.lens = lens; }
+
 int orc_finalize( orc_scene *s, uint64_t light_seed )
 {
 	build_bvh( s );
@@ -1302,11 +1310,12 @@ int orc_render( const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32
 				for ( uint32_t k = 0; k < spp; ++k )
 				{
 					Rng rng( seed, uint64_t( y ) * W + x, k );
-					V3 d = lens.dir( x, y, k );
-					V3 L = estimator == ORC_KOISHI ? radiance_koishi( s, s->cam.pos, d, max_bounce, rng )
+					V3 ro, d;
+					lens.ray( x, y, k, ro, d );
+					V3 L = estimator == ORC_KOISHI ? radiance_koishi( s, ro, d, max_bounce, rng )
 						   : estimator >= ORC_AOV_NORMAL
-							   ? aov_koishi( s, s->cam.pos, d, estimator, rng )
-							   : radiance_mis( s, s->cam.pos, d, max_bounce, rng, estimator == ORC_MIS ? 0 : estimator );
+							   ? aov_koishi( s, ro, d, estimator, rng )
+							   : radiance_mis( s, ro, d, max_bounce, rng, estimator == ORC_MIS ? 0 : estimator );
 					if ( !finite3( L ) ) continue;  // cpuMulticore.cu:58-64
 					++c;
 					for ( int ch = 0; ch < 3; ++ch ) a[ ch ] += L[ ch ], q[ ch ] += L[ ch ] * L[ ch ];

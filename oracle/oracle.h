@@ -60,6 +60,8 @@ int orc_add_mesh(orc_scene *s, const float *v, uint32_t nv, const float *n, cons
                  uint32_t nt, int shader);
 int orc_add_sphere(orc_scene *s, const float *center, float radius, int shader);
 void orc_set_camera(orc_scene *s, const float *pos, const float *target, const float *up, float fovx);
+/* CameraConfig::lens: 0 pinhole, 1 orthographic (lens.hpp:40-66). */
+void orc_set_lens(orc_scene *s, int lens);
 /* Builds the BVH and the light list; light_seed is the 48-bit state the
  * 1024-point tables are drawn from (ORC_KOISHI). */
 int orc_finalize(orc_scene *s, uint64_t light_seed);

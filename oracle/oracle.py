@@ -45,7 +45,7 @@ def lib():
             "orc_shade": (I, [P, I, I, P, P, P, I, P, P]),
             "orc_add_mesh": (I, [P, P, U32, P, P, U32, I]),
             "orc_add_sphere": (I, [P, P, F, I]),
-            "orc_set_camera": (None, [P, P, P, P, F]),
+            "orc_set_camera": (None, [P, P, P, P, F]), "orc_set_lens": (None, [P, I]),
             "orc_finalize": (I, [P, U64]), "orc_num_lights": (I, [P]),
             "orc_light_table": (D, [P, I, P]),
             "orc_trace": (None, [P, P, U64, P, P, P, P, P]),
@@ -166,6 +166,7 @@ class OracleScene:
         tgt = np.asarray(cam["target"], np.float32)
         up = np.asarray(cam.get("upaxis", [0, 0, 1]), np.float32)
         L.orc_set_camera(self.h, _p(pos), _p(tgt), _p(up), float(cam.get("fovx", 90)))
+        L.orc_set_lens(self.h, 1 if cam.get("lens", "pinhole") == "orthographic" else 0)
         L.orc_finalize(self.h, light_seed)
 
     def __del__(self):

@@ -280,7 +280,10 @@ int cmd_render( int argc, char **argv )
 	uint32_t mb = argc > 8 ? std::stoul( argv[ 8 ] ) : L.max_bounce;
 	harness_rng::base_seed() = seed;
 	auto kern = Factory<Kernel>::create( kernel_config( mb, kname ) );
-	PinholeLens lens( L.scene->camera[ 0 ], W, H, spp );
+	// the Renderer's lens choice (src/core/renderer/renderer.cu:30-38)
+	PinholeLens pinhole( L.scene->camera[ 0 ], W, H, spp );
+	OrthographicLens ortho( L.scene->camera[ 0 ], W, H, spp );
+	const Lens &lens = L.scene->camera[ 0 ].lens == 1 ? static_cast<const Lens &>( ortho ) : pinhole;
 	std::vector<double> sum( size_t( W ) * H * 3 ), sq( size_t( W ) * H * 3 );
 	std::vector<uint32_t> cnt( size_t( W ) * H );
 	std::atomic<uint32_t> nextRow{ 0 };
@@ -457,7 +460,11 @@ int cmd_bench( int argc, char **argv )
 	tp[ "kernel" ] = json::array( { "Radiance", kp } );
 	auto tracer = Factory<Tracer>::create( Config( "CPUMulticore", tp ) );
 	util::Image<3> image( W, H );
-	poly::object<Lens> lens = poly::make_object<PinholeLens>( L.scene->camera[ 0 ], W, H, spp );
+	poly::object<Lens> lens;
+	if ( L.scene->camera[ 0 ].lens == 1 )
+		lens = poly::make_object<OrthographicLens>( L.scene->camera[ 0 ], W, H, spp );
+	else
+		lens = poly::make_object<PinholeLens>( L.scene->camera[ 0 ], W, H, spp );
 	SamplerGenerator gen;
 	Properties pp;
 	pp[ "enable" ] = false;

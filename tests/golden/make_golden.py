@@ -18,13 +18,15 @@ stores its answers:
                    Radiance, Visibility and HalfVector renders of the box with
                    GlassBSDF, RefractionBSDF, Transparent, Blackhole, Mixed
                    (Fresnel and Constant fac) and a pointLight as light 0
+  c0_ortho_film.npz
+                   config 0 through the OrthographicLens (lens.hpp:40-53)
   shaders.npz      Shader::execute of each reference shader (nested Mixed
                    included) on scripted draws: for shared records
                    {wo, wi, u[12]} the f, emission and draw count of
                    compute_f_by_wi_wo and the wi, f, emission and draw count
                    of sample_wi_f_by_wo (the harness's `shade` command)
 
-Usage:  python tests/golden/make_golden.py [--aov-only | --materials-only]
+Usage:  python tests/golden/make_golden.py [--aov-only | --materials-only | --ortho-only]
 (the harness's render threads take rows dynamically, so a film regenerated
 from the same seed is a different Monte Carlo draw of the same image)
 """
@@ -168,6 +170,16 @@ def make_shaders(tmp):
                         configs=json.dumps(shader_configs()))
 
 
+def make_ortho(tmp):
+    d = scenes.config0_ortho()
+    scenes.write_scene(d, tmp)
+    run("render", f"{d.name}.json", FILM_W, FILM_H, FILM_SPP, os.cpu_count(), "film.crf", d.max_bounce, 59, cwd=tmp)
+    film = oracle.read_crf(os.path.join(tmp, "film.crf"))
+    np.savez_compressed(os.path.join(HERE, "c0_ortho_film.npz"), sum=film.sum, sumsq=film.sumsq, count=film.count,
+                        width=FILM_W, height=FILM_H, spp=FILM_SPP, max_bounce=d.max_bounce,
+                        scene_hash=scene_hash(d, full=True), lens=d.camera["lens"])
+
+
 def make_materials(tmp):
     m = scenes.config_materials()
     scenes.write_scene(m, tmp)
@@ -185,13 +197,16 @@ def make_materials(tmp):
                         scene_hash=scene_hash(m, full=True))
 
 
-def main(aov_only=False, materials_only=False):
+def main(aov_only=False, materials_only=False, ortho_only=False):
     if not oracle.ref_available():
         sys.exit("build the reference harness first: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
         if materials_only:
             make_shaders(tmp)
             make_materials(tmp)
+            return
+        if ortho_only:
+            make_ortho(tmp)
             return
         c0 = scenes.config0()
         scenes.write_scene(c0, tmp)
@@ -245,4 +260,5 @@ def main(aov_only=False, materials_only=False):
 
 
 if __name__ == "__main__":
-    main(aov_only="--aov-only" in sys.argv, materials_only="--materials-only" in sys.argv)
+    main(aov_only="--aov-only" in sys.argv, materials_only="--materials-only" in sys.argv,
+         ortho_only="--ortho-only" in sys.argv)

@@ -84,6 +84,9 @@ def test_shader_registry_and_errors(cr):
         pos = np.array([1, 2, 3], np.float32)
         assert lib.cr_scene_add_point_light(h, C.c_void_p(pos.ctypes.data), None, 2.0) == 0
         assert lib.cr_scene_add_point_light(h, None, None, 2.0) == -1
+        # CameraConfig::lens (config.hpp:14-27)
+        assert lib.cr_scene_set_lens(h, 1) == 0 and lib.cr_scene_set_lens(h, 0) == 0
+        assert lib.cr_scene_set_lens(h, 2) == -1
     finally:
         lib.cr_scene_destroy(h)
 

@@ -47,6 +47,22 @@ def test_device_shader_execute_matches_reference(cr, index):
             np.testing.assert_allclose(a[same], b[same], rtol=0, atol=tol)
 
 
+def test_device_math_kats(cr):
+    """test/math.cu:6-29 (refract both ways, Fresnel at ior 1.4) through the
+    device shaders, as the oracle's known-answer test reaches them."""
+    require_gpu()
+    from test_oracle_kats import FRESNEL, MATH_KATS, REFRACT, math_kat_inputs
+    wo, u, wo_fr, u_fr = math_kat_inputs()
+    f, wi, _, used = cr.shader_execute(REFRACT, cr.SHADE_SAMPLE, wo, u)
+    assert np.all(used == 3)
+    np.testing.assert_allclose(wi[0], MATH_KATS["refract_in"][1], atol=1e-4)
+    np.testing.assert_allclose(wi[1], MATH_KATS["refract_out"][1], atol=1e-4)
+    np.testing.assert_allclose(f[:, 0], [1.33 ** 2, 1.0], rtol=1e-6)
+    f, wi, _, _ = cr.shader_execute(FRESNEL, cr.SHADE_SAMPLE, wo_fr, u_fr)
+    assert np.all(f[0] == 1) and np.allclose(wi[0], -wo_fr[0], atol=1e-7)
+    assert np.all(f[1] == 0)
+
+
 # Caustics through the glass spheres (a Lambert floor vertex, two refractions
 # with the reference's 1/eta^2 gain, then the emitter) make the image mean
 # heavy-tailed: across oracle seeds at 512 spp it spreads by +-0.7%, about

@@ -56,6 +56,23 @@ def test_koishi_render_matches_reference(cr, c0_scene):
     assert abs(f4.mean.mean() / ref.mean.mean() - 1) < 0.01
 
 
+def test_orthographic_render_matches_reference(cr, scenes):
+    """The OrthographicLens (lens.hpp:40-53) against the reference's own render."""
+    g = golden("c0_ortho_film.npz")
+    W, H, spp, mb = int(g["width"]), int(g["height"]), int(g["spp"]), int(g["max_bounce"])
+    ref = O.Film(g["sum"], g["sumsq"], g["count"])
+    f = render_film(cr, cr.Scene.from_desc(scenes.config0_ortho()), W, H, spp, seeds=[13], estimator=cr.KOISHI,
+                    max_bounce=mb)
+    z = zscores(f, ref)
+    assert (z > 3).mean() < 0.01 and z.max() < 5.5, ((z > 3).mean(), z.max())
+    assert abs(f.mean.mean() / ref.mean.mean() - 1) < 0.01
+    # the MIS estimator takes the lens too
+    o = O.OracleScene(scenes.config0_ortho()).render(24, 24, 256, 7, O.MIS, seed=3)
+    m = render_film(cr, cr.Scene.from_desc(scenes.config0_ortho()), 24, 24, 256, seeds=[17, 18], estimator=cr.MIS)
+    zm = zscores(m, o)
+    assert (zm > 3).mean() < 0.01 and zm.max() < 5.5, ((zm > 3).mean(), zm.max())
+
+
 def test_mis_render_matches_oracle(cr, scenes, c0_scene):
     d = scenes.config0()
     W, H, spp = 32, 32, 256

@@ -102,3 +102,17 @@ def test_debug_kernels_match_reference(oracle, c0, kernel):
         z = np.abs(f.mean - ref.mean) / np.sqrt(f.var_of_mean + ref.var_of_mean + floor + 1e-30)
         assert (z > 3).mean() < 0.01, (z > 3).mean()
         assert abs(f.mean.mean() / ref.mean.mean() - 1) < 0.01
+
+
+def test_orthographic_render_matches_reference(oracle, scenes):
+    """OrthographicLens::sample (lens.hpp:40-53) through the reference's own
+    render of config 0 (tests/golden/c0_ortho_film.npz)."""
+    g = golden("c0_ortho_film.npz")
+    d = scenes.config0_ortho()
+    assert str(g["scene_hash"]) == scene_hash(d, full=True) and str(g["lens"]) == "orthographic"
+    W, H, spp = int(g["width"]), int(g["height"]), int(g["spp"])
+    f = oracle.OracleScene(d).render(W, H, spp, int(g["max_bounce"]), oracle.KOISHI, seed=61)
+    ref = oracle.Film(g["sum"], g["sumsq"], g["count"])
+    z = np.abs(f.mean - ref.mean) / np.sqrt(f.var_of_mean + ref.var_of_mean + 1e-30)
+    assert (z > 3).mean() < 0.01 and (z > 5).mean() == 0, ((z > 3).mean(), z.max())
+    assert abs(f.mean.mean() / ref.mean.mean() - 1) < 0.01
