@@ -75,7 +75,7 @@ class GuideConfig(C.Structure):
     """cr_guide_config: the guide's training schedule."""
     _fields_ = [("lr", C.c_float), ("select_prob", C.c_float), ("train_paths", C.c_uint32),
                 ("steps_per_wave", C.c_uint32), ("warmup_steps", C.c_uint32), ("product_target", C.c_uint32),
-                ("max_steps", C.c_uint32)]
+                ("max_steps", C.c_uint32), ("guided_bounces", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -2086,6 +2086,7 @@ int cr_guide_configure( cr_scene *s, const cr_guide_config *in, cr_guide_config 
 			g.steps_per_wave = in->steps_per_wave, g.warmup_steps = in->warmup_steps;
 			g.product_target = in->product_target != 0;
 			g.max_steps = in->max_steps;
+			g.guided_bounces = in->guided_bounces;
 		}
 		if ( out )
 		{
@@ -2093,6 +2094,7 @@ int cr_guide_configure( cr_scene *s, const cr_guide_config *in, cr_guide_config 
 			out->steps_per_wave = g.steps_per_wave, out->warmup_steps = g.warmup_steps;
 			out->product_target = g.product_target ? 1u : 0u;
 			out->max_steps = g.max_steps;
+			out->guided_bounces = g.guided_bounces;
 		}
 	} );
 }

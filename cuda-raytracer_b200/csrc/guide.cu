@@ -597,6 +597,7 @@ GuideDev GuideState::dev() const
 {
 	GuideDev g;
 	g.grid = grid, g.W = W, g.b = b, g.bmin = bmin, g.binv = binv, g.select_prob = select_prob;
+	g.guided_bounces = guided_bounces;
 	return g;
 }
 

@@ -27,7 +27,16 @@ struct GuideDev
 	const float *b;      // [G_LAYERS][64] biases
 	float3 bmin, binv;   // scene box: x -> (x - bmin) * binv in [0,1]^3
 	float select_prob;   // probability of sampling the guide at a vertex
+	uint32_t guided_bounces;  // vertices 0 .. guided_bounces-1 sample the guide (0: all)
 };
+
+// Whether vertex `bounce` of a path of at most max_bounce + 1 vertices
+// samples the guide: the guide shapes continuations only, so never the last
+// vertex, and only the first guided_bounces vertices when that is set.
+__host__ __device__ __forceinline__ bool guided_vertex( const GuideDev &g, uint32_t bounce, uint32_t max_bounce )
+{
+	return bounce < max_bounce && ( g.guided_bounces == 0 || bounce < g.guided_bounces );
+}
 
 // Luminance (Rec. 709 weights): the scalar the guide's training weights use.
 __host__ __device__ __forceinline__ float lum( float3 c ) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
@@ -160,10 +169,36 @@ __device__ __forceinline__ float mixture_pdf( const Lobe *lb, float3 w )
 	return p;
 }
 
+// A mixture prepared for repeated evaluation at one vertex: per lobe the mean,
+// the weight, kappa log2(e) and log2(weight * vMF normaliser), so that the
+// density costs one exp2 per lobe.
+struct PreparedLobe
+{
+	float3 mu;
+	float weight, k2, c;
+};
+
+__device__ __forceinline__ void prepare_lobe( const Lobe &l, PreparedLobe &p )
+{
+	const float norm = l.kappa / ( 2.f * PI_F * ( -expm1f( -2.f * l.kappa ) ) );
+	p.mu = l.mu, p.weight = l.weight;
+	p.k2 = l.kappa * 1.4426950408889634f;
+	p.c = log2f( l.weight * norm );  // -inf for a lobe of weight 0
+}
+
+// mixture_pdf of the prepared lobes.
+__device__ __forceinline__ float prepared_pdf( const PreparedLobe *lb, float3 w )
+{
+	float p = 0.f;
+#pragma unroll
+	for ( int k = 0; k < G_LOBES; ++k ) p += exp2f( fmaf( lb[ k ].k2, dot( lb[ k ].mu, w ) - 1.f, lb[ k ].c ) );
+	return p;
+}
+
 // Sample the mixture: lobe by weight (u0), then a vMF direction with the
 // numerically stable inversion of Jakob ("Numerically stable sampling of the
 // von Mises Fisher distribution on S2", 2012).
-__device__ __forceinline__ float3 mixture_sample( const Lobe *lb, float u0, float u1, float u2 )
+__device__ __forceinline__ float3 mixture_sample( const PreparedLobe *lb, float u0, float u1, float u2 )
 {
 	int k = 0;
 	float acc = 0.f;
@@ -172,8 +207,9 @@ __device__ __forceinline__ float3 mixture_sample( const Lobe *lb, float u0, floa
 		acc += lb[ k ].weight;
 		if ( u0 < acc ) break;
 	}
-	const Lobe &l = lb[ k ];
-	float w = 1.f + logf( u1 + ( 1.f - u1 ) * expf( -2.f * l.kappa ) ) / l.kappa;
+	const PreparedLobe &l = lb[ k ];
+	const float kappa = l.k2 * 0.6931471805599453f;
+	float w = 1.f + logf( u1 + ( 1.f - u1 ) * expf( -2.f * kappa ) ) / kappa;
 	w = fminf( fmaxf( w, -1.f ), 1.f );
 	float r = sqrtf( fmaxf( 0.f, 1.f - w * w ) ), s, c;
 	sincosf( 2.f * PI_F * u2, &s, &c );

@@ -40,7 +40,8 @@ struct GuideState
 	uint32_t steps_per_wave = 2;    // batches (Adam steps) recorded and trained per wave
 	uint32_t warmup_steps = 8;      // steps before the guide is first sampled
 	bool product_target = true;     // fit Li * f * cos (the integrand) instead of Li
-	uint32_t max_steps = 0;         // training budget in Adam steps (0: train every wave)
+	uint32_t max_steps = 600;       // training budget in Adam steps (0: train every wave)
+	uint32_t guided_bounces = 3;    // leading vertices that sample the guide (0: all but the last)
 	uint32_t packed_step = ~0u;     // step whose weights Wp holds (~0: none)
 	GuideRecords rec;
 	uint32_t rec_capacity = 0;

@@ -402,8 +402,9 @@ __device__ __forceinline__ void store_lobes( uint4 *dst, const Lobe *lb )
 	for ( int j = 0; j < 5; ++j ) dst[ j ] = make_uint4( h[ 4 * j ], h[ 4 * j + 1 ], h[ 4 * j + 2 ], h[ 4 * j + 3 ] );
 }
 
-__device__ __forceinline__ void load_lobes( const uint4 *src, Lobe *lb )
+__device__ __forceinline__ void load_lobes( const uint4 *src, PreparedLobe *pl )
 {
+	Lobe lb[ G_LOBES ];
 	float v[ 5 * G_LOBES ];
 #pragma unroll
 	for ( int j = 0; j < 5; ++j )
@@ -430,7 +431,11 @@ __device__ __forceinline__ void load_lobes( const uint4 *src, Lobe *lb )
 	}
 	const float inv = wsum > 0.f ? 1.f / wsum : 0.f;
 #pragma unroll
-	for ( int k = 0; k < G_LOBES; ++k ) lb[ k ].weight = wsum > 0.f ? lb[ k ].weight * inv : 1.f / G_LOBES;
+	for ( int k = 0; k < G_LOBES; ++k )
+	{
+		lb[ k ].weight = wsum > 0.f ? lb[ k ].weight * inv : 1.f / G_LOBES;
+		prepare_lobe( lb[ k ], pl[ k ] );
+	}
 }
 
 __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
@@ -466,9 +471,8 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	Frame fr = onb_frame( s.ns );
 	float3 wo = fr.local( -d );
 	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
-	Lobe lb[ G_LOBES ];
-	// the guide shapes continuations only: none follows the last vertex
-	const bool guided = cfg.guide_sample && bounce < cfg.max_bounce;
+	PreparedLobe lb[ G_LOBES ];
+	const bool guided = cfg.guide_sample && guided_vertex( cfg.guide, bounce, cfg.max_bounce );
 	const float sel = guided ? cfg.guide.select_prob : 0.f;
 	if ( guided ) load_lobes( lobes, lb );
 	if ( sc.n_lights )
@@ -491,7 +495,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 			float pb;
 			float3 f = mis_eval( sh, wo, wi, pb );
 			// one-sample MIS of guide and BSDF: the continuation density
-			if ( guided ) pb = sel * mixture_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
+			if ( guided ) pb = sel * prepared_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
 			if ( !is_zero( f ) )
 			{
 				// the last vertex has no continuation that could reach the light:
@@ -535,7 +539,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		}
 		float pb;
 		float3 f = mis_eval( sh, wo, wi, pb );
-		pdf = sel * mixture_pdf( lb, nd ) + ( 1.f - sel ) * pb;
+		pdf = sel * prepared_pdf( lb, nd ) + ( 1.f - sel ) * pb;
 		wt = pdf > 0.f ? f * ( wi.z / pdf ) : f3( 0.f, 0.f, 0.f );
 	}
 	else
@@ -1218,7 +1222,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				else
 					k_traverse<ExtendIO, false, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 			} );
-			if ( wc.guide_sample && b < cfg.max_bounce )
+			if ( wc.guide_sample && guided_vertex( wc.guide, b, cfg.max_bounce ) )
 				timed( 4, [&] {
 					k_guide_infer<<<sms * 2, tc::THREADS, tc::SMEM_BYTES, st>>>( sc, wc, wb, b, guide->Wp );
 				} );

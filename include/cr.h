@@ -338,7 +338,11 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   product_target  1: fit the integrand Li f cos at each vertex; 0: fit the
  *                   incident (indirect) radiance Li alone [1]
  *   max_steps       training budget: after this many Adam steps renders sample
- *                   the guide without recording or training (0: no budget) [0] */
+ *                   the guide without recording or training (0: no budget) [600]
+ *   guided_bounces  vertices 0 .. guided_bounces-1 of a path sample the guide
+ *                   (and only their bounces run the guide's inference); later
+ *                   vertices sample the BSDF alone (0: every vertex but the
+ *                   last) [3] */
 typedef struct cr_guide_config {
     float lr;
     float select_prob;
@@ -347,6 +351,7 @@ typedef struct cr_guide_config {
     uint32_t warmup_steps;
     uint32_t product_target;
     uint32_t max_steps;
+    uint32_t guided_bounces;
 } cr_guide_config;
 /* Apply `in` (when not NULL) and report the schedule in `out` (when not NULL). */
 int cr_guide_configure(cr_scene *s, const cr_guide_config *in, cr_guide_config *out);

@@ -90,7 +90,7 @@ def test_guide_configure_validates(guided):
     import cuda_raytracer_b200 as crm
     cfg = g.configure()
     assert cfg["train_paths"] == 32768 and cfg["steps_per_wave"] == 2 and cfg["warmup_steps"] == 8
-    assert cfg["product_target"] == 1
+    assert cfg["product_target"] == 1 and cfg["max_steps"] == 600 and cfg["guided_bounces"] == 3
     for bad in ({"lr": 0.0}, {"select_prob": 1.0}, {"train_paths": 0}, {"steps_per_wave": 65}):
         with pytest.raises(crm.CrError):
             g.configure(**bad)
@@ -146,15 +146,18 @@ def test_tc_gradients_match_fp64(guided):
         assert exact < 0.15, (name, errs)
 
 
-def test_guided_render_is_unbiased(cr, scenes):
+@pytest.mark.parametrize("guided_bounces", [3, 0, 1])
+def test_guided_render_is_unbiased(cr, scenes, guided_bounces):
     """Guided MIS and plain MIS films agree within 3 sigma: one-sample MIS of
     the learned mixture with the BSDF keeps the estimator unbiased while the
-    guide trains online during the render."""
+    guide trains online during the render, whichever vertices (the first 3,
+    all but the last, the first) sample the guide."""
     require_gpu()
     d = scenes.config0()
     s = cr.Scene.from_desc(d)
     gd = cr.Guide(s).reset(seed=3)
-    gd.configure(steps_per_wave=2, warmup_steps=4)  # sample the guide from the third wave on
+    # sample the guide from the third wave on
+    gd.configure(steps_per_wave=2, warmup_steps=4, guided_bounces=guided_bounces)
     W, H, spp = 32, 32, 256
     plain = render_film(cr, s, W, H, spp, seeds=[21, 22], estimator=cr.MIS)
     import torch
