@@ -242,7 +242,11 @@ struct VertexRng
 	uint32_t bounce, blk;
 	float4 b;
 	int i;
-	__device__ __forceinline__ VertexRng( uint2 k, uint64_t s, uint32_t bn ) : key( k ), g( s ), bounce( bn ), blk( 0 ), i( 4 ) {}
+	// b0: block 0, already drawn; start: draws of it already taken
+	__device__ __forceinline__ VertexRng( uint2 k, uint64_t s, uint32_t bn, float4 b0, int start )
+		: key( k ), g( s ), bounce( bn ), blk( 1 ), b( b0 ), i( start )
+	{
+	}
 	__device__ __forceinline__ float next()
 	{
 		if ( i == 4 ) b = rand4( key, g, bounce, blk++ ), i = 0;
@@ -323,90 +327,113 @@ __device__ __forceinline__ int koishi_leaf( const DevShader *tab, int idx, float
 	return idx;
 }
 
-// Koishi estimator, compute_f_by_wi_wo of table entry idx: Lambert
-// (lambert.hpp:31-33), GlossyBSDF (glossy.hpp:27-29), Emission as white
-// Lambert that also sets the varyings' emission (emission.hpp:22-27),
-// GlassBSDF (glass.hpp:25-53: a Fresnel draw picks the reflection or the
-// transmission half-vector), and zero for Transparent (transparent.hpp:24-26),
-// Blackhole (blackhole.hpp:17-20) and RefractionBSDF (refraction.hpp:35-38).
-template <class Rng>
-__device__ __forceinline__ float3 koishi_eval( const DevShader *tab, int idx, float3 wo, float3 wi, Rng &rng,
-											   float3 &emission )
+// compute_f_by_wi_wo of a shader that draws no selection number (all but
+// Mixed and GlassBSDF): Lambert (lambert.hpp:31-33), GlossyBSDF
+// (glossy.hpp:27-29), Emission as white Lambert that also sets the varyings'
+// emission (emission.hpp:22-27), and zero for Transparent
+// (transparent.hpp:24-26), Blackhole (blackhole.hpp:17-20) and
+// RefractionBSDF (refraction.hpp:35-38).
+__device__ __forceinline__ float3 leaf_eval( const DevShader &sh, float3 wo, float3 wi, float3 &emission )
 {
-	const DevShader &sh = tab[ koishi_leaf( tab, idx, wo, rng ) ];
-	emission = f3( 0.f, 0.f, 0.f );
+	emission = sh.type == SH_EMISSION ? f3( sh.emission ) : f3( 0.f, 0.f, 0.f );
 	switch ( sh.type )
 	{
-	case SH_EMISSION:
-		emission = f3( sh.emission );
-		// fall through: Emission shades as white Lambert
 	case SH_LAMBERT:
+	case SH_EMISSION:
 		return wi.z >= 0.f ? f3( sh.albedo ) * ( 1.0f / PI_F ) : f3( 0.f, 0.f, 0.f );
 	case SH_GLOSSY:
 		return f3( sh.color ) * dist_f( sh, normalize( wo + wi ) );
-	case SH_GLASS:
-		if ( rng.next() < fresnel_fac( sh.ior, wo ) ) return f3( sh.color ) * dist_f( sh, normalize( wo + wi ) );
-		return f3( sh.color ) * dist_f( sh, normalize( wo + wi * sh.ior ) );
 	default:
 		return f3( 0.f, 0.f, 0.f );
 	}
 }
 
 // The transmission half of RefractionBSDF and GlassBSDF (refraction.hpp:24-33,
-// glass.hpp:40-49): a half-vector from the distribution, flipped to wo's side,
-// refracts wo; f = color scaled by 1/eta^2 when entering.  wi is left as it
-// was when the refraction fails (f = 0).
-template <class Rng>
-__device__ __forceinline__ float3 koishi_refract( const DevShader &sh, float3 wo, Rng &rng, float3 &wi )
+// glass.hpp:40-49) for a half-vector h from the distribution: flipped to wo's
+// side, it refracts wo; f = color scaled by 1/eta^2 when entering.  wi is
+// left as it was when the refraction fails (f = 0).
+__device__ __forceinline__ float3 koishi_refract( const DevShader &sh, float3 wo, float3 h, float3 &wi )
 {
-	float3 h = dist_sample( sh, rng );
 	const float eta = wo.z > 0.f ? 1.f / sh.ior : sh.ior;
 	if ( wo.z < 0.f ) h = -h;
 	if ( !refract_dir( wo, h, eta, wi ) ) return f3( 0.f, 0.f, 0.f );
 	return f3( sh.color ) / ( eta < 1.f ? eta * eta : 1.f );
 }
 
-// Koishi estimator, sample_wi_f_by_wo of table entry idx: Lambert
-// (lambert.hpp:26-30 with cosine.hpp:18-23: f = color * R), GlossyBSDF
-// (glossy.hpp:22-26), Transparent (wi = -wo, f = color), Blackhole
-// (wi = +z, f = 0), RefractionBSDF and GlassBSDF (glass.hpp:25-49).  Returns
-// f; the caller multiplies by |cos|.  wi is in/out (see koishi_refract);
-// emission is what the leaf writes to the varyings (Emission only).
-template <class Rng>
-__device__ __forceinline__ float3 koishi_sample( const DevShader *tab, int idx, float3 wo, Rng &rng, float3 &wi,
-												 float3 &emission )
+// sample_wi_f_by_wo of a shader that draws no selection number, given the
+// first two numbers (u1, u2) of its sampler.sample3() (Transparent and
+// Blackhole draw none): Lambert (lambert.hpp:26-30 with cosine.hpp:18-23:
+// f = color * R), GlossyBSDF (glossy.hpp:22-26), Transparent (wi = -wo,
+// f = color), Blackhole (wi = +z, f = 0), RefractionBSDF.  Returns f; the
+// caller multiplies by |cos|.  wi is in/out (see koishi_refract); emission is
+// what the shader writes to the varyings (Emission only).
+__device__ __forceinline__ float3 leaf_sample( const DevShader &sh, float3 wo, float u1, float u2, float3 &wi,
+											   float3 &emission )
 {
-	const DevShader &sh = tab[ koishi_leaf( tab, idx, wo, rng ) ];
 	emission = sh.type == SH_EMISSION ? f3( sh.emission ) : f3( 0.f, 0.f, 0.f );
 	switch ( sh.type )
 	{
 	case SH_LAMBERT:
 	case SH_EMISSION:
-	{
-		const float u1 = rng.next(), u2 = rng.next();
-		rng.next();
 		wi = sample_cos( u1, u2 );
 		return wi.z >= 0.f ? f3( sh.albedo ) : f3( 0.f, 0.f, 0.f );
-	}
 	case SH_GLOSSY:
-		wi = reflect( wo, dist_sample( sh, rng ) );
+		wi = reflect( wo, sh.dist == DIST_COSINE ? sample_cos( u1, u2 ) : beckmann_sample( sh.alpha2, u1, u2 ) );
 		return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
 	case SH_TRANSPARENT:
 		wi = -wo;
 		return f3( sh.color );
 	case SH_REFRACTION:
-		return koishi_refract( sh, wo, rng, wi );
-	case SH_GLASS:
-		if ( rng.next() < fresnel_fac( sh.ior, wo ) )
-		{
-			wi = reflect( wo, dist_sample( sh, rng ) );
-			return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
-		}
-		return koishi_refract( sh, wo, rng, wi );
+		return koishi_refract( sh, wo, sh.dist == DIST_COSINE ? sample_cos( u1, u2 ) : beckmann_sample( sh.alpha2, u1, u2 ),
+							   wi );
 	default:  // Blackhole
 		wi = f3( 0.f, 0.f, 1.f );
 		return f3( 0.f, 0.f, 0.f );
 	}
+}
+
+// Whether a shader draws numbers in its sample_wi_f_by_wo (sampler.sample3()).
+__device__ __forceinline__ bool samples_draw( int type ) { return type != SH_TRANSPARENT && type != SH_BLACKHOLE; }
+
+// Koishi estimator, compute_f_by_wi_wo of table entry idx with the draws the
+// reference makes: one per Mixed on the way to the leaf, and GlassBSDF's
+// Fresnel draw picking the reflection or the transmission half-vector
+// (glass.hpp:25-53).
+template <class Rng>
+__device__ __forceinline__ float3 koishi_eval( const DevShader *tab, int idx, float3 wo, float3 wi, Rng &rng,
+											   float3 &emission )
+{
+	const DevShader &sh = tab[ koishi_leaf( tab, idx, wo, rng ) ];
+	if ( sh.type != SH_GLASS ) return leaf_eval( sh, wo, wi, emission );
+	emission = f3( 0.f, 0.f, 0.f );
+	if ( rng.next() < fresnel_fac( sh.ior, wo ) ) return f3( sh.color ) * dist_f( sh, normalize( wo + wi ) );
+	return f3( sh.color ) * dist_f( sh, normalize( wo + wi * sh.ior ) );
+}
+
+// Koishi estimator, sample_wi_f_by_wo of table entry idx with the draws the
+// reference makes (Mixed selections, GlassBSDF's Fresnel draw, then the
+// shader's sampler.sample3()).
+template <class Rng>
+__device__ __forceinline__ float3 koishi_sample( const DevShader *tab, int idx, float3 wo, Rng &rng, float3 &wi,
+												 float3 &emission )
+{
+	const DevShader &sh = tab[ koishi_leaf( tab, idx, wo, rng ) ];
+	if ( sh.type == SH_GLASS )
+	{
+		emission = f3( 0.f, 0.f, 0.f );
+		const bool refl = rng.next() < fresnel_fac( sh.ior, wo );
+		const float3 h = dist_sample( sh, rng );
+		if ( !refl ) return koishi_refract( sh, wo, h, wi );
+		wi = reflect( wo, h );
+		return wo.z * wi.z > 0.f ? f3( sh.color ) : f3( 0.f, 0.f, 0.f );
+	}
+	float u1 = 0.5f, u2 = 0.5f;
+	if ( samples_draw( sh.type ) )
+	{
+		u1 = rng.next(), u2 = rng.next();
+		rng.next();
+	}
+	return leaf_sample( sh, wo, u1, u2, wi, emission );
 }
 
 // MIS estimator BSDFs: Lambert albedo/pi with cosine pdf; Beckmann microfacet

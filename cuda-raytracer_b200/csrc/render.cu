@@ -60,19 +60,35 @@ __device__ __forceinline__ uint32_t warp_append( bool want, uint32_t *counter )
 // PinholeLens (:56-66) shoots from the camera through the stratified point on
 // the image plane; OrthographicLens (:40-53) moves the origin by that plane
 // offset times 4 / width and shoots along the view direction.
+// The products and sums are written as explicit fused multiply-adds so that
+// every kernel that generates camera rays (single and batched renders) forms
+// bit-identical rays, whatever the compiler would contract in each context.
+__device__ __forceinline__ float3 fma3( float3 a, float s, float3 b )
+{
+	return f3( fmaf( a.x, s, b.x ), fmaf( a.y, s, b.y ), fmaf( a.z, s, b.z ) );
+}
+
+__device__ __forceinline__ float3 normalize_fma( float3 a )
+{
+	const float l2 = fmaf( a.x, a.x, fmaf( a.y, a.y, __fmul_rn( a.z, a.z ) ) );
+	return a * ( 1.0f / sqrtf( l2 ) );
+}
+
 __device__ __forceinline__ void camera_ray( const DevCamera &c, uint32_t x, uint32_t y, uint32_t k, float3 &o, float3 &d )
 {
 	const float fx = float( x ) - float( c.width ) * 0.5f, fy = float( y ) - float( c.height ) * 0.5f;
+	const float kx = float( k % c.pw ), ky = float( k / c.pw );
 	if ( c.lens == 1 )
 	{
-		const float3 p = f3( c.u ) * fx + f3( c.v ) * fy + ( f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
-		o = f3( c.o ) + p * 4.f / float( c.width );
-		d = normalize( f3( c.n ) );
+		const float3 p = fma3( f3( c.v ), fy, fma3( f3( c.u ), fx, fma3( f3( c.dv ), ky, fma3( f3( c.du ), kx, f3( 0.f, 0.f, 0.f ) ) ) ) );
+		const float s = 4.f / float( c.width );
+		o = fma3( p, s, f3( c.o ) );
+		d = normalize_fma( f3( c.n ) );
 		return;
 	}
-	const float3 t = f3( c.n ) + f3( c.u ) * fx + f3( c.v ) * fy;
+	const float3 t = fma3( f3( c.v ), fy, fma3( f3( c.u ), fx, f3( c.n ) ) );
 	o = f3( c.o );
-	d = normalize( t + f3( c.du ) * float( k % c.pw ) + f3( c.dv ) * float( k / c.pw ) );
+	d = normalize_fma( fma3( f3( c.dv ), ky, fma3( f3( c.du ), kx, t ) ) );
 }
 
 __global__ void k_generate( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa )
@@ -314,7 +330,11 @@ __device__ __forceinline__ void koishi_light_sample( const DevScene &sc, const D
 }
 
 // One vertex of RadianceKernel::execute (radiance.cu:22-71), reference
-// semantics, with the vertex's uniforms drawn in the reference's order.
+// semantics.  The vertex's numbers come in the reference's order: light
+// choice and light point (draws 0-2, also reserved when the scene has no
+// light), then the shaders' draws and the Russian roulette draw.  A shader
+// without selection draws (all but Mixed and GlassBSDF) takes a fixed layout:
+// sample3 = draws 3-5, roulette = draw 6.
 __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
 											  uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
 											  float4 &L4, PathOut &out )
@@ -324,15 +344,18 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 	Frame fr = koishi_frame( s.ns );
 	float3 wo = fr.local( -d );
 	float3 beta = f3( beta4 ), L = f3( L4 );
-	VertexRng rng( key, g, bounce );
+	const DevShader sh = sc.shaders[ s.shader ];
+	const bool simple = sh.type != SH_MIXED && sh.type != SH_GLASS;
+	const float4 r0 = rand4( key, g, bounce, 0 );
+	VertexRng rng( key, g, bounce, r0, 3 );
 	float3 wi = f3( 0.f, 0.f, 0.f );
 	if ( sc.n_lights )
 	{
 		uint32_t nl = sc.n_lights;
-		uint32_t idx = min( uint32_t( floorf( rng.next() * float( nl ) ) ), nl - 1 );
+		uint32_t idx = min( uint32_t( floorf( r0.x * float( nl ) ) ), nl - 1 );
 		float lpdf = 1.f / float( nl );
 		const DevLight lt = sc.lights[ idx ];
-		const float ux = rng.next(), uy = rng.next();
+		const float ux = r0.y, uy = r0.z;
 		float3 lp, li;
 		koishi_light_sample( sc, lt, s.p, ux, uy, lp, li );
 		float3 dd = lp - s.p;   // LocalVaryings::emitSeg (varyings.hpp:27-37)
@@ -342,7 +365,7 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 		float st = length( dd - 2.f * diff );
 		wi = fr.local( normalize( lp - s.p ) );
 		float3 emission;
-		float3 f = koishi_eval( sc.shaders, s.shader, wo, wi, rng, emission );
+		float3 f = simple ? leaf_eval( sh, wo, wi, emission ) : koishi_eval( sc.shaders, s.shader, wo, wi, rng, emission );
 		float3 c = beta * f * li * ( fabsf( wi.z ) / lpdf );
 		if ( !finite3( c ) )
 			L = f3( NAN, NAN, NAN );
@@ -355,8 +378,19 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 		}
 		L = L + beta * emission;  // radiance.cu:39
 	}
-	float3 emission_s;
-	float3 f = koishi_sample( sc.shaders, s.shader, wo, rng, wi, emission_s );  // radiance.cu:55-60
+	float3 emission_s, f;
+	float u_rr;
+	if ( simple )
+	{
+		const float4 r1 = rand4( key, g, bounce, 1 );
+		f = leaf_sample( sh, wo, r0.w, r1.x, wi, emission_s );  // radiance.cu:55-60
+		u_rr = r1.z;
+	}
+	else
+	{
+		f = koishi_sample( sc.shaders, s.shader, wo, rng, wi, emission_s );
+		u_rr = rng.next();
+	}
 	beta = beta * f * fabsf( wi.z );
 	float3 nd = fr.global( wi );
 	float3 no = s.p + nd * KOISHI_EPS;
@@ -365,7 +399,7 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 	if ( rr < 1.f && bounce > 3 )
 	{
 		float q = fmaxf( .05f, 1.f - rr );
-		if ( rng.next() < q )
+		if ( u_rr < q )
 			alive = false;
 		else
 			beta = beta / ( 1.f - q );
@@ -624,7 +658,9 @@ __global__ void k_generate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa )
 
 // BATCH: the wave mixes several jobs; each path shades in its job's scene with
 // its job's random key, and `sc` and `key` are unused.
-template <bool BATCH>
+// One instantiation per estimator, so that the reference estimator's shading
+// is not held to the registers of the guided MIS shading.
+template <bool BATCH, int EST>
 __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
 												  uint32_t bounce, uint2 key, BatchDev bd )
 {
@@ -671,7 +707,7 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 					const BatchJobDev &job = bd.jobs[ j ];
 					const uint2 jkey = philox_key( job.seed + *bd.seed_offset );
 					const uint64_t g = gw - job.first_sample;
-					if ( cfg.estimator == EST_MIS )
+					if constexpr ( EST == EST_MIS )
 						shade_mis( bd.scenes[ j ], cfg, jkey, g, bounce, ro, rd, h, beta, L, out, nullptr, 0xFFFFFFFFu );
 					else
 						shade_koishi( bd.scenes[ j ], cfg, jkey, g, bounce, ro, rd, h, beta, L, out );
@@ -680,7 +716,7 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 				{
 					uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
 					uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
-					if ( cfg.estimator == EST_MIS )
+					if constexpr ( EST == EST_MIS )
 						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
 								   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 : nullptr,
 								   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
@@ -1089,7 +1125,12 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 				k_traverse<BatchExtendIO, false, false><<<g_ext, 128, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err, wb.work,
 																			   cfg.refill_min );
 			} );
-			timed( 2, [&] { k_shade<true><<<g_shade, 128, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd ); } );
+			timed( 2, [&] {
+				if ( cfg.estimator == EST_MIS )
+					k_shade<true, EST_MIS><<<g_shade, 128, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
+				else
+					k_shade<true, EST_KOISHI><<<g_shade, 128, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
+			} );
 			timed( 1, [&] {
 				BatchShadowIO io;
 				io.queue = wb.shadow_queue, io.ray_o = wb.sh_o, io.ray_d = wb.sh_d, io.contrib = wb.sh_c, io.L = wb.L;
@@ -1229,7 +1270,12 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 			if ( cfg.kernel != KERNEL_RADIANCE )
 				timed( 2, [&] { k_aov<<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, key ); } );
 			else
-				timed( 2, [&] { k_shade<false><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} ); } );
+				timed( 2, [&] {
+					if ( cfg.estimator == EST_MIS )
+						k_shade<false, EST_MIS><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+					else
+						k_shade<false, EST_KOISHI><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+				} );
 			if ( sc.n_lights && cfg.kernel != KERNEL_NORMAL && cfg.kernel != KERNEL_HALFVECTOR )
 				timed( 1, [&] {
 					ShadowIO io{ wb.shadow_queue, wb.sh_o, wb.sh_d, wb.sh_c, wb.L };
