@@ -60,8 +60,8 @@ __host__ __device__ __forceinline__ uint32_t grid_index( int l, uint32_t ix, uin
 	return ( ix * 1u ^ iy * 2654435761u ^ iz * 805459861u ) & uint32_t( G_T - 1 );
 }
 
-// Real spherical harmonics up to degree 3 of a unit vector (16 terms),
-// orthonormal basis.
+// Real spherical harmonics of bands l = 0..3 of a unit vector (16 terms,
+// "degree 4" when counting bands), orthonormal basis.
 __host__ __device__ __forceinline__ void sh16( float x, float y, float z, float *o )
 {
 	const float c0 = 0.28209479177387814f, c1 = 0.4886025119029199f;
