@@ -1079,6 +1079,11 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 		d.prim = int( p );
 		d.light = prim_light[ p ];
 		ds.push_back( d );
+		// the sphere as a BVH primitive: its box (the builder's bounds of the
+		// three points) and, in the third record, centre and r^2
+		src.push_back( make_float4( hs.c[ 0 ] - d.r, hs.c[ 1 ] - d.r, hs.c[ 2 ] - d.r, 0.f ) );
+		src.push_back( make_float4( hs.c[ 0 ] + d.r, hs.c[ 1 ] + d.r, hs.c[ 2 ] + d.r, 0.f ) );
+		src.push_back( make_float4( hs.c[ 0 ], hs.c[ 1 ], hs.c[ 2 ], d.r2 ) );
 	}
 	float sc = 1;
 	for ( int a = 0; a < 3; ++a )
@@ -1100,14 +1105,17 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	s->err.upload( std::vector<uint32_t>( 2, 0 ) );  // [0] error word, [1] query work cursor
 	s->lights = lights;
 	s->tables_host = tables;
-	if ( nt )
+	// BVH over the triangles (ids 0 .. nt-1) and the spheres (ids nt ..)
+	const uint64_t n_prims = src.size() / 3;
+	if ( n_prims >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many primitives" );
+	if ( n_prims )
 	{
 		float4 *d_src = nullptr;
 		cuda_check( cudaMallocAsync( (void **)&d_src, sizeof( float4 ) * src.size(), st ), "cudaMalloc" );
 		cuda_check( cudaMemcpyAsync( d_src, src.data(), sizeof( float4 ) * src.size(), cudaMemcpyHostToDevice, st ), "upload" );
 		try
 		{
-			build_wide_bvh( d_src, uint32_t( nt ), s->bvh, st, s->build );
+			build_wide_bvh( d_src, uint32_t( n_prims ), s->bvh, st, s->build );
 		}
 		catch ( const std::exception &e )
 		{
@@ -1137,7 +1145,8 @@ DevScene dev_scene( const cr_scene *s )
 	d.light_cdf = s->light_cdf.p;
 	d.prim_first = s->prim_first.p;
 	d.n_nodes = s->bvh.n_nodes;
-	d.n_tris = uint32_t( s->n_tris );
+	d.n_tris = s->bvh.n_tris;  // BVH primitives: the triangles, then the spheres
+	d.sph_base = uint32_t( s->n_tris );
 	d.n_spheres = uint32_t( s->dspheres.n );
 	d.n_lights = uint32_t( s->dlights.n );
 	d.n_shaders = uint32_t( s->dshaders.n );

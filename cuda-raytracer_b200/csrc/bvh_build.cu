@@ -566,7 +566,7 @@ __global__ void k_collapse( const WorkItem *work, const uint32_t *n_work, WorkIt
 				float4 a = src[ 3 * size_t( prim ) ], bb = src[ 3 * size_t( prim ) + 1 ], cc = src[ 3 * size_t( prim ) + 2 ];
 				dst[ 0 ] = make_float4( a.x, a.y, a.z, __uint_as_float( prim ) );
 				dst[ 1 ] = make_float4( bb.x, bb.y, bb.z, 0.f );
-				dst[ 2 ] = make_float4( cc.x, cc.y, cc.z, 0.f );
+				dst[ 2 ] = cc;  // w: 0 for a triangle, r^2 for a sphere
 			}
 			toff += b.count;
 		}

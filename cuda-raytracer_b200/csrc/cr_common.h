@@ -2,8 +2,10 @@
 //
 // HBM layout of one committed scene (all arrays 16-byte aligned):
 //   nodes    WNode[n_nodes]        80 B  quantised 8-wide BVH, root = node 0
-//   tris     float4[3*n_tris]      48 B  per triangle in BVH leaf order:
-//                                        (v0.xyz, global id), (v1.xyz, -), (v2.xyz, -)
+//   tris     float4[3*n_tris]      48 B  per BVH primitive in leaf order; a triangle:
+//                                        (v0.xyz, global id), (v1.xyz, -), (v2.xyz, -);
+//                                        a sphere (id sph_base + sphere index):
+//                                        (box lo.xyz, id), (box hi.xyz, -), (centre.xyz, r^2)
 //   attrs    float4[3*n_tris]      48 B  per triangle in global order:
 //                                        (n0.xyz, shader), (n1.xyz, prim), (n2.xyz, light)
 //   spheres  DevSphere[n_spheres]
@@ -145,6 +147,7 @@ struct DevScene
 	const float *light_cdf;
 	const uint32_t *prim_first;  // first global triangle of each primitive
 	uint32_t n_nodes, n_tris, n_spheres, n_lights, n_shaders;
+	uint32_t sph_base;  // BVH primitive ids from here on are spheres (n_tris counts both)
 	float scene_scale;
 	DevCamera cam;
 };

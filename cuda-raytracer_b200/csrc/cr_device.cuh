@@ -143,15 +143,16 @@ __device__ __forceinline__ bool tri_test( const RayPre &r, float3 v0, float3 v1,
 // taken from the perpendicular vector itself, and the smaller-magnitude root
 // comes from the product of the roots (c / q), as in Haines et al.,
 // "Precision Improvements for Ray/Sphere Intersection" (Ray Tracing Gems, 2019).
-__device__ __forceinline__ bool sphere_test( const DevSphere &s, float3 o, float3 d, float tmin, float tmax, float &t )
+__device__ __forceinline__ bool sphere_test( float3 centre, float r2, float3 o, float3 d, float tmin, float tmax,
+											 float &t )
 {
-	float3 oc = f3( s.c ) - o;
+	float3 oc = centre - o;
 	float poc = dot( d, oc );
 	float3 perp = oc - d * poc;
-	float det = s.r2 - dot( perp, perp );
+	float det = r2 - dot( perp, perp );
 	if ( det < 0.f ) return false;
 	float q = poc + copysignf( sqrtf( det ), poc );  // root of larger magnitude
-	float c = dot( oc, oc ) - s.r2;
+	float c = dot( oc, oc ) - r2;
 	float r0 = q != 0.f ? c / q : 0.f, r1 = q;
 	float t_near = fminf( r0, r1 ), t_far = fmaxf( r0, r1 );
 	t = t_near < 0.f ? t_far : t_near;

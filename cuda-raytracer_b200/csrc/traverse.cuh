@@ -88,8 +88,7 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 	// this lane's geometry: the kernel's scene, or the current ray's in a batch
 	const WNode *nodes = sc.nodes;
 	const float4 *tris = sc.tris;
-	const DevSphere *spheres = sc.spheres;
-	uint32_t n_nodes = sc.n_nodes, n_tris = sc.n_tris, n_spheres = sc.n_spheres;
+	uint32_t n_nodes = sc.n_nodes, n_tris = sc.n_tris, sph_base = sc.sph_base;
 	for ( ;; )
 	{
 		if ( !exhausted )
@@ -112,25 +111,15 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 						if constexpr ( IO::MULTI )
 						{
 							const DevScene *ps = io.scene( item );
-							nodes = ps->nodes, tris = ps->tris, spheres = ps->spheres;
-							n_nodes = ps->n_nodes, n_tris = ps->n_tris, n_spheres = ps->n_spheres;
+							nodes = ps->nodes, tris = ps->tris;
+							n_nodes = ps->n_nodes, n_tris = ps->n_tris, sph_base = ps->sph_base;
 						}
 						hit.t = tmax;
 						hit.id = HIT_MISS;
 						hit.u = hit.v = 0.f;
 						found = false;
-						bool done = false;
-						for ( uint32_t s = 0; s < n_spheres && !done; ++s )
-						{
-							float t;
-							if ( sphere_test( spheres[ s ], o, d, tmin, hit.t, t ) )
-							{
-								hit.t = t, hit.id = HIT_SPHERE | s, found = true;
-								if ( ANY ) done = true;
-							}
-						}
 						// A NaN ray would pass every slab test; it hits nothing.
-						if ( done || n_nodes == 0 || !finite3( o ) || !finite3( d ) )
+						if ( n_nodes == 0 || !finite3( o ) || !finite3( d ) )
 							io.finish( item, hit, found );
 						else
 						{
@@ -175,10 +164,15 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 					const float4 *tp = tris + 3 * size_t( ti );
 					float4 a = __ldg( tp ), b = __ldg( tp + 1 ), c = __ldg( tp + 2 );
 					if ( COUNT ) ++wtris;
-					float t, u, v;
-					if ( tri_test( r, f3( a ), f3( b ), f3( c ), tmin, hit.t, t, u, v ) )
+					float t, u = 0.f, v = 0.f;
+					const uint32_t gid = __float_as_uint( a.w );
+					// a sphere record: (box lo, id), (box hi, -), (centre, r^2)
+					const bool sphere = gid >= sph_base;
+					if ( sphere ? sphere_test( f3( c ), c.w, r.o, r.d, tmin, hit.t, t )
+								: tri_test( r, f3( a ), f3( b ), f3( c ), tmin, hit.t, t, u, v ) )
 					{
-						hit.t = t, hit.id = ti, hit.u = u, hit.v = v, found = true;
+						hit.t = t, hit.id = sphere ? ( HIT_SPHERE | ( gid - sph_base ) ) : ti, hit.u = u, hit.v = v;
+						found = true;
 						if ( ANY ) done = true;
 					}
 				}
