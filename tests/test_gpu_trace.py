@@ -76,7 +76,7 @@ def test_any_hit_matches_reference_segments(cr, scenes):
 
 
 def test_edge_cases(cr):
-    # a lone sphere: no triangles, no BVH
+    # a lone sphere: no triangles; the BVH holds the sphere alone
     d_sphere = _tiny_scene(cr, tris=False)
     rays = np.array([[0, 0, -5, 0, 0, 1, np.inf], [0, 3, -5, 0, 0, 1, np.inf], [0, 0, -5, 0, 0, 1, 3.0]], np.float32)
     h = d_sphere.trace(rays)
@@ -129,3 +129,63 @@ def test_full_size_mesh_against_fp64(cr, scenes, oracle):
     assert same.mean() >= 0.999, same.mean()
     ok = same & (prim >= 0)
     assert np.max(np.abs(hits["t"][ok] - t[ok]) / t[ok]) <= 1e-5
+
+
+def _sphere_field(scenes, n, seed, with_box=True):
+    """n spheres of random radii in the config-0 box (overlaps allowed)."""
+    rng = np.random.default_rng(seed)
+    d = scenes.config0()
+    if not with_box:
+        d.groups = []
+    lo = np.array([0.3, scenes.FRONT + 0.3, 0.3])
+    hi = np.array([scenes.S - 0.3, scenes.S - 0.3, scenes.S - 0.3])
+    c = scenes._rot_points(lo + (hi - lo) * rng.random((n, 3)))
+    r = rng.uniform(0.02, 0.3, n) if n > 1 else np.ones(1)
+    d.spheres = [{"o": [float(x) for x in c[i]], "r": float(r[i]), "shader": "ball" if i % 2 else "glossy"}
+                 for i in range(n)]
+    return d
+
+
+@pytest.mark.parametrize("n_spheres,with_box", [(1500, True), (300, False), (1, False)])
+def test_spheres_in_the_bvh_match_fp64(cr, scenes, oracle, n_spheres, with_box):
+    """Spheres are BVH primitives: closest hits and shadow answers on a field
+    of many spheres (with and without the box's triangles, and one sphere
+    alone) equal the FP64 oracle's, which tests every sphere per ray."""
+    d = _sphere_field(scenes, n_spheres, 40 + n_spheres, with_box)
+    s = cr.Scene.from_desc(d)
+    rays = make_rays(d, 4096, 9)
+    hits = s.trace(rays)
+    o = oracle.OracleScene(d)
+    p, tri, t, _, _ = o.trace(rays)
+    same = (hits["prim"] == p) & (hits["tri"] == tri)
+    fin = np.isfinite(t) & np.isfinite(hits["t"])
+    dt = np.abs(np.where(fin, hits["t"], 0.0) - np.where(fin, t, 0.0))
+    ties = ~same & fin & (dt <= 1e-6 * np.maximum(np.abs(np.where(fin, t, 0.0)), 1e-6))
+    assert (same | ties).all(), np.nonzero(~(same | ties))[0][:8]
+    sph = same & (p >= len(d.groups))
+    assert sph.sum() > 100
+    # t error: 1e-5 relative, plus what the direction's rounding does: both
+    # the oracle's and the kernel's sphere formulas take the FP32 direction as
+    # unit length, which it is to ~1e-7, and that moves t by about
+    # |oc|^2 * 1e-7 / sqrt(det), with sqrt(det) = |cos| r at the hit (small
+    # far spheres amplify it); away from grazing incidence and the ray origin
+    idx = p[sph] - len(d.groups)
+    cen = np.array([d.spheres[i]["o"] for i in idx], np.float64)
+    rad = np.array([d.spheres[i]["r"] for i in idx], np.float64)
+    ro, rd = rays[sph, :3].astype(np.float64), rays[sph, 3:6].astype(np.float64)
+    nrm = (ro + rd * t[sph][:, None] - cen) / rad[:, None]
+    cosv = np.abs((nrm * rd).sum(1))
+    steep = ( cosv >= 0.1 ) & ( t[sph] >= 0.05 )
+    err = np.abs(hits["t"][sph].astype(np.float64) - t[sph])
+    allow = 1e-5 * t[sph] + 5e-7 * ((cen - ro) ** 2).sum(1) / np.maximum(cosv * rad, 1e-3)
+    assert steep.mean() > 0.8 and (err[steep] <= allow[steep]).all(), (steep.mean(), (err / allow)[steep].max())
+    assert (err <= 1e-3 * (t[sph] + 1.0)).all(), err.max()
+    # any-hit queries on the same rays, cut at half (unoccluded) or 1.5 times
+    # (occluded) the closest distance, or at 5 units for a miss
+    segs = rays.copy()
+    cut = np.where(np.arange(len(rays)) % 2 == 0, 0.5, 1.5)
+    segs[:, 6] = np.where(np.isfinite(t), cut * t, 5.0).astype(np.float32)
+    occ = s.trace(segs, any_hit=True)["prim"] >= 0
+    ref = o.occluded(segs).astype(bool)
+    assert (occ == ref).mean() >= 0.999
+    assert 0.1 < ref.mean() < 0.9 or n_spheres == 1
