@@ -310,15 +310,24 @@ DevShader make_shader( const Json &cfg, ShaderTable &tab, const std::string &nam
 	return s;
 }
 
-// Whether a shader is outside the MIS estimator's BSDFs (Lambert, Beckmann
-// GlossyBSDF, Emission); Mixed and the transmissive shaders have reference
-// semantics only.
-bool koishi_only( const DevShader &s )
+// Whether the MIS estimator's BSDFs leave out a shader: the microfacet ones
+// need the Beckmann distribution, and a Mixed two such leaves (no nesting).
+bool mis_leaf_ok( const DevShader &s )
 {
-	if ( s.type == SH_MIXED ) return true;
-	if ( s.type == SH_GLOSSY ) return s.dist != DIST_BECKMANN;
-	return s.type != SH_LAMBERT && s.type != SH_EMISSION;
+	if ( s.type == SH_MIXED ) return false;
+	if ( s.type == SH_GLOSSY || s.type == SH_GLASS || s.type == SH_REFRACTION ) return s.dist == DIST_BECKMANN;
+	return true;
 }
+
+bool koishi_only( const ShaderTable &tab, const DevShader &s )
+{
+	if ( s.type == SH_MIXED ) return !mis_leaf_ok( tab[ s.child[ 0 ] ].second ) || !mis_leaf_ok( tab[ s.child[ 1 ] ].second );
+	return !mis_leaf_ok( s );
+}
+
+// The single-shader MIS helpers (cr_bsdf_eval / cr_bsdf_sample) cover the
+// reflection-only BSDFs; renders cover the rest.
+bool mis_helper_ok( const DevShader &s ) { return s.type == SH_LAMBERT || s.type == SH_EMISSION || ( s.type == SH_GLOSSY && s.dist == DIST_BECKMANN ); }
 
 int shader_id( cr_scene *s, const std::string &name )
 {
@@ -983,11 +992,10 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	// every Emission-shaded primitive in primitive order (scene.cu:200-216).
 	std::vector<DevLight> lights( s->point_lights );
 	s->mis_blocker.clear();
-	if ( !s->point_lights.empty() ) s->mis_blocker = "pointLight";
 	for ( const HostPrim &hp : s->prims )
 	{
 		int shader = hp.kind == 0 ? s->meshes[ hp.index ].shader : s->spheres[ hp.index ].shader;
-		if ( s->mis_blocker.empty() && koishi_only( s->shaders[ shader ].second ) )
+		if ( s->mis_blocker.empty() && koishi_only( s->shaders, s->shaders[ shader ].second ) )
 			s->mis_blocker = "shader " + s->shaders[ shader ].first;
 	}
 	std::vector<float4> tables, ltris;
@@ -1221,8 +1229,8 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	c.estimator = desc->estimator < 0 ? s->estimator : desc->estimator;
 	if ( c.estimator != EST_KOISHI && c.estimator != EST_MIS ) fail( CR_ERR_INVALID, "unknown estimator" );
 	if ( c.estimator == EST_MIS && !s->mis_blocker.empty() )
-		fail( CR_ERR_UNSUPPORTED, "the MIS estimator covers Lambert, Beckmann GlossyBSDF and Emission area lights; " +
-									  s->mis_blocker + " has the reference estimator only" );
+		fail( CR_ERR_UNSUPPORTED, "the MIS estimator takes microfacet shaders with the Beckmann distribution and "
+								  "Mixed of two leaves; " + s->mis_blocker + " has the reference estimator only" );
 	c.x0 = x0, c.y0 = y0, c.ww = x1 - x0, c.wh = y1 - y0;
 	c.seed = desc->seed;
 	r.samples = uint64_t( c.ww ) * c.wh * c.spp;
@@ -2265,7 +2273,8 @@ static DevShader shader_from_json( int est, const char *js )
 	DevShader sh = make_shader( parse_json( js ), tab, "shader" );
 	if ( sh.type == SH_MIXED || sh.type == SH_GLASS )
 		fail( CR_ERR_INVALID, "Mixed and GlassBSDF draw selection numbers: use cr_shader_execute" );
-	if ( est == EST_MIS && koishi_only( sh ) ) fail( CR_ERR_UNSUPPORTED, "the MIS estimator does not cover this shader" );
+	if ( est == EST_MIS && !mis_helper_ok( sh ) )
+		fail( CR_ERR_UNSUPPORTED, "the MIS helpers cover Lambert, Beckmann GlossyBSDF and Emission; render to test the others" );
 	return sh;
 }
 

@@ -497,6 +497,173 @@ __device__ __forceinline__ float3 mis_sample( const DevShader &sh, float3 wo, fl
 	return f3( sh.albedo );
 }
 
+// The MIS estimator's remaining shaders, physically restated (the reference's
+// versions are the koishi_* functions): RefractionBSDF and GlassBSDF as the
+// rough dielectric of Walter et al. ("Microfacet Models for Refraction through
+// Rough Surfaces", EGSR 2007) with a Beckmann distribution (Refraction: its
+// transmission alone), Transparent as a delta pass-through, Blackhole black,
+// Mixed as the fac-weighted mixture of two such leaves.  wo.z > 0 (the frame
+// faces the incoming ray); `entering`: wo lies outside the surface as built,
+// which sets the dielectric's index on either side.
+
+// Smith G1 of direction v for microfacet normal h, either side of the surface.
+__device__ __forceinline__ float smith_g1h( float alpha, float3 v, float3 h )
+{
+	if ( dot( v, h ) * v.z <= 0.f ) return 0.f;
+	return smith_g1( alpha, f3( v.x, v.y, fabsf( v.z ) ) );
+}
+
+// Unpolarised Fresnel reflectance of a dielectric interface for cos_o > 0 on
+// the side of index 1 and relative index eta of the other side.
+__device__ __forceinline__ float fresnel_dielectric( float cos_o, float eta )
+{
+	const float s2 = ( 1.f - cos_o * cos_o ) / ( eta * eta );
+	if ( s2 >= 1.f ) return 1.f;
+	const float ct = sqrtf( 1.f - s2 );
+	const float rs = ( cos_o - eta * ct ) / ( cos_o + eta * ct ), rp = ( eta * cos_o - ct ) / ( eta * cos_o + ct );
+	return .5f * ( rs * rs + rp * rp );
+}
+
+__device__ __forceinline__ bool mis_transmits( int type )
+{
+	return type == SH_GLASS || type == SH_REFRACTION || type == SH_TRANSPARENT;
+}
+
+// f and pdf of a rough dielectric leaf for wi on either side.
+__device__ __forceinline__ float3 dielectric_eval( const DevShader &sh, float3 wo, float3 wi, bool entering, float &pdf )
+{
+	pdf = 0.f;
+	const float eo = entering ? 1.f : sh.ior, et = entering ? sh.ior : 1.f;
+	if ( wi.z > 0.f )
+	{
+		if ( sh.type == SH_REFRACTION ) return f3( 0.f, 0.f, 0.f );
+		const float3 h = normalize( wo + wi );
+		const float F = fresnel_dielectric( dot( wo, h ), et / eo );
+		const float D = beckmann_d( sh.alpha2, h );
+		const float G = smith_g1h( sh.alpha, wo, h ) * smith_g1h( sh.alpha, wi, h );
+		pdf = F * D * h.z / ( 4.f * fabsf( dot( wo, h ) ) );
+		return f3( sh.color ) * ( F * D * G / ( 4.f * wo.z * wi.z ) );
+	}
+	if ( !( wi.z < 0.f ) ) return f3( 0.f, 0.f, 0.f );
+	float3 h = normalize( -( wo * eo + wi * et ) );
+	if ( h.z < 0.f ) h = -h;
+	const float co = dot( wo, h ), ci = dot( wi, h );
+	if ( co <= 0.f || ci >= 0.f ) return f3( 0.f, 0.f, 0.f );
+	const float F = sh.type == SH_GLASS ? fresnel_dielectric( co, et / eo ) : 0.f;
+	const float D = beckmann_d( sh.alpha2, h );
+	const float G = smith_g1h( sh.alpha, wo, h ) * smith_g1h( sh.alpha, wi, h );
+	const float den = et * ci + eo * co;
+	pdf = ( 1.f - F ) * D * h.z * et * et * fabsf( ci ) / ( den * den );
+	return f3( sh.color ) * ( ( 1.f - F ) * D * G * fabsf( ci ) * co * eo * eo / ( fabsf( wi.z ) * wo.z * den * den ) );
+}
+
+// f and pdf of any leaf (not Mixed) for the MIS estimator.
+__device__ __forceinline__ float3 mis_eval_leaf( const DevShader &sh, float3 wo, float3 wi, bool entering, float &pdf )
+{
+	pdf = 0.f;
+	if ( wo.z <= 0.f ) return f3( 0.f, 0.f, 0.f );
+	switch ( sh.type )
+	{
+	case SH_LAMBERT:
+	case SH_EMISSION:
+	case SH_GLOSSY:
+		return mis_eval( sh, wo, wi, pdf );
+	case SH_GLASS:
+	case SH_REFRACTION:
+		return dielectric_eval( sh, wo, wi, entering, pdf );
+	default:  // Transparent (delta), Blackhole
+		return f3( 0.f, 0.f, 0.f );
+	}
+}
+
+// Mixed's fac: the Constant, or the Fresnel scala with the reference's side
+// convention (fresnel.hpp:17-31: the cosine of wo against the surface as built).
+__device__ __forceinline__ float mis_fac( const DevShader &m, float3 wo, bool entering )
+{
+	if ( m.fac_kind != FAC_FRESNEL ) return fminf( 1.f, fmaxf( 0.f, m.fac ) );
+	return fresnel_fac( m.ior, f3( wo.x, wo.y, entering ? wo.z : -wo.z ) );
+}
+
+// f and pdf of table entry idx: a leaf, or a Mixed of two leaves.
+__device__ __forceinline__ float3 mis_eval_tab( const DevShader *tab, int idx, float3 wo, float3 wi, bool entering,
+												float &pdf )
+{
+	const DevShader &sh = tab[ idx ];
+	if ( sh.type != SH_MIXED ) return mis_eval_leaf( sh, wo, wi, entering, pdf );
+	const float F = mis_fac( sh, wo, entering );
+	float pa, pb;
+	const float3 fa = mis_eval_leaf( tab[ sh.child[ 0 ] ], wo, wi, entering, pa );
+	const float3 fb = mis_eval_leaf( tab[ sh.child[ 1 ] ], wo, wi, entering, pb );
+	pdf = ( 1.f - F ) * pa + F * pb;
+	return fa * ( 1.f - F ) + fb * F;
+}
+
+// Sampled direction of a leaf (u_sel picks a dielectric's reflection); false
+// when it yields none.  Transparent's is the delta direction -wo.
+__device__ __forceinline__ bool mis_sample_dir_leaf( const DevShader &sh, float3 wo, bool entering, float u_sel, float u1,
+													 float u2, float3 &wi )
+{
+	if ( wo.z <= 0.f ) return false;
+	switch ( sh.type )
+	{
+	case SH_TRANSPARENT:
+		wi = -wo;
+		return true;
+	case SH_GLOSSY:
+	{
+		const float3 h = beckmann_sample( sh.alpha2, u1, u2 );
+		wi = reflect( wo, h );
+		return wi.z > 0.f && dot( wo, h ) > 0.f;
+	}
+	case SH_GLASS:
+	case SH_REFRACTION:
+	{
+		const float eo = entering ? 1.f : sh.ior, et = entering ? sh.ior : 1.f;
+		const float3 h = beckmann_sample( sh.alpha2, u1, u2 );
+		const float co = dot( wo, h );
+		if ( co <= 0.f ) return false;
+		const float F = sh.type == SH_GLASS ? fresnel_dielectric( co, et / eo ) : 0.f;
+		if ( u_sel < F )
+		{
+			wi = reflect( wo, h );
+			return wi.z > 0.f;
+		}
+		if ( !refract_dir( wo, h, eo / et, wi ) ) return false;
+		return wi.z < 0.f;
+	}
+	case SH_LAMBERT:
+	case SH_EMISSION:
+		wi = sample_cos( u1, u2 );
+		return wi.z > 0.f;
+	default:  // Blackhole
+		return false;
+	}
+}
+
+// Sample of table entry idx: returns the weight f|cos|/pdf with wi and pdf;
+// `delta` for Transparent's pass-through (weight = color, no density).
+__device__ __forceinline__ float3 mis_sample_tab( const DevShader *tab, int idx, float3 wo, bool entering, float u_sel,
+												  float u1, float u2, float3 &wi, float &pdf, bool &delta )
+{
+	pdf = 0.f, delta = false;
+	const DevShader *leaf = &tab[ idx ];
+	if ( leaf->type == SH_MIXED )
+	{
+		const float F = mis_fac( *leaf, wo, entering );
+		const bool b = u_sel < F;
+		u_sel = b ? u_sel / F : ( u_sel - F ) / ( 1.f - F );
+		leaf = &tab[ leaf->child[ b ? 1 : 0 ] ];
+	}
+	if ( !mis_sample_dir_leaf( *leaf, wo, entering, u_sel, u1, u2, wi ) ) return f3( 0.f, 0.f, 0.f );
+	if ( leaf->type == SH_TRANSPARENT )
+	{
+		delta = true;
+		return f3( leaf->color );
+	}
+	const float3 f = mis_eval_tab( tab, idx, wo, wi, entering, pdf );
+	return pdf > 0.f ? f * ( fabsf( wi.z ) / pdf ) : f3( 0.f, 0.f, 0.f );
+}
+
 // Spawn point offset off a surface along its geometric normal by an amount
 // that scales with the point's magnitude (Waechter and Binder, "A Fast and
 // Robust Method for Avoiding Self-Intersection", Ray Tracing Gems 2019).

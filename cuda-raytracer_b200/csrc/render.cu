@@ -484,7 +484,9 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	if ( sh.type == SH_EMISSION )
 	{
 		float w = 1.f;
-		if ( bounce > 0 && s.light >= 0 )
+		// beta4.w: the previous continuation's density, negative after a delta
+		// (pass-through) continuation, which next-event estimation cannot sample
+		if ( bounce > 0 && s.light >= 0 && beta4.w >= 0.f )
 		{
 			float cosl = fabsf( dot( s.ng, d ) );
 			float pb = beta4.w;
@@ -499,14 +501,22 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	// leaves the lights themselves to next-event estimation.
 	if ( rec_i != 0xFFFFFFFFu && bounce > 0 ) cfg.rec.L[ rec_i - 1 ] = make_float4( L.x, L.y, L.z, 0.f );
 	// Two-sided shading: the geometric normal faces the incoming ray and the
-	// shading normal is put on the same side.
+	// shading normal is put on the same side.  `entering`: the ray arrives from
+	// outside the surface as built (the dielectrics' side).
+	const bool entering = dot( s.ng, d ) < 0.f;
 	if ( dot( s.ng, d ) > 0.f ) s.ng = -s.ng;
 	if ( dot( s.ns, s.ng ) < 0.f ) s.ns = -s.ns;
 	Frame fr = onb_frame( s.ns );
 	float3 wo = fr.local( -d );
 	float4 r0 = rand4( key, g, bounce, 0 ), r1 = rand4( key, g, bounce, 1 );
+	// Lambert, Glossy and Emission take the reflection-only fast path; the
+	// other shaders (dielectrics, pass-through, black, mixtures) the general one
+	const bool simple = sh.type == SH_LAMBERT || sh.type == SH_GLOSSY || sh.type == SH_EMISSION;
+	const bool transmits = !simple && ( mis_transmits( sh.type ) ||
+										( sh.type == SH_MIXED && ( mis_transmits( sc.shaders[ sh.child[ 0 ] ].type ) ||
+																   mis_transmits( sc.shaders[ sh.child[ 1 ] ].type ) ) ) );
 	PreparedLobe lb[ G_LOBES ];
-	const bool guided = cfg.guide_sample && guided_vertex( cfg.guide, bounce, cfg.max_bounce );
+	const bool guided = simple && cfg.guide_sample && guided_vertex( cfg.guide, bounce, cfg.max_bounce );
 	const float sel = guided ? cfg.guide.select_prob : 0.f;
 	if ( guided ) load_lobes( lobes, lb );
 	if ( sc.n_lights )
@@ -515,34 +525,41 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		uint32_t idx = min( uint32_t( floorf( r0.x * nl ) ), nli - 1 );
 		float ur = r0.x * nl - float( idx );
 		const DevLight lt = sc.lights[ idx ];
-		float3 lp, ln;
-		float pdfA;
-		mis_light_point( sc, lt, ur, r0.y, r0.z, lp, ln, pdfA );
+		const bool point = lt.kind == LIGHT_POINT;
+		float3 lp, ln = f3( 0.f, 0.f, 1.f );
+		float pdfA = 1.f;
+		if ( point )
+			lp = f3( lt.pos );
+		else
+			mis_light_point( sc, lt, ur, r0.y, r0.z, lp, ln, pdfA );
 		float3 dw = lp - s.p;
 		float dist2 = dot( dw, dw ), dist = sqrtf( dist2 );
 		float3 wiw = dw / dist;
-		float cosl = fabsf( dot( ln, wiw ) );
-		if ( cosl > 0.f && dist > 0.f && dot( wiw, s.ng ) > 0.f )
+		// a point light of intensity I = color * strength gives I cos / r^2 and
+		// is reached by next-event estimation alone (weight 1)
+		float cosl = point ? 1.f : fabsf( dot( ln, wiw ) );
+		if ( cosl > 0.f && dist > 0.f && ( transmits || dot( wiw, s.ng ) > 0.f ) )
 		{
-			float pl = pdfA * dist2 / cosl / nl;
+			float pl = point ? dist2 / nl : pdfA * dist2 / cosl / nl;
 			float3 wi = fr.local( wiw );
 			float pb;
-			float3 f = mis_eval( sh, wo, wi, pb );
+			float3 f = simple ? mis_eval( sh, wo, wi, pb ) : mis_eval_tab( sc.shaders, s.shader, wo, wi, entering, pb );
 			// one-sample MIS of guide and BSDF: the continuation density
 			if ( guided ) pb = sel * prepared_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
 			if ( !is_zero( f ) )
 			{
 				// the last vertex has no continuation that could reach the light:
 				// its light sample takes the whole weight
-				float w = bounce == cfg.max_bounce ? 1.f : pl * pl / ( pl * pl + pb * pb );
-				float3 c = beta * f * f3( lt.emission ) * ( wi.z * w / pl );
+				float w = bounce == cfg.max_bounce || point ? 1.f : pl * pl / ( pl * pl + pb * pb );
+				float3 c = beta * f * f3( lt.emission ) * ( fabsf( wi.z ) * w / pl );
 				if ( finite3( c ) && !is_zero( c ) )
 				{
 					// Both ends leave their surfaces: the shading point along its
-					// geometric normal, the light point along the light's normal
-					// towards the shading point; the ray runs between the two.
-					float3 so = offset_ray( s.p, s.ng );
-					float3 to = offset_ray( lp, dot( ln, wiw ) < 0.f ? ln : -ln );
+					// geometric normal (on the light's side), the light point along
+					// the light's normal towards the shading point; the ray runs
+					// between the two.  A point light is its own end.
+					float3 so = offset_ray( s.p, dot( wiw, s.ng ) > 0.f ? s.ng : -s.ng );
+					float3 to = point ? lp : offset_ray( lp, dot( ln, wiw ) < 0.f ? ln : -ln );
 					float3 sd = to - so;
 					float len = length( sd );
 					sd = sd / len;
@@ -557,7 +574,15 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	float3 wi;
 	float pdf;
 	float3 wt, nd;
-	if ( guided )
+	bool delta = false;
+	if ( !simple )
+	{
+		// a selection number for Mixed and the dielectrics
+		const float us = rand4( key, g, bounce, 2 ).x;
+		wt = mis_sample_tab( sc.shaders, s.shader, wo, entering, us, r1.x, r1.y, wi, pdf, delta );
+		nd = fr.global( wi );
+	}
+	else if ( guided )
 	{
 		// one-sample MIS: the guide with probability sel, else the BSDF; the
 		// weight uses the combined density of both strategies
@@ -582,7 +607,9 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		nd = fr.global( wi );
 	}
 	beta = beta * wt;
-	bool alive = !is_zero( beta ) && dot( nd, s.ng ) > 0.f;
+	// a continuation through the surface leaves from its far side
+	const bool through = wi.z < 0.f;
+	bool alive = !is_zero( beta ) && ( through ? dot( nd, s.ng ) < 0.f : dot( nd, s.ng ) > 0.f );
 	float rr = maxc( beta );
 	if ( alive && rr < 1.f && bounce > 3 )
 	{
@@ -593,7 +620,8 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 			beta = beta / ( 1.f - q );
 	}
 	if ( bounce + 1 > cfg.max_bounce || !finite3( beta ) ) alive = false;
-	float3 no = offset_ray( s.p, s.ng );
+	float3 no = offset_ray( s.p, through ? -s.ng : s.ng );
+	if ( delta ) pdf = 0.f;  // no density: not a training sample
 	if ( rec_i != 0xFFFFFFFFu )
 	{
 		// training record of this vertex (its radiance target follows once the
@@ -605,7 +633,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		cfg.rec.om[ rec_i ] = make_float4( nd.x, nd.y, nd.z, pdf );
 		cfg.rec.T[ rec_i ] = make_float4( beta.x, beta.y, beta.z, 0.f );
 	}
-	beta4 = make_float4( beta.x, beta.y, beta.z, pdf );
+	beta4 = make_float4( beta.x, beta.y, beta.z, delta ? -1.f : pdf );
 	L4 = make_float4( L.x, L.y, L.z, 0.f );
 	out.alive = alive;
 	out.ro = make_float4( no.x, no.y, no.z, 0.f );

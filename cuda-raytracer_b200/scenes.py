@@ -288,11 +288,13 @@ def config0_ortho(width=256, height=256, spp=64) -> SceneDesc:
     return d
 
 
-def config_materials(width=256, height=256, spp=64) -> SceneDesc:
+def config_materials(width=256, height=256, spp=64, cosine=True, point_light=True) -> SceneDesc:
     """The box with the reference's remaining shaders and a point light:
     GlassBSDF, RefractionBSDF, Transparent, Blackhole, Mixed over a Fresnel
-    and over a Constant fac (one with a Cosine GlossyBSDF), lit by the ceiling
-    panel and by a pointLight (the first light in the list)."""
+    and over a Constant fac (one with a Cosine GlossyBSDF; `cosine=False`:
+    a Beckmann one, which the MIS estimator takes), lit by the ceiling panel
+    and by a pointLight (the first light in the list; `point_light=False`
+    leaves it out)."""
     sh = box_shaders(50.0)
     beck = lambda a: ["Beckmann", {"roughness": a}]
     sh["glass"] = ["GlassBSDF", {"ior": 1.5, "distribution": beck(0.2), "color": [0.95, 0.97, 1.0]}]
@@ -304,12 +306,13 @@ def config_materials(width=256, height=256, spp=64) -> SceneDesc:
     sh["hole"] = ["Blackhole", {}]
     sh["blend"] = ["Mixed", {"fac": ["Constant", {"value": 0.35}],
                              "shaders": [["Lambert", {"R": [0.2, 0.5, 0.7], "color": [1, 1, 1]}],
-                                         ["GlossyBSDF", {"distribution": ["Cosine", {}], "color": [0.8, 0.8, 0.6]}]]}]
+                                         ["GlossyBSDF", {"distribution": ["Cosine", {}] if cosine else beck(0.4),
+                                                         "color": [0.8, 0.8, 0.6]}]]}]
     place = [("glass", [1.6, 1.6, 1.0], 1.0), ("coat", [3.9, 3.6, 1.0], 1.0), ("water", [3.8, 1.0, 0.6], 0.6),
              ("veil", [1.4, 3.9, 0.8], 0.8), ("hole", [2.8, 4.7, 2.8], 0.4), ("blend", [2.6, 2.6, 0.45], 0.45)]
     spheres = [{"o": [float(x) for x in _rot_points(c)], "r": r, "shader": n} for n, c, r in place]
     lights = [{"position": [float(x) for x in _rot_points([2.0, 2.0, 4.2])], "color": [1.0, 0.9, 0.8],
-               "strength": 1.5}]
+               "strength": 1.5}] if point_light else []
     return SceneDesc(groups=box_groups(), spheres=spheres, shaders=sh, camera=box_camera(), point_lights=lights,
                      width=width, height=height, spp=spp, max_bounce=7, name="materials")
 

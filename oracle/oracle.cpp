@@ -615,6 +615,15 @@ V3 k_sample( const std::vector<Shader> &tab, int idx, V3 wo, Draws &u, V3 &wi, V
 // ORC_MIS BSDFs: Lambert color*R/pi with cosine pdf; Beckmann microfacet
 // reflection color*D*G/(4 cos_o cos_i) with Walter et al.'s Smith G1 and the
 // half-vector pdf D cos_h / (4 |wo.h|); Emission reflects as white Lambert.
+// The remaining shaders, physically restated (the reference's own versions
+// are the ORC_KOISHI ones above): RefractionBSDF and GlassBSDF as the rough
+// dielectric of Walter et al. ("Microfacet Models for Refraction through
+// Rough Surfaces", EGSR 2007) with a Beckmann distribution (Refraction: its
+// transmission alone), Transparent as a delta pass-through, Blackhole black,
+// Mixed as the fac-weighted mixture of two such leaves.  wo.z > 0 always (the
+// frame faces the incoming ray); `entering` says whether wo lies outside the
+// surface (against the geometric normal as built), which sets the dielectric's
+// index on either side.
 double smith_g1( double alpha, V3 w )
 {
 	double c = w.z;
@@ -626,10 +635,62 @@ double smith_g1( double alpha, V3 w )
 	return ( 3.535 * a + 2.181 * a * a ) / ( 1 + 2.276 * a + 2.577 * a * a );
 }
 
-void m_eval( const Shader &sh, V3 wo, V3 wi, V3 &f, double &pdf )
+// Smith G1 of direction v for microfacet normal h, either side of the surface.
+double smith_g1h( double alpha, V3 v, V3 h )
+{
+	if ( dot( v, h ) * v.z <= 0 ) return 0;
+	return smith_g1( alpha, V3( v.x, v.y, std::fabs( v.z ) ) );
+}
+
+// Unpolarised Fresnel reflectance of a dielectric interface for cos_o > 0 on
+// the side of index 1 and relative index eta of the other side.
+double fresnel_dielectric( double cos_o, double eta )
+{
+	double s2 = ( 1 - cos_o * cos_o ) / ( eta * eta );
+	if ( s2 >= 1 ) return 1;
+	double ct = std::sqrt( 1 - s2 );
+	double rs = ( cos_o - eta * ct ) / ( cos_o + eta * ct ), rp = ( eta * cos_o - ct ) / ( eta * cos_o + ct );
+	return .5 * ( rs * rs + rp * rp );
+}
+
+bool m_delta( const Shader &sh ) { return sh.type == ORC_TRANSPARENT; }
+bool m_transmits( const Shader &sh ) { return sh.type == ORC_GLASS || sh.type == ORC_REFRACTION || sh.type == ORC_TRANSPARENT; }
+
+// f and pdf of a leaf (not Mixed); a delta or black leaf has none.
+void m_eval_leaf( const Shader &sh, V3 wo, V3 wi, bool entering, V3 &f, double &pdf )
 {
 	f = V3(), pdf = 0;
-	if ( wo.z <= 0 || wi.z <= 0 ) return;
+	if ( wo.z <= 0 ) return;
+	if ( sh.type == ORC_GLASS || sh.type == ORC_REFRACTION )
+	{
+		const double eo = entering ? 1 : sh.ior, et = entering ? sh.ior : 1;
+		const double a = sh.alpha, a2 = a * a;
+		if ( wi.z > 0 )
+		{
+			if ( sh.type == ORC_REFRACTION ) return;
+			V3 h = normalize( wo + wi );
+			double F = fresnel_dielectric( dot( wo, h ), et / eo );
+			double D = beckmann_f( a2, h ) / std::fabs( h.z );
+			double G = smith_g1h( a, wo, h ) * smith_g1h( a, wi, h );
+			f = sh.color * ( F * D * G / ( 4 * wo.z * wi.z ) );
+			pdf = F * D * h.z / ( 4 * std::fabs( dot( wo, h ) ) );
+		}
+		else if ( wi.z < 0 )
+		{
+			V3 h = normalize( -( wo * eo + wi * et ) );
+			if ( h.z < 0 ) h = -h;
+			double co = dot( wo, h ), ci = dot( wi, h );
+			if ( co <= 0 || ci >= 0 ) return;
+			double F = sh.type == ORC_GLASS ? fresnel_dielectric( co, et / eo ) : 0;
+			double D = beckmann_f( a2, h ) / std::fabs( h.z );
+			double G = smith_g1h( a, wo, h ) * smith_g1h( a, wi, h );
+			double den = et * ci + eo * co;
+			f = sh.color * ( ( 1 - F ) * D * G * std::fabs( ci ) * co * eo * eo / ( std::fabs( wi.z ) * wo.z * den * den ) );
+			pdf = ( 1 - F ) * D * h.z * et * et * std::fabs( ci ) / ( den * den );
+		}
+		return;
+	}
+	if ( sh.type == ORC_TRANSPARENT || sh.type == ORC_BLACKHOLE || sh.type == ORC_MIXED || wi.z <= 0 ) return;
 	if ( sh.type == ORC_GLOSSY )
 	{
 		V3 h = normalize( wo + wi );
@@ -645,21 +706,100 @@ void m_eval( const Shader &sh, V3 wo, V3 wi, V3 &f, double &pdf )
 	pdf = wi.z / PI;
 }
 
-void m_sample( const Shader &sh, V3 wo, double u1, double u2, V3 &wi, V3 &weight, double &pdf )
+// Mixed's fac for the MIS estimator: the Constant, or the Fresnel scala with
+// the reference's side convention (fresnel.hpp:17-31, cos of wo against the
+// surface as built).
+double m_fac( const Shader &m, V3 wo, bool entering )
 {
-	weight = V3(), pdf = 0;
-	if ( sh.type == ORC_GLOSSY )
+	if ( m.fac_kind != ORC_FAC_FRESNEL ) return std::min( 1.0, std::max( 0.0, m.fac ) );
+	double cosi = entering ? wo.z : -wo.z;
+	double e = cosi > 0 ? 1 / m.ior : m.ior;
+	cosi = std::fabs( cosi );
+	double sr = e * std::sqrt( std::max( 0., 1 - cosi * cosi ) );
+	if ( sr >= 1 ) return 1;
+	double cr = std::sqrt( std::max( 0., 1 - sr * sr ) );
+	double par = ( cosi - e * cr ) / ( cosi + e * cr ), perp = ( e * cosi - cr ) / ( e * cosi + cr );
+	return .5 * ( par * par + perp * perp );
+}
+
+// f and pdf of table entry idx (a leaf, or a Mixed of two leaves).
+void m_eval( const std::vector<Shader> &tab, int idx, V3 wo, V3 wi, bool entering, V3 &f, double &pdf )
+{
+	const Shader &sh = tab[ idx ];
+	if ( sh.type != ORC_MIXED ) return m_eval_leaf( sh, wo, wi, entering, f, pdf );
+	double F = m_fac( sh, wo, entering );
+	V3 fa, fb;
+	double pa, pb;
+	m_eval_leaf( tab[ sh.child[ 0 ] ], wo, wi, entering, fa, pa );
+	m_eval_leaf( tab[ sh.child[ 1 ] ], wo, wi, entering, fb, pb );
+	f = fa * ( 1 - F ) + fb * F;
+	pdf = ( 1 - F ) * pa + F * pb;
+}
+
+// Direction of a leaf's sampling (u_sel picks a dielectric's reflection);
+// false when it yields none.  Transparent is the delta direction -wo.
+bool m_sample_dir_leaf( const Shader &sh, V3 wo, bool entering, double u_sel, double u1, double u2, V3 &wi )
+{
+	if ( wo.z <= 0 ) return false;
+	switch ( sh.type )
+	{
+	case ORC_TRANSPARENT:
+		wi = -wo;
+		return true;
+	case ORC_BLACKHOLE:
+	case ORC_MIXED:
+		return false;
+	case ORC_GLOSSY:
 	{
 		V3 h = beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
 		wi = reflect( wo, h );
-		if ( wo.z <= 0 || wi.z <= 0 || dot( wo, h ) <= 0 ) return;
+		return wi.z > 0 && dot( wo, h ) > 0;
 	}
-	else
+	case ORC_GLASS:
+	case ORC_REFRACTION:
+	{
+		const double eo = entering ? 1 : sh.ior, et = entering ? sh.ior : 1;
+		V3 h = beckmann_sample( sh.alpha * sh.alpha, u1, u2 );
+		double co = dot( wo, h );
+		if ( co <= 0 ) return false;
+		double F = sh.type == ORC_GLASS ? fresnel_dielectric( co, et / eo ) : 0;
+		if ( u_sel < F )
+		{
+			wi = reflect( wo, h );
+			return wi.z > 0;
+		}
+		if ( !refract( wo, h, eo / et, wi ) ) return false;
+		return wi.z < 0;
+	}
+	default:
 		wi = sample_cos( u1, u2 );
-	if ( wo.z <= 0 || wi.z <= 0 ) return;
+		return wi.z > 0;
+	}
+}
+
+// Sample of table entry idx: wi, weight f|cos|/pdf and pdf; delta for a
+// Transparent pass-through (weight = color, no density).
+void m_sample( const std::vector<Shader> &tab, int idx, V3 wo, bool entering, double u_sel, double u1, double u2,
+			   V3 &wi, V3 &weight, double &pdf, bool &delta )
+{
+	weight = V3(), pdf = 0, delta = false;
+	const Shader *leaf = &tab[ idx ];
+	if ( leaf->type == ORC_MIXED )
+	{
+		double F = m_fac( *leaf, wo, entering );
+		bool b = u_sel < F;
+		u_sel = b ? u_sel / F : ( u_sel - F ) / ( 1 - F );
+		leaf = &tab[ leaf->child[ b ? 1 : 0 ] ];
+	}
+	if ( !m_sample_dir_leaf( *leaf, wo, entering, u_sel, u1, u2, wi ) ) return;
+	if ( m_delta( *leaf ) )
+	{
+		weight = leaf->color, delta = true;
+		return;
+	}
 	V3 f;
-	m_eval( sh, wo, wi, f, pdf );
-	if ( pdf > 0 ) weight = f * ( wi.z / pdf );
+	m_eval( tab, idx, wo, wi, entering, f, pdf );
+	if ( pdf > 0 ) weight = f * ( std::fabs( wi.z ) / pdf );
 }
 
 // Building an orthonormal basis, revisited (Duff et al., JCGT 2017).
@@ -858,6 +998,7 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng, 
 	V3 L, beta( 1, 1, 1 );
 	size_t nl = s->lights.size();
 	double prev_pdf = 0;
+	bool prev_delta = false;
 	for ( uint32_t bounce = 0;; ++bounce )
 	{
 		Hit h;
@@ -878,8 +1019,8 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng, 
 		if ( sh.type == ORC_EMISSION )
 		{
 			double w = 1;
-			if ( bounce > 0 && variant == 3 ) w = 0;
-			if ( bounce > 0 && variant == 0 )
+			if ( bounce > 0 && variant == 3 && !prev_delta ) w = 0;
+			if ( bounce > 0 && variant == 0 && !prev_delta )
 			{
 				const Light &lt = s->lights[ pr.light ];
 				double cosl = std::fabs( dot( ng, d ) );
@@ -890,54 +1031,81 @@ V3 radiance_mis( const orc_scene *s, V3 o, V3 d, uint32_t max_bounce, Rng &rng, 
 			}
 			L = L + beta * sh.emission * w;
 		}
+		// wo outside the surface as built: the dielectrics' index on either side
+		const bool entering = dot( ng, d ) < 0;
 		if ( dot( ng, d ) > 0 ) ng = -ng;
 		if ( dot( ns, ng ) < 0 ) ns = -ns;
 		Frame fr;
 		fr.n = ns;
 		onb( ns, fr.u, fr.v );
 		V3 wo = fr.local( -d );
+		const bool transmits = m_transmits( sh ) ||
+							   ( sh.type == ORC_MIXED && ( m_transmits( s->shaders[ sh.child[ 0 ] ] ) ||
+														   m_transmits( s->shaders[ sh.child[ 1 ] ] ) ) );
 		if ( nl && variant != 2 )
 		{
 			double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
 			size_t idx = std::min( size_t( std::floor( u0 * double( nl ) ) ), nl - 1 );
 			double ur = u0 * double( nl ) - double( idx );
 			const Light &lt = s->lights[ idx ];
-			V3 lp, ln;
-			double pdfA;
-			mis_light_sample( s, lt, ur, u1, u2, lp, ln, pdfA );
-			V3 dw = lp - p;
-			double dist2 = dot( dw, dw ), dist = std::sqrt( dist2 );
-			V3 wiw = dw / dist;
-			double cosl = std::fabs( dot( ln, wiw ) );
-			if ( cosl > 0 && dist > 0 )
+			if ( lt.kind == 2 )
 			{
-				double pl = pdfA * dist2 / cosl / double( nl );
-				V3 wi = fr.local( wiw );
-				V3 f;
-				double pb;
-				m_eval( sh, wo, wi, f, pb );
-				if ( ( f.x > 0 || f.y > 0 || f.z > 0 ) && dot( wiw, ng ) > 0 &&
-					 !occluded_ray( s, p, wiw, 1e-7 * s->scale, dist * ( 1 - 1e-4 ) ) )
+				// a point light of intensity color * strength: irradiance I cos / r^2,
+				// sampled only by NEE (weight 1)
+				V3 dw = lt.pos - p;
+				double dist2 = dot( dw, dw ), dist = std::sqrt( dist2 );
+				V3 wiw = dw / dist;
+				if ( dist > 0 && ( dot( wiw, ng ) > 0 || transmits ) )
 				{
-					// The last vertex has no continuation that could reach the light,
-					// so its light sample takes the whole weight: the estimate is then
-					// the light of all paths of at most max_bounce + 1 segments, for
-					// whatever continuation density the other vertices use.
-					double w = variant == 3 || bounce == max_bounce ? 1.0 : pl * pl / ( pl * pl + pb * pb );
-					L = L + beta * f * s->shaders[ s->prims[ lt.prim ].shader ].emission * ( wi.z * w / pl );
+					V3 wi = fr.local( wiw ), f;
+					double pb;
+					m_eval( s->shaders, pr.shader, wo, wi, entering, f, pb );
+					if ( ( f.x > 0 || f.y > 0 || f.z > 0 ) && !occluded_ray( s, p, wiw, 1e-7 * s->scale, dist * ( 1 - 1e-4 ) ) )
+						L = L + beta * f * lt.emission * ( std::fabs( wi.z ) * double( nl ) / dist2 );
+				}
+			}
+			else
+			{
+				V3 lp, ln;
+				double pdfA;
+				mis_light_sample( s, lt, ur, u1, u2, lp, ln, pdfA );
+				V3 dw = lp - p;
+				double dist2 = dot( dw, dw ), dist = std::sqrt( dist2 );
+				V3 wiw = dw / dist;
+				double cosl = std::fabs( dot( ln, wiw ) );
+				if ( cosl > 0 && dist > 0 )
+				{
+					double pl = pdfA * dist2 / cosl / double( nl );
+					V3 wi = fr.local( wiw );
+					V3 f;
+					double pb;
+					m_eval( s->shaders, pr.shader, wo, wi, entering, f, pb );
+					if ( ( f.x > 0 || f.y > 0 || f.z > 0 ) && ( dot( wiw, ng ) > 0 || transmits ) &&
+						 !occluded_ray( s, p, wiw, 1e-7 * s->scale, dist * ( 1 - 1e-4 ) ) )
+					{
+						// The last vertex has no continuation that could reach the light,
+						// so its light sample takes the whole weight: the estimate is then
+						// the light of all paths of at most max_bounce + 1 segments, for
+						// whatever continuation density the other vertices use.
+						double w = variant == 3 || bounce == max_bounce ? 1.0 : pl * pl / ( pl * pl + pb * pb );
+						L = L + beta * f * s->shaders[ s->prims[ lt.prim ].shader ].emission * ( std::fabs( wi.z ) * w / pl );
+					}
 				}
 			}
 		}
-		double u1 = rng.next(), u2 = rng.next();
+		double u1 = rng.next(), u2 = rng.next(), us = rng.next();
 		V3 wi, wt;
 		double pdf;
-		m_sample( sh, wo, u1, u2, wi, wt, pdf );
+		bool delta;
+		m_sample( s->shaders, pr.shader, wo, entering, us, u1, u2, wi, wt, pdf, delta );
 		beta = beta * wt;
 		if ( beta.x == 0 && beta.y == 0 && beta.z == 0 ) break;
-		prev_pdf = pdf;
+		prev_pdf = pdf, prev_delta = delta;
 		d = fr.global( wi );
-		if ( dot( d, ng ) <= 0 ) break;
-		o = p + ng * ( 1e-7 * s->scale );
+		// a continuation on the far side of the surface leaves from that side
+		const bool through = wi.z < 0;
+		if ( through ? dot( d, ng ) >= 0 : dot( d, ng ) <= 0 ) break;
+		o = p + ng * ( ( through ? -1e-7 : 1e-7 ) * s->scale );
 		double rr = maxc( beta );
 		if ( rr < 1. && bounce > 3 )
 		{
@@ -1119,6 +1287,25 @@ int orc_add_shader( orc_scene *s, int type, const double *p )
 	return int( s->shaders.size() - 1 );
 }
 
+void orc_mis_eval( const orc_scene *s, int shader, const double *wo, const double *wi, int entering, double *f,
+				   double *pdf )
+{
+	V3 ff;
+	m_eval( s->shaders, shader, V3( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), V3( wi[ 0 ], wi[ 1 ], wi[ 2 ] ), entering != 0, ff, *pdf );
+	f[ 0 ] = ff.x, f[ 1 ] = ff.y, f[ 2 ] = ff.z;
+}
+
+int orc_mis_sample( const orc_scene *s, int shader, const double *wo, int entering, const double *u, double *wi,
+					double *weight, double *pdf )
+{
+	V3 w, i;
+	bool delta;
+	m_sample( s->shaders, shader, V3( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), entering != 0, u[ 2 ], u[ 0 ], u[ 1 ], i, w, *pdf, delta );
+	wi[ 0 ] = i.x, wi[ 1 ] = i.y, wi[ 2 ] = i.z;
+	weight[ 0 ] = w.x, weight[ 1 ] = w.y, weight[ 2 ] = w.z;
+	return delta ? 1 : 0;
+}
+
 int orc_add_point_light( orc_scene *s, const float *pos, const double *color, double strength )
 {
 	// PointLight (pointLight.hpp:13-18): emission = color * strength in float
@@ -1285,13 +1472,19 @@ int orc_render( const orc_scene *s, uint32_t W, uint32_t H, uint32_t spp, uint32
 	if ( x1 > W || y1 > H || x0 >= x1 || y0 >= y1 || spp == 0 ) return -1;
 	if ( estimator != ORC_KOISHI && estimator < ORC_AOV_NORMAL )
 	{
-		// the corrected estimator covers Lambert, Beckmann Glossy and Emission area lights
-		if ( !s->point_lights.empty() ) return -2;
+		// the corrected estimator: microfacet shaders with the Beckmann
+		// distribution, and Mixed of two leaves
+		auto leaf_ok = [&]( const Shader &sh ) {
+			if ( sh.type == ORC_MIXED ) return false;
+			if ( sh.type == ORC_GLOSSY || sh.type == ORC_GLASS || sh.type == ORC_REFRACTION )
+				return sh.dist == ORC_DIST_BECKMANN;
+			return true;
+		};
 		for ( const Prim &p : s->prims )
 		{
 			const Shader &sh = s->shaders[ p.shader ];
-			bool ok = sh.type == ORC_LAMBERT || sh.type == ORC_EMISSION ||
-					  ( sh.type == ORC_GLOSSY && sh.dist == ORC_DIST_BECKMANN );
+			bool ok = sh.type == ORC_MIXED ? leaf_ok( s->shaders[ sh.child[ 0 ] ] ) && leaf_ok( s->shaders[ sh.child[ 1 ] ] )
+										   : leaf_ok( sh );
 			if ( !ok ) return -2;
 		}
 	}
@@ -1347,7 +1540,7 @@ void orc_bsdf_eval( int estimator, int type, const double *params, const double 
 	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i( wi[ 0 ], wi[ 1 ], wi[ 2 ] ), ff3, e;
 	double pp = 0;
 	if ( estimator == ORC_MIS )
-		m_eval( sh, o, i, ff3, pp );
+		m_eval_leaf( sh, o, i, true, ff3, pp );
 	else
 	{
 		ArrayDraws d( nullptr, 0 );
@@ -1364,7 +1557,10 @@ void orc_bsdf_sample( int estimator, int type, const double *params, const doubl
 	V3 o( wo[ 0 ], wo[ 1 ], wo[ 2 ] ), i, w;
 	double pp = 0;
 	if ( estimator == ORC_MIS )
-		m_sample( sh, o, u[ 0 ], u[ 1 ], i, w, pp );
+	{
+		bool delta;
+		m_sample( std::vector<Shader>{ sh }, 0, o, true, 0.5, u[ 0 ], u[ 1 ], i, w, pp, delta );
+	}
 	else
 	{
 		ArrayDraws d( u, 2 );

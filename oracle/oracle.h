@@ -55,6 +55,15 @@ int orc_add_point_light(orc_scene *s, const float *pos, const double *color, dou
  * (draws past k read 0.5). */
 int orc_shade(const orc_scene *s, int shader, int target, const double *wo, double *wi, const double *u, int k,
               double *f, double *emission);
+/* ORC_MIS BSDF of shader id (a leaf or a Mixed of two leaves) in the local
+ * frame, wo.z > 0; entering: wo lies outside the surface as built.  eval: f
+ * and pdf of wi; sample (u = {u1, u2, selection}): wi, weight f|cos|/pdf and
+ * pdf; returns 1 for the delta (Transparent) direction, whose weight is its
+ * colour and which has no density. */
+void orc_mis_eval(const orc_scene *s, int shader, const double *wo, const double *wi, int entering, double *f,
+                  double *pdf);
+int orc_mis_sample(const orc_scene *s, int shader, const double *wo, int entering, const double *u, double *wi,
+                   double *weight, double *pdf);
 /* Primitives are numbered in the order they are added. Returns the prim id. */
 int orc_add_mesh(orc_scene *s, const float *v, uint32_t nv, const float *n, const uint32_t *idx,
                  uint32_t nt, int shader);

@@ -43,6 +43,8 @@ def lib():
             "orc_add_shader": (I, [P, I, P]),
             "orc_add_point_light": (I, [P, P, P, D]),
             "orc_shade": (I, [P, I, I, P, P, P, I, P, P]),
+            "orc_mis_eval": (None, [P, I, P, P, I, P, P]),
+            "orc_mis_sample": (I, [P, I, P, I, P, P, P, P]),
             "orc_add_mesh": (I, [P, P, U32, P, P, U32, I]),
             "orc_add_sphere": (I, [P, P, F, I]),
             "orc_set_camera": (None, [P, P, P, P, F]), "orc_set_lens": (None, [P, I]),
@@ -232,6 +234,28 @@ class OracleShader:
             lib().orc_scene_free(self.h)
         except Exception:
             pass
+
+    def mis_eval(self, wo, wi, entering=True):
+        """MIS-estimator f and pdf per (wo, wi) pair."""
+        wo, wi = (np.ascontiguousarray(x, np.float64) for x in (wo, wi))
+        f, pdf = np.zeros((len(wo), 3)), np.zeros(len(wo))
+        L, ff, pp = lib(), np.zeros(3), np.zeros(1)
+        for i in range(len(wo)):
+            L.orc_mis_eval(self.h, self.id, _p(wo[i]), _p(wi[i]), int(entering), _p(ff), _p(pp))
+            f[i], pdf[i] = ff, pp[0]
+        return f, pdf
+
+    def mis_sample(self, wo, u, entering=True):
+        """MIS-estimator samples per wo with u = (u1, u2, selection): wi,
+        weight, pdf, delta."""
+        wo, u = (np.ascontiguousarray(x, np.float64) for x in (wo, u))
+        n = len(wo)
+        wi, w, pdf, delta = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(n, bool)
+        L, a, b, pp = lib(), np.zeros(3), np.zeros(3), np.zeros(1)
+        for i in range(n):
+            delta[i] = L.orc_mis_sample(self.h, self.id, _p(wo[i]), int(entering), _p(u[i]), _p(a), _p(b), _p(pp)) == 1
+            wi[i], w[i], pdf[i] = a, b, pp[0]
+        return wi, w, pdf, delta
 
     def execute(self, target, wo, u, wi=None):
         """Per sample: f, wi, emission, draws used (target 0 eval, 1 sample)."""

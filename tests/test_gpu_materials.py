@@ -127,3 +127,45 @@ def test_mis_and_guiding_refuse_reference_only_shaders(cr, mats_scene):
         cr.bsdf_eval(cr.KOISHI, shader_configs()[-1], np.zeros((1, 3)) + [0, 0, 1], np.zeros((1, 3)) + [0, 0, 1])
     film, _ = mats_scene.render(8, 8, 4, estimator=cr.KOISHI)
     assert np.isfinite(film).all()
+
+
+def test_mis_materials_render_matches_oracle(cr, scenes):
+    """The MIS estimator over the rough dielectrics, the pass-through, the
+    blackhole, the mixtures and the point light (1 / r^2) against the FP64
+    oracle's MIS restatement."""
+    require_gpu()
+    d = scenes.config_materials(cosine=False)
+    sc = cr.Scene.from_desc(d)
+    W, H, spp = 32, 32, 1024
+    o = O.OracleScene(d).render(W, H, spp, 7, O.MIS, seed=71)
+    f = render_film(cr, sc, W, H, spp, seeds=[19, 20], estimator=cr.MIS)
+    z = zscores(f, o)
+    assert (z > 3).mean() < 0.01, (z > 3).mean()
+    assert z.max() < 5.5
+    assert abs(f.mean.mean() / o.mean.mean() - 1) < IMAGE_RTOL
+
+
+def test_guided_materials_render_is_unbiased(cr, scenes):
+    """Guiding on a scene with dielectrics and a pass-through (the guide samples
+    only the reflection-only vertices) agrees with plain MIS."""
+    require_gpu()
+    import torch
+    d = scenes.config_materials(cosine=False, point_light=False)
+    s = cr.Scene.from_desc(d)
+    cr.Guide(s).reset(seed=3).configure(steps_per_wave=2, warmup_steps=4)
+    W, H, spp = 24, 24, 512
+    plain = render_film(cr, s, W, H, spp, seeds=[21, 22], estimator=cr.MIS)
+    n = W * H
+    acc = [torch.zeros(n * 3, dtype=torch.float64, device="cuda"), torch.zeros(n * 3, dtype=torch.float64, device="cuda"),
+           torch.zeros(n, dtype=torch.int32, device="cuda")]
+    for seed in (31, 32):
+        desc = cr.render_desc(W, H, spp, max_bounce=7, estimator=cr.MIS, seed=seed, guiding=True, wave_paths=65536)
+        s.render_device(desc, acc[0].data_ptr(), acc[1].data_ptr(), acc[2].data_ptr(),
+                        stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    guided = O.Film(acc[0].cpu().numpy().reshape(H, W, 3), acc[1].cpu().numpy().reshape(H, W, 3),
+                    acc[2].cpu().numpy().astype(np.uint32).reshape(H, W))
+    assert cr.Guide(s).info()["step"] > 4
+    z = zscores(guided, plain)
+    assert (z > 3).mean() < 0.02, (z > 3).mean()
+    assert abs(guided.mean.mean() / plain.mean.mean() - 1) < IMAGE_RTOL
