@@ -118,8 +118,12 @@ int cr_scene_create_empty(cr_scene **out);
  * (Beckmann or Cosine distribution), Emission, Transparent, Blackhole,
  * RefractionBSDF, GlassBSDF and Mixed (fac Constant or Fresnel, nested
  * Mixed up to 16 deep).  config_json is the reference's [Type, {props}]
- * array.  The MIS estimator renders Lambert, Beckmann GlossyBSDF and
- * Emission only; the others have reference semantics (CR_ESTIMATOR_KOISHI).
+ * array.  CR_ESTIMATOR_KOISHI renders them all with the reference's
+ * semantics; CR_ESTIMATOR_MIS with physically restated BSDFs (rough
+ * dielectrics after Walter et al. 2007, Transparent as a delta pass-through)
+ * for microfacet shaders with the Beckmann distribution and Mixed of two
+ * leaves, and refuses the rest (Cosine-distribution microfacet shaders,
+ * nested Mixed).
  * Returns the shader id (>= 0) or an error code. */
 int cr_scene_add_shader(cr_scene *s, const char *name, const char *config_json);
 
@@ -134,8 +138,9 @@ int cr_scene_add_sphere(cr_scene *s, const float *center, float radius, const ch
 
 /* The "pointLight" asset (src/core/meta/scene.cu:156-163, pointLight.hpp:13-18):
  * emission = color (null: white) * strength, delivered to a lit point without
- * distance falloff.  Point lights precede the area lights in the light list.
- * Reference estimator only.  Returns the point light's index. */
+ * distance falloff (the reference estimator; CR_ESTIMATOR_MIS treats it as a
+ * point of intensity color * strength, with 1/r^2 falloff).  Point lights
+ * precede the area lights in the light list.  Returns the point light's index. */
 int cr_scene_add_point_light(cr_scene *s, const float *position, const float *color, float strength);
 
 /* CameraConfig (src/util/config.hpp:12-35), pinhole lens; `target` is a

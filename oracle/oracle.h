@@ -15,7 +15,12 @@
  *   ORC_MIS:    the corrected estimator the CUDA path also implements
  *               (power-heuristic MIS of BSDF sampling and area-light NEE,
  *               energy-consistent Lambert and Beckmann microfacet BSDFs,
- *               area-proportional light sampling, two-sided shading).
+ *               rough dielectrics after Walter et al. 2007, a delta
+ *               pass-through for Transparent, Mixed of two leaves, point
+ *               lights with 1/r^2 falloff, area-proportional light
+ *               sampling, two-sided shading).  orc_render's estimators 2
+ *               and 3 run it with BSDF sampling alone and with the light
+ *               samples' weights alone, for consistency checks.
  */
 #ifndef CR_ORACLE_H
 #define CR_ORACLE_H
