@@ -150,3 +150,32 @@ def test_empty_batch_is_rejected(cr):
     """cr_batch_create refuses an empty job table before touching the GPU."""
     with pytest.raises(cr.CrError):
         cr.Batch([])
+
+
+def test_scene_schema_errors_before_any_gpu_work(cr):
+    """Scene::Scene's schema checks (scene.cu:27-168, config.hpp:14-27): the
+    parse fails, with the reference's messages, before the scene is uploaded."""
+    lib = cr.lib()
+
+    def create(doc):
+        out = C.c_void_p()
+        rc = lib.cr_scene_create(json.dumps(doc).encode(), b".", C.byref(out))
+        assert not out.value
+        return rc, lib.cr_last_error().decode()
+
+    cam = {"lens": "pinhole", "position": [0, 0, 0], "target": [0, 1, 0]}
+    base = lambda assets, shaders=None, camera=cam: {"scene": {"camera": [camera], "assets": assets,
+                                                               "shaders": shaders or {}}}
+    rc, msg = create(base([["pointLight", {"color": [1, 1, 1]}]]))
+    assert rc == -2 and "position" in msg
+    rc, msg = create(base([["areaLight", {}]]))
+    assert rc == -2 and "unknown light type" in msg
+    rc, msg = create(base([["teapot", {}]]))
+    assert rc == -2 and "unknown asset type" in msg
+    rc, msg = create(base([], camera=dict(cam, lens="fisheye")))
+    assert rc == -2 and "unknown lens type" in msg
+    rc, msg = create(base([["sphere", {"o": [0, 2, 0], "r": 1, "shader": "s"}]],
+                          {"s": ["Mixed", {"fac": ["Constant", {"value": 0.5}]}]}))
+    assert rc == -2 and "shaders" in msg
+    rc, msg = create(base([["sphere", {"o": [0, 2, 0], "r": 1, "shader": "missing"}]]))
+    assert rc == -1 and "not found" in msg
