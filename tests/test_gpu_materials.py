@@ -169,3 +169,23 @@ def test_guided_materials_render_is_unbiased(cr, scenes):
     z = zscores(guided, plain)
     assert (z > 3).mean() < 0.02, (z > 3).mean()
     assert abs(guided.mean.mean() / plain.mean.mean() - 1) < IMAGE_RTOL
+
+
+def test_device_random_shader_trees_match_oracle(cr, oracle):
+    """cr_shader_execute on 24 random shader trees (nested Mixed, every leaf
+    kind, both distributions and facs) against the oracle on the same draws."""
+    require_gpu()
+    from test_oracle_materials import F_ATOL as FA, F_RTOL as FR, WI_ATOL as WA, fuzz_records, random_shader
+    rng = np.random.default_rng(2025)
+    for _ in range(24):
+        cfg = random_shader(rng)
+        wo, wi, u = fuzz_records(rng, 512)
+        o = oracle.OracleShader(cfg)
+        ref = [o.execute(t, wo, u, wi) for t in (0, 1)]
+        got = [cr.shader_execute(cfg, t, wo, u, wi) for t in (cr.SHADE_EVAL, cr.SHADE_SAMPLE)]
+        same = (got[0][3] == ref[0][3]) & (got[1][3] == ref[1][3])
+        assert same.sum() >= 510, cfg
+        for (gf, gw, ge, _), (rf, rw, re, _) in zip(got, ref):
+            np.testing.assert_allclose(gf[same], rf[same], rtol=FR, atol=FA)
+            np.testing.assert_allclose(ge[same], re[same], rtol=FR, atol=FA)
+            np.testing.assert_allclose(gw[same], rw[same], rtol=0, atol=WA)

@@ -110,3 +110,61 @@ def test_point_light_debug_kernels_match_reference(oracle, mats, kernel):
 def test_mis_refuses_reference_only_scenes(oracle, mats):
     with pytest.raises(RuntimeError, match="-2"):
         oracle.OracleScene(mats).render(8, 8, 1, 7, oracle.MIS, seed=1)
+
+
+def random_shader(rng, depth=0):
+    """A random shader config of the reference's registry, Mixed nested up to
+    three deep."""
+    beck = lambda: ["Beckmann", {"roughness": float(rng.uniform(0.05, 0.8))}]
+    dist = lambda: beck() if rng.random() < 0.7 else ["Cosine", {}]
+    col = lambda: [float(x) for x in rng.uniform(0.2, 1.0, 3)]
+    kinds = ["Lambert", "GlossyBSDF", "Emission", "Transparent", "Blackhole", "RefractionBSDF", "GlassBSDF"]
+    if depth < 3:
+        kinds += ["Mixed"] * 3
+    k = kinds[rng.integers(len(kinds))]
+    if k == "Lambert":
+        return [k, {"R": col(), "color": col()}]
+    if k == "GlossyBSDF":
+        return [k, {"distribution": dist(), "color": col()}]
+    if k == "Emission":
+        return [k, {"color": col(), "strength": float(rng.uniform(1, 10))}]
+    if k == "Transparent":
+        return [k, {"color": col()}]
+    if k == "Blackhole":
+        return [k, {}]
+    if k in ("RefractionBSDF", "GlassBSDF"):
+        return [k, {"ior": float(rng.uniform(1.1, 2.0)), "distribution": dist(), "color": col()}]
+    fac = ["Constant", {"value": float(rng.uniform(0, 1))}] if rng.random() < 0.5 else \
+        ["Fresnel", {"ior": float(rng.uniform(1.1, 2.0))}]
+    return ["Mixed", {"fac": fac, "shaders": [random_shader(rng, depth + 1), random_shader(rng, depth + 1)]}]
+
+
+def fuzz_records(rng, n, k=16):
+    d = rng.normal(size=(2 * n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return d[:n].astype(np.float32), d[n:].astype(np.float32), rng.random((n, k)).astype(np.float32)
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference harness not built")
+def test_random_shader_trees_match_reference(oracle, tmp_path):
+    """Shader::execute of 24 random shader trees (nested Mixed with every
+    leaf kind, both distributions and both facs), the reference's own code on
+    scripted draws (the harness's `shade` command) against the oracle."""
+    rng = np.random.default_rng(2024)
+    for i in range(24):
+        cfg = random_shader(rng)
+        wo, wi, u = fuzz_records(rng, 256)
+        (tmp_path / "s.json").write_text(json.dumps(cfg))
+        np.concatenate([wo, wi, u], 1).astype(np.float32).tofile(tmp_path / "r.f32")
+        oracle.ref_run("shade", "s.json", "r.f32", u.shape[1], "o.f32", cwd=str(tmp_path))
+        out = np.fromfile(tmp_path / "o.f32", np.float32).reshape(256, 17)
+        o = oracle.OracleShader(cfg)
+        fe, _, ee, ue = o.execute(0, wo, u, wi)
+        fs, ws, es, us = o.execute(1, wo, u, wi)
+        same = (ue == out[:, 6]) & (us == out[:, 16])
+        assert same.sum() >= 255, (cfg, np.nonzero(~same))
+        np.testing.assert_allclose(fe[same], out[same, 0:3], rtol=F_RTOL, atol=F_ATOL, err_msg=json.dumps(cfg))
+        np.testing.assert_allclose(ee[same], out[same, 3:6], rtol=F_RTOL, atol=F_ATOL)
+        np.testing.assert_allclose(ws[same], out[same, 7:10], rtol=0, atol=WI_ATOL)
+        np.testing.assert_allclose(fs[same], out[same, 10:13], rtol=F_RTOL, atol=F_ATOL)
+        np.testing.assert_allclose(es[same], out[same, 13:16], rtol=F_RTOL, atol=F_ATOL)
