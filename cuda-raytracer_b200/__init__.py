@@ -114,6 +114,7 @@ def lib():
             "cr_scene_add_sphere": (I, [P, P, F, C.c_char_p]),
             "cr_scene_add_point_light": (I, [P, P, P, F]),
             "cr_scene_set_lens": (I, [P, I]),
+            "cr_bvh_build": (I, [P]),
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
             "cr_scene_set_kernel": (I, [P, C.c_char_p]), "cr_mesh_file_info": (I, [C.c_char_p, P, P, P, P]),

@@ -1548,6 +1548,8 @@ int cr_scene_commit( cr_scene *s, uint64_t light_seed, void *stream )
 	} );
 }
 
+int cr_bvh_build( cr_scene *s ) { return cr_scene_commit( s, 0x330E, nullptr ); }
+
 int cr_scene_info( const cr_scene *s, uint64_t *nt, uint32_t *np, uint32_t *nl, uint32_t *nn )
 {
 	return guarded( [&] {

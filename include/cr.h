@@ -162,6 +162,9 @@ int cr_scene_set_lens(cr_scene *s, int lens);
  * light_seed seeds the reference-compatible light-point tables
  * (src/core/primitive/mesh.hpp:61-84). */
 int cr_scene_commit(cr_scene *s, uint64_t light_seed, void *stream);
+/* cr_scene_commit with the light seed that scene loading uses (the 48-bit
+ * state 0x330E) on the scene's own stream: the one-call BVH build. */
+int cr_bvh_build(cr_scene *s);
 
 /* Parses a mesh file the way an ["import", {"path"}] asset does (OBJ with
  * per-usemtl groups, PLY as one "DefaultMaterial" group, or CRM) without

@@ -111,7 +111,8 @@ def _tiny_scene(cr, tris):
     z = np.zeros(3, np.float32)
     assert lib.cr_scene_set_camera(s.h, p(z), p(np.array([0, 0, 1], np.float32)), p(np.array([0, 1, 0], np.float32)),
                                    60.0) == 0
-    assert lib.cr_scene_commit(s.h, 1, None) == 0, lib.cr_last_error()
+    # the sphere scene builds through the one-call alias
+    assert ( lib.cr_scene_commit(s.h, 1, None) if tris else lib.cr_bvh_build(s.h) ) == 0, lib.cr_last_error()
     return s
 
 
