@@ -20,13 +20,16 @@ stores its answers:
                    (Fresnel and Constant fac) and a pointLight as light 0
   c0_ortho_film.npz
                    config 0 through the OrthographicLens (lens.hpp:40-53)
+  spheres_trace.npz
+                   closest hits on a field of 300 spheres (Sphere::intersect,
+                   sphere.hpp:31-54, over every sphere per ray)
   shaders.npz      Shader::execute of each reference shader (nested Mixed
                    included) on scripted draws: for shared records
                    {wo, wi, u[12]} the f, emission and draw count of
                    compute_f_by_wi_wo and the wi, f, emission and draw count
                    of sample_wi_f_by_wo (the harness's `shade` command)
 
-Usage:  python tests/golden/make_golden.py [--aov-only | --materials-only | --ortho-only]
+Usage:  python tests/golden/make_golden.py [--aov-only | --materials-only | --ortho-only | --spheres-only]
 (the harness's render threads take rows dynamically, so a film regenerated
 from the same seed is a different Monte Carlo draw of the same image)
 """
@@ -180,6 +183,33 @@ def make_ortho(tmp):
                         scene_hash=scene_hash(d, full=True), lens=d.camera["lens"])
 
 
+def sphere_field(n=300, seed=340):
+    """n spheres of random radii in the config-0 box with the box's walls
+    removed: every hit is a sphere."""
+    rng = np.random.default_rng(seed)
+    d = scenes.config0()
+    d.groups = []
+    lo = np.array([0.3, scenes.FRONT + 0.3, 0.3])
+    hi = np.array([scenes.S - 0.3, scenes.S - 0.3, scenes.S - 0.3])
+    c = scenes._rot_points(lo + (hi - lo) * rng.random((n, 3)))
+    r = rng.uniform(0.02, 0.3, n)
+    d.spheres = [{"o": [float(x) for x in c[i]], "r": float(r[i]), "shader": "ball" if i % 2 else "glossy"}
+                 for i in range(n)]
+    d.name = "sphere_field"
+    return d
+
+
+def make_spheres(tmp):
+    d = sphere_field()
+    scenes.write_scene(d, tmp)
+    rays = make_rays(d, 2048, 12)
+    rays.tofile(os.path.join(tmp, "rays.f32"))
+    run("trace", f"{d.name}.json", "rays.f32", "hits.bin", cwd=tmp)
+    hits = np.fromfile(os.path.join(tmp, "hits.bin"), "<i4").reshape(-1, 4)
+    np.savez_compressed(os.path.join(HERE, "spheres_trace.npz"), rays=rays, kind=hits[:, 0], index=hits[:, 1],
+                        tri=hits[:, 2], t=hits[:, 3].view(np.float32), scene_hash=scene_hash(d))
+
+
 def make_materials(tmp):
     m = scenes.config_materials()
     scenes.write_scene(m, tmp)
@@ -197,7 +227,7 @@ def make_materials(tmp):
                         scene_hash=scene_hash(m, full=True))
 
 
-def main(aov_only=False, materials_only=False, ortho_only=False):
+def main(aov_only=False, materials_only=False, ortho_only=False, spheres_only=False):
     if not oracle.ref_available():
         sys.exit("build the reference harness first: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
@@ -207,6 +237,9 @@ def main(aov_only=False, materials_only=False, ortho_only=False):
             return
         if ortho_only:
             make_ortho(tmp)
+            return
+        if spheres_only:
+            make_spheres(tmp)
             return
         c0 = scenes.config0()
         scenes.write_scene(c0, tmp)
@@ -261,4 +294,4 @@ def main(aov_only=False, materials_only=False, ortho_only=False):
 
 if __name__ == "__main__":
     main(aov_only="--aov-only" in sys.argv, materials_only="--materials-only" in sys.argv,
-         ortho_only="--ortho-only" in sys.argv)
+         ortho_only="--ortho-only" in sys.argv, spheres_only="--spheres-only" in sys.argv)

@@ -190,3 +190,20 @@ def test_spheres_in_the_bvh_match_fp64(cr, scenes, oracle, n_spheres, with_box):
     ref = o.occluded(segs).astype(bool)
     assert (occ == ref).mean() >= 0.999
     assert 0.1 < ref.mean() < 0.9 or n_spheres == 1
+
+
+def test_sphere_field_matches_reference(cr):
+    """Spheres through the BVH against the reference's own Sphere::intersect
+    over every sphere (tests/golden/spheres_trace.npz)."""
+    from golden.make_golden import sphere_field
+    from test_oracle_golden import _sphere_t_allowance
+    g = golden("spheres_trace.npz")
+    d = sphere_field()
+    hits = cr.Scene.from_desc(d).trace(g["rays"])
+    p = hits["prim"]
+    same = (np.where(p < 0, -1, 1) == g["kind"]) & (np.where(p < 0, -1, p) == g["index"])
+    assert same.mean() >= 0.999, np.nonzero(~same)[0][:8]
+    both = same & (p >= 0)
+    t = hits["t"][both].astype(np.float64)
+    err = np.abs(t - g["t"][both])
+    assert (err <= 2 * _sphere_t_allowance(d, g["rays"][both], p[both], t)).all()

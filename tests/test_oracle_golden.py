@@ -116,3 +116,32 @@ def test_orthographic_render_matches_reference(oracle, scenes):
     z = np.abs(f.mean - ref.mean) / np.sqrt(f.var_of_mean + ref.var_of_mean + 1e-30)
     assert (z > 3).mean() < 0.01 and (z > 5).mean() == 0, ((z > 3).mean(), z.max())
     assert abs(f.mean.mean() / ref.mean.mean() - 1) < 0.01
+
+
+def _sphere_t_allowance(desc, rays, idx, t):
+    """1e-5 relative, plus what FP32 ray-sphere arithmetic loses on small far
+    spheres: the direction is unit length to ~1e-7 and the reference's
+    |oc|^2 - (d.oc)^2 cancels, both moving t by about |oc|^2 * 1e-7 / sqrt(det),
+    with sqrt(det) = |cos| r at the hit."""
+    cen = np.array([desc.spheres[i]["o"] for i in idx], np.float64)
+    rad = np.array([desc.spheres[i]["r"] for i in idx], np.float64)
+    ro, rd = rays[:, :3].astype(np.float64), rays[:, 3:6].astype(np.float64)
+    nrm = (ro + rd * t[:, None] - cen) / rad[:, None]
+    cos = np.abs((nrm * rd).sum(1))
+    return 1e-5 * t + 5e-7 * ((cen - ro) ** 2).sum(1) / np.maximum(cos * rad, 1e-3)
+
+
+def test_sphere_field_matches_reference(oracle):
+    """Closest hits on 300 spheres: the oracle against the reference's own
+    Sphere::intersect over every sphere (tests/golden/spheres_trace.npz)."""
+    from golden.make_golden import sphere_field
+    g = golden("spheres_trace.npz")
+    d = sphere_field()
+    assert str(g["scene_hash"]) == scene_hash(d)
+    p, tri, t, _, _ = oracle.OracleScene(d).trace(g["rays"])
+    kind = np.where(p < 0, -1, 1)
+    assert np.array_equal(kind, g["kind"]) and np.array_equal(np.where(p < 0, -1, p), g["index"])
+    hit = p >= 0
+    assert 0.3 < hit.mean() < 0.9
+    err = np.abs(t[hit] - g["t"][hit])
+    assert (err <= _sphere_t_allowance(d, g["rays"][hit], p[hit], t[hit])).all()
