@@ -23,6 +23,8 @@ stores its answers:
   spheres_trace.npz
                    closest hits on a field of 300 spheres (Sphere::intersect,
                    sphere.hpp:31-54, over every sphere per ray)
+  ico_film.npz     a Radiance render of the displaced icosphere scene (20
+                   Lambert / Beckmann patch materials)
   shaders.npz      Shader::execute of each reference shader (nested Mixed
                    included) on scripted draws: for shared records
                    {wo, wi, u[12]} the f, emission and draw count of
@@ -30,6 +32,7 @@ stores its answers:
                    of sample_wi_f_by_wo (the harness's `shade` command)
 
 Usage:  python tests/golden/make_golden.py [--aov-only | --materials-only | --ortho-only | --spheres-only]
+(--spheres-only also writes ico_film.npz)
 (the harness's render threads take rows dynamically, so a film regenerated
 from the same seed is a different Monte Carlo draw of the same image)
 """
@@ -199,6 +202,16 @@ def sphere_field(n=300, seed=340):
     return d
 
 
+def make_ico_film(tmp):
+    d = ico_scene()
+    scenes.write_scene(d, tmp)
+    run("render", f"{d.name}.json", FILM_W, FILM_H, FILM_SPP, os.cpu_count(), "film.crf", d.max_bounce, 67, cwd=tmp)
+    film = oracle.read_crf(os.path.join(tmp, "film.crf"))
+    np.savez_compressed(os.path.join(HERE, "ico_film.npz"), sum=film.sum, sumsq=film.sumsq, count=film.count,
+                        width=FILM_W, height=FILM_H, spp=FILM_SPP, max_bounce=d.max_bounce,
+                        scene_hash=scene_hash(d, full=True))
+
+
 def make_spheres(tmp):
     d = sphere_field()
     scenes.write_scene(d, tmp)
@@ -240,6 +253,7 @@ def main(aov_only=False, materials_only=False, ortho_only=False, spheres_only=Fa
             return
         if spheres_only:
             make_spheres(tmp)
+            make_ico_film(tmp)
             return
         c0 = scenes.config0()
         scenes.write_scene(c0, tmp)
