@@ -452,7 +452,8 @@ std::vector<Group> load_obj( const std::string &path )
 	};
 	std::vector<std::string> order;
 	std::map<std::string, std::vector<std::array<Corner, 3>>> faces;
-	std::string mat = "default";
+	// faces before any usemtl: the material assimp gives a mesh without one
+	std::string mat = "DefaultMaterial";
 	std::string line;
 	size_t lineno = 0;
 	auto fix = []( long i, size_t count ) -> long { return i < 0 ? long( count ) + i : i - 1; };

@@ -92,3 +92,17 @@ def test_ply_without_normals_and_bad_files(cr, scenes, tmp_path):
         cr.mesh_file_info(str(trunc))
     with pytest.raises(cr.CrError):
         cr.mesh_file_info(str(tmp_path / "missing.ply"))
+
+
+def test_obj_faces_without_material_bind_to_default_material(cr, tmp_path):
+    """OBJ faces before any usemtl get the material name assimp gives a mesh
+    without one, "DefaultMaterial"; the shader lookup fails (before any GPU
+    work) when the scene does not define it."""
+    import ctypes as C
+    import json
+    (tmp_path / "m.obj").write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
+    doc = {"scene": {"camera": [{"position": [0, 0, -1], "target": [0, 0, 1]}],
+                     "assets": [["import", {"path": "m.obj"}]], "shaders": {}}}
+    out = C.c_void_p()
+    rc = cr.lib().cr_scene_create(json.dumps(doc).encode(), str(tmp_path).encode(), C.byref(out))
+    assert rc == -1 and b"DefaultMaterial" in cr.lib().cr_last_error()
