@@ -179,3 +179,12 @@ def test_scene_schema_errors_before_any_gpu_work(cr):
     assert rc == -2 and "shaders" in msg
     rc, msg = create(base([["sphere", {"o": [0, 2, 0], "r": 1, "shader": "missing"}]]))
     assert rc == -1 and "not found" in msg
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference sources not built here")
+def test_integration_plugin_compiles_against_the_reference():
+    """The Tracer plugin the integration guide shows a maintainer adding
+    compiles against the reference's own headers (make -C oracle plugin-check)."""
+    import subprocess
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "plugin-check"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
