@@ -7,9 +7,13 @@ path: the kernel registry (``Factory<Kernel>``, src/core/kernel/kernel.impl.cu:1
 holds ``"Radiance"`` and the reference's debug kernels ``"Normal"``,
 ``"Visibility"`` and ``"HalfVector"``, the tracer registry (``Factory<Tracer>``,
 src/core/tracer/tracer.impl.cu:8-11) holds ``"CudaWavefront"`` and accepts the
-reference's ``"CPUMulticore"`` name for scene files written for it.  Every
-query runs on the GPU; there is no CPU fallback, and importing this module
-on a machine where the library is missing raises immediately on first use.
+reference's ``"CPUMulticore"`` name for scene files written for it, and the
+shader registry (``Factory<Shader>``, src/ext/shader/shader.impl.cu:16-23)
+holds all eight reference shaders, which ``shader_execute`` runs one
+``Shader::execute`` at a time.  Scenes take spheres, meshes, point lights and
+the pinhole or orthographic lens.  Every query runs on the GPU; there is no
+CPU fallback, and importing this module on a machine where the library is
+missing raises immediately on first use.
 """
 from __future__ import annotations
 
