@@ -21,8 +21,9 @@ def batch_scenes(cr, scenes):
     a = cr.Scene.from_desc(scenes.config0())
     b = cr.Scene.from_desc(scenes.config2(3, max_triangles=6000))
     c = cr.Scene.from_desc(scenes.config2(7, max_triangles=20000))
+    o = cr.Scene.from_desc(scenes.config0_ortho())  # the orthographic lens
     # (scene, width, height, spp, seed): uneven sizes; scene a twice with other seeds
-    return [(a, 48, 40, 16, 11), (b, 64, 64, 8, 12), (a, 33, 17, 5, 13), (c, 80, 48, 4, 14)]
+    return [(a, 48, 40, 16, 11), (b, 64, 64, 8, 12), (a, 33, 17, 5, 13), (c, 80, 48, 4, 14), (o, 40, 24, 6, 15)]
 
 
 def _single(cr, torch, job, estimator, seed_add=0, acc=None):
