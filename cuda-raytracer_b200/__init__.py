@@ -144,6 +144,7 @@ def lib():
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
             "cr_shader_execute": (I, [C.c_char_p, I, P, P, P, U32, U64, P, P, P]),
+            "cr_philox4x32_10": (I, [P, U64, P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -435,6 +436,15 @@ def bsdf_eval(estimator, shader_cfg, wo, wi):
     pdf = np.zeros(n, np.float32)
     _check(lib().cr_bsdf_eval(estimator, json.dumps(shader_cfg).encode(), _p(wo), _p(wi), n, _p(f), _p(pdf)))
     return f, pdf
+
+
+def philox4x32_10(ctr_key):
+    """The render's device Philox4x32-10 generator on (n, 6) words (c0..c3,
+    k0, k1); returns (n, 4) uint32 outputs."""
+    ck = np.ascontiguousarray(np.asarray(ctr_key, dtype=np.uint32).reshape(-1, 6))
+    out = np.zeros((len(ck), 4), np.uint32)
+    _check(lib().cr_philox4x32_10(_p(ck), len(ck), _p(out)))
+    return out
 
 
 SHADE_EVAL, SHADE_SAMPLE = 0, 1

@@ -1318,18 +1318,17 @@ void render_device( cr_scene *s, const cr_render_desc *desc, double *sum, double
 // ------------------------------------------------------------------ PNG
 uint32_t crc32( const unsigned char *p, size_t n, uint32_t c = 0xFFFFFFFFu )
 {
-	static uint32_t table[ 256 ];
-	static bool init = false;
-	if ( !init )
-	{
+	// built once, thread-safely (a function-local static)
+	static const std::array<uint32_t, 256> table = [] {
+		std::array<uint32_t, 256> t{};
 		for ( uint32_t i = 0; i < 256; ++i )
 		{
 			uint32_t x = i;
 			for ( int k = 0; k < 8; ++k ) x = ( x & 1 ) ? 0xEDB88320u ^ ( x >> 1 ) : x >> 1;
-			table[ i ] = x;
+			t[ i ] = x;
 		}
-		init = true;
-	}
+		return t;
+	}();
 	for ( size_t i = 0; i < n; ++i ) c = table[ ( c ^ p[ i ] ) & 0xFF ] ^ ( c >> 8 );
 	return c;
 }
@@ -1423,6 +1422,11 @@ int cr::prepare_render( cr_scene *s, const cr_render_desc *desc, DevScene &sc, R
 }
 
 void cr::set_last_error( const std::string &msg ) { g_last_error = msg; }
+
+uint32_t cr::effective_max_bounce( const cr_scene *s, const cr_render_desc *desc )
+{
+	return desc->max_bounce == UINT32_MAX ? s->max_bounce : desc->max_bounce;
+}
 
 // ====================================================================== C ABI
 extern "C" {
@@ -2279,6 +2283,25 @@ static DevShader shader_from_json( int est, const char *js )
 	if ( est == EST_MIS && !mis_helper_ok( sh ) )
 		fail( CR_ERR_UNSUPPORTED, "the MIS helpers cover Lambert, Beckmann GlossyBSDF and Emission; render to test the others" );
 	return sh;
+}
+
+int cr_philox4x32_10( const uint32_t *ctr_key, uint64_t n, uint32_t *out )
+{
+	return guarded( [&] {
+		if ( !n ) return;
+		if ( !ctr_key || !out ) fail( CR_ERR_INVALID, "null argument" );
+		if ( n > ( 1ull << 28 ) ) fail( CR_ERR_INVALID, "at most 2^28 pairs per call" );
+		uint32_t *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( uint32_t ) * 10 * n ), "cudaMalloc" );
+		cudaError_t e = cudaMemcpy( d, ctr_key, 24 * n, cudaMemcpyHostToDevice );
+		if ( e == cudaSuccess )
+		{
+			launch_philox( d, n, d + 6 * n, nullptr );
+			e = cudaMemcpy( out, d + 6 * n, 16 * n, cudaMemcpyDeviceToHost );
+		}
+		cudaFree( d );
+		cuda_check( e, "philox" );
+	} );
 }
 
 int cr_bsdf_eval( int est, const char *shader_json, const float *wo, const float *wi, uint64_t n, float *f, float *pdf )

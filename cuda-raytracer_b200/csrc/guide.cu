@@ -24,6 +24,7 @@
 #include "guide.cuh"
 #include "guide.h"
 #include "guide_tc.cuh"
+#include "render.h"
 
 namespace cr
 {
@@ -636,18 +637,8 @@ void GuideState::gradients( const GuideRecords &r, uint32_t n, cudaStream_t st, 
 {
 	if ( tensor_cores )
 	{
-		static bool tattr = false;
-		if ( !tattr )
-		{
-			check( cudaFuncSetAttribute( k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-										 int( tt::SMEM_BYTES ) ),
-				   "guide tc train smem" );
-			tattr = true;
-		}
-		int device = 0, sms = 0;
-		check( cudaGetDevice( &device ), "device" );
-		check( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, device ), "device" );
-		uint32_t blocks = std::min<uint32_t>( ( n + tt::THREADS - 1 ) / tt::THREADS, uint32_t( sms ) );
+		ensure_smem_limit( reinterpret_cast<const void *>( k_guide_train_tc ), int( tt::SMEM_BYTES ), "guide tc train smem" );
+		uint32_t blocks = std::min<uint32_t>( ( n + tt::THREADS - 1 ) / tt::THREADS, uint32_t( sm_count() ) );
 		if ( blocks == 0 ) return;
 		pack_weights( st );
 		check( cudaMemsetAsync( loss, 0, 4, st ), "guide train" );
@@ -655,14 +646,8 @@ void GuideState::gradients( const GuideRecords &r, uint32_t n, cudaStream_t st, 
 		check( cudaGetLastError(), "guide train" );
 		return;
 	}
-	static bool attr = false;
-	if ( !attr )
-	{
-		check( cudaFuncSetAttribute( k_guide_train_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, int( TRAIN_SMEM ) ),
-			   "guide smem" );
-		attr = true;
-	}
-	uint32_t blocks = std::min<uint32_t>( ( n + TRAIN_ROWS - 1 ) / TRAIN_ROWS, 148 * 2 );
+	ensure_smem_limit( reinterpret_cast<const void *>( k_guide_train_fp32 ), int( TRAIN_SMEM ), "guide smem" );
+	uint32_t blocks = std::min<uint32_t>( ( n + TRAIN_ROWS - 1 ) / TRAIN_ROWS, uint32_t( sm_count() ) * 2 );
 	if ( blocks == 0 ) return;
 	check( cudaMemsetAsync( loss, 0, 4, st ), "guide train" );
 	k_guide_train_fp32<<<blocks, TRAIN_ROWS, TRAIN_SMEM, st>>>( r, n, dev(), wsum, gW, gb, ggrid, loss );
@@ -698,20 +683,10 @@ void GuideState::pack_weights( cudaStream_t st )
 uint32_t GuideState::forward_batch_tc( const float *d_in, uint32_t n, float *d_out, cudaStream_t st )
 {
 	if ( reinterpret_cast<uintptr_t>( d_out ) % 16 ) throw std::runtime_error( "guide forward: output not 16-byte aligned" );
-	static bool attr = false;
-	if ( !attr )
-	{
-		check( cudaFuncSetAttribute( k_guide_forward_batch_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-									 int( tc::SMEM_BYTES ) ),
-			   "guide tc smem" );
-		attr = true;
-	}
+	ensure_smem_limit( reinterpret_cast<const void *>( k_guide_forward_batch_tc ), int( tc::SMEM_BYTES ), "guide tc smem" );
 	check( cudaMemsetAsync( err, 0, 4, st ), "guide forward" );
 	pack_weights( st );
-	int device = 0, sms = 0;
-	check( cudaGetDevice( &device ), "device" );
-	check( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, device ), "device" );
-	uint32_t blocks = std::min<uint32_t>( ( n + tc::THREADS - 1 ) / tc::THREADS, uint32_t( sms ) * 2 );
+	uint32_t blocks = std::min<uint32_t>( ( n + tc::THREADS - 1 ) / tc::THREADS, uint32_t( sm_count() ) * 2 );
 	if ( blocks )
 		k_guide_forward_batch_tc<<<blocks, tc::THREADS, tc::SMEM_BYTES, st>>>( dev(), Wp, d_in, n, d_out, err );
 	check( cudaGetLastError(), "guide forward" );

@@ -13,6 +13,10 @@ namespace cr
 // allocation, no synchronisation.  Returns CR_OK or an error code with the
 // message in `err`.
 int prepare_render( cr_scene *s, const cr_render_desc *desc, DevScene &sc, RenderConfig &cfg, std::string &err );
+// The max_bounce a render request resolves to: desc->max_bounce, or the
+// scene's (from its kernel's "maxBounce") when the request leaves it at
+// UINT32_MAX.  Host work only.
+uint32_t effective_max_bounce( const cr_scene *s, const cr_render_desc *desc );
 // Records the message returned by cr_last_error() on this thread.
 void set_last_error( const std::string &msg );
 }  // namespace cr

@@ -107,6 +107,22 @@ extern "C" int cr_render_device_noalloc( cr_scene *s, const cr_render_desc *desc
 						std::to_string( CR_NOALLOC_MAX_WAVE_PATHS ) + " paths" );
 		return CR_ERR_INVALID;
 	}
+	// Requests this entry point cannot serve are refused before the request is
+	// resolved: resolving a guided request would set up the scene's guide and
+	// its training records, which allocates.
+	if ( desc->guiding )
+	{
+		set_last_error( "cr_render_device_noalloc does not take guided renders (the guide's training records are "
+						"allocated per scene); use cr_render_device" );
+		return CR_ERR_UNSUPPORTED;
+	}
+	const uint32_t max_bounce = effective_max_bounce( s, desc );
+	if ( max_bounce > CR_NOALLOC_MAX_BOUNCE )
+	{
+		set_last_error( "max_bounce " + std::to_string( max_bounce ) + " exceeds the no-allocation maximum of " +
+						std::to_string( CR_NOALLOC_MAX_BOUNCE ) );
+		return CR_ERR_INVALID;
+	}
 	DevScene sc;
 	RenderConfig cfg;
 	int rc = prepare_render( s, desc, sc, cfg, err );
@@ -114,12 +130,6 @@ extern "C" int cr_render_device_noalloc( cr_scene *s, const cr_render_desc *desc
 	{
 		set_last_error( err );
 		return rc;
-	}
-	if ( cfg.max_bounce > CR_NOALLOC_MAX_BOUNCE )
-	{
-		set_last_error( "max_bounce " + std::to_string( cfg.max_bounce ) + " exceeds the no-allocation maximum of " +
-						std::to_string( CR_NOALLOC_MAX_BOUNCE ) );
-		return CR_ERR_INVALID;
 	}
 	unsigned char *base = nullptr;
 	rc = scratch_address( &base, err );

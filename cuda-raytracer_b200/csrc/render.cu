@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -994,6 +996,17 @@ __global__ void k_shader_execute( const DevShader *tab, int target, const float 
 	}
 }
 
+// The render's generator on scripted (counter, key) pairs (cr_philox4x32_10).
+__global__ void k_philox( const uint32_t *ck, uint64_t n, uint32_t *out )
+{
+	for ( uint64_t i = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; i < n; i += uint64_t( gridDim.x ) * blockDim.x )
+	{
+		const uint32_t *q = ck + 6 * i;
+		const uint4 r = philox4x32_10( make_uint4( q[ 0 ], q[ 1 ], q[ 2 ], q[ 3 ] ), make_uint2( q[ 4 ], q[ 5 ] ) );
+		out[ 4 * i ] = r.x, out[ 4 * i + 1 ] = r.y, out[ 4 * i + 2 ] = r.z, out[ 4 * i + 3 ] = r.w;
+	}
+}
+
 void check( cudaError_t e, const char *what )
 {
 	if ( e != cudaSuccess ) throw std::runtime_error( std::string( what ) + ": " + cudaGetErrorString( e ) );
@@ -1027,17 +1040,42 @@ struct EventPool
 
 }  // namespace
 
+namespace
+{
+constexpr int MAX_DEVICES = 64;
+std::mutex g_dev_mutex;
+int g_sms[ MAX_DEVICES ] = {};
+std::set<std::pair<int, const void *>> g_smem_set;
+
+int current_device()
+{
+	int dev = 0;
+	check( cudaGetDevice( &dev ), "cudaGetDevice" );
+	return dev;
+}
+}  // namespace
+
 int sm_count()
 {
-	static int n = 0;
-	if ( !n )
+	const int dev = current_device();
+	if ( dev < 0 || dev >= MAX_DEVICES ) throw std::runtime_error( "device index out of range" );
+	std::lock_guard<std::mutex> lock( g_dev_mutex );
+	if ( !g_sms[ dev ] )
 	{
-		int dev = 0;
-		cudaGetDevice( &dev );
-		cudaDeviceGetAttribute( &n, cudaDevAttrMultiProcessorCount, dev );
-		if ( n <= 0 ) n = 148;
+		int n = 0;
+		check( cudaDeviceGetAttribute( &n, cudaDevAttrMultiProcessorCount, dev ), "SM count" );
+		g_sms[ dev ] = n > 0 ? n : 148;
 	}
-	return n;
+	return g_sms[ dev ];
+}
+
+void ensure_smem_limit( const void *fn, int bytes, const char *what )
+{
+	const int dev = current_device();
+	std::lock_guard<std::mutex> lock( g_dev_mutex );
+	if ( g_smem_set.count( { dev, fn } ) ) return;
+	check( cudaFuncSetAttribute( fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes ), what );
+	g_smem_set.insert( { dev, fn } );
 }
 
 void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaStream_t st )
@@ -1253,13 +1291,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		if ( cfg.guiding && guide->step >= guide->warmup_steps )
 		{
 			wc.guide_sample = true;
-			static bool smem_attr0 = false;
-			if ( !smem_attr0 )
-			{
-				check( cudaFuncSetAttribute( k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int( tc::SMEM_BYTES ) ),
-					   "guide inference smem" );
-				smem_attr0 = true;
-			}
+			ensure_smem_limit( reinterpret_cast<const void *>( k_guide_infer ), int( tc::SMEM_BYTES ), "guide inference smem" );
 			if ( guide->packed_step != guide->step )  // BF16 copy of the weights this wave samples with
 			{
 				guide->pack_weights( st );
@@ -1388,6 +1420,14 @@ void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hi
 		k_traverse<QueryIO, false, false><<<g, 128, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
 																  QUERY_REFILL_MIN );
 	check( cudaGetLastError(), "trace launch" );
+}
+
+void launch_philox( const uint32_t *ctr_key, uint64_t n, uint32_t *out, cudaStream_t st )
+{
+	if ( !n ) return;
+	int g = int( std::min<uint64_t>( ( n + 255 ) / 256, 4096 ) );
+	k_philox<<<g, 256, 0, st>>>( ctr_key, n, out );
+	check( cudaGetLastError(), "philox launch" );
 }
 
 void launch_bsdf_eval( int est, const DevShader &sh, const float *wo, const float *wi, uint64_t n, float *f, float *pdf,

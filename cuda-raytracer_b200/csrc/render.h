@@ -126,5 +126,15 @@ void launch_bsdf_sample( int estimator, const DevShader &sh, const float *wo, co
 void launch_shader_execute( const DevShader *tab, int target, const float *wo, float *wi, const float *u, uint32_t k,
 							uint64_t n, float *f, float *emission, uint32_t *used, cudaStream_t st );
 
+// Philox4x32-10 of the render (cr_device.cuh) on n (c0..c3, k0, k1) device
+// words; out n x 4 device words.
+void launch_philox( const uint32_t *ctr_key, uint64_t n, uint32_t *out, cudaStream_t st );
+
+// SMs of the current device (cached per device).
 int sm_count();
+
+// Raises the dynamic shared-memory limit of kernel `fn` to `bytes` on the
+// current device.  The attribute belongs to a device's context, so it is set
+// once per (device, kernel); thread-safe.
+void ensure_smem_limit( const void *fn, int bytes, const char *what );
 }  // namespace cr

@@ -259,7 +259,8 @@ int cr_render_device(cr_scene *s, const cr_render_desc *desc, double *d_sum, dou
  * must already be committed; the caller passes the film buffers as for
  * cr_render_device.  desc->wave_paths above CR_NOALLOC_MAX_WAVE_PATHS, or a
  * max_bounce above CR_NOALLOC_MAX_BOUNCE, is rejected with CR_ERR_INVALID
- * (wave_paths 0 means the maximum).  The first call on a device looks up the
+ * (wave_paths 0 means the maximum); a guided request (desc->guiding) with
+ * CR_ERR_UNSUPPORTED, before anything about the scene changes.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) with that device current;
  * make that first call before any stream capture.  Every call on a device
  * shares the one array, so calls whose work overlaps on the GPU (concurrent
@@ -421,6 +422,15 @@ int cr_bsdf_sample(int estimator, const char *shader_json, const float *wo, cons
 #define CR_SHADE_SAMPLE 1
 int cr_shader_execute(const char *shader_json, int target, const float *wo, float *wi, const float *u, uint32_t k,
                       uint64_t n, float *f, float *emission, uint32_t *used);
+
+/* --------------------------------------------------- random number parity */
+/* No counterpart in the reference: its Sampler is a 48-bit linear
+ * congruential generator (src/core/misc/sampler.hpp:22-36), which the CUDA
+ * path replaces with counter-based Philox4x32-10 (Salmon et al., SC'11).
+ * Runs the render's own device generator on n (counter, key) pairs, host
+ * arrays: ctr_key n x 6 words (c0, c1, c2, c3, k0, k1), out n x 4 words.
+ * For known-answer tests of the generator. */
+int cr_philox4x32_10(const uint32_t *ctr_key, uint64_t n, uint32_t *out);
 
 #ifdef __cplusplus
 }

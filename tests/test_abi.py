@@ -13,7 +13,7 @@ from conftest import ROOT
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "cr.h")).read()
-    return sorted(set(re.findall(r"\b(cr_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(cr_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_header_declares_the_boundary():
