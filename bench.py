@@ -49,6 +49,8 @@ WIDTH, HEIGHT, SPP, LEVEL, MAX_BOUNCE = 1024, 768, 256, 8, 7
 METRIC = ("Msamples/s (camera paths per second), plain wavefront, 1024x768x256spp, 1.31M-tri displaced icosphere; "
           "time-to-relMSE 1e-3 guided vs plain in 'guiding'")
 NODE_BYTES, TRI_BYTES, RAY_BYTES = 80, 48, 32 + 16
+C0_WORKLOAD = ("config0: box scene (20 triangles, 2 spheres, ceiling light), 256x256 at 64 spp, depth 8, "
+               "reference estimator")
 
 
 def load_pkg():
@@ -173,11 +175,11 @@ def make_workload(tmpdir):
 
 
 # ---------------------------------------------------------------------------- reference arm
-def reference_rate(scene_json, steps, warmup, spp):
+def reference_rate(scene_json, steps, warmup, spp, width=WIDTH, height=HEIGHT):
     """Reference CPU Radiance path (oracle/_ref/cr_ref bench) on all host threads."""
     import oracle
     threads = os.cpu_count() or 1
-    r = subprocess.run([oracle.REF_BIN, "bench", os.path.basename(scene_json), str(WIDTH), str(HEIGHT), str(spp),
+    r = subprocess.run([oracle.REF_BIN, "bench", os.path.basename(scene_json), str(width), str(height), str(spp),
                         str(threads), str(MAX_BOUNCE), str(steps + warmup)], cwd=os.path.dirname(scene_json),
                        capture_output=True, text=True, timeout=3600, check=True)
     runs = [json.loads(l) for l in r.stderr.splitlines() if l.startswith("{")]
@@ -190,6 +192,21 @@ def reference_rate(scene_json, steps, warmup, spp):
     return samples / secs / 1e6, secs / max(len(timed), 1), used, samples // max(len(timed), 1)
 
 
+def reference_config0(repeats=3):
+    """The reference's CPUMulticoreTracer::execute on the whole small box scene
+    (256x256 at 64 spp, depth 8, 20 triangles + 2 spheres): the one
+    configuration it renders in full within seconds, so that both arms time
+    the identical workload.  Returns the line's config0 section."""
+    from cuda_raytracer_b200 import scenes
+    with tempfile.TemporaryDirectory() as tmp:
+        d = scenes.config0()
+        path = scenes.write_scene(d, tmp)
+        rate, sec, cores, samples = reference_rate(path, repeats - 1, 1, d.spp, width=d.width, height=d.height)
+    return {"workload": C0_WORKLOAD, "msamples_per_s": round(rate, 4), "ms_per_render": round(sec * 1e3, 2),
+            "samples_per_render": samples, "cores": cores, "renders_timed": repeats - 1,
+            "kind": "reference", "same_config": True}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -198,6 +215,8 @@ def run_reference(args):
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cr_ref was not built (make -C oracle ref)"}))
         return
+    load_pkg()
+    c0 = reference_config0()
     with tempfile.TemporaryDirectory() as tmp:
         _, path = make_workload(tmp)
         rate, sec, cores, samples = reference_rate(path, args.steps, args.warmup, args.ref_spp)
@@ -211,6 +230,7 @@ def run_reference(args):
         "cpu_baseline": {"value": round(rate, 4), "unit": "Msamples/s", "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(rate, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config0": c0,
     }
     print(json.dumps(line), flush=True)
 
@@ -287,6 +307,91 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
            "speedup": (round(plain["time_to_target_s"] / guided["time_to_target_s"], 3)
                        if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
     sc.close()
+    return out
+
+
+def config0_section(cr, dev, steps, warmup, l2_gbs, with_reference):
+    """The small box scene at its full configuration (256x256, 64 spp, depth 8,
+    reference estimator), the workload both arms run identically.  Device
+    throughput over `steps` renders (CUDA events, L2 flushed between renders),
+    end to end through the public API from host arrays (scene upload, GPU BVH
+    build, render, film to host), the closest-hit kernel's bandwidth against
+    the in-run L2 read peak (the whole scene, 6 KB of nodes and triangles,
+    lives in L2), and the reference CPU tracer on the same full render."""
+    import numpy as np
+    import torch
+    from cuda_raytracer_b200 import scenes
+    d = scenes.config0()
+    W, H, spp = d.width, d.height, d.spp
+    sc = cr.Scene.from_desc(d)
+    n = W * H
+    f = [torch.zeros(n * 3, dtype=torch.float64, device=dev), torch.zeros(n * 3, dtype=torch.float64, device=dev),
+         torch.zeros(n, dtype=torch.int32, device=dev)]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    tune = sc.autotune(cr.render_desc(W, H, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=99),
+                       stream=stream.cuda_stream).as_dict()
+
+    def render(seed, stats=True, count=False):
+        rd = cr.render_desc(W, H, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=seed, count_work=count)
+        return sc.render_device(rd, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), stream=stream.cuda_stream,
+                                stats=stats)
+
+    for w in range(warmup):
+        render(300 + w)
+    cst = render(4242, count=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    tot = {"extend": 0.0, "ext_launches": 0, "launches": 0, "samples": 0}
+    torch.cuda.synchronize(dev)
+    for k in range(steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        st = render(500 + k)
+        ev[k][1].record(stream)
+        tot["extend"] += st.ms_extend
+        tot["ext_launches"] += st.extend_launches
+        tot["launches"] += st.launches
+        tot["samples"] += st.samples
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    ext_bytes = (cst.nodes * NODE_BYTES + cst.tris * TRI_BYTES + cst.rays_extend * RAY_BYTES) / max(cst.extend_launches, 1)
+    ext_ms = tot["extend"] / max(tot["ext_launches"], 1)
+    achieved = ext_bytes / (ext_ms / 1e3) / 1e9
+    times = []
+    for k in range(3):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s2 = cr.Scene.from_desc(d)
+        film, _ = s2.render(W, H, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k,
+                            **{k2: tune[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm")})
+        s2.close()
+        times.append(time.perf_counter() - t0)
+        assert np.isfinite(film).all()
+    e2e_ms = statistics.mean(times[1:]) * 1e3
+    out = {"workload": C0_WORKLOAD, "msamples_per_s": round(tot["samples"] / ms / 1e3, 3),
+           "ms_per_render": round(ms / steps, 3), "renders_timed": steps, "launches_per_render": tot["launches"] // steps,
+           "e2e": {"msamples_per_s": round(n * spp / e2e_ms / 1e3, 3), "ms_per_render": round(e2e_ms, 2),
+                   "h2d_bytes": int(sum(g.v.nbytes + g.n.nbytes + g.f.nbytes for g in d.groups)),
+                   "d2h_bytes": n * 3 * 8, "includes": "scene upload, GPU BVH build, render, film copy to host"},
+           "roofline": {"bound": "l2", "kernel": "k_extend", "achieved": round(achieved, 1), "peak": round(l2_gbs, 1),
+                        "unit": "GB/s", "frac": round(achieved / l2_gbs, 4),
+                        "peak_source": "measured in this run (cr_measure_peaks: 32 MB L2-resident reads)",
+                        "algorithmic_bytes_per_launch": round(ext_bytes), "launch_ms": round(ext_ms, 4),
+                        "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
+                        "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3)},
+           "autotuned": tune}
+    if with_reference:
+        import oracle
+        if oracle.ref_available():
+            ref = reference_config0()
+            out["cpu_baseline"] = {"value": ref["msamples_per_s"], "unit": "Msamples/s", "cores": ref["cores"],
+                                   "kind": "reference", "sample": "the whole configuration (256x256 at 64 spp), "
+                                                                  f"{ref['renders_timed']} timed renders"}
+            out["same_config"] = True
+            out["speedup_vs_reference"] = round(out["msamples_per_s"] / ref["msamples_per_s"], 1)
+            out["e2e_speedup_vs_reference"] = round(out["e2e"]["msamples_per_s"] / ref["msamples_per_s"], 1)
+    sc.close()
+    del flush
     return out
 
 
@@ -607,6 +712,10 @@ def run_ours(args):
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/cr_ref not built"}
 
+    c0 = None
+    if rank == 0 and world == 1 and not args.no_config0:
+        c0 = config0_section(cr, dev, 20, 3, l2_gbs, not args.no_cpu_baseline)
+
     guiding = None
     if rank == 0 and world == 1 and args.guide_seconds > 0:
         del s, q, c, flush
@@ -650,6 +759,7 @@ def run_ours(args):
             "e2e": e2e,
             "clocks": clk,
             "gpu_launches": totals["launches"],
+            "config0": c0,
             "guiding": guiding,
             "batch": batch,
         }
@@ -670,6 +780,7 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=4, help="spp of the reference's bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-config0", action="store_true", help="skip the small box scene's section")
     ap.add_argument("--guide-seconds", type=float, default=25.0,
                     help="device-time cap of each guided/plain time-to-relMSE run (0: skip them)")
     ap.add_argument("--guide-ref-spp", type=int, default=4096)

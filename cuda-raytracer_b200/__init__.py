@@ -125,7 +125,7 @@ def lib():
             "cr_measure_peaks": (I, [P, P, P]),
             "cr_scene_info": (I, [P, P, P, P, P]),
             "cr_scene_destroy": (None, [P]),
-            "cr_light_table": (I, [P, U32, P, P]),
+            "cr_light_table": (I, [P, U32, P, P]), "cr_scene_set_light_table": (I, [P, U32, P, F]),
             "cr_trace_rays": (I, [P, P, U64, P, I]),
             "cr_trace_rays_device": (I, [P, P, U64, P, I, P]),
             "cr_render": (I, [P, P, P, P]),
@@ -289,6 +289,12 @@ class Scene:
         st = Stats()
         _check(lib().cr_render(self.h, C.byref(d), _p(film), C.byref(st)))
         return film, st
+
+    def set_light_table(self, primitive, table, pdf):
+        """cr_scene_set_light_table: the 1024-point table (1024 x 6: p, n) and
+        area pdf of the emissive mesh `primitive`, e.g. a reference Mesh's own."""
+        t = np.ascontiguousarray(table, np.float32).reshape(1024, 6)
+        _check(lib().cr_scene_set_light_table(self.h, int(primitive), _p(t), float(pdf)))
 
     def autotune(self, desc, stream=0):
         """cr_autotune: pick and keep the launch configuration for this scene."""

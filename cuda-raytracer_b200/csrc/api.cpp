@@ -151,6 +151,7 @@ struct cr_scene
 	DevBuf<uint32_t> err;
 	std::vector<DevLight> lights;
 	std::vector<float4> tables_host;
+	std::vector<int> prim_light;  // light id of each primitive, -1 for none (set at commit)
 	std::string mis_blocker;  // why the MIS estimator cannot render this scene (empty: it can)
 	uint64_t n_tris = 0;
 	float scale = 1;
@@ -1114,6 +1115,7 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	s->err.upload( std::vector<uint32_t>( 2, 0 ) );  // [0] error word, [1] query work cursor
 	s->lights = lights;
 	s->tables_host = tables;
+	s->prim_light = prim_light;
 	// BVH over the triangles (ids 0 .. nt-1) and the spheres (ids nt ..)
 	const uint64_t n_prims = src.size() / 3;
 	if ( n_prims >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many primitives" );
@@ -1586,6 +1588,33 @@ int cr_light_table( const cr_scene *s, uint32_t light, float *out, float *pdf )
 	} );
 }
 
+int cr_scene_set_light_table( cr_scene *s, uint32_t primitive, const float *points, float pdf )
+{
+	return guarded( [&] {
+		if ( !s || !points ) fail( CR_ERR_INVALID, "null argument" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		if ( primitive >= s->prim_light.size() || s->prim_light[ primitive ] < 0 )
+			fail( CR_ERR_INVALID, "primitive is not an emissive mesh" );
+		const uint32_t light = uint32_t( s->prim_light[ primitive ] );
+		DevLight &L = s->lights[ light ];
+		if ( L.kind != LIGHT_MESH ) fail( CR_ERR_INVALID, "primitive is not an emissive mesh" );
+		if ( !( pdf > 0.f ) || !std::isfinite( pdf ) ) fail( CR_ERR_INVALID, "light table pdf must be positive" );
+		for ( int i = 0; i < 1024; ++i )
+		{
+			const float *q = points + 6 * i;
+			for ( int k = 0; k < 6; ++k )
+				if ( !std::isfinite( q[ k ] ) ) fail( CR_ERR_INVALID, "light table point is not finite" );
+			s->tables_host[ 2 * ( L.table + i ) ] = make_float4( q[ 0 ], q[ 1 ], q[ 2 ], 0.f );
+			s->tables_host[ 2 * ( L.table + i ) + 1 ] = make_float4( q[ 3 ], q[ 4 ], q[ 5 ], 0.f );
+		}
+		L.koishi_pdf = pdf;
+		cuda_check( cudaMemcpy( s->light_tables.p + 2 * size_t( L.table ), &s->tables_host[ 2 * size_t( L.table ) ],
+								sizeof( float4 ) * 2048, cudaMemcpyHostToDevice ),
+					"light table upload" );
+		cuda_check( cudaMemcpy( s->dlights.p + light, &L, sizeof( DevLight ), cudaMemcpyHostToDevice ), "light upload" );
+	} );
+}
+
 int cr_trace_rays_device( cr_scene *s, const float *d_rays, uint64_t n, cr_hit *d_hits, int any_hit, void *stream )
 {
 	return guarded( [&] {
@@ -1659,6 +1688,126 @@ int cr_render( cr_scene *s, const cr_render_desc *desc, double *film, cr_stats *
 		check_device_error( s, st );
 		for ( size_t p = 0; p < npx; ++p )
 			for ( int c = 0; c < 3; ++c ) film[ 3 * p + c ] = hc[ p ] ? film[ 3 * p + c ] / hc[ p ] : 0.0;
+	} );
+}
+
+int cr_render_profile( cr_scene *s, const cr_render_desc *desc, uint32_t depth, cr_profile_slice *slices,
+					   cr_profile_bounce *bounces, double *film )
+{
+	return guarded( [&] {
+		if ( !slices || ( depth && !bounces ) ) fail( CR_ERR_INVALID, "null argument" );
+		if ( depth > 64 ) fail( CR_ERR_INVALID, "profile depth must be at most 64" );
+		Resolved r = resolve( s, desc );
+		if ( r.cfg.estimator != EST_KOISHI || r.cfg.kernel != KERNEL_RADIANCE || r.cfg.guiding )
+			fail( CR_ERR_UNSUPPORTED, "the profile is RadianceKernel's: the Radiance kernel with the reference estimator" );
+		const uint64_t n = r.samples;
+		if ( n * std::max<uint64_t>( depth, 1 ) > ( 1ull << 28 ) )
+			fail( CR_ERR_INVALID, "profile too large: at most 2^28 bounce records" );
+		cudaStream_t st = s->stream;
+		const size_t npx = size_t( r.cfg.ww ) * r.cfg.wh;
+		ProfileDev pd;
+		pd.depth = depth;
+		double *sum = nullptr, *sq = nullptr;
+		uint32_t *cnt = nullptr;
+		auto release = [&] {
+			for ( void *p : { (void *)pd.slices, (void *)pd.bounces, (void *)sum, (void *)sq, (void *)cnt } )
+				if ( p ) cudaFreeAsync( p, st );
+		};
+		try
+		{
+			cuda_check( cudaMallocAsync( (void **)&pd.slices, sizeof( cr_profile_slice ) * n, st ), "cudaMalloc" );
+			cuda_check( cudaMemsetAsync( pd.slices, 0, sizeof( cr_profile_slice ) * n, st ), "memset" );
+			if ( depth )
+			{
+				cuda_check( cudaMallocAsync( (void **)&pd.bounces, sizeof( cr_profile_bounce ) * n * depth, st ), "cudaMalloc" );
+				cuda_check( cudaMemsetAsync( pd.bounces, 0, sizeof( cr_profile_bounce ) * n * depth, st ), "memset" );
+			}
+			else
+				pd.bounces = reinterpret_cast<cr_profile_bounce *>( pd.slices );  // never written at depth 0
+			cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+			cuda_check( cudaMemsetAsync( sum, 0, npx * 24, st ), "memset" );
+			cuda_check( cudaMemsetAsync( sq, 0, npx * 24, st ), "memset" );
+			cuda_check( cudaMemsetAsync( cnt, 0, npx * 4, st ), "memset" );
+			r.cfg.prof = pd;
+			ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st );
+			render_waves( r.sc, r.cfg, s->wave, sum, sq, cnt, st, nullptr, &s->guide );
+			cuda_check( cudaMemcpyAsync( slices, pd.slices, sizeof( cr_profile_slice ) * n, cudaMemcpyDeviceToHost, st ),
+						"download" );
+			if ( depth )
+				cuda_check( cudaMemcpyAsync( bounces, pd.bounces, sizeof( cr_profile_bounce ) * n * depth,
+											 cudaMemcpyDeviceToHost, st ),
+							"download" );
+			std::vector<uint32_t> hc( npx );
+			std::vector<double> hs( film ? npx * 3 : 0 );
+			if ( film )
+			{
+				cuda_check( cudaMemcpyAsync( hs.data(), sum, npx * 24, cudaMemcpyDeviceToHost, st ), "download" );
+				cuda_check( cudaMemcpyAsync( hc.data(), cnt, npx * 4, cudaMemcpyDeviceToHost, st ), "download" );
+			}
+			cuda_check( cudaStreamSynchronize( st ), "profile" );
+			if ( pd.bounces == reinterpret_cast<cr_profile_bounce *>( pd.slices ) ) pd.bounces = nullptr;
+			release();
+			check_device_error( s, st );
+			if ( film )
+				for ( size_t p = 0; p < npx; ++p )
+					for ( int c = 0; c < 3; ++c ) film[ 3 * p + c ] = hc[ p ] ? hs[ 3 * p + c ] / hc[ p ] : 0.0;
+		}
+		catch ( ... )
+		{
+			if ( pd.bounces == reinterpret_cast<cr_profile_bounce *>( pd.slices ) ) pd.bounces = nullptr;
+			release();
+			throw;
+		}
+	} );
+}
+
+// Profiler::~Profiler (src/core/kernel/kernel.cu) and
+// RadianceKernel::Slice::writeSlice (src/core/kernel/radiance.hpp:31-47): the
+// reference's text, with its vectors printed as "[ x, y, z ]" (vec.hpp:220-251)
+// and numbers in the stream's default format.
+static void write_profile( std::ostream &os, const uint32_t area[ 4 ], uint32_t spp, uint32_t depth,
+						   const cr_profile_slice *slices, const cr_profile_bounce *bounces )
+{
+	auto v3 = [&]( const float *v ) { os << "[ " << v[ 0 ] << ", " << v[ 1 ] << ", " << v[ 2 ] << " ]"; };
+	const uint32_t aw = area[ 2 ] - area[ 0 ], ah = area[ 3 ] - area[ 1 ];
+	for ( uint32_t y = 0; y != ah; ++y )
+		for ( uint32_t x = 0; x != aw; ++x )
+			for ( uint32_t k = 0; k != spp; ++k )
+			{
+				os << "at [ " << x + area[ 0 ] << ", " << y + area[ 1 ] << ", " << k << " ]: " << std::endl;
+				const size_t si = ( size_t( aw ) * y + x ) * spp + k;
+				const cr_profile_slice &sl = slices[ si ];
+				if ( sl.L[ 0 ] >= 1e2f && sl.L[ 1 ] >= 1e2f && sl.L[ 2 ] >= 1e2f )
+				{
+					os << "bounce: " << size_t( sl.bounce ) << " / " << size_t( depth ) << std::endl;
+					for ( uint32_t i = 0; i != std::min( sl.bounce, depth ); ++i )
+					{
+						const cr_profile_bounce &b = bounces[ si * depth + i ];
+						os << "ray: ";
+						v3( b.ray_o );
+						v3( b.ray_d );
+						os << std::endl << "f: ";
+						v3( b.f );
+						os << std::endl << "theta: " << b.theta << std::endl << "L: ";
+						v3( b.L );
+						os << std::endl << "shader: " << b.shader << std::endl;
+					}
+				}
+			}
+}
+
+int cr_profile_write( const char *path, const uint32_t area[ 4 ], uint32_t spp, uint32_t depth,
+					  const cr_profile_slice *slices, const cr_profile_bounce *bounces )
+{
+	return guarded( [&] {
+		if ( !path || !area || !slices || ( depth && !bounces ) ) fail( CR_ERR_INVALID, "null argument" );
+		if ( area[ 2 ] < area[ 0 ] || area[ 3 ] < area[ 1 ] ) fail( CR_ERR_INVALID, "bad profile area" );
+		std::ofstream of( path );
+		if ( !of ) fail( CR_ERR_INVALID, std::string( "cannot write " ) + path );
+		write_profile( of, area, spp, depth, slices, bounces );
+		if ( !of ) fail( CR_ERR_INVALID, std::string( "write failed: " ) + path );
 	} );
 }
 
@@ -2264,8 +2413,49 @@ int cr_render_file( const char *json_path, const char *png_path, const char *pfm
 		std::memset( &d, 0, sizeof d );
 		d.width = w, d.height = h, d.spp = spp, d.max_bounce = UINT32_MAX, d.estimator = -1, d.seed = 1;
 		std::vector<double> film( size_t( w ) * h * 3 );
-		int rc = cr_render( s.get(), &d, film.data(), nullptr );
-		if ( rc != CR_OK ) fail( rc, g_last_error );
+		// The Renderer's profiler (renderer.hpp:17-23, kernel.cu): when enabled,
+		// the tracer renders its area only (cpuMulticore.cu:17; the rest of the
+		// image stays black) and the slices go to its output file.
+		const Json doc = parse_json( text );
+		const Json *pj = doc.find( "profiler" );
+		// a "profiler" block is enabled unless it says otherwise (Profiler::Configuration, kernel.hpp:37-43)
+		const bool profile = pj && pj->number_or( "enable", 1 ) != 0;
+		if ( profile )
+		{
+			uint32_t area[ 4 ] = { 0, 0, w, h };
+			if ( const Json *a = pj->find( "area" ) )
+			{
+				if ( !a->is_array() || a->size() != 4 ) fail( CR_ERR_PARSE, "profiler area must be [x0, y0, x1, y1]" );
+				for ( int i = 0; i < 4; ++i )
+				{
+					const double v = a->at( i ).num;
+					area[ i ] = v < 0 ? 0u : uint32_t( std::min<double>( v, i % 2 ? h : w ) );
+				}
+			}
+			uint32_t depth = 8;  // RadianceKernel::Slice's default (radiance.hpp:27-31)
+			if ( const Json *pp = pj->find( "props" ) ) depth = uint32_t( pp->number_or( "depth", 8 ) );
+			const std::string out = pj->string_or( "output", "a.prof" );
+			if ( area[ 2 ] > area[ 0 ] && area[ 3 ] > area[ 1 ] )
+			{
+				cr_render_desc pdsc = d;
+				pdsc.x0 = area[ 0 ], pdsc.y0 = area[ 1 ], pdsc.x1 = area[ 2 ], pdsc.y1 = area[ 3 ];
+				const size_t aw = area[ 2 ] - area[ 0 ], ah = area[ 3 ] - area[ 1 ], n = aw * ah * spp;
+				std::vector<cr_profile_slice> sl( n );
+				std::vector<cr_profile_bounce> bo( n * depth );
+				std::vector<double> win( aw * ah * 3 );
+				int rc = cr_render_profile( s.get(), &pdsc, depth, sl.data(), bo.data(), win.data() );
+				if ( rc != CR_OK ) fail( rc, g_last_error );
+				for ( size_t y = 0; y < ah; ++y )
+					std::memcpy( &film[ 3 * ( ( area[ 1 ] + y ) * size_t( w ) + area[ 0 ] ) ], &win[ 3 * y * aw ], 24 * aw );
+				rc = cr_profile_write( out.c_str(), area, spp, depth, sl.data(), bo.data() );
+				if ( rc != CR_OK ) fail( rc, g_last_error );
+			}
+		}
+		else
+		{
+			int rc = cr_render( s.get(), &d, film.data(), nullptr );
+			if ( rc != CR_OK ) fail( rc, g_last_error );
+		}
 		write_png( png_path, w, h, film.data() );
 		if ( pfm_path && *pfm_path ) write_pfm( pfm_path, w, h, film.data() );
 	} );

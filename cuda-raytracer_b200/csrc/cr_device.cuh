@@ -159,7 +159,6 @@ __device__ __forceinline__ bool sphere_test( float3 centre, float r2, float3 o, 
 	return t >= 0.f && t > tmin && t < tmax;
 }
 
-__device__ __forceinline__ float q8( uint32_t w, int sh ) { return float( ( w >> sh ) & 0xFFu ); }
 
 // ------------------------------------------------------------------ shading helpers
 // Reference frame (src/core/meta/scene.hpp:48-53): u = n x (0,1,0), v = n x u,

@@ -337,9 +337,25 @@ __device__ __forceinline__ void koishi_light_sample( const DevScene &sc, const D
 // light), then the shaders' draws and the Russian roulette draw.  A shader
 // without selection draws (all but Mixed and GlassBSDF) takes a fixed layout:
 // sample3 = draws 3-5, roulette = draw 6.
+// What a profiled vertex adds to its RadianceKernel::Slice record
+// (radiance.cu:41-53): f for the light sample's direction, theta, the shader,
+// and whether Russian roulette ended the path here.
+struct ProfOut
+{
+	float3 f = { 0.f, 0.f, 0.f };
+	float theta = 0.f;
+	uint32_t shader = 0;
+	bool rr_killed = false;
+};
+
+// PROF: a profiled render, whose paths follow the reference's loop exactly:
+// a path whose throughput is zero (or whose radiance is not finite) goes on
+// bouncing, as it does in radiance.cu, so that the Slice's bounce counter and
+// records match.
+template <bool PROF = false>
 __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
 											  uint32_t bounce, float4 ro, float4 rd, const HitRec &h, float4 &beta4,
-											  float4 &L4, PathOut &out )
+											  float4 &L4, PathOut &out, ProfOut *prof = nullptr )
 {
 	float3 o = f3( ro ), d = f3( rd );
 	Surface s = surface_at( sc, o, d, h, false );
@@ -368,6 +384,7 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 		wi = fr.local( normalize( lp - s.p ) );
 		float3 emission;
 		float3 f = simple ? leaf_eval( sh, wo, wi, emission ) : koishi_eval( sc.shaders, s.shader, wo, wi, rng, emission );
+		if constexpr ( PROF ) prof->f = f;
 		float3 c = beta * f * li * ( fabsf( wi.z ) / lpdf );
 		if ( !finite3( c ) )
 			L = f3( NAN, NAN, NAN );
@@ -379,6 +396,12 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 			out.sc = make_float4( c.x, c.y, c.z, 0.f );
 		}
 		L = L + beta * emission;  // radiance.cu:39
+	}
+	if constexpr ( PROF )
+	{
+		// theta = acos(wo . reflect(wi, +z)), reflect(v, n) = 2 n (n.v) - v (vmath.hpp)
+		prof->theta = acosf( dot( wo, f3( -wi.x, -wi.y, wi.z ) ) );
+		prof->shader = uint32_t( s.shader );
 	}
 	float3 emission_s, f;
 	float u_rr;
@@ -402,11 +425,19 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 	{
 		float q = fmaxf( .05f, 1.f - rr );
 		if ( u_rr < q )
+		{
 			alive = false;
+			if constexpr ( PROF ) prof->rr_killed = true;
+		}
 		else
 			beta = beta / ( 1.f - q );
 	}
-	if ( bounce + 1 > cfg.max_bounce || is_zero( beta ) || !finite3( L ) || !finite3( beta ) ) alive = false;
+	if constexpr ( PROF )
+	{
+		if ( bounce + 1 > cfg.max_bounce ) alive = false;
+	}
+	else if ( bounce + 1 > cfg.max_bounce || is_zero( beta ) || !finite3( L ) || !finite3( beta ) )
+		alive = false;
 	if ( !finite3( L ) ) out.shadow = false;
 	beta4 = make_float4( beta.x, beta.y, beta.z, 0.f );
 	L4 = make_float4( L.x, L.y, L.z, 0.f );
@@ -690,7 +721,9 @@ __global__ void k_generate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa )
 // its job's random key, and `sc` and `key` are unused.
 // One instantiation per estimator, so that the reference estimator's shading
 // is not held to the registers of the guided MIS shading.
-template <bool BATCH, int EST>
+// PROF: a profiled render (reference estimator, one scene): each shaded vertex
+// writes its bounce record and each ending path its slice's bounce counter.
+template <bool BATCH, int EST, bool PROF = false>
 __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
 												  uint32_t bounce, uint2 key, BatchDev bd )
 {
@@ -717,6 +750,11 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 				if ( j * cfg.rec_stride == off && j < cfg.rec_paths ) rec_j = j;
 			}
 			const bool recorded = rec_j != 0xFFFFFFFFu;
+			if constexpr ( PROF )
+			{
+				// the loop's intersect failed here: the slice counts `bounce` vertices
+				if ( h.id == HIT_MISS ) cfg.prof.slices[ wa.first + path ].bounce = bounce;
+			}
 			if ( recorded && bounce > 0 && h.id == HIT_MISS )
 			{
 				// the previous vertex's continuation left the scene: no indirect light
@@ -750,6 +788,27 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
 								   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 : nullptr,
 								   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
+					else if constexpr ( PROF )
+					{
+						ProfOut po;
+						shade_koishi<true>( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out, &po );
+						// the window is the profiler's area: a path's sample index in the
+						// window is its slice (Profiler::at, kernel.hpp:62-68)
+						const uint64_t si = wa.first + path;
+						if ( bounce < cfg.prof.depth )
+						{
+							cr_profile_bounce &r = cfg.prof.bounces[ si * cfg.prof.depth + bounce ];
+							r.ray_o[ 0 ] = ro.x, r.ray_o[ 1 ] = ro.y, r.ray_o[ 2 ] = ro.z;
+							r.ray_d[ 0 ] = rd.x, r.ray_d[ 1 ] = rd.y, r.ray_d[ 2 ] = rd.z;
+							r.f[ 0 ] = po.f.x, r.f[ 1 ] = po.f.y, r.f[ 2 ] = po.f.z;
+							r.theta = po.theta;
+							r.L[ 0 ] = L.x, r.L[ 1 ] = L.y, r.L[ 2 ] = L.z;  // the light sample's share follows
+							r.shader = po.shader;
+						}
+						// Russian roulette breaks before ++bounce; otherwise the loop
+						// counts this vertex
+						if ( !out.alive ) cfg.prof.slices[ si ].bounce = po.rr_killed ? bounce : bounce + 1;
+					}
 					else
 						shade_koishi( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out );
 				}
@@ -801,6 +860,35 @@ __global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_infer( DevScene sc, 
 		store_lobes( wb.lobes + size_t( q[ i ] ) * 5, lb );
 	};
 	tc::mlp_forward_tc<48>( cfg.guide, Wp, n, src, sink, wb.err );
+}
+
+// Profiled renders: after the any-hit pass of `bounce`, each shaded vertex's
+// record takes the path's radiance with its light sample's share (the
+// reference adds the occlusion-tested light sample before it records L).
+__global__ void k_profile_fix( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, uint32_t bounce )
+{
+	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
+	const uint32_t *q = wb.queue[ bounce & 1 ];
+	if ( bounce >= cfg.prof.depth ) return;
+	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
+	{
+		const uint32_t path = q[ i ];
+		if ( wb.hit[ path ].id == HIT_MISS ) continue;
+		const float4 l = wb.L[ path ];
+		float *L = cfg.prof.bounces[ ( wa.first + path ) * cfg.prof.depth + bounce ].L;
+		L[ 0 ] = l.x, L[ 1 ] = l.y, L[ 2 ] = l.z;
+	}
+}
+
+// Profiled renders, end of a wave: each slice takes its sample's radiance.
+__global__ void k_profile_final( RenderConfig cfg, WaveBuffers wb, WaveArgs wa )
+{
+	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wa.n; i += gridDim.x * blockDim.x )
+	{
+		const float4 l = wb.L[ i ];
+		float *L = cfg.prof.slices[ wa.first + i ].L;
+		L[ 0 ] = l.x, L[ 1 ] = l.y, L[ 2 ] = l.z;
+	}
 }
 
 __global__ void k_accumulate( RenderConfig cfg, WaveBuffers wb, WaveArgs wa, double *sum, double *sumsq,
@@ -1188,7 +1276,7 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 				io.scenes = bd.scenes, io.path_job = wb.path_job;
 				const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
 				uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
-				k_traverse<BatchExtendIO, false, false><<<g_ext, 128, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err, wb.work,
+				k_traverse<BatchExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err, wb.work,
 																			   cfg.refill_min );
 			} );
 			timed( 2, [&] {
@@ -1203,7 +1291,7 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 				io.scenes = bd.scenes, io.path_job = wb.path_job;
 				const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
 				uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
-				k_traverse<BatchShadowIO, true, false><<<g_ext, 128, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
+				k_traverse<BatchShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
 																			  wb.work + 2, cfg.refill_min );
 			} );
 		}
@@ -1239,6 +1327,9 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 {
 	if ( cfg.guiding && ( !guide || !wb.lobes || cfg.estimator != EST_MIS ) )
 		throw std::runtime_error( "guided render without a guide, lobe buffer or MIS estimator" );
+	const bool profiled = cfg.prof.slices != nullptr;
+	if ( profiled && ( cfg.estimator != EST_KOISHI || cfg.kernel != KERNEL_RADIANCE || cfg.guiding || !cfg.prof.bounces ) )
+		throw std::runtime_error( "a profiled render takes the Radiance kernel with the reference estimator" );
 	const uint64_t total = uint64_t( cfg.ww ) * cfg.wh * cfg.spp;
 	if ( cfg.wave_paths == 0 || cfg.wave_paths > wb.capacity )
 		throw std::runtime_error( "wave size exceeds the allocated wave buffers" );
@@ -1319,9 +1410,9 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
 				uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
 				if ( cfg.count_work )
-					k_traverse<ExtendIO, false, true><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
+					k_traverse<ExtendIO, false, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 				else
-					k_traverse<ExtendIO, false, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
+					k_traverse<ExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 			} );
 			if ( wc.guide_sample && guided_vertex( wc.guide, b, cfg.max_bounce ) )
 				timed( 4, [&] {
@@ -1333,6 +1424,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				timed( 2, [&] {
 					if ( cfg.estimator == EST_MIS )
 						k_shade<false, EST_MIS><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+					else if ( profiled )
+						k_shade<false, EST_KOISHI, true><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
 					else
 						k_shade<false, EST_KOISHI><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
 				} );
@@ -1342,11 +1435,13 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 					const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
 					uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
 					if ( cfg.count_work )
-						k_traverse<ShadowIO, true, true><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
+						k_traverse<ShadowIO, true, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 					else
-						k_traverse<ShadowIO, true, false><<<g_ext, 128, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
+						k_traverse<ShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 				} );
+			if ( profiled ) timed( 3, [&] { k_profile_fix<<<g_shade, 128, 0, st>>>( wc, wb, wa, b ); } );
 		}
+		if ( profiled ) timed( 3, [&] { k_profile_final<<<g_shade, 128, 0, st>>>( wc, wb, wa ); } );
 		if ( steps )
 			timed( 5, [&] {
 				// online training on this wave's recorded vertices, one Adam step per batch
@@ -1414,10 +1509,10 @@ void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hi
 	int g = int( std::min<uint64_t>( ( n + 127 ) / 128, uint64_t( sm_count() ) * 8 ) );
 	QueryIO io{ rays, out, sc.tris, sc.attrs, sc.spheres, sc.prim_first };
 	if ( any_hit )
-		k_traverse<QueryIO, true, false><<<g, 128, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
+		k_traverse<QueryIO, true, false><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
 																 QUERY_REFILL_MIN );
 	else
-		k_traverse<QueryIO, false, false><<<g, 128, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
+		k_traverse<QueryIO, false, false><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
 																  QUERY_REFILL_MIN );
 	check( cudaGetLastError(), "trace launch" );
 }

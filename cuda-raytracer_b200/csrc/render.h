@@ -3,10 +3,9 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "../../include/cr.h"
 #include "cr_common.h"
 #include "guide.h"
-
-struct cr_hit;
 
 namespace cr
 {
@@ -65,6 +64,15 @@ enum : int32_t
 	KERNEL_HALFVECTOR = 3   // HalfVectorKernel (halfVector.hpp:17-43)
 };
 
+// Per-bounce profile of a profiled render (cr_render_profile), device arrays:
+// one slice per sample of the window, `depth` bounce records per sample.
+struct ProfileDev
+{
+	cr_profile_slice *slices = nullptr;
+	cr_profile_bounce *bounces = nullptr;
+	uint32_t depth = 0;
+};
+
 struct RenderConfig
 {
 	uint32_t spp, max_bounce;
@@ -84,6 +92,7 @@ struct RenderConfig
 	uint32_t rec_paths = 0, rec_stride = 1, rec_offset = 0;
 	uint32_t refill_min = 16;        // traversal: idle lanes per warp that trigger a refill (1..32)
 	int traverse_blocks_per_sm = 8;  // traversal grid = SMs x this (1..8; 128-thread blocks)
+	ProfileDev prof{};               // profiled renders (reference estimator, Radiance kernel)
 };
 
 struct StageTimes

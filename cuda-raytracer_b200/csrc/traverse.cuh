@@ -16,8 +16,23 @@ namespace cr
 {
 constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
 
+// A quantised plane byte q as the float 32768 + q, exactly: the byte goes to
+// bits 8..15 of a float whose exponent makes bit 8 worth 1 (0x47000000 is
+// 2^15).  One byte permute, no integer-to-float conversion.
+__device__ __forceinline__ float q8_biased( uint32_t w, uint32_t i )
+{
+	return __uint_as_float( __byte_perm( w, 0x47000000u, 0x7404u | ( i << 4 ) ) );
+}
+constexpr float Q8_BIAS = 32768.f;
+
 // Intersects the ray with the 8 children of `node`; returns the node-group
 // hits (bits at slot ^ octant) and the triangle-group hits (24-bit mask).
+//
+// Child plane k of an axis lies at p + 2^e q_k, so its ray distance is
+// (p - o) / d + q_k 2^e / d = fma(32768 + q_k, S, B) with S = 2^e / d (exact:
+// a power of two times 1/d) and B = (p - o) / d - 32768 S (one rounding).
+// The extra rounding of B is 2^-9 of one quantisation step S, below the
+// rounding of (p - o) / d for any node further away than a few node widths.
 __device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r, uint32_t node, float tmin,
 											float tlim, uint2 &ng, uint2 &tg )
 {
@@ -28,6 +43,7 @@ __device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r,
 	float3 adj_s = f3( __uint_as_float( ex << 23 ) * r.invd.x, __uint_as_float( ey << 23 ) * r.invd.y,
 					   __uint_as_float( ez << 23 ) * r.invd.z );
 	float3 adj_o = ( p - r.o ) * r.invd;
+	adj_o = f3( fmaf( -Q8_BIAS, adj_s.x, adj_o.x ), fmaf( -Q8_BIAS, adj_s.y, adj_o.y ), fmaf( -Q8_BIAS, adj_s.z, adj_o.z ) );
 	uint32_t nx0 = n2.x, nx1 = n2.y, fx0 = n3.z, fx1 = n3.w;
 	uint32_t ny0 = n2.z, ny1 = n2.w, fy0 = n4.x, fy1 = n4.y;
 	uint32_t nz0 = n3.x, nz1 = n3.y, fz0 = n4.z, fz1 = n4.w;
@@ -39,11 +55,12 @@ __device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r,
 	for ( int i = 0; i < 8; ++i )
 	{
 		const int sh = 8 * ( i & 3 );
+		const uint32_t bi = uint32_t( i & 3 );
 		uint32_t wnx = i < 4 ? nx0 : nx1, wny = i < 4 ? ny0 : ny1, wnz = i < 4 ? nz0 : nz1;
 		uint32_t wfx = i < 4 ? fx0 : fx1, wfy = i < 4 ? fy0 : fy1, wfz = i < 4 ? fz0 : fz1;
-		float tnx = fmaf( q8( wnx, sh ), adj_s.x, adj_o.x ), tfx = fmaf( q8( wfx, sh ), adj_s.x, adj_o.x );
-		float tny = fmaf( q8( wny, sh ), adj_s.y, adj_o.y ), tfy = fmaf( q8( wfy, sh ), adj_s.y, adj_o.y );
-		float tnz = fmaf( q8( wnz, sh ), adj_s.z, adj_o.z ), tfz = fmaf( q8( wfz, sh ), adj_s.z, adj_o.z );
+		float tnx = fmaf( q8_biased( wnx, bi ), adj_s.x, adj_o.x ), tfx = fmaf( q8_biased( wfx, bi ), adj_s.x, adj_o.x );
+		float tny = fmaf( q8_biased( wny, bi ), adj_s.y, adj_o.y ), tfy = fmaf( q8_biased( wfy, bi ), adj_s.y, adj_o.y );
+		float tnz = fmaf( q8_biased( wnz, bi ), adj_s.z, adj_o.z ), tfz = fmaf( q8_biased( wfz, bi ), adj_s.z, adj_o.z );
 		float tn = fmaxf( fmaxf( tnx, tny ), fmaxf( tnz, tmin ) );
 		float tf = fminf( fminf( tfx, tfy ), fminf( tfz, tlim ) );
 		uint32_t meta = ( ( i < 4 ? n1.z : n1.w ) >> sh ) & 0xFFu;
@@ -66,8 +83,11 @@ __device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r,
 //   finish(item, hit, found): store the result
 //   MULTI: the queue mixes the rays of several scenes (a batched render);
 //          scene(item) is the ray's scene, otherwise every ray uses `sc`
+constexpr int TRAVERSE_THREADS = 128;  // threads per block of k_traverse (every launch uses this)
+constexpr int SHARED_STACK = 8;        // stack entries per thread kept in shared memory
+
 template <class IO, bool ANY, bool COUNT>
-__global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, const uint32_t *n_ptr, uint32_t n_host,
+__global__ void __launch_bounds__( TRAVERSE_THREADS, 8 ) k_traverse( DevScene sc, IO io, const uint32_t *n_ptr, uint32_t n_host,
 														uint32_t *cursor, uint32_t *err, unsigned long long *work,
 														uint32_t refill_min )
 {
@@ -83,8 +103,14 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 	HitRec hit;
 	bool found = false;
 	uint2 ng = make_uint2( 0u, 0u ), tg = make_uint2( 0u, 0u );
+	// Traversal stack of (node base, hit mask) groups: the first SHARED_STACK
+	// entries in shared memory (entry k of thread t at [k][t]: a warp's 32
+	// entries are 256 contiguous bytes, no bank conflicts), deeper ones in
+	// local memory, which shallow 8-wide trees rarely reach.
+	__shared__ uint2 sstack[ SHARED_STACK ][ TRAVERSE_THREADS ];
+	uint2 *const my_stack = &sstack[ 0 ][ threadIdx.x ];
 	int sp = 0;
-	uint2 stack[ TRAVERSAL_STACK ];
+	uint2 stack[ TRAVERSAL_STACK - SHARED_STACK ];
 	// this lane's geometry: the kernel's scene, or the current ray's in a batch
 	const WNode *nodes = sc.nodes;
 	const float4 *tris = sc.tris;
@@ -195,8 +221,10 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 				{
 					if ( ng.y > 0x00FFFFFFu )
 					{
-						if ( sp < TRAVERSAL_STACK )
-							stack[ sp++ ] = ng;
+						if ( sp < SHARED_STACK )
+							my_stack[ TRAVERSE_THREADS * sp++ ] = ng;
+						else if ( sp < TRAVERSAL_STACK )
+							stack[ sp++ - SHARED_STACK ] = ng;
 						else
 							atomicOr( err, 1u );
 					}
@@ -205,7 +233,10 @@ __global__ void __launch_bounds__( 128, 8 ) k_traverse( DevScene sc, IO io, cons
 				}
 			}
 			else if ( sp > 0 )
-				ng = stack[ --sp ];
+			{
+				--sp;
+				ng = sp < SHARED_STACK ? my_stack[ TRAVERSE_THREADS * sp ] : stack[ sp - SHARED_STACK ];
+			}
 			else
 				done = true;
 		}

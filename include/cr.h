@@ -229,6 +229,14 @@ int cr_light_table(const cr_scene *s, uint32_t light, float *out, float *pdf);
  * rays: n x {o.x,o.y,o.z, d.x,d.y,d.z, tmax} floats (tmax <= 0 or inf: none).
  * Host buffers; copies are part of the call. */
 int cr_trace_rays(cr_scene *s, const float *rays, uint64_t n, cr_hit *hits, int any_hit);
+/* Mesh::samples and Mesh::pdf (src/core/primitive/mesh.hpp:58-84) handed over
+ * from a reference Scene: replaces the 1024-point light table (points
+ * 1024 x {p.xyz, n.xyz}) and the area pdf that the reference estimator's
+ * AreaLight::sample (src/core/light/areaLight.hpp:19-31) draws from, for the
+ * emissive mesh `primitive` (the id cr_scene_add_mesh returned) of a
+ * committed scene.  The Tracer plugin uses it so that the GPU samples the very
+ * light points the reference's CPU tracer would. */
+int cr_scene_set_light_table(cr_scene *s, uint32_t primitive, const float *points, float pdf);
 
 /* Same on device buffers, asynchronous on `stream`. */
 int cr_trace_rays_device(cr_scene *s, const float *d_rays, uint64_t n, cr_hit *d_hits, int any_hit,
@@ -271,6 +279,44 @@ int cr_render_device(cr_scene *s, const cr_render_desc *desc, double *d_sum, dou
 #define CR_NOALLOC_MAX_BOUNCE 64u
 int cr_render_device_noalloc(cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sumsq,
                              uint32_t *d_count, void *stream);
+
+/* ----------------------------------------------------- per-bounce profile */
+/* RadianceKernel::Slice (src/core/kernel/radiance.hpp:17-55) as the
+ * reference's Profiler keeps it (src/core/kernel/kernel.hpp:35-81): one slice
+ * per sample of the profiled pixel area, holding the sample's radiance, the
+ * loop's bounce counter at exit, and for its first `depth` vertices one
+ * BounceRecord each (radiance.cu:41-53): the ray that reached the vertex, the
+ * shader's f for the light sample's direction, theta = the angle between wo
+ * and that direction mirrored about the normal, the radiance gathered up to
+ * and including the vertex, and the vertex's shader id. */
+typedef struct cr_profile_bounce {
+    float ray_o[3], ray_d[3];
+    float f[3];
+    float theta;
+    float L[3];
+    uint32_t shader;
+} cr_profile_bounce;
+typedef struct cr_profile_slice {
+    uint32_t bounce;
+    float L[3];
+} cr_profile_slice;
+/* Profiled render with the reference estimator (CPUMulticoreTracer::execute
+ * with an enabled Profiler, src/core/tracer/cpuMulticore.cu:17,53-64):
+ * renders the pixel window of `desc` (the profiler's area) and records its
+ * slices, host arrays in the Profiler's order (row, column, sample):
+ * slices ww x wh x spp, bounces ww x wh x spp x depth (depth <= 64).
+ * film_rgb (window-sized, may be NULL) receives the per-pixel means.  For
+ * the records to follow the reference's loop exactly, a profiled path is not
+ * cut short when its throughput reaches zero. */
+int cr_render_profile(cr_scene *s, const cr_render_desc *desc, uint32_t depth, cr_profile_slice *slices,
+                      cr_profile_bounce *bounces, double *film_rgb);
+/* Profiler::~Profiler (kernel.cu): writes the slices of the area
+ * (x0, y0)-(x1, y1) of a profiled render at `spp` samples to `path` in the
+ * reference's text format (an "at [ x, y, k ]: " line per sample; a slice's
+ * records only when its radiance is at least 100 in every channel, as
+ * RadianceKernel::Slice::writeSlice prints them). */
+int cr_profile_write(const char *path, const uint32_t area[4], uint32_t spp, uint32_t depth,
+                     const cr_profile_slice *slices, const cr_profile_bounce *bounces);
 
 /* No counterpart in the reference (its tracer has no launch parameters).
  * Picks the wave size, the traversal refill threshold and the traversal grid

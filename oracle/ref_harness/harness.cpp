@@ -24,6 +24,16 @@
 //       the 1024-point tables of every emissive mesh (src/core/primitive/mesh.hpp:61-84).
 //   bench  <scene.json> <W> <H> <spp> <threads> [maxBounce] [repeats]
 //       wall time of the reference's own CPUMulticoreTracer::execute, once per repeat.
+//   plugin <scene.json> <W> <H> <spp> <out.u8> [seed]      (cr_ref_plugin only)
+//       the CudaWavefront Tracer plugin (cuda-raytracer_b200/plugin/cudaWavefront.hpp)
+//       registered in Factory<Tracer> as src/core/tracer/tracer.impl.cu:8-11
+//       registers the CPU tracer, created by name and run through
+//       Tracer::execute (src/core/tracer/tracer.hpp:20-21) as the Renderer
+//       does; out: the 8-bit W x H x 3 image it wrote.
+//   profile <scene.json> <W> <H> <spp> <x0> <y0> <x1> <y1> <depth> <out.prof> [threads]
+//       CPUMulticoreTracer::execute with an enabled Profiler over the area
+//       (src/core/kernel/kernel.hpp:35-81, src/core/tracer/cpuMulticore.cu:17):
+//       the reference's own per-bounce dump, written by Profiler::~Profiler.
 //   shade  <shader.json> <records.f32> <k> <out.f32>
 //       Shader::execute (src/core/nodes/shader.hpp:17-23) of the [Type, {props}]
 //       shader in shader.json, built by Factory<Shader>::create, for records
@@ -58,8 +68,17 @@
 #include <ext/shader/emission.hpp>
 #include <util/image.hpp>
 
+#ifdef CR_HARNESS_PLUGIN
+#include <cudaWavefront.hpp>
+#endif
+
 using namespace koishi;
 using namespace koishi::core;
+
+#ifdef CR_HARNESS_PLUGIN
+// The registration line a maintainer adds to src/core/tracer/tracer.impl.cu.
+static volatile int cr_plugin_registry[] = { Factory<Tracer>::reg<CudaWavefrontTracer>( "CudaWavefront" ) };
+#endif
 
 namespace
 {
@@ -483,6 +502,78 @@ int cmd_bench( int argc, char **argv )
 
 }  // namespace
 
+int cmd_profile( int argc, char **argv )
+{
+	if ( argc < 12 ) return 1;
+	std::string path = argv[ 2 ];
+	uint32_t W = std::stoul( argv[ 3 ] ), H = std::stoul( argv[ 4 ] ), spp = std::stoul( argv[ 5 ] );
+	uint32_t area[ 4 ] = { uint32_t( std::stoul( argv[ 6 ] ) ), uint32_t( std::stoul( argv[ 7 ] ) ),
+						   uint32_t( std::stoul( argv[ 8 ] ) ), uint32_t( std::stoul( argv[ 9 ] ) ) };
+	uint32_t depth = std::stoul( argv[ 10 ] );
+	std::string out = argv[ 11 ];
+	uint32_t nth = argc > 12 ? std::stoul( argv[ 12 ] ) : std::max( 1u, std::thread::hardware_concurrency() - 1 );
+	Loaded L;
+	load( path, L, 0x330E );
+	Properties tp;
+	tp[ "maxThreads" ] = nth;
+	Properties kp;
+	kp[ "maxBounce" ] = L.max_bounce;
+	tp[ "kernel" ] = json::array( { "Radiance", kp } );
+	auto tracer = Factory<Tracer>::create( Config( "CPUMulticore", tp ) );
+	util::Image<3> image( W, H );
+	poly::object<Lens> lens;
+	if ( L.scene->camera[ 0 ].lens == 1 )
+		lens = poly::make_object<OrthographicLens>( L.scene->camera[ 0 ], W, H, spp );
+	else
+		lens = poly::make_object<PinholeLens>( L.scene->camera[ 0 ], W, H, spp );
+	SamplerGenerator gen;
+	Properties pp;
+	pp[ "enable" ] = true;
+	pp[ "output" ] = out;
+	pp[ "area" ] = json::array( { area[ 0 ], area[ 1 ], area[ 2 ], area[ 3 ] } );
+	Properties sp;
+	sp[ "depth" ] = depth;
+	pp[ "props" ] = sp;
+	{
+		Profiler profiler( pp, tracer->getKernel(), W, H, spp );
+		tracer->execute( image, lens, gen, *L.scene, spp, profiler );
+	}  // ~Profiler writes `out`
+	return 0;
+}
+
+#ifdef CR_HARNESS_PLUGIN
+int cmd_plugin( int argc, char **argv )
+{
+	if ( argc < 7 ) return 1;
+	std::string path = argv[ 2 ];
+	uint32_t W = std::stoul( argv[ 3 ] ), H = std::stoul( argv[ 4 ] ), spp = std::stoul( argv[ 5 ] );
+	std::string out = argv[ 6 ];
+	uint32_t seed = argc > 7 ? std::stoul( argv[ 7 ] ) : 1u;
+	Loaded L;
+	load( path, L, 0x330E );
+	Properties tp;
+	Properties kp;
+	kp[ "maxBounce" ] = L.max_bounce;
+	tp[ "kernel" ] = json::array( { "Radiance", kp } );
+	tp[ "seed" ] = seed;
+	auto tracer = Factory<Tracer>::create( Config( "CudaWavefront", tp ) );
+	util::Image<3> image( W, H );
+	poly::object<Lens> lens;
+	if ( L.scene->camera[ 0 ].lens == 1 )
+		lens = poly::make_object<OrthographicLens>( L.scene->camera[ 0 ], W, H, spp );
+	else
+		lens = poly::make_object<PinholeLens>( L.scene->camera[ 0 ], W, H, spp );
+	SamplerGenerator gen;
+	Properties pp;
+	pp[ "enable" ] = false;
+	Profiler profiler( pp, tracer->getKernel(), W, H, spp );
+	tracer->execute( image, lens, gen, *L.scene, spp, profiler );
+	std::ofstream f( out, std::ios::binary );
+	f.write( (const char *)image.data(), std::streamsize( size_t( W ) * H * 3 ) );
+	return f ? 0 : 2;
+}
+#endif
+
 int cmd_shade( int argc, char **argv )
 {
 	if ( argc < 6 ) return 1;
@@ -538,6 +629,10 @@ int main( int argc, char **argv )
 		else if ( cmd == "lights" ) rc = cmd_lights( argc, argv );
 		else if ( cmd == "bench" ) rc = cmd_bench( argc, argv );
 		else if ( cmd == "shade" ) rc = cmd_shade( argc, argv );
+		else if ( cmd == "profile" ) rc = cmd_profile( argc, argv );
+#ifdef CR_HARNESS_PLUGIN
+		else if ( cmd == "plugin" ) rc = cmd_plugin( argc, argv );
+#endif
 	}
 	catch ( const std::exception &e )
 	{

@@ -181,10 +181,21 @@ def test_scene_schema_errors_before_any_gpu_work(cr):
     assert rc == -1 and "not found" in msg
 
 
-@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference sources not built here")
-def test_integration_plugin_compiles_against_the_reference():
-    """The Tracer plugin the integration guide shows a maintainer adding
-    compiles against the reference's own headers (make -C oracle plugin-check)."""
+def _reference_sources():
+    d = os.environ.get("CR_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
+    return d if os.path.isdir(os.path.join(d, "src")) else None
+
+
+@pytest.mark.skipif(_reference_sources() is None, reason="reference sources absent")
+def test_tracer_plugin_builds_into_the_reference():
+    """The CudaWavefront Tracer plugin (cuda-raytracer_b200/plugin/) compiles
+    against the unmodified reference, registers in Factory<Tracer> and links
+    the library (make -C oracle plugin); the GPU test runs it."""
     import subprocess
-    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "plugin-check"], capture_output=True, text=True)
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "plugin", f"REF={_reference_sources()}"],
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
+    exe = os.path.join(ROOT, "oracle", "_ref", "cr_ref_plugin")
+    assert os.path.exists(exe)
+    r = subprocess.run(["ldd", exe], capture_output=True, text=True)
+    assert "libcr_b200.so" in r.stdout and "not found" not in r.stdout, r.stdout
