@@ -156,9 +156,9 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per k_extend launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "k_extend_traffic.json")
+def profiled_traffic(name="k_extend_traffic.json"):
+    """DRAM bytes per k_extend ray from a committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as fh:
             return json.load(fh)
@@ -499,16 +499,21 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
                         if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
 
 
-def run_config4(args):
+C4_WINDOW = (1760, 990, 2080, 1170)  # the central 320x180 pixels of the 3840x2160 frame
+
+
+def config4_section(cr, dev, steps, warmup, with_reference, ttt_seconds=40.0):
     """The large combined run: 21M triangles (16 instances of 4 displaced
-    1.31M-triangle meshes, flattened into one BVH), 6 lights, 3840x2160, depth
-    12, MIS, learned guiding on; a step is 16 spp of the full image (1024 spp
-    would take a minute per step).  Prints one JSON line: guided Msamples/s as
-    the value, the plain MIS tracer beside it, and the closest-hit roofline."""
+    1.31M-triangle meshes under random rigid transforms, flattened into one
+    BVH), 6 lights, 3840x2160, depth 12, MIS.  A step is 16 spp of the full
+    image (1024 spp would take a minute per step).  Plain and guided
+    Msamples/s (CUDA events, L2 flushed between steps), the closest-hit
+    roofline against HBM (the 1.3 GB BVH and triangles exceed L2), time to
+    relMSE 1e-3 on the central 320x180 window (a converged reference of the
+    whole 4K frame would take hours), and the reference's CPU tracer on that
+    window through its profiler area."""
     import torch
-    cr = load_pkg()
     from cuda_raytracer_b200 import scenes
-    dev = torch.device("cuda", 0)
     W4, H4, SPP4, MB4 = 3840, 2160, 16, 11
     t0 = time.perf_counter()
     desc = scenes.config4()
@@ -525,15 +530,15 @@ def run_config4(args):
                           stream=stream.cuda_stream).as_dict()
 
     def run(guiding, label):
-        for w in range(args.warmup):
+        for w in range(warmup):
             d = cr.render_desc(W4, H4, SPP4, max_bounce=MB4, estimator=cr.MIS, seed=500 + w, guiding=guiding)
             scene.render_device(d, s.data_ptr(), q.data_ptr(), c.data_ptr(), stream=stream.cuda_stream, stats=False)
         torch.cuda.synchronize(dev)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         tot = {"extend": 0.0, "launches": 0, "ext_launches": 0, "samples": 0, "guide": 0.0, "rays": 0}
-        clocks = ClockSampler(0)
+        clocks = ClockSampler(dev.index or 0)
         clocks.start()
-        for k in range(args.steps):
+        for k in range(steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
             d = cr.render_desc(W4, H4, SPP4, max_bounce=MB4, estimator=cr.MIS, seed=900 + k, guiding=guiding)
@@ -549,9 +554,9 @@ def run_config4(args):
         clk = clocks.stop()
         ms = sum(a.elapsed_time(b) for a, b in ev)
         return {"label": label, "msamples_per_s": round(tot["samples"] / ms / 1e3, 3),
-                "mrays_per_s": round(tot["rays"] / ms / 1e3, 2), "ms_per_step": round(ms / args.steps, 2),
-                "ms_guide_per_step": round(tot["guide"] / args.steps, 2), "launches": tot["launches"],
-                "extend_ms_per_launch": tot["extend"] / max(tot["ext_launches"], 1), "clocks": clk}
+                "mrays_per_s": round(tot["rays"] / ms / 1e3, 2), "ms_per_step": round(ms / steps, 2),
+                "ms_guide_per_step": round(tot["guide"] / steps, 2), "launches": tot["launches"],
+                "extend_ms_per_launch": round(tot["extend"] / max(tot["ext_launches"], 1), 4), "clocks": clk}
 
     plain = run(False, "plain MIS")
     cr.Guide(scene).reset(seed=7)
@@ -563,31 +568,66 @@ def run_config4(args):
     ext_launch_bytes = ext_bytes / max(cst.extend_launches, 1)
     achieved = ext_launch_bytes / (plain["extend_ms_per_launch"] / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    # time to relMSE 1e-3 on the central 320x180 window of the frame against a
-    # 32768-spp reference of it (the runs need over 10^4 spp there, so the
-    # reference has at least twice their samples); a converged reference of
-    # the whole 4K frame would take hours
-    ttt = window_time_to_target(cr, scene, W4, H4, (1760, 990, 2080, 1170), MB4, 32768, 40.0, dev)
+    traffic = profiled_traffic("k_extend_traffic_config4.json")
+    del s, q, c, flush
+    torch.cuda.empty_cache()
+    ttt = window_time_to_target(cr, scene, W4, H4, C4_WINDOW, MB4, 32768, ttt_seconds, dev)
+    out = {"workload": "config4: 16 instances of 4 displaced icospheres (level 8) under random rigid transforms in "
+                       "one BVH, 6 lights, 3840x2160, depth 12, MIS estimator, 16 spp per step",
+           "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"], "scene_build_s": round(build_s, 1),
+           "autotuned": tune, "plain": plain, "guided": guided,
+           "roofline": {"bound": "hbm", "kernel": "k_extend (plain MIS steps)", "achieved": round(achieved, 1),
+                        "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                        "traffic": (round(traffic["dram_bytes_per_ray"] * cst.rays_extend / max(cst.extend_launches, 1))
+                                    if traffic else None),
+                        "traffic_note": ("ncu DRAM bytes per ray of one captured launch "
+                                         "(profiles/k_extend_traffic_config4.json) scaled to this run's rays per launch")
+                                        if traffic else None,
+                        "algorithmic_bytes_per_launch": round(ext_launch_bytes),
+                        "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
+                        "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3)},
+           "time_to_relmse": ttt,
+           "note": "time to relMSE 1e-3 measured on the central 320x180 window against a 32768-spp plain reference "
+                   "of that window (a converged reference of the full 4K frame would take hours)"}
+    if with_reference:
+        import oracle
+        if oracle.ref_available():
+            with tempfile.TemporaryDirectory() as tmp:
+                path = scenes.write_scene(desc, tmp)
+                threads = os.cpu_count() or 1
+                x0, y0, x1, y1 = C4_WINDOW
+                t1 = time.perf_counter()
+                r = subprocess.run([oracle.REF_BIN, "bench", os.path.basename(path), str(W4), str(H4), "4",
+                                    str(threads), str(MB4), "1", str(x0), str(y0), str(x1), str(y1)],
+                                   cwd=tmp, capture_output=True, text=True, timeout=1800, check=True)
+                wall = time.perf_counter() - t1
+            run_ = [json.loads(l) for l in r.stderr.splitlines() if l.startswith("{")][-1]
+            out["cpu_baseline"] = {"value": round(run_["samples"] / run_["seconds"] / 1e6, 4), "unit": "Msamples/s",
+                                   "cores": max(1, min(threads, threads - 1)), "kind": "reference",
+                                   "sample": f"the central {x1 - x0}x{y1 - y0} window at 4 spp through the "
+                                             "reference's profiler area (reference estimator, same scene and depth; "
+                                             f"scene load and BVH build excluded, {wall:.0f} s wall in all)"}
+    scene.close()
+    return out
+
+
+def run_config4(args):
+    """--workload config4: the large combined run alone, as one JSON line with
+    guided Msamples/s as its value."""
+    import torch
+    cr = load_pkg()
+    dev = torch.device("cuda", 0)
+    c4 = config4_section(cr, dev, args.steps, args.warmup, not args.no_cpu_baseline)
+    g = c4["guided"]
     line = {
         "metric": "Msamples/s, guided MIS, 3840x2160 at 16 spp per step, 21M-triangle instanced scene, depth 12",
-        "value": guided["msamples_per_s"], "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": guided["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "value": g["msamples_per_s"], "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": g["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, no dataset)",
-        "config": {"workload": "config4: 16 instances of 4 displaced icospheres (level 8) under random rigid "
-                               "transforms in one BVH, 6 lights, 3840x2160, depth 12",
-                   "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"], "spp_per_step": SPP4,
-                   "l2": "flushed between timed steps (256 MB write)", "autotuned": tune,
-                   "scene_build_s": round(build_s, 1)},
-        "plain": plain, "guided": guided,
-        "roofline": {"bound": "hbm", "kernel": "k_extend (plain MIS steps)", "achieved": round(achieved, 1),
-                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "traffic": None, "algorithmic_bytes_per_launch": round(ext_launch_bytes),
-                     "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
-                     "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3)},
-        "clocks": guided["clocks"], "gpu_launches": guided["launches"], "e2e": None, "cpu_baseline": None,
-        "time_to_relmse": ttt,
-        "note": "time to relMSE 1e-3 measured on the central 320x180 window against a 32768-spp plain reference "
-                "of that window (a converged reference of the full 4K frame would take hours)",
+        "config": {"workload": c4["workload"], "triangles": c4["triangles"], "bvh_nodes": c4["bvh_nodes"],
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "roofline": c4["roofline"], "clocks": g["clocks"], "gpu_launches": g["launches"], "e2e": None,
+        "cpu_baseline": c4.get("cpu_baseline"), "config4": c4,
     }
     print(json.dumps(line), flush=True)
 
@@ -645,6 +685,7 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     clocks.start()
     totals = {"extend": 0.0, "shadow": 0.0, "shade": 0.0, "other": 0.0, "launches": 0, "ext_launches": 0,
+              "shadow_launches": 0,
               "rays_extend": 0, "rays_shadow": 0, "samples": 0}
     for k in range(args.steps):
         flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
@@ -657,6 +698,7 @@ def run_ours(args):
         totals["other"] += st.ms_other
         totals["launches"] += st.launches
         totals["ext_launches"] += st.extend_launches
+        totals["shadow_launches"] += st.shadow_launches
         totals["rays_extend"] += st.rays_extend
         totals["rays_shadow"] += st.rays_shadow
         totals["samples"] += st.samples
@@ -678,6 +720,8 @@ def run_ours(args):
     # the working set of this workload's traversal fits in L2
     l2_gbs, fp32_tflops = cr.measure_peaks(stream.cuda_stream)
     ext_flops = (cst.nodes * 96 + cst.tris * 40) / max(cst.extend_launches, 1)  # 8 slab tests x 12 + 40 per triangle
+    # any-hit launches: nodes x 80 B + triangles x 48 B + rays x 48 B (ray in, contribution)
+    sh_bytes = (cst.shadow_nodes * NODE_BYTES + cst.shadow_tris * TRI_BYTES + cst.rays_shadow * 48) / max(cst.shadow_launches, 1)
 
     # end to end through the public API from host arrays
     e2e = None
@@ -724,6 +768,10 @@ def run_ours(args):
     batch = None
     if rank == 0 and world == 1 and args.batch_scenes > 0:
         batch = batched_workload(cr, dev, args.batch_scenes)
+    c4 = None
+    if rank == 0 and world == 1 and not args.no_config4:
+        torch.cuda.empty_cache()
+        c4 = config4_section(cr, dev, 2, 3, not args.no_cpu_baseline)
 
     if rank == 0:
         line = {
@@ -747,6 +795,12 @@ def run_ours(args):
                          "launch_ms": round(ext_launch_ms, 4),
                          "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
                          "tris_per_ray": round(cst.tris / max(cst.rays_extend, 1), 3),
+                         "shadow": {"kernel": "k_shadow (any hit)",
+                                    "rays_per_launch": round(cst.rays_shadow / max(cst.shadow_launches, 1)),
+                                    "nodes_per_ray": round(cst.shadow_nodes / max(cst.rays_shadow, 1), 3),
+                                    "tris_per_ray": round(cst.shadow_tris / max(cst.rays_shadow, 1), 3),
+                                    "launch_ms": round(totals["shadow"] / max(totals["shadow_launches"], 1), 4),
+                                    "achieved_gbs": round(sh_bytes / max(totals["shadow"] / max(totals["shadow_launches"], 1), 1e-9) / 1e6, 1)},
                          "l2": {"achieved": round(achieved, 1), "peak": round(l2_gbs, 1), "unit": "GB/s",
                                 "frac": round(achieved / l2_gbs, 4),
                                 "peak_source": "measured in this run (cr_measure_peaks: 32 MB L2-resident reads)"},
@@ -762,6 +816,7 @@ def run_ours(args):
             "config0": c0,
             "guiding": guiding,
             "batch": batch,
+            "config4": c4,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -781,6 +836,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-config0", action="store_true", help="skip the small box scene's section")
+    ap.add_argument("--no-config4", action="store_true", help="skip the large combined run's section")
     ap.add_argument("--guide-seconds", type=float, default=25.0,
                     help="device-time cap of each guided/plain time-to-relMSE run (0: skip them)")
     ap.add_argument("--guide-ref-spp", type=int, default=4096)

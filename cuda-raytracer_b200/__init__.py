@@ -79,7 +79,7 @@ class GuideConfig(C.Structure):
     """cr_guide_config: the guide's training schedule."""
     _fields_ = [("lr", C.c_float), ("select_prob", C.c_float), ("train_paths", C.c_uint32),
                 ("steps_per_wave", C.c_uint32), ("warmup_steps", C.c_uint32), ("product_target", C.c_uint32),
-                ("max_steps", C.c_uint32), ("guided_bounces", C.c_uint32)]
+                ("max_steps", C.c_uint32), ("guided_bounces", C.c_uint32), ("learn_select", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -366,9 +366,13 @@ class Guide:
 
     def gradients(self, records, tensor_cores=False):
         """Gradients (grid, W, b) of the weighted mixture NLL over records
-        n x {x, wo, n, w, weight}: FP32 pass, or the BF16 tensor-core pass the
+        n x {x, wo, n, w, weight} (and the BSDF density of w when the guide
+        learns its selection): FP32 pass, or the BF16 tensor-core pass the
         renderer trains with."""
         records = np.ascontiguousarray(records, np.float32)
+        width = 14 if self.configure()["learn_select"] else 13
+        if records.ndim != 2 or records.shape[1] != width:
+            raise ValueError(f"records must be n x {width}")
         s = self.info()["sizes"]
         ggrid, gW, gb = (np.zeros(int(n), np.float32) for n in s)
         fn = lib().cr_guide_gradients_tc if tensor_cores else lib().cr_guide_gradients

@@ -1268,6 +1268,17 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	return r;
 }
 
+// Whether the wave state of `paths` paths (WaveBuffers: about 140 bytes per
+// path plus the queue counters) fits in half of the device's free memory.
+bool wave_fits( uint64_t paths, uint32_t max_bounce )
+{
+	size_t free_b = 0, total_b = 0;
+	if ( cudaMemGetInfo( &free_b, &total_b ) != cudaSuccess ) return false;
+	const uint64_t need = paths * ( 6 * sizeof( float4 ) + 3 * sizeof( float4 ) + sizeof( HitRec ) + 4 * sizeof( uint32_t ) ) +
+						  uint64_t( n_counters_for( max_bounce ) ) * 4;
+	return need * 2 <= free_b;
+}
+
 void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t st, bool lobes = false )
 {
 	if ( !( s->wave.capacity >= cap && s->wave_bounces >= max_bounce ) )
@@ -1869,6 +1880,13 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 			double v = rate( w, refill, blocks );
 			if ( v > best ) best = v, wave = w;
 		}
+		// HBM-sized waves (about 140 bytes of state per path): keep doubling
+		// while the sample holds that many paths, memory allows, and it pays
+		for ( uint32_t w = 1u << 24; w <= ( 1u << 26 ) && wave == w / 2 && w <= samples && wave_fits( w, cfg.max_bounce ); w *= 2 )
+		{
+			double v = rate( w, refill, blocks );
+			if ( v > best ) best = v, wave = w;
+		}
 		cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
 		cuda_check( cudaStreamSynchronize( st ), "autotune" );
 		s->tune_wave = wave, s->tune_refill = refill, s->tune_blocks = blocks;
@@ -2143,6 +2161,13 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 			double v = rate( w, refill, blocks );
 			if ( v > best ) best = v, wave = w;
 		}
+		// HBM-sized waves: fewer waves, so fewer launches per render (and graph
+		// nodes per replay); keep doubling while it pays and memory allows
+		for ( uint32_t w = 1u << 24; w <= ( 1u << 26 ) && wave == w / 2 && w <= total && wave_fits( w, b->max_bounce ); w *= 2 )
+		{
+			double v = rate( w, refill, blocks );
+			if ( v > best ) best = v, wave = w;
+		}
 		for ( void *p : { (void *)sum, (void *)sq, (void *)cnt, (void *)d_scenes, (void *)d_jobs } ) cudaFreeAsync( p, st );
 		cuda_check( cudaStreamSynchronize( st ), "batch autotune" );
 		batch_check_error( b );
@@ -2260,6 +2285,7 @@ int cr_guide_configure( cr_scene *s, const cr_guide_config *in, cr_guide_config 
 			g.product_target = in->product_target != 0;
 			g.max_steps = in->max_steps;
 			g.guided_bounces = in->guided_bounces;
+			g.learn_select = in->learn_select != 0;
 		}
 		if ( out )
 		{
@@ -2268,6 +2294,7 @@ int cr_guide_configure( cr_scene *s, const cr_guide_config *in, cr_guide_config 
 			out->product_target = g.product_target ? 1u : 0u;
 			out->max_steps = g.max_steps;
 			out->guided_bounces = g.guided_bounces;
+			out->learn_select = g.learn_select ? 1u : 0u;
 		}
 	} );
 }
@@ -2349,11 +2376,12 @@ int guide_gradients( cr_scene *s, const float *records, uint64_t n, float *gW, f
 	return guarded( [&] {
 		if ( !s || !s->guide.ready ) fail( CR_ERR_STATE, "no guide on this scene (cr_guide_reset first)" );
 		if ( !n || !records ) fail( CR_ERR_INVALID, "no records" );
-		float *d;
-		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * 13 * n ), "cudaMalloc" );
-		cudaMemcpy( d, records, sizeof( float ) * 13 * n, cudaMemcpyHostToDevice );
 		GuideState &g = s->guide;
-		g.load_records( d, uint32_t( n ), nullptr );
+		const uint32_t stride = g.learn_select ? 14u : 13u;
+		float *d;
+		cuda_check( cudaMalloc( (void **)&d, sizeof( float ) * stride * n ), "cudaMalloc" );
+		cudaMemcpy( d, records, sizeof( float ) * stride * n, cudaMemcpyHostToDevice );
+		g.load_records( d, uint32_t( n ), stride, nullptr );
 		cuda_check( cudaMemset( g.err_train, 0, 4 ), "guide gradients" );
 		g.gradients( g.rec, uint32_t( n ), nullptr, tc );
 		cuda_check( cudaDeviceSynchronize(), "guide gradients" );

@@ -79,11 +79,13 @@ __global__ void __launch_bounds__( TRAIN_ROWS ) k_guide_train_fp32( GuideRecords
 	for ( uint32_t base = blockIdx.x * TRAIN_ROWS; base < n; base += gridDim.x * TRAIN_ROWS )
 	{
 		uint32_t r = base + m;
-		float w = 0.f;
+		float w = 0.f, pb = 0.f;
 		float3 x = f3( 0.f, 0.f, 0.f ), wo = x, nn = x, om = x;
 		if ( r < n && rec.x[ r ].w > 0.f )
 		{
-			x = f3( rec.x[ r ] ), wo = f3( rec.wo[ r ] ), nn = f3( rec.n[ r ] ), om = f3( rec.om[ r ] );
+			const float4 n4 = rec.n[ r ];
+			x = f3( rec.x[ r ] ), wo = f3( rec.wo[ r ] ), nn = f3( n4 ), om = f3( rec.om[ r ] );
+			pb = n4.w;
 			w = rec.T[ r ].w * norm;
 		}
 		float in[ G_IN ], out[ G_OUT ], acts[ 4 * G_HID ];
@@ -95,7 +97,8 @@ __global__ void __launch_bounds__( TRAIN_ROWS ) k_guide_train_fp32( GuideRecords
 		float g_out[ G_OUT ];
 		float nll = 0.f;
 		if ( w > 0.f )
-			nll = -w * logf( mixture_nll_grad( out, om, w, g_out ) );
+			nll = -w * logf( g.learn_select ? mixture_nll_grad_select( out, om, pb, w, g_out )
+											: mixture_nll_grad( out, om, w, g_out ) );
 		else
 			for ( int i = 0; i < G_OUT; ++i ) g_out[ i ] = 0.f;
 		for ( int o = 16; o; o >>= 1 ) nll += __shfl_xor_sync( 0xFFFFFFFFu, nll, o );
@@ -285,11 +288,13 @@ __global__ void __launch_bounds__( tt::THREADS, 1 ) k_guide_train_tc( GuideRecor
 	for ( uint32_t base = blockIdx.x * THREADS; base < n; base += gridDim.x * THREADS )
 	{
 		const uint32_t r = base + tid;
-		float w = 0.f;
+		float w = 0.f, pb = 0.f;
 		float3 x = f3( 0.f, 0.f, 0.f ), wo = f3( 0.f, 0.f, 1.f ), nn = f3( 0.f, 0.f, 1.f ), om = f3( 0.f, 0.f, 1.f );
 		if ( r < n && rec.x[ r ].w > 0.f )
 		{
-			x = f3( rec.x[ r ] ), wo = f3( rec.wo[ r ] ), nn = f3( rec.n[ r ] ), om = f3( rec.om[ r ] );
+			const float4 n4 = rec.n[ r ];
+			x = f3( rec.x[ r ] ), wo = f3( rec.wo[ r ] ), nn = f3( n4 ), om = f3( rec.om[ r ] );
+			pb = n4.w;
 			w = rec.T[ r ].w * norm;
 		}
 		float v[ G_IN ];
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__( tt::THREADS, 1 ) k_guide_train_tc( GuideRecor
 		float dz[ G_OUT ];
 		float nll = 0.f;
 		if ( w > 0.f )
-			nll = -w * logf( mixture_nll_grad( v, om, w, dz ) );
+			nll = -w * logf( g.learn_select ? mixture_nll_grad_select( v, om, pb, w, dz ) : mixture_nll_grad( v, om, w, dz ) );
 		else
 #pragma unroll
 			for ( int k = 0; k < G_OUT; ++k ) dz[ k ] = 0.f;
@@ -505,14 +510,16 @@ __global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_forward_batch_tc( Gu
 	tc::mlp_forward_tc<G_OUT>( g, Wp, n, src, sink, err );
 }
 
-__global__ void k_records_from_host( GuideRecords rec, const float *src, uint32_t n )
+// Records of `stride` floats: {x, wo, n, w, weight} and, when stride is 14,
+// the BSDF density of w (learned selection).
+__global__ void k_records_from_host( GuideRecords rec, const float *src, uint32_t n, uint32_t stride )
 {
 	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
 	{
-		const float *q = src + 13 * size_t( i );
+		const float *q = src + stride * size_t( i );
 		rec.x[ i ] = make_float4( q[ 0 ], q[ 1 ], q[ 2 ], q[ 12 ] > 0.f ? 1.f : 0.f );
 		rec.wo[ i ] = make_float4( q[ 3 ], q[ 4 ], q[ 5 ], 0.f );
-		rec.n[ i ] = make_float4( q[ 6 ], q[ 7 ], q[ 8 ], 0.f );
+		rec.n[ i ] = make_float4( q[ 6 ], q[ 7 ], q[ 8 ], stride > 13 ? q[ 13 ] : 0.f );
 		rec.om[ i ] = make_float4( q[ 9 ], q[ 10 ], q[ 11 ], 1.f );
 		rec.T[ i ] = make_float4( 1.f, 1.f, 1.f, q[ 12 ] );
 		rec.L[ i ] = make_float4( 0.f, 0.f, 0.f, 0.f );
@@ -599,6 +606,7 @@ GuideDev GuideState::dev() const
 	GuideDev g;
 	g.grid = grid, g.W = W, g.b = b, g.bmin = bmin, g.binv = binv, g.select_prob = select_prob;
 	g.guided_bounces = guided_bounces;
+	g.learn_select = learn_select ? 1u : 0u;
 	return g;
 }
 
@@ -696,10 +704,10 @@ uint32_t GuideState::forward_batch_tc( const float *d_in, uint32_t n, float *d_o
 	return e;
 }
 
-void GuideState::load_records( const float *d_src, uint32_t n, cudaStream_t st )
+void GuideState::load_records( const float *d_src, uint32_t n, uint32_t stride, cudaStream_t st )
 {
 	ensure_records( n );
-	k_records_from_host<<<std::min<uint32_t>( ( n + 255 ) / 256, 4096 ), 256, 0, st>>>( rec, d_src, n );
+	k_records_from_host<<<std::min<uint32_t>( ( n + 255 ) / 256, 4096 ), 256, 0, st>>>( rec, d_src, n, stride );
 	check( cudaMemsetAsync( wsum, 0, 4, st ), "guide records" );
 	k_sum_weights<<<std::min<uint32_t>( ( n + 255 ) / 256, 1024 ), 256, 0, st>>>( rec, n, wsum );
 	check( cudaGetLastError(), "guide records" );

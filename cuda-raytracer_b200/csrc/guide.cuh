@@ -19,6 +19,11 @@ constexpr int G_SH = 16;                           // SH terms (l = 0..3)
 constexpr int G_USED_IN = G_ENC + G_SH + 3;        // 43 (the rest of the 64 inputs are zero)
 constexpr int G_W = G_HID * G_IN;                  // weights per layer (all 64 x 64)
 constexpr float G_KAPPA_MIN = 0.05f, G_KAPPA_MAX = 5000.f;
+// Learned selection: output G_SEL_OUT is the logit of the probability of
+// sampling the guide rather than the BSDF at a vertex, clamped to
+// [G_SEL_MIN, G_SEL_MAX] so that both strategies keep some samples.
+constexpr int G_SEL_OUT = 40;
+constexpr float G_SEL_MIN = 0.02f, G_SEL_MAX = 0.98f;
 
 struct GuideDev
 {
@@ -26,8 +31,9 @@ struct GuideDev
 	const float *W;      // [G_LAYERS][64 out][64 in], FP32 master weights
 	const float *b;      // [G_LAYERS][64] biases
 	float3 bmin, binv;   // scene box: x -> (x - bmin) * binv in [0,1]^3
-	float select_prob;   // probability of sampling the guide at a vertex
+	float select_prob;   // probability of sampling the guide at a vertex (fixed selection)
 	uint32_t guided_bounces;  // vertices 0 .. guided_bounces-1 sample the guide (0: all)
+	uint32_t learn_select;    // 1: the network's output G_SEL_OUT gives the probability per vertex
 };
 
 // Whether vertex `bounce` of a path of at most max_bounce + 1 vertices
@@ -155,6 +161,15 @@ __device__ __forceinline__ void lobes_from_output( const float *o, Lobe *lb )
 	for ( int k = 0; k < G_LOBES; ++k ) lb[ k ].weight /= sum;
 }
 
+// The learned probability of sampling the guide: sigmoid of the selection
+// logit, clamped; `free` reports whether the clamp left it alone.
+__host__ __device__ __forceinline__ float guide_selection( const float *o, bool *free = nullptr )
+{
+	const float raw = 1.f / ( 1.f + expf( -o[ G_SEL_OUT ] ) );
+	if ( free ) *free = raw > G_SEL_MIN && raw < G_SEL_MAX;
+	return fminf( fmaxf( raw, G_SEL_MIN ), G_SEL_MAX );
+}
+
 // vMF density on the sphere: kappa / (2 pi (1 - exp(-2 kappa))) exp(kappa (mu.w - 1)).
 __device__ __forceinline__ float vmf_pdf( const Lobe &l, float3 w )
 {
@@ -278,5 +293,22 @@ __device__ __forceinline__ float mixture_nll_grad( const float *o, float3 w, flo
 		g[ 5 * k ] = dm.x, g[ 5 * k + 1 ] = dm.y, g[ 5 * k + 2 ] = dm.z;
 	}
 	return q;
+}
+
+// Learned selection: gradient of -log m, m = s q(w) + (1 - s) pb, the density
+// of the one-sample MIS of guide (probability s) and BSDF (density pb) that
+// the renderer samples with, times `scale`; returns m (floored at 1e-30).
+// The lobe outputs get the plain NLL gradient times the guide's share
+// s q / m; the selection logit gets -(q - pb) / m s (1 - s).
+__device__ __forceinline__ float mixture_nll_grad_select( const float *o, float3 w, float pb, float scale, float *g )
+{
+	const float q = mixture_nll_grad( o, w, scale, g );
+	bool free;
+	const float s = guide_selection( o, &free );
+	const float m = fmaxf( s * q + ( 1.f - s ) * pb, 1e-30f );
+	const float r = s * q / m;
+	for ( int i = 0; i < 5 * G_LOBES; ++i ) g[ i ] *= r;
+	g[ G_SEL_OUT ] = free ? -scale * ( q - pb ) / m * s * ( 1.f - s ) : 0.f;
+	return m;
 }
 }  // namespace cr

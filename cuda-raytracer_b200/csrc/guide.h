@@ -9,7 +9,8 @@ namespace cr
 {
 // Training records, SoA (one entry per recorded path vertex):
 //   x  = (position, valid)       wo = (outgoing direction, -)
-//   n  = (shading normal, -)     om = (sampled direction, sampling pdf)
+//   n  = (shading normal, BSDF density of the sampled direction)
+//   om = (sampled direction, sampling pdf)
 //   wo.w = luminance of f * cos for the sampled direction
 //   T  = (throughput after the vertex, training weight)
 //   L  = (radiance the path had gathered once it reached the next vertex,
@@ -42,6 +43,7 @@ struct GuideState
 	bool product_target = true;     // fit Li * f * cos (the integrand) instead of Li
 	uint32_t max_steps = 600;       // training budget in Adam steps (0: train every wave)
 	uint32_t guided_bounces = 3;    // leading vertices that sample the guide (0: all but the last)
+	bool learn_select = false;      // the network also outputs the per-vertex probability of sampling the guide
 	uint32_t packed_step = ~0u;     // step whose weights Wp holds (~0: none)
 	GuideRecords rec;
 	uint32_t rec_capacity = 0;
@@ -72,7 +74,8 @@ struct GuideState
 	// each (d_out 16-byte aligned: stored as float4); returns the device error
 	// word (0: no MMA timed out)
 	uint32_t forward_batch_tc( const float *d_in, uint32_t n, float *d_out, cudaStream_t st );
-	// records from n x 13 floats {x, wo, n, w, weight} (device), for tests
-	void load_records( const float *d_src, uint32_t n, cudaStream_t st );
+	// records from n x stride floats {x, wo, n, w, weight[, bsdf pdf]} (device,
+	// stride 13 or 14), for tests
+	void load_records( const float *d_src, uint32_t n, uint32_t stride, cudaStream_t st );
 };
 }  // namespace cr

@@ -449,9 +449,11 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 // One vertex of the MIS estimator (power heuristic over BSDF sampling and
 // area-light NEE; see cr_device.cuh for the BSDFs).
 // Lobes of one path: 40 FP16 values (mean xyz, kappa, weight per lobe) in 5 x 16
-// bytes.  Decoding renormalises the means and the weights, so that sampling
+// bytes, then the probability of sampling the guide (FP32) in a sixth 16-byte
+// slot.  Decoding renormalises the means and the weights, so that sampling
 // and density evaluation see one exactly normalised mixture.
-__device__ __forceinline__ void store_lobes( uint4 *dst, const Lobe *lb )
+constexpr uint32_t LOBE_SLOTS = 6;  // 16-byte slots per path
+__device__ __forceinline__ void store_lobes( uint4 *dst, const Lobe *lb, float sel )
 {
 	float v[ 5 * G_LOBES ];
 #pragma unroll
@@ -467,9 +469,11 @@ __device__ __forceinline__ void store_lobes( uint4 *dst, const Lobe *lb )
 	}
 #pragma unroll
 	for ( int j = 0; j < 5; ++j ) dst[ j ] = make_uint4( h[ 4 * j ], h[ 4 * j + 1 ], h[ 4 * j + 2 ], h[ 4 * j + 3 ] );
+	dst[ 5 ] = make_uint4( __float_as_uint( sel ), 0u, 0u, 0u );
 }
 
-__device__ __forceinline__ void load_lobes( const uint4 *src, PreparedLobe *pl )
+// Returns the stored probability of sampling the guide.
+__device__ __forceinline__ float load_lobes( const uint4 *src, PreparedLobe *pl )
 {
 	Lobe lb[ G_LOBES ];
 	float v[ 5 * G_LOBES ];
@@ -503,6 +507,7 @@ __device__ __forceinline__ void load_lobes( const uint4 *src, PreparedLobe *pl )
 		lb[ k ].weight = wsum > 0.f ? lb[ k ].weight * inv : 1.f / G_LOBES;
 		prepare_lobe( lb[ k ], pl[ k ] );
 	}
+	return __uint_as_float( src[ 5 ].x );
 }
 
 __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
@@ -550,8 +555,13 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 																   mis_transmits( sc.shaders[ sh.child[ 1 ] ].type ) ) ) );
 	PreparedLobe lb[ G_LOBES ];
 	const bool guided = simple && cfg.guide_sample && guided_vertex( cfg.guide, bounce, cfg.max_bounce );
-	const float sel = guided ? cfg.guide.select_prob : 0.f;
-	if ( guided ) load_lobes( lobes, lb );
+	// the probability of sampling the guide: fixed, or learned per vertex
+	float sel = 0.f;
+	if ( guided )
+	{
+		const float learned = load_lobes( lobes, lb );
+		sel = cfg.guide.learn_select ? learned : cfg.guide.select_prob;
+	}
 	if ( sc.n_lights )
 	{
 		uint32_t nli = sc.n_lights;
@@ -606,6 +616,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	}
 	float3 wi;
 	float pdf;
+	float pb_s = 0.f;  // the BSDF density of the sampled direction (training records)
 	float3 wt, nd;
 	bool delta = false;
 	if ( !simple )
@@ -614,6 +625,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		const float us = rand4( key, g, bounce, 2 ).x;
 		wt = mis_sample_tab( sc.shaders, s.shader, wo, entering, us, r1.x, r1.y, wi, pdf, delta );
 		nd = fr.global( wi );
+		pb_s = pdf;
 	}
 	else if ( guided )
 	{
@@ -633,11 +645,13 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		float3 f = mis_eval( sh, wo, wi, pb );
 		pdf = sel * prepared_pdf( lb, nd ) + ( 1.f - sel ) * pb;
 		wt = pdf > 0.f ? f * ( wi.z / pdf ) : f3( 0.f, 0.f, 0.f );
+		pb_s = pb;
 	}
 	else
 	{
 		wt = mis_sample( sh, wo, r1.x, r1.y, wi, pdf );
 		nd = fr.global( wi );
+		pb_s = pdf;
 	}
 	beta = beta * wt;
 	// a continuation through the surface leaves from its far side
@@ -662,7 +676,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		cfg.rec.x[ rec_i ] = make_float4( s.p.x, s.p.y, s.p.z, alive ? 1.f : 0.f );
 		// w: luminance of f * cos for the sampled direction (wt = f cos / pdf)
 		cfg.rec.wo[ rec_i ] = make_float4( -d.x, -d.y, -d.z, lum( wt ) * pdf );
-		cfg.rec.n[ rec_i ] = make_float4( s.ns.x, s.ns.y, s.ns.z, 0.f );
+		cfg.rec.n[ rec_i ] = make_float4( s.ns.x, s.ns.y, s.ns.z, delta ? 0.f : pb_s );
 		cfg.rec.om[ rec_i ] = make_float4( nd.x, nd.y, nd.z, pdf );
 		cfg.rec.T[ rec_i ] = make_float4( beta.x, beta.y, beta.z, 0.f );
 	}
@@ -786,7 +800,7 @@ __global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg,
 					uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
 					if constexpr ( EST == EST_MIS )
 						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
-								   cfg.guide_sample ? wb.lobes + size_t( path ) * 5 : nullptr,
+								   cfg.guide_sample ? wb.lobes + size_t( path ) * LOBE_SLOTS : nullptr,
 								   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
 					else if constexpr ( PROF )
 					{
@@ -857,7 +871,8 @@ __global__ void __launch_bounds__( tc::THREADS, 2 ) k_guide_infer( DevScene sc, 
 	auto sink = [&]( uint32_t i, const float *out ) {
 		Lobe lb[ G_LOBES ];
 		lobes_from_output( out, lb );
-		store_lobes( wb.lobes + size_t( q[ i ] ) * 5, lb );
+		store_lobes( wb.lobes + size_t( q[ i ] ) * LOBE_SLOTS, lb,
+					 cfg.guide.learn_select ? guide_selection( out ) : cfg.guide.select_prob );
 	};
 	tc::mlp_forward_tc<48>( cfg.guide, Wp, n, src, sink, wb.err );
 }
@@ -1199,7 +1214,7 @@ void free_wave( WaveBuffers &wb, cudaStream_t st )
 void alloc_lobes( WaveBuffers &wb, cudaStream_t st )
 {
 	if ( wb.lobes ) return;
-	alloc( wb.lobes, size_t( wb.capacity ) * 5, st );
+	alloc( wb.lobes, size_t( wb.capacity ) * LOBE_SLOTS, st );
 }
 
 void alloc_batch_state( WaveBuffers &wb, cudaStream_t st )

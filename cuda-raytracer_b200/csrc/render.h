@@ -25,7 +25,7 @@ struct WaveBuffers
 	uint32_t *err = nullptr;                    // device error word
 	unsigned long long *work = nullptr;         // extension [0] nodes [1] triangles, shadow [2] [3]
 	uint4 *lobes = nullptr;                     // guided renders: 8 lobes x (mean, kappa, weight) per path,
-	                                            // FP16, 5 x 16 bytes per path
+	                                            // FP16, and the guide's selection probability: 6 x 16 bytes per path
 	uint32_t *path_job = nullptr;               // batched renders: the job (scene render) of each path
 	unsigned long long *tally = nullptr;        // batched renders: closest-hit and shadow rays traced
 };

@@ -397,7 +397,12 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   guided_bounces  vertices 0 .. guided_bounces-1 of a path sample the guide
  *                   (and only their bounces run the guide's inference); later
  *                   vertices sample the BSDF alone (0: every vertex but the
- *                   last) [3] */
+ *                   last) [3]
+ *   learn_select    1: the network also learns, per vertex, the probability of
+ *                   sampling the guide rather than the BSDF (a sigmoid output
+ *                   clamped to [0.02, 0.98], trained on the density of the
+ *                   one-sample mixture the renderer samples); select_prob is
+ *                   then unused [0] */
 typedef struct cr_guide_config {
     float lr;
     float select_prob;
@@ -407,6 +412,7 @@ typedef struct cr_guide_config {
     uint32_t product_target;
     uint32_t max_steps;
     uint32_t guided_bounces;
+    uint32_t learn_select;
 } cr_guide_config;
 /* Apply `in` (when not NULL) and report the schedule in `out` (when not NULL). */
 int cr_guide_configure(cr_scene *s, const cr_guide_config *in, cr_guide_config *out);
@@ -421,7 +427,8 @@ int cr_guide_forward(cr_scene *s, const float *inputs, uint64_t n, float *out);
  * activations on the tensor cores (tcgen05), FP32 accumulation. */
 int cr_guide_forward_tc(cr_scene *s, const float *inputs, uint64_t n, float *out);
 /* Gradients of the weighted mixture NLL over records n x {x, wo, n, w, weight}
- * (13 floats), normalised by the total weight; parameters are not updated. */
+ * (13 floats; 14 with learn_select, the 14th the BSDF density of w),
+ * normalised by the total weight; parameters are not updated. */
 int cr_guide_gradients(cr_scene *s, const float *records, uint64_t n, float *gW, float *gb, float *ggrid);
 /* The same through the training pass the renderer uses: BF16 operands on the
  * tensor cores (tcgen05), FP32 accumulation. */

@@ -11,7 +11,9 @@ and its gradients can be checked:
 * MLP: 5 linear layers 64 -> 64, ReLU after the first four;
 * output: 8 vMF lobes (normalised mean, softplus concentration clamped to
   [0.05, 5000], softmax weights);
-* loss: sum_r w_r * -log q(w_r) / sum_r w_r, and its exact gradients.
+* loss: sum_r w_r * -log q(w_r) / sum_r w_r, and its exact gradients; with
+  learned selection, -log of the one-sample MIS density s q + (1 - s) p_bsdf,
+  s the sigmoid of output 40 clamped to [0.02, 0.98].
 
 The reference has no learned component; this module is checked against
 finite differences of its own loss (tests/test_oracle_guide.py).
@@ -141,8 +143,46 @@ def nll_grad(o, w, scale):
     return g
 
 
-def loss(grid, W, b, bmin, binv, records):
-    """Weighted NLL of records (n x 13: x, wo, n, w, weight), normalised."""
+# Learned selection: output SEL_OUT is the logit of the probability of sampling
+# the guide (rather than the BSDF) at a vertex, clamped to [SEL_MIN, SEL_MAX].
+# The loss then fits the one-sample MIS density m = s q + (1 - s) p_bsdf that
+# the renderer samples with (the objective of Mueller et al. 2019 applied to
+# the whole mixture), so that q and s are trained together.
+SEL_OUT, SEL_MIN, SEL_MAX = 40, 0.02, 0.98
+
+
+def selection(o):
+    raw = 1 / (1 + np.exp(-o[SEL_OUT]))
+    return min(max(raw, SEL_MIN), SEL_MAX), SEL_MIN < raw < SEL_MAX
+
+
+def density(o, w, pb, learn_select):
+    """The density the loss fits: q(w), or s q(w) + (1 - s) p_bsdf."""
+    q = mixture_pdf(o, w)
+    if not learn_select:
+        return q
+    s, _ = selection(o)
+    return s * q + (1 - s) * pb
+
+
+def nll_grad_select(o, w, pb, scale):
+    """d(-scale * log(s q(w) + (1 - s) pb)) / d o."""
+    mus, kaps, pis = lobes(o)
+    q = max(sum(pis[k] * vmf(mus[k], kaps[k], w) for k in range(LOBES)), 1e-300)
+    s, free = selection(o)
+    m = max(s * q + (1 - s) * pb, 1e-300)
+    g = nll_grad(o, w, scale) * (s * q / m)
+    g[SEL_OUT] = -scale * (q - pb) / m * s * (1 - s) if free else 0.0
+    return g
+
+
+def _pb(r):
+    return r[13] if len(r) > 13 else 0.0
+
+
+def loss(grid, W, b, bmin, binv, records, learn_select=False):
+    """Weighted NLL of records (n x 13: x, wo, n, w, weight; a 14th value, the
+    BSDF density of w, with learned selection), normalised."""
     tot = sum(r[12] for r in records if r[12] > 0)
     s = 0.0
     for r in records:
@@ -150,11 +190,16 @@ def loss(grid, W, b, bmin, binv, records):
             continue
         h0, _ = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
         o, _ = forward(W, b, h0)
-        s += r[12] * -np.log(mixture_pdf(o, r[9:12]))
+        s += r[12] * -np.log(density(o, r[9:12], _pb(r), learn_select))
     return s / tot
 
 
-def gradients(grid, W, b, bmin, binv, records):
+def out_grad(o, r, scale, learn_select):
+    w = np.asarray(r[9:12], np.float64)
+    return nll_grad_select(o, w, _pb(r), scale) if learn_select else nll_grad(o, w, scale)
+
+
+def gradients(grid, W, b, bmin, binv, records, learn_select=False):
     """Exact gradients of `loss` with respect to W, b and the grid."""
     gW, gb, ggrid = np.zeros_like(W), np.zeros_like(b), np.zeros_like(grid)
     tot = sum(r[12] for r in records if r[12] > 0)
@@ -163,7 +208,7 @@ def gradients(grid, W, b, bmin, binv, records):
             continue
         h0, cs = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
         o, zs = forward(W, b, h0)
-        dz = nll_grad(o, np.asarray(r[9:12], np.float64), r[12] / tot)
+        dz = out_grad(o, r, r[12] / tot, learn_select)
         for l in range(LAYERS - 1, -1, -1):
             h = h0 if l == 0 else np.maximum(zs[l - 1], 0.0)
             gW[l] += np.outer(dz, h)
@@ -207,7 +252,7 @@ def forward_bf16(W, b, h0):
         h = bf16(np.maximum(z, 0.0))
 
 
-def gradients_bf16(grid, W, b, bmin, binv, records):
+def gradients_bf16(grid, W, b, bmin, binv, records, learn_select=False):
     """Gradients of `loss` as the tensor-core training pass forms them."""
     gW, gb, ggrid = np.zeros_like(W), np.zeros_like(b), np.zeros_like(grid)
     Wb = bf16(W)
@@ -217,7 +262,7 @@ def gradients_bf16(grid, W, b, bmin, binv, records):
             continue
         h0, cs = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
         o, hs = forward_bf16(W, b, h0)
-        dz = nll_grad(o, np.asarray(r[9:12], np.float64), r[12] / tot)
+        dz = out_grad(o, r, r[12] / tot, learn_select)
         for l in range(LAYERS - 1, -1, -1):
             dzb = bf16(dz)
             gW[l] += np.outer(dzb, hs[l])

@@ -22,8 +22,10 @@
 //       Scene::intersect(Seg) (src/core/meta/scene.hpp:57-67) per segment.
 //   lights <scene.json> <out.lights>
 //       the 1024-point tables of every emissive mesh (src/core/primitive/mesh.hpp:61-84).
-//   bench  <scene.json> <W> <H> <spp> <threads> [maxBounce] [repeats]
-//       wall time of the reference's own CPUMulticoreTracer::execute, once per repeat.
+//   bench  <scene.json> <W> <H> <spp> <threads> [maxBounce] [repeats] [x0 y0 x1 y1]
+//       wall time of the reference's own CPUMulticoreTracer::execute, once per repeat;
+//       with an area, the tracer renders that pixel window only, through an
+//       enabled Profiler (src/core/tracer/cpuMulticore.cu:17), whose dump is discarded.
 //   plugin <scene.json> <W> <H> <spp> <out.u8> [seed]      (cr_ref_plugin only)
 //       the CudaWavefront Tracer plugin (cuda-raytracer_b200/plugin/cudaWavefront.hpp)
 //       registered in Factory<Tracer> as src/core/tracer/tracer.impl.cu:8-11
@@ -486,7 +488,18 @@ int cmd_bench( int argc, char **argv )
 		lens = poly::make_object<PinholeLens>( L.scene->camera[ 0 ], W, H, spp );
 	SamplerGenerator gen;
 	Properties pp;
-	pp[ "enable" ] = false;
+	uint64_t px = uint64_t( W ) * H;
+	if ( argc > 12 )
+	{
+		uint32_t a[ 4 ] = { uint32_t( std::stoul( argv[ 9 ] ) ), uint32_t( std::stoul( argv[ 10 ] ) ),
+							uint32_t( std::stoul( argv[ 11 ] ) ), uint32_t( std::stoul( argv[ 12 ] ) ) };
+		pp[ "enable" ] = true;
+		pp[ "output" ] = "/dev/null";
+		pp[ "area" ] = json::array( { a[ 0 ], a[ 1 ], a[ 2 ], a[ 3 ] } );
+		px = uint64_t( a[ 2 ] - a[ 0 ] ) * ( a[ 3 ] - a[ 1 ] );
+	}
+	else
+		pp[ "enable" ] = false;
 	Profiler profiler( pp, tracer->getKernel(), W, H, spp );
 	int repeats = argc > 8 ? std::stoi( argv[ 8 ] ) : 1;
 	for ( int r = 0; r < repeats; ++r )
@@ -495,7 +508,7 @@ int cmd_bench( int argc, char **argv )
 		tracer->execute( image, lens, gen, *L.scene, spp, profiler );
 		double sec = std::chrono::duration<double>( std::chrono::steady_clock::now() - t0 ).count();
 		std::fprintf( stderr, "{\"seconds\": %.6f, \"samples\": %llu, \"threads\": %u}\n", sec,
-					  (unsigned long long)W * H * spp, nth );
+					  (unsigned long long)( px * spp ), nth );
 	}
 	return 0;
 }

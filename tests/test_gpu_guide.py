@@ -90,7 +90,7 @@ def test_guide_configure_validates(guided):
     import cuda_raytracer_b200 as crm
     cfg = g.configure()
     assert cfg["train_paths"] == 32768 and cfg["steps_per_wave"] == 2 and cfg["warmup_steps"] == 8
-    assert cfg["product_target"] == 1 and cfg["max_steps"] == 600 and cfg["guided_bounces"] == 3
+    assert cfg["product_target"] == 1 and cfg["guided_bounces"] == 3
     for bad in ({"lr": 0.0}, {"select_prob": 1.0}, {"train_paths": 0}, {"steps_per_wave": 65}):
         with pytest.raises(crm.CrError):
             g.configure(**bad)
@@ -146,6 +146,40 @@ def test_tc_gradients_match_fp64(guided):
         assert exact < 0.15, (name, errs)
 
 
+@pytest.mark.parametrize("tensor_cores", [False, True])
+def test_selection_gradients_match_fp64(guided, tensor_cores):
+    """Learned selection: records carry the BSDF density of their direction
+    and the loss fits the one-sample mixture s q + (1 - s) p_bsdf; the
+    gradients of both passes, selection logit included, against FP64 (the
+    tensor-core pass against the BF16-emulating FP64 restatement)."""
+    s, g, grid, W, b, info = guided
+    g.configure(learn_select=1)
+    try:
+        rng = np.random.default_rng(9)
+        n = 300
+        inp = _inputs(rng, n)
+        om = rng.normal(size=(n, 3)); om /= np.linalg.norm(om, axis=1, keepdims=True)
+        wts = rng.uniform(0.05, 3.0, n)
+        wts[::7] = 0.0
+        pb = rng.uniform(0.0, 1.5, n)
+        pb[::5] = 0.0
+        recs = np.concatenate([inp, om, wts[:, None], pb[:, None]], 1).astype(np.float32)
+        ggrid, gW, gb = g.gradients(recs, tensor_cores=tensor_cores)
+        bmin, binv = info["bmin"].astype(np.float64), info["binv"].astype(np.float64)
+        fn = G.gradients_bf16 if tensor_cores else G.gradients
+        rW, rb, rgrid = fn(grid, W, b, bmin, binv, recs.astype(np.float64), learn_select=True)
+        tol = 5e-3 if tensor_cores else 2e-3
+        for got, ref in ((gW, rW), (gb, rb), (ggrid, rgrid)):
+            got = got.reshape(ref.shape)
+            rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+            assert rel < tol, rel
+        # the selection logit's bias gradient itself
+        assert abs(gb.reshape(rb.shape)[4, 40] - rb[4, 40]) <= tol * np.abs(rb[4]).max() + 1e-6
+        assert abs(rb[4, 40]) > 0
+    finally:
+        g.configure(learn_select=0)
+
+
 @pytest.mark.parametrize("guided_bounces", [3, 0, 1])
 def test_guided_render_is_unbiased(cr, scenes, guided_bounces):
     """Guided MIS and plain MIS films agree within 3 sigma: one-sample MIS of
@@ -157,7 +191,8 @@ def test_guided_render_is_unbiased(cr, scenes, guided_bounces):
     s = cr.Scene.from_desc(d)
     gd = cr.Guide(s).reset(seed=3)
     # sample the guide from the third wave on
-    gd.configure(steps_per_wave=2, warmup_steps=4, guided_bounces=guided_bounces)
+    gd.configure(steps_per_wave=2, warmup_steps=4, guided_bounces=guided_bounces, max_steps=600,
+                 learn_select=int(guided_bounces == 3))
     W, H, spp = 32, 32, 256
     plain = render_film(cr, s, W, H, spp, seeds=[21, 22], estimator=cr.MIS)
     import torch

@@ -79,3 +79,31 @@ def test_bf16_rounding_is_nearest_even():
     assert np.isfinite(got[4]) and abs(got[4] / 3.0e38 - 1) < 2 ** -8
     # BF16 keeps FP32's exponent range: tiny values are not flushed
     assert got[5] > 0
+
+
+def test_selection_gradients_match_finite_differences():
+    """Learned selection: the loss of the one-sample MIS density
+    s q + (1 - s) p_bsdf; output 40 (the selection logit) and the lobes both
+    get gradients."""
+    grid, W, b, bmin, binv, recs = _setup(seed=4, n=5)
+    rng = np.random.default_rng(5)
+    recs = [np.concatenate([r, [rng.uniform(0.0, 2.0)]]) for r in recs]
+    recs[0][13] = 0.0  # a direction the BSDF cannot sample
+    b[4][40] = 0.3
+    gW, gb, gg = G.gradients(grid, W, b, bmin, binv, recs, learn_select=True)
+    h = 1e-6
+    L = lambda W_, b_: G.loss(grid, W_, b_, bmin, binv, recs, learn_select=True)
+    for o in (40, 3, 7, 12):
+        bp, bm = b.copy(), b.copy()
+        bp[4, o] += h
+        bm[4, o] -= h
+        fd = (L(W, bp) - L(W, bm)) / (2 * h)
+        assert abs(fd - gb[4, o]) <= 1e-7 + 1e-4 * abs(fd), (o, fd, gb[4, o])
+    for _ in range(8):
+        l, o, i = rng.integers(0, G.LAYERS), rng.integers(0, 41), rng.integers(0, 43)
+        Wp, Wm = W.copy(), W.copy()
+        Wp[l, o, i] += h
+        Wm[l, o, i] -= h
+        fd = (L(Wp, b) - L(Wm, b)) / (2 * h)
+        assert abs(fd - gW[l, o, i]) <= 1e-6 + 1e-4 * abs(fd), (l, o, i, fd, gW[l, o, i])
+    assert abs(gb[4, 40]) > 1e-6
