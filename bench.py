@@ -719,7 +719,17 @@ def run_ours(args):
     # L2-resident read bandwidth and FP32 FMA rate of this GPU, measured now:
     # the working set of this workload's traversal fits in L2
     l2_gbs, fp32_tflops = cr.measure_peaks(stream.cuda_stream)
+    # random 80-byte node and 48-byte triangle gathers from an L2-resident
+    # array of this workload's size (node + triangle records, 73 MB): the
+    # achievable L2 rate for the traversal's access pattern; the kernel reads
+    # nodes and triangles in about a 6:4 byte ratio
+    ws = min(int(info["bvh_nodes"] * NODE_BYTES + info["triangles"] * TRI_BYTES), 100 << 20)
+    g80 = cr.measure_gather(80, ws, stream.cuda_stream)
+    g48 = cr.measure_gather(48, ws, stream.cuda_stream)
     ext_flops = (cst.nodes * 96 + cst.tris * 40) / max(cst.extend_launches, 1)  # 8 slab tests x 12 + 40 per triangle
+    # the gather peak for this kernel's mix of node and triangle bytes (harmonic)
+    nb, tb = cst.nodes * NODE_BYTES, cst.tris * TRI_BYTES
+    gather_peak = (nb + tb) / (nb / g80 + tb / g48) if nb + tb > 0 else g80
     # any-hit launches: nodes x 80 B + triangles x 48 B + rays x 48 B (ray in, contribution)
     sh_bytes = (cst.shadow_nodes * NODE_BYTES + cst.shadow_tris * TRI_BYTES + cst.rays_shadow * 48) / max(cst.shadow_launches, 1)
 
@@ -804,6 +814,12 @@ def run_ours(args):
                          "l2": {"achieved": round(achieved, 1), "peak": round(l2_gbs, 1), "unit": "GB/s",
                                 "frac": round(achieved / l2_gbs, 4),
                                 "peak_source": "measured in this run (cr_measure_peaks: 32 MB L2-resident reads)"},
+                         "l2_gather": {"achieved": round(achieved, 1), "peak": round(gather_peak, 1), "unit": "GB/s",
+                                       "frac": round(achieved / gather_peak, 4),
+                                       "peak_source": ("measured in this run (cr_measure_gather: random 80-byte "
+                                                       f"node and 48-byte triangle records from an L2-resident "
+                                                       f"{ws >> 20} MB array, {g80:.0f} and {g48:.0f} GB/s, "
+                                                       "weighted by this kernel's node/triangle bytes)")},
                          "fp32": {"achieved": round(ext_flops / (ext_launch_ms / 1e3) / 1e12, 3),
                                   "peak": round(fp32_tflops, 2), "unit": "TFLOP/s",
                                   "frac": round(ext_flops / (ext_launch_ms / 1e3) / 1e12 / fp32_tflops, 4),

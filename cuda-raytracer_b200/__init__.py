@@ -122,7 +122,7 @@ def lib():
             "cr_scene_set_camera": (I, [P, P, P, P, F]),
             "cr_scene_commit": (I, [P, U64, P]), "cr_scene_set_build": (I, [P, P]),
             "cr_scene_set_kernel": (I, [P, C.c_char_p]), "cr_mesh_file_info": (I, [C.c_char_p, P, P, P, P]),
-            "cr_measure_peaks": (I, [P, P, P]),
+            "cr_measure_peaks": (I, [P, P, P]), "cr_measure_gather": (I, [P, U32, U64, P]),
             "cr_scene_info": (I, [P, P, P, P, P]),
             "cr_scene_destroy": (None, [P]),
             "cr_light_table": (I, [P, U32, P, P]), "cr_scene_set_light_table": (I, [P, U32, P, F]),
@@ -392,6 +392,14 @@ def measure_peaks(stream=0):
     l2, fp = C.c_double(), C.c_double()
     _check(lib().cr_measure_peaks(C.c_void_p(stream), C.byref(l2), C.byref(fp)))
     return l2.value, fp.value
+
+
+def measure_gather(record_bytes=80, array_bytes=64 << 20, stream=0):
+    """cr_measure_gather: GB/s of random whole-record gathers (80-byte nodes or
+    48-byte triangles) from an array of array_bytes (L2-resident below 126 MB)."""
+    g = C.c_double()
+    _check(lib().cr_measure_gather(C.c_void_p(stream), record_bytes, array_bytes, C.byref(g)))
+    return g.value
 
 
 class Batch:

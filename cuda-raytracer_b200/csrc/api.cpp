@@ -2009,6 +2009,18 @@ int cr_measure_peaks( void *stream, double *l2_read_gbs, double *fp32_tflops )
 	} );
 }
 
+extern "C" int cr_measure_gather_impl( void *stream, uint32_t record_bytes, uint64_t array_bytes, double *gbs,
+									   const char **err );
+
+int cr_measure_gather( void *stream, uint32_t record_bytes, uint64_t array_bytes, double *gbs )
+{
+	return guarded( [&] {
+		const char *err = nullptr;
+		if ( cr_measure_gather_impl( stream, record_bytes, array_bytes, gbs, &err ) != 0 )
+			fail( CR_ERR_INVALID, err ? err : "gather measurement failed" );
+	} );
+}
+
 int cr_mesh_file_info( const char *path, uint32_t *n_groups, uint64_t *n_vertices, uint64_t *n_triangles,
 					   double *checksum )
 {
@@ -2048,7 +2060,7 @@ int cr_scene_set_build( cr_scene *s, const cr_build_config *cfg )
 		if ( !s || !cfg ) fail( CR_ERR_INVALID, "null argument" );
 		if ( s->committed ) fail( CR_ERR_STATE, "the BVH options must be set before cr_scene_commit" );
 		if ( cfg->builder != CR_BUILD_PLOC && cfg->builder != CR_BUILD_LBVH ) fail( CR_ERR_INVALID, "unknown builder" );
-		if ( cfg->max_leaf < 1 || cfg->max_leaf > 4 ) fail( CR_ERR_INVALID, "max_leaf must be in [1, 4]" );
+		if ( cfg->max_leaf < 1 || cfg->max_leaf > 3 ) fail( CR_ERR_INVALID, "max_leaf must be in [1, 3]" );
 		if ( cfg->ploc_radius < 1 || cfg->ploc_radius > 256 ) fail( CR_ERR_INVALID, "ploc_radius must be in [1, 256]" );
 		if ( !( cfg->cost_node > 0.f ) || !( cfg->cost_tri > 0.f ) || !( cfg->wide_cost_node > 0.f ) ||
 			 !( cfg->wide_cost_tri > 0.f ) )

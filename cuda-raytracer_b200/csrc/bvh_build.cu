@@ -558,7 +558,8 @@ __global__ void k_collapse( const WorkItem *work, const uint32_t *n_work, WorkIt
 		nd.qhi_z[ s ] = quant_hi( b.hi.z, plo.z, sz, iz );
 		if ( b.leaf )
 		{
-			nd.meta[ s ] = uint8_t( ( b.count << 5 ) | toff );
+			// the leaf's triangle count in unary (1, 3 or 7) above its offset
+			nd.meta[ s ] = uint8_t( ( ( ( 1u << b.count ) - 1u ) << 5 ) | toff );
 			for ( int k = 0; k < b.count; ++k )
 			{
 				uint32_t prim = order[ b.first + k ];
@@ -592,7 +593,8 @@ void check( cudaError_t e, const char *what )
 
 void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st, const BuildParams &bp )
 {
-	if ( bp.max_leaf < 1 || bp.max_leaf > 4 || bp.radius < 1 || bp.radius > 256 || !( bp.cost_node > 0.f ) ||
+	// leaves of at most 3 primitives: a node's meta byte holds the count in unary (3 bits)
+	if ( bp.max_leaf < 1 || bp.max_leaf > 3 || bp.radius < 1 || bp.radius > 256 || !( bp.cost_node > 0.f ) ||
 		 !( bp.cost_tri > 0.f ) )
 		throw std::runtime_error( "bvh: build parameters out of range" );
 	out.n_nodes = 0;

@@ -64,7 +64,7 @@ enum Estimator : int32_t
 //  * child box i = p + 2^e * [q_lo[i], q_hi[i]] per axis (conservatively rounded)
 //  * imask bit i: slot i is an internal node; its index is
 //    child_base + popc(imask & ((1<<i)-1))
-//  * meta[i] for a leaf slot: (n_tris << 5) | offset, triangles
+//  * meta[i] for a leaf slot: (unary n_tris << 5) | offset (unary: 1, 3, 7), triangles
 //    tri_base + offset .. + n_tris - 1 (n_tris 1..3, offset 0..23); 0 if empty
 //  * slots are assigned so that visiting slot (k ^ oct) for k = 0..7 is
 //    roughly front to back for rays whose direction-sign octant is oct.

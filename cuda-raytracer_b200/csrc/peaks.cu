@@ -1,5 +1,6 @@
 // Microbenchmarks for the rooflines the driver's measured peaks do not give:
-// L2-resident read bandwidth and FP32 FMA throughput, measured in the same
+// L2-resident read bandwidth, random record gathers from L2 (the access
+// pattern of BVH traversal) and FP32 FMA throughput, measured in the same
 // process as the kernels they are compared with.
 #include <cuda_runtime.h>
 
@@ -45,7 +46,82 @@ __global__ void k_fma( uint32_t iters, float *sink )
 	for ( int k = 0; k < 8; ++k ) s += a[ k ];
 	if ( s == -1.2345f ) *sink = s;
 }
+// Random whole-record gathers: every thread fetches `iters` records of R
+// 16-byte words at independent pseudo-random indices (xorshift32), through the
+// L1/texture path as the traversal kernels read BVH nodes and triangles.
+template <int R>
+__global__ void __launch_bounds__( 128 ) k_gather( const uint4 *__restrict__ buf, uint32_t n_rec, uint32_t iters,
+												   uint32_t *sink )
+{
+	uint32_t x = 0x9E3779B9u ^ ( blockIdx.x * blockDim.x + threadIdx.x ) * 0x85EBCA6Bu;
+	uint32_t acc = 0;
+	for ( uint32_t i = 0; i < iters; ++i )
+	{
+		x ^= x << 13, x ^= x >> 17, x ^= x << 5;
+		const uint4 *p = buf + size_t( x % n_rec ) * R;
+#pragma unroll
+		for ( int k = 0; k < R; ++k )
+		{
+			const uint4 v = __ldg( p + k );
+			acc ^= v.x ^ v.y ^ v.z ^ v.w;
+		}
+	}
+	if ( acc == 0x12345678u ) *sink = acc;
+}
 }  // namespace
+
+// Achievable rate of random record gathers from an L2-resident array:
+// records of `record_bytes` (80: a wide BVH node, 48: a triangle) from an
+// array of `array_bytes`; returns the gathered bytes per second.
+extern "C" int cr_measure_gather_impl( void *stream, uint32_t record_bytes, uint64_t array_bytes, double *gbs,
+									   const char **err )
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	uint4 *buf = nullptr;
+	uint32_t *sink = nullptr;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	try
+	{
+		if ( record_bytes != 48 && record_bytes != 80 ) throw std::runtime_error( "record_bytes must be 48 or 80" );
+		if ( array_bytes < ( 1u << 20 ) || array_bytes > ( 1ull << 30 ) ) throw std::runtime_error( "array_bytes out of range" );
+		int dev = 0, sms = 0;
+		check( cudaGetDevice( &dev ), "device" );
+		check( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device" );
+		const uint32_t n_rec = uint32_t( array_bytes / record_bytes );
+		check( cudaMalloc( &buf, size_t( n_rec ) * record_bytes ), "cudaMalloc" );
+		check( cudaMalloc( &sink, 4 ), "cudaMalloc" );
+		check( cudaMemsetAsync( buf, 0, size_t( n_rec ) * record_bytes, st ), "memset" );
+		check( cudaEventCreate( &e0 ), "event" );
+		check( cudaEventCreate( &e1 ), "event" );
+		const uint32_t blocks = sms * 8, iters = 2048;
+		auto launch = [&]( uint32_t it ) {
+			if ( record_bytes == 80 )
+				k_gather<5><<<blocks, 128, 0, st>>>( buf, n_rec, it, sink );
+			else
+				k_gather<3><<<blocks, 128, 0, st>>>( buf, n_rec, it, sink );
+		};
+		launch( 256 );  // warm-up: the array into L2
+		check( cudaEventRecord( e0, st ), "event" );
+		launch( iters );
+		check( cudaEventRecord( e1, st ), "event" );
+		check( cudaEventSynchronize( e1 ), "event" );
+		float ms = 0.f;
+		check( cudaEventElapsedTime( &ms, e0, e1 ), "event" );
+		if ( gbs ) *gbs = double( blocks ) * 128.0 * iters * record_bytes / ( ms * 1e-3 ) / 1e9;
+		check( cudaGetLastError(), "gather" );
+	}
+	catch ( const std::exception &ex )
+	{
+		static thread_local std::string msg;
+		msg = ex.what();
+		*err = msg.c_str();
+	}
+	if ( buf ) cudaFree( buf );
+	if ( sink ) cudaFree( sink );
+	if ( e0 ) cudaEventDestroy( e0 );
+	if ( e1 ) cudaEventDestroy( e1 );
+	return *err ? -1 : 0;
+}
 
 extern "C" int cr_measure_peaks_impl( void *stream, double *l2_gbs, double *fp32_tflops, const char **err )
 {

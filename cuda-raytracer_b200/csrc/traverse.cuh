@@ -25,6 +25,20 @@ __device__ __forceinline__ float q8_biased( uint32_t w, uint32_t i )
 }
 constexpr float Q8_BIAS = 32768.f;
 
+// Three-operand max / min (PTX max.f32 / min.f32 with three sources, sm_100).
+__device__ __forceinline__ float fmax3( float a, float b, float c )
+{
+	float d;
+	asm( "max.f32 %0, %1, %2, %3;" : "=f"( d ) : "f"( a ), "f"( b ), "f"( c ) );
+	return d;
+}
+__device__ __forceinline__ float fmin3( float a, float b, float c )
+{
+	float d;
+	asm( "min.f32 %0, %1, %2, %3;" : "=f"( d ) : "f"( a ), "f"( b ), "f"( c ) );
+	return d;
+}
+
 // Intersects the ray with the 8 children of `node`; returns the node-group
 // hits (bits at slot ^ octant) and the triangle-group hits (24-bit mask).
 //
@@ -61,16 +75,19 @@ __device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r,
 		float tnx = fmaf( q8_biased( wnx, bi ), adj_s.x, adj_o.x ), tfx = fmaf( q8_biased( wfx, bi ), adj_s.x, adj_o.x );
 		float tny = fmaf( q8_biased( wny, bi ), adj_s.y, adj_o.y ), tfy = fmaf( q8_biased( wfy, bi ), adj_s.y, adj_o.y );
 		float tnz = fmaf( q8_biased( wnz, bi ), adj_s.z, adj_o.z ), tfz = fmaf( q8_biased( wfz, bi ), adj_s.z, adj_o.z );
-		float tn = fmaxf( fmaxf( tnx, tny ), fmaxf( tnz, tmin ) );
-		float tf = fminf( fminf( tfx, tfy ), fminf( tfz, tlim ) );
-		uint32_t meta = ( ( i < 4 ? n1.z : n1.w ) >> sh ) & 0xFFu;
-		bool internal = ( imask >> i ) & 1u;
+		const float tn = fmax3( tnx, tny, fmaxf( tnz, tmin ) );
+		const float tf = fmin3( tfx, tfy, fminf( tfz, tlim ) );
+		// meta: the leaf's unary triangle count in bits 5..7 above its offset
+		// (0 for internal and empty slots), so its triangles' bits are the
+		// count bits shifted by the offset
+		const uint32_t meta = ( ( i < 4 ? n1.z : n1.w ) >> sh ) & 0xFFu;
+		const bool internal = ( imask >> i ) & 1u;
 		if ( tn <= tf )
 		{
 			if ( internal )
 				node_hits |= 1u << ( i ^ r.oct );
-			else if ( meta )
-				tri_hits |= ( ( 1u << ( meta >> 5 ) ) - 1u ) << ( meta & 31u );
+			else
+				tri_hits |= __funnelshift_l( 0u, meta >> 5, meta );
 		}
 	}
 	ng = node_hits ? make_uint2( n1.x, ( node_hits << 24 ) | imask ) : make_uint2( 0u, 0u );

@@ -188,7 +188,7 @@ int cr_scene_set_kernel(cr_scene *s, const char *name);
  *                CR_BUILD_LBVH: the Morton radix tree (faster build, more
  *                nodes visited per ray)
  *   ploc_radius  clustering search radius in Morton positions [10]
- *   max_leaf     triangles per leaf, 1..4 [3]
+ *   max_leaf     triangles per leaf, 1..3 [3]
  *   cost_node, cost_tri  binary-tree SAH costs of a node visit and a triangle
  *                test [1.2, 1]
  *   collapse     CR_COLLAPSE_SAH: plan the 8-wide collapse by dynamic
@@ -332,6 +332,15 @@ int cr_autotune(cr_scene *s, const cr_render_desc *desc, void *stream, cr_tuning
  * rooflines of traversal when the scene fits in L2 and of its box and
  * triangle tests.  Synchronises `stream`; allocates 32 MB for the call. */
 int cr_measure_peaks(void *stream, double *l2_read_gbs, double *fp32_tflops);
+
+/* No counterpart in the reference.  Measures, on the current device, the
+ * achievable rate of random whole-record gathers, the access pattern of BVH
+ * traversal: records of record_bytes (80: a wide node, 48: a triangle) at
+ * independent pseudo-random indices of an array of array_bytes (1 MB..1 GB;
+ * below the 126 MB L2 it is L2-resident), read through the L1/texture path.
+ * *gbs: gathered bytes per second / 1e9.  Synchronises `stream`; allocates
+ * the array for the call. */
+int cr_measure_gather(void *stream, uint32_t record_bytes, uint64_t array_bytes, double *gbs);
 
 /* ------------------------------------------------------ batched renders */
 /* No counterpart in the reference (its tracer renders one scene per call).
