@@ -13,6 +13,7 @@
 // a Monte Carlo estimate of the KL divergence from the normalised incident
 // radiance to the mixture q (the neural importance sampling objective of
 // Mueller et al., 2019), with Adam.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -478,6 +479,21 @@ __global__ void k_guide_forward_batch( GuideDev g, const float *inp, uint32_t n,
 	}
 }
 
+// FP32 master grid -> the inference's paired FP16 table: slot e of level l
+// holds the features of slots e and e + 1 (mod G_T).
+__global__ void k_pack_grid_pairs( const float *__restrict__ grid, uint2 *__restrict__ pairs )
+{
+	const uint32_t n = uint32_t( G_LEVELS ) * G_T;
+	for ( uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x )
+	{
+		const uint32_t l = i / G_T, e = i % G_T, e1 = ( e + 1 ) & uint32_t( G_T - 1 );
+		const float2 a = reinterpret_cast<const float2 *>( grid )[ size_t( l ) * G_T + e ];
+		const float2 b = reinterpret_cast<const float2 *>( grid )[ size_t( l ) * G_T + e1 ];
+		__half2 ha = __floats2half2_rn( a.x, a.y ), hb = __floats2half2_rn( b.x, b.y );
+		pairs[ i ] = make_uint2( *reinterpret_cast<uint32_t *>( &ha ), *reinterpret_cast<uint32_t *>( &hb ) );
+	}
+}
+
 // FP32 master weights [G_LAYERS][64 out][64 in] -> the BF16 shared-memory
 // images of the tensor-core passes: forward (layer l at l * W_BYTES, element
 // (out, in) at canon(out, in)) and, after it, transposed (element (out, in) at
@@ -561,6 +577,7 @@ void GuideState::init( float3 lo, float3 hi, uint64_t seed )
 	dalloc( W, w_size() ), dalloc( W_m, w_size() ), dalloc( W_v, w_size() ), dalloc( gW, w_size() );
 	dalloc( b, b_size() ), dalloc( b_m, b_size() ), dalloc( b_v, b_size() ), dalloc( gb, b_size() );
 	dalloc( wsum, 1 ), dalloc( loss, 1 ), dalloc( err, 1 ), dalloc( err_train, 1 ), dalloc( Wp, size_t( tc::WP_BYTES ) );
+	dalloc( grid_pairs, size_t( G_LEVELS ) * G_T );
 	check( cudaMemset( loss, 0, 4 ), "guide init" );
 	check( cudaMemset( err_train, 0, 4 ), "guide init" );
 	std::mt19937_64 rng( seed );
@@ -594,6 +611,8 @@ void GuideState::release()
 		if ( p ) cudaFree( p );
 	grid = grid_m = grid_v = ggrid = W = W_m = W_v = gW = b = b_m = b_v = gb = wsum = loss = nullptr;
 	if ( Wp ) cudaFree( Wp );
+	if ( grid_pairs ) cudaFree( grid_pairs );
+	grid_pairs = nullptr;
 	if ( err ) cudaFree( err );
 	if ( err_train ) cudaFree( err_train );
 	Wp = nullptr, err = nullptr, err_train = nullptr;
@@ -604,7 +623,7 @@ void GuideState::release()
 GuideDev GuideState::dev() const
 {
 	GuideDev g;
-	g.grid = grid, g.W = W, g.b = b, g.bmin = bmin, g.binv = binv, g.select_prob = select_prob;
+	g.grid = grid, g.grid_pairs = grid_pairs, g.W = W, g.b = b, g.bmin = bmin, g.binv = binv, g.select_prob = select_prob;
 	g.guided_bounces = guided_bounces;
 	g.learn_select = learn_select ? 1u : 0u;
 	return g;
@@ -685,6 +704,7 @@ void GuideState::forward_batch( const float *d_in, uint32_t n, float *d_out, cud
 void GuideState::pack_weights( cudaStream_t st )
 {
 	k_pack_weights_bf16<<<( G_LAYERS * G_W + 255 ) / 256, 256, 0, st>>>( W, Wp );
+	k_pack_grid_pairs<<<1024, 256, 0, st>>>( grid, grid_pairs );
 	check( cudaGetLastError(), "guide weight packing" );
 }
 

@@ -27,7 +27,10 @@ constexpr float G_SEL_MIN = 0.02f, G_SEL_MAX = 0.98f;
 
 struct GuideDev
 {
-	const float *grid;   // [G_LEVELS][G_T][G_FEAT]
+	const float *grid;   // [G_LEVELS][G_T][G_FEAT], FP32 master
+	// [G_LEVELS][G_T]: FP16 features of slot e and of slot e + 1 (mod G_T; its
+	// +x neighbour), 8 bytes, for the inference's paired gathers
+	const uint2 *grid_pairs;
 	const float *W;      // [G_LAYERS][64 out][64 in], FP32 master weights
 	const float *b;      // [G_LAYERS][64] biases
 	float3 bmin, binv;   // scene box: x -> (x - bmin) * binv in [0,1]^3
@@ -55,15 +58,18 @@ __host__ __device__ __forceinline__ float grid_res( int l )
 	return floorf( r );
 }
 
-// Spatial hash of an integer lattice point (the xor-of-primes hash of
-// Teschner et al. 2003 as used by instant neural graphics primitives); coarse
-// levels whose lattice fits the table are indexed directly.
+// Table slot of an integer lattice point: coarse levels whose lattice fits the
+// table are indexed directly; finer ones hash y and z with the xor-of-primes
+// hash of Teschner et al. (2003) and add x, so that on every level the +x
+// neighbour of a point lives in the next slot (mod the table size).  The
+// inference gathers both x-corners of a cell with one load from a table
+// whose entries are stored paired with their next slot's (guide_tc.cuh).
 __host__ __device__ __forceinline__ uint32_t grid_index( int l, uint32_t ix, uint32_t iy, uint32_t iz )
 {
 	uint32_t res = uint32_t( grid_res( l ) ) + 1u;
 	uint64_t dense = uint64_t( res ) * res * res;
 	if ( dense <= uint64_t( G_T ) ) return ix + res * ( iy + res * iz );
-	return ( ix * 1u ^ iy * 2654435761u ^ iz * 805459861u ) & uint32_t( G_T - 1 );
+	return ( ix + ( iy * 2654435761u ^ iz * 805459861u ) ) & uint32_t( G_T - 1 );
 }
 
 // Real spherical harmonics of bands l = 0..3 of a unit vector (16 terms,

@@ -27,6 +27,7 @@ struct GuideState
 	float *W = nullptr, *W_m = nullptr, *W_v = nullptr, *gW = nullptr;
 	float *b = nullptr, *b_m = nullptr, *b_v = nullptr, *gb = nullptr;
 	uint8_t *Wp = nullptr;    // device: BF16 weights in the tensor-core operand layout (guide_tc.cuh)
+	uint2 *grid_pairs = nullptr;  // device: the inference's paired FP16 copy of the grid (guide.cuh GuideDev)
 	uint32_t *err = nullptr;  // device: error word of the batch forward calls
 	uint32_t *err_train = nullptr;  // device: error word of the tensor-core training pass
 	bool tc_train = true;     // train with the tensor-core pass (false: the FP32 pass)
@@ -69,7 +70,7 @@ struct GuideState
 	void gradients( const GuideRecords &r, uint32_t n, cudaStream_t st, bool tensor_cores );
 	void adam( cudaStream_t st );  // update and clear the gradients
 	void forward_batch( const float *d_in, uint32_t n, float *d_out, cudaStream_t st );
-	void pack_weights( cudaStream_t st );  // W -> Wp
+	void pack_weights( cudaStream_t st );  // W -> Wp and grid -> grid_pairs
 	// BF16 tensor-core forward of n inputs {x, wo, n} (9 floats) to 64 outputs
 	// each (d_out 16-byte aligned: stored as float4); returns the device error
 	// word (0: no MMA timed out)

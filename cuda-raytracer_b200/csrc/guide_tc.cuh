@@ -24,6 +24,7 @@
 // in flight, frees its tensor memory and returns.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "guide.cuh"
 
@@ -155,8 +156,37 @@ __device__ __forceinline__ void store_row( uint8_t *tile, uint32_t r, const floa
 	}
 }
 
-// Row r's network input for (x, wo, n), as guide_encode lays it out, written
-// straight into a canonical K-major tile as BF16, 8 values at a time.
+// Level l's two trilinear features at normalised position u from the paired
+// FP16 table: each of the cell's four (y, z) edges is one 8-byte load that
+// holds both of its x-corners (a slot and its +x neighbour's, the next slot).
+__device__ __forceinline__ float2 level_features_paired( const GuideDev &g, int l, float3 u )
+{
+	const float res = grid_res( l );
+	const float px = fminf( fmaxf( u.x, 0.f ), 1.f ) * res, py = fminf( fmaxf( u.y, 0.f ), 1.f ) * res,
+				pz = fminf( fmaxf( u.z, 0.f ), 1.f ) * res;
+	const float fx = floorf( px ), fy = floorf( py ), fz = floorf( pz );
+	const uint32_t ix = uint32_t( fx ), iy = uint32_t( fy ), iz = uint32_t( fz );
+	const float tx = px - fx, ty = py - fy, tz = pz - fz;
+	const uint2 *tab = g.grid_pairs + size_t( l ) * G_T;
+	float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+	for ( int k = 0; k < 4; ++k )
+	{
+		const uint32_t dy = k & 1, dz = k >> 1;
+		const uint2 pr = __ldg( tab + grid_index( l, ix, iy + dy, iz + dz ) );
+		const float2 a = __half22float2( *reinterpret_cast<const __half2 *>( &pr.x ) );
+		const float2 b = __half22float2( *reinterpret_cast<const __half2 *>( &pr.y ) );
+		const float wyz = ( dy ? ty : 1.f - ty ) * ( dz ? tz : 1.f - tz );
+		const float w0 = wyz * ( 1.f - tx ), w1 = wyz * tx;
+		f0 += w0 * a.x + w1 * b.x;
+		f1 += w0 * a.y + w1 * b.y;
+	}
+	return make_float2( f0, f1 );
+}
+
+// Row r's network input for (x, wo, n), as guide_encode lays it out (the hash
+// features from the paired FP16 table), written straight into a canonical
+// K-major tile as BF16, 8 values at a time.
 __device__ __forceinline__ void encode_store_row( const GuideDev &g, float3 x, float3 wo, float3 n, uint8_t *tile,
 												  uint32_t r )
 {
@@ -165,17 +195,8 @@ __device__ __forceinline__ void encode_store_row( const GuideDev &g, float3 x, f
 #pragma unroll
 	for ( int l = 0; l < G_LEVELS; ++l )
 	{
-		GridCorners c;
-		grid_corners( l, u, c );
-		float f0 = 0.f, f1 = 0.f;
-		const float *tab = g.grid + size_t( l ) * G_T * G_FEAT;
-#pragma unroll
-		for ( int k = 0; k < 8; ++k )
-		{
-			float2 v = *reinterpret_cast<const float2 *>( tab + 2 * c.idx[ k ] );
-			f0 += c.w[ k ] * v.x;
-			f1 += c.w[ k ] * v.y;
-		}
+		const float2 f = level_features_paired( g, l, u );
+		const float f0 = f.x, f1 = f.y;
 		w[ l & 3 ] = pack_bf16x2( f0, f1 );
 		if ( ( l & 3 ) == 3 )
 			*reinterpret_cast<uint4 *>( tile + canon( r, 8 * ( l >> 2 ) ) ) = make_uint4( w[ 0 ], w[ 1 ], w[ 2 ], w[ 3 ] );

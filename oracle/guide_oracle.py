@@ -5,7 +5,8 @@ Restates, in double precision with numpy, what the CUDA guide computes
 and its gradients can be checked:
 
 * encoding: 12-level hash grid (resolution floor(4 * 1.5**l), direct indexing
-  where the lattice fits 2**16 entries, else the xor-of-primes spatial hash),
+  where the lattice fits 2**16 entries, else x plus the xor-of-primes hash of
+  y and z),
   2 features per level, trilinear; 16 real SH terms of wo; the normal; zeros
   up to 64 inputs;
 * MLP: 5 linear layers 64 -> 64, ReLU after the first four;
@@ -41,7 +42,7 @@ def grid_index(l, ix, iy, iz):
     res = int(grid_res(l)) + 1
     if res ** 3 <= T:
         return (ix + res * (iy + res * iz)) & 0xFFFFFFFF
-    h = (ix * 1) ^ ((iy * 2654435761) & 0xFFFFFFFF) ^ ((iz * 805459861) & 0xFFFFFFFF)
+    h = ix + (((iy * 2654435761) & 0xFFFFFFFF) ^ ((iz * 805459861) & 0xFFFFFFFF))
     return h & (T - 1)
 
 
