@@ -27,6 +27,13 @@ batch      the batched workload (64 scenes of uneven size, resolution and spp)
 guiding    time to relMSE 1e-3, plain MIS vs learned guiding (tensor-core
            inference and online training included), on the occluded-light
            scene at 1024x1024 (see guided_vs_plain); rank 0 at N = 1 only.
+config0    the small box scene at its full configuration (256x256, 64 spp,
+           depth 8), the one workload both arms run identically: device and
+           end-to-end rates, the L2 roofline, the reference on the same
+           render; rank 0 at N = 1 only.
+config4    the large combined run (21M triangles, 3840x2160, depth 12): plain
+           and guided rates, HBM roofline, window time to relMSE 1e-3 and the
+           reference on that window; rank 0 at N = 1 only.
 Multi-GPU: one process per GPU; each rank renders the workload with its own
 seed (weak scaling, no data-path collective).
 """
