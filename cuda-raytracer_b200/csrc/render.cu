@@ -448,66 +448,103 @@ __device__ __forceinline__ void shade_koishi( const DevScene &sc, const RenderCo
 
 // One vertex of the MIS estimator (power heuristic over BSDF sampling and
 // area-light NEE; see cr_device.cuh for the BSDFs).
-// Lobes of one path: 40 FP16 values (mean xyz, kappa, weight per lobe) in 5 x 16
-// bytes, then the probability of sampling the guide (FP32) in a sixth 16-byte
-// slot.  Decoding renormalises the means and the weights, so that sampling
-// and density evaluation see one exactly normalised mixture.
-constexpr uint32_t LOBE_SLOTS = 6;  // 16-byte slots per path
+// The guide's proposal for one path vertex, written by the inference kernel
+// already prepared for evaluation (9 x 16 bytes):
+//   slot k < 8, lobe k: mean xyz and weight as FP16, then kappa log2(e) and
+//                       log2(P_k * vMF normaliser) as FP32, P_k = weight /
+//                       (sum of the 8 stored weights)
+//   slot 8:             the probability of sampling the guide (FP32)
+// Sampling (lobe k with probability P_k, then the vMF of mean mu_k and
+// concentration kappa_k) and density evaluation (sum_k 2^(k2 (mu.w - 1) + c))
+// read the same stored values, the means renormalised after FP16 decoding, so
+// the density is the sampled one to FP32 rounding.  Shading reads the lobes
+// from memory as it evaluates them and keeps none in registers.
+constexpr uint32_t LOBE_SLOTS = 9;  // 16-byte slots per path
+
 __device__ __forceinline__ void store_lobes( uint4 *dst, const Lobe *lb, float sel )
 {
-	float v[ 5 * G_LOBES ];
+	__half wh[ G_LOBES ];
+	float sum = 0.f;
 #pragma unroll
 	for ( int k = 0; k < G_LOBES; ++k )
-		v[ 5 * k ] = lb[ k ].mu.x, v[ 5 * k + 1 ] = lb[ k ].mu.y, v[ 5 * k + 2 ] = lb[ k ].mu.z,
-				v[ 5 * k + 3 ] = lb[ k ].kappa, v[ 5 * k + 4 ] = lb[ k ].weight;
-	uint32_t h[ 5 * G_LOBES / 2 ];
-#pragma unroll
-	for ( int i = 0; i < 5 * G_LOBES / 2; ++i )
 	{
-		__half2 p = __floats2half2_rn( v[ 2 * i ], v[ 2 * i + 1 ] );
-		h[ i ] = *reinterpret_cast<uint32_t *>( &p );
+		wh[ k ] = __float2half_rn( lb[ k ].weight );
+		sum += __half2float( wh[ k ] );
 	}
+	const float inv = sum > 0.f ? 1.f / sum : 0.f;
 #pragma unroll
-	for ( int j = 0; j < 5; ++j ) dst[ j ] = make_uint4( h[ 4 * j ], h[ 4 * j + 1 ], h[ 4 * j + 2 ], h[ 4 * j + 3 ] );
-	dst[ 5 ] = make_uint4( __float_as_uint( sel ), 0u, 0u, 0u );
+	for ( int k = 0; k < G_LOBES; ++k )
+	{
+		const float kap = lb[ k ].kappa;
+		const float norm = kap / ( 2.f * PI_F * ( -expm1f( -2.f * kap ) ) );
+		const float P = sum > 0.f ? __half2float( wh[ k ] ) * inv : 1.f / G_LOBES;
+		const __half2 m01 = __floats2half2_rn( lb[ k ].mu.x, lb[ k ].mu.y );
+		__half2 m2w = __floats2half2_rn( lb[ k ].mu.z, 0.f );
+		m2w.y = sum > 0.f ? wh[ k ] : __float2half_rn( 1.f );
+		dst[ k ] = make_uint4( *reinterpret_cast<const uint32_t *>( &m01 ), *reinterpret_cast<const uint32_t *>( &m2w ),
+							   __float_as_uint( kap * 1.4426950408889634f ), __float_as_uint( log2f( P * norm ) ) );
+	}
+	dst[ 8 ] = make_uint4( __float_as_uint( sel ), 0u, 0u, 0u );
 }
 
-// Returns the stored probability of sampling the guide.
-__device__ __forceinline__ float load_lobes( const uint4 *src, PreparedLobe *pl )
+struct StoredLobe
 {
-	Lobe lb[ G_LOBES ];
-	float v[ 5 * G_LOBES ];
-#pragma unroll
-	for ( int j = 0; j < 5; ++j )
-	{
-		uint4 q = src[ j ];
-		uint32_t w[ 4 ] = { q.x, q.y, q.z, q.w };
-#pragma unroll
-		for ( int t = 0; t < 4; ++t )
-		{
-			float2 f = __half22float2( *reinterpret_cast<const __half2 *>( &w[ t ] ) );
-			v[ 8 * j + 2 * t ] = f.x, v[ 8 * j + 2 * t + 1 ] = f.y;
-		}
-	}
-	float wsum = 0.f;
-#pragma unroll
-	for ( int k = 0; k < G_LOBES; ++k )
-	{
-		float3 m = f3( v[ 5 * k ], v[ 5 * k + 1 ], v[ 5 * k + 2 ] );
-		float l2 = dot( m, m );
-		lb[ k ].mu = l2 > 1e-20f ? m * rsqrtf( l2 ) : f3( 0.f, 0.f, 1.f );
-		lb[ k ].kappa = fminf( fmaxf( v[ 5 * k + 3 ], G_KAPPA_MIN ), G_KAPPA_MAX );
-		lb[ k ].weight = fmaxf( v[ 5 * k + 4 ], 0.f );
-		wsum += lb[ k ].weight;
-	}
-	const float inv = wsum > 0.f ? 1.f / wsum : 0.f;
+	float3 mu;
+	float weight, k2, c;
+};
+
+__device__ __forceinline__ StoredLobe load_lobe( const uint4 *rec, int k )
+{
+	const uint4 q = rec[ k ];
+	const float2 m01 = __half22float2( *reinterpret_cast<const __half2 *>( &q.x ) );
+	const float2 m2w = __half22float2( *reinterpret_cast<const __half2 *>( &q.y ) );
+	StoredLobe l;
+	const float3 m = f3( m01.x, m01.y, m2w.x );
+	const float l2 = dot( m, m );
+	l.mu = l2 > 1e-20f ? m * rsqrtf( l2 ) : f3( 0.f, 0.f, 1.f );
+	l.weight = m2w.y;
+	l.k2 = __uint_as_float( q.z );
+	l.c = __uint_as_float( q.w );
+	return l;
+}
+
+// The stored mixture's density at direction w.
+__device__ __forceinline__ float stored_pdf( const uint4 *rec, float3 w )
+{
+	float p = 0.f;
 #pragma unroll
 	for ( int k = 0; k < G_LOBES; ++k )
 	{
-		lb[ k ].weight = wsum > 0.f ? lb[ k ].weight * inv : 1.f / G_LOBES;
-		prepare_lobe( lb[ k ], pl[ k ] );
+		const StoredLobe l = load_lobe( rec, k );
+		p += exp2f( fmaf( l.k2, dot( l.mu, w ) - 1.f, l.c ) );
 	}
-	return __uint_as_float( src[ 5 ].x );
+	return p;
+}
+
+// A direction from the stored mixture: lobe k with probability P_k (u0), then
+// its vMF by the numerically stable inversion of Jakob ("Numerically stable
+// sampling of the von Mises Fisher distribution on S2", 2012).
+__device__ __forceinline__ float3 stored_sample( const uint4 *rec, float u0, float u1, float u2 )
+{
+	float sum = 0.f;
+#pragma unroll
+	for ( int k = 0; k < G_LOBES; ++k ) sum += __half2float( __ushort_as_half( uint16_t( rec[ k ].y >> 16 ) ) );
+	const float target = u0 * sum;
+	int k = 0;
+	float acc = 0.f;
+	for ( ; k < G_LOBES - 1; ++k )
+	{
+		acc += __half2float( __ushort_as_half( uint16_t( rec[ k ].y >> 16 ) ) );
+		if ( target < acc ) break;
+	}
+	const StoredLobe l = load_lobe( rec, k );
+	const float kappa = l.k2 * 0.6931471805599453f;
+	float w = 1.f + logf( u1 + ( 1.f - u1 ) * expf( -2.f * kappa ) ) / kappa;
+	w = fminf( fmaxf( w, -1.f ), 1.f );
+	float r = sqrtf( fmaxf( 0.f, 1.f - w * w ) ), s, c;
+	sincosf( 2.f * PI_F * u2, &s, &c );
+	Frame f = onb_frame( l.mu );
+	return normalize( f.u * ( r * c ) + f.v * ( r * s ) + f.n * w );
 }
 
 __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfig &cfg, uint2 key, uint64_t g,
@@ -553,15 +590,10 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	const bool transmits = !simple && ( mis_transmits( sh.type ) ||
 										( sh.type == SH_MIXED && ( mis_transmits( sc.shaders[ sh.child[ 0 ] ].type ) ||
 																   mis_transmits( sc.shaders[ sh.child[ 1 ] ].type ) ) ) );
-	PreparedLobe lb[ G_LOBES ];
 	const bool guided = simple && cfg.guide_sample && guided_vertex( cfg.guide, bounce, cfg.max_bounce );
 	// the probability of sampling the guide: fixed, or learned per vertex
 	float sel = 0.f;
-	if ( guided )
-	{
-		const float learned = load_lobes( lobes, lb );
-		sel = cfg.guide.learn_select ? learned : cfg.guide.select_prob;
-	}
+	if ( guided ) sel = cfg.guide.learn_select ? __uint_as_float( lobes[ 8 ].x ) : cfg.guide.select_prob;
 	if ( sc.n_lights )
 	{
 		uint32_t nli = sc.n_lights;
@@ -588,7 +620,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 			float pb;
 			float3 f = simple ? mis_eval( sh, wo, wi, pb ) : mis_eval_tab( sc.shaders, s.shader, wo, wi, entering, pb );
 			// one-sample MIS of guide and BSDF: the continuation density
-			if ( guided ) pb = sel * prepared_pdf( lb, wiw ) + ( 1.f - sel ) * pb;
+			if ( guided ) pb = sel * stored_pdf( lobes, wiw ) + ( 1.f - sel ) * pb;
 			if ( !is_zero( f ) )
 			{
 				// the last vertex has no continuation that could reach the light:
@@ -633,7 +665,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		// weight uses the combined density of both strategies
 		if ( r1.z < sel )
 		{
-			nd = mixture_sample( lb, r1.w, r1.x, r1.y );
+			nd = stored_sample( lobes, r1.w, r1.x, r1.y );
 			wi = fr.local( nd );
 		}
 		else
@@ -643,7 +675,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 		}
 		float pb;
 		float3 f = mis_eval( sh, wo, wi, pb );
-		pdf = sel * prepared_pdf( lb, nd ) + ( 1.f - sel ) * pb;
+		pdf = sel * stored_pdf( lobes, nd ) + ( 1.f - sel ) * pb;
 		wt = pdf > 0.f ? f * ( wi.z / pdf ) : f3( 0.f, 0.f, 0.f );
 		pb_s = pb;
 	}
