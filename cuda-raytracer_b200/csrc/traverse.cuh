@@ -5,10 +5,11 @@
 // Each warp owns 32 traversal states.  A lane that finishes its ray is refilled
 // from the queue (one atomic per warp) once enough lanes are idle, so a warp no
 // longer waits for its slowest ray.  Every iteration the warp votes between a
-// node step (each lane with no pending triangles visits one wide node, pops, or
-// finishes) and a triangle step (each lane with pending triangles tests one),
-// taking the triangle step once a quarter of the active lanes want it; the
-// other lanes wait, so lanes in one iteration run the same code.
+// node step (each lane with no pending triangles visits one wide node, popping
+// the stack first when its current group is exhausted, or finishes) and a
+// triangle step (each lane with pending triangles tests one), taking the
+// triangle step once a quarter of the active lanes want it; the other lanes
+// wait, so lanes in one iteration run the same code.
 #pragma once
 #include "cr_device.cuh"
 
@@ -223,6 +224,13 @@ __global__ void __launch_bounds__( TRAVERSE_THREADS, 8 ) k_traverse( DevScene sc
 		}
 		else if ( !tg.y )
 		{
+			// an exhausted group: pop the next one and visit its next child in
+			// this same step (a pushed group always has a child left)
+			if ( ng.y <= 0x00FFFFFFu && sp > 0 )
+			{
+				--sp;
+				ng = sp < SHARED_STACK ? my_stack[ TRAVERSE_THREADS * sp ] : stack[ sp - SHARED_STACK ];
+			}
 			if ( ng.y > 0x00FFFFFFu )
 			{
 				uint32_t b = __ffs( ng.y >> 24 ) - 1;
@@ -248,11 +256,6 @@ __global__ void __launch_bounds__( TRAVERSE_THREADS, 8 ) k_traverse( DevScene sc
 					if ( COUNT ) ++wnodes;
 					visit_node( nodes, r, node, tmin, hit.t * grow, ng, tg );
 				}
-			}
-			else if ( sp > 0 )
-			{
-				--sp;
-				ng = sp < SHARED_STACK ? my_stack[ TRAVERSE_THREADS * sp ] : stack[ sp - SHARED_STACK ];
 			}
 			else
 				done = true;
