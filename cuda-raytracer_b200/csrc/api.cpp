@@ -162,6 +162,7 @@ struct cr_scene
 	// launch configuration (defaults, or the choice of cr_autotune)
 	uint32_t tune_wave = 1u << 22, tune_refill = 16;
 	int tune_blocks = 8;
+	uint32_t tune_shade = 128;
 	BuildParams build;  // BVH build options (cr_scene_set_build)
 
 	~cr_scene() { release(); }
@@ -1245,6 +1246,9 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	c.refill_min = desc->refill_min ? std::min<uint32_t>( desc->refill_min, 32 ) : s->tune_refill;
 	c.traverse_blocks_per_sm =
 		desc->traverse_blocks_per_sm ? int( std::min<uint32_t>( desc->traverse_blocks_per_sm, 8 ) ) : s->tune_blocks;
+	if ( desc->shade_threads && desc->shade_threads != 64 && desc->shade_threads != 128 && desc->shade_threads != 256 )
+		fail( CR_ERR_INVALID, "shade_threads must be 64, 128 or 256" );
+	c.shade_threads = desc->shade_threads ? desc->shade_threads : s->tune_shade;
 	r.sc = dev_scene( s );
 	r.sc.cam = make_camera( s->cam, desc->width, desc->height, desc->spp );
 	c.kernel = kernel;
@@ -1847,12 +1851,13 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
 		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
 		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
-		uint32_t tried = 0;
+		uint32_t tried = 0, shade = 128;
 		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
 			RenderConfig c = cfg;
 			c.wave_paths = uint32_t( std::min<uint64_t>( wave, samples ) );
 			c.refill_min = refill;
 			c.traverse_blocks_per_sm = blocks;
+			c.shade_threads = shade;
 			ensure_wave( s, c.wave_paths, c.max_bounce, st );
 			StageTimes warm, t;
 			render_waves( sc, c, s->wave, sum, sq, cnt, st, &warm );
@@ -1874,6 +1879,17 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 			double v = rate( wave, refill, b );
 			if ( v > best ) best = v, blocks = b;
 		}
+		// the shading kernel's block size (its grid keeps 1024 threads per SM)
+		for ( uint32_t t : { 64u, 256u } )
+		{
+			const uint32_t keep = shade;
+			shade = t;
+			double v = rate( wave, refill, blocks );
+			if ( v > best )
+				best = v;
+			else
+				shade = keep;
+		}
 		for ( uint32_t w : { 1u << 20, 1u << 21, 1u << 23 } )
 		{
 			if ( w > samples && wave >= samples ) continue;
@@ -1889,8 +1905,9 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		}
 		cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
 		cuda_check( cudaStreamSynchronize( st ), "autotune" );
-		s->tune_wave = wave, s->tune_refill = refill, s->tune_blocks = blocks;
+		s->tune_wave = wave, s->tune_refill = refill, s->tune_blocks = blocks, s->tune_shade = shade;
 		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
+		out->shade_threads = shade;
 		out->candidates_tried = tried;
 		out->msamples_per_s = best;
 		out->default_msamples_per_s = dflt;
@@ -1914,6 +1931,7 @@ struct cr_batch
 	uint32_t wave_bounces = 0;
 	uint32_t tune_wave = 1u << 22, tune_refill = 16;
 	int tune_blocks = 8;
+	uint32_t tune_shade = 128;
 	cudaGraph_t graph = nullptr;
 	cudaGraphExec_t exec = nullptr;
 	uint32_t launches_per_render = 0;
@@ -1978,7 +1996,8 @@ void batch_ensure_wave( cr_batch *b, uint32_t cap )
 	alloc_batch_state( b->wave, b->stream );
 }
 
-RenderConfig batch_config( const cr_batch *b, uint32_t wave, uint32_t refill, int blocks, uint64_t total )
+RenderConfig batch_config( const cr_batch *b, uint32_t wave, uint32_t refill, int blocks, uint64_t total,
+						   uint32_t shade = 128 )
 {
 	RenderConfig c{};
 	c.spp = 1, c.max_bounce = b->max_bounce, c.estimator = b->estimator;
@@ -1986,6 +2005,7 @@ RenderConfig batch_config( const cr_batch *b, uint32_t wave, uint32_t refill, in
 	c.wave_paths = uint32_t( std::min<uint64_t>( wave, total ) );
 	c.count_work = false;
 	c.refill_min = refill, c.traverse_blocks_per_sm = blocks;
+	c.shade_threads = shade;
 	return c;
 }
 
@@ -2145,8 +2165,9 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 		upload( d_jobs, jobs.data(), sizeof( BatchJobDev ) * n, st );
 		BatchDev bd{ d_scenes, d_jobs, b->d_seed, n };
 		uint32_t tried = 0;
+		uint32_t shade = 128;
 		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
-			RenderConfig c = batch_config( b, wave, refill, blocks, total );
+			RenderConfig c = batch_config( b, wave, refill, blocks, total, shade );
 			batch_ensure_wave( b, c.wave_paths );
 			StageTimes warm, t;
 			render_batch_waves( bd, jobs.data(), n, c, b->wave, st, &warm );
@@ -2167,6 +2188,17 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 			double v = rate( wave, refill, bl );
 			if ( v > best ) best = v, blocks = bl;
 		}
+		// the shading kernel's block size (its grid keeps 1024 threads per SM)
+		for ( uint32_t t : { 64u, 256u } )
+		{
+			const uint32_t keep = shade;
+			shade = t;
+			double v = rate( wave, refill, blocks );
+			if ( v > best )
+				best = v;
+			else
+				shade = keep;
+		}
 		for ( uint32_t w : { 1u << 21, 1u << 23 } )
 		{
 			if ( w > total && wave >= total ) continue;
@@ -2183,7 +2215,8 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 		for ( void *p : { (void *)sum, (void *)sq, (void *)cnt, (void *)d_scenes, (void *)d_jobs } ) cudaFreeAsync( p, st );
 		cuda_check( cudaStreamSynchronize( st ), "batch autotune" );
 		batch_check_error( b );
-		b->tune_wave = wave, b->tune_refill = refill, b->tune_blocks = blocks;
+		b->tune_wave = wave, b->tune_refill = refill, b->tune_blocks = blocks, b->tune_shade = shade;
+		out->shade_threads = shade;
 		b->drop_graph();
 		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
 		out->candidates_tried = tried;
@@ -2198,7 +2231,7 @@ int cr_batch_render( cr_batch *b, uint64_t seed_offset, cr_stats *stats )
 		if ( !b ) fail( CR_ERR_INVALID, "null batch" );
 		cudaStream_t st = b->stream;
 		const uint32_t n = uint32_t( b->jobs.size() );
-		RenderConfig c = batch_config( b, b->tune_wave, b->tune_refill, b->tune_blocks, b->total );
+		RenderConfig c = batch_config( b, b->tune_wave, b->tune_refill, b->tune_blocks, b->total, b->tune_shade );
 		if ( !b->exec )
 		{
 			// capture the whole batch (every wave, every bounce) once

@@ -770,7 +770,7 @@ __global__ void k_generate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa )
 // PROF: a profiled render (reference estimator, one scene): each shaded vertex
 // writes its bounce record and each ending path its slice's bounce counter.
 template <bool BATCH, int EST, bool PROF = false>
-__global__ void __launch_bounds__( 128 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
+__global__ void __launch_bounds__( 256 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
 												  uint32_t bounce, uint2 key, BatchDev bd )
 {
 	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
@@ -1267,7 +1267,8 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 	const uint32_t P = cfg.wave_paths;
 	const int sms = sm_count();
 	const int g_ext = sms * std::max( 1, std::min( 8, cfg.traverse_blocks_per_sm ) );
-	const int g_shade = sms * 8;
+	const uint32_t shade_t = cfg.shade_threads == 64 || cfg.shade_threads == 256 ? cfg.shade_threads : 128u;
+	const int g_shade_k = int( uint32_t( sms ) * 1024u / shade_t );  // k_shade: SMs x 1024 threads
 	EventPool pool;
 	struct Mark
 	{
@@ -1328,9 +1329,9 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 			} );
 			timed( 2, [&] {
 				if ( cfg.estimator == EST_MIS )
-					k_shade<true, EST_MIS><<<g_shade, 128, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
+					k_shade<true, EST_MIS><<<g_shade_k, shade_t, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
 				else
-					k_shade<true, EST_KOISHI><<<g_shade, 128, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
+					k_shade<true, EST_KOISHI><<<g_shade_k, shade_t, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
 			} );
 			timed( 1, [&] {
 				BatchShadowIO io;
@@ -1384,6 +1385,8 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	const int sms = sm_count();
 	const int g_ext = sms * std::max( 1, std::min( 8, cfg.traverse_blocks_per_sm ) );
 	const int g_shade = sms * 8;
+	const uint32_t shade_t = cfg.shade_threads == 64 || cfg.shade_threads == 256 ? cfg.shade_threads : 128u;
+	const int g_shade_k = int( uint32_t( sms ) * 1024u / shade_t );  // k_shade: SMs x 1024 threads
 	const uint2 key = make_uint2( uint32_t( cfg.seed ), uint32_t( cfg.seed >> 32 ) ^ 0x5EED5EEDu );
 	EventPool pool;
 	struct Mark
@@ -1470,11 +1473,11 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 			else
 				timed( 2, [&] {
 					if ( cfg.estimator == EST_MIS )
-						k_shade<false, EST_MIS><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+						k_shade<false, EST_MIS><<<g_shade_k, shade_t, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
 					else if ( profiled )
-						k_shade<false, EST_KOISHI, true><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+						k_shade<false, EST_KOISHI, true><<<g_shade_k, shade_t, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
 					else
-						k_shade<false, EST_KOISHI><<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+						k_shade<false, EST_KOISHI><<<g_shade_k, shade_t, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
 				} );
 			if ( sc.n_lights && cfg.kernel != KERNEL_NORMAL && cfg.kernel != KERNEL_HALFVECTOR )
 				timed( 1, [&] {

@@ -59,6 +59,7 @@ typedef struct cr_render_desc {
     int32_t count_work;      /* 1: also count BVH nodes / triangles visited            */
     uint32_t refill_min;     /* traversal: idle lanes of 32 that trigger a refill; 0 = tuned */
     uint32_t traverse_blocks_per_sm; /* traversal grid, 1..8 blocks per SM; 0 = tuned    */
+    uint32_t shade_threads;  /* shading block size: 64, 128 or 256; 0 = tuned           */
 } cr_render_desc;
 
 /* Launch configuration chosen by cr_autotune (also used by later renders of
@@ -70,6 +71,7 @@ typedef struct cr_tuning {
     uint32_t candidates_tried;
     double msamples_per_s;   /* rate of the chosen configuration on the sample render */
     double default_msamples_per_s; /* rate of the built-in defaults on the same sample */
+    uint32_t shade_threads;  /* shading block size */
 } cr_tuning;
 
 typedef struct cr_stats {
