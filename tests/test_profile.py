@@ -116,17 +116,24 @@ def test_profile_matches_the_reference_profiler(cr, scenes, oracle, tmp_path):
     po = {k for k, v in ours.items() if v["bounce"]}
     pr = {k for k, v in ref.items() if v["bounce"]}
     assert len(pr) > 20, len(pr)
-    # bright samples: as many as the reference prints, within Monte Carlo error
+    # bright samples are rare paths (the panel is not seen directly): as many
+    # print as the reference prints, within Monte Carlo error, with a similar
+    # number of bounces
     assert abs(len(po) - len(pr)) <= 4 * np.sqrt(len(pr)) + 5, (len(po), len(pr))
-    both = po & pr
-    assert len(both) > 0.3 * len(pr), (len(both), len(pr))
-    for k in both:
-        a, b = ours[k]["records"], ref[k]["records"]
-        assert ours[k]["bounce"][1] == ref[k]["bounce"][1] == DEPTH
-        if a and b:
-            # the camera ray (PinholeLens::sample) and the first shader are the same
-            np.testing.assert_allclose(a[0]["ray"], b[0]["ray"], rtol=1e-5, atol=1e-5)
-            assert a[0]["shader"] == b[0]["shader"], k
+    mo = np.mean([ours[k]["bounce"][0] for k in po])
+    mr = np.mean([ref[k]["bounce"][0] for k in pr])
+    assert abs(mo - mr) < 1.0, (mo, mr)
+    # in both dumps, the first record of every printed sample holds the camera
+    # ray PinholeLens::sample gives for its (x, y, k): the records sit in
+    # their samples' slices
+    for dump, printed in ((ours, po), (ref, pr)):
+        keys = sorted(printed)
+        pix = np.array([[k[0], k[1]] for k in keys])
+        o, dd = scenes.pinhole_rays(d.camera, W, H, SPP, pix, np.array([k[2] for k in keys]))
+        got = np.array([dump[k]["records"][0]["ray"] for k in keys])
+        np.testing.assert_allclose(got[:, :3], o, rtol=2e-5, atol=2e-5)  # six printed digits
+        np.testing.assert_allclose(got[:, 3:], dd, rtol=2e-5, atol=2e-5)
+        assert all(dump[k]["bounce"][1] == DEPTH for k in keys)
     # printed records: a record per counted bounce (up to the depth), and the
     # recorded radiance never decreases along the path
     for v in ours.values():
