@@ -53,7 +53,7 @@ class RenderDesc(C.Structure):
                 ("estimator", C.c_int32), ("x0", C.c_uint32), ("y0", C.c_uint32), ("x1", C.c_uint32),
                 ("y1", C.c_uint32), ("seed", C.c_uint64), ("wave_paths", C.c_uint32), ("guiding", C.c_int32),
                 ("count_work", C.c_int32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32),
-                ("shade_threads", C.c_uint32)]
+                ("shade_threads", C.c_uint32), ("rr_start", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -166,7 +166,8 @@ def _p(a):
 
 
 def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, window=None, wave_paths=0,
-                guiding=False, count_work=False, refill_min=0, traverse_blocks_per_sm=0, shade_threads=0):
+                guiding=False, count_work=False, refill_min=0, traverse_blocks_per_sm=0, shade_threads=0,
+                rr_start=0):
     d = RenderDesc()
     d.width, d.height, d.spp = width, height, spp
     d.max_bounce = U32_MAX if max_bounce is None else max_bounce
@@ -180,6 +181,7 @@ def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, win
     d.refill_min = refill_min
     d.traverse_blocks_per_sm = traverse_blocks_per_sm
     d.shade_threads = shade_threads
+    d.rr_start = rr_start
     return d
 
 

@@ -1249,6 +1249,7 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	if ( desc->shade_threads && desc->shade_threads != 64 && desc->shade_threads != 128 && desc->shade_threads != 256 )
 		fail( CR_ERR_INVALID, "shade_threads must be 64, 128 or 256" );
 	c.shade_threads = desc->shade_threads ? desc->shade_threads : s->tune_shade;
+	c.rr_start = desc->rr_start ? desc->rr_start : 4u;
 	r.sc = dev_scene( s );
 	r.sc.cam = make_camera( s->cam, desc->width, desc->height, desc->spp );
 	c.kernel = kernel;

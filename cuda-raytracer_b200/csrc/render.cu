@@ -690,7 +690,7 @@ __device__ __forceinline__ void shade_mis( const DevScene &sc, const RenderConfi
 	const bool through = wi.z < 0.f;
 	bool alive = !is_zero( beta ) && ( through ? dot( nd, s.ng ) < 0.f : dot( nd, s.ng ) > 0.f );
 	float rr = maxc( beta );
-	if ( alive && rr < 1.f && bounce > 3 )
+	if ( alive && rr < 1.f && bounce >= cfg.rr_start )
 	{
 		float q = fmaxf( .05f, 1.f - rr );
 		if ( r0.w < q )

@@ -93,6 +93,7 @@ struct RenderConfig
 	uint32_t refill_min = 16;        // traversal: idle lanes per warp that trigger a refill (1..32)
 	int traverse_blocks_per_sm = 8;  // traversal grid = SMs x this (1..8; 128-thread blocks)
 	uint32_t shade_threads = 128;    // shading block size (64, 128 or 256); grid of SMs x 1024 threads
+	uint32_t rr_start = 4;           // MIS estimator: first bounce at which Russian roulette may end a path
 	ProfileDev prof{};               // profiled renders (reference estimator, Radiance kernel)
 };
 

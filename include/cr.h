@@ -60,6 +60,9 @@ typedef struct cr_render_desc {
     uint32_t refill_min;     /* traversal: idle lanes of 32 that trigger a refill; 0 = tuned */
     uint32_t traverse_blocks_per_sm; /* traversal grid, 1..8 blocks per SM; 0 = tuned    */
     uint32_t shade_threads;  /* shading block size: 64, 128 or 256; 0 = tuned           */
+    uint32_t rr_start;       /* MIS estimator: first bounce at which Russian roulette may
+                                end a path; 0 = 4 (the reference's "after bounce 3", which
+                                the reference estimator always uses); above max_bounce: none */
 } cr_render_desc;
 
 /* Launch configuration chosen by cr_autotune (also used by later renders of

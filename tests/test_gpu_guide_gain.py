@@ -1,7 +1,8 @@
 """What the trained guide gains over the method without it: on the occluded-
-light scene (light behind a wall with a small aperture, Lambert receivers),
-after online training the guided MIS estimator reaches a clearly lower relMSE
-than plain MIS at the same number of samples per pixel."""
+light scene of the guiding benchmark (light behind a wall with a small
+aperture, Beckmann receivers of roughness 0.05-0.5), after online training
+the guided MIS estimator reaches a clearly lower relMSE than plain MIS at the
+same number of samples per pixel."""
 import numpy as np
 import pytest
 
@@ -21,7 +22,7 @@ def _film(torch):
 def test_trained_guide_lowers_error_at_equal_spp(cr, scenes):
     require_gpu()
     import torch
-    sc = cr.Scene.from_desc(scenes.config3(level=6, width=RES, height=RES, diffuse=True))
+    sc = cr.Scene.from_desc(scenes.config3(level=6, width=RES, height=RES))
     stream = torch.cuda.current_stream().cuda_stream
 
     def render(f, spp, seed, guiding, wave=0):
@@ -43,10 +44,11 @@ def test_trained_guide_lowers_error_at_equal_spp(cr, scenes):
 
     # online training on the tracer's own paths (guided renders train as they go)
     g = cr.Guide(sc).reset(seed=5)
+    g.configure(steps_per_wave=16, max_steps=600)
     T = _film(torch)
     for i in range(32):
         render(T, 16, 500 + i, True, wave=1 << 18)
-    assert g.info()["step"] >= 100
+    assert g.info()["step"] == 600  # trained to its budget, then frozen
     plain, guided = [], []
     for rep in range(4):
         for guiding, out in ((False, plain), (True, guided)):
