@@ -1725,21 +1725,19 @@ int cr_render_profile( cr_scene *s, const cr_render_desc *desc, uint32_t depth, 
 		pd.depth = depth;
 		double *sum = nullptr, *sq = nullptr;
 		uint32_t *cnt = nullptr;
-		auto release = [&] {
+		auto release = [&] {  // once: the pointers are cleared
 			for ( void *p : { (void *)pd.slices, (void *)pd.bounces, (void *)sum, (void *)sq, (void *)cnt } )
 				if ( p ) cudaFreeAsync( p, st );
+			pd.slices = nullptr, pd.bounces = nullptr, sum = nullptr, sq = nullptr, cnt = nullptr;
 		};
 		try
 		{
 			cuda_check( cudaMallocAsync( (void **)&pd.slices, sizeof( cr_profile_slice ) * n, st ), "cudaMalloc" );
 			cuda_check( cudaMemsetAsync( pd.slices, 0, sizeof( cr_profile_slice ) * n, st ), "memset" );
-			if ( depth )
-			{
-				cuda_check( cudaMallocAsync( (void **)&pd.bounces, sizeof( cr_profile_bounce ) * n * depth, st ), "cudaMalloc" );
-				cuda_check( cudaMemsetAsync( pd.bounces, 0, sizeof( cr_profile_bounce ) * n * depth, st ), "memset" );
-			}
-			else
-				pd.bounces = reinterpret_cast<cr_profile_bounce *>( pd.slices );  // never written at depth 0
+			// at depth 0 no record is written; one keeps the buffer valid
+			const size_t nb = std::max<size_t>( n * depth, 1 );
+			cuda_check( cudaMallocAsync( (void **)&pd.bounces, sizeof( cr_profile_bounce ) * nb, st ), "cudaMalloc" );
+			cuda_check( cudaMemsetAsync( pd.bounces, 0, sizeof( cr_profile_bounce ) * nb, st ), "memset" );
 			cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
 			cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
 			cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
@@ -1763,7 +1761,6 @@ int cr_render_profile( cr_scene *s, const cr_render_desc *desc, uint32_t depth, 
 				cuda_check( cudaMemcpyAsync( hc.data(), cnt, npx * 4, cudaMemcpyDeviceToHost, st ), "download" );
 			}
 			cuda_check( cudaStreamSynchronize( st ), "profile" );
-			if ( pd.bounces == reinterpret_cast<cr_profile_bounce *>( pd.slices ) ) pd.bounces = nullptr;
 			release();
 			check_device_error( s, st );
 			if ( film )
@@ -1772,7 +1769,6 @@ int cr_render_profile( cr_scene *s, const cr_render_desc *desc, uint32_t depth, 
 		}
 		catch ( ... )
 		{
-			if ( pd.bounces == reinterpret_cast<cr_profile_bounce *>( pd.slices ) ) pd.bounces = nullptr;
 			release();
 			throw;
 		}
