@@ -98,8 +98,8 @@ __global__ void __launch_bounds__( TRAIN_ROWS ) k_guide_train_fp32( GuideRecords
 		float g_out[ G_OUT ];
 		float nll = 0.f;
 		if ( w > 0.f )
-			nll = -w * logf( g.learn_select ? mixture_nll_grad_select( out, om, pb, w, g_out )
-											: mixture_nll_grad( out, om, w, g_out ) );
+			nll = -w * ( g.learn_select ? mixture_nll_grad_select( out, om, pb, w, g_out )
+										: mixture_nll_grad( out, om, w, g_out ) );
 		else
 			for ( int i = 0; i < G_OUT; ++i ) g_out[ i ] = 0.f;
 		for ( int o = 16; o; o >>= 1 ) nll += __shfl_xor_sync( 0xFFFFFFFFu, nll, o );
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__( tt::THREADS, 1 ) k_guide_train_tc( GuideRecor
 		float dz[ G_OUT ];
 		float nll = 0.f;
 		if ( w > 0.f )
-			nll = -w * logf( g.learn_select ? mixture_nll_grad_select( v, om, pb, w, dz ) : mixture_nll_grad( v, om, w, dz ) );
+			nll = -w * ( g.learn_select ? mixture_nll_grad_select( v, om, pb, w, dz ) : mixture_nll_grad( v, om, w, dz ) );
 		else
 #pragma unroll
 			for ( int k = 0; k < G_OUT; ++k ) dz[ k ] = 0.f;

@@ -271,18 +271,29 @@ __device__ __forceinline__ void guide_forward_fp32( const float *__restrict__ W,
 }
 
 // Gradient of -log q(w) with respect to the 40 used outputs, times `scale`;
-// returns q(w) (floored at 1e-30).
+// returns log q(w).  The lobes' log densities and their responsibilities are
+// formed in log space (log-sum-exp), so a direction far from every lobe, whose
+// vMF densities all underflow in FP32 at large kappa, still gets its gradient.
 __device__ __forceinline__ float mixture_nll_grad( const float *o, float3 w, float scale, float *g )
 {
 	Lobe lb[ G_LOBES ];
 	lobes_from_output( o, lb );
-	float v[ G_LOBES ], q = 0.f;
-	for ( int k = 0; k < G_LOBES; ++k ) v[ k ] = vmf_pdf( lb[ k ], w ), q += lb[ k ].weight * v[ k ];
-	q = fmaxf( q, 1e-30f );
+	float lv[ G_LOBES ], mx = -INFINITY;
+	for ( int k = 0; k < G_LOBES; ++k )
+	{
+		const float kap = lb[ k ].kappa;
+		// log(weight * kappa / (2 pi (1 - exp(-2 kappa)))) + kappa (mu.w - 1)
+		lv[ k ] = logf( lb[ k ].weight ) + logf( kap / ( 2.f * PI_F ) ) - log1pf( -expf( -2.f * kap ) ) +
+				  kap * ( dot( lb[ k ].mu, w ) - 1.f );
+		mx = fmaxf( mx, lv[ k ] );
+	}
+	float sum = 0.f;
+	for ( int k = 0; k < G_LOBES; ++k ) sum += expf( lv[ k ] - mx );
+	const float logq = mx + logf( sum );
 	for ( int i = 0; i < G_OUT; ++i ) g[ i ] = 0.f;
 	for ( int k = 0; k < G_LOBES; ++k )
 	{
-		float gam = lb[ k ].weight * v[ k ] / q;  // responsibility
+		float gam = expf( lv[ k ] - logq );  // responsibility
 		// weight logits: pi_k - gamma_k
 		g[ 5 * k + 4 ] = scale * ( lb[ k ].weight - gam );
 		// concentration: d log v / d kappa = 1/kappa - 2/(e^{2 kappa} - 1) + mu.w - 1
@@ -298,23 +309,27 @@ __device__ __forceinline__ float mixture_nll_grad( const float *o, float3 w, flo
 		float3 dm = ( w - lb[ k ].mu * dot( lb[ k ].mu, w ) ) * ( -scale * gam * kap / len );
 		g[ 5 * k ] = dm.x, g[ 5 * k + 1 ] = dm.y, g[ 5 * k + 2 ] = dm.z;
 	}
-	return q;
+	return logq;
 }
 
 // Learned selection: gradient of -log m, m = s q(w) + (1 - s) pb, the density
 // of the one-sample MIS of guide (probability s) and BSDF (density pb) that
-// the renderer samples with, times `scale`; returns m (floored at 1e-30).
+// the renderer samples with, times `scale`; returns log m (in log space too).
 // The lobe outputs get the plain NLL gradient times the guide's share
 // s q / m; the selection logit gets -(q - pb) / m s (1 - s).
 __device__ __forceinline__ float mixture_nll_grad_select( const float *o, float3 w, float pb, float scale, float *g )
 {
-	const float q = mixture_nll_grad( o, w, scale, g );
+	const float logq = mixture_nll_grad( o, w, scale, g );
 	bool free;
 	const float s = guide_selection( o, &free );
-	const float m = fmaxf( s * q + ( 1.f - s ) * pb, 1e-30f );
-	const float r = s * q / m;
+	const float a = logf( s ) + logq;                                   // log(s q)
+	const float c = pb > 0.f ? logf( 1.f - s ) + logf( pb ) : -INFINITY;  // log((1 - s) pb)
+	const float mx = fmaxf( a, c );
+	const float logm = mx + logf( expf( a - mx ) + expf( c - mx ) );
+	const float r = expf( a - logm );  // the guide's share s q / m
 	for ( int i = 0; i < 5 * G_LOBES; ++i ) g[ i ] *= r;
-	g[ G_SEL_OUT ] = free ? -scale * ( q - pb ) / m * s * ( 1.f - s ) : 0.f;
-	return m;
+	// -(q - pb) / m * s (1 - s) = -((1 - s) r - s (1 - r)) with (1 - s) pb / m = 1 - r
+	g[ G_SEL_OUT ] = free ? -scale * ( ( 1.f - s ) * r - s * ( 1.f - r ) ) : 0.f;
+	return logm;
 }
 }  // namespace cr

@@ -117,25 +117,37 @@ def vmf(mu, kap, w):
     return kap / (2 * np.pi * (-np.expm1(-2 * kap))) * np.exp(kap * (mu @ w - 1))
 
 
-def mixture_pdf(o, w):
+def log_vmf(mu, kap, w):
+    return np.log(kap / (2 * np.pi)) - np.log1p(-np.exp(-2 * kap)) + kap * (mu @ w - 1)
+
+
+def log_terms(o, w):
+    """log(pi_k v_k(w)) per lobe and their log-sum-exp, log q(w): in log space,
+    so that directions far from every sharp lobe keep their responsibilities."""
     mus, kaps, pis = lobes(o)
-    return sum(pis[k] * vmf(mus[k], kaps[k], w) for k in range(LOBES))
+    with np.errstate(divide="ignore"):
+        lv = np.array([np.log(pis[k]) + log_vmf(mus[k], kaps[k], w) for k in range(LOBES)])
+    mx = lv.max()
+    return lv, mx + np.log(np.exp(lv - mx).sum())
+
+
+def mixture_pdf(o, w):
+    return np.exp(log_terms(o, w)[1])
 
 
 def nll_grad(o, w, scale):
     """d(-scale * log q(w)) / d o  (first 40 outputs; the rest are zero)."""
     mus, kaps, pis = lobes(o)
-    v = np.array([vmf(mus[k], kaps[k], w) for k in range(LOBES)])
-    q = max((pis * v).sum(), 1e-300)
+    lv, logq = log_terms(o, w)
     g = np.zeros(OUT)
     for k in range(LOBES):
-        gam = pis[k] * v[k] / q
+        gam = np.exp(lv[k] - logq)
         g[5 * k + 4] = scale * (pis[k] - gam)
         raw = o[5 * k + 3]
         sp = softplus(raw)
         clamped = sp < KMIN or sp > KMAX
         kap = kaps[k]
-        dlogv = 1 / kap - 2 / np.expm1(2 * kap) + mus[k] @ w - 1
+        dlogv = 1 / kap - 2 * np.exp(-2 * kap) / -np.expm1(-2 * kap) + mus[k] @ w - 1  # 2 / (e^{2 kappa} - 1)
         sig = 1 / (1 + np.exp(-raw))
         g[5 * k + 3] = 0.0 if clamped else -scale * gam * dlogv * sig
         m = o[5 * k:5 * k + 3]
@@ -157,23 +169,22 @@ def selection(o):
     return min(max(raw, SEL_MIN), SEL_MAX), SEL_MIN < raw < SEL_MAX
 
 
-def density(o, w, pb, learn_select):
-    """The density the loss fits: q(w), or s q(w) + (1 - s) p_bsdf."""
-    q = mixture_pdf(o, w)
+def log_density(o, w, pb, learn_select):
+    """The log of the density the loss fits: q(w), or s q(w) + (1 - s) p_bsdf."""
+    logq = log_terms(o, w)[1]
     if not learn_select:
-        return q
+        return logq
     s, _ = selection(o)
-    return s * q + (1 - s) * pb
+    return np.logaddexp(np.log(s) + logq, np.log(1 - s) + np.log(pb) if pb > 0 else -np.inf)
 
 
 def nll_grad_select(o, w, pb, scale):
     """d(-scale * log(s q(w) + (1 - s) pb)) / d o."""
-    mus, kaps, pis = lobes(o)
-    q = max(sum(pis[k] * vmf(mus[k], kaps[k], w) for k in range(LOBES)), 1e-300)
+    logq = log_terms(o, w)[1]
     s, free = selection(o)
-    m = max(s * q + (1 - s) * pb, 1e-300)
-    g = nll_grad(o, w, scale) * (s * q / m)
-    g[SEL_OUT] = -scale * (q - pb) / m * s * (1 - s) if free else 0.0
+    r = np.exp(np.log(s) + logq - log_density(o, w, pb, True))  # the guide's share s q / m
+    g = nll_grad(o, w, scale) * r
+    g[SEL_OUT] = -scale * ((1 - s) * r - s * (1 - r)) if free else 0.0
     return g
 
 
@@ -191,7 +202,7 @@ def loss(grid, W, b, bmin, binv, records, learn_select=False):
             continue
         h0, _ = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
         o, _ = forward(W, b, h0)
-        s += r[12] * -np.log(density(o, r[9:12], _pb(r), learn_select))
+        s += r[12] * -log_density(o, r[9:12], _pb(r), learn_select)
     return s / tot
 
 

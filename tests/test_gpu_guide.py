@@ -146,6 +146,31 @@ def test_tc_gradients_match_fp64(guided):
         assert exact < 0.15, (name, errs)
 
 
+def test_gradients_where_every_lobe_density_underflows(guided):
+    """Every lobe sharp (kappa near 2000) and far from the recorded
+    directions: the mixture density underflows in FP32, yet the log-space
+    responsibilities give the FP64 oracle's gradients."""
+    s, g, grid, W, b, info = guided
+    b2 = b.copy()
+    b2[4][3:40:5] = 2000.0
+    g.set_params(None, None, b2.astype(np.float32))
+    try:
+        rng = np.random.default_rng(21)
+        n = 64
+        inp = _inputs(rng, n)
+        om = rng.normal(size=(n, 3)); om /= np.linalg.norm(om, axis=1, keepdims=True)
+        recs = np.concatenate([inp, om, rng.uniform(0.1, 2.0, (n, 1))], 1).astype(np.float32)
+        ggrid, gW, gb = g.gradients(recs)
+        rW, rb, rgrid = G.gradients(grid, W, b2, info["bmin"].astype(np.float64), info["binv"].astype(np.float64),
+                                    recs.astype(np.float64))
+        for got, ref in ((gW, rW), (gb, rb), (ggrid, rgrid)):
+            got = got.reshape(ref.shape)
+            assert np.isfinite(got).all()
+            assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 5e-3
+    finally:
+        g.set_params(None, None, b.astype(np.float32))
+
+
 @pytest.mark.parametrize("tensor_cores", [False, True])
 def test_selection_gradients_match_fp64(guided, tensor_cores):
     """Learned selection: records carry the BSDF density of their direction

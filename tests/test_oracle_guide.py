@@ -107,3 +107,23 @@ def test_selection_gradients_match_finite_differences():
         fd = (L(Wp, b) - L(Wm, b)) / (2 * h)
         assert abs(fd - gW[l, o, i]) <= 1e-6 + 1e-4 * abs(fd), (l, o, i, fd, gW[l, o, i])
     assert abs(gb[4, 40]) > 1e-6
+
+
+def test_gradients_where_every_lobe_density_underflows():
+    """Sharp lobes (kappa up to 5000) far from the recorded direction: every
+    vMF density underflows, but the log-space responsibilities keep the
+    gradient finite and equal to finite differences of the log-space loss."""
+    grid, W, b, bmin, binv, recs = _setup(seed=6, n=4)
+    b[4][3:40:5] = 2000.0  # every lobe's kappa near 2000 (below the clamp)
+    logq = [G.log_terms(G.forward(W, b, G.encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])[0])[0], r[9:12])[1]
+            for r in recs]
+    assert min(logq) < -745  # q itself underflows to 0 in FP64 for some record
+    g = G.gradients(grid, W, b, bmin, binv, recs)
+    assert all(np.isfinite(a).all() for a in g)
+    h = 1e-6
+    for o in (0, 1, 2, 3, 4, 8, 9):
+        bp, bm = b.copy(), b.copy()
+        bp[4, o] += h
+        bm[4, o] -= h
+        fd = (G.loss(grid, W, bp, bmin, binv, recs) - G.loss(grid, W, bm, bmin, binv, recs)) / (2 * h)
+        assert abs(fd - g[1][4, o]) <= 1e-6 + 1e-4 * abs(fd), (o, fd, g[1][4, o])
