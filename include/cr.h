@@ -401,7 +401,8 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   select_prob     probability of sampling the guide at a vertex [0.5]
  *   train_paths     paths per training batch [32768: up to 2^18 vertices at
  *                   max_bounce 7]
- *   steps_per_wave  batches (Adam steps) per wave [2]
+ *   steps_per_wave  batches (Adam steps) per wave [16]: the 600-step budget is
+ *                   spent in the first waves, then the guide is frozen
  *   warmup_steps    steps taken before the guide is first sampled [8]; until
  *                   then a guided render samples the BSDF only and trains
  *   product_target  1: fit the integrand Li f cos at each vertex; 0: fit the
