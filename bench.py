@@ -587,8 +587,9 @@ def config4_section(cr, dev, steps, warmup, with_reference, ttt_seconds=40.0):
                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                         "traffic": (round(traffic["dram_bytes_per_ray"] * cst.rays_extend / max(cst.extend_launches, 1))
                                     if traffic else None),
-                        "traffic_note": ("ncu DRAM bytes per ray of one captured launch "
-                                         "(profiles/k_extend_traffic_config4.json) scaled to this run's rays per launch")
+                        "traffic_note": ("ncu DRAM bytes per ray over the closest-hit launches of one captured 1-spp "
+                                         "render (profiles/k_extend_traffic_config4.json), scaled to this run's rays "
+                                         "per launch")
                                         if traffic else None,
                         "algorithmic_bytes_per_launch": round(ext_launch_bytes),
                         "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
@@ -806,8 +807,9 @@ def run_ours(args):
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": (round(traffic["dram_bytes_per_ray"] * cst.rays_extend / max(cst.extend_launches, 1))
                                      if traffic else None),
-                         "traffic_note": ("ncu DRAM bytes per ray of a captured launch (profiles/k_extend_traffic.json) "
-                                          "scaled to this run's rays per launch") if traffic else None,
+                         "traffic_note": ("ncu DRAM bytes per ray over the closest-hit launches of one captured 4-spp "
+                                          "render (profiles/k_extend_traffic.json), scaled to this run's rays per "
+                                          "launch") if traffic else None,
                          "algorithmic_bytes_per_launch": round(ext_launch_bytes),
                          "launch_ms": round(ext_launch_ms, 4),
                          "nodes_per_ray": round(cst.nodes / max(cst.rays_extend, 1), 3),
