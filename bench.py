@@ -251,9 +251,16 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     R a plain MIS render of ref_spp samples per pixel (Var[R] its per-pixel
     variance of the mean, removed so that the figure estimates the error
     against the converged image).  Each run renders 4 spp per call into one
-    film; its clock is the device time of those calls (CUDA events), guided
-    runs including their inference and online training.  A run stops at the
-    target or after tmax_s."""
+    film; its clock is the device time of all its calls (CUDA events).  A run
+    stops at the target or after tmax_s.
+
+    Two plain runs: with the reference's Russian roulette (after bounce 3,
+    the library's default for plain renders) and without roulette; the
+    speed-up is taken against the faster of the two.  The guided run uses the
+    library's defaults for guided renders (no roulette, 600 training steps
+    front-loaded at 16 per wave); its guide first trains on renders into a
+    scratch film until the training budget is spent (clocked), so that the
+    measured film holds only samples of the trained guide."""
     import torch
     from cuda_raytracer_b200 import scenes
     res = 1024
@@ -266,8 +273,9 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
         return (torch.zeros(n * 3, dtype=torch.float64, device=dev), torch.zeros(n * 3, dtype=torch.float64, device=dev),
                 torch.zeros(n, dtype=torch.int32, device=dev))
 
-    def render(f, spp, seed, guiding):
-        desc = cr.render_desc(res, res, spp, max_bounce=MAX_BOUNCE, estimator=cr.MIS, seed=seed, guiding=guiding)
+    def render(f, spp, seed, guiding, rr_start=0):
+        desc = cr.render_desc(res, res, spp, max_bounce=MAX_BOUNCE, estimator=cr.MIS, seed=seed, guiding=guiding,
+                              rr_start=rr_start)
         sc.render_device(desc, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), stream=stream, stats=False)
 
     R = film()
@@ -280,18 +288,29 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     den = Rm * Rm + 1e-2
     del R
 
-    def run(guiding):
-        if guiding:
-            cr.Guide(sc).reset(seed=7)
-        F = film()
+    def timed(f, seed, guiding, rr_start):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ms, spp, k, hit, err = 0.0, 0, 0, None, None
+        e0.record()
+        render(f, 4, seed, guiding, rr_start)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1)
+
+    def run(guiding, rr_start=0):
+        ms, k, train_ms = 0.0, 0, 0.0
+        if guiding:
+            g = cr.Guide(sc).reset(seed=7)
+            budget = g.configure()["max_steps"]
+            T = film()
+            while g.info()["step"] < budget and ms < tmax_s * 1e3:
+                ms += timed(T, 500_000 + k, True, rr_start)
+                k += 1
+            train_ms = ms
+            del T
+        F = film()
+        spp, hit, err = 0, None, None
         while ms < tmax_s * 1e3:
-            e0.record()
-            render(F, 4, 1 + k, guiding)
-            e1.record()
-            torch.cuda.synchronize(dev)
-            ms += e0.elapsed_time(e1)
+            ms += timed(F, 1 + k, guiding, rr_start)
             spp += 4
             k += 1
             c2 = F[2].double().repeat_interleave(3)
@@ -300,19 +319,24 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
                 hit = ms / 1e3
                 break
         return {"time_to_target_s": None if hit is None else round(hit, 3), "spp": spp,
-                "relmse_at_stop": float(f"{err:.4e}"), "device_s": round(ms / 1e3, 3),
-                "msamples_per_s": round(n * spp / (ms / 1e3) / 1e6, 2)}
+                "training_s": round(train_ms / 1e3, 3), "relmse_at_stop": float(f"{err:.4e}"),
+                "device_s": round(ms / 1e3, 3), "msamples_per_s": round(n * spp / ((ms - train_ms) / 1e3) / 1e6, 2)}
 
     plain = run(False)
+    plain_no_rr = run(False, rr_start=MAX_BOUNCE + 1)
     guided = run(True)
     g = cr.Guide(sc)
+    best = [x["time_to_target_s"] for x in (plain, plain_no_rr) if x["time_to_target_s"]]
     out = {"workload": "config3: occluded light (wall with a 0.4x0.4 aperture), 1024x1024, "
                        f"{sc.info()['triangles']} triangles, max depth 8, MIS estimator",
            "metric": f"device seconds to relMSE <= {target:g} against a {ref_spp}-spp plain reference",
-           "reference_spp": ref_spp, "max_seconds": tmax_s, "plain": plain, "guided": guided,
-           "guide": {"steps": g.info()["step"], **{k: v for k, v in g.configure().items()}},
-           "speedup": (round(plain["time_to_target_s"] / guided["time_to_target_s"], 3)
-                       if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
+           "reference_spp": ref_spp, "max_seconds": tmax_s, "plain": plain, "plain_no_roulette": plain_no_rr,
+           "guided": guided,
+           "guide": {"steps": g.info()["step"], **{k: v for k, v in g.configure().items()}, "roulette": "none"},
+           "speedup": (round(min(best) / guided["time_to_target_s"], 3)
+                       if best and guided["time_to_target_s"] else None),
+           "speedup_vs_plain_reference_roulette": (round(plain["time_to_target_s"] / guided["time_to_target_s"], 3)
+                                                   if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
     sc.close()
     return out
 
@@ -501,7 +525,7 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
     plain = run(False)
     guided = run(True)
     return {"window": list(win), "reference_spp": ref_spp, "max_seconds": tmax_s, "target": target,
-            "plain": plain, "guided": guided,
+            "roulette": {"plain": "after bounce 3", "guided": "none"}, "plain": plain, "guided": guided,
             "speedup": (round(plain["time_to_target_s"] / guided["time_to_target_s"], 3)
                         if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
 

@@ -39,11 +39,11 @@ struct GuideState
 	uint32_t step = 0;              // Adam steps taken
 	uint64_t waves = 0;             // waves trained on (moves the record offset)
 	uint32_t train_paths = 32768;   // paths per batch: up to 32768 x 8 = 2^18 vertices at max_bounce 7
-	uint32_t steps_per_wave = 16;   // batches (Adam steps) recorded and trained per wave: front-loaded
+	uint32_t steps_per_wave = 64;   // batches (Adam steps) recorded and trained per wave: front-loaded
 	uint32_t warmup_steps = 8;      // steps before the guide is first sampled
 	bool product_target = true;     // fit Li * f * cos (the integrand) instead of Li
 	uint32_t max_steps = 600;       // training budget in Adam steps (0: train every wave)
-	uint32_t guided_bounces = 3;    // leading vertices that sample the guide (0: all but the last)
+	uint32_t guided_bounces = 4;    // leading vertices that sample the guide (0: all but the last)
 	bool learn_select = false;      // the network also outputs the per-vertex probability of sampling the guide
 	uint32_t packed_step = ~0u;     // step whose weights Wp holds (~0: none)
 	GuideRecords rec;

@@ -61,8 +61,9 @@ typedef struct cr_render_desc {
     uint32_t traverse_blocks_per_sm; /* traversal grid, 1..8 blocks per SM; 0 = tuned    */
     uint32_t shade_threads;  /* shading block size: 64, 128 or 256; 0 = tuned           */
     uint32_t rr_start;       /* MIS estimator: first bounce at which Russian roulette may
-                                end a path; 0 = 4 (the reference's "after bounce 3", which
-                                the reference estimator always uses); above max_bounce: none */
+                                end a path; 0 = the default: 4 (the reference's "after
+                                bounce 3", which the reference estimator always uses) for
+                                plain renders, none for guided renders; above max_bounce: none */
 } cr_render_desc;
 
 /* Launch configuration chosen by cr_autotune (also used by later renders of
@@ -401,8 +402,8 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   select_prob     probability of sampling the guide at a vertex [0.5]
  *   train_paths     paths per training batch [32768: up to 2^18 vertices at
  *                   max_bounce 7]
- *   steps_per_wave  batches (Adam steps) per wave [16]: the 600-step budget is
- *                   spent in the first waves, then the guide is frozen
+ *   steps_per_wave  batches (Adam steps) per wave [64]: the 600-step budget is
+ *                   spent in the first ten waves, then the guide is frozen
  *   warmup_steps    steps taken before the guide is first sampled [8]; until
  *                   then a guided render samples the BSDF only and trains
  *   product_target  1: fit the integrand Li f cos at each vertex; 0: fit the
@@ -412,7 +413,7 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   guided_bounces  vertices 0 .. guided_bounces-1 of a path sample the guide
  *                   (and only their bounces run the guide's inference); later
  *                   vertices sample the BSDF alone (0: every vertex but the
- *                   last) [3]
+ *                   last) [4]
  *   learn_select    1: the network also learns, per vertex, the probability of
  *                   sampling the guide rather than the BSDF (a sigmoid output
  *                   clamped to [0.02, 0.98], trained on the density of the
