@@ -394,7 +394,7 @@ def config0_section(cr, dev, steps, warmup, l2_gbs, with_reference):
         t0 = time.perf_counter()
         s2 = cr.Scene.from_desc(d)
         film, _ = s2.render(W, H, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k,
-                            **{k2: tune[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads")})
+                            **{k2: tune[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads", "bin_rays")})
         s2.close()
         times.append(time.perf_counter() - t0)
         assert np.isfinite(film).all()
@@ -464,7 +464,8 @@ def batched_workload(cr, dev, n_scenes, seed=2):
            "msamples_per_s": round(total / st.ms_total / 1e3, 2), "ms_per_replay": round(st.ms_total, 2),
            "per_scene_calls_msamples_per_s": round(total / ms_single / 1e3, 2),
            "speedup_vs_per_scene_calls": round(ms_single / st.ms_total, 3),
-           "graph_nodes": st.launches, "waves": st.waves, "autotuned": tune,
+           "graph_nodes": st.graph_nodes, "kernel_launches_per_replay": st.launches, "waves": st.waves,
+           "autotuned": tune,
            "scene_build_s": round(t_build, 1)}
     b.close()
     return out
@@ -475,7 +476,8 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
     (x0, y0, x1, y1) of a W x H frame: the reference is a plain MIS render of
     the window at ref_spp; each run renders step_spp per call into one film,
     clocked by CUDA events, until the target or tmax_s (relMSE as in
-    guided_vs_plain, the reference's own variance removed)."""
+    guided_vs_plain, the reference's own variance removed).  The guided run
+    first trains its guide to the budget on a scratch film (clocked)."""
     import torch
     x0, y0, x1, y1 = win
     n = (x1 - x0) * (y1 - y0)
@@ -500,11 +502,22 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
     del R
 
     def run(guiding):
-        if guiding:
-            cr.Guide(scene).reset(seed=7)
-        F = film()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ms, spp, k, hit, err = 0.0, 0, 0, None, None
+        ms, spp, k, hit, err, train_ms = 0.0, 0, 0, None, None, 0.0
+        if guiding:  # train the guide to its budget on a scratch film first (clocked)
+            g = cr.Guide(scene).reset(seed=7)
+            budget = g.configure()["max_steps"]
+            T = film()
+            while g.info()["step"] < budget and ms < tmax_s * 1e3:
+                e0.record()
+                render(T, step_spp, 500_000 + k, True)
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms += e0.elapsed_time(e1)
+                k += 1
+            train_ms = ms
+            del T
+        F = film()
         while ms < tmax_s * 1e3:
             e0.record()
             render(F, step_spp, 1 + k, guiding)
@@ -519,8 +532,8 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
                 hit = ms / 1e3
                 break
         return {"time_to_target_s": None if hit is None else round(hit, 3), "spp": spp,
-                "relmse_at_stop": float(f"{err:.4e}"), "device_s": round(ms / 1e3, 3),
-                "msamples_per_s": round(n * spp / (ms / 1e3) / 1e6, 2)}
+                "training_s": round(train_ms / 1e3, 3), "relmse_at_stop": float(f"{err:.4e}"),
+                "device_s": round(ms / 1e3, 3), "msamples_per_s": round(n * spp / ((ms - train_ms) / 1e3) / 1e6, 2)}
 
     plain = run(False)
     guided = run(True)
@@ -776,7 +789,7 @@ def run_ours(args):
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
             sc2 = cr.Scene.from_desc(desc)
-            tk = {k2: tuning[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads")} if tuning else {}
+            tk = {k2: tuning[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads", "bin_rays")} if tuning else {}
             film, _ = sc2.render(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k, **tk)
             sc2.close()
             times.append(time.perf_counter() - t0)

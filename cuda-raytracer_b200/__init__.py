@@ -53,13 +53,13 @@ class RenderDesc(C.Structure):
                 ("estimator", C.c_int32), ("x0", C.c_uint32), ("y0", C.c_uint32), ("x1", C.c_uint32),
                 ("y1", C.c_uint32), ("seed", C.c_uint64), ("wave_paths", C.c_uint32), ("guiding", C.c_int32),
                 ("count_work", C.c_int32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32),
-                ("shade_threads", C.c_uint32), ("rr_start", C.c_uint32)]
+                ("shade_threads", C.c_uint32), ("rr_start", C.c_uint32), ("bin_rays", C.c_int32)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("wave_paths", C.c_uint32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32),
                 ("candidates_tried", C.c_uint32), ("msamples_per_s", C.c_double),
-                ("default_msamples_per_s", C.c_double), ("shade_threads", C.c_uint32)]
+                ("default_msamples_per_s", C.c_double), ("shade_threads", C.c_uint32), ("bin_rays", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -70,7 +70,8 @@ class Stats(C.Structure):
                 ("ms_shade", C.c_double), ("ms_other", C.c_double), ("ms_guide", C.c_double), ("samples", C.c_uint64),
                 ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64), ("nodes", C.c_uint64),
                 ("tris", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_tris", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32),
-                ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32), ("ms_guide_train", C.c_double)]
+                ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32), ("ms_guide_train", C.c_double),
+                ("graph_nodes", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -141,6 +142,7 @@ def lib():
             "cr_guide_configure": (I, [P, P, P]), "cr_guide_loss": (I, [P, P]),
             "cr_guide_forward_tc": (I, [P, P, U64, P]), "cr_guide_gradients_tc": (I, [P, P, U64, P, P, P]),
             "cr_batch_create": (I, [P, U32, U32, C.c_int32, P, P]), "cr_batch_autotune": (I, [P, P]),
+            "cr_batch_set_tuning": (I, [P, P]),
             "cr_batch_render": (I, [P, U64, P]), "cr_batch_destroy": (None, [P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
@@ -167,7 +169,7 @@ def _p(a):
 
 def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, window=None, wave_paths=0,
                 guiding=False, count_work=False, refill_min=0, traverse_blocks_per_sm=0, shade_threads=0,
-                rr_start=0):
+                rr_start=0, bin_rays=0):
     d = RenderDesc()
     d.width, d.height, d.spp = width, height, spp
     d.max_bounce = U32_MAX if max_bounce is None else max_bounce
@@ -182,6 +184,7 @@ def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, win
     d.traverse_blocks_per_sm = traverse_blocks_per_sm
     d.shade_threads = shade_threads
     d.rr_start = rr_start
+    d.bin_rays = bin_rays
     return d
 
 
@@ -425,6 +428,13 @@ class Batch:
         t = Tuning()
         _check(lib().cr_batch_autotune(self.h, C.byref(t)))
         return t
+
+    def set_tuning(self, wave_paths=0, refill_min=0, traverse_blocks_per_sm=0, shade_threads=0):
+        """cr_batch_set_tuning: launch configuration (0 keeps a field)."""
+        t = Tuning()
+        t.wave_paths, t.refill_min, t.traverse_blocks_per_sm = wave_paths, refill_min, traverse_blocks_per_sm
+        t.shade_threads = shade_threads
+        _check(lib().cr_batch_set_tuning(self.h, C.byref(t)))
 
     def render(self, seed_offset=0, stats=True):
         st = Stats() if stats else None

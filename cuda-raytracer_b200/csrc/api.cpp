@@ -163,6 +163,7 @@ struct cr_scene
 	uint32_t tune_wave = 1u << 22, tune_refill = 16;
 	int tune_blocks = 8;
 	uint32_t tune_shade = 128;
+	bool tune_bin = false;
 	BuildParams build;  // BVH build options (cr_scene_set_build)
 
 	~cr_scene() { release(); }
@@ -1249,6 +1250,7 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 	if ( desc->shade_threads && desc->shade_threads != 64 && desc->shade_threads != 128 && desc->shade_threads != 256 )
 		fail( CR_ERR_INVALID, "shade_threads must be 64, 128 or 256" );
 	c.shade_threads = desc->shade_threads ? desc->shade_threads : s->tune_shade;
+	c.bin_rays = desc->bin_rays ? desc->bin_rays > 0 : s->tune_bin;
 	// plain renders: the reference's roulette after bounce 3; guided renders:
 	// none (on the occluded-light scene roulette's variance is most of what
 	// the guide leaves, and removing it makes guiding 2.7x as efficient as
@@ -1288,7 +1290,8 @@ bool wave_fits( uint64_t paths, uint32_t max_bounce )
 	return need * 2 <= free_b;
 }
 
-void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t st, bool lobes = false )
+void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t st, bool lobes = false,
+				  bool bins = false )
 {
 	if ( !( s->wave.capacity >= cap && s->wave_bounces >= max_bounce ) )
 	{
@@ -1297,6 +1300,7 @@ void ensure_wave( cr_scene *s, uint32_t cap, uint32_t max_bounce, cudaStream_t s
 		s->wave_bounces = max_bounce;
 	}
 	if ( lobes ) alloc_lobes( s->wave, st );
+	if ( bins ) alloc_bins( s->wave, st );
 }
 
 void check_device_error( cr_scene *s, cudaStream_t st )
@@ -1305,7 +1309,8 @@ void check_device_error( cr_scene *s, cudaStream_t st )
 	cuda_check( cudaMemcpyAsync( &e, s->wave.capacity ? s->wave.err : s->err.p, 4, cudaMemcpyDeviceToHost, st ), "error word" );
 	cuda_check( cudaStreamSynchronize( st ), "error word" );
 	if ( e ) fail( CR_ERR_DEVICE, "a traversal kernel reported error flags " + std::to_string( e ) +
-								  " (1: stack overflow, 2: node index or budget, 4: triangle index, 8: guide MMA wait timed out)" );
+								  " (1: stack overflow, 2: node index or budget, 4: triangle index, 8: guide MMA wait timed out, "
+								  "16: ray binning overflow)" );
 }
 
 void fill_stats( cr_stats *out, const StageTimes &t, uint64_t samples )
@@ -1327,7 +1332,7 @@ void render_device( cr_scene *s, const cr_render_desc *desc, double *sum, double
 					cr_stats *stats )
 {
 	Resolved r = resolve( s, desc );
-	ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st, r.cfg.guiding );
+	ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st, r.cfg.guiding, r.cfg.bin_rays );
 	StageTimes t;
 	render_waves( r.sc, r.cfg, s->wave, sum, sq, cnt, st, stats ? &t : nullptr, &s->guide );
 	if ( stats )
@@ -1749,7 +1754,7 @@ int cr_render_profile( cr_scene *s, const cr_render_desc *desc, uint32_t depth, 
 			cuda_check( cudaMemsetAsync( sq, 0, npx * 24, st ), "memset" );
 			cuda_check( cudaMemsetAsync( cnt, 0, npx * 4, st ), "memset" );
 			r.cfg.prof = pd;
-			ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st );
+			ensure_wave( s, r.cfg.wave_paths, r.cfg.max_bounce, st, false, r.cfg.bin_rays );
 			render_waves( r.sc, r.cfg, s->wave, sum, sq, cnt, st, nullptr, &s->guide );
 			cuda_check( cudaMemcpyAsync( slices, pd.slices, sizeof( cr_profile_slice ) * n, cudaMemcpyDeviceToHost, st ),
 						"download" );
@@ -1853,13 +1858,15 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
 		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
 		uint32_t tried = 0, shade = 128;
+		bool bin = false;
 		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
 			RenderConfig c = cfg;
 			c.wave_paths = uint32_t( std::min<uint64_t>( wave, samples ) );
 			c.refill_min = refill;
 			c.traverse_blocks_per_sm = blocks;
 			c.shade_threads = shade;
-			ensure_wave( s, c.wave_paths, c.max_bounce, st );
+			c.bin_rays = bin;
+			ensure_wave( s, c.wave_paths, c.max_bounce, st, false, bin );
 			StageTimes warm, t;
 			render_waves( sc, c, s->wave, sum, sq, cnt, st, &warm );
 			render_waves( sc, c, s->wave, sum, sq, cnt, st, &t );
@@ -1891,6 +1898,15 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 			else
 				shade = keep;
 		}
+		// ray binning before the secondary and shadow traversals
+		{
+			bin = true;
+			double v = rate( wave, refill, blocks );
+			if ( v > best )
+				best = v;
+			else
+				bin = false;
+		}
 		for ( uint32_t w : { 1u << 20, 1u << 21, 1u << 23 } )
 		{
 			if ( w > samples && wave >= samples ) continue;
@@ -1907,8 +1923,10 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
 		cuda_check( cudaStreamSynchronize( st ), "autotune" );
 		s->tune_wave = wave, s->tune_refill = refill, s->tune_blocks = blocks, s->tune_shade = shade;
+		s->tune_bin = bin;
 		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
 		out->shade_threads = shade;
+		out->bin_rays = bin ? 1 : -1;
 		out->candidates_tried = tried;
 		out->msamples_per_s = best;
 		out->default_msamples_per_s = dflt;
@@ -1935,7 +1953,7 @@ struct cr_batch
 	uint32_t tune_shade = 128;
 	cudaGraph_t graph = nullptr;
 	cudaGraphExec_t exec = nullptr;
-	uint32_t launches_per_render = 0;
+	uint32_t graph_nodes = 0;  // kernel nodes of the graph, its loop body counted once
 
 	void drop_graph()
 	{
@@ -2218,11 +2236,29 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 		batch_check_error( b );
 		b->tune_wave = wave, b->tune_refill = refill, b->tune_blocks = blocks, b->tune_shade = shade;
 		out->shade_threads = shade;
+		out->bin_rays = -1;  // batches trace in queue order
 		b->drop_graph();
 		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
 		out->candidates_tried = tried;
 		out->msamples_per_s = best;
 		out->default_msamples_per_s = dflt;
+	} );
+}
+
+int cr_batch_set_tuning( cr_batch *b, const cr_tuning *t )
+{
+	return guarded( [&] {
+		if ( !b || !t ) fail( CR_ERR_INVALID, "null argument" );
+		if ( t->refill_min > 32 ) fail( CR_ERR_INVALID, "refill_min must be 1..32" );
+		if ( t->traverse_blocks_per_sm > 8 ) fail( CR_ERR_INVALID, "traverse_blocks_per_sm must be 1..8" );
+		if ( t->shade_threads && t->shade_threads != 64 && t->shade_threads != 128 && t->shade_threads != 256 )
+			fail( CR_ERR_INVALID, "shade_threads must be 64, 128 or 256" );
+		if ( t->wave_paths > ( 1u << 30 ) ) fail( CR_ERR_INVALID, "wave_paths above 2^30" );
+		if ( t->wave_paths ) b->tune_wave = t->wave_paths;
+		if ( t->refill_min ) b->tune_refill = t->refill_min;
+		if ( t->traverse_blocks_per_sm ) b->tune_blocks = int( t->traverse_blocks_per_sm );
+		if ( t->shade_threads ) b->tune_shade = t->shade_threads;
+		b->drop_graph();
 	} );
 }
 
@@ -2235,27 +2271,12 @@ int cr_batch_render( cr_batch *b, uint64_t seed_offset, cr_stats *stats )
 		RenderConfig c = batch_config( b, b->tune_wave, b->tune_refill, b->tune_blocks, b->total, b->tune_shade );
 		if ( !b->exec )
 		{
-			// capture the whole batch (every wave, every bounce) once
+			// one graph for the whole batch: a device-side loop over its waves
 			batch_ensure_wave( b, c.wave_paths );
 			cuda_check( cudaStreamSynchronize( st ), "batch" );
 			BatchDev bd{ b->d_scenes, b->d_jobs, b->d_seed, n };
-			cuda_check( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ), "graph capture" );
-			try
-			{
-				render_batch_waves( bd, b->jobs.data(), n, c, b->wave, st, nullptr );
-			}
-			catch ( ... )
-			{
-				cudaGraph_t g = nullptr;
-				cudaStreamEndCapture( st, &g );
-				if ( g ) cudaGraphDestroy( g );
-				throw;
-			}
-			cuda_check( cudaStreamEndCapture( st, &b->graph ), "graph capture" );
+			b->graph_nodes = build_batch_graph( bd, b->jobs.data(), n, c, b->wave, st, &b->graph );
 			cuda_check( cudaGraphInstantiate( &b->exec, b->graph, 0 ), "graph instantiate" );
-			size_t nodes = 0;
-			cuda_check( cudaGraphGetNodes( b->graph, nullptr, &nodes ), "graph" );
-			b->launches_per_render = uint32_t( nodes );
 		}
 		upload( b->d_seed, &seed_offset, sizeof( uint64_t ), st );
 		cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -2279,9 +2300,11 @@ int cr_batch_render( cr_batch *b, uint64_t seed_offset, cr_stats *stats )
 			cuda_check( cudaMemcpy( t, b->wave.tally, sizeof t, cudaMemcpyDeviceToHost ), "tally" );
 			StageTimes tm;
 			tm.total = ms, tm.rays_extend = t[ 0 ], tm.rays_shadow = t[ 1 ];
-			tm.launches = b->launches_per_render;
 			tm.waves = uint32_t( ( b->total + c.wave_paths - 1 ) / c.wave_paths );
+			// the body's kernels run once per wave, after the initialising one
+			tm.launches = 1 + tm.waves * ( b->graph_nodes - 1 );
 			fill_stats( stats, tm, b->total );
+			stats->graph_nodes = b->graph_nodes;
 		}
 		else
 			cuda_check( le, "graph launch" );

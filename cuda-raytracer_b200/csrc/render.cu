@@ -38,6 +38,9 @@ namespace
 {
 constexpr float KOISHI_EPS = 4e-3f;  // LocalVaryings::emitRay/emitSeg offset (varyings.hpp:19-37)
 
+constexpr uint32_t BIN_AXIS_BITS = 4;                           // ray binning: 16 cells per axis
+constexpr uint32_t N_BINS = 8u << ( 3 * BIN_AXIS_BITS );        // x 8 octants = 32768 bins
+
 struct WaveArgs
 {
 	uint64_t first;  // first global sample of the wave
@@ -126,6 +129,131 @@ struct ExtendIO
 	}
 	__device__ void finish( uint32_t item, const HitRec &h, bool ) const { hit[ item ] = h; }
 };
+
+// Ray binning: a counting sort of a traversal queue by (direction octant,
+// Morton code of the origin's cell in a 16^3 grid over the root node's box).
+// The persistent traversal kernel hands consecutive queue entries to the lanes
+// of a warp, so after the sort a warp traces rays that start close together
+// and head the same way: they fetch the same nodes and take the same branches.
+// Three launches (count, scan, scatter) and a memset; the order inside a bin
+// is whatever the atomics give, which changes no result (every ray's hit is
+// its own).
+__device__ __forceinline__ uint32_t ray_bin( const float3 lo, const float3 scale, const float4 o, const float4 d )
+{
+	const uint32_t oct = ( d.x < 0.f ? 1u : 0u ) | ( d.y < 0.f ? 2u : 0u ) | ( d.z < 0.f ? 4u : 0u );
+	const float lim = float( ( 1u << BIN_AXIS_BITS ) - 1u );
+	// fmaxf first: a NaN coordinate lands in cell 0
+	const uint32_t cx = uint32_t( fminf( fmaxf( ( o.x - lo.x ) * scale.x, 0.f ), lim ) );
+	const uint32_t cy = uint32_t( fminf( fmaxf( ( o.y - lo.y ) * scale.y, 0.f ), lim ) );
+	const uint32_t cz = uint32_t( fminf( fmaxf( ( o.z - lo.z ) * scale.z, 0.f ), lim ) );
+	uint32_t m = 0;
+#pragma unroll
+	for ( uint32_t k = 0; k < BIN_AXIS_BITS; ++k )
+		m |= ( ( ( cx >> k ) & 1u ) << ( 3 * k ) ) | ( ( ( cy >> k ) & 1u ) << ( 3 * k + 1 ) ) |
+			 ( ( ( cz >> k ) & 1u ) << ( 3 * k + 2 ) );
+	return ( oct << ( 3 * BIN_AXIS_BITS ) ) | m;
+}
+
+// The binning grid: the root node's box (its children's planes span
+// p .. p + 255 * 2^e per axis), cut into 16 cells per axis.
+__device__ __forceinline__ void bin_frame( const WNode *nodes, float3 &lo, float3 &scale )
+{
+	const uint4 n0 = __ldg( reinterpret_cast<const uint4 *>( nodes ) );
+	lo = f3( __uint_as_float( n0.x ), __uint_as_float( n0.y ), __uint_as_float( n0.z ) );
+	const float cells = float( 1u << BIN_AXIS_BITS );
+	scale = f3( cells / ( 255.f * __uint_as_float( ( n0.w & 0xFFu ) << 23 ) ),
+				cells / ( 255.f * __uint_as_float( ( ( n0.w >> 8 ) & 0xFFu ) << 23 ) ),
+				cells / ( 255.f * __uint_as_float( ( ( n0.w >> 16 ) & 0xFFu ) << 23 ) ) );
+}
+
+__global__ void __launch_bounds__( 256 ) k_bin_count( const uint32_t *__restrict__ queue, const uint32_t *n_ptr,
+													  const float4 *__restrict__ ray_o, const float4 *__restrict__ ray_d,
+													  const WNode *nodes, uint32_t *__restrict__ bins )
+{
+	const uint32_t n = *n_ptr, lane = lane_id();
+	float3 lo, scale;
+	bin_frame( nodes, lo, scale );
+	// the block strides together, so every lane of a warp reaches the match
+	for ( uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x )
+	{
+		const uint32_t i = base + threadIdx.x;
+		uint32_t key = ~0u;
+		if ( i < n )
+		{
+			const uint32_t item = queue[ i ];
+			key = ray_bin( lo, scale, ray_o[ item ], ray_d[ item ] );
+		}
+		const uint32_t peers = __match_any_sync( ~0u, key );
+		if ( i < n && lane == uint32_t( __ffs( peers ) - 1 ) ) atomicAdd( bins + key, uint32_t( __popc( peers ) ) );
+	}
+}
+
+// Counts -> exclusive offsets, in place: one block of 1024 threads, N_BINS / 1024 bins each.
+__global__ void __launch_bounds__( 1024 ) k_bin_scan( uint32_t *bins )
+{
+	constexpr uint32_t PER = N_BINS / 1024;
+	__shared__ uint32_t warp_sum[ 32 ];
+	const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+	uint32_t v[ PER ], s = 0;
+#pragma unroll
+	for ( uint32_t k = 0; k < PER; ++k ) v[ k ] = bins[ t * PER + k ], s += v[ k ];
+	uint32_t x = s;  // inclusive scan of the threads' sums within the warp
+#pragma unroll
+	for ( int o = 1; o < 32; o <<= 1 )
+	{
+		const uint32_t y = __shfl_up_sync( ~0u, x, o );
+		if ( lane >= uint32_t( o ) ) x += y;
+	}
+	if ( lane == 31 ) warp_sum[ warp ] = x;
+	__syncthreads();
+	if ( warp == 0 )
+	{
+		uint32_t w = warp_sum[ lane ];
+#pragma unroll
+		for ( int o = 1; o < 32; o <<= 1 )
+		{
+			const uint32_t y = __shfl_up_sync( ~0u, w, o );
+			if ( lane >= uint32_t( o ) ) w += y;
+		}
+		warp_sum[ lane ] = w;
+	}
+	__syncthreads();
+	uint32_t run = x - s + ( warp ? warp_sum[ warp - 1 ] : 0u );
+#pragma unroll
+	for ( uint32_t k = 0; k < PER; ++k ) bins[ t * PER + k ] = run, run += v[ k ];
+}
+
+__global__ void __launch_bounds__( 256 ) k_bin_scatter( const uint32_t *__restrict__ queue, const uint32_t *n_ptr,
+														const float4 *__restrict__ ray_o, const float4 *__restrict__ ray_d,
+														const WNode *nodes, uint32_t *__restrict__ bins,
+														uint32_t *__restrict__ out, uint32_t *err )
+{
+	const uint32_t n = *n_ptr, lane = lane_id();
+	float3 lo, scale;
+	bin_frame( nodes, lo, scale );
+	for ( uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x )
+	{
+		const uint32_t i = base + threadIdx.x;
+		uint32_t key = ~0u, item = 0;
+		if ( i < n )
+		{
+			item = queue[ i ];
+			key = ray_bin( lo, scale, ray_o[ item ], ray_d[ item ] );
+		}
+		const uint32_t peers = __match_any_sync( ~0u, key );
+		const uint32_t leader = __ffs( peers ) - 1;
+		uint32_t pos = 0;
+		if ( i < n && lane == leader ) pos = atomicAdd( bins + key, uint32_t( __popc( peers ) ) );
+		pos = __shfl_sync( ~0u, pos, leader ) + __popc( peers & ( ( 1u << lane ) - 1u ) );
+		if ( i < n )
+		{
+			if ( pos < n )
+				out[ pos ] = item;
+			else
+				atomicOr( err, 16u );
+		}
+	}
+}
 
 // Shadow queue of one bounce: an unoccluded ray adds its contribution.
 struct ShadowIO
@@ -741,8 +869,9 @@ __device__ __forceinline__ uint32_t find_job( const BatchJobDev *jobs, uint32_t 
 }
 
 // Camera rays of a batched wave: global sample -> job -> pixel and sample index.
-__global__ void k_generate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa )
+__global__ void k_generate_batch( BatchDev bd, WaveBuffers wb )
 {
+	const WaveArgs wa{ wb.bwave->first, wb.bwave->n };
 	if ( blockIdx.x == 0 && threadIdx.x == 0 ) wb.counters[ CNT_EXT ] = wa.n;
 	for ( uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < wa.n; s += gridDim.x * blockDim.x )
 	{
@@ -773,6 +902,7 @@ template <bool BATCH, int EST, bool PROF = false>
 __global__ void __launch_bounds__( 256 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
 												  uint32_t bounce, uint2 key, BatchDev bd )
 {
+	if constexpr ( BATCH ) wa = WaveArgs{ wb.bwave->first, wb.bwave->n };  // the wave runs from device memory
 	const uint32_t n = wb.counters[ CPB * bounce + CNT_EXT ];
 	const uint32_t *q = wb.queue[ bounce & 1 ];
 	uint32_t *nq = wb.queue[ ( bounce + 1 ) & 1 ];
@@ -1033,9 +1163,11 @@ __global__ void __launch_bounds__( 128 ) k_aov( DevScene sc, RenderConfig cfg, W
 
 // Film accumulation of a batched wave: global pixels p0..p1 (those whose
 // samples meet the wave), each into its job's film.
-__global__ void k_accumulate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa, uint64_t p0, uint64_t p1 )
+__global__ void k_accumulate_batch( BatchDev bd, WaveBuffers wb )
 {
-	for ( uint64_t p = p0 + blockIdx.x * blockDim.x + threadIdx.x; p <= p1; p += gridDim.x * blockDim.x )
+	const BatchWave w = *wb.bwave;
+	const WaveArgs wa{ w.first, w.n };
+	for ( uint64_t p = w.p0 + blockIdx.x * blockDim.x + threadIdx.x; p <= w.p1 && w.n; p += gridDim.x * blockDim.x )
 	{
 		const uint32_t j = find_job<true>( bd.jobs, bd.n_jobs, p );
 		const BatchJobDev &job = bd.jobs[ j ];
@@ -1058,14 +1190,54 @@ __global__ void k_accumulate_batch( BatchDev bd, WaveBuffers wb, WaveArgs wa, ui
 	}
 }
 
-// Adds one wave's queue lengths to the running ray tally (batched renders,
-// which keep no host round trip per wave).
-__global__ void k_tally( const uint32_t *counters, uint32_t max_bounce, unsigned long long *tally )
+// Global pixel of global sample g of a batch.
+__device__ __forceinline__ uint64_t batch_pixel( const BatchDev &bd, uint64_t g )
 {
-	if ( threadIdx.x != 0 || blockIdx.x != 0 ) return;
+	const BatchJobDev &job = bd.jobs[ find_job<false>( bd.jobs, bd.n_jobs, g ) ];
+	return job.first_pixel + ( g - job.first_sample ) / job.spp;
+}
+
+// Before the first wave of a batched render: wave 0, ray tally cleared.
+__global__ void k_batch_init( WaveBuffers wb )
+{
+	if ( threadIdx.x || blockIdx.x ) return;
+	wb.bwave->index = 0;
+	wb.tally[ 0 ] = wb.tally[ 1 ] = 0;
+}
+
+// Start of a batched wave: its samples and pixel range from its index, and
+// cleared queue counters.  One block.
+__global__ void k_batch_wave_begin( BatchDev bd, WaveBuffers wb, uint64_t total, uint32_t wave_paths )
+{
+	for ( uint32_t i = threadIdx.x; i < wb.n_counters; i += blockDim.x ) wb.counters[ i ] = 0;
+	if ( threadIdx.x ) return;
+	BatchWave &w = *wb.bwave;
+	const uint64_t first = uint64_t( w.index ) * wave_paths;
+	w.first = first;
+	if ( first >= total )  // no wave this far (the loop stops before it)
+	{
+		w.n = 0, w.p0 = 1, w.p1 = 0;
+		return;
+	}
+	w.n = total - first < wave_paths ? uint32_t( total - first ) : wave_paths;
+	w.p0 = batch_pixel( bd, first );
+	w.p1 = batch_pixel( bd, first + w.n - 1 );
+}
+
+// End of a batched wave: adds its queue lengths to the running ray tally,
+// advances the wave index and, in the graph, runs the loop again while waves
+// remain.
+__global__ void k_batch_wave_end( WaveBuffers wb, uint32_t max_bounce, uint64_t total, uint32_t wave_paths,
+								  cudaGraphConditionalHandle loop, int looped )
+{
+	if ( threadIdx.x || blockIdx.x ) return;
 	unsigned long long e = 0, sh = 0;
-	for ( uint32_t b = 0; b <= max_bounce; ++b ) e += counters[ CPB * b + CNT_EXT ], sh += counters[ CPB * b + CNT_SHADOW ];
-	tally[ 0 ] += e, tally[ 1 ] += sh;
+	for ( uint32_t b = 0; b <= max_bounce; ++b )
+		e += wb.counters[ CPB * b + CNT_EXT ], sh += wb.counters[ CPB * b + CNT_SHADOW ];
+	wb.tally[ 0 ] += e, wb.tally[ 1 ] += sh;
+	const uint32_t next = wb.bwave->index + 1;
+	wb.bwave->index = next;
+	if ( looped ) cudaGraphSetConditional( loop, uint64_t( next ) * wave_paths < total ? 1u : 0u );
 }
 
 // Single-node shader kernels behind cr_bsdf_eval / cr_bsdf_sample (the host
@@ -1237,10 +1409,27 @@ void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaSt
 void free_wave( WaveBuffers &wb, cudaStream_t st )
 {
 	void *ps[] = { wb.ray_o, wb.ray_d, wb.hit, wb.beta, wb.L, wb.queue[ 0 ], wb.queue[ 1 ], wb.shadow_queue,
-				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work, wb.lobes, wb.path_job, wb.tally };
+				   wb.sh_o, wb.sh_d, wb.sh_c, wb.counters, wb.err, wb.work, wb.lobes, wb.path_job, wb.tally,
+				   wb.binned, wb.bins, wb.bwave };
 	for ( void *p : ps )
 		if ( p ) cudaFreeAsync( p, st );
 	wb = WaveBuffers();
+}
+
+// Sort queue[0 .. *n) into wb.binned (the launches of one traversal stage).
+void bin_queue( const DevScene &sc, const WaveBuffers &wb, const uint32_t *queue, const uint32_t *n,
+				const float4 *ray_o, const float4 *ray_d, int grid, cudaStream_t st )
+{
+	check( cudaMemsetAsync( wb.bins, 0, sizeof( uint32_t ) * N_BINS, st ), "memset" );
+	k_bin_count<<<grid, 256, 0, st>>>( queue, n, ray_o, ray_d, sc.nodes, wb.bins );
+	k_bin_scan<<<1, 1024, 0, st>>>( wb.bins );
+	k_bin_scatter<<<grid, 256, 0, st>>>( queue, n, ray_o, ray_d, sc.nodes, wb.bins, wb.binned, wb.err );
+}
+
+void alloc_bins( WaveBuffers &wb, cudaStream_t st )
+{
+	if ( !wb.binned ) alloc( wb.binned, wb.capacity, st );
+	if ( !wb.bins ) alloc( wb.bins, N_BINS, st );
 }
 
 void alloc_lobes( WaveBuffers &wb, cudaStream_t st )
@@ -1253,22 +1442,85 @@ void alloc_batch_state( WaveBuffers &wb, cudaStream_t st )
 {
 	if ( !wb.path_job ) alloc( wb.path_job, wb.capacity, st );
 	if ( !wb.tally ) alloc( wb.tally, 2, st );
+	if ( !wb.bwave ) alloc( wb.bwave, 1, st );
 }
 
-void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
-						 WaveBuffers &wb, cudaStream_t st, StageTimes *times )
+namespace
 {
-	if ( n_jobs == 0 ) return;
-	if ( !wb.path_job || !wb.tally ) throw std::runtime_error( "batched render without its wave state" );
+// Samples of a batch: the last job's end.
+uint64_t batch_total( const BatchJobDev *jobs, uint32_t n_jobs )
+{
+	const BatchJobDev &last = jobs[ n_jobs - 1 ];
+	return last.first_sample + uint64_t( last.width ) * last.height * last.spp;
+}
+
+void check_batch_state( uint32_t n_jobs, const RenderConfig &cfg, const WaveBuffers &wb )
+{
+	if ( n_jobs == 0 ) throw std::runtime_error( "batched render without jobs" );
+	if ( !wb.path_job || !wb.tally || !wb.bwave ) throw std::runtime_error( "batched render without its wave state" );
 	if ( cfg.wave_paths == 0 || cfg.wave_paths > wb.capacity )
 		throw std::runtime_error( "wave size exceeds the allocated wave buffers" );
-	const BatchJobDev &last = jobs[ n_jobs - 1 ];
-	const uint64_t total = last.first_sample + uint64_t( last.width ) * last.height * last.spp;
-	const uint32_t P = cfg.wave_paths;
+}
+
+// One wave of a batched render, every kernel reading the wave from
+// wb.bwave: begin (wave bounds, counters), generation, max_bounce + 1 x
+// (closest hit, shading, shadow rays), accumulation, end (tally, next wave
+// and, when `looped`, the graph loop's condition).  timed(kind, launch) wraps
+// each stage.
+template <class Timed>
+void batch_wave_kernels( const BatchDev &bd, const RenderConfig &cfg, WaveBuffers &wb, uint64_t total, cudaStream_t st,
+						 Timed &&timed, cudaGraphConditionalHandle loop, bool looped )
+{
 	const int sms = sm_count();
 	const int g_ext = sms * std::max( 1, std::min( 8, cfg.traverse_blocks_per_sm ) );
 	const uint32_t shade_t = cfg.shade_threads == 64 || cfg.shade_threads == 256 ? cfg.shade_threads : 128u;
 	const int g_shade_k = int( uint32_t( sms ) * 1024u / shade_t );  // k_shade: SMs x 1024 threads
+	const int g_wide = sms * 16;                                      // generation and accumulation
+	const uint32_t P = cfg.wave_paths;
+	timed( 3, [&] {
+		k_batch_wave_begin<<<1, 256, 0, st>>>( bd, wb, total, P );
+		k_generate_batch<<<g_wide, 256, 0, st>>>( bd, wb );
+	} );
+	for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
+	{
+		timed( 0, [&] {
+			BatchExtendIO io;
+			io.queue = wb.queue[ b & 1 ], io.ray_o = wb.ray_o, io.ray_d = wb.ray_d, io.hit = wb.hit;
+			io.scenes = bd.scenes, io.path_job = wb.path_job;
+			const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
+			uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
+			k_traverse<BatchExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
+																						  wb.work, cfg.refill_min );
+		} );
+		timed( 2, [&] {
+			if ( cfg.estimator == EST_MIS )
+				k_shade<true, EST_MIS><<<g_shade_k, shade_t, 0, st>>>( DevScene{}, cfg, wb, WaveArgs{}, b, uint2{}, bd );
+			else
+				k_shade<true, EST_KOISHI><<<g_shade_k, shade_t, 0, st>>>( DevScene{}, cfg, wb, WaveArgs{}, b, uint2{}, bd );
+		} );
+		timed( 1, [&] {
+			BatchShadowIO io;
+			io.queue = wb.shadow_queue, io.ray_o = wb.sh_o, io.ray_d = wb.sh_d, io.contrib = wb.sh_c, io.L = wb.L;
+			io.scenes = bd.scenes, io.path_job = wb.path_job;
+			const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
+			uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
+			k_traverse<BatchShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
+																						 wb.work + 2, cfg.refill_min );
+		} );
+	}
+	timed( 3, [&] {
+		k_accumulate_batch<<<g_wide, 256, 0, st>>>( bd, wb );
+		k_batch_wave_end<<<1, 32, 0, st>>>( wb, cfg.max_bounce, total, P, loop, looped ? 1 : 0 );
+	} );
+	check( cudaGetLastError(), "batched render launch" );
+}
+}  // namespace
+
+void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
+						 WaveBuffers &wb, cudaStream_t st, StageTimes *times )
+{
+	check_batch_state( n_jobs, cfg, wb );
+	const uint64_t total = batch_total( jobs, n_jobs );
 	EventPool pool;
 	struct Mark
 	{
@@ -1297,59 +1549,10 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 		if ( kind == 0 ) times->extend_launches++;
 		if ( kind == 1 ) times->shadow_launches++;
 	};
-	// global pixel of a global sample (host copy of the job table)
-	auto pixel_of = [&]( uint64_t g ) {
-		uint32_t lo = 0, hi = n_jobs;
-		while ( hi - lo > 1 )
-		{
-			uint32_t mid = ( lo + hi ) >> 1;
-			( jobs[ mid ].first_sample <= g ? lo : hi ) = mid;
-		}
-		return jobs[ lo ].first_pixel + ( g - jobs[ lo ].first_sample ) / jobs[ lo ].spp;
-	};
-	check( cudaMemsetAsync( wb.tally, 0, 2 * sizeof( unsigned long long ), st ), "memset" );
-	for ( uint64_t first = 0; first < total; first += P )
+	k_batch_init<<<1, 32, 0, st>>>( wb );
+	for ( uint64_t first = 0; first < total; first += cfg.wave_paths )
 	{
-		WaveArgs wa{ first, uint32_t( std::min<uint64_t>( P, total - first ) ) };
-		check( cudaMemsetAsync( wb.counters, 0, sizeof( uint32_t ) * wb.n_counters, st ), "memset" );
-		timed( 3, [&] {
-			int gg = int( std::min<uint64_t>( ( wa.n + 255 ) / 256, uint64_t( sms ) * 16 ) );
-			k_generate_batch<<<gg, 256, 0, st>>>( bd, wb, wa );
-		} );
-		for ( uint32_t b = 0; b <= cfg.max_bounce; ++b )
-		{
-			timed( 0, [&] {
-				BatchExtendIO io;
-				io.queue = wb.queue[ b & 1 ], io.ray_o = wb.ray_o, io.ray_d = wb.ray_d, io.hit = wb.hit;
-				io.scenes = bd.scenes, io.path_job = wb.path_job;
-				const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
-				uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
-				k_traverse<BatchExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err, wb.work,
-																			   cfg.refill_min );
-			} );
-			timed( 2, [&] {
-				if ( cfg.estimator == EST_MIS )
-					k_shade<true, EST_MIS><<<g_shade_k, shade_t, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
-				else
-					k_shade<true, EST_KOISHI><<<g_shade_k, shade_t, 0, st>>>( DevScene{}, cfg, wb, wa, b, uint2{}, bd );
-			} );
-			timed( 1, [&] {
-				BatchShadowIO io;
-				io.queue = wb.shadow_queue, io.ray_o = wb.sh_o, io.ray_d = wb.sh_d, io.contrib = wb.sh_c, io.L = wb.L;
-				io.scenes = bd.scenes, io.path_job = wb.path_job;
-				const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
-				uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
-				k_traverse<BatchShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
-																			  wb.work + 2, cfg.refill_min );
-			} );
-		}
-		timed( 3, [&] {
-			const uint64_t p0 = pixel_of( first ), p1 = pixel_of( first + wa.n - 1 );
-			int gg = int( std::min<uint64_t>( ( p1 - p0 + 256 ) / 256, uint64_t( sms ) * 16 ) );
-			k_accumulate_batch<<<gg, 256, 0, st>>>( bd, wb, wa, p0, p1 );
-			k_tally<<<1, 32, 0, st>>>( wb.counters, cfg.max_bounce, wb.tally );
-		} );
-		check( cudaGetLastError(), "batched render launch" );
+		batch_wave_kernels( bd, cfg, wb, total, st, timed, cudaGraphConditionalHandle{}, false );
 		if ( times ) times->waves++;
 	}
 	if ( times )
@@ -1367,6 +1570,64 @@ void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n
 		unsigned long long t[ 2 ];
 		check( cudaMemcpy( t, wb.tally, sizeof t, cudaMemcpyDeviceToHost ), "tally" );
 		times->rays_extend += t[ 0 ], times->rays_shadow += t[ 1 ];
+	}
+}
+
+
+uint32_t build_batch_graph( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
+							WaveBuffers &wb, cudaStream_t st, cudaGraph_t *out )
+{
+	check_batch_state( n_jobs, cfg, wb );
+	const uint64_t total = batch_total( jobs, n_jobs );
+	cudaGraph_t g = nullptr;
+	check( cudaGraphCreate( &g, 0 ), "graph" );
+	// a capture that fails part-way is ended before the error propagates
+	auto captured = [&]( cudaGraph_t into, auto &&launch ) {
+		check( cudaStreamBeginCaptureToGraph( st, into, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal ),
+			   "graph capture" );
+		try
+		{
+			launch();
+		}
+		catch ( ... )
+		{
+			cudaStreamEndCapture( st, &into );
+			throw;
+		}
+		check( cudaStreamEndCapture( st, &into ), "graph capture" );
+	};
+	try
+	{
+		captured( g, [&] {
+			k_batch_init<<<1, 32, 0, st>>>( wb );
+			check( cudaGetLastError(), "batched render launch" );
+		} );
+		cudaGraphNode_t init = nullptr;
+		size_t n_init = 1;
+		check( cudaGraphGetNodes( g, &init, &n_init ), "graph" );
+		if ( n_init != 1 ) throw std::runtime_error( "batch graph: unexpected initial nodes" );
+		// the loop runs at least once (a batch has samples); its body decides whether to go on
+		cudaGraphConditionalHandle loop{};
+		check( cudaGraphConditionalHandleCreate( &loop, g, 1u, cudaGraphCondAssignDefault ), "graph conditional" );
+		cudaGraphNodeParams cp{};
+		cp.type = cudaGraphNodeTypeConditional;
+		cp.conditional.handle = loop;
+		cp.conditional.type = cudaGraphCondTypeWhile;
+		cp.conditional.size = 1;
+		cudaGraphNode_t cond = nullptr;
+		check( cudaGraphAddNode( &cond, g, &init, 1, &cp ), "graph conditional" );
+		cudaGraph_t body = cp.conditional.phGraph_out[ 0 ];
+		auto direct = []( int, auto &&launch ) { launch(); };
+		captured( body, [&] { batch_wave_kernels( bd, cfg, wb, total, st, direct, loop, true ); } );
+		size_t n_body = 0;
+		check( cudaGraphGetNodes( body, nullptr, &n_body ), "graph" );
+		*out = g;
+		return uint32_t( 1 + n_body );
+	}
+	catch ( ... )
+	{
+		cudaGraphDestroy( g );
+		throw;
 	}
 }
 
@@ -1388,6 +1649,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 	const uint32_t shade_t = cfg.shade_threads == 64 || cfg.shade_threads == 256 ? cfg.shade_threads : 128u;
 	const int g_shade_k = int( uint32_t( sms ) * 1024u / shade_t );  // k_shade: SMs x 1024 threads
 	const uint2 key = make_uint2( uint32_t( cfg.seed ), uint32_t( cfg.seed >> 32 ) ^ 0x5EED5EEDu );
+	const bool binning = cfg.bin_rays && wb.binned && wb.bins && sc.n_nodes > 0;
 	EventPool pool;
 	struct Mark
 	{
@@ -1442,7 +1704,10 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		if ( training )
 		{
 			batch = std::min( guide->train_paths, wa.n );
-			wc.rec_paths = uint32_t( std::min<uint64_t>( uint64_t( batch ) * guide->steps_per_wave, wa.n ) );
+			// steps this wave: steps_per_wave, or what is left of the budget
+			uint32_t take = guide->steps_per_wave;
+			if ( guide->max_steps ) take = std::min( take, guide->max_steps - guide->step );
+			wc.rec_paths = uint32_t( std::min<uint64_t>( uint64_t( batch ) * take, wa.n ) );
 			steps = ( wc.rec_paths + batch - 1 ) / batch;
 			wc.rec_stride = wa.n / wc.rec_paths;
 			wc.rec_offset = uint32_t( ( guide->waves++ * 2654435761ull ) % wc.rec_stride );
@@ -1459,6 +1724,12 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				ExtendIO io{ wb.queue[ b & 1 ], wb.ray_o, wb.ray_d, wb.hit };
 				const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
 				uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
+				// camera rays are coherent in pixel order already
+				if ( binning && b > 0 )
+				{
+					bin_queue( sc, wb, io.queue, n, wb.ray_o, wb.ray_d, g_shade, st );
+					io.queue = wb.binned;
+				}
 				if ( cfg.count_work )
 					k_traverse<ExtendIO, false, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
 				else
@@ -1484,6 +1755,11 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 					ShadowIO io{ wb.shadow_queue, wb.sh_o, wb.sh_d, wb.sh_c, wb.L };
 					const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
 					uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
+					if ( binning )
+					{
+						bin_queue( sc, wb, io.queue, n, wb.sh_o, wb.sh_d, g_shade, st );
+						io.queue = wb.binned;
+					}
 					if ( cfg.count_work )
 						k_traverse<ShadowIO, true, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
 					else

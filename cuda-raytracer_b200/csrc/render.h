@@ -10,6 +10,8 @@
 namespace cr
 {
 // Per-path SoA state of one wave, sized for `capacity` paths.
+struct BatchWave;
+
 struct WaveBuffers
 {
 	uint32_t capacity = 0;
@@ -28,6 +30,9 @@ struct WaveBuffers
 	                                            // FP16, and the guide's selection probability: 6 x 16 bytes per path
 	uint32_t *path_job = nullptr;               // batched renders: the job (scene render) of each path
 	unsigned long long *tally = nullptr;        // batched renders: closest-hit and shadow rays traced
+	uint32_t *binned = nullptr;                 // ray binning: the sorted queue of one traversal launch
+	uint32_t *bins = nullptr;                   // ray binning: per-bin counts, then offsets (N_BINS)
+	BatchWave *bwave = nullptr;                 // batched renders: the current wave
 };
 
 // One scene's render inside a batch (device copy).  A job renders its whole
@@ -40,6 +45,16 @@ struct BatchJobDev
 	uint64_t seed;
 	double *sum, *sumsq;
 	uint32_t *count;
+};
+
+// The current wave of a batched render, in device memory: the kernels of a
+// wave read it, so that one captured wave body serves every wave.
+struct BatchWave
+{
+	uint64_t first;   // first global sample of the wave
+	uint64_t p0, p1;  // first and last global pixel of the wave's samples (p0 > p1: none)
+	uint32_t n;       // samples in the wave
+	uint32_t index;   // wave number
 };
 
 struct BatchDev
@@ -94,6 +109,7 @@ struct RenderConfig
 	int traverse_blocks_per_sm = 8;  // traversal grid = SMs x this (1..8; 128-thread blocks)
 	uint32_t shade_threads = 128;    // shading block size (64, 128 or 256); grid of SMs x 1024 threads
 	uint32_t rr_start = 4;           // MIS estimator: first bounce at which Russian roulette may end a path
+	bool bin_rays = false;           // sort secondary and shadow queues by (octant, origin cell) before tracing
 	ProfileDev prof{};               // profiled renders (reference estimator, Radiance kernel)
 };
 
@@ -114,16 +130,25 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				   double *film_sumsq, uint32_t *film_count, cudaStream_t st, StageTimes *times,
 				   GuideState *guide = nullptr );
 void alloc_lobes( WaveBuffers &wb, cudaStream_t st );
+void alloc_bins( WaveBuffers &wb, cudaStream_t st );  // ray binning buffers (RenderConfig::bin_rays)
 void alloc_batch_state( WaveBuffers &wb, cudaStream_t st );
 
 // Batched render of many scenes: the waves run over the concatenated samples
 // of all jobs, so one launch per stage serves every scene.  `jobs` is the host
-// copy of the device job table.  cfg carries the launch configuration, the
-// estimator and max_bounce (window and spp fields are unused).  With `times`
-// null the call issues kernels and memsets only (no synchronisation), so it
-// can be captured into a CUDA graph.
+// copy of the device table.  cfg carries the launch configuration, the
+// estimator and max_bounce (window and spp fields are unused).  The host
+// issues every wave's kernels; `times` (when not null) gets the stage times.
 void render_batch_waves( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
 						 WaveBuffers &wb, cudaStream_t st, StageTimes *times );
+
+// The same render as one CUDA graph: an initialising kernel, then a
+// conditional WHILE node whose body is one wave's kernels (the wave's index
+// lives in device memory; the body's last kernel advances it and ends the loop
+// after the last wave).  The graph is built with stream captures on `st`
+// (which must not be capturing).  Returns the kernel nodes of the graph, the
+// body counted once.
+uint32_t build_batch_graph( const BatchDev &bd, const BatchJobDev *jobs, uint32_t n_jobs, const RenderConfig &cfg,
+							WaveBuffers &wb, cudaStream_t st, cudaGraph_t *out );
 
 void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit,
 				   cr_hit *out, uint32_t *err, cudaStream_t st );

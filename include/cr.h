@@ -64,6 +64,9 @@ typedef struct cr_render_desc {
                                 end a path; 0 = the default: 4 (the reference's "after
                                 bounce 3", which the reference estimator always uses) for
                                 plain renders, none for guided renders; above max_bounce: none */
+    int32_t bin_rays;        /* 1: sort each secondary and shadow traversal queue by (ray
+                                octant, origin cell) before tracing; -1: trace in queue
+                                order; 0 = tuned (off until cr_autotune picks it) */
 } cr_render_desc;
 
 /* Launch configuration chosen by cr_autotune (also used by later renders of
@@ -76,6 +79,7 @@ typedef struct cr_tuning {
     double msamples_per_s;   /* rate of the chosen configuration on the sample render */
     double default_msamples_per_s; /* rate of the built-in defaults on the same sample */
     uint32_t shade_threads;  /* shading block size */
+    int32_t bin_rays;        /* 1: ray binning chosen, -1: not */
 } cr_tuning;
 
 typedef struct cr_stats {
@@ -97,6 +101,9 @@ typedef struct cr_stats {
     uint32_t extend_launches;
     uint32_t shadow_launches;
     double ms_guide_train; /* guide training steps (part of ms_guide)         */
+    uint32_t graph_nodes;  /* cr_batch_render: kernel nodes of the replayed CUDA graph
+                              (an initialising kernel and the wave loop's body, which
+                              runs once per wave); 0 for other calls            */
 } cr_stats;
 
 /* ------------------------------------------------------------------ errors */
@@ -353,10 +360,14 @@ int cr_measure_gather(void *stream, uint32_t record_bytes, uint64_t array_bytes,
  * A batch renders many committed scenes, each at its own resolution and spp,
  * in shared waves: the paths of all jobs are concatenated, so one persistent
  * traversal launch per bounce serves every scene and small images do not
- * leave the GPU idle.  The first cr_batch_render captures the batch's whole
- * kernel sequence into a CUDA graph on the batch's stream; later calls
- * replay it.  Jobs render their whole image; estimator and max_bounce are
- * shared; learned guiding is not used in batches. */
+ * leave the GPU idle.  The first cr_batch_render builds one CUDA graph on
+ * the batch's stream: an initialising kernel and a conditional WHILE node
+ * whose body is one wave's kernels (generation, max_bounce + 1 x closest
+ * hit, shading and shadow rays, accumulation); the wave index lives in
+ * device memory and the body's last kernel ends the loop after the last
+ * wave.  Later calls replay the graph.  Jobs render their whole image;
+ * estimator and max_bounce are shared; learned guiding is not used in
+ * batches. */
 typedef struct cr_batch cr_batch;
 typedef struct cr_batch_job {
     cr_scene *scene;         /* committed scene (may appear in several jobs) */
@@ -377,6 +388,11 @@ int cr_batch_create(const cr_batch_job *jobs, uint32_t n_jobs, uint32_t max_boun
  * candidate; the choice is kept (the next render captures a new graph).
  * Synchronises; allocates temporary films. */
 int cr_batch_autotune(cr_batch *b, cr_tuning *out);
+/* Sets the batch's launch configuration from `t` (wave_paths, refill_min,
+ * traverse_blocks_per_sm, shade_threads; a zero field keeps the current
+ * value), e.g. a tuning kept from an earlier run.  The next render builds a
+ * new graph. */
+int cr_batch_set_tuning(cr_batch *b, const cr_tuning *t);
 /* One render of every job into its film, job seeds offset by seed_offset.
  * With stats NULL the call only enqueues the graph (asynchronous); with
  * stats it waits, checks the device error word and fills the totals and the

@@ -240,10 +240,8 @@ def gradients(grid, W, b, bmin, binv, records, learn_select=False):
 # and k_guide_train_tc): the same arithmetic in FP64 with the operands rounded
 # to BF16 (round to nearest even) where the kernels round them: the encoding and
 # the hidden activations, the weights, and the output gradient of every layer as
-# it enters the two backward products.  The tensor-core passes read the hash
-# table from its paired FP16 copy, so the grid is rounded to FP16 (round to
-# nearest even, from its FP32 master values) before the encoding.  Biases,
-# accumulations, bias gradients and the ReLU masks stay unrounded.
+# it enters the two backward products.  Biases, accumulations, bias gradients and
+# the ReLU masks stay unrounded.
 
 def bf16(a):
     """Round to the nearest BF16 value (ties to even), returned as float64."""
@@ -251,11 +249,6 @@ def bf16(a):
     u = f.view(np.uint32).astype(np.uint64)
     u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
-
-
-def fp16(a):
-    """Round FP32 values to the nearest FP16 value (ties to even), as float64."""
-    return np.asarray(a, np.float64).astype(np.float32).astype(np.float16).astype(np.float64)
 
 
 def forward_bf16(W, b, h0):
@@ -275,12 +268,11 @@ def gradients_bf16(grid, W, b, bmin, binv, records, learn_select=False):
     """Gradients of `loss` as the tensor-core training pass forms them."""
     gW, gb, ggrid = np.zeros_like(W), np.zeros_like(b), np.zeros_like(grid)
     Wb = bf16(W)
-    grid16 = fp16(grid)
     tot = sum(r[12] for r in records if r[12] > 0)
     for r in records:
         if r[12] <= 0:
             continue
-        h0, cs = encode(grid16, bmin, binv, r[0:3], r[3:6], r[6:9])
+        h0, cs = encode(grid, bmin, binv, r[0:3], r[3:6], r[6:9])
         o, hs = forward_bf16(W, b, h0)
         dz = out_grad(o, r, r[12] / tot, learn_select)
         for l in range(LAYERS - 1, -1, -1):

@@ -82,6 +82,43 @@ def test_batch_graph_replays_accumulate(cr, batch_scenes):
     b.close()
 
 
+@pytest.mark.parametrize("wave", [1000, 4099])
+def test_batch_graph_loops_over_many_waves(cr, batch_scenes, wave):
+    """Small waves: the graph's device-side loop runs many times (waves that
+    cut jobs and pixels at odd places), with the same films as stand-alone
+    renders, and the graph holds one wave's kernels, not every wave's."""
+    import torch
+    films = [_films(torch, j[1], j[2]) for j in batch_scenes]
+    jobs = [(j[0], j[1], j[2], j[3], j[4], f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr())
+            for j, f in zip(batch_scenes, films)]
+    b = cr.Batch(jobs, max_bounce=7, estimator=1, stream=torch.cuda.current_stream().cuda_stream)
+    b.set_tuning(wave_paths=wave)
+    st = b.render(0)
+    total = sum(j[1] * j[2] * j[3] for j in batch_scenes)
+    assert st.samples == total and st.waves == -(-total // wave) and st.waves > 10
+    assert st.graph_nodes == 1 + 4 + 3 * 8  # init; begin, generate, 8 x 3 stages, accumulate, end
+    assert st.launches == 1 + st.waves * (st.graph_nodes - 1)
+    assert st.rays_extend >= total
+    for job, f in zip(batch_scenes, films):
+        _assert_same(f, _single(cr, torch, job, 1))
+    # a replay adds the next seed's samples
+    b.render(1, stats=False)
+    for job, f in zip(batch_scenes, films):
+        ref = _single(cr, torch, job, 1)
+        _assert_same(f, _single(cr, torch, job, 1, seed_add=1, acc=ref))
+    b.close()
+
+
+def test_batch_set_tuning_validates(cr, batch_scenes):
+    import torch
+    f = _films(torch, 8, 8)
+    b = cr.Batch([(batch_scenes[0][0], 8, 8, 1, 1, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr())])
+    for bad in ({"refill_min": 33}, {"traverse_blocks_per_sm": 9}, {"shade_threads": 96}):
+        with pytest.raises(cr.CrError):
+            b.set_tuning(**bad)
+    b.close()
+
+
 def test_batch_autotune_keeps_results(cr, batch_scenes):
     """The autotuned launch configuration changes the waves, not the film."""
     import torch
