@@ -38,8 +38,8 @@ namespace
 {
 constexpr float KOISHI_EPS = 4e-3f;  // LocalVaryings::emitRay/emitSeg offset (varyings.hpp:19-37)
 
-constexpr uint32_t BIN_AXIS_BITS = 4;                           // ray binning: 16 cells per axis
-constexpr uint32_t N_BINS = 8u << ( 3 * BIN_AXIS_BITS );        // x 8 octants = 32768 bins
+constexpr uint32_t BIN_AXIS_BITS = 3;                           // ray binning: 8 cells per axis
+constexpr uint32_t N_BINS = 8u << ( 3 * BIN_AXIS_BITS );        // x 8 octants = 4096 bins
 
 struct WaveArgs
 {
@@ -131,13 +131,17 @@ struct ExtendIO
 };
 
 // Ray binning: a counting sort of a traversal queue by (direction octant,
-// Morton code of the origin's cell in a 16^3 grid over the root node's box).
+// Morton code of the origin's cell in an 8^3 grid over the root node's box).
 // The persistent traversal kernel hands consecutive queue entries to the lanes
 // of a warp, so after the sort a warp traces rays that start close together
 // and head the same way: they fetch the same nodes and take the same branches.
-// Three launches (count, scan, scatter) and a memset; the order inside a bin
-// is whatever the atomics give, which changes no result (every ray's hit is
-// its own).
+// A memset and three launches: count (per-block shared-memory histograms added
+// to the global one), scan (counts to offsets), scatter (each block reserves
+// its range of every bin it holds with one atomic, then places its rays).
+// Each block takes the same contiguous slice of the queue in both passes, and
+// a warp adds each run of equal keys among its lanes with one atomic.  The
+// order inside a bin is whatever the atomics give, which changes no result
+// (every ray's hit is its own).
 __device__ __forceinline__ uint32_t ray_bin( const float3 lo, const float3 scale, const float4 o, const float4 d )
 {
 	const uint32_t oct = ( d.x < 0.f ? 1u : 0u ) | ( d.y < 0.f ? 2u : 0u ) | ( d.z < 0.f ? 4u : 0u );
@@ -155,7 +159,7 @@ __device__ __forceinline__ uint32_t ray_bin( const float3 lo, const float3 scale
 }
 
 // The binning grid: the root node's box (its children's planes span
-// p .. p + 255 * 2^e per axis), cut into 16 cells per axis.
+// p .. p + 255 * 2^e per axis), cut into 2^BIN_AXIS_BITS cells per axis.
 __device__ __forceinline__ void bin_frame( const WNode *nodes, float3 &lo, float3 &scale )
 {
 	const uint4 n0 = __ldg( reinterpret_cast<const uint4 *>( nodes ) );
@@ -166,37 +170,77 @@ __device__ __forceinline__ void bin_frame( const WNode *nodes, float3 &lo, float
 				cells / ( 255.f * __uint_as_float( ( ( n0.w >> 16 ) & 0xFFu ) << 23 ) ) );
 }
 
-__global__ void __launch_bounds__( 256 ) k_bin_count( const uint32_t *__restrict__ queue, const uint32_t *n_ptr,
-													  const float4 *__restrict__ ray_o, const float4 *__restrict__ ray_d,
-													  const WNode *nodes, uint32_t *__restrict__ bins )
+constexpr int BIN_THREADS = 512;
+
+// This block's slice [lo, hi) of a queue of n entries.
+__device__ __forceinline__ void bin_slice( uint32_t n, uint32_t &lo, uint32_t &hi )
 {
-	const uint32_t n = *n_ptr, lane = lane_id();
-	float3 lo, scale;
-	bin_frame( nodes, lo, scale );
-	// the block strides together, so every lane of a warp reaches the match
-	for ( uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x )
+	const uint32_t per = ( n + gridDim.x - 1 ) / gridDim.x;
+	lo = min( n, blockIdx.x * per );
+	hi = min( n, lo + per );
+}
+
+// Runs of equal keys among a warp's lanes: whether this lane starts one, the
+// run's first lane, and its length (from its first lane).  Lanes with key ~0u
+// (no ray) form runs of their own, which the callers skip.
+struct KeyRun
+{
+	uint32_t first, len;
+};
+__device__ __forceinline__ KeyRun key_run( uint32_t key, uint32_t lane )
+{
+	const uint32_t prev = __shfl_up_sync( ~0u, key, 1 );
+	const uint32_t heads = __ballot_sync( ~0u, lane == 0 || key != prev );
+	const uint32_t first = 31u - __clz( heads & ( 0xFFFFFFFFu >> ( 31u - lane ) ) );  // last head at or below lane
+	const uint32_t after = lane == 31 ? 0u : heads & ( 0xFFFFFFFFu << ( lane + 1 ) );
+	const uint32_t end = after ? uint32_t( __ffs( after ) - 1 ) : 32u;
+	return KeyRun{ first, end - lane };  // len is meaningful on the run's first lane
+}
+
+__global__ void __launch_bounds__( BIN_THREADS ) k_bin_count( const uint32_t *__restrict__ queue, const uint32_t *n_ptr,
+															   const float4 *__restrict__ ray_o,
+															   const float4 *__restrict__ ray_d, const WNode *nodes,
+															   uint32_t *__restrict__ bins )
+{
+	__shared__ uint32_t h[ N_BINS ];
+	for ( uint32_t b = threadIdx.x; b < N_BINS; b += blockDim.x ) h[ b ] = 0;
+	__syncthreads();
+	uint32_t lo, hi;
+	bin_slice( *n_ptr, lo, hi );
+	float3 blo, scale;
+	bin_frame( nodes, blo, scale );
+	const uint32_t lane = lane_id();
+	// the block strides together, so every lane of a warp takes part in the vote
+	for ( uint32_t base = lo; base < hi; base += blockDim.x )
 	{
 		const uint32_t i = base + threadIdx.x;
 		uint32_t key = ~0u;
-		if ( i < n )
+		if ( i < hi )
 		{
 			const uint32_t item = queue[ i ];
-			key = ray_bin( lo, scale, ray_o[ item ], ray_d[ item ] );
+			key = ray_bin( blo, scale, ray_o[ item ], ray_d[ item ] );
 		}
-		const uint32_t peers = __match_any_sync( ~0u, key );
-		if ( i < n && lane == uint32_t( __ffs( peers ) - 1 ) ) atomicAdd( bins + key, uint32_t( __popc( peers ) ) );
+		const KeyRun run = key_run( key, lane );
+		if ( key != ~0u && run.first == lane ) atomicAdd( h + key, run.len );
 	}
+	__syncthreads();
+	for ( uint32_t b = threadIdx.x; b < N_BINS; b += blockDim.x )
+		if ( h[ b ] ) atomicAdd( bins + b, h[ b ] );
 }
 
-// Counts -> exclusive offsets, in place: one block of 1024 threads, N_BINS / 1024 bins each.
+// Counts -> exclusive offsets, in place: one block of 1024 threads, each
+// scanning N_BINS / 1024 consecutive bins staged through shared memory.
 __global__ void __launch_bounds__( 1024 ) k_bin_scan( uint32_t *bins )
 {
 	constexpr uint32_t PER = N_BINS / 1024;
+	__shared__ uint32_t v[ N_BINS ];
 	__shared__ uint32_t warp_sum[ 32 ];
 	const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-	uint32_t v[ PER ], s = 0;
+	for ( uint32_t b = t; b < N_BINS; b += 1024 ) v[ b ] = bins[ b ];
+	__syncthreads();
+	uint32_t s = 0;
 #pragma unroll
-	for ( uint32_t k = 0; k < PER; ++k ) v[ k ] = bins[ t * PER + k ], s += v[ k ];
+	for ( uint32_t k = 0; k < PER; ++k ) s += v[ t * PER + k ];
 	uint32_t x = s;  // inclusive scan of the threads' sums within the warp
 #pragma unroll
 	for ( int o = 1; o < 32; o <<= 1 )
@@ -220,32 +264,64 @@ __global__ void __launch_bounds__( 1024 ) k_bin_scan( uint32_t *bins )
 	__syncthreads();
 	uint32_t run = x - s + ( warp ? warp_sum[ warp - 1 ] : 0u );
 #pragma unroll
-	for ( uint32_t k = 0; k < PER; ++k ) bins[ t * PER + k ] = run, run += v[ k ];
+	for ( uint32_t k = 0; k < PER; ++k )
+	{
+		const uint32_t c = v[ t * PER + k ];
+		v[ t * PER + k ] = run;
+		run += c;
+	}
+	__syncthreads();
+	for ( uint32_t b = t; b < N_BINS; b += 1024 ) bins[ b ] = v[ b ];
 }
 
-__global__ void __launch_bounds__( 256 ) k_bin_scatter( const uint32_t *__restrict__ queue, const uint32_t *n_ptr,
-														const float4 *__restrict__ ray_o, const float4 *__restrict__ ray_d,
-														const WNode *nodes, uint32_t *__restrict__ bins,
-														uint32_t *__restrict__ out, uint32_t *err )
+__global__ void __launch_bounds__( BIN_THREADS ) k_bin_scatter( const uint32_t *__restrict__ queue, const uint32_t *n_ptr,
+																 const float4 *__restrict__ ray_o,
+																 const float4 *__restrict__ ray_d, const WNode *nodes,
+																 uint32_t *__restrict__ bins, uint32_t *__restrict__ out,
+																 uint32_t *err )
 {
-	const uint32_t n = *n_ptr, lane = lane_id();
-	float3 lo, scale;
-	bin_frame( nodes, lo, scale );
-	for ( uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x )
+	__shared__ uint32_t h[ N_BINS ];
+	for ( uint32_t b = threadIdx.x; b < N_BINS; b += blockDim.x ) h[ b ] = 0;
+	__syncthreads();
+	const uint32_t n = *n_ptr;
+	uint32_t lo, hi;
+	bin_slice( n, lo, hi );
+	float3 blo, scale;
+	bin_frame( nodes, blo, scale );
+	const uint32_t lane = lane_id();
+	// pass 1: this block's count per bin (as k_bin_count)
+	for ( uint32_t base = lo; base < hi; base += blockDim.x )
+	{
+		const uint32_t i = base + threadIdx.x;
+		uint32_t key = ~0u;
+		if ( i < hi )
+		{
+			const uint32_t item = queue[ i ];
+			key = ray_bin( blo, scale, ray_o[ item ], ray_d[ item ] );
+		}
+		const KeyRun run = key_run( key, lane );
+		if ( key != ~0u && run.first == lane ) atomicAdd( h + key, run.len );
+	}
+	__syncthreads();
+	// reserve this block's range of each bin it holds
+	for ( uint32_t b = threadIdx.x; b < N_BINS; b += blockDim.x )
+		if ( h[ b ] ) h[ b ] = atomicAdd( bins + b, h[ b ] );
+	__syncthreads();
+	// pass 2: place the rays
+	for ( uint32_t base = lo; base < hi; base += blockDim.x )
 	{
 		const uint32_t i = base + threadIdx.x;
 		uint32_t key = ~0u, item = 0;
-		if ( i < n )
+		if ( i < hi )
 		{
 			item = queue[ i ];
-			key = ray_bin( lo, scale, ray_o[ item ], ray_d[ item ] );
+			key = ray_bin( blo, scale, ray_o[ item ], ray_d[ item ] );
 		}
-		const uint32_t peers = __match_any_sync( ~0u, key );
-		const uint32_t leader = __ffs( peers ) - 1;
+		const KeyRun run = key_run( key, lane );
 		uint32_t pos = 0;
-		if ( i < n && lane == leader ) pos = atomicAdd( bins + key, uint32_t( __popc( peers ) ) );
-		pos = __shfl_sync( ~0u, pos, leader ) + __popc( peers & ( ( 1u << lane ) - 1u ) );
-		if ( i < n )
+		if ( key != ~0u && run.first == lane ) pos = atomicAdd( h + key, run.len );
+		pos = __shfl_sync( ~0u, pos, run.first ) + ( lane - run.first );
+		if ( key != ~0u )
 		{
 			if ( pos < n )
 				out[ pos ] = item;
@@ -1421,9 +1497,9 @@ void bin_queue( const DevScene &sc, const WaveBuffers &wb, const uint32_t *queue
 				const float4 *ray_o, const float4 *ray_d, int grid, cudaStream_t st )
 {
 	check( cudaMemsetAsync( wb.bins, 0, sizeof( uint32_t ) * N_BINS, st ), "memset" );
-	k_bin_count<<<grid, 256, 0, st>>>( queue, n, ray_o, ray_d, sc.nodes, wb.bins );
+	k_bin_count<<<grid, BIN_THREADS, 0, st>>>( queue, n, ray_o, ray_d, sc.nodes, wb.bins );
 	k_bin_scan<<<1, 1024, 0, st>>>( wb.bins );
-	k_bin_scatter<<<grid, 256, 0, st>>>( queue, n, ray_o, ray_d, sc.nodes, wb.bins, wb.binned, wb.err );
+	k_bin_scatter<<<grid, BIN_THREADS, 0, st>>>( queue, n, ray_o, ray_d, sc.nodes, wb.bins, wb.binned, wb.err );
 }
 
 void alloc_bins( WaveBuffers &wb, cudaStream_t st )
@@ -1727,7 +1803,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				// camera rays are coherent in pixel order already
 				if ( binning && b > 0 )
 				{
-					bin_queue( sc, wb, io.queue, n, wb.ray_o, wb.ray_d, g_shade, st );
+					bin_queue( sc, wb, io.queue, n, wb.ray_o, wb.ray_d, sms * 4, st );
 					io.queue = wb.binned;
 				}
 				if ( cfg.count_work )
@@ -1757,7 +1833,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 					uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
 					if ( binning )
 					{
-						bin_queue( sc, wb, io.queue, n, wb.sh_o, wb.sh_d, g_shade, st );
+						bin_queue( sc, wb, io.queue, n, wb.sh_o, wb.sh_d, sms * 4, st );
 						io.queue = wb.binned;
 					}
 					if ( cfg.count_work )

@@ -117,9 +117,18 @@ def test_gradients_match_fp64(guided):
 
 def test_tc_gradients_match_fp64(guided):
     """The tensor-core training pass (BF16 operands, FP32 accumulation) against
-    the FP64 gradients: BF16 rounding of activations, weights and output
-    gradients leaves a few percent of relative error; 300 records span three
-    128-row tiles with a ragged tail."""
+    the BF16-emulating FP64 restatement, record by record and in one batch of
+    300 records (three 128-row tiles with a ragged tail).
+
+    The emulation rounds where the kernel rounds, so only the order of the
+    FP32 accumulations separates them; on most records the two agree to a few
+    FP32 ulps.  Some records' gradients are ill-conditioned: their lower-layer
+    gradients are small differences of large terms, so that BF16 rounding
+    alone moves them by tens of percent (the emulation against exact FP64),
+    and an accumulation-order difference that flips one BF16 rounding moves
+    them as much.  Such a record may leave the emulation by no more than
+    twice its own BF16 sensitivity; the batch is compared on the
+    well-conditioned records."""
     s, g, grid, W, b, info = guided
     rng = np.random.default_rng(3)
     n = 300
@@ -128,19 +137,35 @@ def test_tc_gradients_match_fp64(guided):
     wts = rng.uniform(0.05, 3.0, n)
     wts[::7] = 0.0
     recs = np.concatenate([inp, om, wts[:, None]], 1).astype(np.float32)
-    ggrid, gW, gb = g.gradients(recs, tensor_cores=True)
     bmin, binv = info["bmin"].astype(np.float64), info["binv"].astype(np.float64)
-    # exact FP64 gradients: BF16 rounding alone separates them
-    rW, rb, rgrid = G.gradients(grid, W, b, bmin, binv, recs.astype(np.float64))
-    # FP64 with the kernel's BF16 roundings: only FP32 accumulation separates them
-    eW, eb, egrid = G.gradients_bf16(grid, W, b, bmin, binv, recs.astype(np.float64))
+    rel = lambda a, e: np.linalg.norm(a - e) / max(np.linalg.norm(e), 1e-300)
+    close, well = 0, []
+    for i in np.nonzero(wts > 0)[0]:
+        r64 = recs[i:i + 1].astype(np.float64)
+        _, gW, gb = g.gradients(recs[i:i + 1], tensor_cores=True)
+        gW, gb = gW.reshape(W.shape), gb.reshape(b.shape)
+        eW, eb, _ = G.gradients_bf16(grid, W, b, bmin, binv, r64)
+        xW, xb, _ = G.gradients(grid, W, b, bmin, binv, r64)
+        for l in range(G.LAYERS):
+            sens = rel(eW[l], xW[l])
+            assert rel(gW[l], eW[l]) <= 2.0 * sens + 5e-3, (i, l, rel(gW[l], eW[l]), sens)
+            assert rel(gb[l], eb[l]) <= 2.0 * rel(eb[l], xb[l]) + 5e-3, (i, l)
+        close += rel(gW, eW) < 5e-3
+        if rel(eW, xW) < 0.05:
+            well.append(i)
+    assert close >= 0.9 * int((wts > 0).sum()), close
+    assert len(well) >= 0.8 * int((wts > 0).sum()), len(well)
+    # one batch of the well-conditioned records (zero-weight rows kept as padding)
+    sel = recs[[i for i in range(n) if i in set(well) or wts[i] == 0]]
+    ggrid, gW, gb = g.gradients(sel, tensor_cores=True)
+    rW, rb, rgrid = G.gradients(grid, W, b, bmin, binv, sel.astype(np.float64))
+    eW, eb, egrid = G.gradients_bf16(grid, W, b, bmin, binv, sel.astype(np.float64))
     errs = {}
     for name, got, ref, emu in (("W", gW, rW, eW), ("b", gb, rb, eb), ("grid", ggrid, rgrid, egrid)):
         got = got.reshape(ref.shape)
-        errs[name] = (np.linalg.norm(got - ref) / np.linalg.norm(ref), np.linalg.norm(got - emu) / np.linalg.norm(emu))
+        errs[name] = (rel(got, ref), rel(got, emu))
     for l in range(G.LAYERS):
-        got, emu = gW.reshape(rW.shape)[l], eW[l]
-        errs[f"W{l}"] = (0.0, np.linalg.norm(got - emu) / np.linalg.norm(emu))
+        errs[f"W{l}"] = (0.0, rel(gW.reshape(rW.shape)[l], eW[l]))
     for name, (exact, emulated) in errs.items():
         assert emulated < 5e-3, (name, errs)
         assert exact < 0.15, (name, errs)
