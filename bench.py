@@ -394,7 +394,7 @@ def config0_section(cr, dev, steps, warmup, l2_gbs, with_reference):
         t0 = time.perf_counter()
         s2 = cr.Scene.from_desc(d)
         film, _ = s2.render(W, H, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k,
-                            **{k2: tune[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads", "bin_rays")})
+                            **{k2: tune[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads", "bin_rays", "shadow_vote", "shadow_refill_min")})
         s2.close()
         times.append(time.perf_counter() - t0)
         assert np.isfinite(film).all()
@@ -789,7 +789,7 @@ def run_ours(args):
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
             sc2 = cr.Scene.from_desc(desc)
-            tk = {k2: tuning[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads", "bin_rays")} if tuning else {}
+            tk = {k2: tuning[k2] for k2 in ("wave_paths", "refill_min", "traverse_blocks_per_sm", "shade_threads", "bin_rays", "shadow_vote", "shadow_refill_min")} if tuning else {}
             film, _ = sc2.render(WIDTH, HEIGHT, spp, max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=77 + k, **tk)
             sc2.close()
             times.append(time.perf_counter() - t0)

@@ -53,13 +53,15 @@ class RenderDesc(C.Structure):
                 ("estimator", C.c_int32), ("x0", C.c_uint32), ("y0", C.c_uint32), ("x1", C.c_uint32),
                 ("y1", C.c_uint32), ("seed", C.c_uint64), ("wave_paths", C.c_uint32), ("guiding", C.c_int32),
                 ("count_work", C.c_int32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32),
-                ("shade_threads", C.c_uint32), ("rr_start", C.c_uint32), ("bin_rays", C.c_int32)]
+                ("shade_threads", C.c_uint32), ("rr_start", C.c_uint32), ("bin_rays", C.c_int32),
+                ("shadow_vote", C.c_uint32), ("shadow_refill_min", C.c_uint32)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("wave_paths", C.c_uint32), ("refill_min", C.c_uint32), ("traverse_blocks_per_sm", C.c_uint32),
                 ("candidates_tried", C.c_uint32), ("msamples_per_s", C.c_double),
-                ("default_msamples_per_s", C.c_double), ("shade_threads", C.c_uint32), ("bin_rays", C.c_int32)]
+                ("default_msamples_per_s", C.c_double), ("shade_threads", C.c_uint32), ("bin_rays", C.c_int32),
+                ("shadow_vote", C.c_uint32), ("shadow_refill_min", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -169,7 +171,7 @@ def _p(a):
 
 def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, window=None, wave_paths=0,
                 guiding=False, count_work=False, refill_min=0, traverse_blocks_per_sm=0, shade_threads=0,
-                rr_start=0, bin_rays=0):
+                rr_start=0, bin_rays=0, shadow_vote=0, shadow_refill_min=0):
     d = RenderDesc()
     d.width, d.height, d.spp = width, height, spp
     d.max_bounce = U32_MAX if max_bounce is None else max_bounce
@@ -185,6 +187,8 @@ def render_desc(width, height, spp, max_bounce=None, estimator=None, seed=1, win
     d.shade_threads = shade_threads
     d.rr_start = rr_start
     d.bin_rays = bin_rays
+    d.shadow_vote = shadow_vote
+    d.shadow_refill_min = shadow_refill_min
     return d
 
 

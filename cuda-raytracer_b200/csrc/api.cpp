@@ -164,6 +164,7 @@ struct cr_scene
 	int tune_blocks = 8;
 	uint32_t tune_shade = 128;
 	bool tune_bin = false;
+	uint32_t tune_svote = 4, tune_srefill = 0;
 	BuildParams build;  // BVH build options (cr_scene_set_build)
 
 	~cr_scene() { release(); }
@@ -1251,6 +1252,10 @@ Resolved resolve( cr_scene *s, const cr_render_desc *desc )
 		fail( CR_ERR_INVALID, "shade_threads must be 64, 128 or 256" );
 	c.shade_threads = desc->shade_threads ? desc->shade_threads : s->tune_shade;
 	c.bin_rays = desc->bin_rays ? desc->bin_rays > 0 : s->tune_bin;
+	if ( desc->shadow_vote > 32 || desc->shadow_refill_min > 32 )
+		fail( CR_ERR_INVALID, "shadow_vote and shadow_refill_min must be 1..32" );
+	c.shadow_vote = desc->shadow_vote ? desc->shadow_vote : s->tune_svote;
+	c.shadow_refill_min = desc->shadow_refill_min ? desc->shadow_refill_min : s->tune_srefill;
 	// plain renders: the reference's roulette after bounce 3; guided renders:
 	// none (on the occluded-light scene roulette's variance is most of what
 	// the guide leaves, and removing it makes guiding 2.7x as efficient as
@@ -1857,7 +1862,7 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
 		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
 		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
-		uint32_t tried = 0, shade = 128;
+		uint32_t tried = 0, shade = 128, svote = 4, srefill = 0;
 		bool bin = false;
 		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
 			RenderConfig c = cfg;
@@ -1866,6 +1871,7 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 			c.traverse_blocks_per_sm = blocks;
 			c.shade_threads = shade;
 			c.bin_rays = bin;
+			c.shadow_vote = svote, c.shadow_refill_min = srefill;
 			ensure_wave( s, c.wave_paths, c.max_bounce, st, false, bin );
 			StageTimes warm, t;
 			render_waves( sc, c, s->wave, sum, sq, cnt, st, &warm );
@@ -1898,6 +1904,28 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 			else
 				shade = keep;
 		}
+		// the any-hit traversal's own triangle vote and refill threshold
+		for ( uint32_t v : { 2u, 8u, 32u } )
+		{
+			const uint32_t keep = svote;
+			svote = v;
+			double r = rate( wave, refill, blocks );
+			if ( r > best )
+				best = r;
+			else
+				svote = keep;
+		}
+		for ( uint32_t f : { 4u, 8u, 16u, 24u } )
+		{
+			if ( f == refill ) continue;
+			const uint32_t keep = srefill;
+			srefill = f;
+			double r = rate( wave, refill, blocks );
+			if ( r > best )
+				best = r;
+			else
+				srefill = keep;
+		}
 		// ray binning before the secondary and shadow traversals
 		{
 			bin = true;
@@ -1924,9 +1952,11 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		cuda_check( cudaStreamSynchronize( st ), "autotune" );
 		s->tune_wave = wave, s->tune_refill = refill, s->tune_blocks = blocks, s->tune_shade = shade;
 		s->tune_bin = bin;
+		s->tune_svote = svote, s->tune_srefill = srefill;
 		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
 		out->shade_threads = shade;
 		out->bin_rays = bin ? 1 : -1;
+		out->shadow_vote = svote, out->shadow_refill_min = srefill ? srefill : refill;
 		out->candidates_tried = tried;
 		out->msamples_per_s = best;
 		out->default_msamples_per_s = dflt;
@@ -2237,6 +2267,7 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 		b->tune_wave = wave, b->tune_refill = refill, b->tune_blocks = blocks, b->tune_shade = shade;
 		out->shade_threads = shade;
 		out->bin_rays = -1;  // batches trace in queue order
+		out->shadow_vote = 4, out->shadow_refill_min = refill;
 		b->drop_graph();
 		out->wave_paths = wave, out->refill_min = refill, out->traverse_blocks_per_sm = uint32_t( blocks );
 		out->candidates_tried = tried;

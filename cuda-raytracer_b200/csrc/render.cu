@@ -135,6 +135,9 @@ struct ExtendIO
 // The persistent traversal kernel hands consecutive queue entries to the lanes
 // of a warp, so after the sort a warp traces rays that start close together
 // and head the same way: they fetch the same nodes and take the same branches.
+// Only the traversal reads the sorted queue; shading keeps path order, whose
+// per-path state accesses stay coalesced (shading in sorted order doubled the
+// shading time on the 1.31M-triangle scene).
 // A memset and three launches: count (per-block shared-memory histograms added
 // to the global one), scan (counts to offsets), scatter (each block reserves
 // its range of every bin it holds with one atomic, then places its rays).
@@ -409,6 +412,10 @@ struct QueryIO
 
 // Idle lanes per warp that trigger a refill in batched ray queries.
 constexpr uint32_t QUERY_REFILL_MIN = 16;
+// Closest-hit traversal: a triangle step once a quarter of the active lanes want one.
+constexpr uint32_t EXT_TRI_VOTE = 4;
+// Any-hit traversal: the shadow queue's own refill threshold (0: the closest-hit one).
+inline uint32_t shadow_refill( const RenderConfig &cfg ) { return cfg.shadow_refill_min ? cfg.shadow_refill_min : cfg.refill_min; }
 
 struct Surface
 {
@@ -1566,7 +1573,7 @@ void batch_wave_kernels( const BatchDev &bd, const RenderConfig &cfg, WaveBuffer
 			const uint32_t *n = wb.counters + CPB * b + CNT_EXT;
 			uint32_t *cur = wb.counters + CPB * b + CNT_EXT_CURSOR;
 			k_traverse<BatchExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
-																						  wb.work, cfg.refill_min );
+																						  wb.work, cfg.refill_min, EXT_TRI_VOTE );
 		} );
 		timed( 2, [&] {
 			if ( cfg.estimator == EST_MIS )
@@ -1581,7 +1588,7 @@ void batch_wave_kernels( const BatchDev &bd, const RenderConfig &cfg, WaveBuffer
 			const uint32_t *n = wb.counters + CPB * b + CNT_SHADOW;
 			uint32_t *cur = wb.counters + CPB * b + CNT_SHADOW_CURSOR;
 			k_traverse<BatchShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( DevScene{}, io, n, 0, cur, wb.err,
-																						 wb.work + 2, cfg.refill_min );
+																						 wb.work + 2, shadow_refill( cfg ), cfg.shadow_vote );
 		} );
 	}
 	timed( 3, [&] {
@@ -1807,9 +1814,11 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 					io.queue = wb.binned;
 				}
 				if ( cfg.count_work )
-					k_traverse<ExtendIO, false, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
+					k_traverse<ExtendIO, false, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min,
+																						  EXT_TRI_VOTE );
 				else
-					k_traverse<ExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min );
+					k_traverse<ExtendIO, false, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work, cfg.refill_min,
+																						   EXT_TRI_VOTE );
 			} );
 			if ( wc.guide_sample && guided_vertex( wc.guide, b, cfg.max_bounce ) )
 				timed( 4, [&] {
@@ -1837,9 +1846,11 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 						io.queue = wb.binned;
 					}
 					if ( cfg.count_work )
-						k_traverse<ShadowIO, true, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
+						k_traverse<ShadowIO, true, true><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2,
+																							 shadow_refill( cfg ), cfg.shadow_vote );
 					else
-						k_traverse<ShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2, cfg.refill_min );
+						k_traverse<ShadowIO, true, false><<<g_ext, TRAVERSE_THREADS, 0, st>>>( sc, io, n, 0, cur, wb.err, wb.work + 2,
+																							  shadow_refill( cfg ), cfg.shadow_vote );
 				} );
 			if ( profiled ) timed( 3, [&] { k_profile_fix<<<g_shade, 128, 0, st>>>( wc, wb, wa, b ); } );
 		}
@@ -1912,10 +1923,10 @@ void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hi
 	QueryIO io{ rays, out, sc.tris, sc.attrs, sc.spheres, sc.prim_first };
 	if ( any_hit )
 		k_traverse<QueryIO, true, false><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
-																 QUERY_REFILL_MIN );
+																 QUERY_REFILL_MIN, EXT_TRI_VOTE );
 	else
 		k_traverse<QueryIO, false, false><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
-																  QUERY_REFILL_MIN );
+																  QUERY_REFILL_MIN, EXT_TRI_VOTE );
 	check( cudaGetLastError(), "trace launch" );
 }
 

@@ -110,6 +110,8 @@ struct RenderConfig
 	uint32_t shade_threads = 128;    // shading block size (64, 128 or 256); grid of SMs x 1024 threads
 	uint32_t rr_start = 4;           // MIS estimator: first bounce at which Russian roulette may end a path
 	bool bin_rays = false;           // sort secondary and shadow queues by (octant, origin cell) before tracing
+	uint32_t shadow_vote = 4;        // any-hit traversal: triangle step once this x (lanes wanting one) >= active lanes
+	uint32_t shadow_refill_min = 0;  // any-hit traversal: idle lanes that trigger a refill (0: refill_min)
 	ProfileDev prof{};               // profiled renders (reference estimator, Radiance kernel)
 };
 

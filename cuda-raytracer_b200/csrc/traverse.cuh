@@ -96,7 +96,9 @@ __device__ __forceinline__ void visit_node( const WNode *nodes, const RayPre &r,
 }
 
 // Ray source and result sink of the persistent kernel.  refill_min: idle lanes
-// (1..32) that trigger a refill from the queue.
+// (1..32) that trigger a refill from the queue.  tri_vote: the warp takes a
+// triangle step once tri_vote x (lanes with triangles pending) >= active lanes
+// (4: a quarter; 32: any lane).
 //   load(i, item, o, d, tmin, tmax): the i-th queued ray
 //   finish(item, hit, found): store the result
 //   MULTI: the queue mixes the rays of several scenes (a batched render);
@@ -107,7 +109,7 @@ constexpr int SHARED_STACK = 8;        // stack entries per thread kept in share
 template <class IO, bool ANY, bool COUNT>
 __global__ void __launch_bounds__( TRAVERSE_THREADS, 8 ) k_traverse( DevScene sc, IO io, const uint32_t *n_ptr, uint32_t n_host,
 														uint32_t *cursor, uint32_t *err, unsigned long long *work,
-														uint32_t refill_min )
+														uint32_t refill_min, uint32_t tri_vote )
 {
 	const uint32_t n = n_ptr ? *n_ptr : n_host;
 	const uint32_t lane = threadIdx.x & 31u;
@@ -185,10 +187,10 @@ __global__ void __launch_bounds__( TRAVERSE_THREADS, 8 ) k_traverse( DevScene sc
 			continue;
 		}
 		const uint32_t want_tri = __ballot_sync( FULL_MASK, active && tg.y != 0u );
-		// triangle step once a quarter of the active lanes have triangles
-		// pending (a sweep of 1/32 .. 24/32 on the 1.31M-triangle workload
-		// peaked at 8/32)
-		const bool tri_step = 4 * __popc( want_tri ) >= __popc( act );
+		// triangle step once tri_vote x the lanes with triangles pending cover
+		// the active lanes (closest hit: a quarter; a sweep of 1/32 .. 24/32 on
+		// the 1.31M-triangle workload peaked at 8/32)
+		const bool tri_step = tri_vote * __popc( want_tri ) >= __popc( act );
 		if ( !active ) continue;
 		bool done = false;
 		if ( tri_step )

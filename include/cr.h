@@ -67,6 +67,11 @@ typedef struct cr_render_desc {
     int32_t bin_rays;        /* 1: sort each secondary and shadow traversal queue by (ray
                                 octant, origin cell) before tracing; -1: trace in queue
                                 order; 0 = tuned (off until cr_autotune picks it) */
+    uint32_t shadow_vote;    /* any-hit traversal: a warp tests triangles once shadow_vote x
+                                (lanes with triangles pending) >= its active lanes, 1..32;
+                                0 = tuned (4 until cr_autotune picks it) */
+    uint32_t shadow_refill_min; /* any-hit traversal: idle lanes of 32 that trigger a refill;
+                                0 = tuned (refill_min until cr_autotune picks it) */
 } cr_render_desc;
 
 /* Launch configuration chosen by cr_autotune (also used by later renders of
@@ -80,6 +85,8 @@ typedef struct cr_tuning {
     double default_msamples_per_s; /* rate of the built-in defaults on the same sample */
     uint32_t shade_threads;  /* shading block size */
     int32_t bin_rays;        /* 1: ray binning chosen, -1: not */
+    uint32_t shadow_vote;    /* any-hit triangle-step vote */
+    uint32_t shadow_refill_min; /* any-hit refill threshold */
 } cr_tuning;
 
 typedef struct cr_stats {
