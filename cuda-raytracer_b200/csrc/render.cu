@@ -981,7 +981,9 @@ __global__ void k_generate_batch( BatchDev bd, WaveBuffers wb )
 // is not held to the registers of the guided MIS shading.
 // PROF: a profiled render (reference estimator, one scene): each shaded vertex
 // writes its bounce record and each ending path its slice's bounce counter.
-template <bool BATCH, int EST, bool PROF = false>
+// GUIDED: a guided MIS render (lobes and training records); plain MIS renders
+// take the instantiation without the guide's code, and its registers.
+template <bool BATCH, int EST, bool PROF = false, bool GUIDED = false>
 __global__ void __launch_bounds__( 256 ) k_shade( DevScene sc, RenderConfig cfg, WaveBuffers wb, WaveArgs wa,
 												  uint32_t bounce, uint2 key, BatchDev bd )
 {
@@ -1003,7 +1005,7 @@ __global__ void __launch_bounds__( 256 ) k_shade( DevScene sc, RenderConfig cfg,
 			HitRec h = wb.hit[ path ];
 			const uint32_t stride = cfg.max_bounce + 1;
 			uint32_t rec_j = 0xFFFFFFFFu;
-			if ( cfg.guiding && path >= cfg.rec_offset )
+			if ( GUIDED && cfg.guiding && path >= cfg.rec_offset )
 			{
 				uint32_t off = path - cfg.rec_offset, j = off / cfg.rec_stride;
 				if ( j * cfg.rec_stride == off && j < cfg.rec_paths ) rec_j = j;
@@ -1043,10 +1045,12 @@ __global__ void __launch_bounds__( 256 ) k_shade( DevScene sc, RenderConfig cfg,
 				{
 					uint32_t pix = uint32_t( gw / cfg.spp ), k = uint32_t( gw % cfg.spp );
 					uint64_t g = ( uint64_t( cfg.y0 + pix / cfg.ww ) * sc.cam.width + cfg.x0 + pix % cfg.ww ) * cfg.spp + k;
-					if constexpr ( EST == EST_MIS )
+					if constexpr ( EST == EST_MIS && GUIDED )
 						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out,
 								   cfg.guide_sample ? wb.lobes + size_t( path ) * LOBE_SLOTS : nullptr,
 								   recorded ? rec_j * stride + bounce : 0xFFFFFFFFu );
+					else if constexpr ( EST == EST_MIS )
+						shade_mis( sc, cfg, key, g, bounce, ro, rd, h, beta, L, out, nullptr, 0xFFFFFFFFu );
 					else if constexpr ( PROF )
 					{
 						ProfOut po;
@@ -1828,7 +1832,9 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 				timed( 2, [&] { k_aov<<<g_shade, 128, 0, st>>>( sc, wc, wb, wa, key ); } );
 			else
 				timed( 2, [&] {
-					if ( cfg.estimator == EST_MIS )
+					if ( cfg.estimator == EST_MIS && ( wc.guiding || wc.guide_sample ) )
+						k_shade<false, EST_MIS, false, true><<<g_shade_k, shade_t, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
+					else if ( cfg.estimator == EST_MIS )
 						k_shade<false, EST_MIS><<<g_shade_k, shade_t, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
 					else if ( profiled )
 						k_shade<false, EST_KOISHI, true><<<g_shade_k, shade_t, 0, st>>>( sc, wc, wb, wa, b, key, BatchDev{} );
