@@ -43,7 +43,7 @@ struct GuideState
 	uint32_t warmup_steps = 8;      // steps before the guide is first sampled
 	bool product_target = true;     // fit Li * f * cos (the integrand) instead of Li
 	uint32_t max_steps = 600;       // training budget in Adam steps (0: train every wave)
-	uint32_t guided_bounces = 4;    // leading vertices that sample the guide (0: all but the last)
+	uint32_t guided_bounces = 0;    // leading vertices that sample the guide (0: all but the last)
 	bool learn_select = false;      // the network also outputs the per-vertex probability of sampling the guide
 	uint32_t packed_step = ~0u;     // step whose weights Wp holds (~0: none)
 	GuideRecords rec;

@@ -436,7 +436,7 @@ int cr_guide_info(const cr_scene *s, float *bmin, float *binv, uint32_t *step, u
  *   guided_bounces  vertices 0 .. guided_bounces-1 of a path sample the guide
  *                   (and only their bounces run the guide's inference); later
  *                   vertices sample the BSDF alone (0: every vertex but the
- *                   last) [4]
+ *                   last) [0]
  *   learn_select    1: the network also learns, per vertex, the probability of
  *                   sampling the guide rather than the BSDF (a sigmoid output
  *                   clamped to [0.02, 0.98], trained on the density of the

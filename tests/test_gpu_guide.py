@@ -90,7 +90,7 @@ def test_guide_configure_validates(guided):
     import cuda_raytracer_b200 as crm
     cfg = g.configure()
     assert cfg["train_paths"] == 32768 and cfg["steps_per_wave"] == 64 and cfg["warmup_steps"] == 8
-    assert cfg["product_target"] == 1 and cfg["guided_bounces"] == 4
+    assert cfg["product_target"] == 1 and cfg["guided_bounces"] == 0
     for bad in ({"lr": 0.0}, {"select_prob": 1.0}, {"train_paths": 0}, {"steps_per_wave": 65}):
         with pytest.raises(crm.CrError):
             g.configure(**bad)
