@@ -113,6 +113,12 @@ struct DevBuf
 		cuda_check( cudaMalloc( (void **)&p, sizeof( T ) * n ), "cudaMalloc" );
 		cuda_check( cudaMemcpy( p, h.data(), sizeof( T ) * n, cudaMemcpyHostToDevice ), "upload" );
 	}
+	void alloc( size_t count )
+	{
+		release();
+		n = count;
+		if ( n ) cuda_check( cudaMalloc( (void **)&p, sizeof( T ) * n ), "cudaMalloc" );
+	}
 	void release()
 	{
 		if ( p ) cudaFree( p );
@@ -990,7 +996,6 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	for ( auto &m : s->meshes ) nt += m.idx.size() / 3;
 	if ( nt >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many triangles" );
 	s->n_tris = nt;
-	std::vector<float4> src( 3 * nt ), attrs( 3 * nt );
 	std::vector<uint32_t> prim_first( s->prims.size(), 0 );
 	std::vector<int> prim_light( s->prims.size(), -1 );
 	// Lights: the pointLight assets in asset order (scene.cu:156-163), then
@@ -1054,30 +1059,78 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 		prim_light[ p ] = int( lights.size() );
 		lights.push_back( L );
 	}
-	// Flatten triangles in primitive order.
+	// Flatten triangles in primitive order, on the device: the indexed meshes
+	// go up as they are (12 bytes per vertex and normal, 12 per triangle), and
+	// k_flatten_mesh writes the builder's vertex records and the attribute
+	// records, and the bounds of the referenced vertices.
 	uint64_t g = 0;
-	float lo[ 3 ] = { INFINITY, INFINITY, INFINITY }, hi[ 3 ] = { -INFINITY, -INFINITY, -INFINITY };
+	size_t n_sph = 0;
 	for ( size_t p = 0; p < s->prims.size(); ++p )
 	{
-		const HostPrim &hp = s->prims[ p ];
 		prim_first[ p ] = uint32_t( g );
-		if ( hp.kind != 0 ) continue;
-		const HostMesh &m = s->meshes[ hp.index ];
-		for ( size_t t = 0; t < m.idx.size() / 3; ++t, ++g )
+		if ( s->prims[ p ].kind == 0 )
+			g += s->meshes[ s->prims[ p ].index ].idx.size() / 3;
+		else
+			++n_sph;
+	}
+	const uint64_t n_prims = nt + n_sph;
+	if ( n_prims >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many primitives" );
+	float4 *d_src = nullptr;
+	if ( n_prims ) cuda_check( cudaMallocAsync( (void **)&d_src, sizeof( float4 ) * 3 * n_prims, st ), "cudaMalloc" );
+	// the builder's input lives until the end of the commit, whichever way it ends
+	struct StreamFree
+	{
+		void *p;
+		cudaStream_t st;
+		~StreamFree()
 		{
-			for ( int k = 0; k < 3; ++k )
+			if ( p ) cudaFreeAsync( p, st );
+		}
+	} src_guard{ d_src, st };
+	s->attrs.alloc( 3 * nt );
+	float lo[ 3 ] = { INFINITY, INFINITY, INFINITY }, hi[ 3 ] = { -INFINITY, -INFINITY, -INFINITY };
+	{
+		if ( nt )
+		{
+			size_t nv_all = 0;
+			for ( const HostMesh &m : s->meshes ) nv_all += m.v.size() / 3;
+			float *d_v = nullptr, *d_n = nullptr, *d_b = nullptr;
+			uint32_t *d_idx = nullptr;
+			cuda_check( cudaMallocAsync( (void **)&d_v, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
+			StreamFree v_guard{ d_v, st };
+			cuda_check( cudaMallocAsync( (void **)&d_n, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
+			StreamFree n_guard{ d_n, st };
+			cuda_check( cudaMallocAsync( (void **)&d_idx, sizeof( uint32_t ) * 3 * nt, st ), "cudaMalloc" );
+			StreamFree idx_guard{ d_idx, st };
+			cuda_check( cudaMallocAsync( (void **)&d_b, sizeof( float ) * 6, st ), "cudaMalloc" );
+			StreamFree b_guard{ d_b, st };
+			const float b0[ 6 ] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
+			cuda_check( cudaMemcpyAsync( d_b, b0, sizeof b0, cudaMemcpyHostToDevice, st ), "upload" );
+			size_t vo = 0, io = 0;
+			for ( size_t p = 0; p < s->prims.size(); ++p )
 			{
-				const float *v = &m.v[ 3 * m.idx[ 3 * t + k ] ], *n = &m.n[ 3 * m.idx[ 3 * t + k ] ];
-				src[ 3 * g + k ] = make_float4( v[ 0 ], v[ 1 ], v[ 2 ], 0.f );
-				for ( int a = 0; a < 3; ++a ) lo[ a ] = std::min( lo[ a ], v[ a ] ), hi[ a ] = std::max( hi[ a ], v[ a ] );
-				int w = k == 0 ? m.shader : k == 1 ? int( p ) : prim_light[ p ];
-				float wf;
-				std::memcpy( &wf, &w, 4 );
-				attrs[ 3 * g + k ] = make_float4( n[ 0 ], n[ 1 ], n[ 2 ], wf );
+				const HostPrim &hp = s->prims[ p ];
+				if ( hp.kind != 0 ) continue;
+				const HostMesh &m = s->meshes[ hp.index ];
+				const size_t nv = m.v.size() / 3, nm = m.idx.size() / 3;
+				if ( !nm ) continue;
+				cuda_check( cudaMemcpyAsync( d_v + 3 * vo, m.v.data(), sizeof( float ) * 3 * nv, cudaMemcpyHostToDevice, st ), "upload" );
+				cuda_check( cudaMemcpyAsync( d_n + 3 * vo, m.n.data(), sizeof( float ) * 3 * nv, cudaMemcpyHostToDevice, st ), "upload" );
+				cuda_check( cudaMemcpyAsync( d_idx + 3 * io, m.idx.data(), sizeof( uint32_t ) * 3 * nm, cudaMemcpyHostToDevice, st ),
+							"upload" );
+				FlatMesh fm{ d_v + 3 * vo, d_n + 3 * vo, d_idx + 3 * io, uint32_t( nm ), prim_first[ p ], m.shader, int( p ),
+							 prim_light[ p ] };
+				flatten_mesh( fm, d_src, s->attrs.p, d_b, st );
+				vo += nv, io += nm;
 			}
+			float b[ 6 ];
+			cuda_check( cudaMemcpyAsync( b, d_b, sizeof b, cudaMemcpyDeviceToHost, st ), "bounds" );
+			cuda_check( cudaStreamSynchronize( st ), "flatten" );
+			for ( int a = 0; a < 3; ++a ) lo[ a ] = b[ a ], hi[ a ] = b[ 3 + a ];
 		}
 	}
 	std::vector<DevSphere> ds;
+	std::vector<float4> sph_src;
 	for ( size_t p = 0; p < s->prims.size(); ++p )
 	{
 		const HostPrim &hp = s->prims[ p ];
@@ -1094,10 +1147,13 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 		ds.push_back( d );
 		// the sphere as a BVH primitive: its box (the builder's bounds of the
 		// three points) and, in the third record, centre and r^2
-		src.push_back( make_float4( hs.c[ 0 ] - d.r, hs.c[ 1 ] - d.r, hs.c[ 2 ] - d.r, 0.f ) );
-		src.push_back( make_float4( hs.c[ 0 ] + d.r, hs.c[ 1 ] + d.r, hs.c[ 2 ] + d.r, 0.f ) );
-		src.push_back( make_float4( hs.c[ 0 ], hs.c[ 1 ], hs.c[ 2 ], d.r2 ) );
+		sph_src.push_back( make_float4( hs.c[ 0 ] - d.r, hs.c[ 1 ] - d.r, hs.c[ 2 ] - d.r, 0.f ) );
+		sph_src.push_back( make_float4( hs.c[ 0 ] + d.r, hs.c[ 1 ] + d.r, hs.c[ 2 ] + d.r, 0.f ) );
+		sph_src.push_back( make_float4( hs.c[ 0 ], hs.c[ 1 ], hs.c[ 2 ], d.r2 ) );
 	}
+	if ( !sph_src.empty() )
+		cuda_check( cudaMemcpyAsync( d_src + 3 * nt, sph_src.data(), sizeof( float4 ) * sph_src.size(), cudaMemcpyHostToDevice, st ),
+					"upload" );
 	float sc = 1;
 	for ( int a = 0; a < 3; ++a )
 		if ( std::isfinite( lo[ a ] ) ) sc = std::max( sc, std::max( std::fabs( lo[ a ] ), std::fabs( hi[ a ] ) ) );
@@ -1107,7 +1163,6 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	std::vector<DevShader> dsh;
 	for ( auto &x : s->shaders ) dsh.push_back( x.second );
 
-	s->attrs.upload( attrs );
 	s->dspheres.upload( ds );
 	s->dshaders.upload( dsh );
 	s->dlights.upload( lights );
@@ -1120,23 +1175,16 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	s->tables_host = tables;
 	s->prim_light = prim_light;
 	// BVH over the triangles (ids 0 .. nt-1) and the spheres (ids nt ..)
-	const uint64_t n_prims = src.size() / 3;
-	if ( n_prims >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many primitives" );
 	if ( n_prims )
 	{
-		float4 *d_src = nullptr;
-		cuda_check( cudaMallocAsync( (void **)&d_src, sizeof( float4 ) * src.size(), st ), "cudaMalloc" );
-		cuda_check( cudaMemcpyAsync( d_src, src.data(), sizeof( float4 ) * src.size(), cudaMemcpyHostToDevice, st ), "upload" );
 		try
 		{
 			build_wide_bvh( d_src, uint32_t( n_prims ), s->bvh, st, s->build );
 		}
 		catch ( const std::exception &e )
 		{
-			cudaFreeAsync( d_src, st );
 			fail( CR_ERR_CUDA, e.what() );
 		}
-		cudaFreeAsync( d_src, st );
 		if ( s->bvh.depth > uint32_t( TRAVERSAL_STACK ) )
 			fail( CR_ERR_INVALID, "BVH depth " + std::to_string( s->bvh.depth ) + " exceeds the traversal stack" );
 	}

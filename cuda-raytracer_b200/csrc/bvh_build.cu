@@ -751,4 +751,69 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 		cudaFreeAsync( p, st );
 }
 
+// Float min / max through the integer order of the IEEE bits (non-negative
+// values order as signed ints, negative ones reversed as unsigned).
+__device__ __forceinline__ void atomic_min_float( float *a, float v )
+{
+	if ( v >= 0.f )
+		atomicMin( reinterpret_cast<int *>( a ), __float_as_int( v ) );
+	else
+		atomicMax( reinterpret_cast<unsigned int *>( a ), __float_as_uint( v ) );
+}
+__device__ __forceinline__ void atomic_max_float( float *a, float v )
+{
+	if ( v >= 0.f )
+		atomicMax( reinterpret_cast<int *>( a ), __float_as_int( v ) );
+	else
+		atomicMin( reinterpret_cast<unsigned int *>( a ), __float_as_uint( v ) );
+}
+
+__global__ void k_flatten_mesh( FlatMesh m, float4 *__restrict__ src, float4 *__restrict__ attrs, float *bounds )
+{
+	float lo[ 3 ] = { INFINITY, INFINITY, INFINITY }, hi[ 3 ] = { -INFINITY, -INFINITY, -INFINITY };
+	for ( uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < m.nt; t += gridDim.x * blockDim.x )
+	{
+		const size_t g = m.g0 + t;
+#pragma unroll
+		for ( int k = 0; k < 3; ++k )
+		{
+			const uint32_t vi = m.idx[ 3 * size_t( t ) + k ];
+			const float x = m.v[ 3 * size_t( vi ) ], y = m.v[ 3 * size_t( vi ) + 1 ], z = m.v[ 3 * size_t( vi ) + 2 ];
+			const int w = k == 0 ? m.shader : k == 1 ? m.prim : m.light;
+			src[ 3 * g + k ] = make_float4( x, y, z, 0.f );
+			attrs[ 3 * g + k ] = make_float4( m.n[ 3 * size_t( vi ) ], m.n[ 3 * size_t( vi ) + 1 ], m.n[ 3 * size_t( vi ) + 2 ],
+											  __int_as_float( w ) );
+			// fminf / fmaxf skip a NaN operand, as the host's std::min did
+			lo[ 0 ] = fminf( lo[ 0 ], x ), lo[ 1 ] = fminf( lo[ 1 ], y ), lo[ 2 ] = fminf( lo[ 2 ], z );
+			hi[ 0 ] = fmaxf( hi[ 0 ], x ), hi[ 1 ] = fmaxf( hi[ 1 ], y ), hi[ 2 ] = fmaxf( hi[ 2 ], z );
+		}
+	}
+#pragma unroll
+	for ( int a = 0; a < 3; ++a )
+		for ( int o = 16; o; o >>= 1 )
+		{
+			lo[ a ] = fminf( lo[ a ], __shfl_xor_sync( 0xFFFFFFFFu, lo[ a ], o ) );
+			hi[ a ] = fmaxf( hi[ a ], __shfl_xor_sync( 0xFFFFFFFFu, hi[ a ], o ) );
+		}
+	if ( ( threadIdx.x & 31u ) == 0 )
+		for ( int a = 0; a < 3; ++a )
+		{
+			// NaN coordinates never enter the bounds (fminf / fmaxf drop them);
+			// a warp that saw no vertex holds +inf / -inf, which change nothing
+			if ( !isnan( lo[ a ] ) ) atomic_min_float( bounds + a, lo[ a ] );
+			if ( !isnan( hi[ a ] ) ) atomic_max_float( bounds + 3 + a, hi[ a ] );
+		}
+}
+
+void flatten_mesh( const FlatMesh &m, float4 *src, float4 *attrs, float *bounds, cudaStream_t st )
+{
+	if ( m.nt == 0 ) return;
+	int dev = 0, sms = 0;
+	check( cudaGetDevice( &dev ), "device" );
+	check( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device" );
+	const int grid = int( std::min<uint64_t>( ( m.nt + 255 ) / 256, uint64_t( sms ) * 8 ) );
+	k_flatten_mesh<<<grid, 256, 0, st>>>( m, src, attrs, bounds );
+	check( cudaGetLastError(), "flatten launch" );
+}
+
 }  // namespace cr

@@ -19,7 +19,7 @@ struct WideBvh
 // std::runtime_error on failure.  Synchronises `st` once per tree level.
 // Build options.  ploc: binary tree by locally-ordered clustering (higher
 // quality) within `radius` positions of the Morton order; otherwise the
-// Karras radix tree (faster build).  max_leaf (1..4) triangles per leaf;
+// Karras radix tree (faster build).  max_leaf (1..3) triangles per leaf;
 // cost_node / cost_tri: SAH costs of a node visit and a triangle test.
 struct BuildParams
 {
@@ -35,4 +35,20 @@ struct BuildParams
 };
 void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st,
 					 const BuildParams &bp = BuildParams() );
+
+// One indexed mesh, on the device, flattened into triangles g0 .. g0 + nt - 1:
+// src[3 g + k] = (vertex k, 0) for the builder, attrs[3 g + k] = (normal k,
+// w) with w the int bits of the shader (k = 0), primitive (k = 1) and light
+// (k = 2) ids.  bounds (6 floats: lo xyz, hi xyz, +inf / -inf before the
+// first call) grows over the coordinates (NaN skipped) of the referenced vertices.
+// Indices must be below the vertex count (checked when meshes are added).
+struct FlatMesh
+{
+	const float *v, *n;     // 3 floats per vertex
+	const uint32_t *idx;    // 3 per triangle
+	uint32_t nt;
+	uint64_t g0;
+	int shader, prim, light;
+};
+void flatten_mesh( const FlatMesh &m, float4 *src, float4 *attrs, float *bounds, cudaStream_t st );
 }  // namespace cr

@@ -1,16 +1,19 @@
 // Tensor-core forward pass of the guide MLP on sm_100a (tcgen05 + TMEM).
 //
-// One CTA of 256 threads takes two tiles of 128 rows (queries) at a time.
-// Every thread owns one row: it gathers the row's encoding (hash grid, SH,
-// normal) in FP32, rounds it to BF16 and stores it into the tile's shared
-// memory operand.  For each of the 5 layers one thread issues tcgen05.mma
-// (kind::f16, BF16 x BF16 -> FP32, M = 128, N = 64, K = 16; four K steps per
-// layer and tile) with the activations as A and the layer's BF16 weights as
-// B, both in shared memory; the accumulators live in tensor memory (64
-// columns per tile).  tcgen05.commit signals an mbarrier; the threads then
-// read their row back with tcgen05.ld, add the bias, apply the ReLU, round to
-// BF16 and overwrite their A row for the next layer.  The last layer's row is
-// handed to the caller's sink in FP32.
+// One CTA of 256 threads holds the weights once and runs two independent
+// groups of 128 threads, one per tile of 128 rows (queries).  Every thread
+// owns one row: it gathers the row's encoding (hash grid, SH, normal) in
+// FP32, rounds it to BF16 and stores it into its tile's shared-memory
+// operand.  For each of the 5 layers the group's first thread issues
+// tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M = 128, N = 64, K = 16; four
+// K steps per layer) with the activations as A and the layer's BF16 weights
+// as B, both in shared memory; the accumulators live in tensor memory (64
+// columns per tile).  tcgen05.commit signals the group's mbarrier; the
+// threads then read their row back with tcgen05.ld, add the bias, apply the
+// ReLU, round to BF16 and overwrite their A row for the next layer.  The last
+// layer's row is handed to the caller's sink in FP32.  The groups synchronise
+// on named barriers of their own, so one group's hash-grid gathers overlap
+// the other's MMA round trips.
 //
 // Shared-memory operands use the canonical K-major layout without swizzle:
 // 8 x 16-byte core matrices, element (r, k) at
@@ -44,9 +47,9 @@ constexpr uint32_t TMEM_COLS = 64 * TILES;          // FP32 accumulators: 64 col
 constexpr uint32_t OFF_W = 0;
 constexpr uint32_t OFF_A = OFF_W + G_LAYERS * W_BYTES;          // 40960
 constexpr uint32_t OFF_BIAS = OFF_A + TILES * TILE_BYTES;       // 73728
-constexpr uint32_t OFF_BAR = OFF_BIAS + G_LAYERS * G_HID * 4;   // 75008
-constexpr uint32_t OFF_TMEM = OFF_BAR + 8;                      // 75016
-constexpr uint32_t SMEM_USED = OFF_TMEM + 8;                    // 75024
+constexpr uint32_t OFF_BAR = OFF_BIAS + G_LAYERS * G_HID * 4;   // 75008: one mbarrier per tile
+constexpr uint32_t OFF_TMEM = OFF_BAR + 8 * TILES;              // 75024
+constexpr uint32_t SMEM_USED = OFF_TMEM + 8;                    // 75032
 constexpr uint32_t SMEM_BYTES = SMEM_USED + 128;                // slack for the alignment
 
 // Weight images in device memory: the forward image (layer l: N = out, K = in)
@@ -97,6 +100,41 @@ __device__ __forceinline__ void mma_bf16( uint32_t d_tmem, uint64_t a, uint64_t 
 		:
 		: "r"( d_tmem ), "l"( a ), "l"( b ), "r"( IDESC ), "r"( accumulate )
 		: "memory" );
+}
+
+// Named barrier of tile group t (ids 1 and 2; 0 is __syncthreads), and the
+// same barrier as an OR-reduction of a predicate over the group.
+// (Immediate barrier ids: a register id makes the compiler reserve all 16.)
+static_assert( TILES == 2 && ROWS == 128, "two tile groups of 128 threads" );
+__device__ __forceinline__ void group_sync( uint32_t t )
+{
+	if ( t == 0 )
+		asm volatile( "bar.sync 1, 128;" ::: "memory" );
+	else
+		asm volatile( "bar.sync 2, 128;" ::: "memory" );
+}
+__device__ __forceinline__ bool group_or( uint32_t t, bool pred )
+{
+	uint32_t r;
+	if ( t == 0 )
+		asm volatile(
+			"{\n\t.reg .pred p, q;\n\t"
+			"setp.ne.u32 p, %1, 0;\n\t"
+			"bar.red.or.pred q, 1, 128, p;\n\t"
+			"selp.u32 %0, 1, 0, q;\n\t}"
+			: "=r"( r )
+			: "r"( uint32_t( pred ) )
+			: "memory" );
+	else
+		asm volatile(
+			"{\n\t.reg .pred p, q;\n\t"
+			"setp.ne.u32 p, %1, 0;\n\t"
+			"bar.red.or.pred q, 2, 128, p;\n\t"
+			"selp.u32 %0, 1, 0, q;\n\t}"
+			: "=r"( r )
+			: "r"( uint32_t( pred ) )
+			: "memory" );
+	return r != 0;
 }
 
 __device__ __forceinline__ void mma_commit( uint32_t bar )
@@ -228,7 +266,7 @@ __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t
 	uint8_t *sm = reinterpret_cast<uint8_t *>( ( reinterpret_cast<uintptr_t>( smem_raw ) + 127 ) & ~uintptr_t( 127 ) );
 	const uint32_t tid = threadIdx.x, warp = tid >> 5;
 	const uint32_t tile = tid / ROWS, row = tid % ROWS;
-	const uint32_t bar = smem_u32( sm + OFF_BAR );
+	const uint32_t bar = smem_u32( sm + OFF_BAR ) + 8u * tile;  // this group's mbarrier
 	uint32_t *tmem_slot = reinterpret_cast<uint32_t *>( sm + OFF_TMEM );
 	float *bias = reinterpret_cast<float *>( sm + OFF_BIAS );
 
@@ -239,7 +277,7 @@ __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t
 		for ( uint32_t i = tid; i < G_LAYERS * W_BYTES / 16; i += THREADS ) dst4[ i ] = __ldg( src4 + i );
 		for ( uint32_t i = tid; i < G_LAYERS * G_HID; i += THREADS ) bias[ i ] = g.b[ i ];
 	}
-	if ( tid == 0 )
+	if ( row == 0 )
 	{
 		asm volatile( "mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"( bar ) : "memory" );
 		asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
@@ -274,23 +312,22 @@ __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t
 			for ( int j = 0; j < 8; ++j ) *reinterpret_cast<uint4 *>( my_tile + canon( row, 8 * j ) ) = make_uint4( 0u, 0u, 0u, 0u );
 		for ( int l = 0; l < G_LAYERS; ++l )
 		{
-			// make this thread's A row visible to the tensor core, then one
-			// thread issues the layer for both tiles
+			// make this thread's A row visible to the tensor core, then the
+			// group's first thread issues the layer for its tile
 			fence_async_smem();
 			tc_before_sync();
-			__syncthreads();
-			if ( tid == 0 )
+			group_sync( tile );
+			if ( row == 0 )
 			{
 				tc_after_sync();
-				for ( uint32_t t = 0; t < TILES; ++t )
-					for ( uint32_t k = 0; k < G_IN / 16; ++k )
-						mma_bf16( tmem + t * 64u, sdesc( smem_u32( sm + OFF_A + t * TILE_BYTES ) + k * 2u * LBO ),
-								  sdesc( smem_u32( sm + OFF_W + l * W_BYTES ) + k * 2u * LBO ), k > 0 );
+				for ( uint32_t k = 0; k < G_IN / 16; ++k )
+					mma_bf16( tmem + tile * 64u, sdesc( smem_u32( my_tile ) + k * 2u * LBO ),
+							  sdesc( smem_u32( sm + OFF_W + l * W_BYTES ) + k * 2u * LBO ), k > 0 );
 				mma_commit( bar );
 			}
 			const bool ok = mbar_wait( bar, phase );
 			phase ^= 1u;
-			if ( __syncthreads_or( !ok ) )
+			if ( group_or( tile, !ok ) )
 			{
 				failed = true;
 				break;
@@ -332,10 +369,11 @@ __device__ __forceinline__ void mlp_forward_tc( const GuideDev &g, const uint8_t
 	}
 	if ( failed )
 	{
-		if ( tid == 0 ) atomicOr( err, ERR_MMA_TIMEOUT );
+		if ( row == 0 ) atomicOr( err, ERR_MMA_TIMEOUT );
 		// the timed-out phase once more (bounded): no MMA may still write TMEM below
 		mbar_wait( bar, phase ^ 1u );
 	}
+	// both groups done before the tensor memory goes
 	tc_before_sync();
 	__syncthreads();
 	if ( warp == 0 )
