@@ -144,7 +144,7 @@ def lib():
             "cr_guide_configure": (I, [P, P, P]), "cr_guide_loss": (I, [P, P]),
             "cr_guide_forward_tc": (I, [P, P, U64, P]), "cr_guide_gradients_tc": (I, [P, P, U64, P, P, P]),
             "cr_batch_create": (I, [P, U32, U32, C.c_int32, P, P]), "cr_batch_autotune": (I, [P, P]),
-            "cr_batch_set_tuning": (I, [P, P]),
+            "cr_batch_set_tuning": (I, [P, P]), "cr_trim_memory": (I, []),
             "cr_batch_render": (I, [P, U64, P]), "cr_batch_destroy": (None, [P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
@@ -403,6 +403,12 @@ def measure_peaks(stream=0):
     l2, fp = C.c_double(), C.c_double()
     _check(lib().cr_measure_peaks(C.c_void_p(stream), C.byref(l2), C.byref(fp)))
     return l2.value, fp.value
+
+
+def trim_memory():
+    """cr_trim_memory: hand the wave-state memory the library keeps mapped
+    between renders back to the device."""
+    _check(lib().cr_trim_memory())
 
 
 def measure_gather(record_bytes=80, array_bytes=64 << 20, stream=0):

@@ -1514,6 +1514,11 @@ extern "C" {
 const char *cr_last_error( void ) { return g_last_error.c_str(); }
 const char *cr_version( void ) { return "cr_b200 1.0 (sm_100a)"; }
 
+int cr_trim_memory( void )
+{
+	return guarded( [&] { trim_wave_pools(); } );
+}
+
 int cr_scene_create_empty( cr_scene **out )
 {
 	return guarded( [&] {

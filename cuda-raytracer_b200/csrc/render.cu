@@ -1408,10 +1408,11 @@ void check( cudaError_t e, const char *what )
 	if ( e != cudaSuccess ) throw std::runtime_error( std::string( what ) + ": " + cudaGetErrorString( e ) );
 }
 
+// Wave state comes from the library's own memory pool of the current device.
 template <typename T>
 void alloc( T *&p, size_t n, cudaStream_t st )
 {
-	check( cudaMallocAsync( (void **)&p, sizeof( T ) * std::max<size_t>( n, 1 ), st ), "wave alloc" );
+	check( cudaMallocFromPoolAsync( (void **)&p, sizeof( T ) * std::max<size_t>( n, 1 ), wave_pool(), st ), "wave alloc" );
 }
 
 struct EventPool
@@ -1450,6 +1451,43 @@ int current_device()
 	return dev;
 }
 }  // namespace
+
+// One memory pool per device for the wave state, whose release threshold keeps
+// freed memory mapped: the next scene's (or the next wave size's) buffers then
+// reuse it instead of mapping gigabytes of device memory again.  trim_wave_pools
+// (cr_trim_memory) hands the cached memory back.
+namespace
+{
+cudaMemPool_t g_pools[ MAX_DEVICES ] = {};
+}
+
+cudaMemPool_t wave_pool()
+{
+	const int dev = current_device();
+	if ( dev < 0 || dev >= MAX_DEVICES ) throw std::runtime_error( "device index out of range" );
+	std::lock_guard<std::mutex> lock( g_dev_mutex );
+	if ( !g_pools[ dev ] )
+	{
+		cudaMemPoolProps props{};
+		props.allocType = cudaMemAllocationTypePinned;
+		props.handleTypes = cudaMemHandleTypeNone;
+		props.location.type = cudaMemLocationTypeDevice;
+		props.location.id = dev;
+		cudaMemPool_t pool = nullptr;
+		check( cudaMemPoolCreate( &pool, &props ), "memory pool" );
+		uint64_t keep = UINT64_MAX;
+		check( cudaMemPoolSetAttribute( pool, cudaMemPoolAttrReleaseThreshold, &keep ), "memory pool" );
+		g_pools[ dev ] = pool;
+	}
+	return g_pools[ dev ];
+}
+
+void trim_wave_pools()
+{
+	std::lock_guard<std::mutex> lock( g_dev_mutex );
+	for ( cudaMemPool_t pool : g_pools )
+		if ( pool ) check( cudaMemPoolTrimTo( pool, 0 ), "memory pool trim" );
+}
 
 int sm_count()
 {
