@@ -199,6 +199,65 @@ def reference_rate(scene_json, steps, warmup, spp, width=WIDTH, height=HEIGHT):
     return samples / secs / 1e6, secs / max(len(timed), 1), used, samples // max(len(timed), 1)
 
 
+def layout_comparison(scene, desc, scene_json, n=4096, seed=5):
+    """Bytes per closest-hit query in this build's layout and in the
+    reference's, on the same rays: n camera rays at random pixels and, from
+    each camera ray's hit, one cosine-distributed secondary ray.  Both use
+    bytes = nodes x S_node + primitives x S_prim + 32 (ray in) + 16 (hit out):
+    here wide nodes of 80 bytes and 48-byte primitive records (cr_trace_work);
+    the reference's own walk (oracle/_ref/cr_ref work: Mesh::intersect's
+    depth-first walk of each mesh's binary BVH, mesh.cu:200-267) reads 36-byte
+    node records and 36-byte faces, and tests every sphere (16 bytes)."""
+    import numpy as np
+    import oracle
+    from cuda_raytracer_b200 import scenes
+    rng = np.random.default_rng(seed)
+    px = np.stack([rng.integers(0, desc.width, n), rng.integers(0, desc.height, n)], 1)
+    o, d = scenes.pinhole_rays(desc.camera, desc.width, desc.height, desc.spp, px, rng.integers(0, desc.spp, n))
+    cam = np.concatenate([o, d, np.zeros((n, 1), np.float32)], 1).astype(np.float32)
+    h = scene.trace(cam)
+    sec = []
+    groups = desc.groups
+    for i in np.nonzero(h["prim"] >= 0)[0]:
+        p_ = o[i].astype(np.float64) + d[i].astype(np.float64) * float(h["t"][i])
+        pr = int(h["prim"][i])
+        if pr < len(groups):
+            g = groups[pr]
+            v0, v1, v2 = (g.v[g.f[int(h["tri"][i])][k]].astype(np.float64) for k in range(3))
+            nrm = np.cross(v1 - v0, v2 - v0)
+        else:
+            nrm = p_ - np.asarray(desc.spheres[pr - len(groups)]["o"], np.float64)
+        nrm /= np.linalg.norm(nrm)
+        if np.dot(nrm, d[i]) > 0:
+            nrm = -nrm
+        # cosine-distributed direction about the normal
+        u1, u2 = rng.random(), rng.random()
+        r, phi = np.sqrt(u1), 2 * np.pi * u2
+        t1 = np.cross(nrm, [1.0, 0, 0] if abs(nrm[0]) < 0.9 else [0, 1.0, 0])
+        t1 /= np.linalg.norm(t1)
+        t2 = np.cross(nrm, t1)
+        w = r * np.cos(phi) * t1 + r * np.sin(phi) * t2 + np.sqrt(max(0.0, 1 - u1)) * nrm
+        sec.append(np.concatenate([p_ + nrm * 1e-3, w, [0.0]]))
+    rays = np.concatenate([cam, np.asarray(sec, np.float32).reshape(-1, 7)]).astype(np.float32)
+    nodes, prims = scene.trace_work(rays)
+    with tempfile.TemporaryDirectory() as tmp:
+        rp = os.path.join(tmp, "rays.f32")
+        rays.tofile(rp)
+        r = subprocess.run([oracle.REF_BIN, "work", os.path.basename(scene_json), rp], cwd=os.path.dirname(scene_json),
+                           capture_output=True, text=True, timeout=1800, check=True)
+    ref = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    m = len(rays)
+    ours = (nodes * NODE_BYTES + prims * TRI_BYTES) / m + RAY_BYTES
+    theirs = (ref["nodes"] * 36 + ref["faces"] * 36 + ref["spheres"] * 16) / m + RAY_BYTES
+    return {"sample": f"{n} camera rays at random pixels and {m - n} cosine secondary rays from their hits",
+            "ours": {"nodes_per_ray": round(nodes / m, 3), "prims_per_ray": round(prims / m, 3),
+                     "bytes_per_ray": round(ours, 1), "layout": "80-byte wide nodes, 48-byte primitives"},
+            "reference": {"node_records_per_ray": round(ref["nodes"] / m, 2), "faces_per_ray": round(ref["faces"] / m, 2),
+                          "sphere_tests_per_ray": round(ref["spheres"] / m, 2), "bytes_per_ray": round(theirs, 1),
+                          "layout": "36-byte binary nodes, 36-byte faces (its own BVH walk, counted by oracle/_ref/cr_ref work)"},
+            "ratio": round(theirs / ours, 2)}
+
+
 def reference_config0(repeats=3):
     """The reference's CPUMulticoreTracer::execute on the whole small box scene
     (256x256 at 64 spp, depth 8, 20 triangles + 2 spheres): the one
@@ -800,6 +859,7 @@ def run_ours(args):
                "includes": "scene upload, GPU BVH build, render, film copy to host"}
 
     cpu = None
+    layout = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
@@ -807,6 +867,7 @@ def run_ours(args):
             cpu = {"value": round(rate, 4), "unit": "Msamples/s", "cores": cores, "kind": "reference",
                    "sample": f"{WIDTH}x{HEIGHT} at {args.ref_spp} spp ({samples} paths) of the same scene, "
                              f"{sec:.1f} s of CPU time"}
+            layout = layout_comparison(scene, desc, path)
         else:
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/cr_ref not built"}
@@ -870,7 +931,10 @@ def run_ours(args):
                                   "peak": round(fp32_tflops, 2), "unit": "TFLOP/s",
                                   "frac": round(ext_flops / (ext_launch_ms / 1e3) / 1e12 / fp32_tflops, 4),
                                   "peak_source": "measured in this run (cr_measure_peaks: FMA chains)",
-                                  "flops_per_unit": "96 per wide node (8 slab tests) + 40 per triangle test"}},
+                                  "flops_per_unit": "96 per wide node (8 slab tests) + 40 per triangle test"},
+                         "reference_layout": (dict(layout, gbs_at_this_ray_rate=round(
+                             layout["reference"]["bytes_per_ray"] * cst.rays_extend / max(cst.extend_launches, 1)
+                             / (ext_launch_ms / 1e3) / 1e9, 1)) if layout else None)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,

@@ -145,6 +145,7 @@ def lib():
             "cr_guide_forward_tc": (I, [P, P, U64, P]), "cr_guide_gradients_tc": (I, [P, P, U64, P, P, P]),
             "cr_batch_create": (I, [P, U32, U32, C.c_int32, P, P]), "cr_batch_autotune": (I, [P, P]),
             "cr_batch_set_tuning": (I, [P, P]), "cr_trim_memory": (I, []),
+            "cr_trace_work": (I, [P, P, U64, I, P]),
             "cr_batch_render": (I, [P, U64, P]), "cr_batch_destroy": (None, [P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
@@ -282,6 +283,14 @@ class Scene:
         hits = np.zeros(len(rays), HIT_DTYPE)
         _check(lib().cr_trace_rays(self.h, _p(rays), len(rays), _p(hits), int(bool(any_hit))))
         return hits
+
+    def trace_work(self, rays, any_hit=False):
+        """cr_trace_work: (wide nodes fetched, primitives tested) summed over
+        the rays (n, 7) {o, d, tmax}."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        w = np.zeros(2, np.uint64)
+        _check(lib().cr_trace_work(self.h, _p(rays), len(rays), int(bool(any_hit)), _p(w)))
+        return int(w[0]), int(w[1])
 
     def trace_device(self, rays_ptr, n, hits_ptr, any_hit=False, stream=0):
         _check(lib().cr_trace_rays_device(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr),

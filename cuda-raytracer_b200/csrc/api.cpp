@@ -1730,6 +1730,36 @@ int cr_trace_rays( cr_scene *s, const float *rays, uint64_t n, cr_hit *hits, int
 	} );
 }
 
+int cr_trace_work( cr_scene *s, const float *rays, uint64_t n, int any_hit, uint64_t work[ 2 ] )
+{
+	return guarded( [&] {
+		if ( !s || !work || ( n && !rays ) ) fail( CR_ERR_INVALID, "null argument" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		work[ 0 ] = work[ 1 ] = 0;
+		if ( !n ) return;
+		cudaStream_t st = s->stream;
+		float *dr = nullptr;
+		cr_hit *dh = nullptr;
+		unsigned long long *dw = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&dr, sizeof( float ) * 7 * n, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dh, sizeof( cr_hit ) * n, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dw, sizeof( unsigned long long ) * 2, st ), "cudaMalloc" );
+		cuda_check( cudaMemsetAsync( dw, 0, sizeof( unsigned long long ) * 2, st ), "memset" );
+		cuda_check( cudaMemcpyAsync( dr, rays, sizeof( float ) * 7 * n, cudaMemcpyHostToDevice, st ), "upload" );
+		launch_trace( dev_scene( s ), dr, n, any_hit, dh, s->err.p, st, dw );
+		unsigned long long w[ 2 ];
+		cuda_check( cudaMemcpyAsync( w, dw, sizeof w, cudaMemcpyDeviceToHost, st ), "download" );
+		cudaFreeAsync( dr, st );
+		cudaFreeAsync( dh, st );
+		cudaFreeAsync( dw, st );
+		cuda_check( cudaStreamSynchronize( st ), "trace" );
+		uint32_t e = 0;
+		cuda_check( cudaMemcpy( &e, s->err.p, 4, cudaMemcpyDeviceToHost ), "error word" );
+		if ( e ) fail( CR_ERR_DEVICE, "a traversal kernel reported error flags " + std::to_string( e ) );
+		work[ 0 ] = w[ 0 ], work[ 1 ] = w[ 1 ];
+	} );
+}
+
 int cr_render_device( cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sq, uint32_t *d_cnt,
 					  void *stream, cr_stats *stats )
 {

@@ -1959,7 +1959,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 }
 
 void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit, cr_hit *out, uint32_t *err,
-				   cudaStream_t st )
+				   cudaStream_t st, unsigned long long *work )
 {
 	if ( !n ) return;
 	if ( n >= ( 1ull << 32 ) - 64 ) throw std::runtime_error( "too many rays in one query" );
@@ -1967,8 +1967,15 @@ void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hi
 	check( cudaMemsetAsync( err + 1, 0, sizeof( uint32_t ), st ), "trace cursor" );
 	int g = int( std::min<uint64_t>( ( n + 127 ) / 128, uint64_t( sm_count() ) * 8 ) );
 	QueryIO io{ rays, out, sc.tris, sc.attrs, sc.spheres, sc.prim_first };
-	if ( any_hit )
+	// with `work` (2 counters, added to): the counting build, nodes and primitives tested
+	if ( any_hit && work )
+		k_traverse<QueryIO, true, true><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, work,
+																QUERY_REFILL_MIN, EXT_TRI_VOTE );
+	else if ( any_hit )
 		k_traverse<QueryIO, true, false><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,
+																 QUERY_REFILL_MIN, EXT_TRI_VOTE );
+	else if ( work )
+		k_traverse<QueryIO, false, true><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, work,
 																 QUERY_REFILL_MIN, EXT_TRI_VOTE );
 	else
 		k_traverse<QueryIO, false, false><<<g, TRAVERSE_THREADS, 0, st>>>( sc, io, nullptr, uint32_t( n ), err + 1, err, nullptr,

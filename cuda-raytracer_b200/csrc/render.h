@@ -157,7 +157,7 @@ uint32_t build_batch_graph( const BatchDev &bd, const BatchJobDev *jobs, uint32_
 							WaveBuffers &wb, cudaStream_t st, cudaGraph_t *out );
 
 void launch_trace( const DevScene &sc, const float *rays, uint64_t n, int any_hit,
-				   cr_hit *out, uint32_t *err, cudaStream_t st );
+				   cr_hit *out, uint32_t *err, cudaStream_t st, unsigned long long *work = nullptr );
 
 void launch_bsdf_eval( int estimator, const DevShader &sh, const float *wo, const float *wi, uint64_t n, float *f,
 					   float *pdf, cudaStream_t st );

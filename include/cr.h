@@ -256,6 +256,13 @@ int cr_light_table(const cr_scene *s, uint32_t light, float *out, float *pdf);
  * rays: n x {o.x,o.y,o.z, d.x,d.y,d.z, tmax} floats (tmax <= 0 or inf: none).
  * Host buffers; copies are part of the call. */
 int cr_trace_rays(cr_scene *s, const float *rays, uint64_t n, cr_hit *hits, int any_hit);
+/* No counterpart in the reference.  The traversal work of the same queries:
+ * work[0] = wide-BVH nodes fetched (80 bytes each), work[1] = primitives
+ * tested (48-byte records), summed over the n rays (the counting build of the
+ * traversal kernel; the hits are discarded).  With the reference's own work
+ * on the same rays (binary nodes of 36 bytes, faces of 36 bytes) it gives
+ * the bytes per query of both layouts. */
+int cr_trace_work(cr_scene *s, const float *rays, uint64_t n, int any_hit, uint64_t work[2]);
 /* Mesh::samples and Mesh::pdf (src/core/primitive/mesh.hpp:58-84) handed over
  * from a reference Scene: replaces the 1024-point light table (points
  * 1024 x {p.xyz, n.xyz}) and the area pdf that the reference estimator's

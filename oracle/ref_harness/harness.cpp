@@ -18,6 +18,16 @@
 //   trace  <scene.json> <rays.f32> <out.hits>
 //       closest hit per ray over Scene::primitives with the reference's
 //       per-primitive intersect (src/core/meta/scene.hpp:35-55).
+//   work   <scene.json> <rays.f32>
+//       the reference's traversal work on the rays (as for trace), printed as
+//       one JSON line: for every ray, Scene::intersect(Ray) (scene.hpp:35-55)
+//       asks every primitive; a mesh walks its own BVH as Mesh::intersect(Ray)
+//       does (src/core/primitive/mesh.cu:200-267: depth first, both children's
+//       boxes tested with the reference's Ray::intersect_bbox at every step,
+//       every face of a reached leaf tested, no pruning by distance).  The
+//       walk is restated here over the mesh's own BVHNode and Face arrays to
+//       count what it reads: node records (36 bytes), faces (36 bytes) and
+//       sphere tests.
 //   occlude <scene.json> <segs.f32> <out.u8>
 //       Scene::intersect(Seg) (src/core/meta/scene.hpp:57-67) per segment.
 //   lights <scene.json> <out.lights>
@@ -413,6 +423,62 @@ int cmd_trace( int argc, char **argv )
 	return 0;
 }
 
+// Mesh::intersect(Ray)'s walk (mesh.cu:200-267), counting the node records
+// and faces it reads; the box test is the reference's own.
+void mesh_work( const Mesh &m, const Ray &ray, uint64_t &nodes, uint64_t &faces )
+{
+	if ( !m.bvh.size() ) return;
+	std::vector<uint32_t> stack{ 0 };
+	++nodes;  // the root's record (its offset)
+	while ( !stack.empty() )
+	{
+		uint32_t i = stack.back();
+		stack.pop_back();
+		bool reached = true;
+		while ( uint32_t offset = m.bvh[ i ].offset )
+		{
+			nodes += 2;  // both children's boxes
+			const bool left = ray.intersect_bbox( m.bvh[ i + 1 ].vmin, m.bvh[ i + 1 ].vmax );
+			const bool right = ray.intersect_bbox( m.bvh[ i + offset ].vmin, m.bvh[ i + offset ].vmax );
+			if ( !left && !right )
+			{
+				reached = false;
+				break;
+			}
+			if ( left && right ) stack.push_back( i + offset );
+			i = left ? i + 1 : i + offset;
+		}
+		if ( reached ) faces += m.bvh[ i ].end - m.bvh[ i ].begin;
+	}
+}
+
+int cmd_work( int argc, char **argv )
+{
+	if ( argc < 4 ) return 1;
+	Loaded L;
+	load( argv[ 2 ], L, 0x330E );
+	auto rays = read_f32( argv[ 3 ] );
+	const size_t n = rays.size() / 7;
+	uint64_t nodes = 0, faces = 0, spheres = 0;
+	for ( size_t r = 0; r < n; ++r )
+	{
+		const float *x = &rays[ 7 * r ];
+		Ray ray;
+		ray.o = float3{ x[ 0 ], x[ 1 ], x[ 2 ] };
+		ray.d = normalized_float3( float3{ x[ 3 ], x[ 4 ], x[ 5 ] } );
+		for ( size_t p = 0; p < L.scene->primitives.size(); ++p )
+		{
+			if ( auto *mesh = dynamic_cast<const Mesh *>( &*L.scene->primitives[ p ] ) )
+				mesh_work( *mesh, ray, nodes, faces );
+			else
+				++spheres;
+		}
+	}
+	std::printf( "{\"rays\": %zu, \"nodes\": %llu, \"faces\": %llu, \"spheres\": %llu}\n", n,
+				 (unsigned long long)nodes, (unsigned long long)faces, (unsigned long long)spheres );
+	return 0;
+}
+
 int cmd_occlude( int argc, char **argv )
 {
 	if ( argc < 5 ) return 1;
@@ -638,6 +704,7 @@ int main( int argc, char **argv )
 	{
 		if ( cmd == "render" ) rc = cmd_render( argc, argv );
 		else if ( cmd == "trace" ) rc = cmd_trace( argc, argv );
+		else if ( cmd == "work" ) rc = cmd_work( argc, argv );
 		else if ( cmd == "occlude" ) rc = cmd_occlude( argc, argv );
 		else if ( cmd == "lights" ) rc = cmd_lights( argc, argv );
 		else if ( cmd == "bench" ) rc = cmd_bench( argc, argv );
