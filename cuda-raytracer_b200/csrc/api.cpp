@@ -1089,45 +1089,43 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	} src_guard{ d_src, st };
 	s->attrs.alloc( 3 * nt );
 	float lo[ 3 ] = { INFINITY, INFINITY, INFINITY }, hi[ 3 ] = { -INFINITY, -INFINITY, -INFINITY };
+	if ( nt )
 	{
-		if ( nt )
+		size_t nv_all = 0;
+		for ( const HostMesh &m : s->meshes ) nv_all += m.v.size() / 3;
+		float *d_v = nullptr, *d_n = nullptr, *d_b = nullptr;
+		uint32_t *d_idx = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&d_v, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
+		StreamFree v_guard{ d_v, st };
+		cuda_check( cudaMallocAsync( (void **)&d_n, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
+		StreamFree n_guard{ d_n, st };
+		cuda_check( cudaMallocAsync( (void **)&d_idx, sizeof( uint32_t ) * 3 * nt, st ), "cudaMalloc" );
+		StreamFree idx_guard{ d_idx, st };
+		cuda_check( cudaMallocAsync( (void **)&d_b, sizeof( float ) * 6, st ), "cudaMalloc" );
+		StreamFree b_guard{ d_b, st };
+		const float b0[ 6 ] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
+		cuda_check( cudaMemcpyAsync( d_b, b0, sizeof b0, cudaMemcpyHostToDevice, st ), "upload" );
+		size_t vo = 0, io = 0;
+		for ( size_t p = 0; p < s->prims.size(); ++p )
 		{
-			size_t nv_all = 0;
-			for ( const HostMesh &m : s->meshes ) nv_all += m.v.size() / 3;
-			float *d_v = nullptr, *d_n = nullptr, *d_b = nullptr;
-			uint32_t *d_idx = nullptr;
-			cuda_check( cudaMallocAsync( (void **)&d_v, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
-			StreamFree v_guard{ d_v, st };
-			cuda_check( cudaMallocAsync( (void **)&d_n, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
-			StreamFree n_guard{ d_n, st };
-			cuda_check( cudaMallocAsync( (void **)&d_idx, sizeof( uint32_t ) * 3 * nt, st ), "cudaMalloc" );
-			StreamFree idx_guard{ d_idx, st };
-			cuda_check( cudaMallocAsync( (void **)&d_b, sizeof( float ) * 6, st ), "cudaMalloc" );
-			StreamFree b_guard{ d_b, st };
-			const float b0[ 6 ] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
-			cuda_check( cudaMemcpyAsync( d_b, b0, sizeof b0, cudaMemcpyHostToDevice, st ), "upload" );
-			size_t vo = 0, io = 0;
-			for ( size_t p = 0; p < s->prims.size(); ++p )
-			{
-				const HostPrim &hp = s->prims[ p ];
-				if ( hp.kind != 0 ) continue;
-				const HostMesh &m = s->meshes[ hp.index ];
-				const size_t nv = m.v.size() / 3, nm = m.idx.size() / 3;
-				if ( !nm ) continue;
-				cuda_check( cudaMemcpyAsync( d_v + 3 * vo, m.v.data(), sizeof( float ) * 3 * nv, cudaMemcpyHostToDevice, st ), "upload" );
-				cuda_check( cudaMemcpyAsync( d_n + 3 * vo, m.n.data(), sizeof( float ) * 3 * nv, cudaMemcpyHostToDevice, st ), "upload" );
-				cuda_check( cudaMemcpyAsync( d_idx + 3 * io, m.idx.data(), sizeof( uint32_t ) * 3 * nm, cudaMemcpyHostToDevice, st ),
-							"upload" );
-				FlatMesh fm{ d_v + 3 * vo, d_n + 3 * vo, d_idx + 3 * io, uint32_t( nm ), prim_first[ p ], m.shader, int( p ),
-							 prim_light[ p ] };
-				flatten_mesh( fm, d_src, s->attrs.p, d_b, st );
-				vo += nv, io += nm;
-			}
-			float b[ 6 ];
-			cuda_check( cudaMemcpyAsync( b, d_b, sizeof b, cudaMemcpyDeviceToHost, st ), "bounds" );
-			cuda_check( cudaStreamSynchronize( st ), "flatten" );
-			for ( int a = 0; a < 3; ++a ) lo[ a ] = b[ a ], hi[ a ] = b[ 3 + a ];
+			const HostPrim &hp = s->prims[ p ];
+			if ( hp.kind != 0 ) continue;
+			const HostMesh &m = s->meshes[ hp.index ];
+			const size_t nv = m.v.size() / 3, nm = m.idx.size() / 3;
+			if ( !nm ) continue;
+			cuda_check( cudaMemcpyAsync( d_v + 3 * vo, m.v.data(), sizeof( float ) * 3 * nv, cudaMemcpyHostToDevice, st ), "upload" );
+			cuda_check( cudaMemcpyAsync( d_n + 3 * vo, m.n.data(), sizeof( float ) * 3 * nv, cudaMemcpyHostToDevice, st ), "upload" );
+			cuda_check( cudaMemcpyAsync( d_idx + 3 * io, m.idx.data(), sizeof( uint32_t ) * 3 * nm, cudaMemcpyHostToDevice, st ),
+						"upload" );
+			FlatMesh fm{ d_v + 3 * vo, d_n + 3 * vo, d_idx + 3 * io, uint32_t( nm ), prim_first[ p ], m.shader, int( p ),
+						 prim_light[ p ] };
+			flatten_mesh( fm, d_src, s->attrs.p, d_b, st );
+			vo += nv, io += nm;
 		}
+		float b[ 6 ];
+		cuda_check( cudaMemcpyAsync( b, d_b, sizeof b, cudaMemcpyDeviceToHost, st ), "bounds" );
+		cuda_check( cudaStreamSynchronize( st ), "flatten" );
+		for ( int a = 0; a < 3; ++a ) lo[ a ] = b[ a ], hi[ a ] = b[ 3 + a ];
 	}
 	std::vector<DevSphere> ds;
 	std::vector<float4> sph_src;
