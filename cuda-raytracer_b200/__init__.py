@@ -249,7 +249,7 @@ class Scene:
                              max_leaf=build.get("max_leaf", 3), cost_node=build.get("cost_node", 1.2),
                              cost_tri=build.get("cost_tri", 1.0), collapse=build.get("collapse", 0),
                              wide_cost_node=build.get("wide_cost_node", 1.0),
-                             wide_cost_tri=build.get("wide_cost_tri", 0.3))
+                             wide_cost_tri=build.get("wide_cost_tri", 0.6))
             _check(lib().cr_scene_set_build(s.h, C.byref(bc)))
         _check(lib().cr_scene_commit(s.h, light_seed, None))
         return s

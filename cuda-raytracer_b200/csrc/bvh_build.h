@@ -31,7 +31,7 @@ struct BuildParams
 	// with the costs of a wide-node visit and a triangle test; false: greedy
 	// (open the largest child first)
 	bool dp_collapse = true;
-	float dp_cost_node = 1.0f, dp_cost_tri = 0.3f;
+	float dp_cost_node = 1.0f, dp_cost_tri = 0.6f;
 };
 void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t st,
 					 const BuildParams &bp = BuildParams() );

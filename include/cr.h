@@ -222,7 +222,7 @@ int cr_scene_set_kernel(cr_scene *s, const char *name);
  *                programming over the SAH (PLOC trees) [default], or
  *                CR_COLLAPSE_GREEDY: open the largest child first
  *   wide_cost_node, wide_cost_tri  SAH costs of a wide-node visit and a
- *                triangle test in that plan [1, 0.3] */
+ *                triangle test in that plan [1, 0.6] */
 #define CR_BUILD_PLOC 0
 #define CR_BUILD_LBVH 1
 #define CR_COLLAPSE_SAH 0
