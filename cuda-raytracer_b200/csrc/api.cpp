@@ -1076,7 +1076,7 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	const uint64_t n_prims = nt + n_sph;
 	if ( n_prims >= ( 1ull << 31 ) ) fail( CR_ERR_INVALID, "too many primitives" );
 	float4 *d_src = nullptr;
-	if ( n_prims ) cuda_check( cudaMallocAsync( (void **)&d_src, sizeof( float4 ) * 3 * n_prims, st ), "cudaMalloc" );
+	if ( n_prims ) cuda_check( cudaMallocAsync( (void **)&d_src, sizeof( float4 ) * 3 * n_prims, device_pool(), st ), "cudaMalloc" );
 	// the builder's input lives until the end of the commit, whichever way it ends
 	struct StreamFree
 	{
@@ -1095,13 +1095,13 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 		for ( const HostMesh &m : s->meshes ) nv_all += m.v.size() / 3;
 		float *d_v = nullptr, *d_n = nullptr, *d_b = nullptr;
 		uint32_t *d_idx = nullptr;
-		cuda_check( cudaMallocAsync( (void **)&d_v, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_v, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), device_pool(), st ), "cudaMalloc" );
 		StreamFree v_guard{ d_v, st };
-		cuda_check( cudaMallocAsync( (void **)&d_n, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_n, sizeof( float ) * 3 * std::max<size_t>( nv_all, 1 ), device_pool(), st ), "cudaMalloc" );
 		StreamFree n_guard{ d_n, st };
-		cuda_check( cudaMallocAsync( (void **)&d_idx, sizeof( uint32_t ) * 3 * nt, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_idx, sizeof( uint32_t ) * 3 * nt, device_pool(), st ), "cudaMalloc" );
 		StreamFree idx_guard{ d_idx, st };
-		cuda_check( cudaMallocAsync( (void **)&d_b, sizeof( float ) * 6, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_b, sizeof( float ) * 6, device_pool(), st ), "cudaMalloc" );
 		StreamFree b_guard{ d_b, st };
 		const float b0[ 6 ] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
 		cuda_check( cudaMemcpyAsync( d_b, b0, sizeof b0, cudaMemcpyHostToDevice, st ), "upload" );
@@ -1514,7 +1514,7 @@ const char *cr_version( void ) { return "cr_b200 1.0 (sm_100a)"; }
 
 int cr_trim_memory( void )
 {
-	return guarded( [&] { trim_wave_pools(); } );
+	return guarded( [&] { trim_device_pools(); } );
 }
 
 int cr_scene_create_empty( cr_scene **out )
@@ -1714,8 +1714,8 @@ int cr_trace_rays( cr_scene *s, const float *rays, uint64_t n, cr_hit *hits, int
 		cudaStream_t st = s->stream;
 		float *dr = nullptr;
 		cr_hit *dh = nullptr;
-		cuda_check( cudaMallocAsync( (void **)&dr, sizeof( float ) * 7 * n, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&dh, sizeof( cr_hit ) * n, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dr, sizeof( float ) * 7 * n, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dh, sizeof( cr_hit ) * n, device_pool(), st ), "cudaMalloc" );
 		cuda_check( cudaMemcpyAsync( dr, rays, sizeof( float ) * 7 * n, cudaMemcpyHostToDevice, st ), "upload" );
 		launch_trace( dev_scene( s ), dr, n, any_hit, dh, s->err.p, st );
 		cuda_check( cudaMemcpyAsync( hits, dh, sizeof( cr_hit ) * n, cudaMemcpyDeviceToHost, st ), "download" );
@@ -1739,9 +1739,9 @@ int cr_trace_work( cr_scene *s, const float *rays, uint64_t n, int any_hit, uint
 		float *dr = nullptr;
 		cr_hit *dh = nullptr;
 		unsigned long long *dw = nullptr;
-		cuda_check( cudaMallocAsync( (void **)&dr, sizeof( float ) * 7 * n, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&dh, sizeof( cr_hit ) * n, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&dw, sizeof( unsigned long long ) * 2, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dr, sizeof( float ) * 7 * n, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dh, sizeof( cr_hit ) * n, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&dw, sizeof( unsigned long long ) * 2, device_pool(), st ), "cudaMalloc" );
 		cuda_check( cudaMemsetAsync( dw, 0, sizeof( unsigned long long ) * 2, st ), "memset" );
 		cuda_check( cudaMemcpyAsync( dr, rays, sizeof( float ) * 7 * n, cudaMemcpyHostToDevice, st ), "upload" );
 		launch_trace( dev_scene( s ), dr, n, any_hit, dh, s->err.p, st, dw );
@@ -1776,9 +1776,9 @@ int cr_render( cr_scene *s, const cr_render_desc *desc, double *film, cr_stats *
 		size_t npx = size_t( r.cfg.ww ) * r.cfg.wh;
 		double *sum, *sq;
 		uint32_t *cnt;
-		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, device_pool(), st ), "cudaMalloc" );
 		cuda_check( cudaMemsetAsync( sum, 0, npx * 24, st ), "memset" );
 		cuda_check( cudaMemsetAsync( sq, 0, npx * 24, st ), "memset" );
 		cuda_check( cudaMemsetAsync( cnt, 0, npx * 4, st ), "memset" );
@@ -1827,15 +1827,15 @@ int cr_render_profile( cr_scene *s, const cr_render_desc *desc, uint32_t depth, 
 		};
 		try
 		{
-			cuda_check( cudaMallocAsync( (void **)&pd.slices, sizeof( cr_profile_slice ) * n, st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&pd.slices, sizeof( cr_profile_slice ) * n, device_pool(), st ), "cudaMalloc" );
 			cuda_check( cudaMemsetAsync( pd.slices, 0, sizeof( cr_profile_slice ) * n, st ), "memset" );
 			// at depth 0 no record is written; one keeps the buffer valid
 			const size_t nb = std::max<size_t>( n * depth, 1 );
-			cuda_check( cudaMallocAsync( (void **)&pd.bounces, sizeof( cr_profile_bounce ) * nb, st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&pd.bounces, sizeof( cr_profile_bounce ) * nb, device_pool(), st ), "cudaMalloc" );
 			cuda_check( cudaMemsetAsync( pd.bounces, 0, sizeof( cr_profile_bounce ) * nb, st ), "memset" );
-			cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
-			cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
-			cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, device_pool(), st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, device_pool(), st ), "cudaMalloc" );
+			cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, device_pool(), st ), "cudaMalloc" );
 			cuda_check( cudaMemsetAsync( sum, 0, npx * 24, st ), "memset" );
 			cuda_check( cudaMemsetAsync( sq, 0, npx * 24, st ), "memset" );
 			cuda_check( cudaMemsetAsync( cnt, 0, npx * 4, st ), "memset" );
@@ -1940,9 +1940,9 @@ int cr_autotune( cr_scene *s, const cr_render_desc *desc, void *stream, cr_tunin
 		size_t npx = size_t( cfg.ww ) * cfg.wh;
 		double *sum, *sq;
 		uint32_t *cnt;
-		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, device_pool(), st ), "cudaMalloc" );
 		uint32_t tried = 0, shade = 128, svote = 4, srefill = 0;
 		bool bin = false;
 		auto rate = [&]( uint32_t wave, uint32_t refill, int blocks ) {
@@ -2279,9 +2279,9 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 		uint64_t npx = b->jobs.back().first_pixel + uint64_t( b->jobs.back().width ) * b->jobs.back().height;
 		double *sum = nullptr, *sq = nullptr;
 		uint32_t *cnt = nullptr;
-		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, device_pool(), st ), "cudaMalloc" );
 		std::vector<BatchJobDev> jobs;
 		std::vector<DevScene> scenes;
 		batch_tables( b, 16, sum, sq, cnt, jobs, scenes );
@@ -2289,8 +2289,8 @@ int cr_batch_autotune( cr_batch *b, cr_tuning *out )
 		const uint64_t total = jobs.back().first_sample + uint64_t( jobs.back().width ) * jobs.back().height * jobs.back().spp;
 		DevScene *d_scenes = nullptr;
 		BatchJobDev *d_jobs = nullptr;
-		cuda_check( cudaMallocAsync( (void **)&d_scenes, sizeof( DevScene ) * n, st ), "cudaMalloc" );
-		cuda_check( cudaMallocAsync( (void **)&d_jobs, sizeof( BatchJobDev ) * n, st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_scenes, sizeof( DevScene ) * n, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&d_jobs, sizeof( BatchJobDev ) * n, device_pool(), st ), "cudaMalloc" );
 		upload( d_scenes, scenes.data(), sizeof( DevScene ) * n, st );
 		upload( d_jobs, jobs.data(), sizeof( BatchJobDev ) * n, st );
 		BatchDev bd{ d_scenes, d_jobs, b->d_seed, n };

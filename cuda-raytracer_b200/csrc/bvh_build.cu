@@ -610,20 +610,20 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	WorkItem *wa, *wb;
 	uint32_t *cnt;  // [0] nodes [1] tris [2] depth [3] n_work a [4] n_work b
 	size_t n_b = 2 * size_t( n ) - 1;
-	check( cudaMallocAsync( &blo, sizeof( float4 ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &bhi, sizeof( float4 ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &cb, sizeof( float ) * 6, st ), "bvh alloc" );
-	check( cudaMallocAsync( &keys, sizeof( uint64_t ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &keys2, sizeof( uint64_t ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &vals, sizeof( uint32_t ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &vals2, sizeof( uint32_t ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &bn, sizeof( BNode ) * n_b, st ), "bvh alloc" );
-	check( cudaMallocAsync( &flags, sizeof( int ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &wa, sizeof( WorkItem ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &wb, sizeof( WorkItem ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &cnt, sizeof( uint32_t ) * 8, st ), "bvh alloc" );
-	check( cudaMallocAsync( &out.nodes, sizeof( WNode ) * n, st ), "bvh alloc" );
-	check( cudaMallocAsync( &out.tris, sizeof( float4 ) * 3 * n, st ), "bvh alloc" );
+	check( cudaMallocAsync( &blo, sizeof( float4 ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &bhi, sizeof( float4 ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &cb, sizeof( float ) * 6, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &keys, sizeof( uint64_t ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &keys2, sizeof( uint64_t ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &vals, sizeof( uint32_t ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &vals2, sizeof( uint32_t ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &bn, sizeof( BNode ) * n_b, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &flags, sizeof( int ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &wa, sizeof( WorkItem ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &wb, sizeof( WorkItem ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &cnt, sizeof( uint32_t ) * 8, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &out.nodes, sizeof( WNode ) * n, device_pool(), st ), "bvh alloc" );
+	check( cudaMallocAsync( &out.tris, sizeof( float4 ) * 3 * n, device_pool(), st ), "bvh alloc" );
 
 	float init[ 6 ] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
 	check( cudaMemcpyAsync( cb, init, sizeof init, cudaMemcpyHostToDevice, st ), "bvh init" );
@@ -636,7 +636,7 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 	size_t temp = 0;
 	check( cub::DeviceRadixSort::SortPairs( nullptr, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
 	void *dtemp;
-	check( cudaMallocAsync( &dtemp, temp, st ), "bvh alloc" );
+	check( cudaMallocAsync( &dtemp, temp, device_pool(), st ), "bvh alloc" );
 	check( cub::DeviceRadixSort::SortPairs( dtemp, temp, keys, keys2, vals, vals2, int( n ), 0, 63, st ), "sort" );
 	int root_id = 0;
 	const uint32_t *order = vals2;
@@ -660,7 +660,7 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 		size_t scan_temp = 0;
 		check( cub::DeviceScan::ExclusiveSum( nullptr, scan_temp, keep, pos, int( n ), st ), "scan" );
 		void *stemp;
-		check( cudaMallocAsync( &stemp, scan_temp, st ), "bvh alloc" );
+		check( cudaMallocAsync( &stemp, scan_temp, device_pool(), st ), "bvh alloc" );
 		std::vector<int> round_base;  // first internal id of each merge round
 		int m = int( n ), created = 0;
 		while ( m > 1 )
@@ -698,8 +698,8 @@ void build_wide_bvh( const float4 *d_src, uint32_t n, WideBvh &out, cudaStream_t
 		if ( bp.dp_collapse )
 		{
 			// collapse plan, bottom-up in creation order (children come from earlier rounds)
-			check( cudaMallocAsync( &dp_cost, sizeof( float ) * 8 * n_b, st ), "bvh alloc" );
-			check( cudaMallocAsync( &dp_dec, 8 * n_b, st ), "bvh alloc" );
+			check( cudaMallocAsync( &dp_cost, sizeof( float ) * 8 * n_b, device_pool(), st ), "bvh alloc" );
+			check( cudaMallocAsync( &dp_dec, 8 * n_b, device_pool(), st ), "bvh alloc" );
 			k_dp_leaves<<<( n + tb - 1 ) / tb, tb, 0, st>>>( int( n ), bn, dp_cost, dp_dec, bp );
 			for ( size_t r = 0; r + 1 < round_base.size(); ++r )
 			{

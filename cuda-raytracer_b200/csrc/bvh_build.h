@@ -14,6 +14,10 @@ struct WideBvh
 	uint32_t n_nodes = 0, n_tris = 0, depth = 0;
 };
 
+// The library's memory pool of the current device (render.cu), which keeps
+// freed memory mapped: the builder's scratch and output come from it.
+cudaMemPool_t device_pool();
+
 // d_src: 3 float4 (v0, v1, v2) per triangle in global order, on the device.
 // Allocates out.nodes / out.tris with cudaMallocAsync on `st`; throws
 // std::runtime_error on failure.  Synchronises `st` once per tree level.

@@ -1412,7 +1412,7 @@ void check( cudaError_t e, const char *what )
 template <typename T>
 void alloc( T *&p, size_t n, cudaStream_t st )
 {
-	check( cudaMallocFromPoolAsync( (void **)&p, sizeof( T ) * std::max<size_t>( n, 1 ), wave_pool(), st ), "wave alloc" );
+	check( cudaMallocFromPoolAsync( (void **)&p, sizeof( T ) * std::max<size_t>( n, 1 ), device_pool(), st ), "wave alloc" );
 }
 
 struct EventPool
@@ -1452,16 +1452,18 @@ int current_device()
 }
 }  // namespace
 
-// One memory pool per device for the wave state, whose release threshold keeps
-// freed memory mapped: the next scene's (or the next wave size's) buffers then
-// reuse it instead of mapping gigabytes of device memory again.  trim_wave_pools
-// (cr_trim_memory) hands the cached memory back.
+// One memory pool per device for the library's stream-ordered allocations (wave
+// state, the BVH build's scratch and output, scene upload staging, the films of
+// host-array calls), whose release threshold keeps freed memory mapped: the
+// next scene's or render's buffers then reuse it instead of mapping hundreds of
+// MB to gigabytes of device memory again.  trim_device_pools (cr_trim_memory)
+// hands the cached memory back.
 namespace
 {
 cudaMemPool_t g_pools[ MAX_DEVICES ] = {};
 }
 
-cudaMemPool_t wave_pool()
+cudaMemPool_t device_pool()
 {
 	const int dev = current_device();
 	if ( dev < 0 || dev >= MAX_DEVICES ) throw std::runtime_error( "device index out of range" );
@@ -1482,7 +1484,7 @@ cudaMemPool_t wave_pool()
 	return g_pools[ dev ];
 }
 
-void trim_wave_pools()
+void trim_device_pools()
 {
 	std::lock_guard<std::mutex> lock( g_dev_mutex );
 	for ( cudaMemPool_t pool : g_pools )

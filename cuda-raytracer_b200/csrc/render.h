@@ -125,8 +125,8 @@ struct StageTimes
 void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaStream_t st );
 // The current device's memory pool for wave state, and a hand-back of the
 // memory that the pools keep mapped.
-cudaMemPool_t wave_pool();
-void trim_wave_pools();
+cudaMemPool_t device_pool();
+void trim_device_pools();
 void free_wave( WaveBuffers &wb, cudaStream_t st );
 
 // Render the window into the film (device buffers, accumulated).  When

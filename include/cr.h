@@ -118,12 +118,13 @@ typedef struct cr_stats {
 const char *cr_last_error(void);
 /* Library version string. */
 const char *cr_version(void);
-/* No counterpart in the reference.  Wave state (the paths in flight of a
- * render) comes from a memory pool of the library's own per device, which
- * keeps freed memory mapped so that the next scene's renders reuse it: a
- * process holds up to its largest concurrent wave state (about 140 bytes per
- * path in flight) between renders.  This hands that cached memory back to
- * the device (scenes alive keep their own buffers). */
+/* No counterpart in the reference.  The library's stream-ordered device
+ * memory (wave state: about 140 bytes per path in flight; the BVH build's
+ * scratch; upload staging; the films of host-array calls) comes from a memory
+ * pool of its own per device, which keeps freed memory mapped so that the
+ * next scene or render reuses it: between calls a process holds up to its
+ * largest concurrent use.  This hands that cached memory back to the device
+ * (scenes alive keep their own buffers). */
 int cr_trim_memory(void);
 
 /* ------------------------------------------------------------------ scenes */
