@@ -2387,6 +2387,7 @@ int cr_batch_render( cr_batch *b, uint64_t seed_offset, cr_stats *stats )
 			batch_ensure_wave( b, c.wave_paths );
 			cuda_check( cudaStreamSynchronize( st ), "batch" );
 			BatchDev bd{ b->d_scenes, b->d_jobs, b->d_seed, n };
+			b->drop_graph();  // a graph left by a failed instantiation
 			b->graph_nodes = build_batch_graph( bd, b->jobs.data(), n, c, b->wave, st, &b->graph );
 			cuda_check( cudaGraphInstantiate( &b->exec, b->graph, 0 ), "graph instantiate" );
 		}
