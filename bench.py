@@ -867,7 +867,10 @@ def run_ours(args):
             cpu = {"value": round(rate, 4), "unit": "Msamples/s", "cores": cores, "kind": "reference",
                    "sample": f"{WIDTH}x{HEIGHT} at {args.ref_spp} spp ({samples} paths) of the same scene, "
                              f"{sec:.1f} s of CPU time"}
-            layout = layout_comparison(scene, desc, path)
+            try:
+                layout = layout_comparison(scene, desc, path)
+            except (subprocess.SubprocessError, OSError, ValueError) as e:  # a checker failure must not stop the bench
+                layout = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
         else:
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/cr_ref not built"}
@@ -932,7 +935,8 @@ def run_ours(args):
                                   "frac": round(ext_flops / (ext_launch_ms / 1e3) / 1e12 / fp32_tflops, 4),
                                   "peak_source": "measured in this run (cr_measure_peaks: FMA chains)",
                                   "flops_per_unit": "96 per wide node (8 slab tests) + 40 per triangle test"},
-                         "reference_layout": (dict(layout, gbs_at_this_ray_rate=round(
+                         "reference_layout": (layout if layout and "unavailable" in layout else
+                                              dict(layout, gbs_at_this_ray_rate=round(
                              layout["reference"]["bytes_per_ray"] * cst.rays_extend / max(cst.extend_launches, 1)
                              / (ext_launch_ms / 1e3) / 1e9, 1)) if layout else None)},
             "cpu_baseline": cpu,
