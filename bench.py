@@ -316,10 +316,11 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     Two plain runs: with the reference's Russian roulette (after bounce 3,
     the library's default for plain renders) and without roulette; the
     speed-up is taken against the faster of the two.  The guided run uses the
-    library's defaults for guided renders (no roulette, 600 training steps
-    front-loaded at 16 per wave); its guide first trains on renders into a
-    scratch film until the training budget is spent (clocked), so that the
-    measured film holds only samples of the trained guide."""
+    library's defaults for guided renders (no roulette, every vertex but the
+    last guided, 600 training steps front-loaded at 64 per wave); its guide
+    first trains on 2-spp renders into a scratch film until the training
+    budget is spent (clocked), so that the measured film holds only samples
+    of the trained guide."""
     import torch
     from cuda_raytracer_b200 import scenes
     res = 1024
@@ -347,10 +348,10 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     den = Rm * Rm + 1e-2
     del R
 
-    def timed(f, seed, guiding, rr_start):
+    def timed(f, seed, guiding, rr_start, spp=4):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        render(f, 4, seed, guiding, rr_start)
+        render(f, spp, seed, guiding, rr_start)
         e1.record()
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1)
@@ -362,7 +363,9 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
             budget = g.configure()["max_steps"]
             T = film()
             while g.info()["step"] < budget and ms < tmax_s * 1e3:
-                ms += timed(T, 500_000 + k, True, rr_start)
+                # 2 spp: a wave of 1024 x 1024 x 2 paths is exactly the 64 x 32,768
+                # paths a wave records, so every path rendered for training is used
+                ms += timed(T, 500_000 + k, True, rr_start, spp=2)
                 k += 1
             train_ms = ms
             del T
