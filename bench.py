@@ -572,7 +572,8 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
             T = film()
             while g.info()["step"] < budget and ms < tmax_s * 1e3:
                 e0.record()
-                render(T, step_spp, 500_000 + k, True)
+                # passes of about 64 x 32,768 paths: a wave's recorded paths, all of it
+                render(T, max(1, -(-(64 * 32768) // n)), 500_000 + k, True)
                 e1.record()
                 torch.cuda.synchronize(dev)
                 ms += e0.elapsed_time(e1)
