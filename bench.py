@@ -318,9 +318,9 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     speed-up is taken against the faster of the two.  The guided run uses the
     library's defaults for guided renders (no roulette, every vertex but the
     last guided, 600 training steps front-loaded at 64 per wave); its guide
-    first trains on 2-spp renders into a scratch film until the training
-    budget is spent (clocked), so that the measured film holds only samples
-    of the trained guide."""
+    first trains to its budget on 2-spp scratch passes (cr_guide_train,
+    clocked), so that the measured film holds only samples of the trained
+    guide."""
     import torch
     from cuda_raytracer_b200 import scenes
     res = 1024
@@ -348,10 +348,10 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     den = Rm * Rm + 1e-2
     del R
 
-    def timed(f, seed, guiding, rr_start, spp=4):
+    def timed(f, seed, guiding, rr_start):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        render(f, spp, seed, guiding, rr_start)
+        render(f, 4, seed, guiding, rr_start)
         e1.record()
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1)
@@ -359,16 +359,16 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     def run(guiding, rr_start=0):
         ms, k, train_ms = 0.0, 0, 0.0
         if guiding:
+            # cr_guide_train: passes of 1024 x 1024 x 2 paths, the 64 x 32,768
+            # paths a wave records, so every path rendered for training is used
             g = cr.Guide(sc).reset(seed=7)
-            budget = g.configure()["max_steps"]
-            T = film()
-            while g.info()["step"] < budget and ms < tmax_s * 1e3:
-                # 2 spp: a wave of 1024 x 1024 x 2 paths is exactly the 64 x 32,768
-                # paths a wave records, so every path rendered for training is used
-                ms += timed(T, 500_000 + k, True, rr_start, spp=2)
-                k += 1
-            train_ms = ms
-            del T
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            k = g.train(cr.render_desc(res, res, 1, max_bounce=MAX_BOUNCE, estimator=cr.MIS, seed=500_000,
+                                       guiding=True, rr_start=rr_start), stream=stream)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = train_ms = e0.elapsed_time(e1)
         F = film()
         spp, hit, err = 0, None, None
         while ms < tmax_s * 1e3:
@@ -539,7 +539,8 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
     the window at ref_spp; each run renders step_spp per call into one film,
     clocked by CUDA events, until the target or tmax_s (relMSE as in
     guided_vs_plain, the reference's own variance removed).  The guided run
-    first trains its guide to the budget on a scratch film (clocked)."""
+    first trains its guide to the budget on scratch passes of the window
+    (cr_guide_train, clocked)."""
     import torch
     x0, y0, x1, y1 = win
     n = (x1 - x0) * (y1 - y0)
@@ -566,20 +567,14 @@ def window_time_to_target(cr, scene, W, H, win, max_bounce, ref_spp, tmax_s, dev
     def run(guiding):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ms, spp, k, hit, err, train_ms = 0.0, 0, 0, None, None, 0.0
-        if guiding:  # train the guide to its budget on a scratch film first (clocked)
+        if guiding:  # train the guide to its budget on scratch passes of the window first (clocked)
             g = cr.Guide(scene).reset(seed=7)
-            budget = g.configure()["max_steps"]
-            T = film()
-            while g.info()["step"] < budget and ms < tmax_s * 1e3:
-                e0.record()
-                # passes of about 64 x 32,768 paths: a wave's recorded paths, all of it
-                render(T, max(1, -(-(64 * 32768) // n)), 500_000 + k, True)
-                e1.record()
-                torch.cuda.synchronize(dev)
-                ms += e0.elapsed_time(e1)
-                k += 1
-            train_ms = ms
-            del T
+            e0.record()
+            k = g.train(cr.render_desc(W, H, 1, max_bounce=max_bounce, estimator=cr.MIS, seed=500_000, guiding=True,
+                                       window=win), stream=stream)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = train_ms = e0.elapsed_time(e1)
         F = film()
         while ms < tmax_s * 1e3:
             e0.record()

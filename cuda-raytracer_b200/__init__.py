@@ -145,7 +145,7 @@ def lib():
             "cr_guide_forward_tc": (I, [P, P, U64, P]), "cr_guide_gradients_tc": (I, [P, P, U64, P, P, P]),
             "cr_batch_create": (I, [P, U32, U32, C.c_int32, P, P]), "cr_batch_autotune": (I, [P, P]),
             "cr_batch_set_tuning": (I, [P, P]), "cr_trim_memory": (I, []),
-            "cr_trace_work": (I, [P, P, U64, I, P]),
+            "cr_trace_work": (I, [P, P, U64, I, P]), "cr_guide_train": (I, [P, P, P, P]),
             "cr_batch_render": (I, [P, U64, P]), "cr_batch_destroy": (None, [P]),
             "cr_bsdf_eval": (I, [I, C.c_char_p, P, P, U64, P, P]),
             "cr_bsdf_sample": (I, [I, C.c_char_p, P, P, U64, P, P, P]),
@@ -339,6 +339,13 @@ class Guide:
     def reset(self, seed=1):
         _check(lib().cr_guide_reset(self.scene.h, seed))
         return self
+
+    def train(self, desc, stream=0):
+        """cr_guide_train: train the guide to its budget on scratch passes of
+        desc's image (each one wave recorded whole); returns the passes."""
+        n = C.c_uint32()
+        _check(lib().cr_guide_train(self.scene.h, C.byref(desc), C.c_void_p(stream), C.byref(n)))
+        return n.value
 
     def info(self):
         bmin, binv, sizes = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(3, np.uint32)

@@ -1758,6 +1758,51 @@ int cr_trace_work( cr_scene *s, const float *rays, uint64_t n, int any_hit, uint
 	} );
 }
 
+int cr_guide_train( cr_scene *s, const cr_render_desc *desc, void *stream, uint32_t *passes )
+{
+	return guarded( [&] {
+		if ( !s || !desc ) fail( CR_ERR_INVALID, "null argument" );
+		if ( !s->committed ) fail( CR_ERR_STATE, "scene not committed" );
+		GuideState &g = s->guide;
+		if ( g.max_steps == 0 ) fail( CR_ERR_INVALID, "the guide has no training budget (max_steps 0)" );
+		cr_render_desc d = *desc;
+		d.guiding = 1;
+		d.estimator = CR_ESTIMATOR_MIS;
+		uint32_t x0 = d.x0, y0 = d.y0, x1 = d.x1, y1 = d.y1;
+		if ( !x0 && !y0 && !x1 && !y1 ) x1 = d.width, y1 = d.height;
+		if ( x1 > d.width || y1 > d.height || x0 >= x1 || y0 >= y1 ) fail( CR_ERR_INVALID, "bad pixel window" );
+		const uint64_t npx = uint64_t( x1 - x0 ) * ( y1 - y0 );
+		// a pass of about one wave's recorded paths, recorded whole
+		const uint64_t want = uint64_t( g.steps_per_wave ) * g.train_paths;
+		d.spp = uint32_t( std::max<uint64_t>( 1, std::min<uint64_t>( ( want + npx - 1 ) / npx, 1u << 16 ) ) );
+		cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+		double *sum = nullptr, *sq = nullptr;
+		uint32_t *cnt = nullptr;
+		cuda_check( cudaMallocAsync( (void **)&sum, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&sq, npx * 24, device_pool(), st ), "cudaMalloc" );
+		cuda_check( cudaMallocAsync( (void **)&cnt, npx * 4, device_pool(), st ), "cudaMalloc" );
+		uint32_t k = 0;
+		try
+		{
+			// the first pass sets the guide up if it has none; every pass takes at
+			// least one step, so the loop ends within the budget's count
+			for ( uint32_t guard = 0; g.step < g.max_steps && guard < g.max_steps; ++guard, ++k )
+			{
+				render_device( s, &d, sum, sq, cnt, st, nullptr );
+				d.seed += 0x9E3779B97F4A7C15ull;
+			}
+		}
+		catch ( ... )
+		{
+			cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
+			throw;
+		}
+		cudaFreeAsync( sum, st ), cudaFreeAsync( sq, st ), cudaFreeAsync( cnt, st );
+		check_device_error( s, st );
+		if ( passes ) *passes = k;
+	} );
+}
+
 int cr_render_device( cr_scene *s, const cr_render_desc *desc, double *d_sum, double *d_sq, uint32_t *d_cnt,
 					  void *stream, cr_stats *stats )
 {

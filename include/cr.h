@@ -470,6 +470,14 @@ typedef struct cr_guide_config {
 } cr_guide_config;
 /* Apply `in` (when not NULL) and report the schedule in `out` (when not NULL). */
 int cr_guide_configure(cr_scene *s, const cr_guide_config *in, cr_guide_config *out);
+/* Trains the scene's guide to its budget (max_steps; a guide with none is
+ * refused) on guided MIS renders of desc's image or window into a scratch
+ * film that is then discarded, so that a later guided render of the image
+ * draws every sample with the trained, frozen guide.  Each pass has about
+ * steps_per_wave x train_paths paths (desc->spp is replaced), one wave that is
+ * recorded whole; the seeds run from desc->seed.  On `stream` (NULL: the
+ * scene's); waits for the passes; *passes (when not NULL) = passes rendered. */
+int cr_guide_train(cr_scene *s, const cr_render_desc *desc, void *stream, uint32_t *passes);
 /* Weighted NLL (normalised by the batch weight) of the last training batch. */
 int cr_guide_loss(const cr_scene *s, float *loss);
 /* Copy the parameters out (set = 0) or in (set = 1); NULL arrays are skipped.

@@ -263,3 +263,32 @@ def test_guided_render_is_unbiased(cr, scenes, guided_bounces):
     diff = guided.mean.sum() - plain.mean.sum()
     se = np.sqrt((guided.var_of_mean + plain.var_of_mean).sum())
     assert abs(diff) < 4 * se, (diff / se, guided.mean.mean(), plain.mean.mean())
+
+
+def test_guide_train_spends_the_budget_exactly(cr, scenes):
+    """cr_guide_train: scratch passes of about one recorded wave each until the
+    budget is spent, then guided renders run with the frozen guide; a guide
+    without a budget is refused."""
+    require_gpu()
+    import torch
+    s = cr.Scene.from_desc(scenes.config0())
+    try:
+        g = cr.Guide(s).reset(seed=3)
+        g.configure(max_steps=96, steps_per_wave=16, train_paths=8192, warmup_steps=4)
+        d = cr.render_desc(256, 256, 1, max_bounce=7, estimator=cr.MIS, seed=9, guiding=True)
+        passes = g.train(d)
+        # 16 x 8192 = 131,072 paths per pass at 2 spp of 256 x 256: 16 steps per pass
+        assert g.info()["step"] == 96 and passes == 6
+        f = [torch.zeros(256 * 256 * 3, dtype=torch.float64, device="cuda"),
+             torch.zeros(256 * 256 * 3, dtype=torch.float64, device="cuda"),
+             torch.zeros(256 * 256, dtype=torch.int32, device="cuda")]
+        d4 = cr.render_desc(256, 256, 4, max_bounce=7, estimator=cr.MIS, seed=11, guiding=True)
+        s.render_device(d4, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr())
+        torch.cuda.synchronize()
+        assert g.info()["step"] == 96  # frozen
+        assert np.isfinite(f[0].cpu().numpy()).all() and int(f[2].sum().item()) > 0
+        g.configure(max_steps=0)
+        with pytest.raises(cr.CrError):
+            g.train(d)
+    finally:
+        s.close()
