@@ -100,28 +100,29 @@ struct HostCamera
 	int lens = 0;  // 0 pinhole, 1 orthographic
 };
 
+// A scene's device array: stream-ordered from the library's memory pool and
+// freed on the same stream (a synchronous cudaFree of a scene's arrays stalled
+// scene destruction for up to 0.6 s).
 template <typename T>
 struct DevBuf
 {
 	T *p = nullptr;
 	size_t n = 0;
-	void upload( const std::vector<T> &h )
+	void upload( const std::vector<T> &h, cudaStream_t st )
 	{
-		release();
-		n = h.size();
-		if ( !n ) return;
-		cuda_check( cudaMalloc( (void **)&p, sizeof( T ) * n ), "cudaMalloc" );
-		cuda_check( cudaMemcpy( p, h.data(), sizeof( T ) * n, cudaMemcpyHostToDevice ), "upload" );
+		alloc( h.size(), st );
+		if ( n ) cuda_check( cudaMemcpyAsync( p, h.data(), sizeof( T ) * n, cudaMemcpyHostToDevice, st ), "upload" );
 	}
-	void alloc( size_t count )
+	void alloc( size_t count, cudaStream_t st )
 	{
-		release();
+		release( st );
 		n = count;
-		if ( n ) cuda_check( cudaMalloc( (void **)&p, sizeof( T ) * n ), "cudaMalloc" );
+		if ( n ) cuda_check( cudaMallocAsync( (void **)&p, sizeof( T ) * n, device_pool(), st ), "cudaMalloc" );
 	}
-	void release()
+	// freed in the order of `st`, after the work queued there
+	void release( cudaStream_t st )
 	{
-		if ( p ) cudaFree( p );
+		if ( p ) cudaFreeAsync( p, st );
 		p = nullptr;
 		n = 0;
 	}
@@ -180,8 +181,9 @@ struct cr_scene
 		if ( bvh.nodes ) cudaFreeAsync( bvh.nodes, stream );
 		if ( bvh.tris ) cudaFreeAsync( bvh.tris, stream );
 		bvh = WideBvh();
-		attrs.release(), light_tables.release(), light_tris.release(), light_cdf.release();
-		dspheres.release(), dshaders.release(), dlights.release(), prim_first.release(), err.release();
+		attrs.release( stream ), light_tables.release( stream ), light_tris.release( stream ), light_cdf.release( stream );
+		dspheres.release( stream ), dshaders.release( stream ), dlights.release( stream ), prim_first.release( stream );
+		err.release( stream );
 		if ( stream ) cudaStreamSynchronize( stream );
 		committed = false;
 	}
@@ -1087,7 +1089,7 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 			if ( p ) cudaFreeAsync( p, st );
 		}
 	} src_guard{ d_src, st };
-	s->attrs.alloc( 3 * nt );
+	s->attrs.alloc( 3 * nt, st );
 	float lo[ 3 ] = { INFINITY, INFINITY, INFINITY }, hi[ 3 ] = { -INFINITY, -INFINITY, -INFINITY };
 	if ( nt )
 	{
@@ -1161,14 +1163,14 @@ void commit( cr_scene *s, uint64_t light_seed, cudaStream_t user_stream )
 	std::vector<DevShader> dsh;
 	for ( auto &x : s->shaders ) dsh.push_back( x.second );
 
-	s->dspheres.upload( ds );
-	s->dshaders.upload( dsh );
-	s->dlights.upload( lights );
-	s->light_tables.upload( tables );
-	s->light_tris.upload( ltris );
-	s->light_cdf.upload( cdf );
-	s->prim_first.upload( prim_first );
-	s->err.upload( std::vector<uint32_t>( 2, 0 ) );  // [0] error word, [1] query work cursor
+	s->dspheres.upload( ds, st );
+	s->dshaders.upload( dsh, st );
+	s->dlights.upload( lights, st );
+	s->light_tables.upload( tables, st );
+	s->light_tris.upload( ltris, st );
+	s->light_cdf.upload( cdf, st );
+	s->prim_first.upload( prim_first, st );
+	s->err.upload( std::vector<uint32_t>( 2, 0 ), st );  // [0] error word, [1] query work cursor
 	s->lights = lights;
 	s->tables_host = tables;
 	s->prim_light = prim_light;
