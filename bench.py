@@ -23,10 +23,13 @@ cpu_baseline / --impl reference
            sample of the same workload (full resolution, fewer spp).
 batch      the batched workload (64 scenes of uneven size, resolution and spp)
            as one batch replayed from a CUDA graph, against one call per
-           scene; rank 0 at N = 1 only.
+           scene; the closest-hit L2 roofline over the batch's scenes and the
+           reference on a window of every 8th scene; rank 0 at N = 1 only.
 guiding    time to relMSE 1e-3, plain MIS vs learned guiding (tensor-core
            inference and online training included), on the occluded-light
-           scene at 1024x1024 (see guided_vs_plain); rank 0 at N = 1 only.
+           scene at 1024x1024 (see guided_vs_plain); the guide inference
+           kernel's tensor and L2 rooflines and the reference on a 1-spp
+           render of the scene; rank 0 at N = 1 only.
 config0    the small box scene at its full configuration (256x256, 64 spp,
            depth 8), the one workload both arms run identically: device and
            end-to-end rates, the L2 roofline, the reference on the same
@@ -56,6 +59,9 @@ WIDTH, HEIGHT, SPP, LEVEL, MAX_BOUNCE = 1024, 768, 256, 8, 7
 METRIC = ("Msamples/s (camera paths per second), plain wavefront, 1024x768x256spp, 1.31M-tri displaced icosphere; "
           "time-to-relMSE 1e-3 guided vs plain in 'guiding'")
 NODE_BYTES, TRI_BYTES, RAY_BYTES = 80, 48, 32 + 16
+# the guide's MLP: 5 layers of 64 x 64 (2 FLOP per multiply-add) per inferred
+# path, and 48 hash-grid gathers (12 levels x 4 cell edges) to encode it
+GUIDE_FLOPS_PER_ROW, GUIDE_GATHERS_PER_ROW = 2 * 64 * 64 * 5, 48
 C0_WORKLOAD = ("config0: box scene (20 triangles, 2 spheres, ceiling light), 256x256 at 64 spp, depth 8, "
                "reference estimator")
 
@@ -163,6 +169,15 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def measured_bf16():
+    """Dense BF16 tensor-core peak (burst, TFLOP/s) from the driver's measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
 def profiled_traffic(name="k_extend_traffic.json"):
     """DRAM bytes per k_extend ray from a committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", name)
@@ -197,6 +212,26 @@ def reference_rate(scene_json, steps, warmup, spp, width=WIDTH, height=HEIGHT):
     # threads; the last core spins its progress bar (cpuMulticore.cu:19-21,76-114).
     used = max(1, min(threads, (os.cpu_count() or 1) - 1))
     return samples / secs / 1e6, secs / max(len(timed), 1), used, samples // max(len(timed), 1)
+
+
+def reference_window(desc, spp, max_bounce, win=None):
+    """The reference's CPUMulticoreTracer::execute on all host threads over the
+    pixel window win = (x0, y0, x1, y1) of desc's image (the whole image when
+    None), through the profiler area the harness implements
+    (cpuMulticore.cu:17).  Scene load and BVH build are not timed.  Returns
+    (samples, seconds, threads used)."""
+    import oracle
+    from cuda_raytracer_b200 import scenes
+    threads = os.cpu_count() or 1
+    area = [str(v) for v in win] if win else []
+    with tempfile.TemporaryDirectory() as tmp:
+        path = scenes.write_scene(desc, tmp)
+        r = subprocess.run([oracle.REF_BIN, "bench", os.path.basename(path), str(desc.width), str(desc.height),
+                            str(spp), str(threads), str(max_bounce), "1", *area],
+                           cwd=tmp, capture_output=True, text=True, timeout=1800, check=True)
+    run_ = [json.loads(l) for l in r.stderr.splitlines() if l.startswith("{")][-1]
+    # CPUMulticoreTracer runs min(hardware_concurrency()-1, maxThreads) tracer threads
+    return run_["samples"], run_["seconds"], max(1, min(threads, threads - 1))
 
 
 def layout_comparison(scene, desc, scene_json, n=4096, seed=5):
@@ -302,7 +337,7 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------- our arm
-def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
+def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3, l2_gbs=None, with_reference=False):
     """Time to relMSE <= target, plain MIS vs learned guiding, on the
     occluded-light scene (1024x1024, ~492k triangles, max depth 8).
 
@@ -388,6 +423,32 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
     plain_no_rr = run(False, rr_start=MAX_BOUNCE + 1)
     guided = run(True)
     g = cr.Guide(sc)
+    # the guide's inference kernel (k_guide_infer) on the trained guide: one
+    # 4-spp guided render with stage timing gives its launches, rows and time
+    F = film()
+    st = sc.render_device(cr.render_desc(res, res, 4, max_bounce=MAX_BOUNCE, estimator=cr.MIS, seed=777_777,
+                                         guiding=True), F[0].data_ptr(), F[1].data_ptr(), F[2].data_ptr(),
+                          stream=stream)
+    torch.cuda.synchronize(dev)
+    del F
+    launches = max(st.guide_launches, 1)
+    infer_ms = (st.ms_guide - st.ms_guide_train) / launches
+    rows = st.guide_rows / launches
+    tflops = rows * GUIDE_FLOPS_PER_ROW / (infer_ms / 1e3) / 1e12
+    sector_gbs = rows * GUIDE_GATHERS_PER_ROW * 32 / (infer_ms / 1e3) / 1e9
+    bf16, bf16_kind = measured_bf16()
+    roofline = {"kernel": "k_guide_infer", "bound": "l2 (hash-grid gathers)", "launches": st.guide_launches,
+                "rows_per_launch": round(rows), "launch_ms": round(infer_ms, 4),
+                "ms_per_4spp_render": round(st.ms_total, 2), "ms_guide_per_4spp_render": round(st.ms_guide, 2),
+                "tensor": {"achieved": round(tflops, 2), "peak": bf16, "unit": "TFLOP/s", "frac": round(tflops / bf16, 4),
+                           "peak_source": bf16_kind,
+                           "flops_per_unit": f"{GUIDE_FLOPS_PER_ROW} per row (5 BF16 layers of 64 x 64)"},
+                "l2": {"achieved": round(sector_gbs, 1), "peak": round(l2_gbs, 1) if l2_gbs else None, "unit": "GB/s",
+                       "frac": round(sector_gbs / l2_gbs, 4) if l2_gbs else None,
+                       "peak_source": "measured in this run (cr_measure_peaks: 32 MB L2-resident reads)",
+                       "bytes_per_unit": f"{GUIDE_GATHERS_PER_ROW} random 8-byte hash-grid gathers per row (FP16 "
+                                         "feature pairs of 12 levels x 4 cell edges), counted as the 32-byte "
+                                         "sectors they touch"}}
     best = [x["time_to_target_s"] for x in (plain, plain_no_rr) if x["time_to_target_s"]]
     out = {"workload": "config3: occluded light (wall with a 0.4x0.4 aperture), 1024x1024, "
                        f"{sc.info()['triangles']} triangles, max depth 8, MIS estimator",
@@ -398,7 +459,17 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3):
            "speedup": (round(min(best) / guided["time_to_target_s"], 3)
                        if best and guided["time_to_target_s"] else None),
            "speedup_vs_plain_reference_roulette": (round(plain["time_to_target_s"] / guided["time_to_target_s"], 3)
-                                                   if plain["time_to_target_s"] and guided["time_to_target_s"] else None)}
+                                                   if plain["time_to_target_s"] and guided["time_to_target_s"] else None),
+           "roofline": roofline}
+    if with_reference:
+        import oracle
+        if oracle.ref_available():
+            samples, secs, cores = reference_window(d, 1, MAX_BOUNCE)
+            out["cpu_baseline"] = {"value": round(samples / secs / 1e6, 4), "unit": "Msamples/s", "cores": cores,
+                                   "kind": "reference",
+                                   "sample": f"the whole {res}x{res} image at 1 spp with the reference's own "
+                                             "estimator (it has no MIS or guiding), same scene and depth; scene "
+                                             "load and BVH build excluded"}
     sc.close()
     return out
 
@@ -488,7 +559,7 @@ def config0_section(cr, dev, steps, warmup, l2_gbs, with_reference):
     return out
 
 
-def batched_workload(cr, dev, n_scenes, seed=2):
+def batched_workload(cr, dev, n_scenes, seed=2, l2_gbs=None, with_reference=False):
     """The batched workload: n_scenes seeded scenes (triangle counts
     log-uniform in [1e3, 2e6], square images log-uniform 128..1024, spp from
     {16..256}, 1-4 lights) rendered as one batch replayed from a CUDA graph,
@@ -521,6 +592,30 @@ def batched_workload(cr, dev, n_scenes, seed=2):
     e1.record()
     torch.cuda.synchronize(dev)
     ms_single = e0.elapsed_time(e1)
+    # closest-hit roofline over the batch's scenes: per scene, a timed pass and
+    # a counting pass over the same rays (spp / 16, same seed); the graph's
+    # replay carries no per-kernel timing, and its traversal is the same
+    # kernel over queues that mix the scenes' rays
+    ext_ms, ext_bytes, ext_launches = 0.0, 0.0, 0
+    for (sc, w, h, spp, sd, *_), f in zip(jobs, films):
+        kw = dict(max_bounce=MAX_BOUNCE, estimator=cr.KOISHI, seed=sd + 3)
+        sp = max(1, spp // 16)
+        st_t = sc.render_device(cr.render_desc(w, h, sp, **kw), f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(),
+                                stream=stream)
+        st_c = sc.render_device(cr.render_desc(w, h, sp, count_work=True, **kw), f[0].data_ptr(), f[1].data_ptr(),
+                                f[2].data_ptr(), stream=stream)
+        ext_ms += st_t.ms_extend
+        ext_launches += st_t.extend_launches
+        ext_bytes += st_c.nodes * NODE_BYTES + st_c.tris * TRI_BYTES + st_c.rays_extend * RAY_BYTES
+    achieved = ext_bytes / (ext_ms / 1e3) / 1e9
+    hbm, hbm_kind = measured_peaks()
+    roofline = {"bound": "l2", "kernel": "k_extend (per-scene passes over the batch's scenes at spp / 16)",
+                "achieved": round(achieved, 1), "peak": round(l2_gbs, 1) if l2_gbs else None, "unit": "GB/s",
+                "frac": round(achieved / l2_gbs, 4) if l2_gbs else None,
+                "peak_source": "measured in this run (cr_measure_peaks: 32 MB L2-resident reads)",
+                "hbm": {"peak": hbm, "frac": round(achieved / hbm, 4), "peak_source": hbm_kind},
+                "launches": ext_launches, "launch_ms": round(ext_ms / max(ext_launches, 1), 4),
+                "algorithmic_bytes": round(ext_bytes)}
     out = {"workload": f"config2: {n_scenes} scenes, {sum(d.n_triangles for d in descs)} triangles, "
                        f"{total} samples per replay, depth 8, reference estimator",
            "msamples_per_s": round(total / st.ms_total / 1e3, 2), "ms_per_replay": round(st.ms_total, 2),
@@ -528,8 +623,26 @@ def batched_workload(cr, dev, n_scenes, seed=2):
            "speedup_vs_per_scene_calls": round(ms_single / st.ms_total, 3),
            "graph_nodes": st.graph_nodes, "kernel_launches_per_replay": st.launches, "waves": st.waves,
            "autotuned": tune,
-           "scene_build_s": round(t_build, 1)}
+           "scene_build_s": round(t_build, 1),
+           "roofline": roofline}
     b.close()
+    if with_reference:
+        import oracle
+        if oracle.ref_available():
+            # every 8th scene, its central 32 x 32 window at the scene's own spp
+            samples, secs, cores, t1 = 0, 0.0, 1, time.perf_counter()
+            picked = list(range(0, n_scenes, 8))
+            for i in picked:
+                d = descs[i]
+                x0, y0 = d.width // 2 - 16, d.height // 2 - 16
+                n_, s_, cores = reference_window(d, d.spp, MAX_BOUNCE, (x0, y0, x0 + 32, y0 + 32))
+                samples, secs = samples + n_, secs + s_
+            out["cpu_baseline"] = {"value": round(samples / secs / 1e6, 4), "unit": "Msamples/s", "cores": cores,
+                                   "kind": "reference",
+                                   "sample": f"scenes {picked} of the batch, each its central 32x32 window at its "
+                                             f"own spp through the reference's profiler area ({samples} paths, "
+                                             f"{secs:.1f} s of rendering; scene load and BVH build excluded, "
+                                             f"{time.perf_counter() - t1:.0f} s wall in all)"}
     return out
 
 
@@ -886,10 +999,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and args.guide_seconds > 0:
         del s, q, c, flush
         torch.cuda.empty_cache()
-        guiding = guided_vs_plain(cr, dev, args.guide_seconds, args.guide_ref_spp)
+        guiding = guided_vs_plain(cr, dev, args.guide_seconds, args.guide_ref_spp, l2_gbs=l2_gbs,
+                                  with_reference=not args.no_cpu_baseline)
     batch = None
     if rank == 0 and world == 1 and args.batch_scenes > 0:
-        batch = batched_workload(cr, dev, args.batch_scenes)
+        batch = batched_workload(cr, dev, args.batch_scenes, l2_gbs=l2_gbs, with_reference=not args.no_cpu_baseline)
     c4 = None
     if rank == 0 and world == 1 and not args.no_config4:
         torch.cuda.empty_cache()

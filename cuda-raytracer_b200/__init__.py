@@ -73,7 +73,7 @@ class Stats(C.Structure):
                 ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64), ("nodes", C.c_uint64),
                 ("tris", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_tris", C.c_uint64), ("launches", C.c_uint32), ("waves", C.c_uint32),
                 ("extend_launches", C.c_uint32), ("shadow_launches", C.c_uint32), ("ms_guide_train", C.c_double),
-                ("graph_nodes", C.c_uint32)]
+                ("graph_nodes", C.c_uint32), ("guide_launches", C.c_uint32), ("guide_rows", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1379,6 +1379,7 @@ void fill_stats( cr_stats *out, const StageTimes &t, uint64_t samples )
 	out->nodes = t.nodes, out->tris = t.tris, out->shadow_nodes = t.shadow_nodes, out->shadow_tris = t.shadow_tris;
 	out->launches = t.launches, out->waves = t.waves;
 	out->extend_launches = t.extend_launches, out->shadow_launches = t.shadow_launches;
+	out->guide_launches = t.guide_launches, out->guide_rows = t.guide_rows;
 }
 
 void render_device( cr_scene *s, const cr_render_desc *desc, double *sum, double *sq, uint32_t *cnt, cudaStream_t st,

@@ -1830,6 +1830,7 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 		times->launches++;
 		if ( kind == 0 ) times->extend_launches++;
 		if ( kind == 1 ) times->shadow_launches++;
+		if ( kind == 4 ) times->guide_launches++;
 	};
 	std::vector<uint32_t> host_counts;
 	for ( uint64_t first = 0; first < total; first += P )
@@ -1953,6 +1954,9 @@ void render_waves( const DevScene &sc, const RenderConfig &cfg, WaveBuffers &wb,
 			{
 				times->rays_extend += host_counts[ CPB * b + CNT_EXT ];
 				times->rays_shadow += host_counts[ CPB * b + CNT_SHADOW ];
+				// the guide's inference runs on the bounce's whole extension queue
+				if ( wc.guide_sample && guided_vertex( wc.guide, b, cfg.max_bounce ) )
+					times->guide_rows += host_counts[ CPB * b + CNT_EXT ];
 			}
 		}
 	}

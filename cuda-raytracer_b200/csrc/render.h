@@ -118,8 +118,8 @@ struct RenderConfig
 struct StageTimes
 {
 	double extend = 0, shadow = 0, shade = 0, other = 0, total = 0, guide = 0, guide_train = 0;
-	uint32_t launches = 0, waves = 0, extend_launches = 0, shadow_launches = 0;
-	uint64_t rays_extend = 0, rays_shadow = 0, nodes = 0, tris = 0, shadow_nodes = 0, shadow_tris = 0;
+	uint32_t launches = 0, waves = 0, extend_launches = 0, shadow_launches = 0, guide_launches = 0;
+	uint64_t rays_extend = 0, rays_shadow = 0, nodes = 0, tris = 0, shadow_nodes = 0, shadow_tris = 0, guide_rows = 0;
 };
 
 void alloc_wave( WaveBuffers &wb, uint32_t capacity, uint32_t max_bounce, cudaStream_t st );

@@ -111,6 +111,8 @@ typedef struct cr_stats {
     uint32_t graph_nodes;  /* cr_batch_render: kernel nodes of the replayed CUDA graph
                               (an initialising kernel and the wave loop's body, which
                               runs once per wave); 0 for other calls            */
+    uint32_t guide_launches; /* guide inference launches (one per guided bounce of a wave) */
+    uint64_t guide_rows;     /* paths the guide's inference ran on (its rows)  */
 } cr_stats;
 
 /* ------------------------------------------------------------------ errors */

@@ -283,9 +283,14 @@ def test_guide_train_spends_the_budget_exactly(cr, scenes):
              torch.zeros(256 * 256 * 3, dtype=torch.float64, device="cuda"),
              torch.zeros(256 * 256, dtype=torch.int32, device="cuda")]
         d4 = cr.render_desc(256, 256, 4, max_bounce=7, estimator=cr.MIS, seed=11, guiding=True)
-        s.render_device(d4, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr())
+        st = s.render_device(d4, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr())
         torch.cuda.synchronize()
         assert g.info()["step"] == 96  # frozen
+        # inference on bounces 0..6 of every wave (never the last vertex), on
+        # each bounce's whole extension queue; no training time once frozen
+        assert st.guide_launches == 7 * st.waves
+        assert st.samples <= st.guide_rows < st.rays_extend
+        assert st.ms_guide > 0 and st.ms_guide_train == 0
         assert np.isfinite(f[0].cpu().numpy()).all() and int(f[2].sum().item()) > 0
         g.configure(max_steps=0)
         with pytest.raises(cr.CrError):
