@@ -179,7 +179,7 @@ def measured_bf16():
 
 
 def profiled_traffic(name="k_extend_traffic.json"):
-    """DRAM bytes per k_extend ray from a committed ncu summary, if any."""
+    """DRAM bytes per unit (ray or row) of a kernel from a committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as fh:
@@ -437,8 +437,13 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3, l2_gbs=None, with_ref
     tflops = rows * GUIDE_FLOPS_PER_ROW / (infer_ms / 1e3) / 1e12
     sector_gbs = rows * GUIDE_GATHERS_PER_ROW * 32 / (infer_ms / 1e3) / 1e9
     bf16, bf16_kind = measured_bf16()
+    gtraffic = profiled_traffic("k_guide_infer_traffic.json")
     roofline = {"kernel": "k_guide_infer", "bound": "l2 (hash-grid gathers)", "launches": st.guide_launches,
                 "rows_per_launch": round(rows), "launch_ms": round(infer_ms, 4),
+                "traffic": round(gtraffic["dram_bytes_per_row"] * rows) if gtraffic else None,
+                "traffic_note": ("ncu DRAM bytes per row over the 7 inference launches of one captured 4-spp guided "
+                                 "render of this scene (profiles/k_guide_infer_traffic.json), scaled to this run's "
+                                 "rows per launch") if gtraffic else None,
                 "ms_per_4spp_render": round(st.ms_total, 2), "ms_guide_per_4spp_render": round(st.ms_guide, 2),
                 "tensor": {"achieved": round(tflops, 2), "peak": bf16, "unit": "TFLOP/s", "frac": round(tflops / bf16, 4),
                            "peak_source": bf16_kind,
@@ -1070,6 +1075,46 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def profile_case(name):
+    """Small cases for the ncu captures summarised under profiles/ (a few GB on
+    the device, seconds of GPU work).  Each render prints one JSON line with
+    its stats, so that captured launches can be mapped to renders.
+
+    guide_infer     the occluded-light scene at 1024x1024 with a fresh guide
+                    (seed 7, the library's guiding defaults): five guided MIS
+                    renders of 4 spp, one wave each.  The first wave trains
+                    without sampling the guide; each later one runs
+                    k_guide_infer on bounces 0-6.
+    config4_extend  the large combined scene (21M triangles): one 1-spp MIS
+                    render of the 3840x2160 image at max_bounce 11."""
+    import torch
+    cr = load_pkg()
+    from cuda_raytracer_b200 import scenes
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    if name == "guide_infer":
+        d = scenes.config3(width=1024, height=1024)
+        renders = [cr.render_desc(1024, 1024, 4, max_bounce=MAX_BOUNCE, estimator=cr.MIS, seed=100 + k, guiding=True)
+                   for k in range(5)]
+    else:
+        d = scenes.config4()
+        renders = [cr.render_desc(3840, 2160, 1, max_bounce=11, estimator=cr.MIS, seed=4242)]
+    sc = cr.Scene.from_desc(d)
+    if name == "guide_infer":
+        cr.Guide(sc).reset(seed=7)
+    n = renders[0].width * renders[0].height
+    f = [torch.zeros(n * 3, dtype=torch.float64, device=dev), torch.zeros(n * 3, dtype=torch.float64, device=dev),
+         torch.zeros(n, dtype=torch.int32, device=dev)]
+    for k, rd in enumerate(renders):
+        st = sc.render_device(rd, f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), stream=stream)
+        torch.cuda.synchronize(dev)
+        print(json.dumps({"case": name, "render": k, "waves": st.waves, "extend_launches": st.extend_launches,
+                          "rays_extend": st.rays_extend, "guide_launches": st.guide_launches,
+                          "guide_rows": st.guide_rows, "ms_total": round(st.ms_total, 3)}), flush=True)
+    sc.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1090,10 +1135,14 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (0: skip it)")
     ap.add_argument("--workload", choices=["config1", "config4"], default="config1",
                     help="config1: the headline 1024x768x256spp line; config4: the large combined run")
+    ap.add_argument("--profile-case", choices=["guide_infer", "config4_extend"], default=None,
+                    help="run one small case for an ncu capture (profiles/) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile_case:
+        profile_case(args.profile_case)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "config4":
         run_config4(args)
