@@ -199,3 +199,35 @@ def test_tracer_plugin_builds_into_the_reference():
     assert os.path.exists(exe)
     r = subprocess.run(["ldd", exe], capture_output=True, text=True)
     assert "libcr_b200.so" in r.stdout and "not found" not in r.stdout, r.stdout
+
+
+def _header_struct_fields(text, name):
+    """(field, C type) pairs of `typedef struct name { ... } name;` in order,
+    comments removed; `uint32_t a, b;` gives two fields, pointers read as "*"."""
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    out = []
+    for decl in (d.strip() for d in body.split(";")):
+        if not decl:
+            continue
+        m = re.match(r"([A-Za-z_][A-Za-z_0-9]*)\s*(\*?)\s*(.*)", decl)
+        ctype = "*" if m.group(2) else m.group(1)
+        for nm in m.group(3).split(","):
+            out.append((nm.strip(), ctype))
+    return out
+
+
+def test_ctypes_mirrors_match_the_header(cr):
+    """Every struct the package passes through the C ABI has the header's
+    fields, in the header's order, with the same widths: the library writes
+    whole structs (cr_stats is cleared with memset), so a shorter mirror would
+    be overwritten past its end."""
+    ctype = {"int32_t": C.c_int32, "uint32_t": C.c_uint32, "uint64_t": C.c_uint64, "float": C.c_float,
+             "double": C.c_double, "*": C.c_void_p}
+    with open(os.path.join(ROOT, "include", "cr.h")) as fh:
+        text = fh.read()
+    pairs = {"cr_hit": cr.Hit, "cr_render_desc": cr.RenderDesc, "cr_tuning": cr.Tuning, "cr_stats": cr.Stats,
+             "cr_guide_config": cr.GuideConfig, "cr_build_config": cr.BuildConfig, "cr_batch_job": cr.BatchJob}
+    for cname, py in pairs.items():
+        want = [(n, ctype[t]) for n, t in _header_struct_fields(text, cname)]
+        assert list(py._fields_) == want, cname
