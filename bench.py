@@ -432,13 +432,13 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3, l2_gbs=None, with_ref
     torch.cuda.synchronize(dev)
     del F
     launches = max(st.guide_launches, 1)
-    infer_ms = (st.ms_guide - st.ms_guide_train) / launches
+    infer_ms = max(st.ms_guide - st.ms_guide_train, 1e-6) / launches
     rows = st.guide_rows / launches
     tflops = rows * GUIDE_FLOPS_PER_ROW / (infer_ms / 1e3) / 1e12
     sector_gbs = rows * GUIDE_GATHERS_PER_ROW * 32 / (infer_ms / 1e3) / 1e9
     bf16, bf16_kind = measured_bf16()
     gtraffic = profiled_traffic("k_guide_infer_traffic.json")
-    roofline = {"kernel": "k_guide_infer", "bound": "l2 (hash-grid gathers)", "launches": st.guide_launches,
+    roofline = None if st.guide_launches == 0 else {"kernel": "k_guide_infer", "bound": "l2 (hash-grid gathers)", "launches": st.guide_launches,
                 "rows_per_launch": round(rows), "launch_ms": round(infer_ms, 4),
                 "traffic": round(gtraffic["dram_bytes_per_row"] * rows) if gtraffic else None,
                 "traffic_note": ("ncu DRAM bytes per row over the 7 inference launches of one captured 4-spp guided "
@@ -1111,7 +1111,9 @@ def profile_case(name):
         torch.cuda.synchronize(dev)
         print(json.dumps({"case": name, "render": k, "waves": st.waves, "extend_launches": st.extend_launches,
                           "rays_extend": st.rays_extend, "guide_launches": st.guide_launches,
-                          "guide_rows": st.guide_rows, "ms_total": round(st.ms_total, 3)}), flush=True)
+                          "guide_rows": st.guide_rows, "ms_total": round(st.ms_total, 3),
+                          "ms_guide": round(st.ms_guide, 3), "ms_guide_train": round(st.ms_guide_train, 3)}),
+              flush=True)
     sc.close()
 
 
