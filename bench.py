@@ -170,7 +170,8 @@ def measured_peaks():
 
 
 def measured_bf16():
-    """Dense BF16 tensor-core peak (burst, TFLOP/s) from the driver's measurement."""
+    """Dense BF16 tensor-core peak (burst, TFLOP/s) measured on this GPU type
+    (MEASURED_PEAKS.json), else an earlier measurement of the same part."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
             return float(json.load(fh)["bf16_tflops"]), "measured"
@@ -438,7 +439,8 @@ def guided_vs_plain(cr, dev, tmax_s, ref_spp, target=1e-3, l2_gbs=None, with_ref
     sector_gbs = rows * GUIDE_GATHERS_PER_ROW * 32 / (infer_ms / 1e3) / 1e9
     bf16, bf16_kind = measured_bf16()
     gtraffic = profiled_traffic("k_guide_infer_traffic.json")
-    roofline = None if st.guide_launches == 0 else {"kernel": "k_guide_infer", "bound": "l2 (hash-grid gathers)", "launches": st.guide_launches,
+    roofline = None if st.guide_launches == 0 else {
+                "kernel": "k_guide_infer", "bound": "l2 (hash-grid gathers)", "launches": st.guide_launches,
                 "rows_per_launch": round(rows), "launch_ms": round(infer_ms, 4),
                 "traffic": round(gtraffic["dram_bytes_per_row"] * rows) if gtraffic else None,
                 "traffic_note": ("ncu DRAM bytes per row over the 7 inference launches of one captured 4-spp guided "

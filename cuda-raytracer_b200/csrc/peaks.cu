@@ -1,4 +1,5 @@
-// Microbenchmarks for the rooflines the driver's measured peaks do not give:
+// Microbenchmarks for the rooflines that the measured HBM copy and BF16 GEMM
+// peaks (MEASURED_PEAKS.json) do not give:
 // L2-resident read bandwidth, random record gathers from L2 (the access
 // pattern of BVH traversal) and FP32 FMA throughput, measured in the same
 // process as the kernels they are compared with.
